@@ -1,0 +1,10 @@
+"""B200-native SCB transport sweep and QD-factor moments for the 2D TRT solver of
+jmc9/2D_TRT_ROM_System (drop-in for MODULE TRANSPORT_SOLVES and the QD-factor routines).
+
+The compute path is libtrt_sweep.so (CUDA, sm_100a) behind the C ABI of include/trt_sweep.h; this
+package is its Python mirror plus the problem and quadrature generators used by tests and the bench.
+"""
+from . import problems, quadrature  # noqa: F401
+from .api import (COLLAPSE_INTENSITIES, GQD_In_Calc, MGQD_In_Calc, RT_BC_UPDATE, TRANSPORT_SCB,  # noqa: F401
+                  Bg_planck_calc, Cg_Calc, TransportSweep, fg_Calc, kernel_launches, required_bytes)
+from ._lib import LIB_PATH, TrtError, lib  # noqa: F401

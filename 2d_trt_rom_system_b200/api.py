@@ -1,0 +1,298 @@
+"""Python mirror of the reference interface for the sweep path, over the C ABI (include/trt_sweep.h).
+
+Reference-signature functions take numpy arrays in the reference's Fortran layouts (shape (nx, ny, ...)
+with order='F'), in the argument order of the Fortran subroutine they replace; INTENT(OUT) arrays are
+passed in and filled, as in Fortran.  ``TransportSweep`` wraps the resident-state handle.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, dptr, iptr
+
+
+def _f64(a, shape=None):
+    a = np.asarray(a, dtype=np.float64)
+    if shape is not None and a.shape != tuple(shape):
+        raise ValueError(f"expected shape {tuple(shape)}, got {a.shape}")
+    return np.asfortranarray(a)
+
+
+def _out(a, shape):
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.f_contiguous and a.shape == tuple(shape)):
+        raise ValueError(f"output must be a Fortran-ordered float64 array of shape {tuple(shape)}")
+    return a
+
+
+# --------------------------------------------------------------------------------------------
+# Reference-signature entry points
+# --------------------------------------------------------------------------------------------
+def TRANSPORT_SCB(I_avg, I_edgV, I_edgH, I_crn, Ic_edgV, Ic_edgH, Omega_x, Omega_y, Delx, Dely, A, KapE_in, Src_in,
+                  I_crn_old, c, Delt, Open_Threads, RT_Residual, RT_ResLoc_x, RT_ResLoc_y, Res_Calc):
+    """SUBROUTINE TRANSPORT_SCB, MainSrc/TRANSPORT_SOLVES.f08:14-327."""
+    nx, ny = len(Delx), len(Dely)
+    nm, ng = I_avg.shape[2], I_avg.shape[3]
+    _out(I_avg, (nx, ny, nm, ng)); _out(I_edgV, (nx + 1, ny, nm, ng)); _out(I_edgH, (nx, ny + 1, nm, ng))
+    _out(I_crn, (2 * nx, 2 * ny, nm, ng)); _out(Ic_edgV, (nx + 1, 2 * ny, nm, ng)); _out(Ic_edgH, (2 * nx, ny + 1, nm, ng))
+    ox, oy, dx, dy = _f64(Omega_x, (nm,)), _f64(Omega_y, (nm,)), _f64(Delx), _f64(Dely)
+    A_, K, S, Io = _f64(A, (nx, ny)), _f64(KapE_in, (nx, ny, ng)), _f64(Src_in, (2 * nx, 2 * ny, nm, ng)), \
+        _f64(I_crn_old, (2 * nx, 2 * ny, nm, ng))
+    if Res_Calc:
+        _out(RT_Residual, (4, ng, 5))
+        assert RT_ResLoc_x.dtype == np.int32 and RT_ResLoc_y.dtype == np.int32
+    rc = _lib.lib().trt_transport_scb(nx, ny, nm, ng, dptr(I_avg), dptr(I_edgV), dptr(I_edgH), dptr(I_crn),
+                                      dptr(Ic_edgV), dptr(Ic_edgH), dptr(ox), dptr(oy), dptr(dx), dptr(dy), dptr(A_),
+                                      dptr(K), dptr(S), dptr(Io), float(c), float(Delt), int(Open_Threads),
+                                      dptr(RT_Residual) if Res_Calc else None,
+                                      iptr(RT_ResLoc_x) if Res_Calc else None,
+                                      iptr(RT_ResLoc_y) if Res_Calc else None, 1 if Res_Calc else 0)
+    check(rc, "TRANSPORT_SCB")
+
+
+def COLLAPSE_INTENSITIES(Open_Threads, I_avg, I_edgV, I_edgH, Omega_x, Omega_y, quad_weight, Comp_Unit, Hg_avg_xx,
+                         Hg_avg_yy, Hg_avg_xy, Hg_edgV_xx, Hg_edgV_xy, Hg_edgH_yy, Hg_edgH_xy, Eg_edgV, Eg_edgH,
+                         Eg_avg, Fxg_edgV, Fyg_edgH, E_edgV, E_edgH, E_avg, Fx_edgV, Fy_edgH):
+    """SUBROUTINE COLLAPSE_INTENSITIES, MainSrc/TRANSPORT_SOLVES.f08:381-511."""
+    nx, ny, nm, ng = I_avg.shape
+    Ia, Iv, Ih = _f64(I_avg), _f64(I_edgV, (nx + 1, ny, nm, ng)), _f64(I_edgH, (nx, ny + 1, nm, ng))
+    outs = [Hg_avg_xx, Hg_avg_yy, Hg_avg_xy, Hg_edgV_xx, Hg_edgV_xy, Hg_edgH_yy, Hg_edgH_xy, Eg_edgV, Eg_edgH, Eg_avg,
+            Fxg_edgV, Fyg_edgH, E_edgV, E_edgH, E_avg, Fx_edgV, Fy_edgH]
+    A, V, H = (nx, ny), (nx + 1, ny), (nx, ny + 1)
+    shapes = [A + (ng,)] * 3 + [V + (ng,)] * 2 + [H + (ng,)] * 2 + [V + (ng,), H + (ng,), A + (ng,), V + (ng,),
+                                                                   H + (ng,), V, H, A, V, H]
+    for o, s in zip(outs, shapes):
+        _out(o, s)
+    rc = _lib.lib().trt_collapse_intensities(nx, ny, nm, ng, int(Open_Threads), dptr(Ia), dptr(Iv), dptr(Ih),
+                                             dptr(_f64(Omega_x)), dptr(_f64(Omega_y)), dptr(_f64(quad_weight)),
+                                             float(Comp_Unit), *[dptr(o) for o in outs])
+    check(rc, "COLLAPSE_INTENSITIES")
+
+
+def fg_Calc(fg_avg_xx, fg_avg_yy, fg_avg_xy, fg_edgV_xx, fg_edgV_xy, fg_edgH_yy, fg_edgH_xy, Hg_avg_xx, Hg_avg_yy,
+            Hg_avg_xy, Hg_edgV_xx, Hg_edgV_xy, Hg_edgH_yy, Hg_edgH_xy, HO_Eg_avg, HO_Eg_edgV, HO_Eg_edgH, c,
+            Open_Threads):
+    """SUBROUTINE fg_Calc, MainSrc/MLOQD_SOLVES.f08:619-678."""
+    nx, ny, ng = fg_avg_xx.shape
+    outs = [fg_avg_xx, fg_avg_yy, fg_avg_xy, fg_edgV_xx, fg_edgV_xy, fg_edgH_yy, fg_edgH_xy]
+    for o, s in zip(outs, [(nx, ny, ng)] * 3 + [(nx + 1, ny, ng)] * 2 + [(nx, ny + 1, ng)] * 2):
+        _out(o, s)
+    ins = [_f64(a) for a in (Hg_avg_xx, Hg_avg_yy, Hg_avg_xy, Hg_edgV_xx, Hg_edgV_xy, Hg_edgH_yy, Hg_edgH_xy,
+                             HO_Eg_avg, HO_Eg_edgV, HO_Eg_edgH)]
+    rc = _lib.lib().trt_fg_calc(nx, ny, ng, *[dptr(o) for o in outs], *[dptr(a) for a in ins], float(c),
+                                int(Open_Threads))
+    check(rc, "fg_Calc")
+
+
+def Cg_Calc(Cg_L, Cg_B, Cg_R, Cg_T, I_edgV, I_edgH, Omega_x, Omega_y, quad_weight, Comp_Unit, BC_Type, Open_Threads):
+    """SUBROUTINE Cg_Calc, MainSrc/MLOQD_SOLVES.f08:367-488."""
+    ny, ng = Cg_L.shape
+    nx = Cg_B.shape[0]
+    nm = len(quad_weight)
+    for o, s in zip((Cg_L, Cg_B, Cg_R, Cg_T), ((ny, ng), (nx, ng), (ny, ng), (nx, ng))):
+        _out(o, s)
+    bc = np.ascontiguousarray(BC_Type, dtype=np.int32)
+    rc = _lib.lib().trt_cg_calc(nx, ny, nm, ng, dptr(Cg_L), dptr(Cg_B), dptr(Cg_R), dptr(Cg_T),
+                                dptr(_f64(I_edgV, (nx + 1, ny, nm, ng))), dptr(_f64(I_edgH, (nx, ny + 1, nm, ng))),
+                                dptr(_f64(Omega_x)), dptr(_f64(Omega_y)), dptr(_f64(quad_weight)), float(Comp_Unit),
+                                iptr(bc), int(Open_Threads))
+    check(rc, "Cg_Calc")
+
+
+def MGQD_In_Calc(Eg_in_L, Eg_in_B, Eg_in_R, Eg_in_T, Fg_in_L, Fg_in_B, Fg_in_R, Fg_in_T, I_edgV, I_edgH, Omega_x,
+                 Omega_y, quad_weight, c, Comp_Unit, BC_Type, Open_Threads):
+    """SUBROUTINE MGQD_In_Calc, MainSrc/MLOQD_SOLVES.f08:493-614."""
+    ny, ng = Eg_in_L.shape
+    nx = Eg_in_B.shape[0]
+    nm = len(quad_weight)
+    outs = (Eg_in_L, Eg_in_B, Eg_in_R, Eg_in_T, Fg_in_L, Fg_in_B, Fg_in_R, Fg_in_T)
+    for o, s in zip(outs, ((ny, ng), (nx, ng)) * 4):
+        _out(o, s)
+    bc = np.ascontiguousarray(BC_Type, dtype=np.int32)
+    rc = _lib.lib().trt_mgqd_in_calc(nx, ny, nm, ng, *[dptr(o) for o in outs],
+                                     dptr(_f64(I_edgV, (nx + 1, ny, nm, ng))), dptr(_f64(I_edgH, (nx, ny + 1, nm, ng))),
+                                     dptr(_f64(Omega_x)), dptr(_f64(Omega_y)), dptr(_f64(quad_weight)), float(c),
+                                     float(Comp_Unit), iptr(bc), int(Open_Threads))
+    check(rc, "MGQD_In_Calc")
+
+
+def GQD_In_Calc(E_in_L, E_in_B, E_in_R, E_in_T, F_in_L, F_in_B, F_in_R, F_in_T, Eg_in_L, Eg_in_B, Eg_in_R, Eg_in_T,
+                Fg_in_L, Fg_in_B, Fg_in_R, Fg_in_T):
+    """SUBROUTINE GQD_In_Calc, MainSrc/GLOQD_SOLVES.f08:263-290."""
+    ny, ng = Eg_in_L.shape
+    nx = Eg_in_B.shape[0]
+    outs = (E_in_L, E_in_B, E_in_R, E_in_T, F_in_L, F_in_B, F_in_R, F_in_T)
+    for o, s in zip(outs, ((ny,), (nx,)) * 4):
+        _out(o, s)
+    ins = [_f64(a) for a in (Eg_in_L, Eg_in_B, Eg_in_R, Eg_in_T, Fg_in_L, Fg_in_B, Fg_in_R, Fg_in_T)]
+    rc = _lib.lib().trt_gqd_in_calc(nx, ny, ng, *[dptr(o) for o in outs], *[dptr(a) for a in ins])
+    check(rc, "GQD_In_Calc")
+
+
+def RT_BC_UPDATE(BC_Type, bcT_left, bcT_lower, bcT_right, bcT_upper, Comp_Unit, Nu_g, I_edgV, I_edgH, Ic_edgV,
+                 Ic_edgH):
+    """SUBROUTINE RT_BC_UPDATE, MainSrc/UPDATES.f08:12-105."""
+    nx = I_edgH.shape[0]
+    ny = I_edgV.shape[1]
+    nm, ng = I_edgV.shape[2], I_edgV.shape[3]
+    _out(I_edgV, (nx + 1, ny, nm, ng)); _out(I_edgH, (nx, ny + 1, nm, ng))
+    _out(Ic_edgV, (nx + 1, 2 * ny, nm, ng)); _out(Ic_edgH, (2 * nx, ny + 1, nm, ng))
+    bc = np.ascontiguousarray(BC_Type, dtype=np.int32)
+    rc = _lib.lib().trt_rt_bc_update(nx, ny, nm, ng, iptr(bc), float(bcT_left), float(bcT_lower), float(bcT_right),
+                                     float(bcT_upper), float(Comp_Unit), dptr(_f64(Nu_g, (ng + 1,))), dptr(I_edgV),
+                                     dptr(I_edgH), dptr(Ic_edgV), dptr(Ic_edgH))
+    check(rc, "RT_BC_UPDATE")
+
+
+def Bg_planck_calc(T, nu_low, nu_high, comp_unit):
+    """FUNCTION Bg_planck_calc, MainSrc/TEMP_FUNCTIONS.f08:90-108 (host evaluation in the library)."""
+    return _lib.lib().trt_bg_planck(float(T), float(nu_low), float(nu_high), float(comp_unit))
+
+
+# --------------------------------------------------------------------------------------------
+# Resident-state handle
+# --------------------------------------------------------------------------------------------
+class TransportSweep:
+    """A device-resident sweep instance (trt_create ... trt_destroy).
+
+    Typical time step (Tgen_QDf, ALGORITHMS.f08:1035-1101):
+        s.set_material(KapE, src_iso, c, dt, comp_unit)
+        s.sweep(roll=True, moments=True)
+        out = s.moments(["fg_avg_xx", ...])
+    """
+
+    def __init__(self, nx, ny, Omega_x, Omega_y, quad_weight, Delx, Dely, ng, precision="fp64", hbm_budget=0):
+        L = _lib.lib()
+        self.nx, self.ny, self.ng = int(nx), int(ny), int(ng)
+        self.Omega_x, self.Omega_y, self.w = _f64(Omega_x), _f64(Omega_y), _f64(quad_weight)
+        self.nm = len(self.Omega_x)
+        self.Delx, self.Dely = _f64(Delx, (nx,)), _f64(Dely, (ny,))
+        self.precision = {"fp64": _lib.TRT_PREC_FP64, "fp32": _lib.TRT_PREC_FP32, "mixed": _lib.TRT_PREC_FP32}[precision]
+        st = ctypes.c_int(0)
+        self._h = L.trt_create(self.nx, self.ny, self.nm, self.ng, dptr(self.Omega_x), dptr(self.Omega_y),
+                               dptr(self.w), dptr(self.Delx), dptr(self.Dely), self.precision, int(hbm_budget),
+                               ctypes.byref(st))
+        if not self._h:
+            raise _lib.TrtError(st.value, "trt_create")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().trt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_tiling(self, warps=0, slices=0, stages=0):
+        check(_lib.lib().trt_set_tiling(self._h, int(warps), int(slices), int(stages)), "trt_set_tiling")
+
+    def tiling(self):
+        v = [ctypes.c_int(0) for _ in range(4)]
+        check(_lib.lib().trt_get_tiling(self._h, *[ctypes.byref(x) for x in v]), "trt_get_tiling")
+        return dict(zip(("warps", "slices", "dirs_per_lane", "stages"), [x.value for x in v]))
+
+    def set_material(self, KapE_in, src_iso, c, Delt, Comp_Unit):
+        K = _f64(KapE_in, (self.nx, self.ny, self.ng))
+        S = _f64(src_iso, (self.nx, self.ny, self.ng))
+        check(_lib.lib().trt_set_material(self._h, dptr(K), dptr(S), float(c), float(Delt), float(Comp_Unit)),
+              "trt_set_material")
+
+    def set_material_device(self, d_kap, d_src, c, Delt, Comp_Unit):
+        """Device pointers (ints) to FP64 (nx, ny, ng) Fortran arrays."""
+        check(_lib.lib().trt_set_material_device(self._h, ctypes.c_void_p(d_kap), ctypes.c_void_p(d_src), float(c),
+                                                 float(Delt), float(Comp_Unit)), "trt_set_material_device")
+
+    def set_source_full(self, Src_in):
+        S = None if Src_in is None else _f64(Src_in, (2 * self.nx, 2 * self.ny, self.nm, self.ng))
+        check(_lib.lib().trt_set_source_full(self._h, dptr(S)), "trt_set_source_full")
+
+    def set_boundary(self, Ic_edgV, Ic_edgH, BC_Type=(0, 0, 0, 0)):
+        V = _f64(Ic_edgV, (self.nx + 1, 2 * self.ny, self.nm, self.ng))
+        H = _f64(Ic_edgH, (2 * self.nx, self.ny + 1, self.nm, self.ng))
+        bc = np.ascontiguousarray(BC_Type, dtype=np.int32)
+        check(_lib.lib().trt_set_boundary(self._h, dptr(V), dptr(H), iptr(bc)), "trt_set_boundary")
+
+    def bc_update(self, BC_Type, bcT, Comp_Unit, Nu_g):
+        bc = np.ascontiguousarray(BC_Type, dtype=np.int32)
+        check(_lib.lib().trt_bc_update(self._h, iptr(bc), *[float(t) for t in bcT], float(Comp_Unit),
+                                       dptr(_f64(Nu_g, (self.ng + 1,)))), "trt_bc_update")
+
+    def init_state(self, Tini, bcT, Comp_Unit, Nu_g):
+        check(_lib.lib().trt_init_state(self._h, float(Tini), *[float(t) for t in bcT], float(Comp_Unit),
+                                        dptr(_f64(Nu_g, (self.ng + 1,)))), "trt_init_state")
+
+    def put_state(self, I_crn):
+        I = _f64(I_crn, (2 * self.nx, 2 * self.ny, self.nm, self.ng))
+        check(_lib.lib().trt_put_state(self._h, dptr(I)), "trt_put_state")
+
+    def get_state(self):
+        I = np.empty((2 * self.nx, 2 * self.ny, self.nm, self.ng), order="F")
+        check(_lib.lib().trt_get_state(self._h, dptr(I)), "trt_get_state")
+        return I
+
+    def sweep(self, roll=False, moments=True, res_calc=False, sync=True):
+        flags = (_lib.TRT_ROLL_STATE if roll else 0) | (_lib.TRT_MOMENTS if moments else 0) | \
+            (_lib.TRT_RES_CALC if res_calc else 0)
+        check(_lib.lib().trt_sweep(self._h, flags), "trt_sweep")
+        if sync:
+            self.sync()
+
+    def sync(self):
+        check(_lib.lib().trt_sync(self._h), "trt_sync")
+
+    def moments(self, names=None):
+        names = list(_lib.MOMENT_FIELDS) if names is None else list(names)
+        out = {n: np.zeros(_lib.moment_shape(n, self.nx, self.ny, self.ng), order="F") for n in names}
+        mh = _lib.MomentsHost()
+        for n, a in out.items():
+            setattr(mh, n, dptr(a))
+        check(_lib.lib().trt_moments(self._h, ctypes.byref(mh)), "trt_moments")
+        return out
+
+    def moments_into(self, mh):
+        """Fill a prepared MomentsHost (pinned buffers) without allocating."""
+        check(_lib.lib().trt_moments(self._h, ctypes.byref(mh)), "trt_moments")
+
+    def angular(self, which=("I_avg", "I_edgV", "I_edgH", "Ic_edgV", "Ic_edgH")):
+        nx, ny, nm, ng = self.nx, self.ny, self.nm, self.ng
+        shapes = {"I_avg": (nx, ny, nm, ng), "I_edgV": (nx + 1, ny, nm, ng), "I_edgH": (nx, ny + 1, nm, ng),
+                  "Ic_edgV": (nx + 1, 2 * ny, nm, ng), "Ic_edgH": (2 * nx, ny + 1, nm, ng)}
+        out = {k: np.zeros(shapes[k], order="F") for k in which}
+        args = [dptr(out.get(k)) for k in ("I_avg", "I_edgV", "I_edgH", "Ic_edgV", "Ic_edgH")]
+        check(_lib.lib().trt_get_angular(self._h, *args), "trt_get_angular")
+        return out
+
+    def residual(self):
+        R = np.zeros((4, self.ng, 5), order="F")
+        lx = np.zeros((4, self.ng, 5), dtype=np.int32, order="F")
+        ly = np.zeros((4, self.ng, 5), dtype=np.int32, order="F")
+        check(_lib.lib().trt_get_residual(self._h, dptr(R), iptr(lx), iptr(ly)), "trt_get_residual")
+        return R, lx, ly
+
+    def stream(self):
+        return _lib.lib().trt_stream(self._h)
+
+    def device_output(self, name):
+        return _lib.lib().trt_device_output(self._h, name.encode())
+
+
+def required_bytes(nx, ny, nm, ng, precision="fp64"):
+    p = {"fp64": _lib.TRT_PREC_FP64, "fp32": _lib.TRT_PREC_FP32, "mixed": _lib.TRT_PREC_FP32}[precision]
+    return int(_lib.lib().trt_required_bytes(nx, ny, nm, ng, p))
+
+
+def kernel_launches():
+    return int(_lib.lib().trt_kernel_launches())

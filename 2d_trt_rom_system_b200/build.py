@@ -1,0 +1,52 @@
+"""Builds libtrt_sweep.so (the CUDA library behind include/trt_sweep.h) in place, for sm_100a.
+
+The library is compiled with --fmad=false: every multiply-add that should fuse is written as an
+explicit fma in the source, and every other operation rounds once, as in the reference Fortran.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+LIB = os.path.join(HERE, "libtrt_sweep.so")
+SOURCES = ["trt_api.cu"]
+HEADERS = ["aux_kernels.cuh", "dropin_kernels.cuh", "layout.cuh", "ptx.cuh", "scb_cell.h", "sweep_kernel.cuh"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-shared",
+              "-diag-suppress", "177"]
+
+
+def _nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def _stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(INCLUDE, "trt_sweep.h"),
+                                                                 os.path.abspath(__file__)]
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force=False, verbose=False):
+    """Compile the library if a source is newer than it.  Returns the path of the .so."""
+    if not force and not _stale():
+        return LIB
+    cmd = [_nvcc()] + NVCC_FLAGS + ARCH + ["-I" + INCLUDE, "-I" + CSRC, "-o", LIB + ".tmp"] + \
+        [os.path.join(CSRC, s) for s in SOURCES]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

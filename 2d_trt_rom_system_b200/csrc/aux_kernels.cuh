@@ -1,0 +1,580 @@
+// Device kernels around the sweep: layout conversion, angular exports, moment combination,
+// group sums, boundary updates and residual norms.  Each one cites the reference routine whose
+// result it produces.  All files are built with --fmad=false: operations written as separate
+// multiply and add round twice, as in the reference Fortran.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "layout.cuh"
+#include "sweep_kernel.cuh"
+
+namespace trt {
+
+constexpr double kCLight = 2.99792458e2;   // cm/sh, TRANSPORT_SOLVES.f08:403
+
+// ---------------------------------------------------------------------------------------------
+// State layout conversion: Fortran I_crn(2nx, 2ny, nm, ng) (double) <-> skewed (Real).
+// ---------------------------------------------------------------------------------------------
+struct Geo {
+  int nx, ny, nm, ng, mq;
+  Tiling t;
+  long long blk;
+};
+
+template <class Real>
+__device__ __forceinline__ long long state_index(const Geo& G, int i, int j, int cx, int cy, int m, int g) {
+  constexpr int NV = 16 / (int)sizeof(Real);
+  const int q = m / G.mq, ml = m % G.mq;
+  const SweepPos p = sweep_pos(G.nx, G.ny, G.t, q, i, j);
+  const int c = frame_corner(q, cx, cy);
+  return (long long)(g * 4 + q) * G.blk + skew_offset<NV>(G.mq, G.t, p.T, p.w, ml, p.r, c);
+}
+
+template <class Real>
+__global__ void pack_state_kernel(Geo G, const double* __restrict__ fort, Real* __restrict__ skew) {
+  const long long n = 4LL * G.nx * G.ny * G.nm * G.ng;
+  const long long nxx = 2LL * G.nx, nyy = 2LL * G.ny;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    long long r = k;
+    const int ix = (int)(r % nxx); r /= nxx;
+    const int iy = (int)(r % nyy); r /= nyy;
+    const int m = (int)(r % G.nm); r /= G.nm;
+    const int g = (int)r;
+    skew[state_index<Real>(G, ix >> 1, iy >> 1, ix & 1, iy & 1, m, g)] = (Real)fort[k];
+  }
+}
+
+template <class Real>
+__global__ void unpack_state_kernel(Geo G, const Real* __restrict__ skew, double* __restrict__ fort) {
+  const long long n = 4LL * G.nx * G.ny * G.nm * G.ng;
+  const long long nxx = 2LL * G.nx, nyy = 2LL * G.ny;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    long long r = k;
+    const int ix = (int)(r % nxx); r /= nxx;
+    const int iy = (int)(r % nyy); r /= nyy;
+    const int m = (int)(r % G.nm); r /= G.nm;
+    const int g = (int)r;
+    fort[k] = (double)skew[state_index<Real>(G, ix >> 1, iy >> 1, ix & 1, iy & 1, m, g)];
+  }
+}
+
+// Fill every slot of a skewed buffer that belongs to a cell with one value per (cell, g)
+// (used to initialise the state to B_g(T_ini) as RT_INIT does, INITIALIZERS.f08:84-92).
+template <class Real>
+__global__ void fill_state_kernel(Geo G, const double* __restrict__ per_g, Real* __restrict__ skew) {
+  const long long n = 4LL * G.nx * G.ny * G.nm * G.ng;
+  const long long nxx = 2LL * G.nx, nyy = 2LL * G.ny;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    long long r = k;
+    const int ix = (int)(r % nxx); r /= nxx;
+    const int iy = (int)(r % nyy); r /= nyy;
+    const int m = (int)(r % G.nm); r /= G.nm;
+    const int g = (int)r;
+    skew[state_index<Real>(G, ix >> 1, iy >> 1, ix & 1, iy & 1, m, g)] = (Real)per_g[g];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Corner-edge value Ic on a vertical face f (0..nx) at corner-edge row iy (0..2ny-1) for direction m:
+// the upwind cell's corner (TRANSPORT_SOLVES.f08:86-87,133-134,180-181,227-228) or the boundary
+// array on the inflow face.  Horizontal faces likewise (:88-89,135-136,182-183,229-230).
+// ---------------------------------------------------------------------------------------------
+template <class Real>
+__device__ __forceinline__ Real icV_value(const Geo& G, const Real* st, const Real* bndV, int f, int iy, int m, int g) {
+  const int q = m / G.mq;
+  const bool xpos = (q == 0 || q == 3);   // Omega_x > 0
+  if (xpos) {
+    if (f == 0) return bndV[((size_t)(0 * G.ng + g) * G.nm + m) * 2 * G.ny + iy];
+    return st[state_index<Real>(G, f - 1, iy >> 1, 1, iy & 1, m, g)];
+  } else {
+    if (f == G.nx) return bndV[((size_t)(1 * G.ng + g) * G.nm + m) * 2 * G.ny + iy];
+    return st[state_index<Real>(G, f, iy >> 1, 0, iy & 1, m, g)];
+  }
+}
+
+template <class Real>
+__device__ __forceinline__ Real icH_value(const Geo& G, const Real* st, const Real* bndH, int ix, int f, int m, int g) {
+  const int q = m / G.mq;
+  const bool ypos = (q == 0 || q == 1);   // Omega_y > 0
+  if (ypos) {
+    if (f == 0) return bndH[((size_t)(0 * G.ng + g) * G.nm + m) * 2 * G.nx + ix];
+    return st[state_index<Real>(G, ix >> 1, f - 1, ix & 1, 1, m, g)];
+  } else {
+    if (f == G.ny) return bndH[((size_t)(1 * G.ng + g) * G.nm + m) * 2 * G.nx + ix];
+    return st[state_index<Real>(G, ix >> 1, f, ix & 1, 0, m, g)];
+  }
+}
+
+// Angular exports in the reference layouts: I_avg(nx,ny,nm,ng) (TRANSPORT_SOLVES.f08:96),
+// I_edgV(nx+1,ny,nm,ng) (:92), I_edgH(nx,ny+1,nm,ng) (:93), Ic_edgV(nx+1,2ny,nm,ng),
+// Ic_edgH(2nx,ny+1,nm,ng).  Any output pointer may be null.  Values on inflow faces are the boundary
+// arrays (the reference keeps the caller's values there; the host layer restores them).
+template <class Real>
+__global__ void export_angular_kernel(Geo G, const Real* __restrict__ st, const Real* __restrict__ bndV,
+                                      const Real* __restrict__ bndH, double* I_avg, double* I_edgV, double* I_edgH,
+                                      double* Ic_edgV, double* Ic_edgH) {
+  const int nx = G.nx, ny = G.ny, nm = G.nm, ng = G.ng;
+  const long long nA = (long long)nx * ny * nm * ng;
+  const long long nV = (long long)(nx + 1) * ny * nm * ng;
+  const long long nH = (long long)nx * (ny + 1) * nm * ng;
+  const long long ncV = (long long)(nx + 1) * 2 * ny * nm * ng;
+  const long long ncH = (long long)2 * nx * (ny + 1) * nm * ng;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (I_avg)
+    for (long long k = k0; k < nA; k += stride) {
+      long long r = k;
+      const int i = (int)(r % nx); r /= nx;
+      const int j = (int)(r % ny); r /= ny;
+      const int m = (int)(r % nm);
+      const int g = (int)(r / nm);
+      const double lb = (double)st[state_index<Real>(G, i, j, 0, 0, m, g)];
+      const double rb = (double)st[state_index<Real>(G, i, j, 1, 0, m, g)];
+      const double rt = (double)st[state_index<Real>(G, i, j, 1, 1, m, g)];
+      const double lt = (double)st[state_index<Real>(G, i, j, 0, 1, m, g)];
+      I_avg[k] = (lb + rb + rt + lt) / 4.0;
+    }
+  if (I_edgV)
+    for (long long k = k0; k < nV; k += stride) {
+      long long r = k;
+      const int f = (int)(r % (nx + 1)); r /= (nx + 1);
+      const int j = (int)(r % ny); r /= ny;
+      const int m = (int)(r % nm);
+      const int g = (int)(r / nm);
+      const double b = (double)icV_value<Real>(G, st, bndV, f, 2 * j, m, g);
+      const double t = (double)icV_value<Real>(G, st, bndV, f, 2 * j + 1, m, g);
+      I_edgV[k] = (b + t) / 2.0;
+    }
+  if (I_edgH)
+    for (long long k = k0; k < nH; k += stride) {
+      long long r = k;
+      const int i = (int)(r % nx); r /= nx;
+      const int f = (int)(r % (ny + 1)); r /= (ny + 1);
+      const int m = (int)(r % nm);
+      const int g = (int)(r / nm);
+      const double l = (double)icH_value<Real>(G, st, bndH, 2 * i, f, m, g);
+      const double rr = (double)icH_value<Real>(G, st, bndH, 2 * i + 1, f, m, g);
+      I_edgH[k] = (l + rr) / 2.0;
+    }
+  if (Ic_edgV)
+    for (long long k = k0; k < ncV; k += stride) {
+      long long r = k;
+      const int f = (int)(r % (nx + 1)); r /= (nx + 1);
+      const int iy = (int)(r % (2 * ny)); r /= (2 * ny);
+      const int m = (int)(r % nm);
+      const int g = (int)(r / nm);
+      Ic_edgV[k] = (double)icV_value<Real>(G, st, bndV, f, iy, m, g);
+    }
+  if (Ic_edgH)
+    for (long long k = k0; k < ncH; k += stride) {
+      long long r = k;
+      const int ix = (int)(r % (2 * nx)); r /= (2 * nx);
+      const int f = (int)(r % (ny + 1)); r /= (ny + 1);
+      const int m = (int)(r % nm);
+      const int g = (int)(r / nm);
+      Ic_edgH[k] = (double)icH_value<Real>(G, st, bndH, ix, f, m, g);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Combination of the quadrant partials into the reference's low-order inputs.
+//   COLLAPSE_INTENSITIES  TRANSPORT_SOLVES.f08:441-478  (Hg_*, HO_Eg_*, HO_Fxg_edgV, HO_Fyg_edgH)
+//   fg_Calc               MLOQD_SOLVES.f08:646-674
+//   Cg_Calc               MLOQD_SOLVES.f08:392-484
+//   MGQD_In_Calc          MLOQD_SOLVES.f08:517-610
+// The reference adds eps = 1e-25/Comp_Unit to every intensity in the moment and C_g sums; here the
+// sums of the intensities are taken first and eps times the matching sum of weights is added in
+// FP64 (the same value up to rounding, and finite where FP32 intensities underflow).
+// ---------------------------------------------------------------------------------------------
+struct MomentOut {
+  double *Hg_avg_xx, *Hg_avg_yy, *Hg_avg_xy, *Hg_edgV_xx, *Hg_edgV_xy, *Hg_edgH_yy, *Hg_edgH_xy;
+  double *Eg_avg, *Eg_edgV, *Eg_edgH, *Fxg_edgV, *Fyg_edgH;
+  double *fg_avg_xx, *fg_avg_yy, *fg_avg_xy, *fg_edgV_xx, *fg_edgV_xy, *fg_edgH_yy, *fg_edgH_xy;
+  double *Cg_L, *Cg_B, *Cg_R, *Cg_T;
+  double *Eg_in_L, *Eg_in_B, *Eg_in_R, *Eg_in_T, *Fg_in_L, *Fg_in_B, *Fg_in_R, *Fg_in_T;
+  double *E_avg, *E_edgV, *E_edgH, *Fx_edgV, *Fy_edgH;
+  double *E_in_L, *E_in_B, *E_in_R, *E_in_T, *F_in_L, *F_in_B, *F_in_R, *F_in_T;
+  double *Fyg_edgH_true, *Fy_edgH_true;   // Omega_y-weighted horizontal-face flux (physics reporting)
+};
+
+// Per-quadrant weight sums for the analytic eps terms: [q][kNDirRow] over the mq directions.
+struct WeightSums {
+  double s[4][kNDirRow];
+};
+
+struct CombineArgs {
+  int nx, ny, nm, ng, mq;
+  double eps;          // 1e-25 / Comp_Unit
+  double c;            // speed of light used by fg_Calc (passed in by the reference's caller)
+  int bc[4];           // BC_Type L, B, R, T
+  WeightSums ws;
+  const double* part;  // [4][ng][ny][nx][kNPart]
+  const double* dir;   // [kNDirRow][nm] full direction table (physical), double
+};
+
+// Sum over the directions of quadrant q of w*f(Omega)*(Ic_bot + Ic_top)/2 on an inflow face.
+template <class Real>
+__device__ __forceinline__ void inflow_face_sums(const CombineArgs& A, const Real* bnd, int side, int g, int q,
+                                                 int pos, int len2, double* out /*[kNDirRow]*/) {
+  for (int v = 0; v < kNDirRow; ++v) out[v] = 0.0;
+  for (int ml = 0; ml < A.mq; ++ml) {
+    const int m = q * A.mq + ml;
+    const Real* b = bnd + ((size_t)(side * A.ng + g) * A.nm + m) * len2;
+    const double I = ((double)b[2 * pos] + (double)b[2 * pos + 1]) / 2.0;
+    for (int v = kW; v < kNDirRow; ++v) out[v] += A.dir[v * A.nm + m] * I;
+  }
+}
+
+template <class Real>
+__global__ void combine_kernel(CombineArgs A, const Real* __restrict__ bndV, const Real* __restrict__ bndH,
+                               MomentOut O) {
+  const int nx = A.nx, ny = A.ny, ng = A.ng;
+  const long long nA = (long long)nx * ny * ng, nV = (long long)(nx + 1) * ny * ng, nH = (long long)nx * (ny + 1) * ng;
+  const long long nxy = (long long)nx * ny;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const double eps = A.eps, c = A.c;
+  auto P = [&](int q, int g, int i, int j) { return A.part + (((size_t)(q * ng + g) * ny + j) * nx + i) * kNPart; };
+  auto wsum = [&](int v) { return A.ws.s[0][v] + A.ws.s[1][v] + A.ws.s[2][v] + A.ws.s[3][v]; };
+
+  // cell centres
+  for (long long k = k0; k < nA; k += stride) {
+    const int i = (int)(k % nx), j = (int)((k / nx) % ny), g = (int)(k / nxy);
+    double xx = 0, yy = 0, xy = 0, e = 0;
+    for (int q = 0; q < 4; ++q) {
+      const double* p = P(q, g, i, j);
+      xx += p[kCxx]; yy += p[kCyy]; xy += p[kCxy]; e += p[kCe];
+    }
+    xx += eps * wsum(kWxx); yy += eps * wsum(kWyy); xy += eps * wsum(kWxy); e += eps * wsum(kW);
+    const double Eg = e / kCLight;
+    if (O.Hg_avg_xx) { O.Hg_avg_xx[k] = xx; O.Hg_avg_yy[k] = yy; O.Hg_avg_xy[k] = xy; }
+    if (O.Eg_avg) O.Eg_avg[k] = Eg;
+    if (O.fg_avg_xx) {
+      O.fg_avg_xx[k] = xx / (c * Eg);
+      O.fg_avg_yy[k] = yy / (c * Eg);
+      O.fg_avg_xy[k] = xy / (c * Eg);
+    }
+  }
+  // vertical faces f = 0..nx
+  for (long long k = k0; k < nV; k += stride) {
+    const int f = (int)(k % (nx + 1)), j = (int)((k / (nx + 1)) % ny), g = (int)(k / ((long long)(nx + 1) * ny));
+    double xx = 0, xy = 0, fxs = 0, e = 0;
+    double outF = 0, outE = 0;     // outgoing sums on a boundary face (Cg)
+    double inF = 0, inE = 0;       // incoming sums on a boundary face (MGQD_In_Calc)
+    for (int q = 0; q < 4; ++q) {
+      const bool xpos = (q == 0 || q == 3);
+      const int cell = xpos ? f - 1 : f;     // upwind cell of this face for quadrant q
+      if (cell >= 0 && cell < nx) {
+        const double* p = P(q, g, cell, j);
+        xx += p[kVxx]; xy += p[kVxy]; fxs += p[kVx]; e += p[kVe];
+        if (f == 0 || f == nx) { outF += p[kVx]; outE += p[kVe]; }
+      } else {
+        double s[kNDirRow];
+        inflow_face_sums<Real>(A, bndV, f == 0 ? 0 : 1, g, q, j, 2 * ny, s);
+        xx += s[kWxx]; xy += s[kWxy]; fxs += s[kWx]; e += s[kW];
+        inF += s[kWx]; inE += s[kW];
+      }
+    }
+    xx += eps * wsum(kWxx); xy += eps * wsum(kWxy); fxs += eps * wsum(kWx); e += eps * wsum(kW);
+    const double Eg = e / kCLight;
+    if (O.Hg_edgV_xx) { O.Hg_edgV_xx[k] = xx; O.Hg_edgV_xy[k] = xy; }
+    if (O.Eg_edgV) O.Eg_edgV[k] = Eg;
+    if (O.Fxg_edgV) O.Fxg_edgV[k] = fxs;
+    if (O.fg_edgV_xx) { O.fg_edgV_xx[k] = xx / (c * Eg); O.fg_edgV_xy[k] = xy / (c * Eg); }
+    if (f == 0 || f == nx) {
+      const int side = (f == 0) ? 0 : 2;   // BC_Type index: L = 0, R = 2
+      // outgoing quadrants of this face: left face -> q 1,2 ; right face -> q 0,3
+      const int qa = (f == 0) ? 1 : 0, qb = (f == 0) ? 2 : 3;
+      const long long bi = (long long)j + (long long)ny * g;
+      double* Cg = (f == 0) ? O.Cg_L : O.Cg_R;
+      double* Ein = (f == 0) ? O.Eg_in_L : O.Eg_in_R;
+      double* Fin = (f == 0) ? O.Fg_in_L : O.Fg_in_R;
+      if (Cg) {
+        if (A.bc[side] == 0) {
+          const double num = outF + eps * (A.ws.s[qa][kWx] + A.ws.s[qb][kWx]);
+          const double den = outE + eps * (A.ws.s[qa][kW] + A.ws.s[qb][kW]);
+          Cg[bi] = num / den;
+        } else {
+          Cg[bi] = 0.0;
+        }
+      }
+      if (Ein) {
+        if (A.bc[side] == 0) { Ein[bi] = inE / kCLight; Fin[bi] = inF; }
+        else { Ein[bi] = 0.0; Fin[bi] = 0.0; }
+      }
+    }
+  }
+  // horizontal faces f = 0..ny
+  for (long long k = k0; k < nH; k += stride) {
+    const int i = (int)(k % nx), f = (int)((k / nx) % (ny + 1)), g = (int)(k / ((long long)nx * (ny + 1)));
+    double yy = 0, xy = 0, fys = 0, fxq = 0, e = 0;
+    double outF = 0, outE = 0, inF = 0, inE = 0;
+    for (int q = 0; q < 4; ++q) {
+      const bool ypos = (q == 0 || q == 1);
+      const int cell = ypos ? f - 1 : f;
+      if (cell >= 0 && cell < ny) {
+        const double* p = P(q, g, i, cell);
+        yy += p[kHyy]; xy += p[kHxy]; fys += p[kHy]; fxq += p[kHx]; e += p[kHe];
+        if (f == 0 || f == ny) { outF += p[kHy]; outE += p[kHe]; }
+      } else {
+        double s[kNDirRow];
+        inflow_face_sums<Real>(A, bndH, f == 0 ? 0 : 1, g, q, i, 2 * nx, s);
+        yy += s[kWyy]; xy += s[kWxy]; fys += s[kWy]; fxq += s[kWx]; e += s[kW];
+        inF += s[kWy]; inE += s[kW];
+      }
+    }
+    yy += eps * wsum(kWyy); xy += eps * wsum(kWxy); fys += eps * wsum(kWy); fxq += eps * wsum(kWx);
+    e += eps * wsum(kW);
+    const double Eg = e / kCLight;
+    if (O.Hg_edgH_yy) { O.Hg_edgH_yy[k] = yy; O.Hg_edgH_xy[k] = xy; }
+    if (O.Eg_edgH) O.Eg_edgH[k] = Eg;
+    if (O.Fyg_edgH) O.Fyg_edgH[k] = fxq;           // Omega_x weighted, as TRANSPORT_SOLVES.f08:469
+    if (O.Fyg_edgH_true) O.Fyg_edgH_true[k] = fys;
+    if (O.fg_edgH_yy) { O.fg_edgH_yy[k] = yy / (c * Eg); O.fg_edgH_xy[k] = xy / (c * Eg); }
+    if (f == 0 || f == ny) {
+      const int side = (f == 0) ? 1 : 3;   // BC_Type index: B = 1, T = 3
+      // outgoing quadrants: bottom face -> q 2,3 ; top face -> q 0,1
+      const int qa = (f == 0) ? 2 : 0, qb = (f == 0) ? 3 : 1;
+      const long long bi = (long long)i + (long long)nx * g;
+      double* Cg = (f == 0) ? O.Cg_B : O.Cg_T;
+      double* Ein = (f == 0) ? O.Eg_in_B : O.Eg_in_T;
+      double* Fin = (f == 0) ? O.Fg_in_B : O.Fg_in_T;
+      if (Cg) {
+        if (A.bc[side] == 0) {
+          const double num = outF + eps * (A.ws.s[qa][kWy] + A.ws.s[qb][kWy]);
+          const double den = outE + eps * (A.ws.s[qa][kW] + A.ws.s[qb][kW]);
+          Cg[bi] = num / den;
+        } else {
+          Cg[bi] = 0.0;
+        }
+      }
+      if (Ein) {
+        if (A.bc[side] == 0) { Ein[bi] = inE / kCLight; Fin[bi] = inF; }
+        else { Ein[bi] = 0.0; Fin[bi] = 0.0; }
+      }
+    }
+  }
+}
+
+// Group sums: COLLAPSE_INTENSITIES totals (TRANSPORT_SOLVES.f08:488-509, sequential in g) and
+// GQD_In_Calc (GLOQD_SOLVES.f08:276-288).
+__global__ void group_sum_kernel(int nx, int ny, int ng, MomentOut O) {
+  const long long nA = (long long)nx * ny, nV = (long long)(nx + 1) * ny, nH = (long long)nx * (ny + 1);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (long long k = k0; k < nA; k += stride)
+    if (O.E_avg && O.Eg_avg) {
+      double s = 0.0;
+      for (int g = 0; g < ng; ++g) s = s + O.Eg_avg[k + nA * g];
+      O.E_avg[k] = s;
+    }
+  for (long long k = k0; k < nV; k += stride) {
+    if (O.E_edgV && O.Eg_edgV) {
+      double s = 0.0;
+      for (int g = 0; g < ng; ++g) s = s + O.Eg_edgV[k + nV * g];
+      O.E_edgV[k] = s;
+    }
+    if (O.Fx_edgV && O.Fxg_edgV) {
+      double s = 0.0;
+      for (int g = 0; g < ng; ++g) s = s + O.Fxg_edgV[k + nV * g];
+      O.Fx_edgV[k] = s;
+    }
+  }
+  for (long long k = k0; k < nH; k += stride) {
+    if (O.E_edgH && O.Eg_edgH) {
+      double s = 0.0;
+      for (int g = 0; g < ng; ++g) s = s + O.Eg_edgH[k + nH * g];
+      O.E_edgH[k] = s;
+    }
+    if (O.Fy_edgH && O.Fyg_edgH) {
+      double s = 0.0;
+      for (int g = 0; g < ng; ++g) s = s + O.Fyg_edgH[k + nH * g];
+      O.Fy_edgH[k] = s;
+    }
+    if (O.Fy_edgH_true && O.Fyg_edgH_true) {
+      double s = 0.0;
+      for (int g = 0; g < ng; ++g) s = s + O.Fyg_edgH_true[k + nH * g];
+      O.Fy_edgH_true[k] = s;
+    }
+  }
+  for (long long k = k0; k < ny; k += stride)
+    if (O.E_in_L && O.Eg_in_L) {
+      double a = 0, b = 0, cc = 0, d = 0;
+      for (int g = 0; g < ng; ++g) {
+        a = a + O.Eg_in_L[k + (long long)ny * g];
+        b = b + O.Eg_in_R[k + (long long)ny * g];
+        cc = cc + O.Fg_in_L[k + (long long)ny * g];
+        d = d + O.Fg_in_R[k + (long long)ny * g];
+      }
+      O.E_in_L[k] = a; O.E_in_R[k] = b; O.F_in_L[k] = cc; O.F_in_R[k] = d;
+    }
+  for (long long k = k0; k < nx; k += stride)
+    if (O.E_in_B && O.Eg_in_B) {
+      double a = 0, b = 0, cc = 0, d = 0;
+      for (int g = 0; g < ng; ++g) {
+        a = a + O.Eg_in_B[k + (long long)nx * g];
+        b = b + O.Eg_in_T[k + (long long)nx * g];
+        cc = cc + O.Fg_in_B[k + (long long)nx * g];
+        d = d + O.Fg_in_T[k + (long long)nx * g];
+      }
+      O.E_in_B[k] = a; O.E_in_T[k] = b; O.F_in_B[k] = cc; O.F_in_T[k] = d;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Boundary arrays (RT_BC_UPDATE, UPDATES.f08:12-105).  Planck sides (type 0) get one value per
+// (side, g) on the inflow directions; reflective sides (type 1) copy the mirrored outflow direction.
+// bndV[side][g][m][2ny] holds Ic_edgV on x = 0 (side 0) and x = nx (side 1); bndH likewise.
+// ---------------------------------------------------------------------------------------------
+template <class Real>
+__global__ void bc_update_kernel(int nx, int ny, int nm, int ng, int4 bc, const double* __restrict__ bval /*[4][ng]*/,
+                                 Real* bndV, Real* bndH) {
+  const int q = nm / 4;
+  const long long nVtot = 2LL * ng * nm * 2 * ny, nHtot = 2LL * ng * nm * 2 * nx;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (long long k = k0; k < nVtot; k += stride) {
+    const int iy = (int)(k % (2 * ny));
+    const int m = (int)((k / (2 * ny)) % nm);
+    const int g = (int)((k / (2LL * ny * nm)) % ng);
+    const int side = (int)(k / (2LL * ny * nm * ng));
+    const int type = side == 0 ? bc.x : bc.z;
+    const bool inflow = side == 0 ? (m < q || m >= 3 * q) : (m >= q && m < 3 * q);
+    if (!inflow) continue;
+    if (type == 0) {
+      bndV[k] = (Real)bval[(side == 0 ? 0 : 2) * ng + g];
+    } else if (type == 1) {
+      int src;
+      if (side == 0) src = (m < q) ? m + q : m - q;        // :36-43
+      else src = (m < 2 * q) ? m - q : m + q;              // :74-81
+      bndV[k] = bndV[k + (long long)(src - m) * 2 * ny];
+    }
+  }
+  for (long long k = k0; k < nHtot; k += stride) {
+    const int ix = (int)(k % (2 * nx));
+    const int m = (int)((k / (2 * nx)) % nm);
+    const int g = (int)((k / (2LL * nx * nm)) % ng);
+    const int side = (int)(k / (2LL * nx * nm * ng));
+    (void)ix; (void)g;
+    const int type = side == 0 ? bc.y : bc.w;
+    const bool inflow = side == 0 ? (m < 2 * q) : (m >= 2 * q);
+    if (!inflow) continue;
+    if (type == 0) {
+      bndH[k] = (Real)bval[(side == 0 ? 1 : 3) * ng + g];
+    } else if (type == 1) {
+      int src;
+      if (side == 0) src = (m < q) ? m + 3 * q : m + q;     // :55-62
+      else src = (m < 3 * q) ? m - q : m - 3 * q;           // :93-100
+      bndH[k] = bndH[k + (long long)(src - m) * 2 * nx];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Residual norms of the corner balance equations, TRANSPORT_SOLVES.f08:249-323, same operation
+// order and the same loop order per (quadrant, group), so results agree bit for bit with a
+// sequential evaluation on identical inputs.  One thread per (m, g); a second pass takes the
+// maxima over the directions of each quadrant in direction order.
+// ---------------------------------------------------------------------------------------------
+template <class Real>
+struct ResidualArgs {
+  Geo G;
+  const double* omx; const double* omy;
+  const double* dx; const double* dy; const double* area;
+  const double* kap;            // KapE_in (nx,ny,ng), double
+  double rcdt;
+  const Real* Inew; const Real* Iold;
+  const Real* qiso;             // isotropic source (nx,ny,ng) or null
+  const Real* srcfull;          // skewed full source or null
+  const Real* bndV; const Real* bndH;
+  double* per_m;                // [ng][nm][5]  max, L1, L2, area-L1, area-L2 per direction
+  int* per_m_loc;               // [ng][nm][2]  (i, j) of the max, 1-based; 0 when no residual > 0
+};
+
+template <class Real>
+__global__ void residual_kernel(ResidualArgs<Real> a) {
+  const Geo& G = a.G;
+  const int nx = G.nx, ny = G.ny, nm = G.nm, ng = G.ng;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nm * ng) return;
+  const int m = k % nm, g = k / nm;
+  const double Ox = a.omx[m], Oy = a.omy[m];
+  double vmax = 0.0, sums[4] = {0.0, 0.0, 0.0, 0.0};
+  int li = 0, lj = 0;
+  for (int j = 0; j < ny; ++j) {
+    for (int i = 0; i < nx; ++i) {
+      const double Aij = a.area[i + (long long)nx * j];
+      const double kp = a.kap[i + (long long)nx * (j + (long long)ny * g)] + a.rcdt;
+      const double dxx = a.dx[i], dyy = a.dy[j];
+      double I[2][2], Sr[2][2];
+      for (int cx = 0; cx < 2; ++cx)
+        for (int cy = 0; cy < 2; ++cy) {
+          const long long si = state_index<Real>(G, i, j, cx, cy, m, g);
+          I[cx][cy] = (double)a.Inew[si];
+          const double io = (double)a.Iold[si];
+          const double sv = a.srcfull ? (double)a.srcfull[si] : (double)a.qiso[i + (long long)nx * (j + (long long)ny * g)];
+          Sr[cx][cy] = fma(io, a.rcdt, sv);
+        }
+      const double vL_b = (double)icV_value<Real>(G, a.Inew, a.bndV, i, 2 * j, m, g);
+      const double vL_t = (double)icV_value<Real>(G, a.Inew, a.bndV, i, 2 * j + 1, m, g);
+      const double vR_b = (double)icV_value<Real>(G, a.Inew, a.bndV, i + 1, 2 * j, m, g);
+      const double vR_t = (double)icV_value<Real>(G, a.Inew, a.bndV, i + 1, 2 * j + 1, m, g);
+      const double hB_l = (double)icH_value<Real>(G, a.Inew, a.bndH, 2 * i, j, m, g);
+      const double hB_r = (double)icH_value<Real>(G, a.Inew, a.bndH, 2 * i + 1, j, m, g);
+      const double hT_l = (double)icH_value<Real>(G, a.Inew, a.bndH, 2 * i, j + 1, m, g);
+      const double hT_r = (double)icH_value<Real>(G, a.Inew, a.bndH, 2 * i + 1, j + 1, m, g);
+      double res[4];
+      res[0] = fabs((Ox * dyy + Oy * dxx + kp * Aij) * I[0][0] / 4.0 + Ox * dyy * I[1][0] / 4.0 +
+                    Oy * dxx * I[0][1] / 4.0 - Ox * dyy * vL_b / 2.0 - Oy * dxx * hB_l / 2.0 - Aij * Sr[0][0] / 4.0);
+      res[1] = fabs((-Ox * dyy + Oy * dxx + kp * Aij) * I[1][0] / 4.0 - Ox * dyy * I[0][0] / 4.0 +
+                    Oy * dxx * I[1][1] / 4.0 + Ox * dyy * vR_b / 2.0 - Oy * dxx * hB_r / 2.0 - Aij * Sr[1][0] / 4.0);
+      res[2] = fabs((-Ox * dyy - Oy * dxx + kp * Aij) * I[1][1] / 4.0 - Ox * dyy * I[0][1] / 4.0 -
+                    Oy * dxx * I[1][0] / 4.0 + Ox * dyy * vR_t / 2.0 + Oy * dxx * hT_r / 2.0 - Aij * Sr[1][1] / 4.0);
+      res[3] = fabs((Ox * dyy - Oy * dxx + kp * Aij) * I[0][1] / 4.0 + Ox * dyy * I[1][1] / 4.0 -
+                    Oy * dxx * I[0][0] / 4.0 - Ox * dyy * vL_t / 2.0 + Oy * dxx * hT_l / 2.0 - Aij * Sr[0][1] / 4.0);
+      for (int kk = 0; kk < 4; ++kk) {
+        if (res[kk] > vmax) { vmax = res[kk]; li = i + 1; lj = j + 1; }
+        sums[0] = sums[0] + res[kk];
+        sums[1] = sums[1] + res[kk] * res[kk];
+        sums[2] = sums[2] + Aij * res[kk] / 4.0;
+        sums[3] = sums[3] + Aij * (res[kk] * res[kk]) / 4.0;
+      }
+    }
+  }
+  double* o = a.per_m + ((size_t)g * nm + m) * 5;
+  o[0] = vmax; o[1] = sums[0]; o[2] = sums[1]; o[3] = sums[2]; o[4] = sums[3];
+  int* l = a.per_m_loc + ((size_t)g * nm + m) * 2;
+  l[0] = li; l[1] = lj;
+}
+
+// RT_Residual(4, ng, 5), RT_ResLoc_x/y(4, ng, 5): maxima over the directions of each quadrant in
+// direction order, strictly greater replaces (TRANSPORT_SOLVES.f08:297-317).  The location of a sum
+// norm is the DO-loop exit value (N_x+1, N_y+1), as in the reference.
+__global__ void residual_reduce_kernel(int nx, int ny, int nm, int ng, const double* per_m, const int* per_m_loc,
+                                       double* res, int* locx, int* locy) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 4 * ng) return;
+  const int q = k % 4, g = k / 4;
+  const int mq = nm / 4;
+  double best[5] = {0, 0, 0, 0, 0};
+  for (int ml = 0; ml < mq; ++ml) {
+    const int m = q * mq + ml;
+    const double* o = per_m + ((size_t)g * nm + m) * 5;
+    const int* l = per_m_loc + ((size_t)g * nm + m) * 2;
+    if (o[0] > best[0]) {
+      best[0] = o[0];
+      locx[q + 4 * g] = l[0];
+      locy[q + 4 * g] = l[1];
+    }
+    for (int v = 1; v < 5; ++v)
+      if (o[v] > best[v]) {
+        best[v] = o[v];
+        locx[q + 4 * (g + ng * v)] = nx + 1;
+        locy[q + 4 * (g + ng * v)] = ny + 1;
+      }
+  }
+  for (int v = 0; v < 5; ++v) res[q + 4 * (g + ng * v)] = best[v];
+}
+
+}  // namespace trt

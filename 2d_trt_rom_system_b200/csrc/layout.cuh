@@ -1,0 +1,121 @@
+// Device data layout of one sweep instance (host and device code).
+//
+// Reference arrays (MainSrc/INITIALIZERS.f08:41-49) are Fortran column-major, e.g.
+// I_crn(2*N_x, 2*N_y, N_m, N_g).  On the device the angular state I_crn is stored in a private
+// "skewed" layout built for the wavefront sweep; every other array keeps the reference layout.
+//
+// Sweep frame.  Quadrant q (0..3 = directions m in [q*mq, (q+1)*mq), ordered (+,+), (-,+), (-,-),
+// (+,-) as INPUT_QUAD builds them, MainSrc/INPUTS.f08:1658-1669) is swept in the frame where x is
+// mirrored when Omega_x < 0 (fx) and y when Omega_y < 0 (fy): i' = fx ? nx-1-i : i, j' likewise.
+// In that frame every quadrant sweeps i' and j' upward, which is the loop order of
+// TRANSPORT_SOLVES.f08:58-241 mirrored.  Corners of a cell are numbered in the frame: 0 = lb,
+// 1 = rb, 2 = rt, 3 = lt.
+//
+// Work decomposition.  One CTA sweeps one (group, quadrant).  It has W warps; a warp holds R rows
+// x S direction slices (R*S = 32, lane = s*R + r).  Lane (s, r) of warp w owns the directions
+// m_q = d*S + s (d < D) of the quadrant and the row rho = w*R + r of a band of H = W*R rows.
+// Bands ("rounds") n = 0..nr-1 cover j' = n*H + rho.  Step T of the CTA puts every lane on the
+// anti-diagonal cell i' = T - rho - n*P (P = period >= max(nx, H)), so lane rows form a wavefront:
+// a cell's left inflow comes from the same lane one step earlier, its bottom inflow from the row
+// below one step earlier.
+//
+// Skewed state layout.  For each (g, q) a block of Tsteps*W chunks; chunk (T, w) holds the cells
+// the lanes of warp w touch at step T, as D sub-blocks (one per d) of nl_d lanes
+// (nl_d = R*min(S, mq - d*S)); a lane's 4 corners are stored as 16-byte vectors ("pairs" for
+// FP64, one vector for FP32), vector-major inside a sub-block so that a warp's load of one vector
+// is one contiguous 16*nl_d-byte run.  A whole CTA step is W contiguous chunks, which one TMA
+// bulk copy stages into shared memory.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define TRT_LHD __host__ __device__ __forceinline__
+#else
+#define TRT_LHD inline
+#endif
+
+namespace trt {
+
+struct Tiling {
+  int W;       // warps per CTA
+  int S;       // direction slices per warp (power of two)
+  int R;       // rows per warp = 32 / S
+  int D;       // directions per lane = ceil(mq / S)
+  int H;       // rows per round = W * R
+  int P;       // period = max(nx, H)
+  int nr;      // rounds = ceil(ny / H)
+  int Tsteps;  // steps of one (g, q) sweep = (nr-1)*P + nx + H - 1
+};
+
+TRT_LHD int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+TRT_LHD Tiling make_tiling(int nx, int ny, int mq, int W, int S) {
+  Tiling t;
+  t.W = W;
+  t.S = S;
+  t.R = 32 / S;
+  t.D = ceil_div(mq, S);
+  t.H = W * t.R;
+  t.P = nx > t.H ? nx : t.H;
+  t.nr = ceil_div(ny, t.H);
+  t.Tsteps = (t.nr - 1) * t.P + nx + t.H - 1;
+  return t;
+}
+
+// Elements per chunk (T, w): mq directions x R rows x 4 corners.
+TRT_LHD long long chunk_elems(int mq, const Tiling& t) { return (long long)mq * t.R * 4; }
+// Elements per (g, q) block.
+TRT_LHD long long block_elems(int mq, const Tiling& t) {
+  return (long long)t.Tsteps * t.W * chunk_elems(mq, t);
+}
+
+// Offset of corner c (frame numbering) of direction m_q of lane (s, r) of warp w at step T,
+// inside one (g, q) block.  NV = 16 / sizeof(Real) values per 16-byte vector.
+template <int NV>
+TRT_LHD long long skew_offset(int mq, const Tiling& t, int T, int w, int mloc, int r, int c) {
+  const int d = mloc / t.S;
+  const int s = mloc % t.S;
+  const int nslice = (mq - d * t.S) < t.S ? (mq - d * t.S) : t.S;
+  const int nl = t.R * nslice;
+  const int lane = s * t.R + r;
+  long long off = ((long long)T * t.W + w) * chunk_elems(mq, t);
+  off += (long long)d * 128;              // all earlier sub-blocks are full (32 lanes x 4)
+  off += (long long)(c / NV) * nl * NV + (long long)lane * NV + (c % NV);
+  return off;
+}
+
+// Map a physical cell (i, j) of quadrant q to (T, w, r) of the sweep.
+struct SweepPos {
+  int T, w, r;
+};
+TRT_LHD SweepPos sweep_pos(int nx, int ny, const Tiling& t, int q, int i, int j) {
+  const bool fx = (q == 1 || q == 2), fy = (q >= 2);
+  const int ip = fx ? nx - 1 - i : i;
+  const int jp = fy ? ny - 1 - j : j;
+  const int n = jp / t.H, rho = jp % t.H;
+  SweepPos p;
+  p.T = n * t.P + ip + rho;
+  p.w = rho / t.R;
+  p.r = rho % t.R;
+  return p;
+}
+
+// Physical corner (cx: 0 left / 1 right, cy: 0 bottom / 1 top) -> frame corner number.
+TRT_LHD int frame_corner(int q, int cx, int cy) {
+  const int fx = (q == 1 || q == 2), fy = (q >= 2);
+  const int sx = cx ^ fx, sy = cy ^ fy;
+  return sy ? (sx ? 2 : 3) : (sx ? 1 : 0);
+}
+
+// Number of values per cell of a quadrant moment partial (13 used + 1 pad).
+constexpr int kNPart = 14;
+// Partial value slots.  Signs are physical (Omega as given by the caller).
+enum PartSlot {
+  kCxx = 0, kCyy, kCxy, kCe,        // cell centre: w Ox^2, w Oy^2, w Ox Oy, w       (x I_avg)
+  kVxx, kVxy, kVx, kVe,             // downwind vertical face: w Ox^2, w Ox Oy, w Ox, w  (x I_edgV)
+  kHyy, kHxy, kHy, kHx, kHe         // downwind horizontal face: w Oy^2, w Ox Oy, w Oy, w Ox, w (x I_edgH)
+};
+
+}  // namespace trt

@@ -1,0 +1,98 @@
+// Per-cell Simple Corner Balance (SCB) solve, shared by the CUDA sweep and the CPU oracle.
+//
+// The reference builds the 4x4 corner matrix in SCB_BGEN (MainSrc/TRANSPORT_SOLVES.f08:332-371) and
+// solves it with the un-vendored LA_TOOLS routine GAUSS_COMPLETE (called at TRANSPORT_SOLVES.f08:79,
+// 126,173,220).  Here the system is solved in closed form.  In the "sweep frame" of a quadrant
+// (x and/or y mirrored so that both direction cosines are non-negative, corners ordered
+// lb, rb, rt, lt of the mirrored cell) the matrix is
+//
+//     B = g*I + a*P + b*R,     g = (|Ox| dy + |Oy| dx + kapE dx dy)/4,  a = |Ox| dy/4,  b = |Oy| dx/4
+//
+// with P, R the two commuting signed permutations of SCB_BGEN (P^2 = R^2 = -I).  With S = P R
+// (S^2 = I):  B (g I - a P - b R) = c I - d S,  c = g^2 + a^2 + b^2,  d = 2ab,  and
+// (c I - d S)(c I + d S) = (c^2 - d^2) I, so
+//
+//     B^-1 = (g I - a P - b R)(c I + d S) / det,   det = (g^2 + (a-b)^2)(g^2 + (a+b)^2) > 0.
+//
+// Because g >= a + b both factors have condition number <= 2, so the formula is as accurate as
+// Gaussian elimination on this matrix (a few ulp normwise).
+//
+// Every multiply-add below is an explicit fused multiply-add and every other operation is a single
+// IEEE operation, so a build without automatic FMA contraction (nvcc --fmad=false, g++
+// -ffp-contract=off) gives bit-identical results on the host and on the device.
+#pragma once
+
+#include <cmath>
+
+#if defined(__CUDACC__)
+#define TRT_HD __host__ __device__ __forceinline__
+#else
+#define TRT_HD inline
+#endif
+
+namespace trt {
+
+TRT_HD double tfma(double x, double y, double z) { return fma(x, y, z); }
+TRT_HD float tfma(float x, float y, float z) { return fmaf(x, y, z); }
+
+// Per-(cell, direction) geometry of the corner matrix, sweep frame.
+template <class R>
+struct ScbGeom {
+  R a, b;      // |Ox| dy / 4, |Oy| dx / 4
+  R hx, hy;    // |Ox| dy / 2, |Oy| dx / 2  (inflow face weights)
+};
+
+template <class R>
+TRT_HD ScbGeom<R> scb_geom(R ax, R ay, R dx, R dy) {
+  ScbGeom<R> G;
+  R axdy = ax * dy;
+  R aydx = ay * dx;
+  G.a = axdy * R(0.25);
+  G.b = aydx * R(0.25);
+  G.hx = axdy * R(0.5);
+  G.hy = aydx * R(0.5);
+  return G;
+}
+
+// gamma of SCB_BGEN: (|Ox| dy + |Oy| dx + kapE * dx*dy) / 4, with the same summation order.
+template <class R>
+TRT_HD R scb_gamma(R ax, R ay, R dx, R dy, R kapE) {
+  R axdy = ax * dy;
+  R aydx = ay * dx;
+  R area = dx * dy;
+  return (axdy + aydx + kapE * area) * R(0.25);
+}
+
+// Solve one cell.  s[k] = total corner source (isotropic/anisotropic source plus I_old/(c dt)),
+// A4 = cell area / 4, vb/vt = inflow corner-edge values on the sweep-left face (bottom, top corner),
+// hl/hr = inflow corner-edge values on the sweep-bottom face (left, right corner).
+// x[] receives the corner intensities lb, rb, rt, lt of the sweep frame.
+template <class R>
+TRT_HD void scb_solve(const ScbGeom<R>& G, R gamma, R A4, const R s[4], R vb, R vt, R hl, R hr, R x[4]) {
+  // right-hand side (TRANSPORT_SOLVES.f08:72-76 in the sweep frame)
+  R Q1 = tfma(G.hy, hl, tfma(G.hx, vb, A4 * s[0]));
+  R Q2 = tfma(G.hy, hr, A4 * s[1]);
+  R Q3 = A4 * s[2];
+  R Q4 = tfma(G.hx, vt, A4 * s[3]);
+
+  const R a = G.a, b = G.b, g = gamma;
+  R g2 = g * g;
+  R c = tfma(g, g, tfma(a, a, b * b));
+  R d = (a + a) * b;
+  R amb = a - b;
+  R apb = a + b;
+  R det = tfma(amb, amb, g2) * tfma(apb, apb, g2);
+  R inv = R(1) / det;
+
+  R y1 = tfma(d, Q3, c * Q1);
+  R y2 = tfma(-d, Q4, c * Q2);
+  R y3 = tfma(d, Q1, c * Q3);
+  R y4 = tfma(-d, Q2, c * Q4);
+
+  x[0] = tfma(-b, y4, tfma(-a, y2, g * y1)) * inv;
+  x[1] = tfma(-b, y3, tfma(a, y1, g * y2)) * inv;
+  x[2] = tfma(b, y2, tfma(a, y4, g * y3)) * inv;
+  x[3] = tfma(b, y1, tfma(-a, y3, g * y4)) * inv;
+}
+
+}  // namespace trt

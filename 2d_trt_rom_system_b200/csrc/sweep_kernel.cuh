@@ -1,0 +1,360 @@
+// SCB transport sweep with fused angular-moment epilogue (sm_100a).
+//
+// Replaces the per-group OpenMP loop of TRANSPORT_SCB (MainSrc/TRANSPORT_SOLVES.f08:50-244) and the
+// angular sums of COLLAPSE_INTENSITIES (TRANSPORT_SOLVES.f08:441-478).  Layout and work
+// decomposition: layout.cuh.  Per CTA step every lane solves its cell for D directions:
+//
+//   * I_crn_old for the whole CTA step is one contiguous run of the skewed state, staged into
+//     shared memory by a TMA bulk copy `stages` steps ahead (mbarrier completion);
+//   * the left inflow of a cell is the right outflow the same lane produced one step earlier
+//     (registers); the bottom inflow is the top outflow of the row below one step earlier:
+//     a warp shuffle inside a warp, a shared-memory handoff between warps, an L2-resident wrap
+//     buffer between rounds, and the boundary arrays on the inflow faces;
+//   * the 13 moment products of a cell are accumulated over the lane's D directions, reduced over
+//     the S slices of the row with xor-shuffles (fixed order), and written once per (cell, g,
+//     quadrant) as a partial; quadrant partials are combined in a fixed order afterwards, so results
+//     are bit-reproducible run to run;
+//   * the new corner intensities are written straight back in the same skewed layout.
+//
+// Every wait is bounded: a TMA phase that does not complete sets the error word and the CTA leaves
+// the loop together (the per-step barrier is a __syncthreads_or on the timeout flag) after a bounded
+// drain of its outstanding copies.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "layout.cuh"
+#include "ptx.cuh"
+#include "scb_cell.h"
+
+namespace trt {
+
+template <class Real>
+struct Vec16;
+template <>
+struct Vec16<double> {
+  using type = double2;
+};
+template <>
+struct Vec16<float> {
+  using type = float4;
+};
+
+// Direction-table rows (per quadrant, mq entries each), physical signs for the moment weights.
+enum DirRow { kAx = 0, kAy, kW, kWxx, kWyy, kWxy, kWx, kWy, kNDirRow };
+
+template <class Real>
+struct SweepArgs {
+  int nx, ny, nm, ng, mq;
+  Tiling t;
+  int stages;
+  long long chunk;          // elements per (T, w) chunk
+  long long blk;            // elements per (g, q) block
+  Real rcdt;                // 1 / (c * dt)
+  const Real* dx;           // (nx)
+  const Real* dy;           // (ny)
+  const Real* area;         // (nx, ny)
+  const Real* kap;          // (nx, ny, ng): KapE_in (without 1/(c dt))
+  const Real* qiso;         // (nx, ny, ng): isotropic corner source, or null with srcfull
+  const Real* srcfull;      // skewed layout, anisotropic per-corner source (drop-in path), or null
+  const Real* dirtab;       // [4][kNDirRow][mq]
+  const Real* Iold;         // skewed
+  Real* Inew;               // skewed
+  Real* bndV;               // [2][ng][nm][2 ny]  Ic_edgV on faces x=0 (side 0) and x=nx (side 1)
+  Real* bndH;               // [2][ng][nm][2 nx]  Ic_edgH on faces y=0 (side 0) and y=ny (side 1)
+  Real* wrap;               // [4 ng][nx][mq][2]  top outflow of the last row of a round
+  double* part;             // [4][ng][ny][nx][kNPart]  quadrant moment partials (physical cells)
+  int* err;                 // error word (bit 0: TMA wait timed out)
+  unsigned max_polls;       // bound on mbarrier polls per wait of the sweep
+  unsigned drain_polls;     // bound on the polls that drain outstanding copies after a timeout
+};
+
+constexpr int kErrTmaTimeout = 1;
+
+template <class Real>
+__host__ __device__ inline size_t sweep_smem_bytes(int W, long long chunk, int stages, int mq) {
+  size_t ring = (size_t)stages * W * chunk * sizeof(Real);
+  size_t bars = (size_t)stages * sizeof(uint64_t);
+  size_t hand = (size_t)2 * W * mq * 2 * sizeof(Real);
+  size_t dtab = (size_t)kNDirRow * mq * sizeof(Real);
+  return ring + bars + hand + dtab + 16;
+}
+
+template <class Real, int S, int DMAX, bool SRC_FULL>
+__global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a) {
+  constexpr int R = 32 / S;
+  constexpr int NV = 16 / (int)sizeof(Real);
+  using V = typename Vec16<Real>::type;
+
+  const Tiling t = a.t;
+  const int W = t.W;
+  const int nx = a.nx, ny = a.ny, nm = a.nm, ng = a.ng, mq = a.mq;
+  const int g = blockIdx.x >> 2, q = blockIdx.x & 3;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = lane / R, r = lane % R;
+  const int rho = warp * R + r;
+  const bool fx = (q == 1 || q == 2), fy = (q >= 2);
+  const int stages = a.stages;
+  const long long chunk = a.chunk;
+  const uint32_t stage_bytes = (uint32_t)(W * chunk * (long long)sizeof(Real));
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  Real* ring = reinterpret_cast<Real*>(smem);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + (size_t)stages * stage_bytes);
+  Real* hand = reinterpret_cast<Real*>(mbar + stages);
+  Real* dtab = hand + 2 * W * mq * 2;
+
+  for (int k = threadIdx.x; k < kNDirRow * mq; k += blockDim.x)
+    dtab[k] = a.dirtab[(size_t)q * kNDirRow * mq + k];
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < stages; ++k) mbar_init(&mbar[k], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  const long long blk_off = (long long)(g * 4 + q) * a.blk;
+  const Real* gold = a.Iold + blk_off;
+  Real* gnew = a.Inew + blk_off;
+  const int Tsteps = t.Tsteps;
+
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < stages && k < Tsteps; ++k) {
+      mbar_arrive_expect_tx(&mbar[k], stage_bytes);
+      tma_bulk_g2s(ring + (size_t)k * W * chunk, gold + (long long)k * W * chunk, stage_bytes, &mbar[k]);
+    }
+  }
+
+  const Real rcdt = a.rcdt;
+  const long long nxy = (long long)nx * ny;
+  Real* wrapc = a.wrap + (size_t)blockIdx.x * nx * mq * 2;
+  double* partg = a.part + ((size_t)(q * ng + g) * nxy) * kNPart;
+  const int sideVin = fx ? 1 : 0, sideVout = fx ? 0 : 1;
+  const int sideHin = fy ? 1 : 0, sideHout = fy ? 0 : 1;
+  const Real* bVin = a.bndV + ((size_t)(sideVin * ng + g) * nm + q * mq) * (2 * ny);
+  Real* bVout = a.bndV + ((size_t)(sideVout * ng + g) * nm + q * mq) * (2 * ny);
+  const Real* bHin = a.bndH + ((size_t)(sideHin * ng + g) * nm + q * mq) * (2 * nx);
+  Real* bHout = a.bndH + ((size_t)(sideHout * ng + g) * nm + q * mq) * (2 * nx);
+
+  Real vb[DMAX], vt[DMAX], hl[DMAX], hr[DMAX];
+#pragma unroll
+  for (int d = 0; d < DMAX; ++d) vb[d] = vt[d] = hl[d] = hr[d] = Real(0);
+
+  bool timed_out = false;
+  int stage = 0;
+  uint32_t phase = 0;
+  int T_break = Tsteps;
+  for (int T = 0; T < Tsteps; ++T) {
+    if (!mbar_wait_bounded(&mbar[stage], phase, a.max_polls)) timed_out = true;
+    const Real* sm = ring + (size_t)stage * W * chunk + (size_t)warp * chunk;
+    const long long gchunk = ((long long)T * W + warp) * chunk;
+
+    const int tau = T - rho;
+    int n = 0, ip = 0, jp = 0;
+    bool active = false;
+    if (tau >= 0 && !timed_out) {
+      n = tau / t.P;
+      ip = tau - n * t.P;
+      jp = n * t.H + rho;
+      active = (n < t.nr) && (ip < nx) && (jp < ny);
+    }
+
+    Real topL[DMAX], topR[DMAX];
+    Real acc[13];
+#pragma unroll
+    for (int v = 0; v < 13; ++v) acc[v] = Real(0);
+#pragma unroll
+    for (int d = 0; d < DMAX; ++d) topL[d] = topR[d] = Real(0);
+
+    int i = 0, j = 0;
+    if (active) {
+      i = fx ? nx - 1 - ip : ip;
+      j = fy ? ny - 1 - jp : jp;
+      const long long cell = (long long)i + (long long)nx * j;
+      const Real dx = a.dx[i], dy = a.dy[j];
+      const Real A4 = a.area[cell] * Real(0.25);
+      const Real kp = a.kap[cell + nxy * g] + rcdt;
+      Real qs = Real(0);
+      if (!SRC_FULL) qs = a.qiso[cell + nxy * g];
+
+      if (ip == 0) {
+#pragma unroll
+        for (int d = 0; d < DMAX; ++d) {
+          const int ml = d * S + s;
+          if (d < t.D && ml < mq) {
+            vb[d] = bVin[(size_t)ml * 2 * ny + 2 * j + (fy ? 1 : 0)];
+            vt[d] = bVin[(size_t)ml * 2 * ny + 2 * j + (fy ? 0 : 1)];
+          }
+        }
+      }
+      if (r == 0) {
+#pragma unroll
+        for (int d = 0; d < DMAX; ++d) {
+          const int ml = d * S + s;
+          if (d < t.D && ml < mq) {
+            if (rho == 0) {
+              if (n == 0) {
+                hl[d] = bHin[(size_t)ml * 2 * nx + 2 * i + (fx ? 1 : 0)];
+                hr[d] = bHin[(size_t)ml * 2 * nx + 2 * i + (fx ? 0 : 1)];
+              } else {
+                hl[d] = wrapc[((size_t)ip * mq + ml) * 2 + 0];
+                hr[d] = wrapc[((size_t)ip * mq + ml) * 2 + 1];
+              }
+            } else {
+              const Real* hb = hand + ((size_t)(((T - 1) & 1) * W + (warp - 1)) * mq + ml) * 2;
+              hl[d] = hb[0];
+              hr[d] = hb[1];
+            }
+          }
+        }
+      }
+
+#pragma unroll
+      for (int d = 0; d < DMAX; ++d) {
+        const int ml = d * S + s;
+        if (d < t.D && ml < mq) {
+          const int nsl = (mq - d * S) < S ? (mq - d * S) : S;
+          const int nl = R * nsl;
+          const Real* sb = sm + d * 128;
+          Real io[4];
+          if (NV == 2) {
+            const double2 p0 = *reinterpret_cast<const double2*>(sb + lane * 2);
+            const double2 p1 = *reinterpret_cast<const double2*>(sb + nl * 2 + lane * 2);
+            io[0] = (Real)p0.x; io[1] = (Real)p0.y; io[2] = (Real)p1.x; io[3] = (Real)p1.y;
+          } else {
+            const float4 p0 = *reinterpret_cast<const float4*>(sb + lane * 4);
+            io[0] = (Real)p0.x; io[1] = (Real)p0.y; io[2] = (Real)p0.z; io[3] = (Real)p0.w;
+          }
+          Real src[4];
+          if (SRC_FULL) {
+            const Real* gs = a.srcfull + blk_off + gchunk + d * 128;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+              src[c] = tfma(io[c], rcdt, gs[(c / NV) * nl * NV + lane * NV + (c % NV)]);
+          } else {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) src[c] = tfma(io[c], rcdt, qs);
+          }
+          const Real ax = dtab[kAx * mq + ml], ay = dtab[kAy * mq + ml];
+          const ScbGeom<Real> G = scb_geom(ax, ay, dx, dy);
+          const Real gam = scb_gamma(ax, ay, dx, dy, kp);
+          Real x[4];
+          scb_solve(G, gam, A4, src, vb[d], vt[d], hl[d], hr[d], x);
+
+          Real* gb = gnew + gchunk + d * 128;
+          if (NV == 2) {
+            *reinterpret_cast<double2*>(gb + lane * 2) = make_double2((double)x[0], (double)x[1]);
+            *reinterpret_cast<double2*>(gb + nl * 2 + lane * 2) = make_double2((double)x[2], (double)x[3]);
+          } else {
+            *reinterpret_cast<float4*>(gb + lane * 4) =
+                make_float4((float)x[0], (float)x[1], (float)x[2], (float)x[3]);
+          }
+
+          // outflow: right face feeds the next column of this lane, top face the next row
+          vb[d] = x[1];
+          vt[d] = x[2];
+          topL[d] = x[3];
+          topR[d] = x[2];
+
+          const Real Iavg = ((x[0] + x[1]) + (x[2] + x[3])) * Real(0.25);
+          const Real Iv = (x[1] + x[2]) * Real(0.5);
+          const Real Ih = (x[3] + x[2]) * Real(0.5);
+          const Real wxx = dtab[kWxx * mq + ml], wyy = dtab[kWyy * mq + ml], wxy = dtab[kWxy * mq + ml];
+          const Real ww = dtab[kW * mq + ml], wx = dtab[kWx * mq + ml], wy = dtab[kWy * mq + ml];
+          acc[kCxx] = tfma(wxx, Iavg, acc[kCxx]);
+          acc[kCyy] = tfma(wyy, Iavg, acc[kCyy]);
+          acc[kCxy] = tfma(wxy, Iavg, acc[kCxy]);
+          acc[kCe] = tfma(ww, Iavg, acc[kCe]);
+          acc[kVxx] = tfma(wxx, Iv, acc[kVxx]);
+          acc[kVxy] = tfma(wxy, Iv, acc[kVxy]);
+          acc[kVx] = tfma(wx, Iv, acc[kVx]);
+          acc[kVe] = tfma(ww, Iv, acc[kVe]);
+          acc[kHyy] = tfma(wyy, Ih, acc[kHyy]);
+          acc[kHxy] = tfma(wxy, Ih, acc[kHxy]);
+          acc[kHy] = tfma(wy, Ih, acc[kHy]);
+          acc[kHx] = tfma(wx, Ih, acc[kHx]);
+          acc[kHe] = tfma(ww, Ih, acc[kHe]);
+
+          if (ip == nx - 1) {
+            bVout[(size_t)ml * 2 * ny + 2 * j + (fy ? 1 : 0)] = x[1];
+            bVout[(size_t)ml * 2 * ny + 2 * j + (fy ? 0 : 1)] = x[2];
+          }
+          if (jp == ny - 1) {
+            bHout[(size_t)ml * 2 * nx + 2 * i + (fx ? 1 : 0)] = x[3];
+            bHout[(size_t)ml * 2 * nx + 2 * i + (fx ? 0 : 1)] = x[2];
+          }
+        }
+      }
+
+      // handoff of the top outflow of the warp's last row
+      if (r == R - 1) {
+#pragma unroll
+        for (int d = 0; d < DMAX; ++d) {
+          const int ml = d * S + s;
+          if (d < t.D && ml < mq) {
+            if (warp < W - 1) {
+              Real* hb = hand + ((size_t)((T & 1) * W + warp) * mq + ml) * 2;
+              hb[0] = topL[d];
+              hb[1] = topR[d];
+            } else if (t.nr > 1) {
+              wrapc[((size_t)ip * mq + ml) * 2 + 0] = topL[d];
+              wrapc[((size_t)ip * mq + ml) * 2 + 1] = topR[d];
+            }
+          }
+        }
+      }
+    }
+
+    // bottom inflow of rows r >= 1 for the next step (rows r == 0 reload it)
+#pragma unroll
+    for (int d = 0; d < DMAX; ++d) {
+      hl[d] = __shfl_up_sync(0xffffffffu, topL[d], 1);
+      hr[d] = __shfl_up_sync(0xffffffffu, topR[d], 1);
+    }
+
+    // moments: reduce over the S slices of each row (fixed xor order), write the quadrant partial
+    double accd[14];
+#pragma unroll
+    for (int v = 0; v < 13; ++v) accd[v] = (double)acc[v];
+    accd[13] = 0.0;
+#pragma unroll
+    for (int o = R; o < 32; o <<= 1) {
+#pragma unroll
+      for (int v = 0; v < 13; ++v) accd[v] += __shfl_xor_sync(0xffffffffu, accd[v], o);
+    }
+    if (active) {
+      double* pc = partg + ((size_t)j * nx + i) * kNPart;
+#pragma unroll
+      for (int p = 0; p < 7; ++p)
+        if (p % S == s) *reinterpret_cast<double2*>(pc + 2 * p) = make_double2(accd[2 * p], accd[2 * p + 1]);
+    }
+
+    const int any_timeout = __syncthreads_or(timed_out ? 1 : 0);
+    if (any_timeout) {
+      timed_out = true;
+      T_break = T;
+      break;
+    }
+    if (threadIdx.x == 0 && T + stages < Tsteps) {
+      mbar_arrive_expect_tx(&mbar[stage], stage_bytes);
+      tma_bulk_g2s(ring + (size_t)stage * W * chunk, gold + (long long)(T + stages) * W * chunk, stage_bytes,
+                   &mbar[stage]);
+    }
+    if (++stage == stages) {
+      stage = 0;
+      phase ^= 1u;
+    }
+  }
+
+  if (timed_out) {
+    if (threadIdx.x == 0) {
+      atomicOr(a.err, kErrTmaTimeout);
+      // drain: the copies of steps T_break .. T_break+stages-1 were issued and may be in flight; the
+      // CTA must not exit before they land in its shared memory.  Waits are bounded.
+      for (int s2 = T_break; s2 < T_break + stages && s2 < Tsteps; ++s2)
+        (void)mbar_wait_bounded(&mbar[s2 % stages], (uint32_t)((s2 / stages) & 1), a.drain_polls);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace trt

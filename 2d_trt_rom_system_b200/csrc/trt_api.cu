@@ -1,0 +1,1270 @@
+// C-ABI of libtrt_sweep.so (declarations and contracts: include/trt_sweep.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "trt_sweep.h"
+#include "aux_kernels.cuh"
+#include "dropin_kernels.cuh"
+#include "sweep_kernel.cuh"
+
+namespace {
+
+std::atomic<unsigned long long> g_launches{0};
+
+#define TRT_CUDA(expr)                                  \
+  do {                                                  \
+    cudaError_t e_ = (expr);                            \
+    if (e_ != cudaSuccess) {                            \
+      if (e_ == cudaErrorMemoryAllocation) {            \
+        cudaGetLastError();                             \
+        return TRT_ERR_NOMEM;                           \
+      }                                                 \
+      return TRT_ERR_CUDA;                              \
+    }                                                   \
+  } while (0)
+
+#define TRT_LAUNCHED() g_launches.fetch_add(1, std::memory_order_relaxed)
+
+int device_check() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) {
+    cudaGetLastError();
+    return TRT_ERR_NODEV;
+  }
+  return TRT_OK;
+}
+
+int grid_for(long long n, int block = 256) {
+  long long b = (n + block - 1) / block;
+  if (b < 1) b = 1;
+  if (b > 148LL * 16) b = 148LL * 16;
+  return (int)b;
+}
+
+// Bg_planck_calc and sigint, MainSrc/TEMP_FUNCTIONS.f08:90-141 (host evaluation).
+double sigint_h(double z) {
+  const double pi = 4.0 * std::atan(1.0);
+  const double pi4 = (pi * pi) * (pi * pi);
+  auto low = [](double x) { return ((x * x) * x) * (1.0 / 3.0 - x / 8.0 + (x * x) / 62.4); };
+  auto high = [&](double x) { return pi4 / 15.0 - std::exp(-x) * (((x * x) * x) + 3.0 * (x * x) + 6.0 * x + 7.28); };
+  if (z <= 1.95) return low(z);
+  if (z > 2.05) return high(z);
+  const double y1 = low(1.95), y2 = high(2.05);
+  return y1 + (y2 - y1) * (z - 1.95) / (2.05 - 1.95);
+}
+
+double bg_planck_h(double T, double nl, double nh, double cu) {
+  if (T <= 1e-15) return 0.0;
+  const double c = 2.99792458e2, erg = 6.24150934e11, h = 6.62613e-19;
+  double sig = sigint_h(nh / T) - sigint_h(nl / T);
+  const double e2 = erg * erg;
+  sig = sig / ((((h * h) * h) * (c * c)) * (e2 * e2) * cu);
+  const double t2 = T * T;
+  return (2.0 * (t2 * t2)) * sig;
+}
+
+struct Shape {
+  int nx, ny, nm, ng, mq;
+};
+
+bool valid_shape(int nx, int ny, int nm, int ng) {
+  return nx >= 1 && ny >= 1 && ng >= 1 && nm >= 4 && nm % 4 == 0 && nx < (1 << 20) && ny < (1 << 20);
+}
+
+// Compiled (slices, max directions per lane) pairs of the sweep kernel.
+struct KernelCfg {
+  int S, DMAX;
+};
+const KernelCfg kCfgs[] = {{1, 2}, {2, 5}, {4, 3}, {4, 6}, {4, 9}, {8, 3}, {8, 5}, {16, 3}, {16, 4}, {32, 2}};
+
+bool pick_cfg(int mq, int prec, int S_req, KernelCfg* out) {
+  bool found = false;
+  KernelCfg best{0, 0};
+  long best_key = 0;
+  for (const KernelCfg& k : kCfgs) {
+    if (S_req && k.S != S_req) continue;
+    const int D = (mq + k.S - 1) / k.S;
+    if (D > k.DMAX) continue;
+    const int waste = k.S * D - mq;
+    // FP64 keeps D <= 5 (registers); then least idle slots; then the smallest DMAX; then larger S
+    const int dpen = (prec == TRT_PREC_FP64 && D > 5) ? 1 : 0;
+    const long key = (long)dpen * 1000000 + waste * 1000 + k.DMAX * 10 + (32 - k.S) / 4;
+    if (!found || key < best_key) {
+      found = true;
+      best = k;
+      best_key = key;
+    }
+  }
+  if (found) *out = best;
+  return found;
+}
+
+template <class Real>
+cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int grid, int block, size_t smem, cudaStream_t st,
+                         const trt::SweepArgs<Real>& a) {
+#define TRT_SWEEP_CASE(S_, D_)                                                                   \
+  if (kc.S == S_ && kc.DMAX == D_) {                                                             \
+    if (src_full) {                                                                              \
+      auto k = trt::scb_sweep_kernel<Real, S_, D_, true>;                                        \
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);           \
+      k<<<grid, block, smem, st>>>(a);                                                           \
+    } else {                                                                                     \
+      auto k = trt::scb_sweep_kernel<Real, S_, D_, false>;                                       \
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);           \
+      k<<<grid, block, smem, st>>>(a);                                                           \
+    }                                                                                            \
+    return cudaGetLastError();                                                                   \
+  }
+  TRT_SWEEP_CASE(1, 2)
+  TRT_SWEEP_CASE(2, 5)
+  TRT_SWEEP_CASE(4, 3)
+  TRT_SWEEP_CASE(4, 6)
+  TRT_SWEEP_CASE(4, 9)
+  TRT_SWEEP_CASE(8, 3)
+  TRT_SWEEP_CASE(8, 5)
+  TRT_SWEEP_CASE(16, 3)
+  TRT_SWEEP_CASE(16, 4)
+  TRT_SWEEP_CASE(32, 2)
+#undef TRT_SWEEP_CASE
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+constexpr unsigned kDefaultWaitPolls = 1u << 22;
+
+struct trt_ctx {
+  int nx = 0, ny = 0, nm = 0, ng = 0, mq = 0, prec = 0;
+  size_t budget = 0, used = 0;
+  cudaStream_t stream = nullptr;
+  int Wreq = 0, Sreq = 0, stages = 3;
+  KernelCfg kc{8, 5};
+  trt::Tiling t{};
+  long long chunk = 0, blk = 0;
+  std::vector<double> omx, omy, w, dx, dy;
+  trt::WeightSums ws{};
+  // device memory
+  std::vector<void*> allocs;
+  double* d_dir = nullptr;      // [kNDirRow][nm]
+  void* d_dirtab = nullptr;     // [4][kNDirRow][mq] Real
+  double *d_dx = nullptr, *d_dy = nullptr, *d_area = nullptr;
+  void *d_dxr = nullptr, *d_dyr = nullptr, *d_arear = nullptr;
+  double *d_kap64 = nullptr, *d_q64 = nullptr;
+  void *d_kap = nullptr, *d_q = nullptr;
+  void* d_state[2] = {nullptr, nullptr};
+  int cur = 0;                  // d_state[cur] = I_crn_old, d_state[1-cur] = I_crn
+  void* d_srcfull = nullptr;
+  bool use_srcfull = false;
+  void *d_bndV = nullptr, *d_bndH = nullptr;
+  void* d_wrap = nullptr;
+  double* d_part = nullptr;
+  int* d_err = nullptr;
+  double* d_outs = nullptr;
+  trt::MomentOut dout{};
+  double *d_res_m = nullptr, *d_res = nullptr;
+  int *d_res_loc = nullptr, *d_resx = nullptr, *d_resy = nullptr;
+  double* d_stage = nullptr;    // per-group staging slab (double, 4*nx*ny*nm)
+  double* d_bval = nullptr;     // [4][ng] Planck boundary values
+  double c = 2.99792458e2, dt = 1.0, comp_unit = 1.0;
+  int bc[4] = {0, 0, 0, 0};
+  bool have_material = false, have_state = false, swept = false, have_moments = false, have_res = false;
+  unsigned wait_polls = kDefaultWaitPolls;
+
+  size_t esz() const { return prec == TRT_PREC_FP64 ? sizeof(double) : sizeof(float); }
+  long long state_elems() const { return 4LL * ng * blk; }
+  trt::Geo geo() const { return trt::Geo{nx, ny, nm, ng, mq, t, blk}; }
+
+  int dalloc(void** p, size_t bytes) {
+    if (budget && used + bytes > budget) return TRT_ERR_BUDGET;
+    void* q = nullptr;
+    if (cudaMalloc(&q, bytes ? bytes : 16) != cudaSuccess) {
+      cudaGetLastError();
+      return TRT_ERR_NOMEM;
+    }
+    allocs.push_back(q);
+    used += bytes;
+    *p = q;
+    return TRT_OK;
+  }
+  void dfree(void* p, size_t bytes) {
+    if (!p) return;
+    cudaFree(p);
+    allocs.erase(std::remove(allocs.begin(), allocs.end(), p), allocs.end());
+    used -= std::min(used, bytes);
+  }
+};
+
+namespace {
+
+template <class T>
+int alloc_t(trt_ctx* c, T** p, size_t n) {
+  void* q = nullptr;
+  int rc = c->dalloc(&q, n * sizeof(T));
+  *p = static_cast<T*>(q);
+  return rc;
+}
+
+// Sizes (elements) of the combined outputs, in MomentOut field order.
+void output_sizes(int nx, int ny, int ng, long long* sz) {
+  const long long A = (long long)nx * ny, V = (long long)(nx + 1) * ny, H = (long long)nx * (ny + 1);
+  long long s[] = {A * ng, A * ng, A * ng, V * ng, V * ng, H * ng, H * ng,   // Hg
+                   A * ng, V * ng, H * ng, V * ng, H * ng,                   // Eg, Fg
+                   A * ng, A * ng, A * ng, V * ng, V * ng, H * ng, H * ng,   // fg
+                   (long long)ny * ng, (long long)nx * ng, (long long)ny * ng, (long long)nx * ng,   // Cg L B R T
+                   (long long)ny * ng, (long long)nx * ng, (long long)ny * ng, (long long)nx * ng,   // Eg_in
+                   (long long)ny * ng, (long long)nx * ng, (long long)ny * ng, (long long)nx * ng,   // Fg_in
+                   A, V, H, V, H,                                                 // E, F totals
+                   ny, nx, ny, nx, ny, nx, ny, nx,                                // E_in, F_in totals
+                   H * ng, H};                                                    // Fy true
+  for (int k = 0; k < (int)(sizeof(s) / sizeof(s[0])); ++k) sz[k] = s[k];
+}
+constexpr int kNOut = 46;
+static_assert(sizeof(trt::MomentOut) == kNOut * sizeof(double*), "MomentOut layout");
+static_assert(sizeof(trt_moments_host) == kNOut * sizeof(double*), "trt_moments_host layout");
+
+const char* kOutNames[kNOut] = {
+    "Hg_avg_xx", "Hg_avg_yy", "Hg_avg_xy", "Hg_edgV_xx", "Hg_edgV_xy", "Hg_edgH_yy", "Hg_edgH_xy",
+    "Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH",
+    "fg_avg_xx", "fg_avg_yy", "fg_avg_xy", "fg_edgV_xx", "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy",
+    "Cg_L", "Cg_B", "Cg_R", "Cg_T",
+    "Eg_in_L", "Eg_in_B", "Eg_in_R", "Eg_in_T", "Fg_in_L", "Fg_in_B", "Fg_in_R", "Fg_in_T",
+    "E_avg", "E_edgV", "E_edgH", "Fx_edgV", "Fy_edgH",
+    "E_in_L", "E_in_B", "E_in_R", "E_in_T", "F_in_L", "F_in_B", "F_in_R", "F_in_T",
+    "Fyg_edgH_true", "Fy_edgH_true"};
+
+size_t layout_state_bytes(int nx, int ny, int mq, int ng, int W, int S, size_t esz) {
+  trt::Tiling t = trt::make_tiling(nx, ny, mq, W, S);
+  return (size_t)4 * ng * trt::block_elems(mq, t) * esz;
+}
+
+int default_W(int R) {
+  int W = 16 / R;
+  if (W < 1) W = 1;
+  if (W > 8) W = 8;
+  return W;
+}
+
+// (Re)compute the tiling and (re)allocate the layout-dependent buffers.
+int setup_layout(trt_ctx* c) {
+  if (!pick_cfg(c->mq, c->prec, c->Sreq, &c->kc)) return c->Sreq ? TRT_ERR_ARG : TRT_ERR_UNSUPPORTED;
+  const int R = 32 / c->kc.S;
+  const int W = c->Wreq ? c->Wreq : default_W(R);
+  c->t = trt::make_tiling(c->nx, c->ny, c->mq, W, c->kc.S);
+  c->chunk = trt::chunk_elems(c->mq, c->t);
+  c->blk = trt::block_elems(c->mq, c->t);
+  // pipeline depth limited by shared memory
+  const size_t esz = c->esz();
+  while (c->stages > 1 && (c->prec == TRT_PREC_FP64 ? trt::sweep_smem_bytes<double>(W, c->chunk, c->stages, c->mq)
+                                                     : trt::sweep_smem_bytes<float>(W, c->chunk, c->stages, c->mq)) >
+                              (size_t)200 * 1024)
+    c->stages--;
+  const size_t sbytes = (size_t)c->state_elems() * esz;
+  for (int k = 0; k < 2; ++k) {
+    if (c->d_state[k]) c->dfree(c->d_state[k], sbytes);
+    c->d_state[k] = nullptr;
+  }
+  if (c->d_srcfull) c->dfree(c->d_srcfull, sbytes), c->d_srcfull = nullptr;
+  c->use_srcfull = false;
+  for (int k = 0; k < 2; ++k) {
+    int rc = c->dalloc(&c->d_state[k], sbytes);
+    if (rc) return rc;
+    TRT_CUDA(cudaMemsetAsync(c->d_state[k], 0, sbytes, c->stream));
+  }
+  c->have_state = false;
+  c->swept = false;
+  return TRT_OK;
+}
+
+template <class Real>
+void fill_dirtab(const trt_ctx* c, std::vector<Real>& tab, std::vector<double>& full, trt::WeightSums& ws) {
+  const int nm = c->nm, mq = c->mq;
+  tab.assign((size_t)4 * trt::kNDirRow * mq, Real(0));
+  full.assign((size_t)trt::kNDirRow * nm, 0.0);
+  std::memset(&ws, 0, sizeof(ws));
+  for (int m = 0; m < nm; ++m) {
+    const double ox = c->omx[m], oy = c->omy[m], ww = c->w[m];
+    double v[trt::kNDirRow];
+    v[trt::kAx] = std::fabs(ox);
+    v[trt::kAy] = std::fabs(oy);
+    v[trt::kW] = ww;
+    v[trt::kWxx] = (ox * ox) * ww;
+    v[trt::kWyy] = (oy * oy) * ww;
+    v[trt::kWxy] = ox * oy * ww;
+    v[trt::kWx] = ox * ww;
+    v[trt::kWy] = oy * ww;
+    const int q = m / mq, ml = m % mq;
+    for (int r = 0; r < trt::kNDirRow; ++r) {
+      tab[((size_t)q * trt::kNDirRow + r) * mq + ml] = (Real)v[r];
+      full[(size_t)r * nm + m] = v[r];
+      if (r >= trt::kW) ws.s[q][r] += v[r];
+    }
+  }
+}
+
+template <class Real>
+__global__ void cast_kernel(long long n, const double* __restrict__ src, Real* __restrict__ dst) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    dst[k] = (Real)src[k];
+}
+
+int ensure_stage(trt_ctx* c) {
+  if (c->d_stage) return TRT_OK;
+  return alloc_t(c, &c->d_stage, (size_t)4 * c->nx * c->ny * c->nm);
+}
+
+// Upload a Fortran corner array (2nx,2ny,nm,ng) into a skewed buffer, one group slab at a time.
+template <class Real>
+int pack_corner_array(trt_ctx* c, const double* host, void* dst) {
+  int rc = ensure_stage(c);
+  if (rc) return rc;
+  const long long slab = 4LL * c->nx * c->ny * c->nm;
+  trt::Geo G = c->geo();
+  for (int g = 0; g < c->ng; ++g) {
+    TRT_CUDA(cudaMemcpyAsync(c->d_stage, host + slab * g, slab * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    trt::Geo Gg = G;
+    Gg.ng = 1;
+    // pack one group: shift the skewed base to group g (block index g*4 + q)
+    Real* base = static_cast<Real*>(dst) + (long long)g * 4 * c->blk;
+    trt::pack_state_kernel<Real><<<grid_for(slab), 256, 0, c->stream>>>(Gg, c->d_stage, base);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+  }
+  TRT_CUDA(cudaStreamSynchronize(c->stream));
+  return TRT_OK;
+}
+
+template <class Real>
+int unpack_corner_array(trt_ctx* c, const void* src, double* host) {
+  int rc = ensure_stage(c);
+  if (rc) return rc;
+  const long long slab = 4LL * c->nx * c->ny * c->nm;
+  trt::Geo G = c->geo();
+  for (int g = 0; g < c->ng; ++g) {
+    trt::Geo Gg = G;
+    Gg.ng = 1;
+    const Real* base = static_cast<const Real*>(src) + (long long)g * 4 * c->blk;
+    trt::unpack_state_kernel<Real><<<grid_for(slab), 256, 0, c->stream>>>(Gg, base, c->d_stage);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+    TRT_CUDA(cudaMemcpyAsync(host + slab * g, c->d_stage, slab * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    TRT_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return TRT_OK;
+}
+
+int check_err(trt_ctx* c) {
+  int h = 0;
+  TRT_CUDA(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  TRT_CUDA(cudaStreamSynchronize(c->stream));
+  if (h) {
+    TRT_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    return TRT_ERR_TIMEOUT;
+  }
+  return TRT_OK;
+}
+
+template <class Real>
+int sweep_impl(trt_ctx* c, unsigned flags) {
+  if (flags & TRT_ROLL_STATE) c->cur = 1 - c->cur;   // I_crn_old <- I_crn (ALGORITHMS.f08:397)
+  trt::SweepArgs<Real> a{};
+  a.nx = c->nx; a.ny = c->ny; a.nm = c->nm; a.ng = c->ng; a.mq = c->mq;
+  a.t = c->t;
+  a.stages = c->stages;
+  a.chunk = c->chunk;
+  a.blk = c->blk;
+  a.rcdt = (Real)(1.0 / (c->c * c->dt));
+  a.dx = (const Real*)c->d_dxr;
+  a.dy = (const Real*)c->d_dyr;
+  a.area = (const Real*)c->d_arear;
+  a.kap = (const Real*)c->d_kap;
+  a.qiso = c->use_srcfull ? nullptr : (const Real*)c->d_q;
+  a.srcfull = c->use_srcfull ? (const Real*)c->d_srcfull : nullptr;
+  a.dirtab = (const Real*)c->d_dirtab;
+  a.Iold = (const Real*)c->d_state[c->cur];
+  a.Inew = (Real*)c->d_state[1 - c->cur];
+  a.bndV = (Real*)c->d_bndV;
+  a.bndH = (Real*)c->d_bndH;
+  a.wrap = (Real*)c->d_wrap;
+  a.part = c->d_part;
+  a.err = c->d_err;
+  a.max_polls = c->wait_polls;
+  a.drain_polls = 1u << 24;
+  const size_t smem = trt::sweep_smem_bytes<Real>(c->t.W, c->chunk, c->stages, c->mq);
+  cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, 4 * c->ng, 32 * c->t.W, smem, c->stream, a);
+  TRT_LAUNCHED();
+  if (e != cudaSuccess) return TRT_ERR_CUDA;
+  c->swept = true;
+
+  if (flags & TRT_MOMENTS) {
+    trt::CombineArgs A{};
+    A.nx = c->nx; A.ny = c->ny; A.nm = c->nm; A.ng = c->ng; A.mq = c->mq;
+    A.eps = 1e-25 / c->comp_unit;
+    A.c = c->c;
+    for (int k = 0; k < 4; ++k) A.bc[k] = c->bc[k];
+    A.ws = c->ws;
+    A.part = c->d_part;
+    A.dir = c->d_dir;
+    const long long n = (long long)(c->nx + 1) * (c->ny + 1) * c->ng;
+    trt::combine_kernel<Real><<<grid_for(n), 256, 0, c->stream>>>(A, (const Real*)c->d_bndV, (const Real*)c->d_bndH,
+                                                                    c->dout);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+    trt::group_sum_kernel<<<grid_for((long long)(c->nx + 1) * (c->ny + 1)), 256, 0, c->stream>>>(c->nx, c->ny,
+                                                                                                 c->ng, c->dout);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+    c->have_moments = true;
+  }
+  if (flags & TRT_RES_CALC) {
+    if (!c->d_res_m) {
+      int rc = alloc_t(c, &c->d_res_m, (size_t)5 * c->nm * c->ng);
+      if (!rc) rc = alloc_t(c, &c->d_res_loc, (size_t)2 * c->nm * c->ng);
+      if (!rc) rc = alloc_t(c, &c->d_res, (size_t)20 * c->ng);
+      if (!rc) rc = alloc_t(c, &c->d_resx, (size_t)20 * c->ng);
+      if (!rc) rc = alloc_t(c, &c->d_resy, (size_t)20 * c->ng);
+      if (rc) return rc;
+    }
+    trt::ResidualArgs<Real> ra{};
+    ra.G = c->geo();
+    // Omega_x and Omega_y follow the kNDirRow rows of the direction table
+    ra.omx = c->d_dir + (size_t)trt::kNDirRow * c->nm;
+    ra.omy = ra.omx + c->nm;
+    ra.dx = c->d_dx; ra.dy = c->d_dy; ra.area = c->d_area;
+    ra.kap = c->d_kap64;
+    ra.rcdt = 1.0 / (c->c * c->dt);
+    ra.Inew = (const Real*)c->d_state[1 - c->cur];
+    ra.Iold = (const Real*)c->d_state[c->cur];
+    ra.qiso = c->use_srcfull ? nullptr : (const Real*)c->d_q;
+    ra.srcfull = c->use_srcfull ? (const Real*)c->d_srcfull : nullptr;
+    ra.bndV = (const Real*)c->d_bndV;
+    ra.bndH = (const Real*)c->d_bndH;
+    ra.per_m = c->d_res_m;
+    ra.per_m_loc = c->d_res_loc;
+    trt::residual_kernel<Real><<<(c->nm * c->ng + 63) / 64, 64, 0, c->stream>>>(ra);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+    trt::residual_reduce_kernel<<<(4 * c->ng + 63) / 64, 64, 0, c->stream>>>(c->nx, c->ny, c->nm, c->ng, c->d_res_m,
+                                                                            c->d_res_loc, c->d_res, c->d_resx,
+                                                                            c->d_resy);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+    c->have_res = true;
+  }
+  return TRT_OK;
+}
+
+template <class Real>
+int set_material_impl(trt_ctx* c, const double* kap, const double* q, bool device) {
+  const size_t n = (size_t)c->nx * c->ny * c->ng;
+  const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  TRT_CUDA(cudaMemcpyAsync(c->d_kap64, kap, n * sizeof(double), kind, c->stream));
+  TRT_CUDA(cudaMemcpyAsync(c->d_q64, q, n * sizeof(double), kind, c->stream));
+  if (sizeof(Real) == sizeof(double)) {
+    TRT_CUDA(cudaMemcpyAsync(c->d_kap, c->d_kap64, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    TRT_CUDA(cudaMemcpyAsync(c->d_q, c->d_q64, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  } else {
+    cast_kernel<float><<<grid_for(n), 256, 0, c->stream>>>(n, c->d_kap64, (float*)c->d_kap);
+    TRT_LAUNCHED();
+    cast_kernel<float><<<grid_for(n), 256, 0, c->stream>>>(n, c->d_q64, (float*)c->d_q);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+  }
+  if (!device) TRT_CUDA(cudaStreamSynchronize(c->stream));
+  return TRT_OK;
+}
+
+// Boundary corner-edge values on the inflow faces from full reference arrays.
+template <class Real>
+int set_boundary_impl(trt_ctx* c, const double* IcV, const double* IcH) {
+  const int nx = c->nx, ny = c->ny, nm = c->nm, ng = c->ng;
+  const size_t nV = (size_t)2 * ng * nm * 2 * ny, nH = (size_t)2 * ng * nm * 2 * nx;
+  std::vector<Real> bV(nV, Real(0)), bH(nH, Real(0));
+  if (IcV) {
+    for (int side = 0; side < 2; ++side)
+      for (int g = 0; g < ng; ++g)
+        for (int m = 0; m < nm; ++m)
+          for (int iy = 0; iy < 2 * ny; ++iy) {
+            const int f = side ? nx : 0;
+            bV[((size_t)(side * ng + g) * nm + m) * 2 * ny + iy] =
+                (Real)IcV[f + (size_t)(nx + 1) * (iy + (size_t)2 * ny * (m + (size_t)nm * g))];
+          }
+  }
+  if (IcH) {
+    for (int side = 0; side < 2; ++side)
+      for (int g = 0; g < ng; ++g)
+        for (int m = 0; m < nm; ++m)
+          for (int ix = 0; ix < 2 * nx; ++ix) {
+            const int f = side ? ny : 0;
+            bH[((size_t)(side * ng + g) * nm + m) * 2 * nx + ix] =
+                (Real)IcH[ix + (size_t)2 * nx * (f + (size_t)(ny + 1) * (m + (size_t)nm * g))];
+          }
+  }
+  TRT_CUDA(cudaMemcpyAsync(c->d_bndV, bV.data(), nV * sizeof(Real), cudaMemcpyHostToDevice, c->stream));
+  TRT_CUDA(cudaMemcpyAsync(c->d_bndH, bH.data(), nH * sizeof(Real), cudaMemcpyHostToDevice, c->stream));
+  TRT_CUDA(cudaStreamSynchronize(c->stream));
+  return TRT_OK;
+}
+
+template <class Real>
+int bc_update_impl(trt_ctx* c, const int* bc, const double* Tb, double cu, const double* nu) {
+  std::vector<double> bval((size_t)4 * c->ng, 0.0);
+  for (int s = 0; s < 4; ++s)
+    for (int g = 0; g < c->ng; ++g) bval[(size_t)s * c->ng + g] = bg_planck_h(Tb[s], nu[g], nu[g + 1], cu);
+  TRT_CUDA(cudaMemcpyAsync(c->d_bval, bval.data(), bval.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  const long long n = 2LL * c->ng * c->nm * 2 * std::max(c->nx, c->ny);
+  trt::bc_update_kernel<Real><<<grid_for(n), 256, 0, c->stream>>>(c->nx, c->ny, c->nm, c->ng,
+                                                                   make_int4(bc[0], bc[1], bc[2], bc[3]), c->d_bval,
+                                                                   (Real*)c->d_bndV, (Real*)c->d_bndH);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  TRT_CUDA(cudaStreamSynchronize(c->stream));
+  return TRT_OK;
+}
+
+template <class Real>
+int init_state_impl(trt_ctx* c, double Tini, const double* Tb, double cu, const double* nu) {
+  std::vector<double> per_g(c->ng);
+  for (int g = 0; g < c->ng; ++g) per_g[g] = bg_planck_h(Tini, nu[g], nu[g + 1], cu);
+  double* d_pg = nullptr;
+  int rc = alloc_t(c, &d_pg, c->ng);
+  if (rc) return rc;
+  TRT_CUDA(cudaMemcpyAsync(d_pg, per_g.data(), c->ng * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  const long long n = 4LL * c->nx * c->ny * c->nm * c->ng;
+  for (int k = 0; k < 2; ++k) {
+    trt::fill_state_kernel<Real><<<grid_for(n), 256, 0, c->stream>>>(c->geo(), d_pg, (Real*)c->d_state[k]);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+  }
+  // every boundary value = Bg(Tini) first (RT_INIT sets all of Ic_edgV/H), then Planck inflow faces
+  std::vector<Real> bV((size_t)2 * c->ng * c->nm * 2 * c->ny), bH((size_t)2 * c->ng * c->nm * 2 * c->nx);
+  for (size_t k = 0; k < bV.size(); ++k) bV[k] = (Real)per_g[(k / ((size_t)c->nm * 2 * c->ny)) % c->ng];
+  for (size_t k = 0; k < bH.size(); ++k) bH[k] = (Real)per_g[(k / ((size_t)c->nm * 2 * c->nx)) % c->ng];
+  TRT_CUDA(cudaMemcpyAsync(c->d_bndV, bV.data(), bV.size() * sizeof(Real), cudaMemcpyHostToDevice, c->stream));
+  TRT_CUDA(cudaMemcpyAsync(c->d_bndH, bH.data(), bH.size() * sizeof(Real), cudaMemcpyHostToDevice, c->stream));
+  TRT_CUDA(cudaStreamSynchronize(c->stream));
+  c->dfree(d_pg, c->ng * sizeof(double));
+  const int zero[4] = {0, 0, 0, 0};
+  rc = bc_update_impl<Real>(c, zero, Tb, cu, nu);
+  if (rc) return rc;
+  c->have_state = true;
+  return TRT_OK;
+}
+
+template <class Real>
+int get_angular_impl(trt_ctx* c, double* I_avg, double* I_edgV, double* I_edgH, double* Ic_edgV, double* Ic_edgH) {
+  const int nx = c->nx, ny = c->ny, nm = c->nm, ng = c->ng;
+  double* outs[5] = {I_avg, I_edgV, I_edgH, Ic_edgV, Ic_edgH};
+  const long long sz[5] = {(long long)nx * ny * nm * ng, (long long)(nx + 1) * ny * nm * ng,
+                           (long long)nx * (ny + 1) * nm * ng, (long long)(nx + 1) * 2 * ny * nm * ng,
+                           (long long)2 * nx * (ny + 1) * nm * ng};
+  const void* st = c->d_state[c->swept ? 1 - c->cur : c->cur];
+  for (int k = 0; k < 5; ++k) {
+    if (!outs[k]) continue;
+    double* d = nullptr;
+    int rc = alloc_t(c, &d, (size_t)sz[k]);
+    if (rc) return rc;
+    double* p[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    p[k] = d;
+    trt::export_angular_kernel<Real><<<grid_for(sz[k]), 256, 0, c->stream>>>(
+        c->geo(), (const Real*)st, (const Real*)c->d_bndV, (const Real*)c->d_bndH, p[0], p[1], p[2], p[3], p[4]);
+    TRT_LAUNCHED();
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(outs[k], d, sz[k] * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    c->dfree(d, sz[k] * sizeof(double));
+    if (e != cudaSuccess) return TRT_ERR_CUDA;
+  }
+  return TRT_OK;
+}
+
+int create_buffers(trt_ctx* c) {
+  int rc;
+  const size_t esz = c->esz();
+  const int nx = c->nx, ny = c->ny, nm = c->nm, ng = c->ng;
+  // direction table: kNDirRow rows, then Omega_x and Omega_y rows
+  std::vector<double> full;
+  if (c->prec == TRT_PREC_FP64) {
+    std::vector<double> tab;
+    fill_dirtab<double>(c, tab, full, c->ws);
+    if ((rc = c->dalloc(&c->d_dirtab, tab.size() * sizeof(double)))) return rc;
+    TRT_CUDA(cudaMemcpy(c->d_dirtab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> tab;
+    fill_dirtab<float>(c, tab, full, c->ws);
+    if ((rc = c->dalloc(&c->d_dirtab, tab.size() * sizeof(float)))) return rc;
+    TRT_CUDA(cudaMemcpy(c->d_dirtab, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  full.insert(full.end(), c->omx.begin(), c->omx.end());
+  full.insert(full.end(), c->omy.begin(), c->omy.end());
+  if ((rc = alloc_t(c, &c->d_dir, full.size()))) return rc;
+  TRT_CUDA(cudaMemcpy(c->d_dir, full.data(), full.size() * sizeof(double), cudaMemcpyHostToDevice));
+
+  std::vector<double> area((size_t)nx * ny);
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) area[i + (size_t)nx * j] = c->dx[i] * c->dy[j];   // OUTER_PROD, INITIALIZERS.f08:152
+  if ((rc = alloc_t(c, &c->d_dx, nx)) || (rc = alloc_t(c, &c->d_dy, ny)) || (rc = alloc_t(c, &c->d_area, (size_t)nx * ny)))
+    return rc;
+  TRT_CUDA(cudaMemcpy(c->d_dx, c->dx.data(), nx * sizeof(double), cudaMemcpyHostToDevice));
+  TRT_CUDA(cudaMemcpy(c->d_dy, c->dy.data(), ny * sizeof(double), cudaMemcpyHostToDevice));
+  TRT_CUDA(cudaMemcpy(c->d_area, area.data(), area.size() * sizeof(double), cudaMemcpyHostToDevice));
+  if ((rc = c->dalloc(&c->d_dxr, nx * esz)) || (rc = c->dalloc(&c->d_dyr, ny * esz)) ||
+      (rc = c->dalloc(&c->d_arear, (size_t)nx * ny * esz)))
+    return rc;
+  if (c->prec == TRT_PREC_FP64) {
+    TRT_CUDA(cudaMemcpy(c->d_dxr, c->d_dx, nx * esz, cudaMemcpyDeviceToDevice));
+    TRT_CUDA(cudaMemcpy(c->d_dyr, c->d_dy, ny * esz, cudaMemcpyDeviceToDevice));
+    TRT_CUDA(cudaMemcpy(c->d_arear, c->d_area, (size_t)nx * ny * esz, cudaMemcpyDeviceToDevice));
+  } else {
+    std::vector<float> f(c->dx.begin(), c->dx.end());
+    TRT_CUDA(cudaMemcpy(c->d_dxr, f.data(), nx * esz, cudaMemcpyHostToDevice));
+    f.assign(c->dy.begin(), c->dy.end());
+    TRT_CUDA(cudaMemcpy(c->d_dyr, f.data(), ny * esz, cudaMemcpyHostToDevice));
+    f.assign(area.begin(), area.end());
+    TRT_CUDA(cudaMemcpy(c->d_arear, f.data(), (size_t)nx * ny * esz, cudaMemcpyHostToDevice));
+  }
+  const size_t ncell = (size_t)nx * ny * ng;
+  if ((rc = alloc_t(c, &c->d_kap64, ncell)) || (rc = alloc_t(c, &c->d_q64, ncell)) ||
+      (rc = c->dalloc(&c->d_kap, ncell * esz)) || (rc = c->dalloc(&c->d_q, ncell * esz)))
+    return rc;
+  if ((rc = c->dalloc(&c->d_bndV, (size_t)2 * ng * nm * 2 * ny * esz)) ||
+      (rc = c->dalloc(&c->d_bndH, (size_t)2 * ng * nm * 2 * nx * esz)))
+    return rc;
+  TRT_CUDA(cudaMemset(c->d_bndV, 0, (size_t)2 * ng * nm * 2 * ny * esz));
+  TRT_CUDA(cudaMemset(c->d_bndH, 0, (size_t)2 * ng * nm * 2 * nx * esz));
+  if ((rc = c->dalloc(&c->d_wrap, (size_t)4 * ng * nx * c->mq * 2 * esz))) return rc;
+  if ((rc = alloc_t(c, &c->d_part, (size_t)4 * ng * nx * ny * trt::kNPart))) return rc;
+  TRT_CUDA(cudaMemset(c->d_part, 0, (size_t)4 * ng * nx * ny * trt::kNPart * sizeof(double)));
+  if ((rc = alloc_t(c, &c->d_err, 1))) return rc;
+  TRT_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+  if ((rc = alloc_t(c, &c->d_bval, (size_t)4 * ng))) return rc;
+  long long sz[kNOut];
+  output_sizes(nx, ny, ng, sz);
+  long long tot = 0;
+  for (int k = 0; k < kNOut; ++k) tot += sz[k];
+  if ((rc = alloc_t(c, &c->d_outs, (size_t)tot))) return rc;
+  TRT_CUDA(cudaMemset(c->d_outs, 0, (size_t)tot * sizeof(double)));
+  double** f = reinterpret_cast<double**>(&c->dout);
+  long long off = 0;
+  for (int k = 0; k < kNOut; ++k) {
+    f[k] = c->d_outs + off;
+    off += sz[k];
+  }
+  return setup_layout(c);
+}
+
+int transport_scb_impl(trt_ctx* c, int nx, int ny, int nm, int ng, double* I_avg, double* I_edgV, double* I_edgH,
+                       double* I_crn, double* Ic_edgV, double* Ic_edgH, const double* A, const double* KapE_in,
+                       const double* Src_in, const double* I_crn_old, double cl, double Delt, double* RT_Residual,
+                       int* RT_ResLoc_x, int* RT_ResLoc_y, int Res_Calc) {
+  int rc;
+  // The reference builds gamma from Delx*Dely (SCB_BGEN :342) and the source term from A(i,j);
+  // this library uses A(i,j) for the source term as well.
+  std::vector<double> area(A, A + (size_t)nx * ny);
+  TRT_CUDA(cudaMemcpyAsync(c->d_area, area.data(), area.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  TRT_CUDA(cudaMemcpyAsync(c->d_arear, c->d_area, area.size() * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  const size_t ncell = (size_t)nx * ny * ng;
+  TRT_CUDA(cudaMemcpyAsync(c->d_kap64, KapE_in, ncell * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  TRT_CUDA(cudaMemcpyAsync(c->d_kap, c->d_kap64, ncell * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  c->c = cl;
+  c->dt = Delt;
+  c->have_material = true;
+  if ((rc = pack_corner_array<double>(c, I_crn_old, c->d_state[c->cur]))) return rc;
+  if (!c->d_srcfull && (rc = c->dalloc(&c->d_srcfull, (size_t)c->state_elems() * sizeof(double)))) return rc;
+  if ((rc = pack_corner_array<double>(c, Src_in, c->d_srcfull))) return rc;
+  c->use_srcfull = true;
+  if ((rc = set_boundary_impl<double>(c, Ic_edgV, Ic_edgH))) return rc;
+  // the caller's I_edgV/I_edgH on inflow faces are not written by TRANSPORT_SCB: keep them
+  const int q = nm / 4;
+  std::vector<double> keepV((size_t)2 * ny * nm * ng), keepH((size_t)2 * nx * nm * ng);
+  for (int g = 0; g < ng; ++g)
+    for (int m = 0; m < nm; ++m) {
+      const bool xpos = (m < q || m >= 3 * q), ypos = (m < 2 * q);
+      for (int j = 0; j < ny; ++j)
+        keepV[(size_t)(g * nm + m) * ny + j] =
+            I_edgV[(xpos ? 0 : nx) + (size_t)(nx + 1) * (j + (size_t)ny * (m + (size_t)nm * g))];
+      for (int i = 0; i < nx; ++i)
+        keepH[(size_t)(g * nm + m) * nx + i] =
+            I_edgH[i + (size_t)nx * ((ypos ? 0 : ny) + (size_t)(ny + 1) * (m + (size_t)nm * g))];
+    }
+  unsigned flags = Res_Calc ? TRT_RES_CALC : 0u;
+  if ((rc = sweep_impl<double>(c, flags))) return rc;
+  if ((rc = check_err(c))) return rc;
+  if ((rc = unpack_corner_array<double>(c, c->d_state[1 - c->cur], I_crn))) return rc;
+  if ((rc = get_angular_impl<double>(c, I_avg, I_edgV, I_edgH, Ic_edgV, Ic_edgH))) return rc;
+  for (int g = 0; g < ng; ++g)
+    for (int m = 0; m < nm; ++m) {
+      const bool xpos = (m < q || m >= 3 * q), ypos = (m < 2 * q);
+      for (int j = 0; j < ny; ++j)
+        I_edgV[(xpos ? 0 : nx) + (size_t)(nx + 1) * (j + (size_t)ny * (m + (size_t)nm * g))] =
+            keepV[(size_t)(g * nm + m) * ny + j];
+      for (int i = 0; i < nx; ++i)
+        I_edgH[i + (size_t)nx * ((ypos ? 0 : ny) + (size_t)(ny + 1) * (m + (size_t)nm * g))] =
+            keepH[(size_t)(g * nm + m) * nx + i];
+    }
+  if (Res_Calc) {
+    // cells not updated by the reference keep the caller's RT_ResLoc values: read them first
+    std::vector<int> lx(RT_ResLoc_x, RT_ResLoc_x + 20 * ng), ly(RT_ResLoc_y, RT_ResLoc_y + 20 * ng);
+    TRT_CUDA(cudaMemcpyAsync(c->d_resx, lx.data(), lx.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    TRT_CUDA(cudaMemcpyAsync(c->d_resy, ly.data(), ly.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    trt::residual_reduce_kernel<<<(4 * ng + 63) / 64, 64, 0, c->stream>>>(nx, ny, nm, ng, c->d_res_m, c->d_res_loc,
+                                                                         c->d_res, c->d_resx, c->d_resy);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+    TRT_CUDA(cudaMemcpyAsync(RT_Residual, c->d_res, 20 * ng * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    TRT_CUDA(cudaMemcpyAsync(RT_ResLoc_x, c->d_resx, 20 * ng * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    TRT_CUDA(cudaMemcpyAsync(RT_ResLoc_y, c->d_resy, 20 * ng * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    TRT_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return TRT_OK;
+}
+
+// Cached handle for the reference-signature entry points, keyed by shape and directions.
+struct DropinCache {
+  std::mutex mu;
+  trt_ctx* ctx = nullptr;
+  std::vector<double> key;
+} g_cache;
+
+trt_ctx* cached_ctx(int nx, int ny, int nm, int ng, const double* ox, const double* oy, const double* dx,
+                    const double* dy, int* rc) {
+  std::vector<double> key = {(double)nx, (double)ny, (double)nm, (double)ng};
+  key.insert(key.end(), ox, ox + nm);
+  key.insert(key.end(), oy, oy + nm);
+  key.insert(key.end(), dx, dx + nx);
+  key.insert(key.end(), dy, dy + ny);
+  if (g_cache.ctx && g_cache.key == key) {
+    *rc = TRT_OK;
+    return g_cache.ctx;
+  }
+  if (g_cache.ctx) trt_destroy(g_cache.ctx);
+  g_cache.ctx = nullptr;
+  std::vector<double> w(nm, 1.0);
+  trt_ctx* c = trt_create(nx, ny, nm, ng, ox, oy, w.data(), dx, dy, TRT_PREC_FP64, 0, rc);
+  if (!c) return nullptr;
+  g_cache.ctx = c;
+  g_cache.key = key;
+  return c;
+}
+
+// Scoped device buffer for the stateless entry points.
+struct DBuf {
+  double* p = nullptr;
+  ~DBuf() {
+    if (p) cudaFree(p);
+  }
+  int alloc(size_t n) {
+    if (cudaMalloc(&p, (n ? n : 1) * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      return TRT_ERR_NOMEM;
+    }
+    return TRT_OK;
+  }
+  int put(const double* h, size_t n) {
+    int rc = alloc(n);
+    if (rc) return rc;
+    return cudaMemcpy(p, h, n * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess ? TRT_OK : TRT_ERR_CUDA;
+  }
+  int get(double* h, size_t n) const {
+    return cudaMemcpy(h, p, n * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess ? TRT_OK : TRT_ERR_CUDA;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+const char* trt_strerror(int code) {
+  switch (code) {
+    case TRT_OK: return "ok";
+    case TRT_ERR_ARG: return "invalid argument or array extent";
+    case TRT_ERR_CUDA: return "CUDA runtime error";
+    case TRT_ERR_NOMEM: return "device memory allocation failed";
+    case TRT_ERR_BUDGET: return "request exceeds the device-memory budget of the handle";
+    case TRT_ERR_TIMEOUT: return "a bounded device-side wait gave up (the handle stays usable)";
+    case TRT_ERR_STATE: return "call order: a required input has not been set";
+    case TRT_ERR_NODEV: return "no CUDA device available";
+    case TRT_ERR_UNSUPPORTED: return "shape outside the compiled kernel set";
+    default: return "unknown error";
+  }
+}
+
+unsigned long long trt_kernel_launches(void) { return g_launches.load(); }
+
+double trt_bg_planck(double T, double nu_low, double nu_high, double Comp_Unit) {
+  return bg_planck_h(T, nu_low, nu_high, Comp_Unit);
+}
+
+size_t trt_required_bytes(int n_x, int n_y, int n_m, int n_g, int precision) {
+  if (!valid_shape(n_x, n_y, n_m, n_g)) return 0;
+  const int mq = n_m / 4;
+  KernelCfg kc;
+  if (!pick_cfg(mq, precision, 0, &kc)) return 0;
+  const size_t esz = precision == TRT_PREC_FP64 ? 8 : 4;
+  const int W = default_W(32 / kc.S);
+  size_t b = 2 * layout_state_bytes(n_x, n_y, mq, n_g, W, kc.S, esz);
+  const size_t ncell = (size_t)n_x * n_y * n_g;
+  b += ncell * (16 + 2 * esz);
+  b += (size_t)2 * n_g * n_m * 2 * (n_x + n_y) * esz;
+  b += (size_t)4 * n_g * n_x * mq * 2 * esz;
+  b += (size_t)4 * n_g * n_x * n_y * trt::kNPart * 8;
+  long long sz[kNOut];
+  output_sizes(n_x, n_y, n_g, sz);
+  for (int k = 0; k < kNOut; ++k) b += sz[k] * 8;
+  b += (size_t)4 * n_x * n_y * n_m * 8;   // staging slab
+  return b + (1 << 20);
+}
+
+trt_ctx* trt_create(int n_x, int n_y, int n_m, int n_g, const double* Omega_x, const double* Omega_y,
+                    const double* quad_weight, const double* Delx, const double* Dely, int precision,
+                    size_t hbm_budget, int* status) {
+  int dummy;
+  if (!status) status = &dummy;
+  if (!valid_shape(n_x, n_y, n_m, n_g) || !Omega_x || !Omega_y || !quad_weight || !Delx || !Dely ||
+      (precision != TRT_PREC_FP64 && precision != TRT_PREC_FP32)) {
+    *status = TRT_ERR_ARG;
+    return nullptr;
+  }
+  if ((*status = device_check())) return nullptr;
+  trt_ctx* c = new (std::nothrow) trt_ctx();
+  if (!c) {
+    *status = TRT_ERR_NOMEM;
+    return nullptr;
+  }
+  c->nx = n_x; c->ny = n_y; c->nm = n_m; c->ng = n_g; c->mq = n_m / 4;
+  c->prec = precision;
+  c->budget = hbm_budget;
+  c->omx.assign(Omega_x, Omega_x + n_m);
+  c->omy.assign(Omega_y, Omega_y + n_m);
+  c->w.assign(quad_weight, quad_weight + n_m);
+  c->dx.assign(Delx, Delx + n_x);
+  c->dy.assign(Dely, Dely + n_y);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    *status = TRT_ERR_CUDA;
+    return nullptr;
+  }
+  int rc = create_buffers(c);
+  if (rc == TRT_OK && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = TRT_ERR_CUDA;
+  if (rc) {
+    trt_destroy(c);
+    *status = rc;
+    return nullptr;
+  }
+  *status = TRT_OK;
+  return c;
+}
+
+void trt_destroy(trt_ctx* c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (void* p : c->allocs) cudaFree(p);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int trt_set_tiling(trt_ctx* c, int warps_per_cta, int slices, int stages) {
+  if (!c || warps_per_cta < 0 || warps_per_cta > 16 || stages < 0 || stages > 4) return TRT_ERR_ARG;
+  if (slices && (slices & (slices - 1))) return TRT_ERR_ARG;
+  if (slices > 32) return TRT_ERR_ARG;
+  c->Wreq = warps_per_cta;
+  c->Sreq = slices;
+  c->stages = stages ? stages : 3;
+  return setup_layout(c);
+}
+
+int trt_get_tiling(const trt_ctx* c, int* W, int* S, int* D, int* stages) {
+  if (!c) return TRT_ERR_ARG;
+  if (W) *W = c->t.W;
+  if (S) *S = c->t.S;
+  if (D) *D = c->t.D;
+  if (stages) *stages = c->stages;
+  return TRT_OK;
+}
+
+int trt_set_material(trt_ctx* c, const double* KapE_in, const double* src_iso, double cl, double Delt,
+                     double Comp_Unit) {
+  if (!c || !KapE_in || !src_iso || !(cl > 0) || !(Delt > 0) || !(Comp_Unit > 0)) return TRT_ERR_ARG;
+  c->c = cl; c->dt = Delt; c->comp_unit = Comp_Unit;
+  int rc = c->prec == TRT_PREC_FP64 ? set_material_impl<double>(c, KapE_in, src_iso, false)
+                                    : set_material_impl<float>(c, KapE_in, src_iso, false);
+  if (!rc) c->have_material = true;
+  return rc;
+}
+
+int trt_set_material_device(trt_ctx* c, const double* KapE_in, const double* src_iso, double cl, double Delt,
+                            double Comp_Unit) {
+  if (!c || !KapE_in || !src_iso || !(cl > 0) || !(Delt > 0) || !(Comp_Unit > 0)) return TRT_ERR_ARG;
+  c->c = cl; c->dt = Delt; c->comp_unit = Comp_Unit;
+  int rc = c->prec == TRT_PREC_FP64 ? set_material_impl<double>(c, KapE_in, src_iso, true)
+                                    : set_material_impl<float>(c, KapE_in, src_iso, true);
+  if (!rc) c->have_material = true;
+  return rc;
+}
+
+int trt_set_source_full(trt_ctx* c, const double* Src_in) {
+  if (!c) return TRT_ERR_ARG;
+  if (!Src_in) {
+    c->use_srcfull = false;
+    return TRT_OK;
+  }
+  const size_t bytes = (size_t)c->state_elems() * c->esz();
+  if (!c->d_srcfull) {
+    int rc = c->dalloc(&c->d_srcfull, bytes);
+    if (rc) return rc;
+  }
+  int rc = c->prec == TRT_PREC_FP64 ? pack_corner_array<double>(c, Src_in, c->d_srcfull)
+                                    : pack_corner_array<float>(c, Src_in, c->d_srcfull);
+  if (!rc) c->use_srcfull = true;
+  return rc;
+}
+
+int trt_set_boundary(trt_ctx* c, const double* Ic_edgV, const double* Ic_edgH, const int* BC_Type) {
+  if (!c) return TRT_ERR_ARG;
+  if (BC_Type)
+    for (int k = 0; k < 4; ++k) c->bc[k] = BC_Type[k];
+  return c->prec == TRT_PREC_FP64 ? set_boundary_impl<double>(c, Ic_edgV, Ic_edgH)
+                                  : set_boundary_impl<float>(c, Ic_edgV, Ic_edgH);
+}
+
+int trt_bc_update(trt_ctx* c, const int* BC_Type, double bcT_left, double bcT_lower, double bcT_right,
+                  double bcT_upper, double Comp_Unit, const double* Nu_g) {
+  if (!c || !BC_Type || !Nu_g) return TRT_ERR_ARG;
+  for (int k = 0; k < 4; ++k) c->bc[k] = BC_Type[k];
+  const double Tb[4] = {bcT_left, bcT_lower, bcT_right, bcT_upper};
+  return c->prec == TRT_PREC_FP64 ? bc_update_impl<double>(c, BC_Type, Tb, Comp_Unit, Nu_g)
+                                  : bc_update_impl<float>(c, BC_Type, Tb, Comp_Unit, Nu_g);
+}
+
+int trt_init_state(trt_ctx* c, double Tini, double bcT_left, double bcT_lower, double bcT_right, double bcT_upper,
+                   double Comp_Unit, const double* Nu_g) {
+  if (!c || !Nu_g || !(Comp_Unit > 0)) return TRT_ERR_ARG;
+  c->comp_unit = Comp_Unit;
+  const double Tb[4] = {bcT_left, bcT_lower, bcT_right, bcT_upper};
+  c->swept = false;
+  return c->prec == TRT_PREC_FP64 ? init_state_impl<double>(c, Tini, Tb, Comp_Unit, Nu_g)
+                                  : init_state_impl<float>(c, Tini, Tb, Comp_Unit, Nu_g);
+}
+
+int trt_put_state(trt_ctx* c, const double* I_crn) {
+  if (!c || !I_crn) return TRT_ERR_ARG;
+  int rc = c->prec == TRT_PREC_FP64 ? pack_corner_array<double>(c, I_crn, c->d_state[c->cur])
+                                    : pack_corner_array<float>(c, I_crn, c->d_state[c->cur]);
+  if (!rc) {
+    c->have_state = true;
+    c->swept = false;
+  }
+  return rc;
+}
+
+int trt_get_state(trt_ctx* c, double* I_crn) {
+  if (!c || !I_crn) return TRT_ERR_ARG;
+  const void* st = c->d_state[c->swept ? 1 - c->cur : c->cur];
+  return c->prec == TRT_PREC_FP64 ? unpack_corner_array<double>(c, st, I_crn)
+                                  : unpack_corner_array<float>(c, st, I_crn);
+}
+
+int trt_sweep(trt_ctx* c, unsigned flags) {
+  if (!c) return TRT_ERR_ARG;
+  if (!c->have_material || (!c->have_state && !c->swept)) return TRT_ERR_STATE;
+  return c->prec == TRT_PREC_FP64 ? sweep_impl<double>(c, flags) : sweep_impl<float>(c, flags);
+}
+
+int trt_sync(trt_ctx* c) {
+  if (!c) return TRT_ERR_ARG;
+  TRT_CUDA(cudaStreamSynchronize(c->stream));
+  return check_err(c);
+}
+
+int trt_moments(trt_ctx* c, const trt_moments_host* out) {
+  if (!c || !out) return TRT_ERR_ARG;
+  if (!c->have_moments) return TRT_ERR_STATE;
+  int rc = trt_sync(c);
+  if (rc) return rc;
+  long long sz[kNOut];
+  output_sizes(c->nx, c->ny, c->ng, sz);
+  const double* const* h = reinterpret_cast<const double* const*>(out);
+  double* const* d = reinterpret_cast<double* const*>(&c->dout);
+  for (int k = 0; k < kNOut; ++k)
+    if (h[k]) TRT_CUDA(cudaMemcpyAsync((void*)h[k], d[k], sz[k] * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  TRT_CUDA(cudaStreamSynchronize(c->stream));
+  return TRT_OK;
+}
+
+int trt_get_angular(trt_ctx* c, double* I_avg, double* I_edgV, double* I_edgH, double* Ic_edgV, double* Ic_edgH) {
+  if (!c) return TRT_ERR_ARG;
+  int rc = trt_sync(c);
+  if (rc) return rc;
+  return c->prec == TRT_PREC_FP64 ? get_angular_impl<double>(c, I_avg, I_edgV, I_edgH, Ic_edgV, Ic_edgH)
+                                  : get_angular_impl<float>(c, I_avg, I_edgV, I_edgH, Ic_edgV, Ic_edgH);
+}
+
+int trt_get_residual(trt_ctx* c, double* RT_Residual, int* RT_ResLoc_x, int* RT_ResLoc_y) {
+  if (!c || !RT_Residual || !RT_ResLoc_x || !RT_ResLoc_y) return TRT_ERR_ARG;
+  if (!c->have_res) return TRT_ERR_STATE;
+  int rc = trt_sync(c);
+  if (rc) return rc;
+  TRT_CUDA(cudaMemcpy(RT_Residual, c->d_res, 20 * c->ng * sizeof(double), cudaMemcpyDeviceToHost));
+  TRT_CUDA(cudaMemcpy(RT_ResLoc_x, c->d_resx, 20 * c->ng * sizeof(int), cudaMemcpyDeviceToHost));
+  TRT_CUDA(cudaMemcpy(RT_ResLoc_y, c->d_resy, 20 * c->ng * sizeof(int), cudaMemcpyDeviceToHost));
+  return TRT_OK;
+}
+
+void* trt_stream(trt_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int trt_set_wait_limit(trt_ctx* c, unsigned polls) {
+  if (!c) return TRT_ERR_ARG;
+  c->wait_polls = polls ? polls : kDefaultWaitPolls;
+  return TRT_OK;
+}
+
+int trt_set_wait_limit_zero(trt_ctx* c) {
+  if (!c) return TRT_ERR_ARG;
+  c->wait_polls = 0;
+  return TRT_OK;
+}
+
+const double* trt_device_output(trt_ctx* c, const char* name) {
+  if (!c || !name) return nullptr;
+  double* const* d = reinterpret_cast<double* const*>(&c->dout);
+  for (int k = 0; k < kNOut; ++k)
+    if (std::strcmp(kOutNames[k], name) == 0) return d[k];
+  return nullptr;
+}
+
+int trt_transport_scb(int n_x, int n_y, int n_m, int n_g, double* I_avg, double* I_edgV, double* I_edgH,
+                      double* I_crn, double* Ic_edgV, double* Ic_edgH, const double* Omega_x,
+                      const double* Omega_y, const double* Delx, const double* Dely, const double* A,
+                      const double* KapE_in, const double* Src_in, const double* I_crn_old, double c,
+                      double Delt, int Open_Threads, double* RT_Residual, int* RT_ResLoc_x, int* RT_ResLoc_y,
+                      int Res_Calc) {
+  (void)Open_Threads;
+  if (!valid_shape(n_x, n_y, n_m, n_g) || !I_avg || !I_edgV || !I_edgH || !I_crn || !Ic_edgV || !Ic_edgH ||
+      !Omega_x || !Omega_y || !Delx || !Dely || !A || !KapE_in || !Src_in || !I_crn_old ||
+      (Res_Calc && (!RT_Residual || !RT_ResLoc_x || !RT_ResLoc_y)))
+    return TRT_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g_cache.mu);
+  int rc = TRT_OK;
+  trt_ctx* ctx = cached_ctx(n_x, n_y, n_m, n_g, Omega_x, Omega_y, Delx, Dely, &rc);
+  if (!ctx) return rc;
+  return transport_scb_impl(ctx, n_x, n_y, n_m, n_g, I_avg, I_edgV, I_edgH, I_crn, Ic_edgV, Ic_edgH, A, KapE_in,
+                            Src_in, I_crn_old, c, Delt, RT_Residual, RT_ResLoc_x, RT_ResLoc_y, Res_Calc);
+}
+
+int trt_collapse_intensities(int n_x, int n_y, int n_m, int n_g, int Open_Threads, const double* I_avg,
+                             const double* I_edgV, const double* I_edgH, const double* Omega_x,
+                             const double* Omega_y, const double* quad_weight, double Comp_Unit,
+                             double* Hg_avg_xx, double* Hg_avg_yy, double* Hg_avg_xy, double* Hg_edgV_xx,
+                             double* Hg_edgV_xy, double* Hg_edgH_yy, double* Hg_edgH_xy, double* Eg_edgV,
+                             double* Eg_edgH, double* Eg_avg, double* Fxg_edgV, double* Fyg_edgH,
+                             double* E_edgV, double* E_edgH, double* E_avg, double* Fx_edgV, double* Fy_edgH) {
+  (void)Open_Threads;
+  if (!valid_shape(n_x, n_y, n_m, n_g) || !(Comp_Unit != 0)) return TRT_ERR_ARG;
+  int rc = device_check();
+  if (rc) return rc;
+  const size_t nA = (size_t)n_x * n_y, nV = (size_t)(n_x + 1) * n_y, nH = (size_t)n_x * (n_y + 1);
+  DBuf dIa, dIv, dIh, dox, doy, dw;
+  if ((rc = dIa.put(I_avg, nA * n_m * n_g)) || (rc = dIv.put(I_edgV, nV * n_m * n_g)) ||
+      (rc = dIh.put(I_edgH, nH * n_m * n_g)) || (rc = dox.put(Omega_x, n_m)) || (rc = doy.put(Omega_y, n_m)) ||
+      (rc = dw.put(quad_weight, n_m)))
+    return rc;
+  DBuf o[17];
+  const size_t szs[17] = {nA * n_g, nA * n_g, nA * n_g, nV * n_g, nV * n_g, nH * n_g, nH * n_g, nV * n_g, nH * n_g,
+                          nA * n_g, nV * n_g, nH * n_g, nV,       nH,       nA,       nV,       nH};
+  for (int k = 0; k < 17; ++k)
+    if ((rc = o[k].alloc(szs[k]))) return rc;
+  double eps = 1e-25;
+  eps = eps / Comp_Unit;
+  trt::collapse_dropin_kernel<<<grid_for((long long)nV * n_g + nH * n_g), 256>>>(
+      n_x, n_y, n_m, n_g, dIa.p, dIv.p, dIh.p, dox.p, doy.p, dw.p, eps, o[0].p, o[1].p, o[2].p, o[3].p, o[4].p,
+      o[5].p, o[6].p, o[7].p, o[8].p, o[9].p, o[10].p, o[11].p);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  trt::MomentOut M{};
+  M.Eg_avg = o[9].p; M.Eg_edgV = o[7].p; M.Eg_edgH = o[8].p; M.Fxg_edgV = o[10].p; M.Fyg_edgH = o[11].p;
+  M.E_edgV = o[12].p; M.E_edgH = o[13].p; M.E_avg = o[14].p; M.Fx_edgV = o[15].p; M.Fy_edgH = o[16].p;
+  trt::group_sum_kernel<<<grid_for((long long)(n_x + 1) * (n_y + 1)), 256>>>(n_x, n_y, n_g, M);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  double* hs[17] = {Hg_avg_xx, Hg_avg_yy, Hg_avg_xy, Hg_edgV_xx, Hg_edgV_xy, Hg_edgH_yy, Hg_edgH_xy, Eg_edgV, Eg_edgH,
+                    Eg_avg,    Fxg_edgV,  Fyg_edgH,  E_edgV,     E_edgH,     E_avg,      Fx_edgV,    Fy_edgH};
+  for (int k = 0; k < 17; ++k)
+    if (hs[k] && (rc = o[k].get(hs[k], szs[k]))) return rc;
+  return TRT_OK;
+}
+
+int trt_fg_calc(int n_x, int n_y, int n_g, double* fg_avg_xx, double* fg_avg_yy, double* fg_avg_xy,
+                double* fg_edgV_xx, double* fg_edgV_xy, double* fg_edgH_yy, double* fg_edgH_xy,
+                const double* Hg_avg_xx, const double* Hg_avg_yy, const double* Hg_avg_xy,
+                const double* Hg_edgV_xx, const double* Hg_edgV_xy, const double* Hg_edgH_yy,
+                const double* Hg_edgH_xy, const double* HO_Eg_avg, const double* HO_Eg_edgV,
+                const double* HO_Eg_edgH, double c, int Open_Threads) {
+  (void)Open_Threads;
+  if (n_x < 1 || n_y < 1 || n_g < 1) return TRT_ERR_ARG;
+  int rc = device_check();
+  if (rc) return rc;
+  const size_t nA = (size_t)n_x * n_y * n_g, nV = (size_t)(n_x + 1) * n_y * n_g, nH = (size_t)n_x * (n_y + 1) * n_g;
+  DBuf in[10], out[7];
+  const double* hin[10] = {Hg_avg_xx, Hg_avg_yy, Hg_avg_xy, Hg_edgV_xx, Hg_edgV_xy, Hg_edgH_yy, Hg_edgH_xy,
+                           HO_Eg_avg, HO_Eg_edgV, HO_Eg_edgH};
+  const size_t nin[10] = {nA, nA, nA, nV, nV, nH, nH, nA, nV, nH};
+  for (int k = 0; k < 10; ++k)
+    if ((rc = in[k].put(hin[k], nin[k]))) return rc;
+  double* hout[7] = {fg_avg_xx, fg_avg_yy, fg_avg_xy, fg_edgV_xx, fg_edgV_xy, fg_edgH_yy, fg_edgH_xy};
+  const size_t nout[7] = {nA, nA, nA, nV, nV, nH, nH};
+  for (int k = 0; k < 7; ++k)
+    if ((rc = out[k].alloc(nout[k]))) return rc;
+  trt::fg_dropin_kernel<<<grid_for((long long)nV + nH), 256>>>(
+      (long long)nA, (long long)nV, (long long)nH, c, in[0].p, in[1].p, in[2].p, in[3].p, in[4].p, in[5].p, in[6].p,
+      in[7].p, in[8].p, in[9].p, out[0].p, out[1].p, out[2].p, out[3].p, out[4].p, out[5].p, out[6].p);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  for (int k = 0; k < 7; ++k)
+    if ((rc = out[k].get(hout[k], nout[k]))) return rc;
+  return TRT_OK;
+}
+
+static int boundary_common(int n_x, int n_y, int n_m, int n_g, int mode, const int* BC_Type, const double* I_edgV,
+                           const double* I_edgH, const double* Ox, const double* Oy, const double* w, double eps,
+                           double c, double* L, double* B, double* R, double* T, double* FL, double* FB, double* FR,
+                           double* FT) {
+  if (!valid_shape(n_x, n_y, n_m, n_g) || !BC_Type) return TRT_ERR_ARG;
+  int rc = device_check();
+  if (rc) return rc;
+  const size_t nV = (size_t)(n_x + 1) * n_y * n_m * n_g, nH = (size_t)n_x * (n_y + 1) * n_m * n_g;
+  DBuf dV, dH, dox, doy, dw, o[8];
+  if ((rc = dV.put(I_edgV, nV)) || (rc = dH.put(I_edgH, nH)) || (rc = dox.put(Ox, n_m)) || (rc = doy.put(Oy, n_m)) ||
+      (rc = dw.put(w, n_m)))
+    return rc;
+  const size_t ny_g = (size_t)n_y * n_g, nx_g = (size_t)n_x * n_g;
+  const size_t sz[8] = {ny_g, nx_g, ny_g, nx_g, ny_g, nx_g, ny_g, nx_g};
+  for (int k = 0; k < 8; ++k)
+    if ((rc = o[k].alloc(sz[k]))) return rc;
+  trt::boundary_dropin_kernel<<<grid_for(2LL * (n_x + n_y) * n_g), 256>>>(
+      n_x, n_y, n_m, n_g, mode, make_int4(BC_Type[0], BC_Type[1], BC_Type[2], BC_Type[3]), dV.p, dH.p, dox.p, doy.p,
+      dw.p, eps, c, o[0].p, o[1].p, o[2].p, o[3].p, o[4].p, o[5].p, o[6].p, o[7].p);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  double* h[8] = {L, B, R, T, FL, FB, FR, FT};
+  for (int k = 0; k < (mode == 0 ? 4 : 8); ++k)
+    if (h[k] && (rc = o[k].get(h[k], sz[k]))) return rc;
+  return TRT_OK;
+}
+
+int trt_cg_calc(int n_x, int n_y, int n_m, int n_g, double* Cg_L, double* Cg_B, double* Cg_R, double* Cg_T,
+                const double* I_edgV, const double* I_edgH, const double* Omega_x, const double* Omega_y,
+                const double* quad_weight, double Comp_Unit, const int* BC_Type, int Open_Threads) {
+  (void)Open_Threads;
+  if (!(Comp_Unit != 0)) return TRT_ERR_ARG;
+  double eps = 1e-25;
+  eps = eps / Comp_Unit;
+  return boundary_common(n_x, n_y, n_m, n_g, 0, BC_Type, I_edgV, I_edgH, Omega_x, Omega_y, quad_weight, eps, 1.0, Cg_L,
+                         Cg_B, Cg_R, Cg_T, nullptr, nullptr, nullptr, nullptr);
+}
+
+int trt_mgqd_in_calc(int n_x, int n_y, int n_m, int n_g, double* Eg_in_L, double* Eg_in_B, double* Eg_in_R,
+                     double* Eg_in_T, double* Fg_in_L, double* Fg_in_B, double* Fg_in_R, double* Fg_in_T,
+                     const double* I_edgV, const double* I_edgH, const double* Omega_x, const double* Omega_y,
+                     const double* quad_weight, double c, double Comp_Unit, const int* BC_Type,
+                     int Open_Threads) {
+  (void)Open_Threads;
+  (void)Comp_Unit;
+  return boundary_common(n_x, n_y, n_m, n_g, 1, BC_Type, I_edgV, I_edgH, Omega_x, Omega_y, quad_weight, 0.0, c,
+                         Eg_in_L, Eg_in_B, Eg_in_R, Eg_in_T, Fg_in_L, Fg_in_B, Fg_in_R, Fg_in_T);
+}
+
+int trt_gqd_in_calc(int n_x, int n_y, int n_g, double* E_in_L, double* E_in_B, double* E_in_R, double* E_in_T,
+                    double* F_in_L, double* F_in_B, double* F_in_R, double* F_in_T, const double* Eg_in_L,
+                    const double* Eg_in_B, const double* Eg_in_R, const double* Eg_in_T, const double* Fg_in_L,
+                    const double* Fg_in_B, const double* Fg_in_R, const double* Fg_in_T) {
+  if (n_x < 1 || n_y < 1 || n_g < 1) return TRT_ERR_ARG;
+  int rc = device_check();
+  if (rc) return rc;
+  const size_t ny_g = (size_t)n_y * n_g, nx_g = (size_t)n_x * n_g;
+  DBuf in[8], out[8];
+  const double* hin[8] = {Eg_in_L, Eg_in_B, Eg_in_R, Eg_in_T, Fg_in_L, Fg_in_B, Fg_in_R, Fg_in_T};
+  const size_t nin[8] = {ny_g, nx_g, ny_g, nx_g, ny_g, nx_g, ny_g, nx_g};
+  for (int k = 0; k < 8; ++k)
+    if ((rc = in[k].put(hin[k], nin[k]))) return rc;
+  double* hout[8] = {E_in_L, E_in_B, E_in_R, E_in_T, F_in_L, F_in_B, F_in_R, F_in_T};
+  const size_t nout[8] = {(size_t)n_y, (size_t)n_x, (size_t)n_y, (size_t)n_x,
+                          (size_t)n_y, (size_t)n_x, (size_t)n_y, (size_t)n_x};
+  for (int k = 0; k < 8; ++k)
+    if ((rc = out[k].alloc(nout[k]))) return rc;
+  trt::MomentOut M{};
+  M.Eg_in_L = in[0].p; M.Eg_in_B = in[1].p; M.Eg_in_R = in[2].p; M.Eg_in_T = in[3].p;
+  M.Fg_in_L = in[4].p; M.Fg_in_B = in[5].p; M.Fg_in_R = in[6].p; M.Fg_in_T = in[7].p;
+  M.E_in_L = out[0].p; M.E_in_B = out[1].p; M.E_in_R = out[2].p; M.E_in_T = out[3].p;
+  M.F_in_L = out[4].p; M.F_in_B = out[5].p; M.F_in_R = out[6].p; M.F_in_T = out[7].p;
+  trt::group_sum_kernel<<<grid_for(std::max(n_x, n_y)), 256>>>(n_x, n_y, n_g, M);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  for (int k = 0; k < 8; ++k)
+    if ((rc = out[k].get(hout[k], nout[k]))) return rc;
+  return TRT_OK;
+}
+
+int trt_rt_bc_update(int n_x, int n_y, int n_m, int n_g, const int* BC_Type, double bcT_left, double bcT_lower,
+                     double bcT_right, double bcT_upper, double Comp_Unit, const double* Nu_g, double* I_edgV,
+                     double* I_edgH, double* Ic_edgV, double* Ic_edgH) {
+  if (!valid_shape(n_x, n_y, n_m, n_g) || !BC_Type || !Nu_g || !I_edgV || !I_edgH || !Ic_edgV || !Ic_edgH)
+    return TRT_ERR_ARG;
+  int rc = device_check();
+  if (rc) return rc;
+  // Boundary faces are gathered into face-major device arrays, updated on the device by the same
+  // kernel the resident handle uses, and scattered back.  I_edgV/I_edgH faces travel as pairs of
+  // equal values so that one kernel serves both the corner-edge and the cell-edge arrays.
+  const int nx = n_x, ny = n_y, nm = n_m, ng = n_g;
+  const size_t nbV = (size_t)2 * ng * nm * 2 * ny, nbH = (size_t)2 * ng * nm * 2 * nx;
+  std::vector<double> cV(nbV), cH(nbH), eV(nbV), eH(nbH);
+  for (int side = 0; side < 2; ++side)
+    for (int g = 0; g < ng; ++g)
+      for (int m = 0; m < nm; ++m) {
+        const size_t bv = ((size_t)(side * ng + g) * nm + m) * 2 * ny, bh = ((size_t)(side * ng + g) * nm + m) * 2 * nx;
+        const int fv = side ? nx : 0, fh = side ? ny : 0;
+        for (int iy = 0; iy < 2 * ny; ++iy) cV[bv + iy] = Ic_edgV[fv + (size_t)(nx + 1) * (iy + (size_t)2 * ny * (m + (size_t)nm * g))];
+        for (int ix = 0; ix < 2 * nx; ++ix) cH[bh + ix] = Ic_edgH[ix + (size_t)2 * nx * (fh + (size_t)(ny + 1) * (m + (size_t)nm * g))];
+        for (int j = 0; j < ny; ++j) eV[bv + 2 * j] = eV[bv + 2 * j + 1] = I_edgV[fv + (size_t)(nx + 1) * (j + (size_t)ny * (m + (size_t)nm * g))];
+        for (int i = 0; i < nx; ++i) eH[bh + 2 * i] = eH[bh + 2 * i + 1] = I_edgH[i + (size_t)nx * (fh + (size_t)(ny + 1) * (m + (size_t)nm * g))];
+      }
+  std::vector<double> bval((size_t)4 * ng);
+  const double Tb[4] = {bcT_left, bcT_lower, bcT_right, bcT_upper};
+  for (int s = 0; s < 4; ++s)
+    for (int g = 0; g < ng; ++g) bval[(size_t)s * ng + g] = bg_planck_h(Tb[s], Nu_g[g], Nu_g[g + 1], Comp_Unit);
+  DBuf dcV, dcH, deV, deH, dbv;
+  if ((rc = dcV.put(cV.data(), nbV)) || (rc = dcH.put(cH.data(), nbH)) || (rc = deV.put(eV.data(), nbV)) ||
+      (rc = deH.put(eH.data(), nbH)) || (rc = dbv.put(bval.data(), bval.size())))
+    return rc;
+  const int4 bc = make_int4(BC_Type[0], BC_Type[1], BC_Type[2], BC_Type[3]);
+  const long long n = 2LL * ng * nm * 2 * std::max(nx, ny);
+  trt::bc_update_kernel<double><<<grid_for(n), 256>>>(nx, ny, nm, ng, bc, dbv.p, dcV.p, dcH.p);
+  TRT_LAUNCHED();
+  trt::bc_update_kernel<double><<<grid_for(n), 256>>>(nx, ny, nm, ng, bc, dbv.p, deV.p, deH.p);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  if ((rc = dcV.get(cV.data(), nbV)) || (rc = dcH.get(cH.data(), nbH)) || (rc = deV.get(eV.data(), nbV)) ||
+      (rc = deH.get(eH.data(), nbH)))
+    return rc;
+  for (int side = 0; side < 2; ++side)
+    for (int g = 0; g < ng; ++g)
+      for (int m = 0; m < nm; ++m) {
+        const size_t bv = ((size_t)(side * ng + g) * nm + m) * 2 * ny, bh = ((size_t)(side * ng + g) * nm + m) * 2 * nx;
+        const int fv = side ? nx : 0, fh = side ? ny : 0;
+        for (int iy = 0; iy < 2 * ny; ++iy) Ic_edgV[fv + (size_t)(nx + 1) * (iy + (size_t)2 * ny * (m + (size_t)nm * g))] = cV[bv + iy];
+        for (int ix = 0; ix < 2 * nx; ++ix) Ic_edgH[ix + (size_t)2 * nx * (fh + (size_t)(ny + 1) * (m + (size_t)nm * g))] = cH[bh + ix];
+        for (int j = 0; j < ny; ++j) I_edgV[fv + (size_t)(nx + 1) * (j + (size_t)ny * (m + (size_t)nm * g))] = eV[bv + 2 * j];
+        for (int i = 0; i < nx; ++i) I_edgH[i + (size_t)nx * (fh + (size_t)(ny + 1) * (m + (size_t)nm * g))] = eH[bh + 2 * i];
+      }
+  return TRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,359 @@
+"""Benchmark of the SCB transport sweep + QD-factor moments (the hot path of the 2D TRT solver).
+
+Metric: cell-angle-group updates/s (one update = one (cell, direction, group) SCB corner solve).
+Workload: config C1 -- 256x256 cells, 50 log-spaced groups, S16 (144 directions), 16 seeded material
+rectangles; synthetic data (seeded materials at a fixed temperature field, Planck inflow on the left).
+A step is one time step of the hot path: I_crn_old <- I_crn, one full sweep of all directions and
+groups, and the combination of moments, QD factors (fg), boundary factors (Cg) and incoming E/F.
+The corner state (15 GB FP64 / 7.5 GB FP32) is far larger than L2, so no flush is needed.
+
+  value        mixed precision (FP32 sweep, FP64 moment combination), inputs resident in HBM
+  plain_fp64   the same with FP64 throughout
+  e2e          through the C ABI with host buffers: H2D of the step's material (KapE, KapB*Bg) from
+               pinned memory, sweep + moments, D2H of fg, Cg, E and the group energies
+  roofline     scb_sweep_kernel alone (CUDA events on the library's stream), algorithmic bytes
+               B = 8*s + (8*8 + 48*8)/N_m per update (s = 8 FP64 / 4 FP32) over the measured HBM peak
+  cpu_baseline the CPU oracle (restatement of TRANSPORT_SCB with its OpenMP-over-groups loop,
+               g++ -O2 -fopenmp) on the first G_s groups of C1, one thread per group
+
+--impl reference times that CPU restatement alone (the reference Fortran cannot be built here).
+Multi-GPU (torchrun, one rank per GPU): each rank sweeps its own C1 instance (independent instances,
+no collective on the data path): weak scaling, time = max over ranks.
+"""
+import argparse
+import importlib
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", default="C1", choices=["C0", "C1"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--tiling", default="", help="warps,slices,stages override for both precisions")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            P = json.load(f)
+        return float(P["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def bytes_per_update(nm, prec):
+    s = 8 if prec == "fp64" else 4
+    return 8 * s + (8 * 8 + 48 * 8) / nm
+
+
+def traffic_from_profile(prec):
+    """Per-launch DRAM bytes of scb_sweep_kernel from the committed ncu summary, scaled to C1."""
+    path = os.path.join(ROOT, "profiles", "scb_sweep_c1.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_per_c1_launch_%s:\s*([0-9.eE+]+)" % prec, txt)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0:
+                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and "Active" in s[3 + k]
+                          and not s[3 + k].startswith("Not")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_problem(name):
+    pkg = importlib.import_module("2d_trt_rom_system_b200")
+    prob = pkg.problems.config1() if name == "C1" else pkg.problems.config0()
+    return pkg, prob
+
+
+def setup_instance(pkg, prob, precision, tiling):
+    ox, oy, w = prob.directions()
+    s = pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng, precision=precision)
+    if tiling:
+        s.set_tiling(*tiling)
+    s.init_state(prob.T0 * 1e3, [t * 1e3 for t in prob.bcT], pkg.problems.COMP_UNIT, prob.nu_eV)
+    # a temperature field between the cold initial state and the hot boundary
+    x = (np.arange(prob.nx) + 0.5) / prob.nx
+    T = np.asfortranarray(np.broadcast_to((prob.T0 + 0.5 * np.exp(-8 * x))[:, None], (prob.nx, prob.ny)))
+    kap, src = prob.material(T)
+    s.set_material(kap, src, pkg.problems.C_LIGHT, prob.dt, pkg.problems.COMP_UNIT)
+    return s, kap, src
+
+
+def time_resident(pkg, torch, s, steps, warmup, flags):
+    L = pkg.lib()
+    stream = torch.cuda.ExternalStream(s.stream())
+    for _ in range(warmup):
+        assert L.trt_sweep(s.handle, flags) == 0
+    s.sync()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    n0 = pkg.kernel_launches()
+    e0.record(stream)
+    for _ in range(steps):
+        assert L.trt_sweep(s.handle, flags) == 0
+    e1.record(stream)
+    s.sync()
+    n1 = pkg.kernel_launches()
+    return e0.elapsed_time(e1) / steps, n1 - n0
+
+
+def time_e2e(pkg, torch, s, prob, kap, src, steps, warmup):
+    """Per step: H2D of the material from pinned memory, sweep + moments, D2H of the step's result."""
+    import ctypes
+    names = ["fg_avg_xx", "fg_avg_yy", "fg_avg_xy", "fg_edgV_xx", "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy",
+             "Cg_L", "Cg_B", "Cg_R", "Cg_T", "Eg_avg", "E_avg"]
+    pin = lambda shape: torch.empty(int(np.prod(shape)), dtype=torch.float64, pin_memory=True).numpy()
+    kp = pin(kap.shape)
+    sp = pin(src.shape)
+    kp[:] = kap.ravel(order="F")
+    sp[:] = src.ravel(order="F")
+    outs = {n: pin(pkg._lib.moment_shape(n, prob.nx, prob.ny, prob.ng)) for n in names}
+    mh = pkg._lib.MomentsHost()
+    for n, a in outs.items():
+        setattr(mh, n, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    L = pkg.lib()
+    D = ctypes.POINTER(ctypes.c_double)
+    flags = pkg._lib.TRT_ROLL_STATE | pkg._lib.TRT_MOMENTS
+    C, CU = pkg.problems.C_LIGHT, pkg.problems.COMP_UNIT
+
+    def step():
+        assert L.trt_set_material(s.handle, kp.ctypes.data_as(D), sp.ctypes.data_as(D), C, prob.dt, CU) == 0
+        assert L.trt_sweep(s.handle, flags) == 0
+        assert L.trt_moments(s.handle, ctypes.byref(mh)) == 0
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    h2d = kp.nbytes + sp.nbytes
+    d2h = sum(a.nbytes for a in outs.values())
+    return dt, h2d, d2h
+
+
+def cpu_baseline(prob_full, budget_s=20.0):
+    """The oracle sweep (reference loop order, OpenMP over groups) on the first G_s groups."""
+    from oracle import oracle as O
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from common import sweep_inputs
+    pkg = importlib.import_module("2d_trt_rom_system_b200")
+    cores = os.cpu_count() or 1
+    gs = max(1, min(cores, 8, prob_full.ng))
+    prob = pkg.problems.config1(groups=prob_full.ng) if prob_full.name == "C1" else prob_full
+    prob = pkg.problems.Problem(prob.name, prob.nx, prob.ny, prob.xlen, prob.ylen, prob.edges[:gs + 1], prob.quad,
+                                prob.kappa0, prob.cv, prob.T0, prob.bcT)
+    d = sweep_inputs(prob, seed=0)
+    upd = prob.updates_per_sweep()
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < 5 and (time.perf_counter() - t_start) < budget_s:
+        t0 = time.perf_counter()
+        O.transport_scb(d["I_edgV"], d["I_edgH"], d["Ic_edgV"], d["Ic_edgH"], d["Omega_x"], d["Omega_y"], d["Delx"],
+                        d["Dely"], d["A"], d["KapE_in"], d["Src_in"], d["I_crn_old"], d["c"], d["dt"], threads=gs)
+        times.append(time.perf_counter() - t0)
+    med = float(np.median(times))
+    return {"value": upd / med, "unit": "updates/s", "cores": gs, "kind": "port",
+            "sample": f"{prob.name} first {gs} of {prob_full.ng} groups ({upd:.3g} updates), median of {len(times)} "
+                      f"sweeps, {gs} threads (OpenMP over groups), g++ -O2 -fopenmp, host has {cores} cores"}
+
+
+def dist_setup(args):
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return ws, rank, local
+
+
+def reduce_max(ws, val):
+    if ws == 1:
+        return val
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([val], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    pkg, prob = build_problem(args.config)
+    cb = cpu_baseline(prob, budget_s=60.0)
+    line = {"metric": "cell-angle-group updates/s", "value": cb["value"], "unit": "updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{prob.name}: {prob.nx}x{prob.ny} cells, {prob.ng} groups, {prob.quad} "
+                                   f"({prob.nm} directions)", "sample": cb["sample"]},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "CPU restatement of TRANSPORT_SCB (reference Fortran not buildable: no Fortran compiler, "
+                    "un-vendored LA_TOOLS)"}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    ws, rank, local = dist_setup(args)
+    pkg, prob = build_problem(args.config)
+    tiling = tuple(int(x) for x in args.tiling.split(",")) if args.tiling else None
+    upd = prob.updates_per_sweep()
+    peak, peak_kind = peaks()
+    flags = pkg._lib.TRT_ROLL_STATE | pkg._lib.TRT_MOMENTS
+    res = {}
+    precs = ["fp32"] + ([] if args.no_fp64 else ["fp64"])
+    clocks = None
+    for prec in precs:
+        s, kap, src = setup_instance(pkg, prob, "mixed" if prec == "fp32" else "fp64", tiling)
+        try:
+            barrier(ws)
+            if prec == "fp32":
+                with ClockSampler(local) as cs:
+                    ms, launches = time_resident(pkg, torch, s, args.steps, args.warmup, flags)
+                clocks = cs.summary()
+            else:
+                ms, launches = time_resident(pkg, torch, s, args.steps, args.warmup, flags)
+            ms = reduce_max(ws, ms)
+            # sweep kernel alone (no moments, no roll): per-launch duration for the roofline
+            ms_k, _ = time_resident(pkg, torch, s, max(3, args.steps // 2), 1, 0)
+            ms_k = reduce_max(ws, ms_k)
+            e2e = time_e2e(pkg, torch, s, prob, kap, src, max(3, args.steps // 4), 1) if prec == "fp32" else None
+            tl = s.tiling()
+        finally:
+            s.close()
+        B = bytes_per_update(prob.nm, prec)
+        ach = upd * B / (ms_k * 1e-3) / 1e9
+        res[prec] = dict(ms=ms, launches=launches, ms_kernel=ms_k, achieved=ach, tiling=tl, e2e=e2e, B=B)
+    main_ = res["fp32"]
+    line = {
+        "metric": "cell-angle-group updates/s",
+        "value": ws * upd / (main_["ms"] * 1e-3),
+        "unit": "updates/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": main_["ms"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 sweep, f64 moments",
+        "data": "synthetic",
+        "config": {"workload": f"{prob.name}: {prob.nx}x{prob.ny} cells, {prob.ng} log-spaced groups, {prob.quad} "
+                               f"({prob.nm} directions), 16 seeded material rectangles",
+                   "updates_per_sweep": upd, "step": "roll state + full sweep + moments/fg/Cg/E_in",
+                   "l2": "inputs larger than L2 (corner state 7.5 GB FP32 / 15 GB FP64)",
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+                   "tiling_fp32": main_["tiling"]},
+        "roofline": {"bound": "hbm", "achieved": main_["achieved"], "peak": peak, "unit": "GB/s",
+                     "frac": main_["achieved"] / peak, "traffic": traffic_from_profile("fp32"),
+                     "kernel": "scb_sweep_kernel<float>", "bytes_per_update": main_["B"],
+                     "peak_source": f"{peak_kind} hbm_gbs", "kernel_ms": main_["ms_kernel"]},
+        "gpu_launches": main_["launches"],
+        "clocks": clocks,
+    }
+    if "fp64" in res:
+        r = res["fp64"]
+        line["plain_fp64"] = {"value": ws * upd / (r["ms"] * 1e-3), "ms_per_step": r["ms"], "dtype": "f64",
+                              "roofline": {"achieved": r["achieved"], "peak": peak, "frac": r["achieved"] / peak,
+                                           "unit": "GB/s", "kernel_ms": r["ms_kernel"], "bytes_per_update": r["B"],
+                                           "traffic": traffic_from_profile("fp64")},
+                              "tiling": r["tiling"]}
+        line["mixed_over_fp64"] = line["value"] / line["plain_fp64"]["value"]
+    dt, h2d, d2h = main_["e2e"]
+    dt = reduce_max(ws, dt)
+    line["e2e"] = {"value": ws * upd / dt, "unit": "updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                   "ms_per_step": dt * 1e3, "path": "trt_set_material(host) + trt_sweep + trt_moments(host), pinned"}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(prob)
+    if rank == 0:
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

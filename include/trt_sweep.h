@@ -1,0 +1,215 @@
+/*
+ * trt_sweep.h -- C ABI of the B200 SCB transport sweep library (libtrt_sweep.so).
+ *
+ * Drop-in for the hot path of jmc9/2D_TRT_ROM_System: MODULE TRANSPORT_SOLVES
+ * (MainSrc/TRANSPORT_SOLVES.f08) and the QD-factor routines of MODULE MLOQD_SOLVES / GLOQD_SOLVES
+ * that consume its output.  Two layers:
+ *
+ *  1. Reference-signature entry points (trt_transport_scb, trt_collapse_intensities, ...): the same
+ *     arguments, in the same order and the same Fortran column-major layouts, as the Fortran
+ *     subroutine each one replaces, plus the array extents that Fortran's assumed-shape arrays carry
+ *     implicitly.  All arrays are host memory owned by the caller.  A Fortran shim module with
+ *     BIND(C) interfaces re-exposes them under the original subroutine names.
+ *  2. A resident-state handle (trt_create ... trt_destroy): the corner intensities I_crn and the
+ *     boundary intensities stay in device memory between calls; only materials go in and moments,
+ *     QD factors and boundary factors come out.
+ *
+ * Conventions: every array argument is a plain pointer to doubles (REAL*8) or ints (INTEGER), in the
+ * reference's layout; indices inside arrays follow Fortran order (first index fastest).  Every
+ * function returns 0 on success or a negative TRT_ERR_* code (the reference STOPs; a shim STOPs
+ * with trt_strerror(code)).  A handle is single-threaded and not re-entrant; it owns one CUDA stream.
+ * Functions that return data to host memory synchronise that stream.  There is no CPU fallback: with
+ * no usable CUDA device every call returns TRT_ERR_NODEV.
+ */
+#ifndef TRT_SWEEP_H
+#define TRT_SWEEP_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TRT_OK 0
+#define TRT_ERR_ARG (-1)          /* invalid argument or extent */
+#define TRT_ERR_CUDA (-2)         /* CUDA runtime error */
+#define TRT_ERR_NOMEM (-3)        /* device or pinned allocation failed */
+#define TRT_ERR_BUDGET (-4)       /* request exceeds the handle's device-memory budget */
+#define TRT_ERR_TIMEOUT (-5)      /* a bounded device-side wait gave up; the handle stays usable */
+#define TRT_ERR_STATE (-6)        /* call order: e.g. trt_sweep before trt_set_material */
+#define TRT_ERR_NODEV (-7)        /* no CUDA device */
+#define TRT_ERR_UNSUPPORTED (-8)  /* shape outside the compiled kernel set (N_m/4 > 64) */
+
+#define TRT_PREC_FP64 0   /* plain: FP64 state and arithmetic throughout */
+#define TRT_PREC_FP32 1   /* mixed: FP32 state and sweep, FP64 moment combination and QD factors */
+
+/* trt_sweep flags */
+#define TRT_ROLL_STATE 1u  /* I_crn_old = I_crn before sweeping (start of a time step, ALGORITHMS.f08:397) */
+#define TRT_MOMENTS 2u     /* combine moments, fg, Cg, incoming E/F and group sums after the sweep */
+#define TRT_RES_CALC 4u    /* corner-balance residual norms (TRANSPORT_SOLVES.f08:249-323) */
+
+/* ---------------------------------------------------------------------------------------------
+ * Layer 1: reference-signature entry points.
+ * ------------------------------------------------------------------------------------------- */
+
+/* Replaces SUBROUTINE TRANSPORT_SCB, MainSrc/TRANSPORT_SOLVES.f08:14-27 (body :28-327).
+ * I_avg(n_x,n_y,n_m,n_g), I_edgV(n_x+1,n_y,n_m,n_g), I_edgH(n_x,n_y+1,n_m,n_g): out (entries on inflow
+ * faces are left as the caller had them, as in the reference); I_crn(2n_x,2n_y,n_m,n_g): out;
+ * Ic_edgV(n_x+1,2n_y,n_m,n_g), Ic_edgH(2n_x,n_y+1,n_m,n_g): in (inflow faces) / out;
+ * A(n_x,n_y); KapE_in(n_x,n_y,n_g); Src_in, I_crn_old (2n_x,2n_y,n_m,n_g);
+ * RT_Residual(4,n_g,5), RT_ResLoc_x/y(4,n_g,5): written when Res_Calc != 0.
+ * Open_Threads is accepted for signature compatibility and ignored. */
+int trt_transport_scb(int n_x, int n_y, int n_m, int n_g, double* I_avg, double* I_edgV, double* I_edgH,
+                      double* I_crn, double* Ic_edgV, double* Ic_edgH, const double* Omega_x,
+                      const double* Omega_y, const double* Delx, const double* Dely, const double* A,
+                      const double* KapE_in, const double* Src_in, const double* I_crn_old, double c,
+                      double Delt, int Open_Threads, double* RT_Residual, int* RT_ResLoc_x, int* RT_ResLoc_y,
+                      int Res_Calc);
+
+/* Replaces SUBROUTINE COLLAPSE_INTENSITIES, MainSrc/TRANSPORT_SOLVES.f08:381-397 (body :398-511).
+ * Group-resolved outputs are (n_x[+1], n_y[+1], n_g), totals (n_x[+1], n_y[+1]). */
+int trt_collapse_intensities(int n_x, int n_y, int n_m, int n_g, int Open_Threads, const double* I_avg,
+                             const double* I_edgV, const double* I_edgH, const double* Omega_x,
+                             const double* Omega_y, const double* quad_weight, double Comp_Unit,
+                             double* Hg_avg_xx, double* Hg_avg_yy, double* Hg_avg_xy, double* Hg_edgV_xx,
+                             double* Hg_edgV_xy, double* Hg_edgH_yy, double* Hg_edgH_xy, double* Eg_edgV,
+                             double* Eg_edgH, double* Eg_avg, double* Fxg_edgV, double* Fyg_edgH,
+                             double* E_edgV, double* E_edgH, double* E_avg, double* Fx_edgV, double* Fy_edgH);
+
+/* Replaces SUBROUTINE fg_Calc, MainSrc/MLOQD_SOLVES.f08:619-621 (body :622-678). */
+int trt_fg_calc(int n_x, int n_y, int n_g, double* fg_avg_xx, double* fg_avg_yy, double* fg_avg_xy,
+                double* fg_edgV_xx, double* fg_edgV_xy, double* fg_edgH_yy, double* fg_edgH_xy,
+                const double* Hg_avg_xx, const double* Hg_avg_yy, const double* Hg_avg_xy,
+                const double* Hg_edgV_xx, const double* Hg_edgV_xy, const double* Hg_edgH_yy,
+                const double* Hg_edgH_xy, const double* HO_Eg_avg, const double* HO_Eg_edgV,
+                const double* HO_Eg_edgH, double c, int Open_Threads);
+
+/* Replaces SUBROUTINE Cg_Calc, MainSrc/MLOQD_SOLVES.f08:367 (body :368-488).
+ * Cg_L/Cg_R(n_y,n_g), Cg_B/Cg_T(n_x,n_g); BC_Type(4) = L, B, R, T. */
+int trt_cg_calc(int n_x, int n_y, int n_m, int n_g, double* Cg_L, double* Cg_B, double* Cg_R, double* Cg_T,
+                const double* I_edgV, const double* I_edgH, const double* Omega_x, const double* Omega_y,
+                const double* quad_weight, double Comp_Unit, const int* BC_Type, int Open_Threads);
+
+/* Replaces SUBROUTINE MGQD_In_Calc, MainSrc/MLOQD_SOLVES.f08:493-494 (body :495-614). */
+int trt_mgqd_in_calc(int n_x, int n_y, int n_m, int n_g, double* Eg_in_L, double* Eg_in_B, double* Eg_in_R,
+                     double* Eg_in_T, double* Fg_in_L, double* Fg_in_B, double* Fg_in_R, double* Fg_in_T,
+                     const double* I_edgV, const double* I_edgH, const double* Omega_x, const double* Omega_y,
+                     const double* quad_weight, double c, double Comp_Unit, const int* BC_Type,
+                     int Open_Threads);
+
+/* Replaces SUBROUTINE GQD_In_Calc, MainSrc/GLOQD_SOLVES.f08:263-264 (body :265-290). */
+int trt_gqd_in_calc(int n_x, int n_y, int n_g, double* E_in_L, double* E_in_B, double* E_in_R, double* E_in_T,
+                    double* F_in_L, double* F_in_B, double* F_in_R, double* F_in_T, const double* Eg_in_L,
+                    const double* Eg_in_B, const double* Eg_in_R, const double* Eg_in_T, const double* Fg_in_L,
+                    const double* Fg_in_B, const double* Fg_in_R, const double* Fg_in_T);
+
+/* Replaces SUBROUTINE RT_BC_UPDATE, MainSrc/UPDATES.f08:12 (body :13-105). Nu_g has n_g+1 edges. */
+int trt_rt_bc_update(int n_x, int n_y, int n_m, int n_g, const int* BC_Type, double bcT_left, double bcT_lower,
+                     double bcT_right, double bcT_upper, double Comp_Unit, const double* Nu_g, double* I_edgV,
+                     double* I_edgH, double* Ic_edgV, double* Ic_edgH);
+
+/* Bg_planck_calc, MainSrc/TEMP_FUNCTIONS.f08:90-108 (host evaluation, used for boundary values). */
+double trt_bg_planck(double T, double nu_low, double nu_high, double Comp_Unit);
+
+/* ---------------------------------------------------------------------------------------------
+ * Layer 2: resident-state handle.  Replaces the state hand-off of ALGORITHMS.f08:397 and the call
+ * sequence TRANSPORT_SCB -> COLLAPSE_INTENSITIES -> [RT_BC_UPDATE, MGQD_In_Calc] -> fg_Calc ->
+ * Cg_Calc of ALGORITHMS.f08:541-572 and :1045-1095.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct trt_ctx trt_ctx;
+
+/* Host destinations for trt_moments; any NULL field is skipped.  Shapes as in the reference
+ * (RT_INIT/MGQD_INIT, MainSrc/INITIALIZERS.f08:51-76,193-230).  Fyg_edgH/Fy_edgH are weighted
+ * by Omega_x as COLLAPSE_INTENSITIES writes them (TRANSPORT_SOLVES.f08:469); Fyg_edgH_true/
+ * Fy_edgH_true are the Omega_y-weighted fluxes. */
+typedef struct trt_moments_host {
+  double *Hg_avg_xx, *Hg_avg_yy, *Hg_avg_xy, *Hg_edgV_xx, *Hg_edgV_xy, *Hg_edgH_yy, *Hg_edgH_xy;
+  double *Eg_avg, *Eg_edgV, *Eg_edgH, *Fxg_edgV, *Fyg_edgH;
+  double *fg_avg_xx, *fg_avg_yy, *fg_avg_xy, *fg_edgV_xx, *fg_edgV_xy, *fg_edgH_yy, *fg_edgH_xy;
+  double *Cg_L, *Cg_B, *Cg_R, *Cg_T;
+  double *Eg_in_L, *Eg_in_B, *Eg_in_R, *Eg_in_T, *Fg_in_L, *Fg_in_B, *Fg_in_R, *Fg_in_T;
+  double *E_avg, *E_edgV, *E_edgH, *Fx_edgV, *Fy_edgH;
+  double *E_in_L, *E_in_B, *E_in_R, *E_in_T, *F_in_L, *F_in_B, *F_in_R, *F_in_T;
+  double *Fyg_edgH_true, *Fy_edgH_true;
+} trt_moments_host;
+
+/* Create a handle for an n_x x n_y grid, n_m directions (n_m % 4 == 0, quadrant-ordered as
+ * INPUT_QUAD builds them, INPUTS.f08:1658-1669) and n_g groups.  precision = TRT_PREC_*.
+ * hbm_budget = bytes of device memory the handle may allocate (0 = no limit).  *status receives 0 or
+ * a TRT_ERR_* code; NULL is returned on failure. */
+trt_ctx* trt_create(int n_x, int n_y, int n_m, int n_g, const double* Omega_x, const double* Omega_y,
+                    const double* quad_weight, const double* Delx, const double* Dely, int precision,
+                    size_t hbm_budget, int* status);
+void trt_destroy(trt_ctx* ctx);
+
+/* Device bytes a handle of this shape would allocate (for admission against a budget). */
+size_t trt_required_bytes(int n_x, int n_y, int n_m, int n_g, int precision);
+
+/* Kernel tiling: warps per CTA (1..16), direction slices per warp (1,2,4,8,16,32; 0 = automatic),
+ * TMA pipeline stages (1..4).  Re-lays out the resident state. */
+int trt_set_tiling(trt_ctx* ctx, int warps_per_cta, int slices, int stages);
+int trt_get_tiling(const trt_ctx* ctx, int* warps_per_cta, int* slices, int* dirs_per_lane, int* stages);
+
+/* Material for the next sweeps: KapE_in(n_x,n_y,n_g) (the opacity before the 1/(c*Delt) term of
+ * TRANSPORT_SOLVES.f08:47) and the isotropic corner source src_iso(n_x,n_y,n_g) = KapB*Bg
+ * (UPDATES.f08:141-150).  c and Delt as passed to TRANSPORT_SCB; Comp_Unit as passed to
+ * COLLAPSE_INTENSITIES (eps = 1e-25/Comp_Unit). */
+int trt_set_material(trt_ctx* ctx, const double* KapE_in, const double* src_iso, double c, double Delt,
+                     double Comp_Unit);
+/* Same with device pointers (FP64, same layouts), stream-ordered on the handle's stream. */
+int trt_set_material_device(trt_ctx* ctx, const double* d_KapE_in, const double* d_src_iso, double c,
+                            double Delt, double Comp_Unit);
+/* Anisotropic per-corner source Src_in(2n_x,2n_y,n_m,n_g) instead of src_iso (NULL reverts). */
+int trt_set_source_full(trt_ctx* ctx, const double* Src_in);
+
+/* Boundary corner-edge intensities on the inflow faces, taken from full reference arrays
+ * Ic_edgV(n_x+1,2n_y,n_m,n_g) and Ic_edgH(2n_x,n_y+1,n_m,n_g); BC_Type(4) = L, B, R, T selects
+ * Planck/vacuum (0) or reflective (1) sides for the moment combination. */
+int trt_set_boundary(trt_ctx* ctx, const double* Ic_edgV, const double* Ic_edgH, const int* BC_Type);
+/* RT_BC_UPDATE (UPDATES.f08:12-105) applied to the resident boundary intensities. */
+int trt_bc_update(trt_ctx* ctx, const int* BC_Type, double bcT_left, double bcT_lower, double bcT_right,
+                  double bcT_upper, double Comp_Unit, const double* Nu_g);
+
+/* RT_INIT (INITIALIZERS.f08:84-107): I_crn = I_crn_old = Bg(Tini) per group, then the Planck
+ * inflow faces of RT_BC_UPDATE((/0,0,0,0/), ...). */
+int trt_init_state(trt_ctx* ctx, double Tini, double bcT_left, double bcT_lower, double bcT_right,
+                   double bcT_upper, double Comp_Unit, const double* Nu_g);
+/* I_crn_old <- I_crn(2n_x,2n_y,n_m,n_g) (restart input). */
+int trt_put_state(trt_ctx* ctx, const double* I_crn);
+/* I_crn(2n_x,2n_y,n_m,n_g) of the latest sweep (restart output / state hand-off). */
+int trt_get_state(trt_ctx* ctx, double* I_crn);
+
+/* One sweep of all directions and groups, enqueued on the handle's stream (flags: TRT_*). */
+int trt_sweep(trt_ctx* ctx, unsigned flags);
+/* Wait for the handle's stream; returns the first error a device-side check reported. */
+int trt_sync(trt_ctx* ctx);
+/* Copy the combined moments / factors of the latest TRT_MOMENTS sweep to host memory. */
+int trt_moments(trt_ctx* ctx, const trt_moments_host* out);
+/* Angular intensities of the latest sweep in the reference layouts (any pointer may be NULL). */
+int trt_get_angular(trt_ctx* ctx, double* I_avg, double* I_edgV, double* I_edgH, double* Ic_edgV,
+                    double* Ic_edgH);
+/* Residual norms of the latest TRT_RES_CALC sweep: RT_Residual(4,n_g,5), RT_ResLoc_x/y(4,n_g,5). */
+int trt_get_residual(trt_ctx* ctx, double* RT_Residual, int* RT_ResLoc_x, int* RT_ResLoc_y);
+
+/* The handle's cudaStream_t (as void*), for callers that order their own work after a sweep. */
+void* trt_stream(trt_ctx* ctx);
+/* Device pointer of a combined output (name as in trt_moments_host, e.g. "fg_avg_xx"), or NULL. */
+const double* trt_device_output(trt_ctx* ctx, const char* name);
+
+/* Bound on the polls of each device-side wait of the sweep (0 = default).  The failure path of a
+ * wait that never completes is exercised with trt_set_wait_limit_zero: every wait gives up at once,
+ * the kernel drains its outstanding copies, sets its error word and returns; trt_sync then reports
+ * TRT_ERR_TIMEOUT and the handle stays usable. */
+int trt_set_wait_limit(trt_ctx* ctx, unsigned polls);
+int trt_set_wait_limit_zero(trt_ctx* ctx);
+
+/* Message for a TRT_ERR_* code. */
+const char* trt_strerror(int code);
+/* Number of kernels this library has launched in this process (instrumentation). */
+unsigned long long trt_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TRT_SWEEP_H */

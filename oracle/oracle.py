@@ -1,0 +1,191 @@
+"""ctypes wrapper of the CPU oracle (liboracle.so, trt_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, the smoke check and the CPU-baseline leg of bench.py,
+as the checker.  Parity status of the oracle: UNPINNED (see trt_oracle.cpp).
+
+Functions mirror the reference subroutines (Fortran argument order, Fortran-ordered numpy arrays).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_i, _d = ctypes.c_int, ctypes.c_double
+
+_SIG = {
+    "oracle_sigint": (_d, [_d]),
+    "oracle_bg_planck": (_d, [_d, _d, _d, _d]),
+    "oracle_kapb": (_d, [_d, _d, _d]),
+    "oracle_scb_cell_ge": (None, [_d, _d, _d, _d, _d, _D]),
+    "oracle_transport_scb": (_i, [_i, _i, _i, _i] + [_D] * 6 + [_D] * 8 + [_d, _d, _i, _D, _I, _I, _i, _i]),
+    "oracle_collapse_intensities": (_i, [_i, _i, _i, _i, _i, _D, _D, _D, _D, _D, _D, _d] + [_D] * 17),
+    "oracle_fg_calc": (_i, [_i, _i, _i] + [_D] * 17 + [_d, _i]),
+    "oracle_cg_calc": (_i, [_i, _i, _i, _i] + [_D] * 9 + [_d, _I, _i]),
+    "oracle_mgqd_in_calc": (_i, [_i, _i, _i, _i] + [_D] * 13 + [_d, _d, _I, _i]),
+    "oracle_gqd_in_calc": (_i, [_i, _i, _i] + [_D] * 16),
+    "oracle_rt_bc_update": (_i, [_i, _i, _i, _i, _I, _d, _d, _d, _d, _d, _D, _D, _D, _D, _D]),
+    "oracle_openmp_max_threads": (_i, []),
+}
+
+_lib = None
+
+
+def build():
+    """Compile liboracle.so with the Makefile beside this file (g++, -O2 -fopenmp)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        for n, (r, a) in _SIG.items():
+            f = getattr(L, n)
+            f.restype, f.argtypes = r, a
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    if a is None:
+        return None
+    if a.dtype == np.int32:
+        return a.ctypes.data_as(_I)
+    assert a.dtype == np.float64 and a.flags.f_contiguous
+    return a.ctypes.data_as(_D)
+
+
+def F(a, dtype=np.float64):
+    return np.asfortranarray(np.asarray(a, dtype=dtype))
+
+
+def zeros(*shape):
+    return np.zeros(shape, order="F")
+
+
+def transport_scb(I_edgV, I_edgH, Ic_edgV, Ic_edgH, Omega_x, Omega_y, Delx, Dely, A, KapE_in, Src_in, I_crn_old, c,
+                  Delt, threads=1, res_calc=False, solver=0, RT_ResLoc_init=0):
+    """TRANSPORT_SCB.  I_edgV/I_edgH/Ic_edgV/Ic_edgH are copied (in/out in the reference); returns a dict."""
+    nx, ny = len(Delx), len(Dely)
+    nm = len(Omega_x)
+    ng = KapE_in.shape[2]
+    out = dict(I_avg=zeros(nx, ny, nm, ng), I_edgV=F(I_edgV).copy(order="F"), I_edgH=F(I_edgH).copy(order="F"),
+               I_crn=zeros(2 * nx, 2 * ny, nm, ng), Ic_edgV=F(Ic_edgV).copy(order="F"),
+               Ic_edgH=F(Ic_edgH).copy(order="F"), RT_Residual=zeros(4, ng, 5),
+               RT_ResLoc_x=np.full((4, ng, 5), RT_ResLoc_init, dtype=np.int32, order="F"),
+               RT_ResLoc_y=np.full((4, ng, 5), RT_ResLoc_init, dtype=np.int32, order="F"))
+    args = [F(Omega_x), F(Omega_y), F(Delx), F(Dely), F(A), F(KapE_in), F(Src_in), F(I_crn_old)]
+    rc = lib().oracle_transport_scb(nx, ny, nm, ng, _p(out["I_avg"]), _p(out["I_edgV"]), _p(out["I_edgH"]),
+                                    _p(out["I_crn"]), _p(out["Ic_edgV"]), _p(out["Ic_edgH"]), *[_p(a) for a in args],
+                                    float(c), float(Delt), int(threads), _p(out["RT_Residual"]),
+                                    _p(out["RT_ResLoc_x"]), _p(out["RT_ResLoc_y"]), 1 if res_calc else 0, int(solver))
+    assert rc == 0
+    return out
+
+
+COLLAPSE_OUT = ["Hg_avg_xx", "Hg_avg_yy", "Hg_avg_xy", "Hg_edgV_xx", "Hg_edgV_xy", "Hg_edgH_yy", "Hg_edgH_xy",
+                "Eg_edgV", "Eg_edgH", "Eg_avg", "Fxg_edgV", "Fyg_edgH", "E_edgV", "E_edgH", "E_avg", "Fx_edgV",
+                "Fy_edgH"]
+
+
+def collapse_intensities(I_avg, I_edgV, I_edgH, Omega_x, Omega_y, quad_weight, comp_unit, threads=1):
+    nx, ny, nm, ng = I_avg.shape
+    A, V, H = (nx, ny), (nx + 1, ny), (nx, ny + 1)
+    shapes = [A + (ng,)] * 3 + [V + (ng,)] * 2 + [H + (ng,)] * 2 + [V + (ng,), H + (ng,), A + (ng,), V + (ng,),
+                                                                   H + (ng,), V, H, A, V, H]
+    out = {k: zeros(*s) for k, s in zip(COLLAPSE_OUT, shapes)}
+    rc = lib().oracle_collapse_intensities(nx, ny, nm, ng, int(threads), _p(F(I_avg)), _p(F(I_edgV)), _p(F(I_edgH)),
+                                           _p(F(Omega_x)), _p(F(Omega_y)), _p(F(quad_weight)), float(comp_unit),
+                                           *[_p(out[k]) for k in COLLAPSE_OUT])
+    assert rc == 0
+    return out
+
+
+FG_OUT = ["fg_avg_xx", "fg_avg_yy", "fg_avg_xy", "fg_edgV_xx", "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy"]
+
+
+def fg_calc(m, c, threads=1):
+    """m: dict with Hg_* and Eg_avg/Eg_edgV/Eg_edgH (HO_Eg_*)."""
+    nx, ny, ng = m["Hg_avg_xx"].shape
+    shapes = [(nx, ny, ng)] * 3 + [(nx + 1, ny, ng)] * 2 + [(nx, ny + 1, ng)] * 2
+    out = {k: zeros(*s) for k, s in zip(FG_OUT, shapes)}
+    ins = [F(m[k]) for k in ("Hg_avg_xx", "Hg_avg_yy", "Hg_avg_xy", "Hg_edgV_xx", "Hg_edgV_xy", "Hg_edgH_yy",
+                             "Hg_edgH_xy", "Eg_avg", "Eg_edgV", "Eg_edgH")]
+    rc = lib().oracle_fg_calc(nx, ny, ng, *[_p(out[k]) for k in FG_OUT], *[_p(a) for a in ins], float(c), int(threads))
+    assert rc == 0
+    return out
+
+
+def cg_calc(I_edgV, I_edgH, Omega_x, Omega_y, quad_weight, comp_unit, bc_type, threads=1):
+    nxp, ny, nm, ng = I_edgV.shape
+    nx = nxp - 1
+    out = dict(Cg_L=zeros(ny, ng), Cg_B=zeros(nx, ng), Cg_R=zeros(ny, ng), Cg_T=zeros(nx, ng))
+    rc = lib().oracle_cg_calc(nx, ny, nm, ng, _p(out["Cg_L"]), _p(out["Cg_B"]), _p(out["Cg_R"]), _p(out["Cg_T"]),
+                              _p(F(I_edgV)), _p(F(I_edgH)), _p(F(Omega_x)), _p(F(Omega_y)), _p(F(quad_weight)),
+                              float(comp_unit), _p(np.ascontiguousarray(bc_type, dtype=np.int32)), int(threads))
+    assert rc == 0
+    return out
+
+
+IN_OUT = ["Eg_in_L", "Eg_in_B", "Eg_in_R", "Eg_in_T", "Fg_in_L", "Fg_in_B", "Fg_in_R", "Fg_in_T"]
+
+
+def mgqd_in_calc(I_edgV, I_edgH, Omega_x, Omega_y, quad_weight, c, comp_unit, bc_type, threads=1):
+    nxp, ny, nm, ng = I_edgV.shape
+    nx = nxp - 1
+    out = {k: zeros(ny if k[-1] in "LR" else nx, ng) for k in IN_OUT}
+    rc = lib().oracle_mgqd_in_calc(nx, ny, nm, ng, *[_p(out[k]) for k in IN_OUT], _p(F(I_edgV)), _p(F(I_edgH)),
+                                   _p(F(Omega_x)), _p(F(Omega_y)), _p(F(quad_weight)), float(c), float(comp_unit),
+                                   _p(np.ascontiguousarray(bc_type, dtype=np.int32)), int(threads))
+    assert rc == 0
+    return out
+
+
+def gqd_in_calc(m):
+    nx = m["Eg_in_B"].shape[0]
+    ny, ng = m["Eg_in_L"].shape
+    keys = ["E_in_L", "E_in_B", "E_in_R", "E_in_T", "F_in_L", "F_in_B", "F_in_R", "F_in_T"]
+    out = {k: zeros(ny if k[-1] in "LR" else nx) for k in keys}
+    rc = lib().oracle_gqd_in_calc(nx, ny, ng, *[_p(out[k]) for k in keys], *[_p(F(m[k])) for k in IN_OUT])
+    assert rc == 0
+    return out
+
+
+def rt_bc_update(bc_type, bcT_left, bcT_lower, bcT_right, bcT_upper, comp_unit, nu_g, I_edgV, I_edgH, Ic_edgV,
+                 Ic_edgH):
+    """In-place on Fortran-ordered copies; returns them."""
+    arrs = [F(a).copy(order="F") for a in (I_edgV, I_edgH, Ic_edgV, Ic_edgH)]
+    nx = arrs[1].shape[0]
+    ny, nm, ng = arrs[0].shape[1], arrs[0].shape[2], arrs[0].shape[3]
+    rc = lib().oracle_rt_bc_update(nx, ny, nm, ng, _p(np.ascontiguousarray(bc_type, dtype=np.int32)),
+                                   float(bcT_left), float(bcT_lower), float(bcT_right), float(bcT_upper),
+                                   float(comp_unit), _p(F(nu_g)), *[_p(a) for a in arrs])
+    assert rc == 0
+    return arrs
+
+
+def bg_planck(T, nu_lo, nu_hi, comp_unit):
+    return lib().oracle_bg_planck(float(T), float(nu_lo), float(nu_hi), float(comp_unit))
+
+
+def sigint(z):
+    return lib().oracle_sigint(float(z))
+
+
+def scb_cell_ge(omx, omy, dx, dy, kapE, Q):
+    q = np.ascontiguousarray(Q, dtype=np.float64).copy()
+    lib().oracle_scb_cell_ge(float(omx), float(omy), float(dx), float(dy), float(kapE), q.ctypes.data_as(_D))
+    return q
+
+
+def max_threads():
+    return lib().oracle_openmp_max_threads()

@@ -1,0 +1,68 @@
+"""The C ABI library loads and exports every symbol include/trt_sweep.h declares (CPU only, no kernels)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from common import pkg
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "trt_sweep.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(trt_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_reference_signatures():
+    names = declared_functions()
+    for n in ("trt_transport_scb", "trt_collapse_intensities", "trt_fg_calc", "trt_cg_calc", "trt_mgqd_in_calc",
+              "trt_gqd_in_calc", "trt_rt_bc_update", "trt_create", "trt_sweep", "trt_moments", "trt_destroy",
+              "trt_strerror", "trt_get_state", "trt_put_state", "trt_get_angular"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    L = ctypes.CDLL(pkg.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+    # and the Python binding declares a signature for each of them
+    assert set(declared_functions()) <= set(pkg._lib.SIGNATURES)
+
+
+def test_strerror_codes():
+    L = pkg.lib()
+    for code in range(0, -9, -1):
+        msg = L.trt_strerror(code).decode()
+        assert msg and msg != "unknown error"
+    assert L.trt_strerror(-99).decode() == "unknown error"
+
+
+def test_required_bytes_and_argument_checks():
+    L = pkg.lib()
+    assert L.trt_required_bytes(0, 4, 8, 1, 0) == 0           # invalid extent
+    assert L.trt_required_bytes(4, 4, 6, 1, 0) == 0           # N_m not a multiple of 4
+    b64 = L.trt_required_bytes(256, 256, 144, 50, 0)
+    b32 = L.trt_required_bytes(256, 256, 144, 50, 1)
+    # two FP64 corner states of config C1 are ~30 GB; FP32 halves them
+    assert 29e9 < b64 < 40e9 and 14e9 < b32 < 22e9
+    st = ctypes.c_int(0)
+    d = np.zeros(8)
+    h = L.trt_create(0, 4, 8, 1, *[d.ctypes.data_as(ctypes.POINTER(ctypes.c_double))] * 5, 0, 0, ctypes.byref(st))
+    assert not h and st.value == pkg._lib.TRT_ERR_ARG
+
+
+def test_no_device_is_reported_not_emulated():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    L = pkg.lib()
+    st = ctypes.c_int(0)
+    one = np.ones(8)
+    p = one.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    h = L.trt_create(4, 4, 8, 1, p, p, p, p, p, 0, 0, ctypes.byref(st))
+    assert not h and st.value == pkg._lib.TRT_ERR_NODEV

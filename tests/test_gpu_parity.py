@@ -1,0 +1,353 @@
+"""GPU parity: the CUDA library, called through its C ABI, against the CPU oracle.
+
+Bars:
+  * FP64 sweep vs the oracle's device-arithmetic mode (closed-form cell solve, solver 1): bit-identical;
+  * FP64 sweep vs the reference restatement (Gaussian elimination with complete pivoting, solver 0):
+    <= 1e-12 relative per group;
+  * moments / QD factors / boundary factors (fused epilogue, different summation order): <= 1e-13;
+  * reference-signature moment routines (same summation order): bit-identical;
+  * FP32 ("mixed") sweep: <= 1e-5 relative per group.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from common import CU, C, golden_arrays, load_golden, oracle_full, pkg, rel_err, rel_err_per_group, sweep_inputs
+
+pytestmark = pytest.mark.gpu
+
+MOM_KEYS = ("Hg_avg_xx", "Hg_avg_yy", "Hg_avg_xy", "Hg_edgV_xx", "Hg_edgV_xy", "Hg_edgH_yy", "Hg_edgH_xy",
+            "Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH", "E_avg", "E_edgV", "E_edgH", "Fx_edgV",
+            "Fy_edgH")
+FG_KEYS = ("fg_avg_xx", "fg_avg_yy", "fg_avg_xy", "fg_edgV_xx", "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy")
+BND_KEYS = ("Cg_L", "Cg_B", "Cg_R", "Cg_T", "Eg_in_L", "Eg_in_B", "Eg_in_R", "Eg_in_T", "Fg_in_L", "Fg_in_B",
+            "Fg_in_R", "Fg_in_T", "E_in_L", "E_in_B", "E_in_R", "E_in_T", "F_in_L", "F_in_B", "F_in_R", "F_in_T")
+
+
+def dropin_sweep(d, res_calc=False):
+    nx, ny, nm, ng = len(d["Delx"]), len(d["Dely"]), len(d["Omega_x"]), d["KapE_in"].shape[2]
+    out = dict(I_avg=np.zeros((nx, ny, nm, ng), order="F"), I_edgV=d["I_edgV"].copy(order="F"),
+               I_edgH=d["I_edgH"].copy(order="F"), I_crn=np.zeros((2 * nx, 2 * ny, nm, ng), order="F"),
+               Ic_edgV=d["Ic_edgV"].copy(order="F"), Ic_edgH=d["Ic_edgH"].copy(order="F"),
+               RT_Residual=np.zeros((4, ng, 5), order="F"),
+               RT_ResLoc_x=np.zeros((4, ng, 5), dtype=np.int32, order="F"),
+               RT_ResLoc_y=np.zeros((4, ng, 5), dtype=np.int32, order="F"))
+    pkg.TRANSPORT_SCB(out["I_avg"], out["I_edgV"], out["I_edgH"], out["I_crn"], out["Ic_edgV"], out["Ic_edgH"],
+                      d["Omega_x"], d["Omega_y"], d["Delx"], d["Dely"], d["A"], d["KapE_in"], d["Src_in"],
+                      d["I_crn_old"], d["c"], d["dt"], 1, out["RT_Residual"], out["RT_ResLoc_x"], out["RT_ResLoc_y"],
+                      res_calc)
+    return out
+
+
+def resident(d, precision="fp64", tiling=None, bc_type=(0, 0, 0, 0)):
+    nx, ny, ng = len(d["Delx"]), len(d["Dely"]), d["KapE_in"].shape[2]
+    s = pkg.TransportSweep(nx, ny, d["Omega_x"], d["Omega_y"], d["w"], d["Delx"], d["Dely"], ng, precision=precision)
+    if tiling:
+        s.set_tiling(**tiling)
+    s.put_state(d["I_crn_old"])
+    s.set_boundary(d["Ic_edgV"], d["Ic_edgH"], bc_type)
+    s.set_material(d["KapE_in"], d["src_iso"], d["c"], d["dt"], CU)
+    return s
+
+
+SHAPES = [("C0", lambda: pkg.problems.config0()),
+          ("3x4_S8", lambda: pkg.problems.random_small(1, 3, 4, 3, "S8")),
+          ("1x1_S8", lambda: pkg.problems.random_small(2, 1, 1, 2, "S8")),
+          ("5x7_S12", lambda: pkg.problems.random_small(3, 5, 7, 2, "S12")),
+          ("37x21_S16", lambda: pkg.problems.random_small(4, 37, 21, 2, "S16")),
+          ("2x3_1dtest", lambda: pkg.problems.random_small(5, 2, 3, 2, "1d_test")),
+          ("9x40_abu20", lambda: pkg.problems.random_small(6, 9, 40, 1, "abu20"))]
+
+
+@pytest.mark.parametrize("name,make", SHAPES, ids=[s[0] for s in SHAPES])
+def test_dropin_transport_scb_bit_identical_to_oracle(oracle, name, make):
+    d = sweep_inputs(make(), seed=7)
+    g = dropin_sweep(d, res_calc=True)
+    r1 = oracle_full(d, solver=1, res_calc=True)
+    for k in ("I_crn", "I_avg", "I_edgV", "I_edgH", "Ic_edgV", "Ic_edgH"):
+        assert np.array_equal(g[k], r1[k]), k
+    assert np.array_equal(g["RT_Residual"], r1["RT_Residual"])
+    assert np.array_equal(g["RT_ResLoc_x"], r1["RT_ResLoc_x"]) and np.array_equal(g["RT_ResLoc_y"], r1["RT_ResLoc_y"])
+    r0 = oracle_full(d, solver=0)
+    for k in ("I_crn", "I_avg", "I_edgV", "I_edgH"):
+        assert rel_err_per_group(g[k], r0[k]) <= 1e-12, k
+
+
+@pytest.mark.parametrize("case", load_golden(), ids=lambda c: c["name"])
+def test_dropin_matches_exact_rational_sweep(case):
+    d, exp = golden_arrays(case)
+    g = dropin_sweep(d)
+    for k in ("I_crn", "I_avg", "Ic_edgV", "Ic_edgH"):
+        assert rel_err_per_group(g[k], exp[k]) < 2e-14, k
+
+
+@pytest.mark.parametrize("name,make", SHAPES[:5], ids=[s[0] for s in SHAPES[:5]])
+def test_resident_sweep_and_fused_moments(oracle, name, make):
+    prob = make()
+    d = sweep_inputs(prob, seed=11)
+    ref = oracle_full(d, solver=1)
+    with resident(d) as s:
+        s.sweep(moments=True)
+        I = s.get_state()
+        m = s.moments()
+    assert np.array_equal(I, ref["I_crn"])
+    for k in MOM_KEYS:
+        gaxis = -1 if m[k].ndim == 3 else None
+        err = rel_err_per_group(m[k], ref[k]) if gaxis else rel_err(m[k], ref[k])
+        assert err < 1e-13, k
+    for k in FG_KEYS:
+        assert np.max(np.abs(m[k] - ref[k])) < 1e-13, k
+    for k in BND_KEYS:
+        assert rel_err(m[k], ref[k]) < 1e-13 or np.max(np.abs(m[k] - ref[k])) < 1e-300, k
+    # Omega_y-weighted horizontal flux (the reference's Fyg_edgH is Omega_x-weighted, :469): the
+    # oracle's collapse with Omega_y passed as the x cosine yields it
+    rc = oracle.collapse_intensities(ref["I_avg"], ref["I_edgV"], ref["I_edgH"], d["Omega_y"], d["Omega_y"], d["w"],
+                                     CU)
+    assert rel_err_per_group(m["Fyg_edgH_true"], rc["Fyg_edgH"]) < 1e-13
+
+
+@pytest.mark.parametrize("tiling", [dict(warps=1), dict(warps=2, stages=1), dict(warps=8, stages=2),
+                                    dict(warps=3, stages=4), dict(warps=16)])
+def test_tiling_does_not_change_results(tiling):
+    prob = pkg.problems.random_small(8, 33, 29, 2, "S16")
+    d = sweep_inputs(prob, seed=5)
+    with resident(d) as s:
+        s.sweep()
+        I0, m0 = s.get_state(), s.moments(["Eg_avg", "fg_edgV_xy", "Cg_T"])
+    with resident(d, tiling=tiling) as s:
+        s.sweep()
+        I1, m1 = s.get_state(), s.moments(["Eg_avg", "fg_edgV_xy", "Cg_T"])
+    assert np.array_equal(I0, I1)
+    for k in m0:
+        assert np.array_equal(m0[k], m1[k]), k
+
+
+@pytest.mark.parametrize("slices", [1, 2, 4, 8, 16, 32])
+def test_direction_slicing_variants(oracle, slices):
+    prob = pkg.problems.random_small(9, 12, 10, 2, "S8")
+    d = sweep_inputs(prob, seed=9)
+    ref = oracle_full(d, solver=1)
+    try:
+        s = resident(d, tiling=dict(slices=slices))
+    except pkg.TrtError:
+        pytest.skip(f"no compiled kernel with {slices} slices for 10 directions per quadrant")
+    with s:
+        s.sweep()
+        I = s.get_state()
+        m = s.moments(["Eg_avg", "fg_avg_xy"])
+    assert np.array_equal(I, ref["I_crn"])
+    assert rel_err_per_group(m["Eg_avg"], ref["Eg_avg"]) < 1e-13
+
+
+def test_multi_step_state_roll(oracle):
+    """Three time steps: I_crn_old <- I_crn between steps (ALGORITHMS.f08:397), with a new material each step."""
+    prob = pkg.problems.random_small(10, 11, 9, 3, "S8")
+    d = sweep_inputs(prob, seed=1)
+    rng = np.random.default_rng(3)
+    with resident(d) as s:
+        I_old = d["I_crn_old"]
+        for step in range(3):
+            T = prob.T0 * rng.uniform(0.5, 3.0, (prob.nx, prob.ny))
+            kap, src = prob.material(T)
+            dd = dict(d, KapE_in=kap, src_iso=src,
+                      Src_in=np.asfortranarray(np.repeat(np.repeat(src, 2, 0), 2, 1)[:, :, None, :].repeat(prob.nm, 2)),
+                      I_crn_old=I_old)
+            ref = oracle_full(dd, solver=1)
+            s.set_material(kap, src, d["c"], d["dt"], CU)
+            s.sweep(roll=(step > 0), moments=True)
+            I = s.get_state()
+            assert np.array_equal(I, ref["I_crn"]), step
+            m = s.moments(["fg_avg_xx", "Cg_L"])
+            assert np.max(np.abs(m["fg_avg_xx"] - ref["fg_avg_xx"])) < 1e-13
+            I_old = ref["I_crn"]
+
+
+def test_reflective_boundaries(oracle):
+    """Reflective left and top sides: sweep, combine, RT_BC_UPDATE (mirror copies), sweep again."""
+    prob = pkg.problems.random_small(12, 6, 5, 2, "S8")
+    d = sweep_inputs(prob, seed=4)
+    bc = (1, 0, 0, 1)
+    bT = d["bcT_eV"]
+    with resident(d, bc_type=bc) as s:
+        ref = oracle_full(d, solver=1, bc_type=bc)
+        s.sweep(moments=True)
+        assert np.array_equal(s.get_state(), ref["I_crn"])
+        m = s.moments(["Cg_L", "Cg_T", "Cg_R", "Eg_in_L", "Eg_in_R", "E_in_L", "F_in_R"])
+        for k in m:
+            assert rel_err(m[k], ref[k]) < 1e-13 or np.max(np.abs(m[k] - ref[k])) == 0, k
+        s.bc_update(bc, bT, CU, d["nu"])
+        IV, IH, IcV, IcH = oracle.rt_bc_update(bc, *bT, CU, d["nu"], ref["I_edgV"], ref["I_edgH"], ref["Ic_edgV"],
+                                               ref["Ic_edgH"])
+        d2 = dict(d, I_edgV=IV, I_edgH=IH, Ic_edgV=IcV, Ic_edgH=IcH)
+        ref2 = oracle_full(d2, solver=1, bc_type=bc)
+        s.sweep(moments=True)
+        assert np.array_equal(s.get_state(), ref2["I_crn"])
+        ang = s.angular(("Ic_edgV", "Ic_edgH"))
+        assert np.array_equal(ang["Ic_edgV"], ref2["Ic_edgV"]) and np.array_equal(ang["Ic_edgH"], ref2["Ic_edgH"])
+
+
+def test_init_state_matches_rt_init(oracle):
+    """RT_INIT: corners and boundaries at Bg(Tini), then the Planck inflow faces."""
+    prob = pkg.problems.random_small(13, 4, 6, 3, "S12")
+    ox, oy, w = prob.directions()
+    with pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng) as s:
+        s.init_state(prob.T0 * 1e3, [t * 1e3 for t in prob.bcT], CU, prob.nu_eV)
+        I = s.get_state()
+        ang = s.angular(("Ic_edgV", "Ic_edgH"))
+    d = sweep_inputs(prob, random_old=False)
+    # the host Planck evaluations differ only in the exp of the C library vs numpy (<= 1 ulp)
+    assert rel_err_per_group(I, d["I_crn_old"]) < 1e-15
+    assert rel_err_per_group(ang["Ic_edgV"], d["Ic_edgV"]) < 1e-15
+    assert rel_err_per_group(ang["Ic_edgH"], d["Ic_edgH"]) < 1e-15
+
+
+def test_fp32_mixed_sweep_against_fp64_oracle(oracle):
+    prob = pkg.problems.config0()
+    d = sweep_inputs(prob, seed=2)
+    ref = oracle_full(d, solver=0)
+    with resident(d, precision="fp32") as s:
+        s.sweep(moments=True)
+        I = s.get_state()
+        m = s.moments(["Eg_avg", "E_avg", "fg_avg_xx", "fg_edgV_xx", "Cg_L", "Fx_edgV"])
+    assert rel_err_per_group(I, ref["I_crn"]) < 1e-5
+    assert rel_err(m["E_avg"], ref["E_avg"]) < 1e-5
+    assert np.max(np.abs(m["fg_avg_xx"] - ref["fg_avg_xx"])) < 1e-5
+    assert np.all(np.isfinite(m["fg_edgV_xx"]))
+
+
+def test_reference_signature_moment_routines_bit_identical(oracle):
+    prob = pkg.problems.random_small(14, 7, 6, 3, "S12")
+    d = sweep_inputs(prob, seed=8)
+    r = oracle_full(d, solver=0)
+    nx, ny, ng = prob.nx, prob.ny, prob.ng
+    A, V, H = (nx, ny), (nx + 1, ny), (nx, ny + 1)
+    shapes = [A + (ng,)] * 3 + [V + (ng,)] * 2 + [H + (ng,)] * 2 + [V + (ng,), H + (ng,), A + (ng,), V + (ng,),
+                                                                   H + (ng,), V, H, A, V, H]
+    names = oracle.COLLAPSE_OUT
+    out = {k: np.zeros(s, order="F") for k, s in zip(names, shapes)}
+    pkg.COLLAPSE_INTENSITIES(4, r["I_avg"], r["I_edgV"], r["I_edgH"], d["Omega_x"], d["Omega_y"], d["w"], CU,
+                             *[out[k] for k in names])
+    for k in names:
+        assert np.array_equal(out[k], r[k]), k
+    fg = {k: np.zeros_like(r[k], order="F") for k in oracle.FG_OUT}
+    pkg.fg_Calc(*[fg[k] for k in oracle.FG_OUT], *[r[k] for k in ("Hg_avg_xx", "Hg_avg_yy", "Hg_avg_xy",
+                                                                   "Hg_edgV_xx", "Hg_edgV_xy", "Hg_edgH_yy",
+                                                                   "Hg_edgH_xy", "Eg_avg", "Eg_edgV", "Eg_edgH")],
+                C, 4)
+    for k in oracle.FG_OUT:
+        assert np.array_equal(fg[k], r[k]), k
+    for bc in ((0, 0, 0, 0), (1, 0, 1, 0), (0, 1, 0, 1)):
+        rr = oracle.cg_calc(r["I_edgV"], r["I_edgH"], d["Omega_x"], d["Omega_y"], d["w"], CU, bc)
+        cg = {k: np.zeros_like(rr[k], order="F") for k in ("Cg_L", "Cg_B", "Cg_R", "Cg_T")}
+        pkg.Cg_Calc(cg["Cg_L"], cg["Cg_B"], cg["Cg_R"], cg["Cg_T"], r["I_edgV"], r["I_edgH"], d["Omega_x"],
+                    d["Omega_y"], d["w"], CU, bc, 4)
+        for k in cg:
+            assert np.array_equal(cg[k], rr[k]), (bc, k)
+        ri = oracle.mgqd_in_calc(r["I_edgV"], r["I_edgH"], d["Omega_x"], d["Omega_y"], d["w"], C, CU, bc)
+        gi = {k: np.zeros_like(ri[k], order="F") for k in oracle.IN_OUT}
+        pkg.MGQD_In_Calc(*[gi[k] for k in oracle.IN_OUT], r["I_edgV"], r["I_edgH"], d["Omega_x"], d["Omega_y"],
+                         d["w"], C, CU, bc, 4)
+        for k in gi:
+            assert np.array_equal(gi[k], ri[k]), (bc, k)
+        rg = oracle.gqd_in_calc(ri)
+        gg = {k: np.zeros_like(rg[k]) for k in rg}
+        pkg.GQD_In_Calc(*[gg[k] for k in ("E_in_L", "E_in_B", "E_in_R", "E_in_T", "F_in_L", "F_in_B", "F_in_R",
+                                          "F_in_T")], *[ri[k] for k in oracle.IN_OUT])
+        for k in gg:
+            assert np.array_equal(gg[k], rg[k]), k
+
+
+def test_rt_bc_update_signature_bit_identical(oracle):
+    prob = pkg.problems.random_small(15, 5, 4, 2, "S8")
+    d = sweep_inputs(prob, seed=3)
+    r = oracle_full(d, solver=1)
+    for bc in ((0, 0, 0, 0), (1, 1, 1, 1), (1, 0, 0, 1)):
+        exp = oracle.rt_bc_update(bc, 800.0, 0.0, 300.0, 50.0, CU, d["nu"], r["I_edgV"], r["I_edgH"], r["Ic_edgV"],
+                                  r["Ic_edgH"])
+        got = [r[k].copy(order="F") for k in ("I_edgV", "I_edgH", "Ic_edgV", "Ic_edgH")]
+        pkg.RT_BC_UPDATE(bc, 800.0, 0.0, 300.0, 50.0, CU, d["nu"], *got)
+        for a, b in zip(got, exp):
+            assert np.array_equal(a, b), bc
+
+
+def _c1_moments(s, prob, kap, src, Tini, bcT, names=("E_avg", "Fx_edgV", "Eg_avg", "fg_avg_xx")):
+    s.init_state(Tini, bcT, CU, prob.nu_eV)
+    s.set_material(kap, src, C, prob.dt, CU)
+    s.sweep(moments=True)
+    return s.moments(names)
+
+
+def test_superposition_and_scaling_at_full_c1_size():
+    """Size-independent properties at the C1 size (256^2 cells, 50 groups, S16): the sweep is linear in
+    (source, inflow) from a zero state -- inflow+source = inflow alone + source alone -- and doubling
+    the source doubles every intensity moment."""
+    prob = pkg.problems.config1()
+    ox, oy, w = prob.directions()
+    kap, src = prob.material(np.full((prob.nx, prob.ny), 0.3))
+    zero = np.zeros_like(src, order="F")
+    with pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng) as s:
+        both = _c1_moments(s, prob, kap, src, 0.0, [1000.0, 0.0, 0.0, 0.0])
+        only_src = _c1_moments(s, prob, kap, src, 0.0, [0.0, 0.0, 0.0, 0.0])
+        only_bc = _c1_moments(s, prob, kap, zero, 0.0, [1000.0, 0.0, 0.0, 0.0])
+        twice = _c1_moments(s, prob, kap, np.asfortranarray(2.0 * src), 0.0, [0.0, 0.0, 0.0, 0.0])
+    assert np.all(np.isfinite(both["E_avg"])) and np.all(both["E_avg"] > 0)
+    assert rel_err(both["E_avg"], only_src["E_avg"] + only_bc["E_avg"]) < 1e-12
+    assert rel_err(both["Fx_edgV"], only_src["Fx_edgV"] + only_bc["Fx_edgV"]) < 1e-12
+    assert rel_err_per_group(twice["Eg_avg"], 2.0 * only_src["Eg_avg"]) < 1e-12
+
+
+def test_equilibrium_at_full_c1_size():
+    """Infinite-medium equilibrium at the C1 size: state, inflow and source at one temperature keep
+    every intensity at B_g, so E_g = 4 pi B_g / c and the QD and boundary factors are the quadrature's
+    moments."""
+    prob = pkg.problems.config1()
+    ox, oy, w = prob.directions()
+    T = 0.05
+    kap, src = prob.material(np.full((prob.nx, prob.ny), T))
+    with pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng) as s:
+        m = _c1_moments(s, prob, kap, src, T * 1e3, [T * 1e3] * 4,
+                        names=("Eg_avg", "fg_avg_xx", "fg_avg_xy", "fg_edgH_yy", "Cg_B"))
+    nu = prob.nu_eV
+    B = np.array([pkg.problems.bg_planck(T * 1e3, nu[g], nu[g + 1]) for g in range(prob.ng)])
+    live = B > 1e-200
+    expE = 4 * np.pi * B / C
+    got = m["Eg_avg"][:, :, live] - 1e-38 * np.sum(w) / C
+    assert np.max(np.abs(got / expE[live] - 1.0)) < 1e-11
+    assert np.max(np.abs(m["fg_avg_xx"][:, :, live] - np.sum(w * ox * ox) / np.sum(w))) < 1e-12
+    assert np.max(np.abs(m["fg_avg_xy"][:, :, live])) < 1e-12
+    q = len(w) // 4
+    out_B = slice(2 * q, 4 * q)
+    assert np.max(np.abs(m["Cg_B"][:, live] - np.sum(oy[out_B] * w[out_B]) / np.sum(w[out_B]))) < 1e-12
+
+
+def test_api_errors_and_timeout_path():
+    prob = pkg.problems.random_small(16, 8, 8, 2, "S8")
+    d = sweep_inputs(prob, seed=1)
+    ox, oy, w = d["Omega_x"], d["Omega_y"], d["w"]
+    with pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, d["Delx"], d["Dely"], prob.ng) as s:
+        with pytest.raises(pkg.TrtError) as e:
+            s.sweep()
+        assert e.value.code == pkg._lib.TRT_ERR_STATE
+    with pytest.raises(pkg.TrtError) as e:
+        pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, d["Delx"], d["Dely"], prob.ng, hbm_budget=1024)
+    assert e.value.code == pkg._lib.TRT_ERR_BUDGET
+    # a wait that never completes: every poll budget zero -> error status, then the handle recovers
+    ref = oracle_full(d, solver=1)
+    with resident(d) as s:
+        L = pkg.lib()
+        assert L.trt_set_wait_limit_zero(s.handle) == 0
+        assert L.trt_sweep(s.handle, 2) == 0
+        assert L.trt_sync(s.handle) == pkg._lib.TRT_ERR_TIMEOUT
+        assert L.trt_set_wait_limit(s.handle, 0) == 0
+        s.sweep(moments=True)
+        assert np.array_equal(s.get_state(), ref["I_crn"])
+
+
+def test_launch_counter_counts_library_kernels():
+    before = pkg.kernel_launches()
+    prob = pkg.problems.random_small(17, 4, 4, 1, "S8")
+    d = sweep_inputs(prob)
+    with resident(d) as s:
+        s.sweep(moments=True)
+    assert pkg.kernel_launches() - before >= 3
