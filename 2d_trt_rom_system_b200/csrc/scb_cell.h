@@ -35,7 +35,9 @@ namespace trt {
 TRT_HD double tfma(double x, double y, double z) { return fma(x, y, z); }
 TRT_HD float tfma(float x, float y, float z) { return fmaf(x, y, z); }
 
-// Per-(cell, direction) geometry of the corner matrix, sweep frame.
+// Per-(cell, direction) geometry of the corner matrix, sweep frame.  ax4 = |Omega_x|/4 and
+// ay4 = |Omega_y|/4 are per-direction constants; scaling by powers of two is exact, so
+// a = ax4*dy equals (|Ox| dy)/4 of SCB_BGEN bit for bit.
 template <class R>
 struct ScbGeom {
   R a, b;      // |Ox| dy / 4, |Oy| dx / 4
@@ -43,24 +45,26 @@ struct ScbGeom {
 };
 
 template <class R>
-TRT_HD ScbGeom<R> scb_geom(R ax, R ay, R dx, R dy) {
+TRT_HD ScbGeom<R> scb_geom(R ax4, R ay4, R dx, R dy) {
   ScbGeom<R> G;
-  R axdy = ax * dy;
-  R aydx = ay * dx;
-  G.a = axdy * R(0.25);
-  G.b = aydx * R(0.25);
-  G.hx = axdy * R(0.5);
-  G.hy = aydx * R(0.5);
+  G.a = ax4 * dy;
+  G.b = ay4 * dx;
+  G.hx = G.a + G.a;
+  G.hy = G.b + G.b;
   return G;
 }
 
-// gamma of SCB_BGEN: (|Ox| dy + |Oy| dx + kapE * dx*dy) / 4, with the same summation order.
+// kA4 = (kapE * dx*dy) / 4, shared by every direction of a cell.
 template <class R>
-TRT_HD R scb_gamma(R ax, R ay, R dx, R dy, R kapE) {
-  R axdy = ax * dy;
-  R aydx = ay * dx;
-  R area = dx * dy;
-  return (axdy + aydx + kapE * area) * R(0.25);
+TRT_HD R scb_kA4(R dx, R dy, R kapE) {
+  return (kapE * (dx * dy)) * R(0.25);
+}
+
+// gamma of SCB_BGEN, (|Ox| dy + |Oy| dx + kapE dx dy) / 4: the same sum with every term scaled by
+// the exact factor 1/4 first.
+template <class R>
+TRT_HD R scb_gamma(const ScbGeom<R>& G, R kA4) {
+  return (G.a + G.b) + kA4;
 }
 
 // Solve one cell.  s[k] = total corner source (isotropic/anisotropic source plus I_old/(c dt)),

@@ -80,11 +80,45 @@ __host__ __device__ inline size_t sweep_smem_bytes(int W, long long chunk, int s
   return ring + bars + hand + dtab + 16;
 }
 
-template <class Real, int S, int DMAX, bool SRC_FULL>
+// Reduce-scatter of the 16 moment slots over the S slices of a row (xor partners R, 2R, ..., 16):
+// after log2(S) levels every lane holds 16/S consecutive slots summed over the slices, in a fixed
+// order.  Returns the index of the first slot this lane holds.
+// With S = 32 the last level is a plain pairwise sum and only the lower lane of the pair owns the
+// slot (*owner = false for the other).
+template <int S, int R>
+__device__ __forceinline__ int slice_reduce_scatter(double (&v)[16], int s, bool* owner) {
+  int base = 0;
+  int width = 16;
+  *owner = true;
+#pragma unroll
+  for (int o = 16; o >= R; o >>= 1) {
+    if (o >= R * S) continue;   // lane bits above the slice bits: not a slice partner
+    const bool upper = (s & (o / R)) != 0;
+    if (width == 1) {
+      v[0] = v[0] + __shfl_xor_sync(0xffffffffu, v[0], o);
+      if (upper) *owner = false;
+      continue;
+    }
+    const int half = width / 2;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (k < half) {
+        const double send = upper ? v[k] : v[k + half];
+        const double keep = upper ? v[k + half] : v[k];
+        v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+    }
+    if (upper) base += half;
+    width = half;
+  }
+  return base;
+}
+
+template <class Real, int S, int D, bool SRC_FULL>
 __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a) {
   constexpr int R = 32 / S;
   constexpr int NV = 16 / (int)sizeof(Real);
-  using V = typename Vec16<Real>::type;
+  constexpr int NSLOT = S >= 16 ? 1 : 16 / S;   // moment slots a lane holds after the reduce-scatter
 
   const Tiling t = a.t;
   const int W = t.W;
@@ -95,8 +129,11 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   const int rho = warp * R + r;
   const bool fx = (q == 1 || q == 2), fy = (q >= 2);
   const int stages = a.stages;
-  const long long chunk = a.chunk;
-  const uint32_t stage_bytes = (uint32_t)(W * chunk * (long long)sizeof(Real));
+  const int chunk = (int)a.chunk;
+  const uint32_t stage_bytes = (uint32_t)(W * chunk * (int)sizeof(Real));
+  // slices of the last direction block that hold a direction (all slices of the earlier blocks do)
+  const int s_last = mq - (D - 1) * S;
+  const int nl_last = R * s_last;
 
   extern __shared__ __align__(128) unsigned char smem[];
   Real* ring = reinterpret_cast<Real*>(smem);
@@ -104,8 +141,11 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   Real* hand = reinterpret_cast<Real*>(mbar + stages);
   Real* dtab = hand + 2 * W * mq * 2;
 
-  for (int k = threadIdx.x; k < kNDirRow * mq; k += blockDim.x)
-    dtab[k] = a.dirtab[(size_t)q * kNDirRow * mq + k];
+  for (int k = threadIdx.x; k < kNDirRow * mq; k += blockDim.x) {
+    Real v = a.dirtab[(size_t)q * kNDirRow * mq + k];
+    if (k < 2 * mq) v = v * Real(0.25);   // |Omega| / 4 for the corner-matrix geometry
+    dtab[k] = v;
+  }
   if (threadIdx.x == 0) {
     for (int k = 0; k < stages; ++k) mbar_init(&mbar[k], 1);
     fence_mbar_init();
@@ -125,7 +165,7 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   }
 
   const Real rcdt = a.rcdt;
-  const long long nxy = (long long)nx * ny;
+  const int nxy = nx * ny;
   Real* wrapc = a.wrap + (size_t)blockIdx.x * nx * mq * 2;
   double* partg = a.part + ((size_t)(q * ng + g) * nxy) * kNPart;
   const int sideVin = fx ? 1 : 0, sideVout = fx ? 0 : 1;
@@ -134,10 +174,33 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   Real* bVout = a.bndV + ((size_t)(sideVout * ng + g) * nm + q * mq) * (2 * ny);
   const Real* bHin = a.bndH + ((size_t)(sideHin * ng + g) * nm + q * mq) * (2 * nx);
   Real* bHout = a.bndH + ((size_t)(sideHout * ng + g) * nm + q * mq) * (2 * nx);
+  const Real* kapg = a.kap + (size_t)nxy * g;
+  const Real* qisog = SRC_FULL ? nullptr : a.qiso + (size_t)nxy * g;
+  const int byo = fy ? 1 : 0;   // physical corner-edge offset of the frame's bottom corner
+  const int bxo = fx ? 1 : 0;   // ... of the frame's left corner
 
-  Real vb[DMAX], vt[DMAX], hl[DMAX], hr[DMAX];
+  Real vb[D], vt[D], hl[D], hr[D];
 #pragma unroll
-  for (int d = 0; d < DMAX; ++d) vb[d] = vt[d] = hl[d] = hr[d] = Real(0);
+  for (int d = 0; d < D; ++d) vb[d] = vt[d] = hl[d] = hr[d] = Real(0);
+
+  // lane position: column ip of round n (ip < 0 before the lane starts); advanced incrementally
+  int ip = -rho, n = 0;
+  // material of the lane's cell at the current step, loaded one step ahead
+  Real mdx = Real(0), mdy = Real(0), mA4 = Real(0), mkp = Real(0), mqs = Real(0);
+  auto load_material = [&](int ipn, int nn) {
+    const int jpn = nn * t.H + rho;
+    if (ipn >= 0 && ipn < nx && nn < t.nr && jpn < ny) {
+      const int i = fx ? nx - 1 - ipn : ipn;
+      const int j = fy ? ny - 1 - jpn : jpn;
+      const int cell = i + nx * j;
+      mdx = a.dx[i];
+      mdy = a.dy[j];
+      mA4 = a.area[cell] * Real(0.25);
+      mkp = kapg[cell] + rcdt;
+      if (!SRC_FULL) mqs = qisog[cell];
+    }
+  };
+  load_material(ip, n);
 
   bool timed_out = false;
   int stage = 0;
@@ -146,74 +209,66 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   for (int T = 0; T < Tsteps; ++T) {
     if (!mbar_wait_bounded(&mbar[stage], phase, a.max_polls)) timed_out = true;
     const Real* sm = ring + (size_t)stage * W * chunk + (size_t)warp * chunk;
-    const long long gchunk = ((long long)T * W + warp) * chunk;
+    const int gchunk = (T * W + warp) * chunk;
 
-    const int tau = T - rho;
-    int n = 0, ip = 0, jp = 0;
-    bool active = false;
-    if (tau >= 0 && !timed_out) {
-      n = tau / t.P;
-      ip = tau - n * t.P;
-      jp = n * t.H + rho;
-      active = (n < t.nr) && (ip < nx) && (jp < ny);
-    }
+    const int jp = n * t.H + rho;
+    const bool active = !timed_out && ip >= 0 && ip < nx && n < t.nr && jp < ny;
+    const int i = fx ? nx - 1 - ip : ip;
+    const int j = fy ? ny - 1 - jp : jp;
 
-    Real topL[DMAX], topR[DMAX];
+    Real topL[D], topR[D];
     Real acc[13];
 #pragma unroll
     for (int v = 0; v < 13; ++v) acc[v] = Real(0);
 #pragma unroll
-    for (int d = 0; d < DMAX; ++d) topL[d] = topR[d] = Real(0);
+    for (int d = 0; d < D; ++d) topL[d] = topR[d] = Real(0);
 
-    int i = 0, j = 0;
     if (active) {
-      i = fx ? nx - 1 - ip : ip;
-      j = fy ? ny - 1 - jp : jp;
-      const long long cell = (long long)i + (long long)nx * j;
-      const Real dx = a.dx[i], dy = a.dy[j];
-      const Real A4 = a.area[cell] * Real(0.25);
-      const Real kp = a.kap[cell + nxy * g] + rcdt;
-      Real qs = Real(0);
-      if (!SRC_FULL) qs = a.qiso[cell + nxy * g];
-
+      const Real dx = mdx, dy = mdy, A4 = mA4, kp = mkp, qs = mqs;
       if (ip == 0) {
 #pragma unroll
-        for (int d = 0; d < DMAX; ++d) {
+        for (int d = 0; d < D; ++d) {
           const int ml = d * S + s;
-          if (d < t.D && ml < mq) {
-            vb[d] = bVin[(size_t)ml * 2 * ny + 2 * j + (fy ? 1 : 0)];
-            vt[d] = bVin[(size_t)ml * 2 * ny + 2 * j + (fy ? 0 : 1)];
+          if (d < D - 1 || s < s_last) {
+            vb[d] = bVin[ml * 2 * ny + 2 * j + byo];
+            vt[d] = bVin[ml * 2 * ny + 2 * j + 1 - byo];
           }
         }
       }
       if (r == 0) {
 #pragma unroll
-        for (int d = 0; d < DMAX; ++d) {
+        for (int d = 0; d < D; ++d) {
           const int ml = d * S + s;
-          if (d < t.D && ml < mq) {
+          if (d < D - 1 || s < s_last) {
+            const Real* src;
+            int o0, o1;
             if (rho == 0) {
               if (n == 0) {
-                hl[d] = bHin[(size_t)ml * 2 * nx + 2 * i + (fx ? 1 : 0)];
-                hr[d] = bHin[(size_t)ml * 2 * nx + 2 * i + (fx ? 0 : 1)];
+                src = bHin + ml * 2 * nx + 2 * i;
+                o0 = bxo;
+                o1 = 1 - bxo;
               } else {
-                hl[d] = wrapc[((size_t)ip * mq + ml) * 2 + 0];
-                hr[d] = wrapc[((size_t)ip * mq + ml) * 2 + 1];
+                src = wrapc + (ip * mq + ml) * 2;
+                o0 = 0;
+                o1 = 1;
               }
             } else {
-              const Real* hb = hand + ((size_t)(((T - 1) & 1) * W + (warp - 1)) * mq + ml) * 2;
-              hl[d] = hb[0];
-              hr[d] = hb[1];
+              src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mq + ml) * 2;
+              o0 = 0;
+              o1 = 1;
             }
+            hl[d] = src[o0];
+            hr[d] = src[o1];
           }
         }
       }
 
+      const Real kA4 = scb_kA4(dx, dy, kp);
 #pragma unroll
-      for (int d = 0; d < DMAX; ++d) {
+      for (int d = 0; d < D; ++d) {
         const int ml = d * S + s;
-        if (d < t.D && ml < mq) {
-          const int nsl = (mq - d * S) < S ? (mq - d * S) : S;
-          const int nl = R * nsl;
+        if (d < D - 1 || s < s_last) {
+          const int nl = (d < D - 1) ? 32 : nl_last;
           const Real* sb = sm + d * 128;
           Real io[4];
           if (NV == 2) {
@@ -234,9 +289,8 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
 #pragma unroll
             for (int c = 0; c < 4; ++c) src[c] = tfma(io[c], rcdt, qs);
           }
-          const Real ax = dtab[kAx * mq + ml], ay = dtab[kAy * mq + ml];
-          const ScbGeom<Real> G = scb_geom(ax, ay, dx, dy);
-          const Real gam = scb_gamma(ax, ay, dx, dy, kp);
+          const ScbGeom<Real> G = scb_geom(dtab[kAx * mq + ml], dtab[kAy * mq + ml], dx, dy);
+          const Real gam = scb_gamma(G, kA4);
           Real x[4];
           scb_solve(G, gam, A4, src, vb[d], vt[d], hl[d], hr[d], x);
 
@@ -245,10 +299,8 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
             *reinterpret_cast<double2*>(gb + lane * 2) = make_double2((double)x[0], (double)x[1]);
             *reinterpret_cast<double2*>(gb + nl * 2 + lane * 2) = make_double2((double)x[2], (double)x[3]);
           } else {
-            *reinterpret_cast<float4*>(gb + lane * 4) =
-                make_float4((float)x[0], (float)x[1], (float)x[2], (float)x[3]);
+            *reinterpret_cast<float4*>(gb + lane * 4) = make_float4((float)x[0], (float)x[1], (float)x[2], (float)x[3]);
           }
-
           // outflow: right face feeds the next column of this lane, top face the next row
           vb[d] = x[1];
           vt[d] = x[2];
@@ -273,31 +325,31 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
           acc[kHy] = tfma(wy, Ih, acc[kHy]);
           acc[kHx] = tfma(wx, Ih, acc[kHx]);
           acc[kHe] = tfma(ww, Ih, acc[kHe]);
-
-          if (ip == nx - 1) {
-            bVout[(size_t)ml * 2 * ny + 2 * j + (fy ? 1 : 0)] = x[1];
-            bVout[(size_t)ml * 2 * ny + 2 * j + (fy ? 0 : 1)] = x[2];
-          }
-          if (jp == ny - 1) {
-            bHout[(size_t)ml * 2 * nx + 2 * i + (fx ? 1 : 0)] = x[3];
-            bHout[(size_t)ml * 2 * nx + 2 * i + (fx ? 0 : 1)] = x[2];
-          }
         }
       }
 
-      // handoff of the top outflow of the warp's last row
-      if (r == R - 1) {
+      // outflow boundary faces and the handoff of the warp's last row
+      const bool right_edge = (ip == nx - 1), top_edge = (jp == ny - 1), last_row = (r == R - 1);
+      if (right_edge || top_edge || last_row) {
 #pragma unroll
-        for (int d = 0; d < DMAX; ++d) {
+        for (int d = 0; d < D; ++d) {
           const int ml = d * S + s;
-          if (d < t.D && ml < mq) {
-            if (warp < W - 1) {
-              Real* hb = hand + ((size_t)((T & 1) * W + warp) * mq + ml) * 2;
-              hb[0] = topL[d];
-              hb[1] = topR[d];
-            } else if (t.nr > 1) {
-              wrapc[((size_t)ip * mq + ml) * 2 + 0] = topL[d];
-              wrapc[((size_t)ip * mq + ml) * 2 + 1] = topR[d];
+          if (d < D - 1 || s < s_last) {
+            if (right_edge) {
+              bVout[ml * 2 * ny + 2 * j + byo] = vb[d];
+              bVout[ml * 2 * ny + 2 * j + 1 - byo] = vt[d];
+            }
+            if (top_edge) {
+              bHout[ml * 2 * nx + 2 * i + bxo] = topL[d];
+              bHout[ml * 2 * nx + 2 * i + 1 - bxo] = topR[d];
+            }
+            if (last_row) {
+              Real* dst = (warp < W - 1) ? hand + (((T & 1) * W + warp) * mq + ml) * 2
+                                         : wrapc + (ip * mq + ml) * 2;
+              if (warp < W - 1 || t.nr > 1) {
+                dst[0] = topL[d];
+                dst[1] = topR[d];
+              }
             }
           }
         }
@@ -306,27 +358,37 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
 
     // bottom inflow of rows r >= 1 for the next step (rows r == 0 reload it)
 #pragma unroll
-    for (int d = 0; d < DMAX; ++d) {
+    for (int d = 0; d < D; ++d) {
       hl[d] = __shfl_up_sync(0xffffffffu, topL[d], 1);
       hr[d] = __shfl_up_sync(0xffffffffu, topR[d], 1);
     }
 
-    // moments: reduce over the S slices of each row (fixed xor order), write the quadrant partial
-    double accd[14];
+    // moments: reduce-scatter over the S slices of each row, then each lane writes its slots
+    double mv[16];
 #pragma unroll
-    for (int v = 0; v < 13; ++v) accd[v] = (double)acc[v];
-    accd[13] = 0.0;
+    for (int v = 0; v < 13; ++v) mv[v] = (double)acc[v];
+    mv[13] = mv[14] = mv[15] = 0.0;
+    bool owner;
+    const int base = slice_reduce_scatter<S, R>(mv, s, &owner);
+    if (active && owner) {
+      double* pc = partg + (size_t)(j * nx + i) * kNPart;
 #pragma unroll
-    for (int o = R; o < 32; o <<= 1) {
-#pragma unroll
-      for (int v = 0; v < 13; ++v) accd[v] += __shfl_xor_sync(0xffffffffu, accd[v], o);
+      for (int k = 0; k < NSLOT; k += 2) {
+        if (NSLOT == 1) {
+          if (base < kNPart) pc[base] = mv[0];
+        } else if (base + k < kNPart) {
+          *reinterpret_cast<double2*>(pc + base + k) = make_double2(mv[k], mv[k + 1]);
+        }
+      }
     }
-    if (active) {
-      double* pc = partg + ((size_t)j * nx + i) * kNPart;
-#pragma unroll
-      for (int p = 0; p < 7; ++p)
-        if (p % S == s) *reinterpret_cast<double2*>(pc + 2 * p) = make_double2(accd[2 * p], accd[2 * p + 1]);
+
+    // advance the lane and prefetch the material of its next cell
+    ++ip;
+    if (ip == t.P) {
+      ip = 0;
+      ++n;
     }
+    load_material(ip, n);
 
     const int any_timeout = __syncthreads_or(timed_out ? 1 : 0);
     if (any_timeout) {

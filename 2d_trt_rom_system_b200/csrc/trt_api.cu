@@ -79,11 +79,12 @@ bool valid_shape(int nx, int ny, int nm, int ng) {
   return nx >= 1 && ny >= 1 && ng >= 1 && nm >= 4 && nm % 4 == 0 && nx < (1 << 20) && ny < (1 << 20);
 }
 
-// Compiled (slices, max directions per lane) pairs of the sweep kernel.
+// Compiled (slices, directions per lane) pairs of the sweep kernel; D is exact (ceil(mq / S)).
 struct KernelCfg {
-  int S, DMAX;
+  int S, D;
 };
-const KernelCfg kCfgs[] = {{1, 2}, {2, 5}, {4, 3}, {4, 6}, {4, 9}, {8, 3}, {8, 5}, {16, 3}, {16, 4}, {32, 2}};
+const KernelCfg kCfgs[] = {{1, 2}, {2, 5}, {4, 3}, {4, 6}, {4, 9}, {8, 2}, {8, 3}, {8, 4}, {8, 5},
+                           {16, 1}, {16, 2}, {16, 3}, {32, 1}, {32, 2}};
 
 bool pick_cfg(int mq, int prec, int S_req, KernelCfg* out) {
   bool found = false;
@@ -91,12 +92,11 @@ bool pick_cfg(int mq, int prec, int S_req, KernelCfg* out) {
   long best_key = 0;
   for (const KernelCfg& k : kCfgs) {
     if (S_req && k.S != S_req) continue;
-    const int D = (mq + k.S - 1) / k.S;
-    if (D > k.DMAX) continue;
-    const int waste = k.S * D - mq;
-    // FP64 keeps D <= 5 (registers); then least idle slots; then the smallest DMAX; then larger S
-    const int dpen = (prec == TRT_PREC_FP64 && D > 5) ? 1 : 0;
-    const long key = (long)dpen * 1000000 + waste * 1000 + k.DMAX * 10 + (32 - k.S) / 4;
+    if ((mq + k.S - 1) / k.S != k.D) continue;
+    const int waste = k.S * k.D - mq;
+    // FP64 keeps D <= 5 (registers); then least idle slots; then fewer slices (fewer shuffles)
+    const int dpen = (prec == TRT_PREC_FP64 && k.D > 5) ? 1 : 0;
+    const long key = (long)dpen * 1000000 + waste * 1000 + k.S;
     if (!found || key < best_key) {
       found = true;
       best = k;
@@ -111,7 +111,7 @@ template <class Real>
 cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int grid, int block, size_t smem, cudaStream_t st,
                          const trt::SweepArgs<Real>& a) {
 #define TRT_SWEEP_CASE(S_, D_)                                                                   \
-  if (kc.S == S_ && kc.DMAX == D_) {                                                             \
+  if (kc.S == S_ && kc.D == D_) {                                                                \
     if (src_full) {                                                                              \
       auto k = trt::scb_sweep_kernel<Real, S_, D_, true>;                                        \
       cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);           \
@@ -128,10 +128,14 @@ cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int grid, int block
   TRT_SWEEP_CASE(4, 3)
   TRT_SWEEP_CASE(4, 6)
   TRT_SWEEP_CASE(4, 9)
+  TRT_SWEEP_CASE(8, 2)
   TRT_SWEEP_CASE(8, 3)
+  TRT_SWEEP_CASE(8, 4)
   TRT_SWEEP_CASE(8, 5)
+  TRT_SWEEP_CASE(16, 1)
+  TRT_SWEEP_CASE(16, 2)
   TRT_SWEEP_CASE(16, 3)
-  TRT_SWEEP_CASE(16, 4)
+  TRT_SWEEP_CASE(32, 1)
   TRT_SWEEP_CASE(32, 2)
 #undef TRT_SWEEP_CASE
   return cudaErrorInvalidValue;
@@ -145,7 +149,7 @@ struct trt_ctx {
   int nx = 0, ny = 0, nm = 0, ng = 0, mq = 0, prec = 0;
   size_t budget = 0, used = 0;
   cudaStream_t stream = nullptr;
-  int Wreq = 0, Sreq = 0, stages = 3;
+  int Wreq = 0, Sreq = 0, stages = 2;
   KernelCfg kc{8, 5};
   trt::Tiling t{};
   long long chunk = 0, blk = 0;
@@ -245,8 +249,10 @@ size_t layout_state_bytes(int nx, int ny, int mq, int ng, int W, int S, size_t e
   return (size_t)4 * ng * trt::block_elems(mq, t) * esz;
 }
 
+// Default warps per CTA: 32 rows per round (8 warps of 4 rows for 8 slices), at most 8 warps so
+// that two CTAs fit an SM.
 int default_W(int R) {
-  int W = 16 / R;
+  int W = 32 / R;
   if (W < 1) W = 1;
   if (W > 8) W = 8;
   return W;
@@ -878,7 +884,7 @@ int trt_set_tiling(trt_ctx* c, int warps_per_cta, int slices, int stages) {
   if (slices > 32) return TRT_ERR_ARG;
   c->Wreq = warps_per_cta;
   c->Sreq = slices;
-  c->stages = stages ? stages : 3;
+  c->stages = stages ? stages : 2;
   return setup_layout(c);
 }
 

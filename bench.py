@@ -46,6 +46,11 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--tiling", default="", help="warps,slices,stages override for both precisions")
+    p.add_argument("--profile", default="", choices=["", "fp64", "fp32"],
+                   help="only run --warmup + --steps sweeps (no moments) of one precision, for ncu")
+    p.add_argument("--n", type=int, default=0, help="grid size override (profiling small cases)")
+    p.add_argument("--groups", type=int, default=0, help="group count override (profiling small cases)")
+    p.add_argument("--tiling-sweep", action="store_true", help="time the sweep kernel over a set of tilings")
     return p.parse_args()
 
 
@@ -119,10 +124,56 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def build_problem(name):
+def build_problem(name, n=0, groups=0):
     pkg = importlib.import_module("2d_trt_rom_system_b200")
-    prob = pkg.problems.config1() if name == "C1" else pkg.problems.config0()
+    if name == "C1":
+        prob = pkg.problems.config1(n=n or 256, groups=groups or 50)
+    else:
+        prob = pkg.problems.config0()
     return pkg, prob
+
+
+def run_profile(args):
+    """Plain sweeps of one instance (the command ncu captures)."""
+    import torch
+    torch.cuda.set_device(0)
+    pkg, prob = build_problem(args.config, args.n, args.groups)
+    tiling = tuple(int(x) for x in args.tiling.split(",")) if args.tiling else None
+    s, _, _ = setup_instance(pkg, prob, "mixed" if args.profile == "fp32" else "fp64", tiling)
+    try:
+        ms, n = time_resident(pkg, torch, s, args.steps, args.warmup, 0)
+        print(json.dumps({"profile": args.profile, "workload": f"{prob.nx}x{prob.ny} G={prob.ng} {prob.quad}",
+                          "ms_per_sweep": ms, "tiling": s.tiling(), "launches": n}))
+    finally:
+        s.close()
+    return 0
+
+
+def run_tiling_sweep(args):
+    import torch
+    torch.cuda.set_device(0)
+    pkg, prob = build_problem(args.config, args.n, args.groups)
+    upd = prob.updates_per_sweep()
+    peak, _ = peaks()
+    for prec in ("fp64", "fp32"):
+        s, _, _ = setup_instance(pkg, prob, "mixed" if prec == "fp32" else "fp64", None)
+        try:
+            for W in (2, 4, 8, 12, 16):
+                for S in (0, 4, 8, 16):
+                    for st in (2, 3):
+                        try:
+                            s.set_tiling(W, S, st)
+                        except pkg.TrtError:
+                            continue
+                        s.init_state(prob.T0 * 1e3, [t * 1e3 for t in prob.bcT], pkg.problems.COMP_UNIT, prob.nu_eV)
+                        ms, _ = time_resident(pkg, torch, s, 5, 1, 0)
+                        B = bytes_per_update(prob.nm, prec)
+                        print(json.dumps({"prec": prec, "tiling": s.tiling(), "kernel_ms": ms,
+                                          "gupd_s": upd / ms / 1e6, "frac": upd * B / (ms * 1e-3) / 1e9 / peak}),
+                              flush=True)
+        finally:
+            s.close()
+    return 0
 
 
 def setup_instance(pkg, prob, precision, tiling):
@@ -275,9 +326,13 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile:
+        return run_profile(args)
+    if args.tiling_sweep:
+        return run_tiling_sweep(args)
     import torch
     ws, rank, local = dist_setup(args)
-    pkg, prob = build_problem(args.config)
+    pkg, prob = build_problem(args.config, args.n, args.groups)
     tiling = tuple(int(x) for x in args.tiling.split(",")) if args.tiling else None
     upd = prob.updates_per_sweep()
     peak, peak_kind = peaks()

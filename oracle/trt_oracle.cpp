@@ -283,8 +283,8 @@ int oracle_transport_scb(int nx, int ny, int nm, int ng, double* I_avg, double* 
               const int vface = fx ? i + 1 : i;   // inflow vertical face
               const int hface = fy ? j + 1 : j;   // inflow horizontal face
               const double ax = std::fabs(Ox), ay = std::fabs(Oy);
-              trt::ScbGeom<double> G = trt::scb_geom(ax, ay, Delx[i], Dely[j]);
-              double gam = trt::scb_gamma(ax, ay, Delx[i], Dely[j], kap);
+              trt::ScbGeom<double> G = trt::scb_geom(ax * 0.25, ay * 0.25, Delx[i], Dely[j]);
+              double gam = trt::scb_gamma(G, trt::scb_kA4(Delx[i], Dely[j], kap));
               double s[4] = {S(sl, sb), S(sr, sb), S(sr, st), S(sl, st)};
               double x[4];
               trt::scb_solve(G, gam, Aij * 0.25, s, Ic_edgV[icv(vface, sb, m, g)],

@@ -25,6 +25,19 @@ BND_KEYS = ("Cg_L", "Cg_B", "Cg_R", "Cg_T", "Eg_in_L", "Eg_in_B", "Eg_in_R", "Eg
             "Fg_in_R", "Fg_in_T", "E_in_L", "E_in_B", "E_in_R", "E_in_T", "F_in_L", "F_in_B", "F_in_R", "F_in_T")
 
 
+def moment_err(m, ref, k):
+    """max |a - b| over the scale of the matching energy sum: moments with cancelling terms (H_xy, F)
+    are compared against sum w I of the same group and location, not against their own size."""
+    loc = "avg" if "avg" in k else ("edgV" if "edgV" in k else "edgH")
+    E = ref[{"avg": "Eg_avg", "edgV": "Eg_edgV", "edgH": "Eg_edgH"}[loc]] if ref[k].ndim == 3 else \
+        ref[{"avg": "E_avg", "edgV": "E_edgV", "edgH": "E_edgH"}[loc]]
+    diff = np.abs(np.asarray(m[k]) - ref[k])
+    if ref[k].ndim == 3:
+        scale = C * np.max(np.abs(E), axis=(0, 1))
+        return float(np.max(np.max(diff, axis=(0, 1)) / scale))
+    return float(np.max(diff) / (C * np.max(np.abs(E))))
+
+
 def dropin_sweep(d, res_calc=False):
     nx, ny, nm, ng = len(d["Delx"]), len(d["Dely"]), len(d["Omega_x"]), d["KapE_in"].shape[2]
     out = dict(I_avg=np.zeros((nx, ny, nm, ng), order="F"), I_edgV=d["I_edgV"].copy(order="F"),
@@ -93,9 +106,7 @@ def test_resident_sweep_and_fused_moments(oracle, name, make):
         m = s.moments()
     assert np.array_equal(I, ref["I_crn"])
     for k in MOM_KEYS:
-        gaxis = -1 if m[k].ndim == 3 else None
-        err = rel_err_per_group(m[k], ref[k]) if gaxis else rel_err(m[k], ref[k])
-        assert err < 1e-13, k
+        assert moment_err(m, ref, k) < 1e-13, k
     for k in FG_KEYS:
         assert np.max(np.abs(m[k] - ref[k])) < 1e-13, k
     for k in BND_KEYS:
@@ -104,7 +115,8 @@ def test_resident_sweep_and_fused_moments(oracle, name, make):
     # oracle's collapse with Omega_y passed as the x cosine yields it
     rc = oracle.collapse_intensities(ref["I_avg"], ref["I_edgV"], ref["I_edgH"], d["Omega_y"], d["Omega_y"], d["w"],
                                      CU)
-    assert rel_err_per_group(m["Fyg_edgH_true"], rc["Fyg_edgH"]) < 1e-13
+    m2 = dict(m, Fyg_edgH=m["Fyg_edgH_true"])
+    assert moment_err(m2, dict(ref, Fyg_edgH=rc["Fyg_edgH"]), "Fyg_edgH") < 1e-13
 
 
 @pytest.mark.parametrize("tiling", [dict(warps=1), dict(warps=2, stages=1), dict(warps=8, stages=2),
@@ -210,10 +222,14 @@ def test_fp32_mixed_sweep_against_fp64_oracle(oracle):
         s.sweep(moments=True)
         I = s.get_state()
         m = s.moments(["Eg_avg", "E_avg", "fg_avg_xx", "fg_edgV_xx", "Cg_L", "Fx_edgV"])
-    assert rel_err_per_group(I, ref["I_crn"]) < 1e-5
+    # groups carrying energy (the others sit at FP32 underflow / the eps floor) to 1e-5 per group
+    gmax = np.max(np.abs(ref["I_crn"]), axis=(0, 1, 2))
+    live = gmax > 1e-20 * gmax.max()
+    assert rel_err_per_group(I[..., live], ref["I_crn"][..., live]) < 1e-5
     assert rel_err(m["E_avg"], ref["E_avg"]) < 1e-5
-    assert np.max(np.abs(m["fg_avg_xx"] - ref["fg_avg_xx"])) < 1e-5
-    assert np.all(np.isfinite(m["fg_edgV_xx"]))
+    assert rel_err(m["Fx_edgV"], ref["Fx_edgV"], scale=C * np.max(ref["E_edgV"])) < 1e-5
+    assert np.max(np.abs(m["fg_avg_xx"] - ref["fg_avg_xx"])[..., live]) < 1e-5
+    assert np.all(np.isfinite(m["fg_edgV_xx"])) and np.all(np.isfinite(m["Cg_L"]))
 
 
 def test_reference_signature_moment_routines_bit_identical(oracle):
@@ -294,7 +310,10 @@ def test_superposition_and_scaling_at_full_c1_size():
     assert np.all(np.isfinite(both["E_avg"])) and np.all(both["E_avg"] > 0)
     assert rel_err(both["E_avg"], only_src["E_avg"] + only_bc["E_avg"]) < 1e-12
     assert rel_err(both["Fx_edgV"], only_src["Fx_edgV"] + only_bc["Fx_edgV"]) < 1e-12
-    assert rel_err_per_group(twice["Eg_avg"], 2.0 * only_src["Eg_avg"]) < 1e-12
+    # E_g = (sum w I + eps sum w) / c: remove the eps floor before comparing the doubled source
+    floor = 1e-25 / CU * np.sum(w) / C
+    big = np.max(only_src["Eg_avg"], axis=(0, 1)) > 1e6 * floor
+    assert rel_err_per_group((twice["Eg_avg"] - floor)[..., big], 2.0 * (only_src["Eg_avg"] - floor)[..., big]) < 1e-12
 
 
 def test_equilibrium_at_full_c1_size():
