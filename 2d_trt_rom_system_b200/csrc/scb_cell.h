@@ -99,4 +99,42 @@ TRT_HD void scb_solve(const ScbGeom<R>& G, R gamma, R A4, const R s[4], R vb, R 
   x[3] = tfma(b, y1, tfma(-a, y3, g * y4)) * inv;
 }
 
+// Same solve for FP32 state ("mixed" precision).  det ~ gamma^4 overflows FP32 in optically thick
+// cells (kappa*dx ~ 1e11 gives gamma ~ 1e10), so the system is scaled by 1/gamma first:
+// B/gamma = I + a'P + b'R with a' = a/gamma, b' = b/gamma <= 1, whose inverse factors have
+// determinant det' in [1, 5]; x = (I - a'P - b'R)(c'I + d'S) Q / (gamma det').
+TRT_HD float frcp(float v) {
+#if defined(__CUDA_ARCH__)
+  return __fdividef(1.0f, v);
+#else
+  return 1.0f / v;
+#endif
+}
+
+TRT_HD void scb_solve(const ScbGeom<float>& G, float gamma, float A4, const float s[4], float vb, float vt, float hl,
+                      float hr, float x[4]) {
+  float Q1 = tfma(G.hy, hl, tfma(G.hx, vb, A4 * s[0]));
+  float Q2 = tfma(G.hy, hr, A4 * s[1]);
+  float Q3 = A4 * s[2];
+  float Q4 = tfma(G.hx, vt, A4 * s[3]);
+
+  const float r = frcp(gamma);
+  const float a = G.a * r, b = G.b * r;
+  const float c = tfma(a, a, tfma(b, b, 1.0f));
+  const float d = (a + a) * b;
+  const float amb = a - b, apb = a + b;
+  const float det = tfma(amb, amb, 1.0f) * tfma(apb, apb, 1.0f);
+  const float inv = r * frcp(det);
+
+  const float y1 = tfma(d, Q3, c * Q1);
+  const float y2 = tfma(-d, Q4, c * Q2);
+  const float y3 = tfma(d, Q1, c * Q3);
+  const float y4 = tfma(-d, Q2, c * Q4);
+
+  x[0] = tfma(-b, y4, tfma(-a, y2, y1)) * inv;
+  x[1] = tfma(-b, y3, tfma(a, y1, y2)) * inv;
+  x[2] = tfma(b, y2, tfma(a, y4, y3)) * inv;
+  x[3] = tfma(b, y1, tfma(-a, y3, y4)) * inv;
+}
+
 }  // namespace trt

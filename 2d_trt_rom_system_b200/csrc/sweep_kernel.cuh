@@ -114,8 +114,20 @@ __device__ __forceinline__ int slice_reduce_scatter(double (&v)[16], int s, bool
   return base;
 }
 
+// Kahan-compensated add: sum + p with the running compensation term.
+template <class Real>
+__device__ __forceinline__ void kahan_add(Real& sum, Real& comp, Real p) {
+  const Real y = p - comp;
+  const Real t = sum + y;
+  comp = (t - sum) - y;
+  sum = t;
+}
+
+// The FP32 ("mixed") sweep accumulates its per-lane moment sums with Kahan compensation; the FP64
+// sweep accumulates with fused multiply-adds.  Sums over slices, quadrants and groups are FP64.
 template <class Real, int S, int D, bool SRC_FULL>
 __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a) {
+  constexpr bool KAHAN = sizeof(Real) == 4;
   constexpr int R = 32 / S;
   constexpr int NV = 16 / (int)sizeof(Real);
   constexpr int NSLOT = S >= 16 ? 1 : 16 / S;   // moment slots a lane holds after the reduce-scatter
@@ -217,9 +229,9 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
     const int j = fy ? ny - 1 - jp : jp;
 
     Real topL[D], topR[D];
-    Real acc[13];
+    Real acc[13], cmp[13];
 #pragma unroll
-    for (int v = 0; v < 13; ++v) acc[v] = Real(0);
+    for (int v = 0; v < 13; ++v) acc[v] = cmp[v] = Real(0);
 #pragma unroll
     for (int d = 0; d < D; ++d) topL[d] = topR[d] = Real(0);
 
@@ -312,19 +324,36 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
           const Real Ih = (x[3] + x[2]) * Real(0.5);
           const Real wxx = dtab[kWxx * mq + ml], wyy = dtab[kWyy * mq + ml], wxy = dtab[kWxy * mq + ml];
           const Real ww = dtab[kW * mq + ml], wx = dtab[kWx * mq + ml], wy = dtab[kWy * mq + ml];
-          acc[kCxx] = tfma(wxx, Iavg, acc[kCxx]);
-          acc[kCyy] = tfma(wyy, Iavg, acc[kCyy]);
-          acc[kCxy] = tfma(wxy, Iavg, acc[kCxy]);
-          acc[kCe] = tfma(ww, Iavg, acc[kCe]);
-          acc[kVxx] = tfma(wxx, Iv, acc[kVxx]);
-          acc[kVxy] = tfma(wxy, Iv, acc[kVxy]);
-          acc[kVx] = tfma(wx, Iv, acc[kVx]);
-          acc[kVe] = tfma(ww, Iv, acc[kVe]);
-          acc[kHyy] = tfma(wyy, Ih, acc[kHyy]);
-          acc[kHxy] = tfma(wxy, Ih, acc[kHxy]);
-          acc[kHy] = tfma(wy, Ih, acc[kHy]);
-          acc[kHx] = tfma(wx, Ih, acc[kHx]);
-          acc[kHe] = tfma(ww, Ih, acc[kHe]);
+          if (KAHAN) {
+            // FP32 sums with Kahan compensation (the compensation terms live in cmp[])
+            kahan_add(acc[kCxx], cmp[kCxx], wxx * Iavg);
+            kahan_add(acc[kCyy], cmp[kCyy], wyy * Iavg);
+            kahan_add(acc[kCxy], cmp[kCxy], wxy * Iavg);
+            kahan_add(acc[kCe], cmp[kCe], ww * Iavg);
+            kahan_add(acc[kVxx], cmp[kVxx], wxx * Iv);
+            kahan_add(acc[kVxy], cmp[kVxy], wxy * Iv);
+            kahan_add(acc[kVx], cmp[kVx], wx * Iv);
+            kahan_add(acc[kVe], cmp[kVe], ww * Iv);
+            kahan_add(acc[kHyy], cmp[kHyy], wyy * Ih);
+            kahan_add(acc[kHxy], cmp[kHxy], wxy * Ih);
+            kahan_add(acc[kHy], cmp[kHy], wy * Ih);
+            kahan_add(acc[kHx], cmp[kHx], wx * Ih);
+            kahan_add(acc[kHe], cmp[kHe], ww * Ih);
+          } else {
+            acc[kCxx] = tfma(wxx, Iavg, acc[kCxx]);
+            acc[kCyy] = tfma(wyy, Iavg, acc[kCyy]);
+            acc[kCxy] = tfma(wxy, Iavg, acc[kCxy]);
+            acc[kCe] = tfma(ww, Iavg, acc[kCe]);
+            acc[kVxx] = tfma(wxx, Iv, acc[kVxx]);
+            acc[kVxy] = tfma(wxy, Iv, acc[kVxy]);
+            acc[kVx] = tfma(wx, Iv, acc[kVx]);
+            acc[kVe] = tfma(ww, Iv, acc[kVe]);
+            acc[kHyy] = tfma(wyy, Ih, acc[kHyy]);
+            acc[kHxy] = tfma(wxy, Ih, acc[kHxy]);
+            acc[kHy] = tfma(wy, Ih, acc[kHy]);
+            acc[kHx] = tfma(wx, Ih, acc[kHx]);
+            acc[kHe] = tfma(ww, Ih, acc[kHe]);
+          }
         }
       }
 
@@ -366,7 +395,7 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
     // moments: reduce-scatter over the S slices of each row, then each lane writes its slots
     double mv[16];
 #pragma unroll
-    for (int v = 0; v < 13; ++v) mv[v] = (double)acc[v];
+    for (int v = 0; v < 13; ++v) mv[v] = KAHAN ? (double)acc[v] - (double)cmp[v] : (double)acc[v];
     mv[13] = mv[14] = mv[15] = 0.0;
     bool owner;
     const int base = slice_reduce_scatter<S, R>(mv, s, &owner);

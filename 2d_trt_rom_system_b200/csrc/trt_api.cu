@@ -249,12 +249,11 @@ size_t layout_state_bytes(int nx, int ny, int mq, int ng, int W, int S, size_t e
   return (size_t)4 * ng * trt::block_elems(mq, t) * esz;
 }
 
-// Default warps per CTA: 32 rows per round (8 warps of 4 rows for 8 slices), at most 8 warps so
-// that two CTAs fit an SM.
-int default_W(int R) {
-  int W = 32 / R;
-  if (W < 1) W = 1;
-  if (W > 8) W = 8;
+// Default warps per CTA: 8 (two CTAs of 256 threads fit an SM at <= 128 registers); measured best
+// for C1 in both precisions.  Fewer when a round would exceed the grid height by far.
+int default_W(int R, int ny) {
+  int W = 8;
+  while (W > 1 && (W / 2) * R >= ny) W /= 2;
   return W;
 }
 
@@ -262,7 +261,7 @@ int default_W(int R) {
 int setup_layout(trt_ctx* c) {
   if (!pick_cfg(c->mq, c->prec, c->Sreq, &c->kc)) return c->Sreq ? TRT_ERR_ARG : TRT_ERR_UNSUPPORTED;
   const int R = 32 / c->kc.S;
-  const int W = c->Wreq ? c->Wreq : default_W(R);
+  const int W = c->Wreq ? c->Wreq : default_W(R, c->ny);
   c->t = trt::make_tiling(c->nx, c->ny, c->mq, W, c->kc.S);
   c->chunk = trt::chunk_elems(c->mq, c->t);
   c->blk = trt::block_elems(c->mq, c->t);
@@ -815,7 +814,7 @@ size_t trt_required_bytes(int n_x, int n_y, int n_m, int n_g, int precision) {
   KernelCfg kc;
   if (!pick_cfg(mq, precision, 0, &kc)) return 0;
   const size_t esz = precision == TRT_PREC_FP64 ? 8 : 4;
-  const int W = default_W(32 / kc.S);
+  const int W = default_W(32 / kc.S, n_y);
   size_t b = 2 * layout_state_bytes(n_x, n_y, mq, n_g, W, kc.S, esz);
   const size_t ncell = (size_t)n_x * n_y * n_g;
   b += ncell * (16 + 2 * esz);
