@@ -20,6 +20,7 @@ TRT_ERR_TIMEOUT = -5
 TRT_ERR_STATE = -6
 TRT_ERR_NODEV = -7
 TRT_ERR_UNSUPPORTED = -8
+TRT_ERR_SCRATCH = -9
 
 TRT_PREC_FP64 = 0
 TRT_PREC_FP32 = 1
@@ -99,6 +100,7 @@ SIGNATURES = {
     "trt_device_output": (_P, [_P, ctypes.c_char_p]),
     "trt_strerror": (ctypes.c_char_p, [_i]),
     "trt_kernel_launches": (ctypes.c_ulonglong, []),
+    "trt_transport_residual_noalloc": (_i, [_i, _i, _i, _i] + [_P] * 11 + [_d, _d, _P, _P, _P, _P]),
 }
 
 _lib = None

@@ -798,6 +798,7 @@ const char* trt_strerror(int code) {
     case TRT_ERR_STATE: return "call order: a required input has not been set";
     case TRT_ERR_NODEV: return "no CUDA device available";
     case TRT_ERR_UNSUPPORTED: return "shape outside the compiled kernel set";
+    case TRT_ERR_SCRATCH: return "problem exceeds the fixed scratch of the no-allocation entry point (n_m*n_g > 65536)";
     default: return "unknown error";
   }
 }
@@ -1273,3 +1274,156 @@ int trt_rt_bc_update(int n_x, int n_y, int n_m, int n_g, const int* BC_Type, dou
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// trt_transport_residual_noalloc: the corner-balance residual norms of TRANSPORT_SCB computed
+// without allocating device memory.
+//
+// Some callers cannot call cudaMalloc: a host code that hands the library a fixed, pre-sized device
+// arena and owns all allocation itself, or a solver loop that must not pay cudaMalloc/cudaFree's
+// implicit device synchronisation in the middle of an iteration.  For them the residual kernel's
+// per-(direction, group) scratch lives in the file-scope array below instead of in memory the
+// resident handle allocates; the caller passes every input and output as device pointers.
+//
+// Limit: n_m * n_g <= kNoAllocMaxDirGroups (65536 direction-group pairs, 3 MiB of scratch that every
+// GPU which loads the library holds until the process exits).  Larger problems are rejected with
+// TRT_ERR_SCRATCH before anything is launched.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxDirGroups = 1 << 16;
+constexpr size_t kNoAllocNormBytes = (size_t)kNoAllocMaxDirGroups * 5 * sizeof(double);
+constexpr size_t kNoAllocScratchBytes = kNoAllocNormBytes + (size_t)kNoAllocMaxDirGroups * 2 * sizeof(int);
+// In host code this name is only a host-side stand-in: its device address comes from
+// cudaGetSymbolAddress (noalloc_scratch below) and is what the kernels receive.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch on the current device, looked up once per device (with that device
+// current) on the first call made on it.
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return TRT_ERR_NODEV;
+  }
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return TRT_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      cudaGetLastError();
+      return TRT_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return TRT_OK;
+}
+
+// Residual norms of one (m, g) over the reference layouts I_crn(2nx,2ny,nm,ng),
+// Ic_edgV(nx+1,2ny,nm,ng), Ic_edgH(2nx,ny+1,nm,ng); the expressions and loop order of
+// TRANSPORT_SOLVES.f08:256-309, the source formed as the sweep forms it (fma(I_crn_old, 1/(c dt),
+// Src_in)).
+__global__ void residual_fortran_kernel(int nx, int ny, int nm, int ng, const double* __restrict__ I_crn,
+                                        const double* __restrict__ Ic_edgV, const double* __restrict__ Ic_edgH,
+                                        const double* __restrict__ omx, const double* __restrict__ omy,
+                                        const double* __restrict__ Delx, const double* __restrict__ Dely,
+                                        const double* __restrict__ A, const double* __restrict__ KapE_in,
+                                        const double* __restrict__ Src_in, const double* __restrict__ I_crn_old,
+                                        double rcdt, double* per_m, int* per_m_loc) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nm * ng) return;
+  const int m = k % nm, g = k / nm;
+  const double Ox = omx[m], Oy = omy[m];
+  const long long n2x = 2LL * nx, n2y = 2LL * ny;
+  const long long cbase = n2x * n2y * (m + (long long)nm * g);
+  const long long vbase = (long long)(nx + 1) * n2y * (m + (long long)nm * g);
+  const long long hbase = n2x * (ny + 1) * (m + (long long)nm * g);
+  double vmax = 0.0, sums[4] = {0.0, 0.0, 0.0, 0.0};
+  int li = 0, lj = 0;
+  for (int j = 0; j < ny; ++j) {
+    for (int i = 0; i < nx; ++i) {
+      const double Aij = A[i + (long long)nx * j];
+      const double kp = KapE_in[i + (long long)nx * (j + (long long)ny * g)] + rcdt;
+      const double dxx = Delx[i], dyy = Dely[j];
+      double I[2][2], Sr[2][2];
+      for (int cx = 0; cx < 2; ++cx)
+        for (int cy = 0; cy < 2; ++cy) {
+          const long long ci = cbase + (2 * i + cx) + n2x * (2 * j + cy);
+          I[cx][cy] = I_crn[ci];
+          Sr[cx][cy] = fma(I_crn_old[ci], rcdt, Src_in[ci]);
+        }
+      auto V = [&](int f, int iy) { return Ic_edgV[vbase + f + (long long)(nx + 1) * iy]; };
+      auto H = [&](int ix, int f) { return Ic_edgH[hbase + ix + n2x * f]; };
+      double res[4];
+      res[0] = fabs((Ox * dyy + Oy * dxx + kp * Aij) * I[0][0] / 4.0 + Ox * dyy * I[1][0] / 4.0 +
+                    Oy * dxx * I[0][1] / 4.0 - Ox * dyy * V(i, 2 * j) / 2.0 - Oy * dxx * H(2 * i, j) / 2.0 -
+                    Aij * Sr[0][0] / 4.0);
+      res[1] = fabs((-Ox * dyy + Oy * dxx + kp * Aij) * I[1][0] / 4.0 - Ox * dyy * I[0][0] / 4.0 +
+                    Oy * dxx * I[1][1] / 4.0 + Ox * dyy * V(i + 1, 2 * j) / 2.0 - Oy * dxx * H(2 * i + 1, j) / 2.0 -
+                    Aij * Sr[1][0] / 4.0);
+      res[2] = fabs((-Ox * dyy - Oy * dxx + kp * Aij) * I[1][1] / 4.0 - Ox * dyy * I[0][1] / 4.0 -
+                    Oy * dxx * I[1][0] / 4.0 + Ox * dyy * V(i + 1, 2 * j + 1) / 2.0 +
+                    Oy * dxx * H(2 * i + 1, j + 1) / 2.0 - Aij * Sr[1][1] / 4.0);
+      res[3] = fabs((Ox * dyy - Oy * dxx + kp * Aij) * I[0][1] / 4.0 + Ox * dyy * I[1][1] / 4.0 -
+                    Oy * dxx * I[0][0] / 4.0 - Ox * dyy * V(i, 2 * j + 1) / 2.0 + Oy * dxx * H(2 * i, j + 1) / 2.0 -
+                    Aij * Sr[0][1] / 4.0);
+      for (int kk = 0; kk < 4; ++kk) {
+        if (res[kk] > vmax) {
+          vmax = res[kk];
+          li = i + 1;
+          lj = j + 1;
+        }
+        sums[0] = sums[0] + res[kk];
+        sums[1] = sums[1] + res[kk] * res[kk];
+        sums[2] = sums[2] + Aij * res[kk] / 4.0;
+        sums[3] = sums[3] + Aij * (res[kk] * res[kk]) / 4.0;
+      }
+    }
+  }
+  double* o = per_m + ((size_t)g * nm + m) * 5;
+  o[0] = vmax; o[1] = sums[0]; o[2] = sums[1]; o[3] = sums[2]; o[4] = sums[3];
+  int* l = per_m_loc + ((size_t)g * nm + m) * 2;
+  l[0] = li;
+  l[1] = lj;
+}
+
+}  // namespace
+
+extern "C" int trt_transport_residual_noalloc(int n_x, int n_y, int n_m, int n_g, const double* I_crn,
+                                              const double* Ic_edgV, const double* Ic_edgH, const double* Omega_x,
+                                              const double* Omega_y, const double* Delx, const double* Dely,
+                                              const double* A, const double* KapE_in, const double* Src_in,
+                                              const double* I_crn_old, double c, double Delt, double* RT_Residual,
+                                              int* RT_ResLoc_x, int* RT_ResLoc_y, void* stream) {
+  if (!valid_shape(n_x, n_y, n_m, n_g) || !I_crn || !Ic_edgV || !Ic_edgH || !Omega_x || !Omega_y || !Delx ||
+      !Dely || !A || !KapE_in || !Src_in || !I_crn_old || !RT_Residual || !RT_ResLoc_x || !RT_ResLoc_y ||
+      !(c > 0) || !(Delt > 0))
+    return TRT_ERR_ARG;
+  if ((long long)n_m * n_g > kNoAllocMaxDirGroups) return TRT_ERR_SCRATCH;
+  void* scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  double* per_m = static_cast<double*>(scratch);
+  int* per_m_loc = reinterpret_cast<int*>(static_cast<unsigned char*>(scratch) + kNoAllocNormBytes);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // every scratch slot the reduction reads is written by the first kernel of the same call, so no
+  // clearing is needed; RT_ResLoc_x/y keep the caller's values where no norm exceeds zero, as in
+  // the reference
+  const int mg = n_m * n_g;
+  residual_fortran_kernel<<<(mg + 63) / 64, 64, 0, st>>>(n_x, n_y, n_m, n_g, I_crn, Ic_edgV, Ic_edgH, Omega_x,
+                                                         Omega_y, Delx, Dely, A, KapE_in, Src_in, I_crn_old,
+                                                         1.0 / (c * Delt), per_m, per_m_loc);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  trt::residual_reduce_kernel<<<(4 * n_g + 63) / 64, 64, 0, st>>>(n_x, n_y, n_m, n_g, per_m, per_m_loc, RT_Residual,
+                                                                  RT_ResLoc_x, RT_ResLoc_y);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  return TRT_OK;
+}

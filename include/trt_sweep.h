@@ -39,6 +39,7 @@ extern "C" {
 #define TRT_ERR_STATE (-6)        /* call order: e.g. trt_sweep before trt_set_material */
 #define TRT_ERR_NODEV (-7)        /* no CUDA device */
 #define TRT_ERR_UNSUPPORTED (-8)  /* shape outside the compiled kernel set (N_m/4 > 64) */
+#define TRT_ERR_SCRATCH (-9)      /* problem larger than the fixed scratch of trt_transport_residual_noalloc */
 
 #define TRT_PREC_FP64 0   /* plain: FP64 state and arithmetic throughout */
 #define TRT_PREC_FP32 1   /* mixed: FP32 state and sweep, FP64 moment combination and QD factors */
@@ -202,6 +203,24 @@ const double* trt_device_output(trt_ctx* ctx, const char* name);
  * TRT_ERR_TIMEOUT and the handle stays usable. */
 int trt_set_wait_limit(trt_ctx* ctx, unsigned polls);
 int trt_set_wait_limit_zero(trt_ctx* ctx);
+
+/* No counterpart in the reference.  Residual norms RT_Residual(4,n_g,5), RT_ResLoc_x/y(4,n_g,5) of
+ * TRANSPORT_SCB's corner-balance equations (the Res_Calc block of TRANSPORT_SOLVES.f08:249-323) for
+ * callers that cannot allocate device memory: a host code that owns a fixed, pre-sized device arena,
+ * or a loop that must not pay the device synchronisation of cudaMalloc/cudaFree.  Every pointer is a
+ * DEVICE pointer to the caller's array in the reference's Fortran layout (the I_crn, Ic_edgV, Ic_edgH
+ * that TRANSPORT_SCB produced, and its inputs); the work is enqueued on `stream` (NULL = default
+ * stream) and the outputs are valid once that stream has synchronised.  Nothing is allocated: the
+ * per-(direction, group) scratch is a fixed device array of the library (3 MiB, held by every GPU that
+ * loads the library until exit), which limits n_m*n_g to 65536 (TRT_ERR_SCRATCH beyond).  The first
+ * call on a device looks up that array's address (with the device current); make that first call
+ * before any stream capture.  All calls share the array and it keeps the last call's contents; calls
+ * whose kernels overlap on the GPU race on it, so serialise them (one stream, or synchronise). */
+int trt_transport_residual_noalloc(int n_x, int n_y, int n_m, int n_g, const double* I_crn, const double* Ic_edgV,
+                                   const double* Ic_edgH, const double* Omega_x, const double* Omega_y,
+                                   const double* Delx, const double* Dely, const double* A, const double* KapE_in,
+                                   const double* Src_in, const double* I_crn_old, double c, double Delt,
+                                   double* RT_Residual, int* RT_ResLoc_x, int* RT_ResLoc_y, void* stream);
 
 /* Message for a TRT_ERR_* code. */
 const char* trt_strerror(int code);
