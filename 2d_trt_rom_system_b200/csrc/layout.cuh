@@ -15,7 +15,7 @@
 // x S direction slices (R*S = 32, lane = s*R + r).  Lane (s, r) of warp w owns the directions
 // m_q = d*S + s (d < D) of the quadrant and the row rho = w*R + r of a band of H = W*R rows.
 // Bands ("rounds") n = 0..nr-1 cover j' = n*H + rho.  Step T of the CTA puts every lane on the
-// anti-diagonal cell i' = T - rho - n*P (P = period >= max(nx, H)), so lane rows form a wavefront:
+// anti-diagonal cell i' = T - rho - n*P (P = period, nx <= P, H < P), so lane rows form a wavefront:
 // a cell's left inflow comes from the same lane one step earlier, its bottom inflow from the row
 // below one step earlier.
 //
@@ -44,7 +44,7 @@ struct Tiling {
   int R;       // rows per warp = 32 / S
   int D;       // directions per lane = ceil(mq / S)
   int H;       // rows per round = W * R
-  int P;       // period = max(nx, H)
+  int P;       // period = max(nx, H + 1)
   int nr;      // rounds = ceil(ny / H)
   int Tsteps;  // steps of one (g, q) sweep = (nr-1)*P + nx + H - 1
 };
@@ -58,7 +58,7 @@ TRT_LHD Tiling make_tiling(int nx, int ny, int mq, int W, int S) {
   t.R = 32 / S;
   t.D = ceil_div(mq, S);
   t.H = W * t.R;
-  t.P = nx > t.H ? nx : t.H;
+  t.P = nx > t.H ? nx : t.H + 1;   // P > H: a round's wrap entry is written a step before it is prefetched
   t.nr = ceil_div(ny, t.H);
   t.Tsteps = (t.nr - 1) * t.P + nx + t.H - 1;
   return t;

@@ -58,6 +58,7 @@ struct SweepArgs {
   const Real* qiso;         // (nx, ny, ng): isotropic corner source, or null with srcfull
   const Real* srcfull;      // skewed layout, anisotropic per-corner source (drop-in path), or null
   const Real* dirtab;       // [4][kNDirRow][mq]
+  const double* dir64;      // [kNDirRow][nm] FP64 direction table (moment weights)
   const Real* Iold;         // skewed
   Real* Inew;               // skewed
   Real* bndV;               // [2][ng][nm][2 ny]  Ic_edgV on faces x=0 (side 0) and x=nx (side 1)
@@ -72,12 +73,13 @@ struct SweepArgs {
 constexpr int kErrTmaTimeout = 1;
 
 template <class Real>
-__host__ __device__ inline size_t sweep_smem_bytes(int W, long long chunk, int stages, int mq) {
+__host__ __device__ inline size_t sweep_smem_bytes(int W, long long chunk, int stages, int mq, int D) {
   size_t ring = (size_t)stages * W * chunk * sizeof(Real);
   size_t bars = (size_t)stages * sizeof(uint64_t);
   size_t hand = (size_t)2 * W * mq * 2 * sizeof(Real);
   size_t dtab = (size_t)kNDirRow * mq * sizeof(Real);
-  return ring + bars + hand + dtab + 16;
+  size_t wtab = (size_t)6 * mq * sizeof(double);
+  return ring + bars + hand + dtab + wtab + 32;
 }
 
 // Reduce-scatter of the 16 moment slots over the S slices of a row (xor partners R, 2R, ..., 16):
@@ -114,20 +116,19 @@ __device__ __forceinline__ int slice_reduce_scatter(double (&v)[16], int s, bool
   return base;
 }
 
-// Kahan-compensated add: sum + p with the running compensation term.
-template <class Real>
-__device__ __forceinline__ void kahan_add(Real& sum, Real& comp, Real p) {
-  const Real y = p - comp;
-  const Real t = sum + y;
-  comp = (t - sum) - y;
-  sum = t;
-}
-
-// The FP32 ("mixed") sweep accumulates its per-lane moment sums with Kahan compensation; the FP64
-// sweep accumulates with fused multiply-adds.  Sums over slices, quadrants and groups are FP64.
+// Both precisions accumulate the per-lane moment sums in FP64: the FP32 ("mixed") sweep's
+// intensities are converted exactly and multiplied by FP64 weights on the otherwise idle FP64 pipe,
+// so the sums carry no FP32 rounding at all (stronger than a Kahan-compensated FP32 sum, and cheaper
+// on this part: measured 7.2 ms with Kahan vs the FP64-accumulating kernel on C1).  Sums over
+// slices, quadrants and groups are FP64 as well.
+// Two variants of the step body, chosen by precision (measured on C1, each the faster for its type):
+//  * FP32: global inflows prefetched one step ahead, every lane computes every direction slot and the
+//    bottom-inflow shuffle runs inline (no per-direction top-face registers);
+//  * FP64: global inflows loaded at the step start, only live slots compute, top faces kept in
+//    registers and shuffled after the direction loop (fits 128 registers without spills).
 template <class Real, int S, int D, bool SRC_FULL>
 __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a) {
-  constexpr bool KAHAN = sizeof(Real) == 4;
+  constexpr bool kLeanFP32 = sizeof(Real) == 4;
   constexpr int R = 32 / S;
   constexpr int NV = 16 / (int)sizeof(Real);
   constexpr int NSLOT = S >= 16 ? 1 : 16 / S;   // moment slots a lane holds after the reduce-scatter
@@ -152,11 +153,18 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + (size_t)stages * stage_bytes);
   Real* hand = reinterpret_cast<Real*>(mbar + stages);
   Real* dtab = hand + 2 * W * mq * 2;
+  double* wtab = reinterpret_cast<double*>(
+      (reinterpret_cast<uintptr_t>(dtab + kNDirRow * mq) + 15) & ~static_cast<uintptr_t>(15));
 
   for (int k = threadIdx.x; k < kNDirRow * mq; k += blockDim.x) {
     Real v = a.dirtab[(size_t)q * kNDirRow * mq + k];
     if (k < 2 * mq) v = v * Real(0.25);   // |Omega| / 4 for the corner-matrix geometry
     dtab[k] = v;
+  }
+  // moment weights w, w Ox^2, w Oy^2, w Ox Oy, w Ox, w Oy of the quadrant's directions, FP64
+  if constexpr (kLeanFP32) {
+    for (int k = threadIdx.x; k < 6 * mq; k += blockDim.x)
+      wtab[k] = a.dir64[(size_t)(kW + k / mq) * nm + q * mq + k % mq];
   }
   if (threadIdx.x == 0) {
     for (int k = 0; k < stages; ++k) mbar_init(&mbar[k], 1);
@@ -212,7 +220,45 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
       if (!SRC_FULL) mqs = qisog[cell];
     }
   };
+  // Inflows that come from global memory, loaded one step ahead into the inflow registers: the
+  // sweep-left boundary face at the start of a round, and for the CTA's first row the sweep-bottom
+  // boundary face (round 0) or the wrap buffer (later rounds).  The wrap entry for column ip of
+  // round n was written at step (n-1)P + ip + H - 1, before the barrier that precedes this prefetch
+  // (P > H).
+  auto load_inflow = [&](int ipn, int nn) {
+    if constexpr (!kLeanFP32) return;
+    const int jpn = nn * t.H + rho;
+    if (!(ipn >= 0 && ipn < nx && nn < t.nr && jpn < ny)) return;
+    const int in = fx ? nx - 1 - ipn : ipn;
+    const int jn = fy ? ny - 1 - jpn : jpn;
+    if (ipn == 0) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        const int ml = d * S + s;
+        if (d < D - 1 || s < s_last) {
+          vb[d] = bVin[ml * 2 * ny + 2 * jn + byo];
+          vt[d] = bVin[ml * 2 * ny + 2 * jn + 1 - byo];
+        }
+      }
+    }
+    if (rho == 0) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        const int ml = d * S + s;
+        if (d < D - 1 || s < s_last) {
+          if (nn == 0) {
+            hl[d] = bHin[ml * 2 * nx + 2 * in + bxo];
+            hr[d] = bHin[ml * 2 * nx + 2 * in + 1 - bxo];
+          } else {
+            hl[d] = wrapc[(ipn * mq + ml) * 2 + 0];
+            hr[d] = wrapc[(ipn * mq + ml) * 2 + 1];
+          }
+        }
+      }
+    }
+  };
   load_material(ip, n);
+  if (kLeanFP32) load_inflow(ip, n);
 
   bool timed_out = false;
   int stage = 0;
@@ -223,89 +269,269 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
     const Real* sm = ring + (size_t)stage * W * chunk + (size_t)warp * chunk;
     const int gchunk = (T * W + warp) * chunk;
 
-    const int jp = n * t.H + rho;
-    const bool active = !timed_out && ip >= 0 && ip < nx && n < t.nr && jp < ny;
-    const int i = fx ? nx - 1 - ip : ip;
-    const int j = fy ? ny - 1 - jp : jp;
+    int i, j;
+    bool active;
+    double acc[13];
+    if constexpr (!kLeanFP32) {
+      const int jp = n * t.H + rho;
+      active = !timed_out && ip >= 0 && ip < nx && n < t.nr && jp < ny;
+      i = fx ? nx - 1 - ip : ip;
+      j = fy ? ny - 1 - jp : jp;
 
-    Real topL[D], topR[D];
-    Real acc[13], cmp[13];
-#pragma unroll
-    for (int v = 0; v < 13; ++v) acc[v] = cmp[v] = Real(0);
-#pragma unroll
-    for (int d = 0; d < D; ++d) topL[d] = topR[d] = Real(0);
+      Real topL[D], topR[D];
+  #pragma unroll
+      for (int v = 0; v < 13; ++v) acc[v] = 0.0;
+  #pragma unroll
+      for (int d = 0; d < D; ++d) topL[d] = topR[d] = Real(0);
 
-    if (active) {
-      const Real dx = mdx, dy = mdy, A4 = mA4, kp = mkp, qs = mqs;
-      if (ip == 0) {
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-          const int ml = d * S + s;
-          if (d < D - 1 || s < s_last) {
-            vb[d] = bVin[ml * 2 * ny + 2 * j + byo];
-            vt[d] = bVin[ml * 2 * ny + 2 * j + 1 - byo];
+      if (active) {
+        const Real dx = mdx, dy = mdy, A4 = mA4, kp = mkp, qs = mqs;
+        if (ip == 0) {
+  #pragma unroll
+          for (int d = 0; d < D; ++d) {
+            const int ml = d * S + s;
+            if (d < D - 1 || s < s_last) {
+              vb[d] = bVin[ml * 2 * ny + 2 * j + byo];
+              vt[d] = bVin[ml * 2 * ny + 2 * j + 1 - byo];
+            }
           }
         }
-      }
-      if (r == 0) {
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-          const int ml = d * S + s;
-          if (d < D - 1 || s < s_last) {
-            const Real* src;
-            int o0, o1;
-            if (rho == 0) {
-              if (n == 0) {
-                src = bHin + ml * 2 * nx + 2 * i;
-                o0 = bxo;
-                o1 = 1 - bxo;
+        if (r == 0) {
+  #pragma unroll
+          for (int d = 0; d < D; ++d) {
+            const int ml = d * S + s;
+            if (d < D - 1 || s < s_last) {
+              const Real* src;
+              int o0, o1;
+              if (rho == 0) {
+                if (n == 0) {
+                  src = bHin + ml * 2 * nx + 2 * i;
+                  o0 = bxo;
+                  o1 = 1 - bxo;
+                } else {
+                  src = wrapc + (ip * mq + ml) * 2;
+                  o0 = 0;
+                  o1 = 1;
+                }
               } else {
-                src = wrapc + (ip * mq + ml) * 2;
+                src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mq + ml) * 2;
                 o0 = 0;
                 o1 = 1;
               }
-            } else {
-              src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mq + ml) * 2;
-              o0 = 0;
-              o1 = 1;
+              hl[d] = src[o0];
+              hr[d] = src[o1];
             }
-            hl[d] = src[o0];
-            hr[d] = src[o1];
+          }
+        }
+
+        const Real kA4 = scb_kA4(dx, dy, kp);
+  #pragma unroll
+        for (int d = 0; d < D; ++d) {
+          const int ml = d * S + s;
+          if (d < D - 1 || s < s_last) {
+            const int nl = (d < D - 1) ? 32 : nl_last;
+            const Real* sb = sm + d * 128;
+            Real io[4];
+            if (NV == 2) {
+              const double2 p0 = *reinterpret_cast<const double2*>(sb + lane * 2);
+              const double2 p1 = *reinterpret_cast<const double2*>(sb + nl * 2 + lane * 2);
+              io[0] = (Real)p0.x; io[1] = (Real)p0.y; io[2] = (Real)p1.x; io[3] = (Real)p1.y;
+            } else {
+              const float4 p0 = *reinterpret_cast<const float4*>(sb + lane * 4);
+              io[0] = (Real)p0.x; io[1] = (Real)p0.y; io[2] = (Real)p0.z; io[3] = (Real)p0.w;
+            }
+            Real src[4];
+            if (SRC_FULL) {
+              const Real* gs = a.srcfull + blk_off + gchunk + d * 128;
+  #pragma unroll
+              for (int c = 0; c < 4; ++c)
+                src[c] = tfma(io[c], rcdt, gs[(c / NV) * nl * NV + lane * NV + (c % NV)]);
+            } else {
+  #pragma unroll
+              for (int c = 0; c < 4; ++c) src[c] = tfma(io[c], rcdt, qs);
+            }
+            const ScbGeom<Real> G = scb_geom(dtab[kAx * mq + ml], dtab[kAy * mq + ml], dx, dy);
+            const Real gam = scb_gamma(G, kA4);
+            Real x[4];
+            scb_solve(G, gam, A4, src, vb[d], vt[d], hl[d], hr[d], x);
+
+            Real* gb = gnew + gchunk + d * 128;
+            if (NV == 2) {
+              *reinterpret_cast<double2*>(gb + lane * 2) = make_double2((double)x[0], (double)x[1]);
+              *reinterpret_cast<double2*>(gb + nl * 2 + lane * 2) = make_double2((double)x[2], (double)x[3]);
+            } else {
+              *reinterpret_cast<float4*>(gb + lane * 4) = make_float4((float)x[0], (float)x[1], (float)x[2], (float)x[3]);
+            }
+            // outflow: right face feeds the next column of this lane, top face the next row
+            vb[d] = x[1];
+            vt[d] = x[2];
+            topL[d] = x[3];
+            topR[d] = x[2];
+
+            const Real Iavg = ((x[0] + x[1]) + (x[2] + x[3])) * Real(0.25);
+            const Real Iv = (x[1] + x[2]) * Real(0.5);
+            const Real Ih = (x[3] + x[2]) * Real(0.5);
+            const Real wxx = dtab[kWxx * mq + ml], wyy = dtab[kWyy * mq + ml], wxy = dtab[kWxy * mq + ml];
+            const Real ww = dtab[kW * mq + ml], wx = dtab[kWx * mq + ml], wy = dtab[kWy * mq + ml];
+            {
+              acc[kCxx] = tfma(wxx, Iavg, acc[kCxx]);
+              acc[kCyy] = tfma(wyy, Iavg, acc[kCyy]);
+              acc[kCxy] = tfma(wxy, Iavg, acc[kCxy]);
+              acc[kCe] = tfma(ww, Iavg, acc[kCe]);
+              acc[kVxx] = tfma(wxx, Iv, acc[kVxx]);
+              acc[kVxy] = tfma(wxy, Iv, acc[kVxy]);
+              acc[kVx] = tfma(wx, Iv, acc[kVx]);
+              acc[kVe] = tfma(ww, Iv, acc[kVe]);
+              acc[kHyy] = tfma(wyy, Ih, acc[kHyy]);
+              acc[kHxy] = tfma(wxy, Ih, acc[kHxy]);
+              acc[kHy] = tfma(wy, Ih, acc[kHy]);
+              acc[kHx] = tfma(wx, Ih, acc[kHx]);
+              acc[kHe] = tfma(ww, Ih, acc[kHe]);
+            }
+          }
+        }
+
+        // outflow boundary faces and the handoff of the warp's last row
+        const bool right_edge = (ip == nx - 1), top_edge = (jp == ny - 1), last_row = (r == R - 1);
+        if (right_edge || top_edge || last_row) {
+  #pragma unroll
+          for (int d = 0; d < D; ++d) {
+            const int ml = d * S + s;
+            if (d < D - 1 || s < s_last) {
+              if (right_edge) {
+                bVout[ml * 2 * ny + 2 * j + byo] = vb[d];
+                bVout[ml * 2 * ny + 2 * j + 1 - byo] = vt[d];
+              }
+              if (top_edge) {
+                bHout[ml * 2 * nx + 2 * i + bxo] = topL[d];
+                bHout[ml * 2 * nx + 2 * i + 1 - bxo] = topR[d];
+              }
+              if (last_row) {
+                Real* dst = (warp < W - 1) ? hand + (((T & 1) * W + warp) * mq + ml) * 2
+                                           : wrapc + (ip * mq + ml) * 2;
+                if (warp < W - 1 || t.nr > 1) {
+                  dst[0] = topL[d];
+                  dst[1] = topR[d];
+                }
+              }
+            }
           }
         }
       }
 
-      const Real kA4 = scb_kA4(dx, dy, kp);
-#pragma unroll
+      // bottom inflow of rows r >= 1 for the next step (rows r == 0 reload it)
+  #pragma unroll
       for (int d = 0; d < D; ++d) {
-        const int ml = d * S + s;
-        if (d < D - 1 || s < s_last) {
-          const int nl = (d < D - 1) ? 32 : nl_last;
-          const Real* sb = sm + d * 128;
-          Real io[4];
-          if (NV == 2) {
-            const double2 p0 = *reinterpret_cast<const double2*>(sb + lane * 2);
-            const double2 p1 = *reinterpret_cast<const double2*>(sb + nl * 2 + lane * 2);
-            io[0] = (Real)p0.x; io[1] = (Real)p0.y; io[2] = (Real)p1.x; io[3] = (Real)p1.y;
-          } else {
-            const float4 p0 = *reinterpret_cast<const float4*>(sb + lane * 4);
-            io[0] = (Real)p0.x; io[1] = (Real)p0.y; io[2] = (Real)p0.z; io[3] = (Real)p0.w;
-          }
-          Real src[4];
-          if (SRC_FULL) {
-            const Real* gs = a.srcfull + blk_off + gchunk + d * 128;
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-              src[c] = tfma(io[c], rcdt, gs[(c / NV) * nl * NV + lane * NV + (c % NV)]);
-          } else {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) src[c] = tfma(io[c], rcdt, qs);
-          }
-          const ScbGeom<Real> G = scb_geom(dtab[kAx * mq + ml], dtab[kAy * mq + ml], dx, dy);
-          const Real gam = scb_gamma(G, kA4);
-          Real x[4];
-          scb_solve(G, gam, A4, src, vb[d], vt[d], hl[d], hr[d], x);
+        hl[d] = __shfl_up_sync(0xffffffffu, topL[d], 1);
+        hr[d] = __shfl_up_sync(0xffffffffu, topR[d], 1);
+      }
 
+    } else {
+      const int jp = n * t.H + rho;
+      active = !timed_out && ip >= 0 && ip < nx && n < t.nr && jp < ny;
+      i = fx ? nx - 1 - ip : ip;
+      j = fy ? ny - 1 - jp : jp;
+      const Real dx = mdx, dy = mdy, A4 = mA4, kp = mkp, qs = mqs;
+
+      if (!kLeanFP32 && active) {
+        // global-memory inflows: the sweep-left boundary face at the start of a round, and for the
+        // CTA's first row the sweep-bottom boundary face (round 0) or the wrap buffer
+        if (ip == 0) {
+  #pragma unroll
+          for (int d = 0; d < D; ++d) {
+            const int ml = d * S + s;
+            if (d < D - 1 || s < s_last) {
+              vb[d] = bVin[ml * 2 * ny + 2 * j + byo];
+              vt[d] = bVin[ml * 2 * ny + 2 * j + 1 - byo];
+            }
+          }
+        }
+        if (rho == 0) {
+  #pragma unroll
+          for (int d = 0; d < D; ++d) {
+            const int ml = d * S + s;
+            if (d < D - 1 || s < s_last) {
+              if (n == 0) {
+                hl[d] = bHin[ml * 2 * nx + 2 * i + bxo];
+                hr[d] = bHin[ml * 2 * nx + 2 * i + 1 - bxo];
+              } else {
+                hl[d] = wrapc[(ip * mq + ml) * 2 + 0];
+                hr[d] = wrapc[(ip * mq + ml) * 2 + 1];
+              }
+            }
+          }
+        }
+      }
+      // bottom inflow of a warp's first row from the warp below (shared memory, written last step)
+      if (active && r == 0 && warp > 0) {
+  #pragma unroll
+        for (int d = 0; d < D; ++d) {
+          const int ml = d * S + s;
+          if (d < D - 1 || s < s_last) {
+            const Real* src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mq + ml) * 2;
+            hl[d] = src[0];
+            hr[d] = src[1];
+          }
+        }
+      }
+
+      const bool right_edge = active && (ip == nx - 1);
+      const bool top_edge = active && (jp == ny - 1);
+      const bool last_row = active && (r == R - 1) && (warp < W - 1 || t.nr > 1);
+      Real* hand_dst = (warp < W - 1) ? hand + ((T & 1) * W + warp) * mq * 2 : wrapc + ip * mq * 2;
+
+  #pragma unroll
+      for (int v = 0; v < 13; ++v) acc[v] = 0.0;
+      Real topL[kLeanFP32 ? 1 : D], topR[kLeanFP32 ? 1 : D];
+      const Real kA4 = scb_kA4(dx, dy, kp);
+
+  #pragma unroll
+      for (int d = 0; d < D; ++d) {
+        const bool valid = (d < D - 1) || (s < s_last);
+        // FP32: every lane computes every slot (idle slots and inactive lanes on valid addresses, results
+        // discarded) so the bottom-inflow shuffle runs inline; FP64: only live slots compute.
+        if (!kLeanFP32 && !(active && valid)) continue;
+        const int ml = valid ? d * S + s : 0;
+        const int ln = valid ? lane : 0;
+        const bool live = active && valid;
+        const int nl = (d < D - 1) ? 32 : nl_last;
+        const Real* sb = sm + d * 128;
+        Real io[4];
+        if (NV == 2) {
+          const double2 p0 = *reinterpret_cast<const double2*>(sb + ln * 2);
+          const double2 p1 = *reinterpret_cast<const double2*>(sb + nl * 2 + ln * 2);
+          io[0] = (Real)p0.x; io[1] = (Real)p0.y; io[2] = (Real)p1.x; io[3] = (Real)p1.y;
+        } else {
+          const float4 p0 = *reinterpret_cast<const float4*>(sb + ln * 4);
+          io[0] = (Real)p0.x; io[1] = (Real)p0.y; io[2] = (Real)p0.z; io[3] = (Real)p0.w;
+        }
+        Real src[4];
+        if (SRC_FULL) {
+          const Real* gs = a.srcfull + blk_off + gchunk + d * 128;
+  #pragma unroll
+          for (int c = 0; c < 4; ++c)
+            src[c] = tfma(io[c], rcdt, live ? gs[(c / NV) * nl * NV + ln * NV + (c % NV)] : Real(0));
+        } else {
+  #pragma unroll
+          for (int c = 0; c < 4; ++c) src[c] = tfma(io[c], rcdt, qs);
+        }
+        const ScbGeom<Real> G = scb_geom(dtab[kAx * mq + ml], dtab[kAy * mq + ml], dx, dy);
+        const Real gam = scb_gamma(G, kA4);
+        Real x[4];
+        scb_solve(G, gam, A4, src, vb[d], vt[d], hl[d], hr[d], x);
+
+        // outflow: right face feeds this lane's next column, top face the next row
+        vb[d] = x[1];
+        vt[d] = x[2];
+        if (kLeanFP32) {
+          hl[d] = __shfl_up_sync(0xffffffffu, x[3], 1);
+          hr[d] = __shfl_up_sync(0xffffffffu, x[2], 1);
+        } else {
+          topL[kLeanFP32 ? 0 : d] = x[3];
+          topR[kLeanFP32 ? 0 : d] = x[2];
+        }
+
+        if (live) {
           Real* gb = gnew + gchunk + d * 128;
           if (NV == 2) {
             *reinterpret_cast<double2*>(gb + lane * 2) = make_double2((double)x[0], (double)x[1]);
@@ -313,89 +539,77 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
           } else {
             *reinterpret_cast<float4*>(gb + lane * 4) = make_float4((float)x[0], (float)x[1], (float)x[2], (float)x[3]);
           }
-          // outflow: right face feeds the next column of this lane, top face the next row
-          vb[d] = x[1];
-          vt[d] = x[2];
-          topL[d] = x[3];
-          topR[d] = x[2];
-
-          const Real Iavg = ((x[0] + x[1]) + (x[2] + x[3])) * Real(0.25);
-          const Real Iv = (x[1] + x[2]) * Real(0.5);
-          const Real Ih = (x[3] + x[2]) * Real(0.5);
-          const Real wxx = dtab[kWxx * mq + ml], wyy = dtab[kWyy * mq + ml], wxy = dtab[kWxy * mq + ml];
-          const Real ww = dtab[kW * mq + ml], wx = dtab[kWx * mq + ml], wy = dtab[kWy * mq + ml];
-          if (KAHAN) {
-            // FP32 sums with Kahan compensation (the compensation terms live in cmp[])
-            kahan_add(acc[kCxx], cmp[kCxx], wxx * Iavg);
-            kahan_add(acc[kCyy], cmp[kCyy], wyy * Iavg);
-            kahan_add(acc[kCxy], cmp[kCxy], wxy * Iavg);
-            kahan_add(acc[kCe], cmp[kCe], ww * Iavg);
-            kahan_add(acc[kVxx], cmp[kVxx], wxx * Iv);
-            kahan_add(acc[kVxy], cmp[kVxy], wxy * Iv);
-            kahan_add(acc[kVx], cmp[kVx], wx * Iv);
-            kahan_add(acc[kVe], cmp[kVe], ww * Iv);
-            kahan_add(acc[kHyy], cmp[kHyy], wyy * Ih);
-            kahan_add(acc[kHxy], cmp[kHxy], wxy * Ih);
-            kahan_add(acc[kHy], cmp[kHy], wy * Ih);
-            kahan_add(acc[kHx], cmp[kHx], wx * Ih);
-            kahan_add(acc[kHe], cmp[kHe], ww * Ih);
-          } else {
-            acc[kCxx] = tfma(wxx, Iavg, acc[kCxx]);
-            acc[kCyy] = tfma(wyy, Iavg, acc[kCyy]);
-            acc[kCxy] = tfma(wxy, Iavg, acc[kCxy]);
-            acc[kCe] = tfma(ww, Iavg, acc[kCe]);
-            acc[kVxx] = tfma(wxx, Iv, acc[kVxx]);
-            acc[kVxy] = tfma(wxy, Iv, acc[kVxy]);
-            acc[kVx] = tfma(wx, Iv, acc[kVx]);
-            acc[kVe] = tfma(ww, Iv, acc[kVe]);
-            acc[kHyy] = tfma(wyy, Ih, acc[kHyy]);
-            acc[kHxy] = tfma(wxy, Ih, acc[kHxy]);
-            acc[kHy] = tfma(wy, Ih, acc[kHy]);
-            acc[kHx] = tfma(wx, Ih, acc[kHx]);
-            acc[kHe] = tfma(ww, Ih, acc[kHe]);
+          if (kLeanFP32) {
+            if (right_edge) {
+              bVout[ml * 2 * ny + 2 * j + byo] = x[1];
+              bVout[ml * 2 * ny + 2 * j + 1 - byo] = x[2];
+            }
+            if (top_edge) {
+              bHout[ml * 2 * nx + 2 * i + bxo] = x[3];
+              bHout[ml * 2 * nx + 2 * i + 1 - bxo] = x[2];
+            }
+            if (last_row) {
+              hand_dst[ml * 2 + 0] = x[3];
+              hand_dst[ml * 2 + 1] = x[2];
+            }
           }
+          const double Iavg = (double)(((x[0] + x[1]) + (x[2] + x[3])) * Real(0.25));
+          const double Iv = (double)((x[1] + x[2]) * Real(0.5));
+          const double Ih = (double)((x[3] + x[2]) * Real(0.5));
+          const double ww = wtab[0 * mq + ml], wxx = wtab[1 * mq + ml], wyy = wtab[2 * mq + ml];
+          const double wxy = wtab[3 * mq + ml], wx = wtab[4 * mq + ml], wy = wtab[5 * mq + ml];
+          acc[kCxx] = fma(wxx, Iavg, acc[kCxx]);
+          acc[kCyy] = fma(wyy, Iavg, acc[kCyy]);
+          acc[kCxy] = fma(wxy, Iavg, acc[kCxy]);
+          acc[kCe] = fma(ww, Iavg, acc[kCe]);
+          acc[kVxx] = fma(wxx, Iv, acc[kVxx]);
+          acc[kVxy] = fma(wxy, Iv, acc[kVxy]);
+          acc[kVx] = fma(wx, Iv, acc[kVx]);
+          acc[kVe] = fma(ww, Iv, acc[kVe]);
+          acc[kHyy] = fma(wyy, Ih, acc[kHyy]);
+          acc[kHxy] = fma(wxy, Ih, acc[kHxy]);
+          acc[kHy] = fma(wy, Ih, acc[kHy]);
+          acc[kHx] = fma(wx, Ih, acc[kHx]);
+          acc[kHe] = fma(ww, Ih, acc[kHe]);
         }
       }
 
-      // outflow boundary faces and the handoff of the warp's last row
-      const bool right_edge = (ip == nx - 1), top_edge = (jp == ny - 1), last_row = (r == R - 1);
-      if (right_edge || top_edge || last_row) {
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-          const int ml = d * S + s;
-          if (d < D - 1 || s < s_last) {
-            if (right_edge) {
-              bVout[ml * 2 * ny + 2 * j + byo] = vb[d];
-              bVout[ml * 2 * ny + 2 * j + 1 - byo] = vt[d];
-            }
-            if (top_edge) {
-              bHout[ml * 2 * nx + 2 * i + bxo] = topL[d];
-              bHout[ml * 2 * nx + 2 * i + 1 - bxo] = topR[d];
-            }
-            if (last_row) {
-              Real* dst = (warp < W - 1) ? hand + (((T & 1) * W + warp) * mq + ml) * 2
-                                         : wrapc + (ip * mq + ml) * 2;
-              if (warp < W - 1 || t.nr > 1) {
-                dst[0] = topL[d];
-                dst[1] = topR[d];
+      if (!kLeanFP32) {
+        // FP64: outflow boundary faces, the handoff of the warp's last row and the bottom-inflow
+        // shuffle, after the direction loop
+        if (right_edge || top_edge || last_row) {
+  #pragma unroll
+          for (int d = 0; d < D; ++d) {
+            const int ml = d * S + s;
+            if (d < D - 1 || s < s_last) {
+              if (right_edge) {
+                bVout[ml * 2 * ny + 2 * j + byo] = vb[d];
+                bVout[ml * 2 * ny + 2 * j + 1 - byo] = vt[d];
+              }
+              if (top_edge) {
+                bHout[ml * 2 * nx + 2 * i + bxo] = topL[kLeanFP32 ? 0 : d];
+                bHout[ml * 2 * nx + 2 * i + 1 - bxo] = topR[kLeanFP32 ? 0 : d];
+              }
+              if (last_row) {
+                hand_dst[ml * 2 + 0] = topL[kLeanFP32 ? 0 : d];
+                hand_dst[ml * 2 + 1] = topR[kLeanFP32 ? 0 : d];
               }
             }
           }
         }
+  #pragma unroll
+        for (int d = 0; d < D; ++d) {
+          hl[d] = __shfl_up_sync(0xffffffffu, topL[kLeanFP32 ? 0 : d], 1);
+          hr[d] = __shfl_up_sync(0xffffffffu, topR[kLeanFP32 ? 0 : d], 1);
+        }
       }
-    }
 
-    // bottom inflow of rows r >= 1 for the next step (rows r == 0 reload it)
-#pragma unroll
-    for (int d = 0; d < D; ++d) {
-      hl[d] = __shfl_up_sync(0xffffffffu, topL[d], 1);
-      hr[d] = __shfl_up_sync(0xffffffffu, topR[d], 1);
     }
 
     // moments: reduce-scatter over the S slices of each row, then each lane writes its slots
     double mv[16];
 #pragma unroll
-    for (int v = 0; v < 13; ++v) mv[v] = KAHAN ? (double)acc[v] - (double)cmp[v] : (double)acc[v];
+    for (int v = 0; v < 13; ++v) mv[v] = acc[v];
     mv[13] = mv[14] = mv[15] = 0.0;
     bool owner;
     const int base = slice_reduce_scatter<S, R>(mv, s, &owner);
@@ -411,13 +625,14 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
       }
     }
 
-    // advance the lane and prefetch the material of its next cell
+    // advance the lane and prefetch the material and the global-memory inflows of its next cell
     ++ip;
     if (ip == t.P) {
       ip = 0;
       ++n;
     }
     load_material(ip, n);
+    if (kLeanFP32) load_inflow(ip, n);
 
     const int any_timeout = __syncthreads_or(timed_out ? 1 : 0);
     if (any_timeout) {

@@ -267,10 +267,12 @@ int setup_layout(trt_ctx* c) {
   c->blk = trt::block_elems(c->mq, c->t);
   // pipeline depth limited by shared memory
   const size_t esz = c->esz();
-  while (c->stages > 1 && (c->prec == TRT_PREC_FP64 ? trt::sweep_smem_bytes<double>(W, c->chunk, c->stages, c->mq)
-                                                     : trt::sweep_smem_bytes<float>(W, c->chunk, c->stages, c->mq)) >
-                              (size_t)200 * 1024)
-    c->stages--;
+  auto smem_at = [&](int st) {
+    return c->prec == TRT_PREC_FP64 ? trt::sweep_smem_bytes<double>(W, c->chunk, st, c->mq, c->t.D)
+                                    : trt::sweep_smem_bytes<float>(W, c->chunk, st, c->mq, c->t.D);
+  };
+  while (c->stages > 1 && smem_at(c->stages) > (size_t)200 * 1024) c->stages--;
+  if (smem_at(c->stages) > (size_t)220 * 1024) return TRT_ERR_ARG;   // tiling does not fit an SM
   const size_t sbytes = (size_t)c->state_elems() * esz;
   for (int k = 0; k < 2; ++k) {
     if (c->d_state[k]) c->dfree(c->d_state[k], sbytes);
@@ -393,6 +395,7 @@ int sweep_impl(trt_ctx* c, unsigned flags) {
   a.qiso = c->use_srcfull ? nullptr : (const Real*)c->d_q;
   a.srcfull = c->use_srcfull ? (const Real*)c->d_srcfull : nullptr;
   a.dirtab = (const Real*)c->d_dirtab;
+  a.dir64 = c->d_dir;
   a.Iold = (const Real*)c->d_state[c->cur];
   a.Inew = (Real*)c->d_state[1 - c->cur];
   a.bndV = (Real*)c->d_bndV;
@@ -402,7 +405,7 @@ int sweep_impl(trt_ctx* c, unsigned flags) {
   a.err = c->d_err;
   a.max_polls = c->wait_polls;
   a.drain_polls = 1u << 24;
-  const size_t smem = trt::sweep_smem_bytes<Real>(c->t.W, c->chunk, c->stages, c->mq);
+  const size_t smem = trt::sweep_smem_bytes<Real>(c->t.W, c->chunk, c->stages, c->mq, c->t.D);
   cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, 4 * c->ng, 32 * c->t.W, smem, c->stream, a);
   TRT_LAUNCHED();
   if (e != cudaSuccess) return TRT_ERR_CUDA;

@@ -158,7 +158,7 @@ def run_tiling_sweep(args):
     for prec in ("fp64", "fp32"):
         s, _, _ = setup_instance(pkg, prob, "mixed" if prec == "fp32" else "fp64", None)
         try:
-            for W in (2, 4, 8, 12, 16):
+            for W in (4, 6, 8, 12, 16):
                 for S in (0, 4, 8, 16):
                     for st in (2, 3):
                         try:
