@@ -79,8 +79,8 @@ SIGNATURES = {
     "trt_create": (_P, [_i, _i, _i, _i, _D, _D, _D, _D, _D, _i, ctypes.c_size_t, _I]),
     "trt_destroy": (None, [_P]),
     "trt_required_bytes": (ctypes.c_size_t, [_i, _i, _i, _i, _i]),
-    "trt_set_tiling": (_i, [_P, _i, _i, _i]),
-    "trt_get_tiling": (_i, [_P, _I, _I, _I, _I]),
+    "trt_set_tiling": (_i, [_P, _i, _i, _i, _i]),
+    "trt_get_tiling": (_i, [_P, _I, _I, _I, _I, _I]),
     "trt_set_material": (_i, [_P, _D, _D, _d, _d, _d]),
     "trt_set_material_device": (_i, [_P, _P, _P, _d, _d, _d]),
     "trt_set_source_full": (_i, [_P, _D]),

@@ -196,13 +196,15 @@ class TransportSweep:
     def handle(self):
         return self._h
 
-    def set_tiling(self, warps=0, slices=0, stages=0):
-        check(_lib.lib().trt_set_tiling(self._h, int(warps), int(slices), int(stages)), "trt_set_tiling")
+    def set_tiling(self, warps=0, slices=0, stages=0, splits=0):
+        """Kernel tiling (0 = default for each); re-lays out the state, which must be put again."""
+        check(_lib.lib().trt_set_tiling(self._h, int(warps), int(slices), int(stages), int(splits)),
+              "trt_set_tiling")
 
     def tiling(self):
-        v = [ctypes.c_int(0) for _ in range(4)]
+        v = [ctypes.c_int(0) for _ in range(5)]
         check(_lib.lib().trt_get_tiling(self._h, *[ctypes.byref(x) for x in v]), "trt_get_tiling")
-        return dict(zip(("warps", "slices", "dirs_per_lane", "stages"), [x.value for x in v]))
+        return dict(zip(("warps", "slices", "dirs_per_lane", "stages", "splits"), [x.value for x in v]))
 
     def set_material(self, KapE_in, src_iso, c, Delt, Comp_Unit):
         K = _f64(KapE_in, (self.nx, self.ny, self.ng))

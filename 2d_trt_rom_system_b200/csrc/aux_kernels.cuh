@@ -25,10 +25,14 @@ struct Geo {
 template <class Real>
 __device__ __forceinline__ long long state_index(const Geo& G, int i, int j, int cx, int cy, int m, int g) {
   constexpr int NV = 16 / (int)sizeof(Real);
-  const int q = m / G.mq, ml = m % G.mq;
+  const int q = m / G.mq, mlq = m % G.mq;
+  // split h holds quadrant-local directions [split_first(h), split_first(h) + split_count(h))
+  const int NH = G.t.NH, base = G.mq / NH, rem = G.mq % NH;
+  const int h = mlq < rem * (base + 1) ? mlq / (base + 1) : rem + (mlq - rem * (base + 1)) / base;
+  const int ml = mlq - split_first(G.mq, NH, h);
   const SweepPos p = sweep_pos(G.nx, G.ny, G.t, q, i, j);
   const int c = frame_corner(q, cx, cy);
-  return (long long)(g * 4 + q) * G.blk + skew_offset<NV>(G.mq, G.t, p.T, p.w, ml, p.r, c);
+  return ((long long)(g * 4 + q) * NH + h) * G.blk + skew_offset<NV>(G.t, p.T, p.w, ml, p.r, c);
 }
 
 template <class Real>
@@ -208,8 +212,9 @@ struct CombineArgs {
   double eps;          // 1e-25 / Comp_Unit
   double c;            // speed of light used by fg_Calc (passed in by the reference's caller)
   int bc[4];           // BC_Type L, B, R, T
+  int nh;              // direction splits per quadrant (partials per quadrant)
   WeightSums ws;
-  const double* part;  // [4][ng][ny][nx][kNPart]
+  const double* part;  // [4*nh][ng][ny][nx][kNPart]
   const double* dir;   // [kNDirRow][nm] full direction table (physical), double
 };
 
@@ -235,15 +240,17 @@ __global__ void combine_kernel(CombineArgs A, const Real* __restrict__ bndV, con
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const double eps = A.eps, c = A.c;
-  auto P = [&](int q, int g, int i, int j) { return A.part + (((size_t)(q * ng + g) * ny + j) * nx + i) * kNPart; };
+  // partial of quadrant q, direction split h
+  auto P = [&](int qh, int g, int i, int j) { return A.part + (((size_t)(qh * ng + g) * ny + j) * nx + i) * kNPart; };
+  const int NH = A.nh;
   auto wsum = [&](int v) { return A.ws.s[0][v] + A.ws.s[1][v] + A.ws.s[2][v] + A.ws.s[3][v]; };
 
   // cell centres
   for (long long k = k0; k < nA; k += stride) {
     const int i = (int)(k % nx), j = (int)((k / nx) % ny), g = (int)(k / nxy);
     double xx = 0, yy = 0, xy = 0, e = 0;
-    for (int q = 0; q < 4; ++q) {
-      const double* p = P(q, g, i, j);
+    for (int qh = 0; qh < 4 * NH; ++qh) {
+      const double* p = P(qh, g, i, j);
       xx += p[kCxx]; yy += p[kCyy]; xy += p[kCxy]; e += p[kCe];
     }
     xx += eps * wsum(kWxx); yy += eps * wsum(kWyy); xy += eps * wsum(kWxy); e += eps * wsum(kW);
@@ -266,9 +273,11 @@ __global__ void combine_kernel(CombineArgs A, const Real* __restrict__ bndV, con
       const bool xpos = (q == 0 || q == 3);
       const int cell = xpos ? f - 1 : f;     // upwind cell of this face for quadrant q
       if (cell >= 0 && cell < nx) {
-        const double* p = P(q, g, cell, j);
-        xx += p[kVxx]; xy += p[kVxy]; fxs += p[kVx]; e += p[kVe];
-        if (f == 0 || f == nx) { outF += p[kVx]; outE += p[kVe]; }
+        for (int h = 0; h < NH; ++h) {
+          const double* p = P(q * NH + h, g, cell, j);
+          xx += p[kVxx]; xy += p[kVxy]; fxs += p[kVx]; e += p[kVe];
+          if (f == 0 || f == nx) { outF += p[kVx]; outE += p[kVe]; }
+        }
       } else {
         double s[kNDirRow];
         inflow_face_sums<Real>(A, bndV, f == 0 ? 0 : 1, g, q, j, 2 * ny, s);
@@ -314,9 +323,11 @@ __global__ void combine_kernel(CombineArgs A, const Real* __restrict__ bndV, con
       const bool ypos = (q == 0 || q == 1);
       const int cell = ypos ? f - 1 : f;
       if (cell >= 0 && cell < ny) {
-        const double* p = P(q, g, i, cell);
-        yy += p[kHyy]; xy += p[kHxy]; fys += p[kHy]; fxq += p[kHx]; e += p[kHe];
-        if (f == 0 || f == ny) { outF += p[kHy]; outE += p[kHe]; }
+        for (int h = 0; h < NH; ++h) {
+          const double* p = P(q * NH + h, g, i, cell);
+          yy += p[kHyy]; xy += p[kHxy]; fys += p[kHy]; fxq += p[kHx]; e += p[kHe];
+          if (f == 0 || f == ny) { outF += p[kHy]; outE += p[kHe]; }
+        }
       } else {
         double s[kNDirRow];
         inflow_face_sums<Real>(A, bndH, f == 0 ? 0 : 1, g, q, i, 2 * nx, s);

@@ -11,17 +11,19 @@
 // TRANSPORT_SOLVES.f08:58-241 mirrored.  Corners of a cell are numbered in the frame: 0 = lb,
 // 1 = rb, 2 = rt, 3 = lt.
 //
-// Work decomposition.  One CTA sweeps one (group, quadrant).  It has W warps; a warp holds R rows
-// x S direction slices (R*S = 32, lane = s*R + r).  Lane (s, r) of warp w owns the directions
-// m_q = d*S + s (d < D) of the quadrant and the row rho = w*R + r of a band of H = W*R rows.
+// Work decomposition.  One CTA sweeps one (group, quadrant, direction split): the mq directions of
+// a quadrant are split into NH contiguous parts of floor/ceil(mq/NH) directions (more CTAs than
+// (group, quadrant) pairs balance the SMs).  A CTA has W warps; a warp holds R rows x S direction
+// slices (R*S = 32, lane = s*R + r).  Lane (s, r) of warp w owns the directions d*S + s (d < D) of
+// its split and the row rho = w*R + r of a band of H = W*R rows.
 // Bands ("rounds") n = 0..nr-1 cover j' = n*H + rho.  Step T of the CTA puts every lane on the
 // anti-diagonal cell i' = T - rho - n*P (P = period, nx <= P, H < P), so lane rows form a wavefront:
 // a cell's left inflow comes from the same lane one step earlier, its bottom inflow from the row
 // below one step earlier.
 //
-// Skewed state layout.  For each (g, q) a block of Tsteps*W chunks; chunk (T, w) holds the cells
+// Skewed state layout.  For each (g, q, h) a block of Tsteps*W chunks; chunk (T, w) holds the cells
 // the lanes of warp w touch at step T, as D sub-blocks (one per d) of nl_d lanes
-// (nl_d = R*min(S, mq - d*S)); a lane's 4 corners are stored as 16-byte vectors ("pairs" for
+// (nl_d = R*min(S, mqc - d*S), mqc = ceil(mq/NH)); a lane's 4 corners are stored as 16-byte vectors ("pairs" for
 // FP64, one vector for FP32), vector-major inside a sub-block so that a warp's load of one vector
 // is one contiguous 16*nl_d-byte run.  A whole CTA step is W contiguous chunks, which one TMA
 // bulk copy stages into shared memory.
@@ -42,7 +44,9 @@ struct Tiling {
   int W;       // warps per CTA
   int S;       // direction slices per warp (power of two)
   int R;       // rows per warp = 32 / S
-  int D;       // directions per lane = ceil(mq / S)
+  int NH;      // direction splits per quadrant (CTAs per (group, quadrant))
+  int mqc;     // directions of the largest split = ceil(mq / NH) (chunk width)
+  int D;       // directions per lane = ceil(mqc / S)
   int H;       // rows per round = W * R
   int P;       // period = max(nx, H + 1)
   int nr;      // rounds = ceil(ny / H)
@@ -51,12 +55,14 @@ struct Tiling {
 
 TRT_LHD int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
-TRT_LHD Tiling make_tiling(int nx, int ny, int mq, int W, int S) {
+TRT_LHD Tiling make_tiling(int nx, int ny, int mq, int W, int S, int NH) {
   Tiling t;
   t.W = W;
   t.S = S;
   t.R = 32 / S;
-  t.D = ceil_div(mq, S);
+  t.NH = NH;
+  t.mqc = ceil_div(mq, NH);
+  t.D = ceil_div(t.mqc, S);
   t.H = W * t.R;
   t.P = nx > t.H ? nx : t.H + 1;   // P > H: a round's wrap entry is written a step before it is prefetched
   t.nr = ceil_div(ny, t.H);
@@ -64,23 +70,25 @@ TRT_LHD Tiling make_tiling(int nx, int ny, int mq, int W, int S) {
   return t;
 }
 
-// Elements per chunk (T, w): mq directions x R rows x 4 corners.
-TRT_LHD long long chunk_elems(int mq, const Tiling& t) { return (long long)mq * t.R * 4; }
-// Elements per (g, q) block.
-TRT_LHD long long block_elems(int mq, const Tiling& t) {
-  return (long long)t.Tsteps * t.W * chunk_elems(mq, t);
-}
+// Direction split h of a quadrant: first quadrant-local direction and count (floor/ceil(mq/NH)).
+TRT_LHD int split_first(int mq, int NH, int h) { return h * (mq / NH) + (h < mq % NH ? h : mq % NH); }
+TRT_LHD int split_count(int mq, int NH, int h) { return mq / NH + (h < mq % NH ? 1 : 0); }
 
-// Offset of corner c (frame numbering) of direction m_q of lane (s, r) of warp w at step T,
-// inside one (g, q) block.  NV = 16 / sizeof(Real) values per 16-byte vector.
+// Elements per chunk (T, w): mqc directions x R rows x 4 corners.
+TRT_LHD long long chunk_elems(const Tiling& t) { return (long long)t.mqc * t.R * 4; }
+// Elements per (g, q, h) block.
+TRT_LHD long long block_elems(const Tiling& t) { return (long long)t.Tsteps * t.W * chunk_elems(t); }
+
+// Offset of corner c (frame numbering) of split-local direction mloc of lane (s, r) of warp w at
+// step T, inside one (g, q, h) block.  NV = 16 / sizeof(Real) values per 16-byte vector.
 template <int NV>
-TRT_LHD long long skew_offset(int mq, const Tiling& t, int T, int w, int mloc, int r, int c) {
+TRT_LHD long long skew_offset(const Tiling& t, int T, int w, int mloc, int r, int c) {
   const int d = mloc / t.S;
   const int s = mloc % t.S;
-  const int nslice = (mq - d * t.S) < t.S ? (mq - d * t.S) : t.S;
+  const int nslice = (t.mqc - d * t.S) < t.S ? (t.mqc - d * t.S) : t.S;
   const int nl = t.R * nslice;
   const int lane = s * t.R + r;
-  long long off = ((long long)T * t.W + w) * chunk_elems(mq, t);
+  long long off = ((long long)T * t.W + w) * chunk_elems(t);
   off += (long long)d * 128;              // all earlier sub-blocks are full (32 lanes x 4)
   off += (long long)(c / NV) * nl * NV + (long long)lane * NV + (c % NV);
   return off;

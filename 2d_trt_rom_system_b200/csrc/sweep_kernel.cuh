@@ -73,12 +73,12 @@ struct SweepArgs {
 constexpr int kErrTmaTimeout = 1;
 
 template <class Real>
-__host__ __device__ inline size_t sweep_smem_bytes(int W, long long chunk, int stages, int mq, int D) {
+__host__ __device__ inline size_t sweep_smem_bytes(int W, long long chunk, int stages, int mqc, int D) {
   size_t ring = (size_t)stages * W * chunk * sizeof(Real);
   size_t bars = (size_t)stages * sizeof(uint64_t);
-  size_t hand = (size_t)2 * W * mq * 2 * sizeof(Real);
-  size_t dtab = (size_t)kNDirRow * mq * sizeof(Real);
-  size_t wtab = (size_t)6 * mq * sizeof(double);
+  size_t hand = (size_t)2 * W * mqc * 2 * sizeof(Real);
+  size_t dtab = (size_t)kNDirRow * mqc * sizeof(Real);
+  size_t wtab = (size_t)6 * mqc * sizeof(double) + 16;
   return ring + bars + hand + dtab + wtab + 32;
 }
 
@@ -136,7 +136,10 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   const Tiling t = a.t;
   const int W = t.W;
   const int nx = a.nx, ny = a.ny, nm = a.nm, ng = a.ng, mq = a.mq;
-  const int g = blockIdx.x >> 2, q = blockIdx.x & 3;
+  const int h = blockIdx.x % t.NH, g = (blockIdx.x / t.NH) >> 2, q = (blockIdx.x / t.NH) & 3;
+  const int mqc = t.mqc;                           // chunk width (directions of the largest split)
+  const int mo = split_first(mq, t.NH, h);         // first quadrant-local direction of this split
+  const int mq_h = split_count(mq, t.NH, h);       // directions of this split
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int s = lane / R, r = lane % R;
   const int rho = warp * R + r;
@@ -145,26 +148,30 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   const int chunk = (int)a.chunk;
   const uint32_t stage_bytes = (uint32_t)(W * chunk * (int)sizeof(Real));
   // slices of the last direction block that hold a direction (all slices of the earlier blocks do)
-  const int s_last = mq - (D - 1) * S;
-  const int nl_last = R * s_last;
+  const int s_last = mq_h - (D - 1) * S;
+  const int nl_last = R * (mqc - (D - 1) * S);
 
   extern __shared__ __align__(128) unsigned char smem[];
   Real* ring = reinterpret_cast<Real*>(smem);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + (size_t)stages * stage_bytes);
   Real* hand = reinterpret_cast<Real*>(mbar + stages);
-  Real* dtab = hand + 2 * W * mq * 2;
+  Real* dtab = hand + 2 * W * mqc * 2;
   double* wtab = reinterpret_cast<double*>(
-      (reinterpret_cast<uintptr_t>(dtab + kNDirRow * mq) + 15) & ~static_cast<uintptr_t>(15));
+      (reinterpret_cast<uintptr_t>(dtab + kNDirRow * mqc) + 15) & ~static_cast<uintptr_t>(15));
 
-  for (int k = threadIdx.x; k < kNDirRow * mq; k += blockDim.x) {
-    Real v = a.dirtab[(size_t)q * kNDirRow * mq + k];
-    if (k < 2 * mq) v = v * Real(0.25);   // |Omega| / 4 for the corner-matrix geometry
+  // direction table of this split: row k of split-local direction ml at dtab[k * mqc + ml]
+  for (int k = threadIdx.x; k < kNDirRow * mqc; k += blockDim.x) {
+    const int row = k / mqc, col = k % mqc;
+    Real v = col < mq_h ? a.dirtab[((size_t)q * kNDirRow + row) * mq + mo + col] : Real(0);
+    if (row < 2) v = v * Real(0.25);   // |Omega| / 4 for the corner-matrix geometry
     dtab[k] = v;
   }
-  // moment weights w, w Ox^2, w Oy^2, w Ox Oy, w Ox, w Oy of the quadrant's directions, FP64
+  // moment weights w, w Ox^2, w Oy^2, w Ox Oy, w Ox, w Oy of the split's directions, FP64
   if constexpr (kLeanFP32) {
-    for (int k = threadIdx.x; k < 6 * mq; k += blockDim.x)
-      wtab[k] = a.dir64[(size_t)(kW + k / mq) * nm + q * mq + k % mq];
+    for (int k = threadIdx.x; k < 6 * mqc; k += blockDim.x) {
+      const int row = k / mqc, col = k % mqc;
+      wtab[k] = col < mq_h ? a.dir64[(size_t)(kW + row) * nm + q * mq + mo + col] : 0.0;
+    }
   }
   if (threadIdx.x == 0) {
     for (int k = 0; k < stages; ++k) mbar_init(&mbar[k], 1);
@@ -172,7 +179,7 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   }
   __syncthreads();
 
-  const long long blk_off = (long long)(g * 4 + q) * a.blk;
+  const long long blk_off = (long long)blockIdx.x * a.blk;
   const Real* gold = a.Iold + blk_off;
   Real* gnew = a.Inew + blk_off;
   const int Tsteps = t.Tsteps;
@@ -186,14 +193,14 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
 
   const Real rcdt = a.rcdt;
   const int nxy = nx * ny;
-  Real* wrapc = a.wrap + (size_t)blockIdx.x * nx * mq * 2;
-  double* partg = a.part + ((size_t)(q * ng + g) * nxy) * kNPart;
+  Real* wrapc = a.wrap + (size_t)blockIdx.x * nx * mqc * 2;
+  double* partg = a.part + ((size_t)((q * t.NH + h) * ng + g) * nxy) * kNPart;
   const int sideVin = fx ? 1 : 0, sideVout = fx ? 0 : 1;
   const int sideHin = fy ? 1 : 0, sideHout = fy ? 0 : 1;
-  const Real* bVin = a.bndV + ((size_t)(sideVin * ng + g) * nm + q * mq) * (2 * ny);
-  Real* bVout = a.bndV + ((size_t)(sideVout * ng + g) * nm + q * mq) * (2 * ny);
-  const Real* bHin = a.bndH + ((size_t)(sideHin * ng + g) * nm + q * mq) * (2 * nx);
-  Real* bHout = a.bndH + ((size_t)(sideHout * ng + g) * nm + q * mq) * (2 * nx);
+  const Real* bVin = a.bndV + ((size_t)(sideVin * ng + g) * nm + q * mq + mo) * (2 * ny);
+  Real* bVout = a.bndV + ((size_t)(sideVout * ng + g) * nm + q * mq + mo) * (2 * ny);
+  const Real* bHin = a.bndH + ((size_t)(sideHin * ng + g) * nm + q * mq + mo) * (2 * nx);
+  Real* bHout = a.bndH + ((size_t)(sideHout * ng + g) * nm + q * mq + mo) * (2 * nx);
   const Real* kapg = a.kap + (size_t)nxy * g;
   const Real* qisog = SRC_FULL ? nullptr : a.qiso + (size_t)nxy * g;
   const int byo = fy ? 1 : 0;   // physical corner-edge offset of the frame's bottom corner
@@ -250,8 +257,8 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
             hl[d] = bHin[ml * 2 * nx + 2 * in + bxo];
             hr[d] = bHin[ml * 2 * nx + 2 * in + 1 - bxo];
           } else {
-            hl[d] = wrapc[(ipn * mq + ml) * 2 + 0];
-            hr[d] = wrapc[(ipn * mq + ml) * 2 + 1];
+            hl[d] = wrapc[(ipn * mqc + ml) * 2 + 0];
+            hr[d] = wrapc[(ipn * mqc + ml) * 2 + 1];
           }
         }
       }
@@ -309,12 +316,12 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
                   o0 = bxo;
                   o1 = 1 - bxo;
                 } else {
-                  src = wrapc + (ip * mq + ml) * 2;
+                  src = wrapc + (ip * mqc + ml) * 2;
                   o0 = 0;
                   o1 = 1;
                 }
               } else {
-                src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mq + ml) * 2;
+                src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mqc + ml) * 2;
                 o0 = 0;
                 o1 = 1;
               }
@@ -350,7 +357,7 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   #pragma unroll
               for (int c = 0; c < 4; ++c) src[c] = tfma(io[c], rcdt, qs);
             }
-            const ScbGeom<Real> G = scb_geom(dtab[kAx * mq + ml], dtab[kAy * mq + ml], dx, dy);
+            const ScbGeom<Real> G = scb_geom(dtab[kAx * mqc + ml], dtab[kAy * mqc + ml], dx, dy);
             const Real gam = scb_gamma(G, kA4);
             Real x[4];
             scb_solve(G, gam, A4, src, vb[d], vt[d], hl[d], hr[d], x);
@@ -371,8 +378,8 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
             const Real Iavg = ((x[0] + x[1]) + (x[2] + x[3])) * Real(0.25);
             const Real Iv = (x[1] + x[2]) * Real(0.5);
             const Real Ih = (x[3] + x[2]) * Real(0.5);
-            const Real wxx = dtab[kWxx * mq + ml], wyy = dtab[kWyy * mq + ml], wxy = dtab[kWxy * mq + ml];
-            const Real ww = dtab[kW * mq + ml], wx = dtab[kWx * mq + ml], wy = dtab[kWy * mq + ml];
+            const Real wxx = dtab[kWxx * mqc + ml], wyy = dtab[kWyy * mqc + ml], wxy = dtab[kWxy * mqc + ml];
+            const Real ww = dtab[kW * mqc + ml], wx = dtab[kWx * mqc + ml], wy = dtab[kWy * mqc + ml];
             {
               acc[kCxx] = tfma(wxx, Iavg, acc[kCxx]);
               acc[kCyy] = tfma(wyy, Iavg, acc[kCyy]);
@@ -407,8 +414,8 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
                 bHout[ml * 2 * nx + 2 * i + 1 - bxo] = topR[d];
               }
               if (last_row) {
-                Real* dst = (warp < W - 1) ? hand + (((T & 1) * W + warp) * mq + ml) * 2
-                                           : wrapc + (ip * mq + ml) * 2;
+                Real* dst = (warp < W - 1) ? hand + (((T & 1) * W + warp) * mqc + ml) * 2
+                                           : wrapc + (ip * mqc + ml) * 2;
                 if (warp < W - 1 || t.nr > 1) {
                   dst[0] = topL[d];
                   dst[1] = topR[d];
@@ -455,8 +462,8 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
                 hl[d] = bHin[ml * 2 * nx + 2 * i + bxo];
                 hr[d] = bHin[ml * 2 * nx + 2 * i + 1 - bxo];
               } else {
-                hl[d] = wrapc[(ip * mq + ml) * 2 + 0];
-                hr[d] = wrapc[(ip * mq + ml) * 2 + 1];
+                hl[d] = wrapc[(ip * mqc + ml) * 2 + 0];
+                hr[d] = wrapc[(ip * mqc + ml) * 2 + 1];
               }
             }
           }
@@ -468,7 +475,7 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
         for (int d = 0; d < D; ++d) {
           const int ml = d * S + s;
           if (d < D - 1 || s < s_last) {
-            const Real* src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mq + ml) * 2;
+            const Real* src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mqc + ml) * 2;
             hl[d] = src[0];
             hr[d] = src[1];
           }
@@ -478,7 +485,7 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
       const bool right_edge = active && (ip == nx - 1);
       const bool top_edge = active && (jp == ny - 1);
       const bool last_row = active && (r == R - 1) && (warp < W - 1 || t.nr > 1);
-      Real* hand_dst = (warp < W - 1) ? hand + ((T & 1) * W + warp) * mq * 2 : wrapc + ip * mq * 2;
+      Real* hand_dst = (warp < W - 1) ? hand + ((T & 1) * W + warp) * mqc * 2 : wrapc + ip * mqc * 2;
 
   #pragma unroll
       for (int v = 0; v < 13; ++v) acc[v] = 0.0;
@@ -515,7 +522,7 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   #pragma unroll
           for (int c = 0; c < 4; ++c) src[c] = tfma(io[c], rcdt, qs);
         }
-        const ScbGeom<Real> G = scb_geom(dtab[kAx * mq + ml], dtab[kAy * mq + ml], dx, dy);
+        const ScbGeom<Real> G = scb_geom(dtab[kAx * mqc + ml], dtab[kAy * mqc + ml], dx, dy);
         const Real gam = scb_gamma(G, kA4);
         Real x[4];
         scb_solve(G, gam, A4, src, vb[d], vt[d], hl[d], hr[d], x);
@@ -556,8 +563,8 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
           const double Iavg = (double)(((x[0] + x[1]) + (x[2] + x[3])) * Real(0.25));
           const double Iv = (double)((x[1] + x[2]) * Real(0.5));
           const double Ih = (double)((x[3] + x[2]) * Real(0.5));
-          const double ww = wtab[0 * mq + ml], wxx = wtab[1 * mq + ml], wyy = wtab[2 * mq + ml];
-          const double wxy = wtab[3 * mq + ml], wx = wtab[4 * mq + ml], wy = wtab[5 * mq + ml];
+          const double ww = wtab[0 * mqc + ml], wxx = wtab[1 * mqc + ml], wyy = wtab[2 * mqc + ml];
+          const double wxy = wtab[3 * mqc + ml], wx = wtab[4 * mqc + ml], wy = wtab[5 * mqc + ml];
           acc[kCxx] = fma(wxx, Iavg, acc[kCxx]);
           acc[kCyy] = fma(wyy, Iavg, acc[kCyy]);
           acc[kCxy] = fma(wxy, Iavg, acc[kCxy]);

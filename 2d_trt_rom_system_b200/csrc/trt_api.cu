@@ -79,21 +79,23 @@ bool valid_shape(int nx, int ny, int nm, int ng) {
   return nx >= 1 && ny >= 1 && ng >= 1 && nm >= 4 && nm % 4 == 0 && nx < (1 << 20) && ny < (1 << 20);
 }
 
-// Compiled (slices, directions per lane) pairs of the sweep kernel; D is exact (ceil(mq / S)).
+// Compiled (slices, directions per lane) pairs of the sweep kernel; D is exact (ceil(ndir / S)) for
+// the ndir directions of a split.
 struct KernelCfg {
   int S, D;
 };
-const KernelCfg kCfgs[] = {{1, 2}, {2, 5}, {4, 3}, {4, 6}, {4, 9}, {8, 2}, {8, 3}, {8, 4}, {8, 5},
-                           {16, 1}, {16, 2}, {16, 3}, {32, 1}, {32, 2}};
+const KernelCfg kCfgs[] = {{1, 2}, {1, 4}, {2, 2}, {2, 3}, {2, 5}, {2, 9}, {4, 1}, {4, 2}, {4, 3}, {4, 5},
+                           {4, 6}, {4, 9}, {8, 1}, {8, 2}, {8, 3}, {8, 4}, {8, 5}, {16, 1}, {16, 2}, {16, 3},
+                           {32, 1}, {32, 2}};
 
-bool pick_cfg(int mq, int prec, int S_req, KernelCfg* out) {
+bool pick_cfg(int ndir, int prec, int S_req, KernelCfg* out) {
   bool found = false;
   KernelCfg best{0, 0};
   long best_key = 0;
   for (const KernelCfg& k : kCfgs) {
     if (S_req && k.S != S_req) continue;
-    if ((mq + k.S - 1) / k.S != k.D) continue;
-    const int waste = k.S * k.D - mq;
+    if ((ndir + k.S - 1) / k.S != k.D) continue;
+    const int waste = k.S * k.D - ndir;
     // FP64 keeps D <= 5 (registers); then least idle slots; then fewer slices (fewer shuffles)
     const int dpen = (prec == TRT_PREC_FP64 && k.D > 5) ? 1 : 0;
     const long key = (long)dpen * 1000000 + waste * 1000 + k.S;
@@ -124,10 +126,18 @@ cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int grid, int block
     return cudaGetLastError();                                                                   \
   }
   TRT_SWEEP_CASE(1, 2)
+  TRT_SWEEP_CASE(1, 4)
+  TRT_SWEEP_CASE(2, 2)
+  TRT_SWEEP_CASE(2, 3)
   TRT_SWEEP_CASE(2, 5)
+  TRT_SWEEP_CASE(2, 9)
+  TRT_SWEEP_CASE(4, 1)
+  TRT_SWEEP_CASE(4, 2)
   TRT_SWEEP_CASE(4, 3)
+  TRT_SWEEP_CASE(4, 5)
   TRT_SWEEP_CASE(4, 6)
   TRT_SWEEP_CASE(4, 9)
+  TRT_SWEEP_CASE(8, 1)
   TRT_SWEEP_CASE(8, 2)
   TRT_SWEEP_CASE(8, 3)
   TRT_SWEEP_CASE(8, 4)
@@ -149,7 +159,7 @@ struct trt_ctx {
   int nx = 0, ny = 0, nm = 0, ng = 0, mq = 0, prec = 0;
   size_t budget = 0, used = 0;
   cudaStream_t stream = nullptr;
-  int Wreq = 0, Sreq = 0, stages = 2;
+  int Wreq = 0, Sreq = 0, NHreq = 0, stages = 2;
   KernelCfg kc{8, 5};
   trt::Tiling t{};
   long long chunk = 0, blk = 0;
@@ -183,7 +193,7 @@ struct trt_ctx {
   unsigned wait_polls = kDefaultWaitPolls;
 
   size_t esz() const { return prec == TRT_PREC_FP64 ? sizeof(double) : sizeof(float); }
-  long long state_elems() const { return 4LL * ng * blk; }
+  long long state_elems() const { return 4LL * ng * t.NH * blk; }
   trt::Geo geo() const { return trt::Geo{nx, ny, nm, ng, mq, t, blk}; }
 
   int dalloc(void** p, size_t bytes) {
@@ -244,49 +254,115 @@ const char* kOutNames[kNOut] = {
     "E_in_L", "E_in_B", "E_in_R", "E_in_T", "F_in_L", "F_in_B", "F_in_R", "F_in_T",
     "Fyg_edgH_true", "Fy_edgH_true"};
 
-size_t layout_state_bytes(int nx, int ny, int mq, int ng, int W, int S, size_t esz) {
-  trt::Tiling t = trt::make_tiling(nx, ny, mq, W, S);
-  return (size_t)4 * ng * trt::block_elems(mq, t) * esz;
+size_t layout_state_bytes(int nx, int ny, int mq, int ng, int W, int S, int NH, size_t esz) {
+  trt::Tiling t = trt::make_tiling(nx, ny, mq, W, S, NH);
+  return (size_t)4 * ng * NH * trt::block_elems(t) * esz;
 }
 
-// Default warps per CTA: 8 (two CTAs of 256 threads fit an SM at <= 128 registers); measured best
-// for C1 in both precisions.  Fewer when a round would exceed the grid height by far.
-int default_W(int R, int ny) {
-  int W = 8;
+// Default tiling.  The grid has 4*ng*NH CTAs (NH = direction splits per quadrant) of W warps; every
+// CTA of one tiling does the same work, so the busiest SM sets the sweep time.  Candidates keep
+// 16 warps per SM resident at <= 128 registers: NH = 1, 2, 4 with W = 8, 4, 2.  The one whose
+// busiest SM carries the least work (ceil(CTAs / SMs) / NH) wins, ties to fewer splits.  C1
+// (50 groups): 200 CTAs put 2 on some SMs (1.48x the mean), 400 half-size CTAs put 3 halves
+// (1.11x the mean): NH = 2, measured 12% faster in FP64 and 11% in FP32.  Fewer warps when a
+// round would exceed the grid height by far.
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) ==
+                                                  cudaSuccess && v > 0)
+      n = v;
+    else {
+      cudaGetLastError();
+      n = 148;
+    }
+  }
+  return n;
+}
+
+int default_W(int R, int ny, int W = 8) {
   while (W > 1 && (W / 2) * R >= ny) W /= 2;
   return W;
 }
 
-// (Re)compute the tiling and (re)allocate the layout-dependent buffers.
+void default_split(int ng, int mq, int* NH, int* W) {
+  const int sms = sm_count();
+  *NH = 1;
+  *W = 8;
+  double best = 0.0;
+  for (int nh = 1; nh <= 4; nh *= 2) {
+    if (nh > 1 && mq < 4 * nh) break;   // at least 4 directions per split
+    const long long ctas = 4LL * ng * nh;
+    const double busiest = (double)((ctas + sms - 1) / sms) / nh;   // work of the busiest SM
+    const double load = (double)ctas / sms / nh / busiest;           // mean / busiest
+    if (load > best + 0.02) {
+      best = load;
+      *NH = nh;
+      *W = 8 / nh;
+    }
+  }
+}
+
+size_t part_bytes(const trt_ctx* c) {
+  return (size_t)4 * c->t.NH * c->ng * c->nx * c->ny * trt::kNPart * sizeof(double);
+}
+size_t wrap_bytes(const trt_ctx* c) { return (size_t)4 * c->ng * c->t.NH * c->nx * c->t.mqc * 2 * c->esz(); }
+
+// (Re)compute the tiling and (re)allocate the layout-dependent buffers (state, source, round wrap
+// buffer, moment partials).
 int setup_layout(trt_ctx* c) {
-  if (!pick_cfg(c->mq, c->prec, c->Sreq, &c->kc)) return c->Sreq ? TRT_ERR_ARG : TRT_ERR_UNSUPPORTED;
+  int NH = 1, Wdef = 8;
+  default_split(c->ng, c->mq, &NH, &Wdef);
+  if (c->NHreq) NH = c->NHreq;
+  if (NH < 1 || NH > c->mq) return TRT_ERR_ARG;
+  const int mqc = (c->mq + NH - 1) / NH;
+  if (!pick_cfg(mqc, c->prec, c->Sreq, &c->kc)) return c->Sreq ? TRT_ERR_ARG : TRT_ERR_UNSUPPORTED;
   const int R = 32 / c->kc.S;
-  const int W = c->Wreq ? c->Wreq : default_W(R, c->ny);
-  c->t = trt::make_tiling(c->nx, c->ny, c->mq, W, c->kc.S);
-  c->chunk = trt::chunk_elems(c->mq, c->t);
-  c->blk = trt::block_elems(c->mq, c->t);
-  // pipeline depth limited by shared memory
+  const int W = c->Wreq ? c->Wreq : default_W(R, c->ny, c->NHreq ? std::max(1, 8 / NH) : Wdef);
   const size_t esz = c->esz();
+  // sizes of the current buffers (t still describes them)
+  const size_t sbytes_old = c->blk ? (size_t)c->state_elems() * esz : 0;
+  const size_t src_old = sbytes_old;
+  const size_t wrap_old = c->blk ? wrap_bytes(c) : 0, part_old = c->blk ? part_bytes(c) : 0;
+  const trt::Tiling t = trt::make_tiling(c->nx, c->ny, c->mq, W, c->kc.S, NH);
+  // pipeline depth limited by shared memory
+  const long long chunk = trt::chunk_elems(t);
   auto smem_at = [&](int st) {
-    return c->prec == TRT_PREC_FP64 ? trt::sweep_smem_bytes<double>(W, c->chunk, st, c->mq, c->t.D)
-                                    : trt::sweep_smem_bytes<float>(W, c->chunk, st, c->mq, c->t.D);
+    return c->prec == TRT_PREC_FP64 ? trt::sweep_smem_bytes<double>(W, chunk, st, t.mqc, t.D)
+                                    : trt::sweep_smem_bytes<float>(W, chunk, st, t.mqc, t.D);
   };
-  while (c->stages > 1 && smem_at(c->stages) > (size_t)200 * 1024) c->stages--;
-  if (smem_at(c->stages) > (size_t)220 * 1024) return TRT_ERR_ARG;   // tiling does not fit an SM
-  const size_t sbytes = (size_t)c->state_elems() * esz;
+  int stages = c->stages;
+  while (stages > 1 && smem_at(stages) > (size_t)200 * 1024) stages--;
+  if (smem_at(stages) > (size_t)220 * 1024) return TRT_ERR_ARG;   // tiling does not fit an SM
   for (int k = 0; k < 2; ++k) {
-    if (c->d_state[k]) c->dfree(c->d_state[k], sbytes);
+    c->dfree(c->d_state[k], sbytes_old);
     c->d_state[k] = nullptr;
   }
-  if (c->d_srcfull) c->dfree(c->d_srcfull, sbytes), c->d_srcfull = nullptr;
+  c->dfree(c->d_srcfull, src_old);
+  c->d_srcfull = nullptr;
+  c->dfree(c->d_wrap, wrap_old);
+  c->d_wrap = nullptr;
+  c->dfree(c->d_part, part_old);
+  c->d_part = nullptr;
   c->use_srcfull = false;
+  c->have_state = false;
+  c->swept = false;
+  c->have_moments = false;
+  c->stages = stages;
+  c->t = t;
+  c->chunk = chunk;
+  c->blk = trt::block_elems(t);
+  const size_t sbytes = (size_t)c->state_elems() * esz;
   for (int k = 0; k < 2; ++k) {
     int rc = c->dalloc(&c->d_state[k], sbytes);
     if (rc) return rc;
     TRT_CUDA(cudaMemsetAsync(c->d_state[k], 0, sbytes, c->stream));
   }
-  c->have_state = false;
-  c->swept = false;
+  int rc = c->dalloc(&c->d_wrap, wrap_bytes(c));
+  if (rc) return rc;
+  if ((rc = alloc_t(c, &c->d_part, part_bytes(c) / sizeof(double)))) return rc;
+  TRT_CUDA(cudaMemsetAsync(c->d_part, 0, part_bytes(c), c->stream));
   return TRT_OK;
 }
 
@@ -338,8 +414,8 @@ int pack_corner_array(trt_ctx* c, const double* host, void* dst) {
     TRT_CUDA(cudaMemcpyAsync(c->d_stage, host + slab * g, slab * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     trt::Geo Gg = G;
     Gg.ng = 1;
-    // pack one group: shift the skewed base to group g (block index g*4 + q)
-    Real* base = static_cast<Real*>(dst) + (long long)g * 4 * c->blk;
+    // pack one group: shift the skewed base to group g (block index (g*4 + q)*NH + h)
+    Real* base = static_cast<Real*>(dst) + (long long)g * 4 * c->t.NH * c->blk;
     trt::pack_state_kernel<Real><<<grid_for(slab), 256, 0, c->stream>>>(Gg, c->d_stage, base);
     TRT_LAUNCHED();
     TRT_CUDA(cudaGetLastError());
@@ -357,7 +433,7 @@ int unpack_corner_array(trt_ctx* c, const void* src, double* host) {
   for (int g = 0; g < c->ng; ++g) {
     trt::Geo Gg = G;
     Gg.ng = 1;
-    const Real* base = static_cast<const Real*>(src) + (long long)g * 4 * c->blk;
+    const Real* base = static_cast<const Real*>(src) + (long long)g * 4 * c->t.NH * c->blk;
     trt::unpack_state_kernel<Real><<<grid_for(slab), 256, 0, c->stream>>>(Gg, base, c->d_stage);
     TRT_LAUNCHED();
     TRT_CUDA(cudaGetLastError());
@@ -405,15 +481,15 @@ int sweep_impl(trt_ctx* c, unsigned flags) {
   a.err = c->d_err;
   a.max_polls = c->wait_polls;
   a.drain_polls = 1u << 24;
-  const size_t smem = trt::sweep_smem_bytes<Real>(c->t.W, c->chunk, c->stages, c->mq, c->t.D);
-  cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, 4 * c->ng, 32 * c->t.W, smem, c->stream, a);
+  const size_t smem = trt::sweep_smem_bytes<Real>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D);
+  cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, 4 * c->ng * c->t.NH, 32 * c->t.W, smem, c->stream, a);
   TRT_LAUNCHED();
   if (e != cudaSuccess) return TRT_ERR_CUDA;
   c->swept = true;
 
   if (flags & TRT_MOMENTS) {
     trt::CombineArgs A{};
-    A.nx = c->nx; A.ny = c->ny; A.nm = c->nm; A.ng = c->ng; A.mq = c->mq;
+    A.nx = c->nx; A.ny = c->ny; A.nm = c->nm; A.ng = c->ng; A.mq = c->mq; A.nh = c->t.NH;
     A.eps = 1e-25 / c->comp_unit;
     A.c = c->c;
     for (int k = 0; k < 4; ++k) A.bc[k] = c->bc[k];
@@ -647,9 +723,6 @@ int create_buffers(trt_ctx* c) {
     return rc;
   TRT_CUDA(cudaMemset(c->d_bndV, 0, (size_t)2 * ng * nm * 2 * ny * esz));
   TRT_CUDA(cudaMemset(c->d_bndH, 0, (size_t)2 * ng * nm * 2 * nx * esz));
-  if ((rc = c->dalloc(&c->d_wrap, (size_t)4 * ng * nx * c->mq * 2 * esz))) return rc;
-  if ((rc = alloc_t(c, &c->d_part, (size_t)4 * ng * nx * ny * trt::kNPart))) return rc;
-  TRT_CUDA(cudaMemset(c->d_part, 0, (size_t)4 * ng * nx * ny * trt::kNPart * sizeof(double)));
   if ((rc = alloc_t(c, &c->d_err, 1))) return rc;
   TRT_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
   if ((rc = alloc_t(c, &c->d_bval, (size_t)4 * ng))) return rc;
@@ -685,7 +758,7 @@ int transport_scb_impl(trt_ctx* c, int nx, int ny, int nm, int ng, double* I_avg
   c->dt = Delt;
   c->have_material = true;
   if ((rc = pack_corner_array<double>(c, I_crn_old, c->d_state[c->cur]))) return rc;
-  if (!c->d_srcfull && (rc = c->dalloc(&c->d_srcfull, (size_t)c->state_elems() * sizeof(double)))) return rc;
+  if (!c->d_srcfull && (rc = c->dalloc(&c->d_srcfull, (size_t)c->state_elems() * c->esz()))) return rc;
   if ((rc = pack_corner_array<double>(c, Src_in, c->d_srcfull))) return rc;
   c->use_srcfull = true;
   if ((rc = set_boundary_impl<double>(c, Ic_edgV, Ic_edgH))) return rc;
@@ -818,13 +891,17 @@ size_t trt_required_bytes(int n_x, int n_y, int n_m, int n_g, int precision) {
   KernelCfg kc;
   if (!pick_cfg(mq, precision, 0, &kc)) return 0;
   const size_t esz = precision == TRT_PREC_FP64 ? 8 : 4;
-  const int W = default_W(32 / kc.S, n_y);
-  size_t b = 2 * layout_state_bytes(n_x, n_y, mq, n_g, W, kc.S, esz);
+  int NH = 1, W = 8;
+  default_split(n_g, mq, &NH, &W);
+  if (!pick_cfg((mq + NH - 1) / NH, precision, 0, &kc)) return 0;
+  W = default_W(32 / kc.S, n_y, W);
+  const int mqc = (mq + NH - 1) / NH;
+  size_t b = 2 * layout_state_bytes(n_x, n_y, mq, n_g, W, kc.S, NH, esz);   // I_crn_old, I_crn
   const size_t ncell = (size_t)n_x * n_y * n_g;
   b += ncell * (16 + 2 * esz);
   b += (size_t)2 * n_g * n_m * 2 * (n_x + n_y) * esz;
-  b += (size_t)4 * n_g * n_x * mq * 2 * esz;
-  b += (size_t)4 * n_g * n_x * n_y * trt::kNPart * 8;
+  b += (size_t)4 * n_g * NH * n_x * mqc * 2 * esz;
+  b += (size_t)4 * NH * n_g * n_x * n_y * trt::kNPart * 8;
   long long sz[kNOut];
   output_sizes(n_x, n_y, n_g, sz);
   for (int k = 0; k < kNOut; ++k) b += sz[k] * 8;
@@ -881,22 +958,24 @@ void trt_destroy(trt_ctx* c) {
   delete c;
 }
 
-int trt_set_tiling(trt_ctx* c, int warps_per_cta, int slices, int stages) {
+int trt_set_tiling(trt_ctx* c, int warps_per_cta, int slices, int stages, int splits) {
   if (!c || warps_per_cta < 0 || warps_per_cta > 16 || stages < 0 || stages > 4) return TRT_ERR_ARG;
   if (slices && (slices & (slices - 1))) return TRT_ERR_ARG;
-  if (slices > 32) return TRT_ERR_ARG;
+  if (slices > 32 || splits < 0 || splits > c->mq) return TRT_ERR_ARG;
   c->Wreq = warps_per_cta;
   c->Sreq = slices;
+  c->NHreq = splits;
   c->stages = stages ? stages : 2;
   return setup_layout(c);
 }
 
-int trt_get_tiling(const trt_ctx* c, int* W, int* S, int* D, int* stages) {
+int trt_get_tiling(const trt_ctx* c, int* W, int* S, int* D, int* stages, int* splits) {
   if (!c) return TRT_ERR_ARG;
   if (W) *W = c->t.W;
   if (S) *S = c->t.S;
   if (D) *D = c->t.D;
   if (stages) *stages = c->stages;
+  if (splits) *splits = c->t.NH;
   return TRT_OK;
 }
 

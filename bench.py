@@ -39,15 +39,15 @@ sys.path.insert(0, ROOT)
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default="C1", choices=["C0", "C1"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
-    p.add_argument("--tiling", default="", help="warps,slices,stages override for both precisions")
+    p.add_argument("--tiling", default="", help="warps,slices,stages[,splits] override for both precisions")
     p.add_argument("--profile", default="", choices=["", "fp64", "fp32"],
-                   help="only run --warmup + --steps sweeps (no moments) of one precision, for ncu")
+                   help="only run --warmup + --steps steps (roll + sweep + moments) of one precision, for ncu")
     p.add_argument("--n", type=int, default=0, help="grid size override (profiling small cases)")
     p.add_argument("--groups", type=int, default=0, help="group count override (profiling small cases)")
     p.add_argument("--tiling-sweep", action="store_true", help="time the sweep kernel over a set of tilings")
@@ -86,31 +86,49 @@ class ClockSampler:
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, period_ms=50):
         self.index = index
+        self.period_ms = period_ms
         self.samples = []
-        self._stop = threading.Event()
+        self._proc = None
         self._t = None
+        self._first = threading.Event()
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                if out.returncode == 0:
-                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [x.strip() for x in line.strip().split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+                self._first.set()
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+        """Start one nvidia-smi in loop mode; return once it has delivered its first sample."""
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                           "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self._proc = None
+            return self
+        self._t = threading.Thread(target=self._read, daemon=True)
         self._t.start()
+        self._first.wait(10)
+        self._n0 = len(self.samples)
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._proc is None:
+            return
+        # keep only the samples taken while the timed region ran (plus the last one before it)
+        n1 = len(self.samples)
+        self._proc.terminate()
+        try:
+            self._proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self._proc.kill()
+            self._proc.wait(5)
+        self._t.join(timeout=5)
+        self.samples = self.samples[max(0, self._n0 - 1):max(n1, self._n0)]
 
     def summary(self):
         if not self.samples:
@@ -141,7 +159,7 @@ def run_profile(args):
     tiling = tuple(int(x) for x in args.tiling.split(",")) if args.tiling else None
     s, _, _ = setup_instance(pkg, prob, "mixed" if args.profile == "fp32" else "fp64", tiling)
     try:
-        ms, n = time_resident(pkg, torch, s, args.steps, args.warmup, 0)
+        ms, n = time_resident(pkg, torch, s, args.steps, args.warmup, pkg._lib.TRT_ROLL_STATE | pkg._lib.TRT_MOMENTS)
         print(json.dumps({"profile": args.profile, "workload": f"{prob.nx}x{prob.ny} G={prob.ng} {prob.quad}",
                           "ms_per_sweep": ms, "tiling": s.tiling(), "launches": n}))
     finally:
@@ -157,20 +175,31 @@ def run_tiling_sweep(args):
     peak, _ = peaks()
     for prec in ("fp64", "fp32"):
         s, _, _ = setup_instance(pkg, prob, "mixed" if prec == "fp32" else "fp64", None)
+        seen = set()
         try:
-            for W in (4, 6, 8, 12, 16):
-                for S in (0, 4, 8, 16):
-                    for st in (2, 3):
-                        try:
-                            s.set_tiling(W, S, st)
-                        except pkg.TrtError:
-                            continue
-                        s.init_state(prob.T0 * 1e3, [t * 1e3 for t in prob.bcT], pkg.problems.COMP_UNIT, prob.nu_eV)
-                        ms, _ = time_resident(pkg, torch, s, 5, 1, 0)
-                        B = bytes_per_update(prob.nm, prec)
-                        print(json.dumps({"prec": prec, "tiling": s.tiling(), "kernel_ms": ms,
-                                          "gupd_s": upd / ms / 1e6, "frac": upd * B / (ms * 1e-3) / 1e9 / peak}),
-                              flush=True)
+            for NH in (1, 2, 3, 4):
+                for W in (2, 4, 6, 8, 12, 16):
+                    for S in (0, 2, 4, 8, 16):
+                        for st in (2, 3):
+                            try:
+                                s.set_tiling(W, S, st, NH)
+                            except pkg.TrtError:
+                                continue
+                            tl = s.tiling()
+                            key = tuple(sorted(tl.items()))
+                            if key in seen:
+                                continue
+                            seen.add(key)
+                            s.init_state(prob.T0 * 1e3, [t * 1e3 for t in prob.bcT], pkg.problems.COMP_UNIT,
+                                         prob.nu_eV)
+                            try:
+                                ms, _ = time_resident(pkg, torch, s, 5, 1, 0)
+                            except pkg.TrtError as e:
+                                print(json.dumps({"prec": prec, "tiling": tl, "error": str(e)}), flush=True)
+                                continue
+                            B = bytes_per_update(prob.nm, prec)
+                            print(json.dumps({"prec": prec, "tiling": tl, "kernel_ms": ms, "gupd_s": upd / ms / 1e6,
+                                              "frac": upd * B / (ms * 1e-3) / 1e9 / peak}), flush=True)
         finally:
             s.close()
     return 0
@@ -194,14 +223,14 @@ def time_resident(pkg, torch, s, steps, warmup, flags):
     L = pkg.lib()
     stream = torch.cuda.ExternalStream(s.stream())
     for _ in range(warmup):
-        assert L.trt_sweep(s.handle, flags) == 0
+        pkg.check(L.trt_sweep(s.handle, flags), "trt_sweep")
     s.sync()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     n0 = pkg.kernel_launches()
     e0.record(stream)
     for _ in range(steps):
-        assert L.trt_sweep(s.handle, flags) == 0
+        pkg.check(L.trt_sweep(s.handle, flags), "trt_sweep")
     e1.record(stream)
     s.sync()
     n1 = pkg.kernel_launches()

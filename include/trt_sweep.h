@@ -143,13 +143,18 @@ trt_ctx* trt_create(int n_x, int n_y, int n_m, int n_g, const double* Omega_x, c
                     size_t hbm_budget, int* status);
 void trt_destroy(trt_ctx* ctx);
 
-/* Device bytes a handle of this shape would allocate (for admission against a budget). */
+/* Device bytes a handle of this shape would allocate with the default tiling (for admission against
+ * a budget).  A full corner source (trt_set_source_full, TRANSPORT_SCB) adds one more state-sized array. */
 size_t trt_required_bytes(int n_x, int n_y, int n_m, int n_g, int precision);
 
-/* Kernel tiling: warps per CTA (1..16), direction slices per warp (1,2,4,8,16,32; 0 = automatic),
- * TMA pipeline stages (1..4).  Re-lays out the resident state. */
-int trt_set_tiling(trt_ctx* ctx, int warps_per_cta, int slices, int stages);
-int trt_get_tiling(const trt_ctx* ctx, int* warps_per_cta, int* slices, int* dirs_per_lane, int* stages);
+/* Kernel tiling: warps per CTA (1..16), direction slices per warp (1,2,4,8,16,32), TMA pipeline
+ * stages (1..4) and direction splits per quadrant (CTAs per (group, quadrant), 1..n_m/4); 0 selects
+ * the default for each.  Re-lays out the resident state (zeroed: put it again afterwards).  Sweep
+ * results do not depend on warps, slices or stages; the moment sums are added in a different order
+ * when the number of splits changes (last-bit differences). */
+int trt_set_tiling(trt_ctx* ctx, int warps_per_cta, int slices, int stages, int splits);
+int trt_get_tiling(const trt_ctx* ctx, int* warps_per_cta, int* slices, int* dirs_per_lane, int* stages,
+                   int* splits);
 
 /* Material for the next sweeps: KapE_in(n_x,n_y,n_g) (the opacity before the 1/(c*Delt) term of
  * TRANSPORT_SOLVES.f08:47) and the isotropic corner source src_iso(n_x,n_y,n_g) = KapB*Bg

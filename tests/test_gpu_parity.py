@@ -152,6 +152,52 @@ def test_direction_slicing_variants(oracle, slices):
     assert rel_err_per_group(m["Eg_avg"], ref["Eg_avg"]) < 1e-13
 
 
+@pytest.mark.parametrize("splits,slices", [(2, 0), (3, 0), (3, 2), (4, 0), (5, 0), (10, 0)])
+def test_direction_splits(oracle, splits, slices):
+    """Each quadrant's 10 directions split over several CTAs (ragged splits included): the state is
+    unchanged bit for bit, the moments only change in the order the split partials are added."""
+    prob = pkg.problems.random_small(12, 13, 11, 2, "S8")
+    d = sweep_inputs(prob, seed=12)
+    ref = oracle_full(d, solver=1)
+    with resident(d, tiling=dict(splits=splits, slices=slices)) as s:
+        assert s.tiling()["splits"] == splits
+        s.sweep(moments=True)
+        I = s.get_state()
+        m = s.moments()
+        ang = s.angular()
+    assert np.array_equal(I, ref["I_crn"])
+    for k in ("I_avg", "I_edgV", "I_edgH"):
+        assert np.array_equal(ang[k], ref[k]), k
+    for k in MOM_KEYS:
+        assert moment_err(m, ref, k) < 1e-13, k
+    for k in BND_KEYS:
+        assert rel_err(m[k], ref[k]) < 1e-13 or np.max(np.abs(m[k] - ref[k])) < 1e-300, k
+
+
+def test_direction_splits_fp32_state_unchanged():
+    prob = pkg.problems.random_small(13, 17, 19, 2, "S12")
+    d = sweep_inputs(prob, seed=13)
+    out = []
+    for splits in (1, 2, 7):
+        with resident(d, precision="fp32", tiling=dict(splits=splits)) as s:
+            s.sweep(moments=True)
+            out.append((s.get_state(), s.moments(["Eg_avg", "Fxg_edgV"])))
+    for I, m in out[1:]:
+        assert np.array_equal(I, out[0][0])
+        for k in m:
+            assert rel_err_per_group(m[k], out[0][1][k]) < 1e-14, k
+
+
+def test_split_count_limits():
+    prob = pkg.problems.random_small(14, 4, 4, 1, "S8")
+    d = sweep_inputs(prob, seed=14)
+    with resident(d) as s:
+        with pytest.raises(pkg.TrtError):
+            s.set_tiling(splits=11)          # more splits than directions per quadrant
+        s.set_tiling(splits=10)
+        assert s.tiling()["splits"] == 10
+
+
 def test_multi_step_state_roll(oracle):
     """Three time steps: I_crn_old <- I_crn between steps (ALGORITHMS.f08:397), with a new material each step."""
     prob = pkg.problems.random_small(10, 11, 9, 3, "S8")

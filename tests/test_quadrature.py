@@ -50,7 +50,7 @@ def test_reference_sets_match_inputs_f08():
     num = r"[-+]?\d*\.\d+d[-+]?\d+|[-+]?\d*\.?\d+d0"
     for name in ("abu36", "abu20"):
         # the table follows the last test of the name (the first one only sets N_m)
-        at = max(m.start() for m in re.finditer(r"IF\s*\(quadrature \.EQ\. '" + name + "'\)", block))
+        at = max(m.start() for m in re.finditer(r"IF\s*\(quadrature \.EQ\. '" + name + r"'\)", block))
         seg = block[at:]
         lists = re.findall(r"\(/(.*?)/\)", seg, flags=re.S)[:3]
         vals = [np.array([float(x.replace("d", "e")) for x in re.findall(num, L)]) for L in lists]
