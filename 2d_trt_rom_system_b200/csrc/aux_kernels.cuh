@@ -214,7 +214,7 @@ struct CombineArgs {
   int bc[4];           // BC_Type L, B, R, T
   int nh;              // direction splits per quadrant (partials per quadrant)
   WeightSums ws;
-  const double* part;  // [4*nh][ng][ny][nx][kNPart]
+  const double* part;  // [4*nh][ng][ny][nx][kNPart] partial records
   const double* dir;   // [kNDirRow][nm] full direction table (physical), double
 };
 
@@ -231,76 +231,176 @@ __device__ __forceinline__ void inflow_face_sums(const CombineArgs& A, const Rea
   }
 }
 
-template <class Real>
-__global__ void combine_kernel(CombineArgs A, const Real* __restrict__ bndV, const Real* __restrict__ bndH,
-                               MomentOut O) {
-  const int nx = A.nx, ny = A.ny, ng = A.ng;
-  const long long nA = (long long)nx * ny * ng, nV = (long long)(nx + 1) * ny * ng, nH = (long long)nx * (ny + 1) * ng;
-  const long long nxy = (long long)nx * ny;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  const long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const double eps = A.eps, c = A.c;
-  // partial of quadrant q, direction split h
-  auto P = [&](int qh, int g, int i, int j) { return A.part + (((size_t)(qh * ng + g) * ny + j) * nx + i) * kNPart; };
-  const int NH = A.nh;
-  auto wsum = [&](int v) { return A.ws.s[0][v] + A.ws.s[1][v] + A.ws.s[2][v] + A.ws.s[3][v]; };
+// Moment epilogue, interior part.  A CTA takes a tile of kCombTX x kCombTY cells of one group; for
+// each (quadrant q, split h) in turn it stages the tile's partial records, plus the column on its
+// left (q = 0, 3) or the row below it (q = 0, 1) where a face needs them, into shared memory with
+// coalesced 16-byte cp.async copies (double-buffered: the copies of the next (q, h) fly while this
+// one is added), then every thread adds the record slots of its cell (i, j) to
+//   * the cell-centre moments (COLLAPSE_INTENSITIES :446-449, fg_Calc :63-65),
+//   * the vertical face f = i when i >= 1 (:450-452, :458; fg_Calc :66-67),
+//   * the horizontal face f = j when j >= 1 (:453-455, :469; fg_Calc :68-69).
+// The boundary faces (f = 0, nx and f = 0, ny) are left to combine_boundary_kernel.  Each sum adds
+// the quadrant partials in the order q = 0..3, split h = 0..NH-1 inside, then the analytic eps term.
+constexpr int kCombTX = 32, kCombTY = 8;
+constexpr int kCombRow = kCombTX + 1;                                 // records per staged row
+constexpr size_t kCombSmem = 2 * (size_t)(kCombTY + 1) * kCombRow * kNPart * sizeof(double);   // double buffer
 
-  // cell centres
-  for (long long k = k0; k < nA; k += stride) {
-    const int i = (int)(k % nx), j = (int)((k / nx) % ny), g = (int)(k / nxy);
-    double xx = 0, yy = 0, xy = 0, e = 0;
-    for (int qh = 0; qh < 4 * NH; ++qh) {
-      const double* p = P(qh, g, i, j);
-      xx += p[kCxx]; yy += p[kCyy]; xy += p[kCxy]; e += p[kCe];
+__global__ void __launch_bounds__(kCombTX * kCombTY) combine_cells_kernel(CombineArgs A, MomentOut O) {
+  // two staging buffers [kCombTY + 1][kCombRow][kNPart]; row 0 / column 0 = halo
+  extern __shared__ __align__(16) double rec[];
+  const int nx = A.nx, ny = A.ny, ng = A.ng, NH = A.nh;
+  const int tx = threadIdx.x % kCombTX, ty = threadIdx.x / kCombTX;
+  const int i0 = blockIdx.x * kCombTX, j0 = blockIdx.y * kCombTY, g = blockIdx.z;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool in = i < nx && j < ny;
+  const int ncol = min(kCombTX, nx - i0), nrow = min(kCombTY, ny - j0);
+  const double eps = A.eps, c = A.c;
+  auto wsum = [&](int v) { return A.ws.s[0][v] + A.ws.s[1][v] + A.ws.s[2][v] + A.ws.s[3][v]; };
+  constexpr int kV2 = kNPart / 2;                      // 16-byte vectors per record
+  constexpr size_t kBuf = (size_t)(kCombTY + 1) * kCombRow * kNPart;
+
+  // issue the copies of (q, h) = qh into buffer b (asynchronous, one commit group)
+  auto stage = [&](int qh, int b) {
+    const int q = qh / NH;
+    const bool left_halo = (q == 0 || q == 3) && i0 > 0;   // vertical faces take cell i - 1
+    const bool low_halo = (q == 0 || q == 1) && j0 > 0;    // horizontal faces take cell j - 1
+    const int c0 = left_halo ? 0 : 1, r0 = low_halo ? 0 : 1;
+    const int rowlen = (ncol + 1 - c0) * kV2;              // vectors per staged row
+    const int nvec = (nrow + 1 - r0) * rowlen;
+    const double2* src = reinterpret_cast<const double2*>(A.part + ((size_t)(qh * ng + g) * ny * nx) * kNPart);
+    double2* dst = reinterpret_cast<double2*>(rec + b * kBuf);
+    for (int v = threadIdx.x; v < nvec; v += kCombTX * kCombTY) {
+      const int rr = r0 + v / rowlen, e = v % rowlen;      // staged row, vector within the row
+      cp_async16(dst + (rr * kCombRow + c0) * kV2 + e, src + ((size_t)(j0 - 1 + rr) * nx + (i0 - 1 + c0)) * kV2 + e);
     }
-    xx += eps * wsum(kWxx); yy += eps * wsum(kWyy); xy += eps * wsum(kWxy); e += eps * wsum(kW);
-    const double Eg = e / kCLight;
-    if (O.Hg_avg_xx) { O.Hg_avg_xx[k] = xx; O.Hg_avg_yy[k] = yy; O.Hg_avg_xy[k] = xy; }
+    cp_async_commit();
+  };
+
+  double cxx = 0, cyy = 0, cxy = 0, ce = 0;            // centre
+  double vxx = 0, vxy = 0, vx = 0, ve = 0;             // vertical face f = i
+  double hyy = 0, hxy = 0, hy = 0, hx = 0, he = 0;     // horizontal face f = j
+  const int nqh = 4 * NH;
+  stage(0, 0);
+  for (int qh = 0; qh < nqh; ++qh) {
+    const int q = qh / NH;
+    if (qh + 1 < nqh) {
+      stage(qh + 1, (qh + 1) & 1);   // that buffer was released by the barrier ending step qh - 1
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    if (in) {
+      const double* own = rec + (qh & 1) * kBuf + ((size_t)(ty + 1) * kCombRow + tx + 1) * kNPart;
+      const double2 a01 = *reinterpret_cast<const double2*>(own + kCxx);
+      const double2 a23 = *reinterpret_cast<const double2*>(own + kCxy);
+      cxx += a01.x; cyy += a01.y; cxy += a23.x; ce += a23.y;
+      const double* pv = (q == 0 || q == 3) ? own - kNPart : own;
+      const double2 v01 = *reinterpret_cast<const double2*>(pv + kVxx);
+      const double2 v23 = *reinterpret_cast<const double2*>(pv + kVx);
+      vxx += v01.x; vxy += v01.y; vx += v23.x; ve += v23.y;
+      const double* ph = (q == 0 || q == 1) ? own - (size_t)kCombRow * kNPart : own;
+      const double2 h01 = *reinterpret_cast<const double2*>(ph + kHyy);
+      const double2 h23 = *reinterpret_cast<const double2*>(ph + kHy);
+      hyy += h01.x; hxy += h01.y; hy += h23.x; hx += h23.y; he += ph[kHe];
+    }
+    __syncthreads();   // buffer qh & 1 is consumed
+  }
+  if (!in) return;
+  const long long k = i + (long long)nx * (j + (long long)ny * g);
+  {
+    cxx += eps * wsum(kWxx); cyy += eps * wsum(kWyy); cxy += eps * wsum(kWxy); ce += eps * wsum(kW);
+    const double Eg = ce / kCLight;
+    if (O.Hg_avg_xx) { O.Hg_avg_xx[k] = cxx; O.Hg_avg_yy[k] = cyy; O.Hg_avg_xy[k] = cxy; }
     if (O.Eg_avg) O.Eg_avg[k] = Eg;
     if (O.fg_avg_xx) {
-      O.fg_avg_xx[k] = xx / (c * Eg);
-      O.fg_avg_yy[k] = yy / (c * Eg);
-      O.fg_avg_xy[k] = xy / (c * Eg);
+      O.fg_avg_xx[k] = cxx / (c * Eg);
+      O.fg_avg_yy[k] = cyy / (c * Eg);
+      O.fg_avg_xy[k] = cxy / (c * Eg);
     }
   }
-  // vertical faces f = 0..nx
-  for (long long k = k0; k < nV; k += stride) {
-    const int f = (int)(k % (nx + 1)), j = (int)((k / (nx + 1)) % ny), g = (int)(k / ((long long)(nx + 1) * ny));
-    double xx = 0, xy = 0, fxs = 0, e = 0;
-    double outF = 0, outE = 0;     // outgoing sums on a boundary face (Cg)
-    double inF = 0, inE = 0;       // incoming sums on a boundary face (MGQD_In_Calc)
-    for (int q = 0; q < 4; ++q) {
-      const bool xpos = (q == 0 || q == 3);
-      const int cell = xpos ? f - 1 : f;     // upwind cell of this face for quadrant q
-      if (cell >= 0 && cell < nx) {
-        for (int h = 0; h < NH; ++h) {
-          const double* p = P(q * NH + h, g, cell, j);
-          xx += p[kVxx]; xy += p[kVxy]; fxs += p[kVx]; e += p[kVe];
-          if (f == 0 || f == nx) { outF += p[kVx]; outE += p[kVe]; }
+  if (i >= 1) {
+    vxx += eps * wsum(kWxx); vxy += eps * wsum(kWxy); vx += eps * wsum(kWx); ve += eps * wsum(kW);
+    const double Eg = ve / kCLight;
+    const long long kv = i + (long long)(nx + 1) * (j + (long long)ny * g);
+    if (O.Hg_edgV_xx) { O.Hg_edgV_xx[kv] = vxx; O.Hg_edgV_xy[kv] = vxy; }
+    if (O.Eg_edgV) O.Eg_edgV[kv] = Eg;
+    if (O.Fxg_edgV) O.Fxg_edgV[kv] = vx;
+    if (O.fg_edgV_xx) { O.fg_edgV_xx[kv] = vxx / (c * Eg); O.fg_edgV_xy[kv] = vxy / (c * Eg); }
+  }
+  if (j >= 1) {
+    hyy += eps * wsum(kWyy); hxy += eps * wsum(kWxy); hy += eps * wsum(kWy); hx += eps * wsum(kWx);
+    he += eps * wsum(kW);
+    const double Eg = he / kCLight;
+    const long long kh = i + (long long)nx * (j + (long long)(ny + 1) * g);
+    if (O.Hg_edgH_yy) { O.Hg_edgH_yy[kh] = hyy; O.Hg_edgH_xy[kh] = hxy; }
+    if (O.Eg_edgH) O.Eg_edgH[kh] = Eg;
+    if (O.Fyg_edgH) O.Fyg_edgH[kh] = hx;           // Omega_x weighted, as TRANSPORT_SOLVES.f08:469
+    if (O.Fyg_edgH_true) O.Fyg_edgH_true[kh] = hy;
+    if (O.fg_edgH_yy) { O.fg_edgH_yy[kh] = hyy / (c * Eg); O.fg_edgH_xy[kh] = hxy / (c * Eg); }
+  }
+}
+
+// Moment epilogue, boundary faces: one thread per face of the four domain edges (vertical faces
+// f = 0, nx; horizontal faces f = 0, ny).  Outgoing quadrants add their partials (and give Cg,
+// Cg_Calc :156-203); incoming quadrants add the caller's boundary intensity, Ic averaged over the
+// face's two corner values (and give E_in/F_in, MGQD_In_Calc :125-178).
+template <class Real>
+__global__ void combine_boundary_kernel(CombineArgs A, const Real* __restrict__ bndV, const Real* __restrict__ bndH,
+                                        MomentOut O) {
+  const int nx = A.nx, ny = A.ny, ng = A.ng;
+  const long long nVb = 2LL * ny * ng, nHb = 2LL * nx * ng;
+  const long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const double eps = A.eps, c = A.c;
+  const int NH = A.nh;
+  // partial slot v of (q, h) = qh at cell (i, j) of group g
+  auto P = [&](int qh, int g, int i, int j, int v) {
+    return A.part[(((size_t)(qh * ng + g) * ny + j) * nx + i) * kNPart + v];
+  };
+  auto wsum = [&](int v) { return A.ws.s[0][v] + A.ws.s[1][v] + A.ws.s[2][v] + A.ws.s[3][v]; };
+
+  for (long long t = k0; t < nVb + nHb; t += stride) {
+    if (t < nVb) {
+      // vertical boundary face: t = j + ny*(g + ng*side), f = 0 (side 0) or nx (side 1)
+      const int j = (int)(t % ny), g = (int)((t / ny) % ng), side = (int)(t / ((long long)ny * ng));
+      const int f = side ? nx : 0;
+      const long long k = f + (long long)(nx + 1) * (j + (long long)ny * g);
+      double xx = 0, xy = 0, fxs = 0, e = 0;
+      double outF = 0, outE = 0;     // outgoing sums on the face (Cg)
+      double inF = 0, inE = 0;       // incoming sums on the face (MGQD_In_Calc)
+      for (int q = 0; q < 4; ++q) {
+        const bool xpos = (q == 0 || q == 3);
+        const int cell = xpos ? f - 1 : f;     // upwind cell of this face for quadrant q
+        if (cell >= 0 && cell < nx) {
+          for (int h = 0; h < NH; ++h) {
+            const int qh = q * NH + h;
+            const double vx = P(qh, g, cell, j, kVx), ve = P(qh, g, cell, j, kVe);
+            xx += P(qh, g, cell, j, kVxx); xy += P(qh, g, cell, j, kVxy); fxs += vx; e += ve;
+            outF += vx; outE += ve;
+          }
+        } else {
+          double sm[kNDirRow];
+          inflow_face_sums<Real>(A, bndV, side, g, q, j, 2 * ny, sm);
+          xx += sm[kWxx]; xy += sm[kWxy]; fxs += sm[kWx]; e += sm[kW];
+          inF += sm[kWx]; inE += sm[kW];
         }
-      } else {
-        double s[kNDirRow];
-        inflow_face_sums<Real>(A, bndV, f == 0 ? 0 : 1, g, q, j, 2 * ny, s);
-        xx += s[kWxx]; xy += s[kWxy]; fxs += s[kWx]; e += s[kW];
-        inF += s[kWx]; inE += s[kW];
       }
-    }
-    xx += eps * wsum(kWxx); xy += eps * wsum(kWxy); fxs += eps * wsum(kWx); e += eps * wsum(kW);
-    const double Eg = e / kCLight;
-    if (O.Hg_edgV_xx) { O.Hg_edgV_xx[k] = xx; O.Hg_edgV_xy[k] = xy; }
-    if (O.Eg_edgV) O.Eg_edgV[k] = Eg;
-    if (O.Fxg_edgV) O.Fxg_edgV[k] = fxs;
-    if (O.fg_edgV_xx) { O.fg_edgV_xx[k] = xx / (c * Eg); O.fg_edgV_xy[k] = xy / (c * Eg); }
-    if (f == 0 || f == nx) {
-      const int side = (f == 0) ? 0 : 2;   // BC_Type index: L = 0, R = 2
+      xx += eps * wsum(kWxx); xy += eps * wsum(kWxy); fxs += eps * wsum(kWx); e += eps * wsum(kW);
+      const double Eg = e / kCLight;
+      if (O.Hg_edgV_xx) { O.Hg_edgV_xx[k] = xx; O.Hg_edgV_xy[k] = xy; }
+      if (O.Eg_edgV) O.Eg_edgV[k] = Eg;
+      if (O.Fxg_edgV) O.Fxg_edgV[k] = fxs;
+      if (O.fg_edgV_xx) { O.fg_edgV_xx[k] = xx / (c * Eg); O.fg_edgV_xy[k] = xy / (c * Eg); }
+      const int bside = side ? 2 : 0;   // BC_Type index: L = 0, R = 2
       // outgoing quadrants of this face: left face -> q 1,2 ; right face -> q 0,3
-      const int qa = (f == 0) ? 1 : 0, qb = (f == 0) ? 2 : 3;
+      const int qa = side ? 0 : 1, qb = side ? 3 : 2;
       const long long bi = (long long)j + (long long)ny * g;
-      double* Cg = (f == 0) ? O.Cg_L : O.Cg_R;
-      double* Ein = (f == 0) ? O.Eg_in_L : O.Eg_in_R;
-      double* Fin = (f == 0) ? O.Fg_in_L : O.Fg_in_R;
+      double* Cg = side ? O.Cg_R : O.Cg_L;
+      double* Ein = side ? O.Eg_in_R : O.Eg_in_L;
+      double* Fin = side ? O.Fg_in_R : O.Fg_in_L;
       if (Cg) {
-        if (A.bc[side] == 0) {
+        if (A.bc[bside] == 0) {
           const double num = outF + eps * (A.ws.s[qa][kWx] + A.ws.s[qb][kWx]);
           const double den = outE + eps * (A.ws.s[qa][kW] + A.ws.s[qb][kW]);
           Cg[bi] = num / den;
@@ -309,50 +409,52 @@ __global__ void combine_kernel(CombineArgs A, const Real* __restrict__ bndV, con
         }
       }
       if (Ein) {
-        if (A.bc[side] == 0) { Ein[bi] = inE / kCLight; Fin[bi] = inF; }
+        if (A.bc[bside] == 0) { Ein[bi] = inE / kCLight; Fin[bi] = inF; }
         else { Ein[bi] = 0.0; Fin[bi] = 0.0; }
       }
-    }
-  }
-  // horizontal faces f = 0..ny
-  for (long long k = k0; k < nH; k += stride) {
-    const int i = (int)(k % nx), f = (int)((k / nx) % (ny + 1)), g = (int)(k / ((long long)nx * (ny + 1)));
-    double yy = 0, xy = 0, fys = 0, fxq = 0, e = 0;
-    double outF = 0, outE = 0, inF = 0, inE = 0;
-    for (int q = 0; q < 4; ++q) {
-      const bool ypos = (q == 0 || q == 1);
-      const int cell = ypos ? f - 1 : f;
-      if (cell >= 0 && cell < ny) {
-        for (int h = 0; h < NH; ++h) {
-          const double* p = P(q * NH + h, g, i, cell);
-          yy += p[kHyy]; xy += p[kHxy]; fys += p[kHy]; fxq += p[kHx]; e += p[kHe];
-          if (f == 0 || f == ny) { outF += p[kHy]; outE += p[kHe]; }
+    } else {
+      // horizontal boundary face: t - nVb = i + nx*(g + ng*side), f = 0 (side 0) or ny (side 1)
+      const long long u = t - nVb;
+      const int i = (int)(u % nx), g = (int)((u / nx) % ng), side = (int)(u / ((long long)nx * ng));
+      const int f = side ? ny : 0;
+      const long long k = i + (long long)nx * (f + (long long)(ny + 1) * g);
+      double yy = 0, xy = 0, fys = 0, fxq = 0, e = 0;
+      double outF = 0, outE = 0, inF = 0, inE = 0;
+      for (int q = 0; q < 4; ++q) {
+        const bool ypos = (q == 0 || q == 1);
+        const int cell = ypos ? f - 1 : f;
+        if (cell >= 0 && cell < ny) {
+          for (int h = 0; h < NH; ++h) {
+            const int qh = q * NH + h;
+            const double hy = P(qh, g, i, cell, kHy), he = P(qh, g, i, cell, kHe);
+            yy += P(qh, g, i, cell, kHyy); xy += P(qh, g, i, cell, kHxy); fys += hy; fxq += P(qh, g, i, cell, kHx);
+            e += he;
+            outF += hy; outE += he;
+          }
+        } else {
+          double sm[kNDirRow];
+          inflow_face_sums<Real>(A, bndH, side, g, q, i, 2 * nx, sm);
+          yy += sm[kWyy]; xy += sm[kWxy]; fys += sm[kWy]; fxq += sm[kWx]; e += sm[kW];
+          inF += sm[kWy]; inE += sm[kW];
         }
-      } else {
-        double s[kNDirRow];
-        inflow_face_sums<Real>(A, bndH, f == 0 ? 0 : 1, g, q, i, 2 * nx, s);
-        yy += s[kWyy]; xy += s[kWxy]; fys += s[kWy]; fxq += s[kWx]; e += s[kW];
-        inF += s[kWy]; inE += s[kW];
       }
-    }
-    yy += eps * wsum(kWyy); xy += eps * wsum(kWxy); fys += eps * wsum(kWy); fxq += eps * wsum(kWx);
-    e += eps * wsum(kW);
-    const double Eg = e / kCLight;
-    if (O.Hg_edgH_yy) { O.Hg_edgH_yy[k] = yy; O.Hg_edgH_xy[k] = xy; }
-    if (O.Eg_edgH) O.Eg_edgH[k] = Eg;
-    if (O.Fyg_edgH) O.Fyg_edgH[k] = fxq;           // Omega_x weighted, as TRANSPORT_SOLVES.f08:469
-    if (O.Fyg_edgH_true) O.Fyg_edgH_true[k] = fys;
-    if (O.fg_edgH_yy) { O.fg_edgH_yy[k] = yy / (c * Eg); O.fg_edgH_xy[k] = xy / (c * Eg); }
-    if (f == 0 || f == ny) {
-      const int side = (f == 0) ? 1 : 3;   // BC_Type index: B = 1, T = 3
+      yy += eps * wsum(kWyy); xy += eps * wsum(kWxy); fys += eps * wsum(kWy); fxq += eps * wsum(kWx);
+      e += eps * wsum(kW);
+      const double Eg = e / kCLight;
+      if (O.Hg_edgH_yy) { O.Hg_edgH_yy[k] = yy; O.Hg_edgH_xy[k] = xy; }
+      if (O.Eg_edgH) O.Eg_edgH[k] = Eg;
+      if (O.Fyg_edgH) O.Fyg_edgH[k] = fxq;           // Omega_x weighted, as TRANSPORT_SOLVES.f08:469
+      if (O.Fyg_edgH_true) O.Fyg_edgH_true[k] = fys;
+      if (O.fg_edgH_yy) { O.fg_edgH_yy[k] = yy / (c * Eg); O.fg_edgH_xy[k] = xy / (c * Eg); }
+      const int bside = side ? 3 : 1;   // BC_Type index: B = 1, T = 3
       // outgoing quadrants: bottom face -> q 2,3 ; top face -> q 0,1
-      const int qa = (f == 0) ? 2 : 0, qb = (f == 0) ? 3 : 1;
+      const int qa = side ? 0 : 2, qb = side ? 1 : 3;
       const long long bi = (long long)i + (long long)nx * g;
-      double* Cg = (f == 0) ? O.Cg_B : O.Cg_T;
-      double* Ein = (f == 0) ? O.Eg_in_B : O.Eg_in_T;
-      double* Fin = (f == 0) ? O.Fg_in_B : O.Fg_in_T;
+      double* Cg = side ? O.Cg_T : O.Cg_B;
+      double* Ein = side ? O.Eg_in_T : O.Eg_in_B;
+      double* Fin = side ? O.Fg_in_T : O.Fg_in_B;
       if (Cg) {
-        if (A.bc[side] == 0) {
+        if (A.bc[bside] == 0) {
           const double num = outF + eps * (A.ws.s[qa][kWy] + A.ws.s[qb][kWy]);
           const double den = outE + eps * (A.ws.s[qa][kW] + A.ws.s[qb][kW]);
           Cg[bi] = num / den;
@@ -361,7 +463,7 @@ __global__ void combine_kernel(CombineArgs A, const Real* __restrict__ bndV, con
         }
       }
       if (Ein) {
-        if (A.bc[side] == 0) { Ein[bi] = inE / kCLight; Fin[bi] = inF; }
+        if (A.bc[bside] == 0) { Ein[bi] = inE / kCLight; Fin[bi] = inF; }
         else { Ein[bi] = 0.0; Fin[bi] = 0.0; }
       }
     }
@@ -369,68 +471,41 @@ __global__ void combine_kernel(CombineArgs A, const Real* __restrict__ bndV, con
 }
 
 // Group sums: COLLAPSE_INTENSITIES totals (TRANSPORT_SOLVES.f08:488-509, sequential in g) and
-// GQD_In_Calc (GLOQD_SOLVES.f08:276-288).
+// GQD_In_Calc (GLOQD_SOLVES.f08:276-288).  One thread per (output array, point), groups added in
+// the order g = 0..ng-1.  Work items: E_avg (nx*ny), E_edgV and Fx_edgV ((nx+1)*ny each), E_edgH,
+// Fy_edgH, Fy_edgH_true (nx*(ny+1) each), E_in/F_in on L and R (ny each) and on B and T (nx each).
+__host__ __device__ inline long long group_sum_items(int nx, int ny) {
+  return (long long)nx * ny + 2LL * (nx + 1) * ny + 3LL * nx * (ny + 1) + 4LL * ny + 4LL * nx;
+}
+
 __global__ void group_sum_kernel(int nx, int ny, int ng, MomentOut O) {
   const long long nA = (long long)nx * ny, nV = (long long)(nx + 1) * ny, nH = (long long)nx * (ny + 1);
+  const long long seg_n[14] = {nA, nV, nV, nH, nH, nH, ny, ny, ny, ny, nx, nx, nx, nx};
+  const double* src[14] = {O.Eg_avg, O.Eg_edgV, O.Fxg_edgV, O.Eg_edgH, O.Fyg_edgH, O.Fyg_edgH_true,
+                           O.Eg_in_L, O.Eg_in_R, O.Fg_in_L, O.Fg_in_R, O.Eg_in_B, O.Eg_in_T, O.Fg_in_B, O.Fg_in_T};
+  double* dst[14] = {O.E_avg, O.E_edgV, O.Fx_edgV, O.E_edgH, O.Fy_edgH, O.Fy_edgH_true,
+                     O.E_in_L, O.E_in_R, O.F_in_L, O.F_in_R, O.E_in_B, O.E_in_T, O.F_in_B, O.F_in_T};
+  const long long total = group_sum_items(nx, ny);
   const long long stride = (long long)gridDim.x * blockDim.x;
-  const long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  for (long long k = k0; k < nA; k += stride)
-    if (O.E_avg && O.Eg_avg) {
-      double s = 0.0;
-      for (int g = 0; g < ng; ++g) s = s + O.Eg_avg[k + nA * g];
-      O.E_avg[k] = s;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += stride) {
+    long long p = t;
+    int a = 0;
+    while (p >= seg_n[a]) p -= seg_n[a++];
+    if (!src[a] || !dst[a]) continue;
+    const double* x = src[a] + p;
+    const long long n = seg_n[a];
+    double s = 0.0;
+    int g = 0;
+    for (; g + 8 <= ng; g += 8) {
+      double v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = x[n * (g + u)];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) s = s + v[u];
     }
-  for (long long k = k0; k < nV; k += stride) {
-    if (O.E_edgV && O.Eg_edgV) {
-      double s = 0.0;
-      for (int g = 0; g < ng; ++g) s = s + O.Eg_edgV[k + nV * g];
-      O.E_edgV[k] = s;
-    }
-    if (O.Fx_edgV && O.Fxg_edgV) {
-      double s = 0.0;
-      for (int g = 0; g < ng; ++g) s = s + O.Fxg_edgV[k + nV * g];
-      O.Fx_edgV[k] = s;
-    }
+    for (; g < ng; ++g) s = s + x[n * g];
+    dst[a][p] = s;
   }
-  for (long long k = k0; k < nH; k += stride) {
-    if (O.E_edgH && O.Eg_edgH) {
-      double s = 0.0;
-      for (int g = 0; g < ng; ++g) s = s + O.Eg_edgH[k + nH * g];
-      O.E_edgH[k] = s;
-    }
-    if (O.Fy_edgH && O.Fyg_edgH) {
-      double s = 0.0;
-      for (int g = 0; g < ng; ++g) s = s + O.Fyg_edgH[k + nH * g];
-      O.Fy_edgH[k] = s;
-    }
-    if (O.Fy_edgH_true && O.Fyg_edgH_true) {
-      double s = 0.0;
-      for (int g = 0; g < ng; ++g) s = s + O.Fyg_edgH_true[k + nH * g];
-      O.Fy_edgH_true[k] = s;
-    }
-  }
-  for (long long k = k0; k < ny; k += stride)
-    if (O.E_in_L && O.Eg_in_L) {
-      double a = 0, b = 0, cc = 0, d = 0;
-      for (int g = 0; g < ng; ++g) {
-        a = a + O.Eg_in_L[k + (long long)ny * g];
-        b = b + O.Eg_in_R[k + (long long)ny * g];
-        cc = cc + O.Fg_in_L[k + (long long)ny * g];
-        d = d + O.Fg_in_R[k + (long long)ny * g];
-      }
-      O.E_in_L[k] = a; O.E_in_R[k] = b; O.F_in_L[k] = cc; O.F_in_R[k] = d;
-    }
-  for (long long k = k0; k < nx; k += stride)
-    if (O.E_in_B && O.Eg_in_B) {
-      double a = 0, b = 0, cc = 0, d = 0;
-      for (int g = 0; g < ng; ++g) {
-        a = a + O.Eg_in_B[k + (long long)nx * g];
-        b = b + O.Eg_in_T[k + (long long)nx * g];
-        cc = cc + O.Fg_in_B[k + (long long)nx * g];
-        d = d + O.Fg_in_T[k + (long long)nx * g];
-      }
-      O.E_in_B[k] = a; O.E_in_T[k] = b; O.F_in_B[k] = cc; O.F_in_T[k] = d;
-    }
 }
 
 // ---------------------------------------------------------------------------------------------

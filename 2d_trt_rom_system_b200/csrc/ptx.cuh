@@ -1,4 +1,4 @@
-// Inline-PTX helpers for sm_100a: mbarriers and 1-D TMA bulk copies (no multicast).
+// Inline-PTX helpers for sm_100a: mbarriers, 1-D TMA bulk copies (no multicast) and cp.async.
 #pragma once
 
 #include <cstdint>
@@ -53,5 +53,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
+
+// 16-byte global -> shared copy through L2 only (cp.async.cg), grouped by commit; wait_group<N>
+// blocks until at most N of this thread's groups are still in flight.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 }  // namespace trt

@@ -496,13 +496,19 @@ int sweep_impl(trt_ctx* c, unsigned flags) {
     A.ws = c->ws;
     A.part = c->d_part;
     A.dir = c->d_dir;
-    const long long n = (long long)(c->nx + 1) * (c->ny + 1) * c->ng;
-    trt::combine_kernel<Real><<<grid_for(n), 256, 0, c->stream>>>(A, (const Real*)c->d_bndV, (const Real*)c->d_bndH,
-                                                                    c->dout);
+    // interior: one CTA per kCombTX x kCombTY tile of cells of one group
+    const dim3 cgrid((c->nx + trt::kCombTX - 1) / trt::kCombTX, (c->ny + trt::kCombTY - 1) / trt::kCombTY, c->ng);
+    cudaFuncSetAttribute(trt::combine_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trt::kCombSmem);
+    trt::combine_cells_kernel<<<cgrid, trt::kCombTX * trt::kCombTY, trt::kCombSmem, c->stream>>>(A, c->dout);
     TRT_LAUNCHED();
     TRT_CUDA(cudaGetLastError());
-    trt::group_sum_kernel<<<grid_for((long long)(c->nx + 1) * (c->ny + 1)), 256, 0, c->stream>>>(c->nx, c->ny,
-                                                                                                 c->ng, c->dout);
+    const long long nb = 2LL * (c->nx + c->ny) * c->ng;
+    trt::combine_boundary_kernel<Real><<<grid_for(nb), 256, 0, c->stream>>>(A, (const Real*)c->d_bndV,
+                                                                            (const Real*)c->d_bndH, c->dout);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+    trt::group_sum_kernel<<<grid_for(trt::group_sum_items(c->nx, c->ny)), 256, 0, c->stream>>>(c->nx, c->ny,
+                                                                                               c->ng, c->dout);
     TRT_LAUNCHED();
     TRT_CUDA(cudaGetLastError());
     c->have_moments = true;
@@ -1180,7 +1186,7 @@ int trt_collapse_intensities(int n_x, int n_y, int n_m, int n_g, int Open_Thread
   trt::MomentOut M{};
   M.Eg_avg = o[9].p; M.Eg_edgV = o[7].p; M.Eg_edgH = o[8].p; M.Fxg_edgV = o[10].p; M.Fyg_edgH = o[11].p;
   M.E_edgV = o[12].p; M.E_edgH = o[13].p; M.E_avg = o[14].p; M.Fx_edgV = o[15].p; M.Fy_edgH = o[16].p;
-  trt::group_sum_kernel<<<grid_for((long long)(n_x + 1) * (n_y + 1)), 256>>>(n_x, n_y, n_g, M);
+  trt::group_sum_kernel<<<grid_for(trt::group_sum_items(n_x, n_y)), 256>>>(n_x, n_y, n_g, M);
   TRT_LAUNCHED();
   TRT_CUDA(cudaGetLastError());
   double* hs[17] = {Hg_avg_xx, Hg_avg_yy, Hg_avg_xy, Hg_edgV_xx, Hg_edgV_xy, Hg_edgH_yy, Hg_edgH_xy, Eg_edgV, Eg_edgH,
@@ -1293,7 +1299,7 @@ int trt_gqd_in_calc(int n_x, int n_y, int n_g, double* E_in_L, double* E_in_B, d
   M.Fg_in_L = in[4].p; M.Fg_in_B = in[5].p; M.Fg_in_R = in[6].p; M.Fg_in_T = in[7].p;
   M.E_in_L = out[0].p; M.E_in_B = out[1].p; M.E_in_R = out[2].p; M.E_in_T = out[3].p;
   M.F_in_L = out[4].p; M.F_in_B = out[5].p; M.F_in_R = out[6].p; M.F_in_T = out[7].p;
-  trt::group_sum_kernel<<<grid_for(std::max(n_x, n_y)), 256>>>(n_x, n_y, n_g, M);
+  trt::group_sum_kernel<<<grid_for(trt::group_sum_items(n_x, n_y)), 256>>>(n_x, n_y, n_g, M);
   TRT_LAUNCHED();
   TRT_CUDA(cudaGetLastError());
   for (int k = 0; k < 8; ++k)
