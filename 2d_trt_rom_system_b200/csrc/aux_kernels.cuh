@@ -214,7 +214,7 @@ struct CombineArgs {
   int bc[4];           // BC_Type L, B, R, T
   int nh;              // direction splits per quadrant (partials per quadrant)
   WeightSums ws;
-  const double* part;  // [4*nh][ng][ny][nx][kNPart] partial records
+  const void* part;    // [4*nh][ng][ny][nx][part_rec<Real>()] partial records (Real = state precision)
   const double* dir;   // [kNDirRow][nm] full direction table (physical), double
 };
 
@@ -243,11 +243,33 @@ __device__ __forceinline__ void inflow_face_sums(const CombineArgs& A, const Rea
 // the quadrant partials in the order q = 0..3, split h = 0..NH-1 inside, then the analytic eps term.
 constexpr int kCombTX = 32, kCombTY = 8;
 constexpr int kCombRow = kCombTX + 1;                                 // records per staged row
-constexpr size_t kCombSmem = 2 * (size_t)(kCombTY + 1) * kCombRow * kNPart * sizeof(double);   // double buffer
+// Staged record stride in shared memory: 112-byte FP64 records are conflict-free for 16-byte loads
+// as they are; 64-byte FP32 records are padded to 80 bytes (8 consecutive records then cover all
+// 32 banks).
+template <class P>
+__host__ __device__ constexpr int comb_rec_stride() { return sizeof(P) == 4 ? 20 : 14; }
+template <class P>
+__host__ __device__ constexpr size_t comb_smem() {   // two staging buffers of records of type P
+  return 2 * (size_t)(kCombTY + 1) * kCombRow * comb_rec_stride<P>() * sizeof(P);
+}
 
+// Slots a..a+3 (a a multiple of 4) of a staged record as doubles.
+__device__ __forceinline__ void rec4(const double* p, int a, double (&v)[4]) {
+  const double2 x = *reinterpret_cast<const double2*>(p + a), y = *reinterpret_cast<const double2*>(p + a + 2);
+  v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+}
+__device__ __forceinline__ void rec4(const float* p, int a, double (&v)[4]) {
+  const float4 x = *reinterpret_cast<const float4*>(p + a);
+  v[0] = (double)x.x; v[1] = (double)x.y; v[2] = (double)x.z; v[3] = (double)x.w;
+}
+
+template <class P>
 __global__ void __launch_bounds__(kCombTX * kCombTY) combine_cells_kernel(CombineArgs A, MomentOut O) {
-  // two staging buffers [kCombTY + 1][kCombRow][kNPart]; row 0 / column 0 = halo
-  extern __shared__ __align__(16) double rec[];
+  // two staging buffers [kCombTY + 1][kCombRow][kRecS]; row 0 / column 0 = halo
+  extern __shared__ __align__(16) unsigned char comb_smem_raw[];
+  P* rec = reinterpret_cast<P*>(comb_smem_raw);
+  constexpr int kRec = part_rec<P>(), kRecS = comb_rec_stride<P>();
+  constexpr int kPerVec = 16 / (int)sizeof(P);          // values per 16-byte vector
   const int nx = A.nx, ny = A.ny, ng = A.ng, NH = A.nh;
   const int tx = threadIdx.x % kCombTX, ty = threadIdx.x / kCombTX;
   const int i0 = blockIdx.x * kCombTX, j0 = blockIdx.y * kCombTY, g = blockIdx.z;
@@ -256,8 +278,8 @@ __global__ void __launch_bounds__(kCombTX * kCombTY) combine_cells_kernel(Combin
   const int ncol = min(kCombTX, nx - i0), nrow = min(kCombTY, ny - j0);
   const double eps = A.eps, c = A.c;
   auto wsum = [&](int v) { return A.ws.s[0][v] + A.ws.s[1][v] + A.ws.s[2][v] + A.ws.s[3][v]; };
-  constexpr int kV2 = kNPart / 2;                      // 16-byte vectors per record
-  constexpr size_t kBuf = (size_t)(kCombTY + 1) * kCombRow * kNPart;
+  constexpr int kV2 = kRec * (int)sizeof(P) / 16;     // 16-byte vectors per record
+  constexpr size_t kBuf = (size_t)(kCombTY + 1) * kCombRow * kRecS;
 
   // issue the copies of (q, h) = qh into buffer b (asynchronous, one commit group)
   auto stage = [&](int qh, int b) {
@@ -267,11 +289,13 @@ __global__ void __launch_bounds__(kCombTX * kCombTY) combine_cells_kernel(Combin
     const int c0 = left_halo ? 0 : 1, r0 = low_halo ? 0 : 1;
     const int rowlen = (ncol + 1 - c0) * kV2;              // vectors per staged row
     const int nvec = (nrow + 1 - r0) * rowlen;
-    const double2* src = reinterpret_cast<const double2*>(A.part + ((size_t)(qh * ng + g) * ny * nx) * kNPart);
-    double2* dst = reinterpret_cast<double2*>(rec + b * kBuf);
+    const uint4* src = reinterpret_cast<const uint4*>(static_cast<const P*>(A.part) + ((size_t)(qh * ng + g) * ny * nx) * kRec);
+    P* dst = rec + b * kBuf;
     for (int v = threadIdx.x; v < nvec; v += kCombTX * kCombTY) {
       const int rr = r0 + v / rowlen, e = v % rowlen;      // staged row, vector within the row
-      cp_async16(dst + (rr * kCombRow + c0) * kV2 + e, src + ((size_t)(j0 - 1 + rr) * nx + (i0 - 1 + c0)) * kV2 + e);
+      const int rc = c0 + e / kV2, part = e % kV2;          // staged record (column), vector within it
+      cp_async16(dst + (rr * kCombRow + rc) * kRecS + part * kPerVec,
+                 src + ((size_t)(j0 - 1 + rr) * nx + (i0 - 1 + c0)) * kV2 + e);
     }
     cp_async_commit();
   };
@@ -291,18 +315,16 @@ __global__ void __launch_bounds__(kCombTX * kCombTY) combine_cells_kernel(Combin
     }
     __syncthreads();
     if (in) {
-      const double* own = rec + (qh & 1) * kBuf + ((size_t)(ty + 1) * kCombRow + tx + 1) * kNPart;
-      const double2 a01 = *reinterpret_cast<const double2*>(own + kCxx);
-      const double2 a23 = *reinterpret_cast<const double2*>(own + kCxy);
-      cxx += a01.x; cyy += a01.y; cxy += a23.x; ce += a23.y;
-      const double* pv = (q == 0 || q == 3) ? own - kNPart : own;
-      const double2 v01 = *reinterpret_cast<const double2*>(pv + kVxx);
-      const double2 v23 = *reinterpret_cast<const double2*>(pv + kVx);
-      vxx += v01.x; vxy += v01.y; vx += v23.x; ve += v23.y;
-      const double* ph = (q == 0 || q == 1) ? own - (size_t)kCombRow * kNPart : own;
-      const double2 h01 = *reinterpret_cast<const double2*>(ph + kHyy);
-      const double2 h23 = *reinterpret_cast<const double2*>(ph + kHy);
-      hyy += h01.x; hxy += h01.y; hy += h23.x; hx += h23.y; he += ph[kHe];
+      const P* own = rec + (qh & 1) * kBuf + ((size_t)(ty + 1) * kCombRow + tx + 1) * kRecS;
+      double u[4];
+      rec4(own, kCxx, u);
+      cxx += u[0]; cyy += u[1]; cxy += u[2]; ce += u[3];
+      const P* pv = (q == 0 || q == 3) ? own - kRecS : own;
+      rec4(pv, kVxx, u);
+      vxx += u[0]; vxy += u[1]; vx += u[2]; ve += u[3];
+      const P* ph = (q == 0 || q == 1) ? own - (size_t)kCombRow * kRecS : own;
+      rec4(ph, kHyy, u);
+      hyy += u[0]; hxy += u[1]; hy += u[2]; hx += u[3]; he += (double)ph[kHe];
     }
     __syncthreads();   // buffer qh & 1 is consumed
   }
@@ -356,7 +378,7 @@ __global__ void combine_boundary_kernel(CombineArgs A, const Real* __restrict__ 
   const int NH = A.nh;
   // partial slot v of (q, h) = qh at cell (i, j) of group g
   auto P = [&](int qh, int g, int i, int j, int v) {
-    return A.part[(((size_t)(qh * ng + g) * ny + j) * nx + i) * kNPart + v];
+    return (double)static_cast<const Real*>(A.part)[(((size_t)(qh * ng + g) * ny + j) * nx + i) * part_rec<Real>() + v];
   };
   auto wsum = [&](int v) { return A.ws.s[0][v] + A.ws.s[1][v] + A.ws.s[2][v] + A.ws.s[3][v]; };
 

@@ -117,8 +117,12 @@ TRT_LHD int frame_corner(int q, int cx, int cy) {
   return sy ? (sx ? 2 : 3) : (sx ? 1 : 0);
 }
 
-// Number of values per cell of a quadrant moment partial (13 used + 1 pad).
-constexpr int kNPart = 14;
+// Moment partial record of one (cell, quadrant, split): 13 values, padded to whole 16-byte vectors.
+// Records hold the state's precision: 14 doubles (112 B) for FP64, 16 floats (64 B) for FP32 (the
+// FP32 sweep's lane sums are FP64 and are rounded once, when the record is written).
+constexpr int kNPartUsed = 13;
+template <class P>
+TRT_LHD constexpr int part_rec() { return sizeof(P) == 4 ? 16 : 14; }
 // Partial value slots.  Signs are physical (Omega as given by the caller).
 enum PartSlot {
   kCxx = 0, kCyy, kCxy, kCe,        // cell centre: w Ox^2, w Oy^2, w Ox Oy, w       (x I_avg)

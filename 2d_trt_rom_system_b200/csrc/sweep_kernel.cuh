@@ -64,7 +64,7 @@ struct SweepArgs {
   Real* bndV;               // [2][ng][nm][2 ny]  Ic_edgV on faces x=0 (side 0) and x=nx (side 1)
   Real* bndH;               // [2][ng][nm][2 nx]  Ic_edgH on faces y=0 (side 0) and y=ny (side 1)
   Real* wrap;               // [4 ng][nx][mq][2]  top outflow of the last row of a round
-  double* part;             // [4][ng][ny][nx][kNPart]  quadrant moment partials (physical cells)
+  Real* part;               // [4*NH][ng][ny][nx][part_rec<Real>()]  moment partial records (physical cells)
   int* err;                 // error word (bit 0: TMA wait timed out)
   unsigned max_polls;       // bound on mbarrier polls per wait of the sweep
   unsigned drain_polls;     // bound on the polls that drain outstanding copies after a timeout
@@ -194,7 +194,8 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   const Real rcdt = a.rcdt;
   const int nxy = nx * ny;
   Real* wrapc = a.wrap + (size_t)blockIdx.x * nx * mqc * 2;
-  double* partg = a.part + ((size_t)((q * t.NH + h) * ng + g) * nxy) * kNPart;
+  constexpr int kRec = part_rec<Real>();
+  Real* partg = a.part + ((size_t)((q * t.NH + h) * ng + g) * nxy) * kRec;
   const int sideVin = fx ? 1 : 0, sideVout = fx ? 0 : 1;
   const int sideHin = fy ? 1 : 0, sideHout = fy ? 0 : 1;
   const Real* bVin = a.bndV + ((size_t)(sideVin * ng + g) * nm + q * mq + mo) * (2 * ny);
@@ -621,13 +622,27 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
     bool owner;
     const int base = slice_reduce_scatter<S, R>(mv, s, &owner);
     if (active && owner) {
-      double* pc = partg + (size_t)(j * nx + i) * kNPart;
+      Real* pc = partg + (size_t)(j * nx + i) * kRec;
+      if constexpr (sizeof(Real) == 8) {
 #pragma unroll
-      for (int k = 0; k < NSLOT; k += 2) {
-        if (NSLOT == 1) {
-          if (base < kNPart) pc[base] = mv[0];
-        } else if (base + k < kNPart) {
-          *reinterpret_cast<double2*>(pc + base + k) = make_double2(mv[k], mv[k + 1]);
+        for (int k = 0; k < NSLOT; k += 2) {
+          if (NSLOT == 1) {
+            if (base < kRec) pc[base] = mv[0];
+          } else if (base + k < kRec) {
+            *reinterpret_cast<double2*>(pc + base + k) = make_double2(mv[k], mv[k + 1]);
+          }
+        }
+      } else {
+        // 16-float record: every slot exists (13..15 are zero pads)
+        if constexpr (NSLOT >= 4) {
+#pragma unroll
+          for (int k = 0; k < NSLOT; k += 4)
+            *reinterpret_cast<float4*>(pc + base + k) =
+                make_float4((float)mv[k], (float)mv[k + 1], (float)mv[k + 2], (float)mv[k + 3]);
+        } else if constexpr (NSLOT == 2) {
+          *reinterpret_cast<float2*>(pc + base) = make_float2((float)mv[0], (float)mv[1]);
+        } else {
+          pc[base] = (float)mv[0];
         }
       }
     }

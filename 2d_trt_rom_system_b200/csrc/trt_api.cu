@@ -179,7 +179,7 @@ struct trt_ctx {
   bool use_srcfull = false;
   void *d_bndV = nullptr, *d_bndH = nullptr;
   void* d_wrap = nullptr;
-  double* d_part = nullptr;
+  void* d_part = nullptr;        // moment partial records (state precision)
   int* d_err = nullptr;
   double* d_outs = nullptr;
   trt::MomentOut dout{};
@@ -305,7 +305,9 @@ void default_split(int ng, int mq, int* NH, int* W) {
 }
 
 size_t part_bytes(const trt_ctx* c) {
-  return (size_t)4 * c->t.NH * c->ng * c->nx * c->ny * trt::kNPart * sizeof(double);
+  const size_t rec = c->prec == TRT_PREC_FP64 ? trt::part_rec<double>() * sizeof(double)
+                                                : trt::part_rec<float>() * sizeof(float);
+  return (size_t)4 * c->t.NH * c->ng * c->nx * c->ny * rec;
 }
 size_t wrap_bytes(const trt_ctx* c) { return (size_t)4 * c->ng * c->t.NH * c->nx * c->t.mqc * 2 * c->esz(); }
 
@@ -361,7 +363,7 @@ int setup_layout(trt_ctx* c) {
   }
   int rc = c->dalloc(&c->d_wrap, wrap_bytes(c));
   if (rc) return rc;
-  if ((rc = alloc_t(c, &c->d_part, part_bytes(c) / sizeof(double)))) return rc;
+  if ((rc = c->dalloc(&c->d_part, part_bytes(c)))) return rc;
   TRT_CUDA(cudaMemsetAsync(c->d_part, 0, part_bytes(c), c->stream));
   return TRT_OK;
 }
@@ -477,7 +479,7 @@ int sweep_impl(trt_ctx* c, unsigned flags) {
   a.bndV = (Real*)c->d_bndV;
   a.bndH = (Real*)c->d_bndH;
   a.wrap = (Real*)c->d_wrap;
-  a.part = c->d_part;
+  a.part = (Real*)c->d_part;
   a.err = c->d_err;
   a.max_polls = c->wait_polls;
   a.drain_polls = 1u << 24;
@@ -498,8 +500,10 @@ int sweep_impl(trt_ctx* c, unsigned flags) {
     A.dir = c->d_dir;
     // interior: one CTA per kCombTX x kCombTY tile of cells of one group
     const dim3 cgrid((c->nx + trt::kCombTX - 1) / trt::kCombTX, (c->ny + trt::kCombTY - 1) / trt::kCombTY, c->ng);
-    cudaFuncSetAttribute(trt::combine_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trt::kCombSmem);
-    trt::combine_cells_kernel<<<cgrid, trt::kCombTX * trt::kCombTY, trt::kCombSmem, c->stream>>>(A, c->dout);
+    cudaFuncSetAttribute(trt::combine_cells_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)trt::comb_smem<Real>());
+    trt::combine_cells_kernel<Real><<<cgrid, trt::kCombTX * trt::kCombTY, trt::comb_smem<Real>(), c->stream>>>(A,
+                                                                                                           c->dout);
     TRT_LAUNCHED();
     TRT_CUDA(cudaGetLastError());
     const long long nb = 2LL * (c->nx + c->ny) * c->ng;
@@ -907,7 +911,7 @@ size_t trt_required_bytes(int n_x, int n_y, int n_m, int n_g, int precision) {
   b += ncell * (16 + 2 * esz);
   b += (size_t)2 * n_g * n_m * 2 * (n_x + n_y) * esz;
   b += (size_t)4 * n_g * NH * n_x * mqc * 2 * esz;
-  b += (size_t)4 * NH * n_g * n_x * n_y * trt::kNPart * 8;
+  b += (size_t)4 * NH * n_g * n_x * n_y * (precision == TRT_PREC_FP64 ? 112 : 64);   // partial records
   long long sz[kNOut];
   output_sizes(n_x, n_y, n_g, sz);
   for (int k = 0; k < kNOut; ++k) b += sz[k] * 8;

@@ -182,10 +182,12 @@ def test_direction_splits_fp32_state_unchanged():
         with resident(d, precision="fp32", tiling=dict(splits=splits)) as s:
             s.sweep(moments=True)
             out.append((s.get_state(), s.moments(["Eg_avg", "Fxg_edgV"])))
+    # FP32 partial records are rounded once per (cell, quadrant, split): splitting changes that
+    # rounding, at the FP32 unit roundoff
     for I, m in out[1:]:
         assert np.array_equal(I, out[0][0])
         for k in m:
-            assert rel_err_per_group(m[k], out[0][1][k]) < 1e-14, k
+            assert rel_err_per_group(m[k], out[0][1][k]) < 1e-6, k
 
 
 def test_split_count_limits():
