@@ -224,7 +224,10 @@ def time_resident(pkg, torch, s, steps, warmup, flags):
     stream = torch.cuda.ExternalStream(s.stream())
     for _ in range(warmup):
         pkg.check(L.trt_sweep(s.handle, flags), "trt_sweep")
+    # timed region bracketed by device synchronisation and a barrier over ranks on both sides
     s.sync()
+    torch.cuda.synchronize()
+    pkg.ranks.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     n0 = pkg.kernel_launches()
@@ -233,6 +236,8 @@ def time_resident(pkg, torch, s, steps, warmup, flags):
         pkg.check(L.trt_sweep(s.handle, flags), "trt_sweep")
     e1.record(stream)
     s.sync()
+    torch.cuda.synchronize()
+    pkg.ranks.barrier()
     n1 = pkg.kernel_launches()
     return e0.elapsed_time(e1) / steps, n1 - n0
 
@@ -263,12 +268,15 @@ def time_e2e(pkg, torch, s, prob, kap, src, steps, warmup):
 
     for _ in range(warmup):
         step()
+    # host wall clock: the region includes the host<->device copies the C ABI makes
     torch.cuda.synchronize()
+    pkg.ranks.barrier()
     t0 = time.perf_counter()
     for _ in range(steps):
         step()
     torch.cuda.synchronize()
     dt = (time.perf_counter() - t0) / steps
+    pkg.ranks.barrier()
     h2d = kp.nbytes + sp.nbytes
     d2h = sum(a.nbytes for a in outs.values())
     return dt, h2d, d2h
@@ -300,43 +308,11 @@ def cpu_baseline(prob_full, budget_s=20.0):
                       f"sweeps, {gs} threads (OpenMP over groups), g++ -O2 -fopenmp, host has {cores} cores"}
 
 
-def dist_setup(args):
-    import torch
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    elif torch.cuda.is_available():
-        torch.cuda.set_device(0)
-    return ws, rank, local
-
-
-def reduce_max(ws, val):
-    if ws == 1:
-        return val
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([val], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
 def run_reference(args):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    pkg, prob = build_problem(args.config)
+    ws, rank, _ = pkg.ranks.world()
     if rank != 0:
         return 0
-    pkg, prob = build_problem(args.config)
     cb = cpu_baseline(prob, budget_s=60.0)
     line = {"metric": "cell-angle-group updates/s", "value": cb["value"], "unit": "updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
@@ -360,8 +336,10 @@ def main():
     if args.tiling_sweep:
         return run_tiling_sweep(args)
     import torch
-    ws, rank, local = dist_setup(args)
     pkg, prob = build_problem(args.config, args.n, args.groups)
+    ranks = pkg.ranks
+    ws, rank, local = ranks.init("nccl")
+    torch.cuda.set_device(local)
     tiling = tuple(int(x) for x in args.tiling.split(",")) if args.tiling else None
     upd = prob.updates_per_sweep()
     peak, peak_kind = peaks()
@@ -372,17 +350,16 @@ def main():
     for prec in precs:
         s, kap, src = setup_instance(pkg, prob, "mixed" if prec == "fp32" else "fp64", tiling)
         try:
-            barrier(ws)
             if prec == "fp32":
                 with ClockSampler(local) as cs:
                     ms, launches = time_resident(pkg, torch, s, args.steps, args.warmup, flags)
                 clocks = cs.summary()
             else:
                 ms, launches = time_resident(pkg, torch, s, args.steps, args.warmup, flags)
-            ms = reduce_max(ws, ms)
+            ms = ranks.reduce_max(ms)
             # sweep kernel alone (no moments, no roll): per-launch duration for the roofline
             ms_k, _ = time_resident(pkg, torch, s, max(3, args.steps // 2), 1, 0)
-            ms_k = reduce_max(ws, ms_k)
+            ms_k = ranks.reduce_max(ms_k)
             e2e = time_e2e(pkg, torch, s, prob, kap, src, max(3, args.steps // 4), 1) if prec == "fp32" else None
             tl = s.tiling()
         finally:
@@ -393,7 +370,7 @@ def main():
     main_ = res["fp32"]
     line = {
         "metric": "cell-angle-group updates/s",
-        "value": ws * upd / (main_["ms"] * 1e-3),
+        "value": ranks.whole_job_rate(upd, main_["ms"] * 1e-3, ws),
         "unit": "updates/s",
         "n_gpus": ws,
         "steps": args.steps,
@@ -419,23 +396,21 @@ def main():
     }
     if "fp64" in res:
         r = res["fp64"]
-        line["plain_fp64"] = {"value": ws * upd / (r["ms"] * 1e-3), "ms_per_step": r["ms"], "dtype": "f64",
+        line["plain_fp64"] = {"value": ranks.whole_job_rate(upd, r["ms"] * 1e-3, ws), "ms_per_step": r["ms"], "dtype": "f64",
                               "roofline": {"achieved": r["achieved"], "peak": peak, "frac": r["achieved"] / peak,
                                            "unit": "GB/s", "kernel_ms": r["ms_kernel"], "bytes_per_update": r["B"],
                                            "traffic": traffic_from_profile("fp64")},
                               "tiling": r["tiling"]}
         line["mixed_over_fp64"] = line["value"] / line["plain_fp64"]["value"]
     dt, h2d, d2h = main_["e2e"]
-    dt = reduce_max(ws, dt)
-    line["e2e"] = {"value": ws * upd / dt, "unit": "updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+    dt = ranks.reduce_max(dt)
+    line["e2e"] = {"value": ranks.whole_job_rate(upd, dt, ws), "unit": "updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                    "ms_per_step": dt * 1e3, "path": "trt_set_material(host) + trt_sweep + trt_moments(host), pinned"}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(prob)
     if rank == 0:
         print(json.dumps(line))
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    ranks.finalize()
     return 0
 
 
