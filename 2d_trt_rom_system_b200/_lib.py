@@ -98,6 +98,10 @@ SIGNATURES = {
     "trt_set_wait_limit": (_i, [_P, ctypes.c_uint]),
     "trt_set_wait_limit_zero": (_i, [_P]),
     "trt_device_output": (_P, [_P, ctypes.c_char_p]),
+    "trt_tstep_setup": (_i, [_P, _D, _D, _D, _D, _d, _d, _d, _d, _I, _D, _i, _d, _i]),
+    "trt_tstep": (_i, [_P, _I, _D, _D]),
+    "trt_get_temperature": (_i, [_P, _D]),
+    "trt_put_temperature": (_i, [_P, _D]),
     "trt_strerror": (ctypes.c_char_p, [_i]),
     "trt_kernel_launches": (ctypes.c_ulonglong, []),
     "trt_transport_residual_noalloc": (_i, [_i, _i, _i, _i] + [_P] * 11 + [_d, _d, _P, _P, _P, _P]),

@@ -236,6 +236,33 @@ class TransportSweep:
         check(_lib.lib().trt_init_state(self._h, float(Tini), *[float(t) for t in bcT], float(Comp_Unit),
                                         dptr(_f64(Nu_g, (self.ng + 1,)))), "trt_init_state")
 
+    def tstep_setup(self, Nu_g, kappa_mult, cV, Temp, Kap0, Comp_Unit, c, Delt, BC_Type=(0, 0, 0, 0),
+                    bcT=(0.0, 0.0, 0.0, 0.0), conv_type=2, conv_ho=1e-12, maxit_rte=150):
+        """Device time stepping with the reference's run_type 'tr_no_qd' (temperatures in eV);
+        kappa_mult(i,j) = Kappa_Mult(Mat(i,j)); cV per cell or a scalar."""
+        shp = (self.nx, self.ny)
+        cv = _f64(np.broadcast_to(np.asarray(cV, dtype=np.float64), shp), shp)
+        bc = np.ascontiguousarray(BC_Type, dtype=np.int32)
+        bt = np.ascontiguousarray(bcT, dtype=np.float64)
+        check(_lib.lib().trt_tstep_setup(self._h, dptr(_f64(Nu_g, (self.ng + 1,))), dptr(_f64(kappa_mult, shp)),
+                                         dptr(cv), dptr(_f64(Temp, shp)), float(Kap0), float(Comp_Unit), float(c),
+                                         float(Delt), iptr(bc), dptr(bt), int(conv_type), float(conv_ho),
+                                         int(maxit_rte)), "trt_tstep_setup")
+
+    def tstep(self):
+        """One backward-Euler time step; returns (outer iterations, T norm, E norm)."""
+        its, tn, en = ctypes.c_int(0), ctypes.c_double(0), ctypes.c_double(0)
+        check(_lib.lib().trt_tstep(self._h, ctypes.byref(its), ctypes.byref(tn), ctypes.byref(en)), "trt_tstep")
+        return its.value, tn.value, en.value
+
+    def temperature(self):
+        T = np.empty((self.nx, self.ny), order="F")
+        check(_lib.lib().trt_get_temperature(self._h, dptr(T)), "trt_get_temperature")
+        return T
+
+    def put_temperature(self, Temp):
+        check(_lib.lib().trt_put_temperature(self._h, dptr(_f64(Temp, (self.nx, self.ny)))), "trt_put_temperature")
+
     def put_state(self, I_crn):
         I = _f64(I_crn, (2 * self.nx, 2 * self.ny, self.nm, self.ng))
         check(_lib.lib().trt_put_state(self._h, dptr(I)), "trt_put_state")

@@ -14,6 +14,7 @@
 #include "aux_kernels.cuh"
 #include "dropin_kernels.cuh"
 #include "sweep_kernel.cuh"
+#include "tstep_kernels.cuh"
 
 namespace {
 
@@ -191,6 +192,14 @@ struct trt_ctx {
   int bc[4] = {0, 0, 0, 0};
   bool have_material = false, have_state = false, swept = false, have_moments = false, have_res = false;
   unsigned wait_polls = kDefaultWaitPolls;
+  // transport-only time step (run_type 'tr_no_qd'): temperature and material model on the device
+  bool ts_ready = false;
+  double *d_T = nullptr, *d_Told = nullptr, *d_Trt1 = nullptr, *d_Trt2 = nullptr;
+  double *d_Ert1 = nullptr, *d_Ert2 = nullptr, *d_nu = nullptr, *d_kmult = nullptr, *d_cv = nullptr;
+  unsigned long long* d_conv = nullptr;   // [2][5] convergence reductions (T, E)
+  double ts_Kap0 = 0.0, ts_conv_ho = 0.0, ts_Tb[4] = {0, 0, 0, 0};
+  int ts_conv_type = 1, ts_maxit = 1, ts_bc[4] = {0, 0, 0, 0};
+  std::vector<double> ts_nu;
 
   size_t esz() const { return prec == TRT_PREC_FP64 ? sizeof(double) : sizeof(float); }
   long long state_elems() const { return 4LL * ng * t.NH * blk; }
@@ -869,6 +878,94 @@ struct DBuf {
   }
 };
 
+// ---------------------------------------------------------------------------------------------
+// Transport-only time step (run_type 'tr_no_qd', ALGORITHMS.f08:389-421, 524-572, 662-668, 816-836).
+// ---------------------------------------------------------------------------------------------
+
+// MATERIAL_UPDATE (UPDATES.f08:110-152) from the device temperature into the sweep's material.
+template <class Real>
+int material_update_impl(trt_ctx* c) {
+  const long long n = (long long)c->nx * c->ny * c->ng;
+  trt::material_update_kernel<Real><<<grid_for(n), 256, 0, c->stream>>>(
+      c->nx, c->ny, c->ng, c->d_T, c->d_nu, c->d_kmult, c->comp_unit, c->d_kap64, c->d_q64, (Real*)c->d_kap,
+      (Real*)c->d_q);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  c->use_srcfull = false;
+  c->have_material = true;
+  return TRT_OK;
+}
+
+// CONVERGENCE (CONVERGENCE_CHECKS.f08:7-44) from the reduced data {max|x-xo|, max|xo-xo2|, max|x|,
+// min|x|, max|1-xo/x|}.
+bool convergence(int conv_type, double eps, const double* r, int its, double* norm) {
+  const double rho = its > 1 ? r[0] / r[1] : 2.0;
+  double nrm = 0.0;
+  if (conv_type == 1) nrm = r[0] / r[2];
+  else if (conv_type == 2) nrm = r[4];
+  else nrm = r[0] / r[3];
+  *norm = nrm;
+  const double new_eps = std::fabs(1.0 / rho - 1.0) * eps;
+  return !(nrm > new_eps);
+}
+
+template <class Real>
+int tstep_impl(trt_ctx* c, int* its_out, double* tnorm_out, double* enorm_out) {
+  const size_t nxy = (size_t)c->nx * c->ny;
+  const size_t bytes = nxy * sizeof(double);
+  // moving last time step data to the _old arrays (ALGORITHMS.f08:395-396) and resetting the
+  // outer-iteration history (:518-521)
+  TRT_CUDA(cudaMemcpyAsync(c->d_Told, c->d_T, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  for (double* p : {c->d_Trt1, c->d_Trt2, c->d_Ert1, c->d_Ert2}) TRT_CUDA(cudaMemsetAsync(p, 0, bytes, c->stream));
+  const bool reflective = c->ts_bc[0] > 0 || c->ts_bc[1] > 0 || c->ts_bc[2] > 0 || c->ts_bc[3] > 0;
+  int its = 0;
+  bool conv = false;
+  double tn = 0.0, en = 0.0;
+  const unsigned long long init[10] = {0, 0, 0, 0x7ff0000000000000ULL, 0, 0, 0, 0, 0x7ff0000000000000ULL, 0};
+  while (!conv && its < c->ts_maxit) {
+    ++its;
+    // RTE solve with the collapse, fg and Cg (:547-569); I_crn_old <- I_crn only on the first
+    int rc = sweep_impl<Real>(c, (its == 1 ? TRT_ROLL_STATE : 0u) | TRT_MOMENTS);
+    if (rc) return rc;
+    if (reflective && (rc = bc_update_impl<Real>(c, c->ts_bc, c->ts_Tb, c->comp_unit, c->ts_nu.data()))) return rc;
+    // MEB_SOLVE with the transport group energies (:666), then MATERIAL_UPDATE (:668)
+    trt::meb_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>(c->nx, c->ny, c->ng, c->dout.Eg_avg, c->d_kap64,
+                                                                      c->d_Told, c->d_cv, c->dt, c->ts_Kap0,
+                                                                      c->comp_unit, c->d_T);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+    if ((rc = material_update_impl<Real>(c))) return rc;
+    // convergence of T and of the transport E (:816-818)
+    TRT_CUDA(cudaMemcpyAsync(c->d_conv, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+    trt::conv_reduce_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>((long long)nxy, c->d_T, c->d_Trt1,
+                                                                              c->d_Trt2, c->d_conv);
+    TRT_LAUNCHED();
+    trt::conv_reduce_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>((long long)nxy, c->dout.E_avg,
+                                                                              c->d_Ert1, c->d_Ert2, c->d_conv + 5);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+    unsigned long long h[10];
+    TRT_CUDA(cudaMemcpyAsync(h, c->d_conv, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    TRT_CUDA(cudaStreamSynchronize(c->stream));
+    if ((rc = check_err(c))) return rc;
+    double r[10];
+    std::memcpy(r, h, sizeof(r));
+    const bool tconv = convergence(c->ts_conv_type, c->ts_conv_ho, r, its, &tn);
+    const bool econv = convergence(c->ts_conv_type, c->ts_conv_ho, r + 5, its, &en);
+    conv = tconv && econv;
+    // current iterate -> last iterate (:834-837)
+    TRT_CUDA(cudaMemcpyAsync(c->d_Ert2, c->d_Ert1, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    TRT_CUDA(cudaMemcpyAsync(c->d_Ert1, c->dout.E_avg, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    TRT_CUDA(cudaMemcpyAsync(c->d_Trt2, c->d_Trt1, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    TRT_CUDA(cudaMemcpyAsync(c->d_Trt1, c->d_T, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  TRT_CUDA(cudaStreamSynchronize(c->stream));
+  if (its_out) *its_out = its;
+  if (tnorm_out) *tnorm_out = tn;
+  if (enorm_out) *enorm_out = en;
+  return TRT_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1128,6 +1225,70 @@ int trt_set_wait_limit(trt_ctx* c, unsigned polls) {
 int trt_set_wait_limit_zero(trt_ctx* c) {
   if (!c) return TRT_ERR_ARG;
   c->wait_polls = 0;
+  return TRT_OK;
+}
+
+int trt_tstep_setup(trt_ctx* c, const double* Nu_g, const double* kappa_mult, const double* cV, const double* Temp,
+                    double Kap0, double Comp_Unit, double cl, double Delt, const int* BC_Type, const double* bcT,
+                    int conv_type, double conv_ho, int maxit_rte) {
+  if (!c || !Nu_g || !kappa_mult || !cV || !Temp || !BC_Type || !bcT || !(Comp_Unit > 0) || !(cl > 0) ||
+      !(Delt > 0) || conv_type < 1 || conv_type > 3 || maxit_rte < 1 || !(conv_ho >= 0))
+    return TRT_ERR_ARG;
+  const size_t nxy = (size_t)c->nx * c->ny;
+  int rc = TRT_OK;
+  if (!c->d_T) {
+    for (double** p : {&c->d_T, &c->d_Told, &c->d_Trt1, &c->d_Trt2, &c->d_Ert1, &c->d_Ert2, &c->d_kmult, &c->d_cv})
+      if ((rc = alloc_t(c, p, nxy))) return rc;
+    if ((rc = alloc_t(c, &c->d_nu, (size_t)c->ng + 1))) return rc;
+    if ((rc = alloc_t(c, &c->d_conv, 10))) return rc;
+  }
+  TRT_CUDA(cudaMemcpyAsync(c->d_T, Temp, nxy * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  TRT_CUDA(cudaMemcpyAsync(c->d_kmult, kappa_mult, nxy * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  TRT_CUDA(cudaMemcpyAsync(c->d_cv, cV, nxy * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  TRT_CUDA(cudaMemcpyAsync(c->d_nu, Nu_g, (c->ng + 1) * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  c->ts_nu.assign(Nu_g, Nu_g + c->ng + 1);
+  for (int k = 0; k < 4; ++k) {
+    c->ts_bc[k] = BC_Type[k];
+    c->bc[k] = BC_Type[k];
+    c->ts_Tb[k] = bcT[k];
+  }
+  c->ts_Kap0 = Kap0;
+  c->ts_conv_type = conv_type;
+  c->ts_conv_ho = conv_ho;
+  c->ts_maxit = maxit_rte;
+  c->c = cl;
+  c->dt = Delt;
+  c->comp_unit = Comp_Unit;
+  // initial material from the initial temperature (INITIALIZERS.f08:137)
+  rc = c->prec == TRT_PREC_FP64 ? material_update_impl<double>(c) : material_update_impl<float>(c);
+  if (rc) return rc;
+  TRT_CUDA(cudaStreamSynchronize(c->stream));
+  c->ts_ready = true;
+  return TRT_OK;
+}
+
+int trt_tstep(trt_ctx* c, int* rt_its, double* T_norm, double* E_norm) {
+  if (!c) return TRT_ERR_ARG;
+  if (!c->ts_ready || (!c->have_state && !c->swept)) return TRT_ERR_STATE;
+  return c->prec == TRT_PREC_FP64 ? tstep_impl<double>(c, rt_its, T_norm, E_norm)
+                                  : tstep_impl<float>(c, rt_its, T_norm, E_norm);
+}
+
+int trt_get_temperature(trt_ctx* c, double* Temp) {
+  if (!c || !Temp) return TRT_ERR_ARG;
+  if (!c->ts_ready) return TRT_ERR_STATE;
+  TRT_CUDA(cudaMemcpyAsync(Temp, c->d_T, (size_t)c->nx * c->ny * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  TRT_CUDA(cudaStreamSynchronize(c->stream));
+  return TRT_OK;
+}
+
+int trt_put_temperature(trt_ctx* c, const double* Temp) {
+  if (!c || !Temp) return TRT_ERR_ARG;
+  if (!c->ts_ready) return TRT_ERR_STATE;
+  TRT_CUDA(cudaMemcpyAsync(c->d_T, Temp, (size_t)c->nx * c->ny * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int rc = c->prec == TRT_PREC_FP64 ? material_update_impl<double>(c) : material_update_impl<float>(c);
+  if (rc) return rc;
+  TRT_CUDA(cudaStreamSynchronize(c->stream));
   return TRT_OK;
 }
 

@@ -199,3 +199,42 @@ def random_small(seed, nx, ny, G, quad="S8", bc_type=(0, 0, 0, 0)):
     bcT = tuple(float(rng.uniform(0.2, 1.5)) for _ in range(4))
     return Problem(f"R{seed}", nx, ny, 1.0 * nx / 10, 1.0 * ny / 10, log_groups(G, 1e-2, 10.0), quad, kappa0, cv,
                    0.3, bcT, bc_type=bc_type)
+
+
+# ---------------------------------------------------------------------------------------------
+# Transport-only time stepping (the reference's run_type 'tr_no_qd') with the reference's own
+# material: the Fleck-Cummings opacity kapB_calc (TEMP_FUNCTIONS.f08:11-32) scaled per cell by
+# Kappa_Mult(Mat(i,j)), Kap0 = 27e9 eV^3/cm (main.f08:22) and the heat capacity of INPUTS.f08:89-121.
+# Temperatures and photon energies are in eV.
+# ---------------------------------------------------------------------------------------------
+KAP0_FC = 27.0 * 1e9
+
+
+def fc_cv(bcT_left_eV, comp_unit=COMP_UNIT):
+    """Cv of INPUTS.f08:121 (with sig_R, aR of :89-90)."""
+    h, c, erg = 6.62613e-19, C_LIGHT, 6.24150934e11
+    pi = math.pi
+    sig_R = 2.0 * pi ** 5 / (15.0 * c ** 2 * h ** 3 * erg ** 4 * comp_unit)
+    aR = 4.0 * sig_R / c
+    return 0.5917 * aR * bcT_left_eV ** 3 * ((1.38e-16) ** 4 * (11600.0 ** 4) * erg ** 4)
+
+
+@dataclasses.dataclass
+class TimeStepSetup:
+    """Inputs of trt_tstep_setup for a Problem: the Problem's grid, groups, quadrature and material map,
+    with the reference's Fleck-Cummings physics (kappa_mult = kappa0 / min(kappa0))."""
+    nu_eV: np.ndarray
+    kappa_mult: np.ndarray
+    cv: float
+    Kap0: float
+    Tini_eV: float
+    bcT_eV: tuple
+    dt: float
+
+
+def fc_timestep_setup(prob, Tini_eV=None):
+    k0 = np.asarray(prob.kappa0, dtype=np.float64)
+    bcT = tuple(t * KEV for t in prob.bcT)
+    Tini = prob.T0 * KEV if Tini_eV is None else Tini_eV
+    return TimeStepSetup(nu_eV=prob.nu_eV, kappa_mult=np.asfortranarray(k0 / k0.min()),
+                         cv=fc_cv(max(bcT[0], 1.0)), Kap0=KAP0_FC, Tini_eV=Tini, bcT_eV=bcT, dt=prob.dt)

@@ -227,6 +227,30 @@ int trt_transport_residual_noalloc(int n_x, int n_y, int n_m, int n_g, const dou
                                    const double* Src_in, const double* I_crn_old, double c, double Delt,
                                    double* RT_Residual, int* RT_ResLoc_x, int* RT_ResLoc_y, void* stream);
 
+/* ---- Transport-only time step on the device (the reference's run_type 'tr_no_qd') ----------------
+ * Replaces, for one handle, the time loop of TRT_MLQD_ALGORITHM with HO_Form 0 and no low-order
+ * solve (MainSrc/ALGORITHMS.f08:389-421 and 524-572, 662-668, 816-836): per time step
+ * Temp_old <- Temp, I_crn_old <- I_crn, then outer iterations of
+ *   TRANSPORT_SCB + COLLAPSE_INTENSITIES + fg_Calc + Cg_Calc  (the fused sweep and epilogue),
+ *   RT_BC_UPDATE when a side is reflective,
+ *   MEB_SOLVE(Temp, HO_Eg_avg, ...)           (UPDATES.f08:185-230),
+ *   MATERIAL_UPDATE(Temp)                      (UPDATES.f08:110-152; KapE = kapB_calc * Kappa_Mult),
+ *   CONVERGENCE on Temp and HO_E_avg           (CONVERGENCE_CHECKS.f08:7-44),
+ * until both converge or maxit_rte iterations.  Temperatures and Nu_g are in eV, as in the reference.
+ * trt_tstep_setup: Nu_g (n_g+1) group edges; kappa_mult (n_x,n_y) = Kappa_Mult(Mat(i,j)); cV (n_x,n_y)
+ * heat capacity per cell (the reference's scalar cV broadcast); Temp (n_x,n_y) initial temperature;
+ * Kap0, Comp_Unit, c, Delt as in the reference; BC_Type[4] and bcT[4] (L, B, R, T) for the reflective
+ * boundary update.  It computes the initial material (INITIALIZERS.f08:137); the angular state comes
+ * from trt_init_state or trt_put_state.  trt_tstep returns the outer-iteration count and the last T
+ * and E norms. */
+int trt_tstep_setup(trt_ctx* ctx, const double* Nu_g, const double* kappa_mult, const double* cV, const double* Temp,
+                    double Kap0, double Comp_Unit, double c, double Delt, const int* BC_Type, const double* bcT,
+                    int conv_type, double conv_ho, int maxit_rte);
+int trt_tstep(trt_ctx* ctx, int* rt_its, double* T_norm, double* E_norm);
+int trt_get_temperature(trt_ctx* ctx, double* Temp);
+/* Replace the device temperature and recompute the material from it (MATERIAL_UPDATE). */
+int trt_put_temperature(trt_ctx* ctx, const double* Temp);
+
 /* Message for a TRT_ERR_* code. */
 const char* trt_strerror(int code);
 /* Number of kernels this library has launched in this process (instrumentation). */

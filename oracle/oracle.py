@@ -31,6 +31,9 @@ _SIG = {
     "oracle_gqd_in_calc": (_i, [_i, _i, _i] + [_D] * 16),
     "oracle_rt_bc_update": (_i, [_i, _i, _i, _i, _I, _d, _d, _d, _d, _d, _D, _D, _D, _D, _D]),
     "oracle_openmp_max_threads": (_i, []),
+    "oracle_material_update": (_i, [_i, _i, _i, _D, _D, _D, _d, _D, _D, _D]),
+    "oracle_meb_solve": (_i, [_i, _i, _i, _D, _D, _D, _D, _d, _D, _d, _d]),
+    "oracle_convergence": (_i, [_i, _d, _D, _D, _D, _i, _i, _D, _D]),
 }
 
 _lib = None
@@ -189,3 +192,74 @@ def scb_cell_ge(omx, omy, dx, dy, kapE, Q):
 
 def max_threads():
     return lib().oracle_openmp_max_threads()
+
+
+def material_update(Temp, Nu_g, kappa_mult, comp_unit):
+    """MATERIAL_UPDATE (UPDATES.f08:110-152): KapE = kapB_calc * Kappa_Mult, src = KapB * Bg, Bg; (nx,ny,ng)."""
+    nx, ny = Temp.shape
+    ng = len(Nu_g) - 1
+    K, S, B = zeros(nx, ny, ng), zeros(nx, ny, ng), zeros(nx, ny, ng)
+    rc = lib().oracle_material_update(nx, ny, ng, _p(F(Temp)), _p(F(Nu_g)), _p(F(kappa_mult)), float(comp_unit),
+                                      _p(K), _p(S), _p(B))
+    assert rc == 0
+    return K, S, B
+
+
+def meb_solve(Temp_old, Eg_HO, KapE, Delt, cV, Kap0, comp_unit):
+    """MEB_SOLVE (UPDATES.f08:185-230) with cV per cell; returns the new Temp."""
+    nx, ny, ng = Eg_HO.shape
+    T = zeros(nx, ny)
+    rc = lib().oracle_meb_solve(nx, ny, ng, _p(T), _p(F(Eg_HO)), _p(F(KapE)), _p(F(Temp_old)), float(Delt),
+                                _p(F(np.broadcast_to(cV, (nx, ny)))), float(Kap0), float(comp_unit))
+    assert rc == 0
+    return T
+
+
+def convergence(conv_type, eps, x, x_old, x_old2, its):
+    """CONVERGENCE (CONVERGENCE_CHECKS.f08:7-44): (converged, norm, rho)."""
+    n = int(np.asarray(x).size)
+    nrm, rho = ctypes.c_double(0), ctypes.c_double(0)
+    ok = lib().oracle_convergence(int(conv_type), float(eps), _p(F(x)), _p(F(x_old)), _p(F(x_old2)), n, int(its),
+                                  ctypes.byref(nrm), ctypes.byref(rho))
+    return bool(ok), nrm.value, rho.value
+
+
+def tr_no_qd_steps(st, Omega_x, Omega_y, quad_weight, Delx, Dely, Nu_g, kappa_mult, cV, Kap0, comp_unit, c, Delt,
+                   steps, conv_type=2, conv_ho=1e-12, maxit=150, bc_type=(0, 0, 0, 0), bcT=(0.0, 0.0, 0.0, 0.0),
+                   threads=4):
+    """Time steps of TRT_MLQD_ALGORITHM with run_type 'tr_no_qd' (ALGORITHMS.f08:389-421, 518-572,
+    662-668, 816-836).  st: dict with I_crn, Ic_edgV, Ic_edgH, I_edgV, I_edgH, Temp (updated in place).
+    Returns one (Temp, HO_E_avg, outer iterations, T norm, E norm) tuple per step."""
+    A = F(np.outer(Delx, Dely))
+    nm = len(Omega_x)
+    KapE, src, _ = material_update(st["Temp"], Nu_g, kappa_mult, comp_unit)   # INITIALIZERS.f08:137
+    hist = []
+    for _ in range(steps):
+        Temp_old = st["Temp"].copy(order="F")
+        I_crn_old = st["I_crn"].copy(order="F")
+        shp = Temp_old.shape
+        T_rt1, T_rt2 = zeros(*shp), zeros(*shp)
+        E_rt1, E_rt2 = zeros(*shp), zeros(*shp)
+        its, conv = 0, False
+        while not conv and its < maxit:
+            its += 1
+            Src_in = F(np.repeat(np.repeat(src, 2, axis=0), 2, axis=1)[:, :, None, :].repeat(nm, axis=2))
+            s = transport_scb(st["I_edgV"], st["I_edgH"], st["Ic_edgV"], st["Ic_edgH"], Omega_x, Omega_y, Delx, Dely,
+                              A, KapE, Src_in, I_crn_old, c, Delt, threads=threads, solver=1)
+            for k in ("I_crn", "I_edgV", "I_edgH", "Ic_edgV", "Ic_edgH"):
+                st[k] = s[k]
+            m = collapse_intensities(s["I_avg"], s["I_edgV"], s["I_edgH"], Omega_x, Omega_y, quad_weight, comp_unit,
+                                     threads=threads)
+            if max(bc_type) > 0:
+                st["I_edgV"], st["I_edgH"], st["Ic_edgV"], st["Ic_edgH"] = rt_bc_update(
+                    bc_type, bcT[0], bcT[1], bcT[2], bcT[3], comp_unit, Nu_g, st["I_edgV"], st["I_edgH"],
+                    st["Ic_edgV"], st["Ic_edgH"])
+            st["Temp"] = meb_solve(Temp_old, m["Eg_avg"], KapE, Delt, cV, Kap0, comp_unit)
+            KapE, src, _ = material_update(st["Temp"], Nu_g, kappa_mult, comp_unit)
+            tc, tn, _ = convergence(conv_type, conv_ho, st["Temp"], T_rt1, T_rt2, its)
+            ec, en, _ = convergence(conv_type, conv_ho, m["E_avg"], E_rt1, E_rt2, its)
+            conv = tc and ec
+            E_rt2, E_rt1 = E_rt1, m["E_avg"].copy(order="F")
+            T_rt2, T_rt1 = T_rt1, st["Temp"].copy(order="F")
+        hist.append((st["Temp"].copy(order="F"), m["E_avg"].copy(order="F"), its, tn, en))
+    return hist

@@ -16,6 +16,9 @@
 //   RT_BC_UPDATE             MainSrc/UPDATES.f08:12-105            -> oracle_rt_bc_update
 //   Bg_planck_calc, sigint   MainSrc/TEMP_FUNCTIONS.f08:90-141     -> oracle_bg_planck, oracle_sigint
 //   kapB_calc                MainSrc/TEMP_FUNCTIONS.f08:11-32      -> oracle_kapb
+//   MATERIAL_UPDATE          MainSrc/UPDATES.f08:110-152           -> oracle_material_update
+//   MEB_SOLVE                MainSrc/UPDATES.f08:185-230           -> oracle_meb_solve
+//   CONVERGENCE              MainSrc/CONVERGENCE_CHECKS.f08:7-44   -> oracle_convergence
 //
 // Third-party arithmetic: the reference solves each 4x4 corner system with GAUSS_COMPLETE from the
 // un-vendored library LA_TOOLS ("libjmcmath", no source and no version in the reference tree).  The
@@ -744,6 +747,72 @@ int oracle_rt_bc_update(int nx, int ny, int nm, int ng, const int* BC_Type, doub
     }
   }
   return 0;
+}
+
+// MATERIAL_UPDATE (UPDATES.f08:110-152), the arrays the sweep and MEB_SOLVE read: per (i, j, g)
+// Bg = Bg_planck_calc(T, nu_g, nu_g+1), KapE = KapB = kapB_calc(T, nu_g, nu_g+1) * kappa_mult(i,j)
+// (kappa_mult = Kappa_Mult(Mat(i,j))) and the isotropic corner source src = KapB * Bg (RT_Src holds
+// this value at every corner and direction).  Temp(nx,ny), Nu_g(ng+1); outputs (nx,ny,ng).
+int oracle_material_update(int nx, int ny, int ng, const double* Temp, const double* Nu_g, const double* kappa_mult,
+                           double Comp_Unit, double* KapE, double* src, double* Bg) {
+  for (int g = 0; g < ng; ++g)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const size_t c = (size_t)i + (size_t)nx * j, k = c + (size_t)nx * ny * g;
+        const double B = bg_planck(Temp[c], Nu_g[g], Nu_g[g + 1], Comp_Unit);
+        const double kB = oracle_kapb(Temp[c], Nu_g[g], Nu_g[g + 1]) * kappa_mult[c];
+        if (Bg) Bg[k] = B;
+        KapE[k] = kB;
+        src[k] = kB * B;
+      }
+  return 0;
+}
+
+// MEB_SOLVE (UPDATES.f08:185-230) with cV per cell (the reference passes one value):
+//   E = sum_g Eg_HO, KapE_Bar = (sum_g KapE*Eg_HO)/E,
+//   Temp = c**2*h**3/(c**2*h**3*cv*Comp_Unit + 8*pi*Delt*Kap0/erg**4)*(Delt*c*KapE_Bar*E + cv*Temp_old)*Comp_Unit.
+int oracle_meb_solve(int nx, int ny, int ng, double* Temp, const double* Eg_HO, const double* KapE,
+                     const double* Temp_old, double Delt, const double* cV, double Kap0, double Comp_Unit) {
+  const double pi = 4.0 * std::atan(1.0);
+  const double c2h3 = (kC * kC) * ((kH * kH) * kH);
+  const double e2 = kErg * kErg;
+  const double lin = (((8.0 * pi) * Delt) * Kap0) / (e2 * e2);
+  const size_t nxy = (size_t)nx * ny;
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const size_t c = (size_t)i + (size_t)nx * j;
+      double E = 0.0, kb = 0.0;
+      for (int g = 0; g < ng; ++g) {
+        E = E + Eg_HO[c + nxy * g];
+        kb = kb + KapE[c + nxy * g] * Eg_HO[c + nxy * g];
+      }
+      kb = kb / E;
+      const double coef = c2h3 / (((c2h3 * cV[c]) * Comp_Unit) + lin);
+      Temp[c] = (coef * ((((Delt * kC) * kb) * E) + cV[c] * Temp_old[c])) * Comp_Unit;
+    }
+  return 0;
+}
+
+// CONVERGENCE (CONVERGENCE_CHECKS.f08:7-44) of a field of n values; returns 1 when converged.
+int oracle_convergence(int conv_type, double eps, const double* x, const double* x_old, const double* x_old2, int n,
+                       int its, double* norm, double* rho) {
+  double d0 = 0.0, d1 = 0.0, mx = 0.0, mn = HUGE_VAL, r2 = 0.0;
+  for (int k = 0; k < n; ++k) {
+    d0 = std::max(d0, std::fabs(x[k] - x_old[k]));
+    d1 = std::max(d1, std::fabs(x_old[k] - x_old2[k]));
+    mx = std::max(mx, std::fabs(x[k]));
+    mn = std::min(mn, std::fabs(x[k]));
+    r2 = std::max(r2, std::fabs(1.0 - x_old[k] / x[k]));
+  }
+  const double r = its > 1 ? d0 / d1 : 2.0;
+  double nrm;
+  if (conv_type == 1) nrm = d0 / mx;
+  else if (conv_type == 2) nrm = r2;
+  else nrm = d0 / mn;
+  if (norm) *norm = nrm;
+  if (rho) *rho = r;
+  const double new_eps = std::fabs(1.0 / r - 1.0) * eps;
+  return nrm > new_eps ? 0 : 1;
 }
 
 int oracle_openmp_max_threads(void) {
