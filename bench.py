@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--n", type=int, default=0, help="grid size override (profiling small cases)")
     p.add_argument("--groups", type=int, default=0, help="group count override (profiling small cases)")
     p.add_argument("--tiling-sweep", action="store_true", help="time the sweep kernel over a set of tilings")
+    p.add_argument("--time-steps", type=int, default=10,
+                   help="time steps of the transport-only time loop (mixed vs FP64 temperature error); 0 = skip")
     return p.parse_args()
 
 
@@ -203,6 +205,52 @@ def run_tiling_sweep(args):
         finally:
             s.close()
     return 0
+
+
+def run_time_steps(pkg, torch, prob, steps, conv_type=2, conv_ho=1e-10, maxit=20):
+    """The reference's transport-only time loop (run_type 'tr_no_qd') on the device, FP64 and mixed from
+    the same initial state: per step the outer iterations of sweep + moments, MEB_SOLVE,
+    MATERIAL_UPDATE and CONVERGENCE.  Reports the mixed run's temperature and energy error against
+    FP64 after every step and the per-step latency (host wall clock, the loop syncs per iteration)."""
+    ts = pkg.problems.fc_timestep_setup(prob)
+    CU, C = pkg.problems.COMP_UNIT, pkg.problems.C_LIGHT
+    ox, oy, w = prob.directions()
+    res = {}
+    for prec in ("fp64", "fp32"):
+        s = pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng,
+                               precision="mixed" if prec == "fp32" else "fp64")
+        try:
+            s.init_state(ts.Tini_eV, list(ts.bcT_eV), CU, ts.nu_eV)
+            s.tstep_setup(ts.nu_eV, ts.kappa_mult, ts.cv, np.full((prob.nx, prob.ny), ts.Tini_eV), ts.Kap0, CU, C,
+                          ts.dt, bcT=ts.bcT_eV, conv_type=conv_type, conv_ho=conv_ho, maxit_rte=maxit)
+            Ts, Es, its, lat = [], [], [], []
+            for _ in range(steps):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                n_it, _, _ = s.tstep()
+                lat.append((time.perf_counter() - t0) * 1e3)
+                its.append(n_it)
+                Ts.append(s.temperature())
+                Es.append(s.moments(["E_avg"])["E_avg"])
+        finally:
+            s.close()
+        res[prec] = dict(T=Ts, E=Es, its=its, lat=lat)
+    rel = lambda a, b: float(np.max(np.abs(a - b) / np.abs(b)))
+    t_err = [rel(a, b) for a, b in zip(res["fp32"]["T"], res["fp64"]["T"])]
+    e_err = [rel(a, b) for a, b in zip(res["fp32"]["E"], res["fp64"]["E"])]
+    upd = prob.updates_per_sweep()
+    out = {"algorithm": "tr_no_qd: (sweep + moments, MEB_SOLVE, MATERIAL_UPDATE, CONVERGENCE) per outer iteration, "
+                        "on the device",
+           "physics": "Fleck-Cummings kapB_calc x Kappa_Mult(kappa0/min kappa0), Kap0 = 27e9, Cv of INPUTS.f08:121; "
+                      "T in eV", "steps": steps, "conv_type": conv_type, "conv_ho": conv_ho, "maxit_rte": maxit,
+           "T_rel_err_max": max(t_err), "E_rel_err_max": max(e_err), "T_rel_err_per_step": t_err}
+    for prec in ("fp64", "fp32"):
+        r = res[prec]
+        lat = np.array(r["lat"])
+        out[prec] = {"outer_its": r["its"], "step_ms_p50": float(np.percentile(lat, 50)),
+                     "step_ms_p99": float(np.percentile(lat, 99)),
+                     "updates_per_s": float(upd * sum(r["its"]) / (lat.sum() * 1e-3))}
+    return out
 
 
 def setup_instance(pkg, prob, precision, tiling):
@@ -406,6 +454,8 @@ def main():
     dt = ranks.reduce_max(dt)
     line["e2e"] = {"value": ranks.whole_job_rate(upd, dt, ws), "unit": "updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                    "ms_per_step": dt * 1e3, "path": "trt_set_material(host) + trt_sweep + trt_moments(host), pinned"}
+    if args.time_steps > 0:
+        line["time_steps"] = run_time_steps(pkg, torch, prob, args.time_steps)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(prob)
     if rank == 0:
