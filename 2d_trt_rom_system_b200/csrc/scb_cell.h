@@ -137,4 +137,58 @@ TRT_HD void scb_solve(const ScbGeom<float>& G, float gamma, float A4, const floa
   x[3] = tfma(b, y1, tfma(-a, y3, y4)) * inv;
 }
 
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+// Two directions at once on the packed FP32x2 pipe of sm_100 (component .x = one direction, .y =
+// another): the FP32 solve above, operation for operation.  Each packed operation rounds each
+// component as the scalar one does, and negations are multiplications by -1 (exact), so both
+// components are bit-identical to two calls of the scalar solve.
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 frcp2(float2 v) { return make_float2(frcp(v.x), frcp(v.y)); }
+
+struct ScbGeom2 {
+  float2 a, b, hx, hy;
+};
+
+__device__ __forceinline__ ScbGeom2 scb_geom2(float2 ax4, float2 ay4, float dx, float dy) {
+  ScbGeom2 G;
+  G.a = __fmul2_rn(ax4, f2(dy));
+  G.b = __fmul2_rn(ay4, f2(dx));
+  G.hx = __fadd2_rn(G.a, G.a);
+  G.hy = __fadd2_rn(G.b, G.b);
+  return G;
+}
+
+__device__ __forceinline__ float2 scb_gamma2(const ScbGeom2& G, float kA4) {
+  return __fadd2_rn(__fadd2_rn(G.a, G.b), f2(kA4));
+}
+
+__device__ __forceinline__ void scb_solve2(const ScbGeom2& G, float2 gamma, float A4, const float2 s[4], float2 vb,
+                                           float2 vt, float2 hl, float2 hr, float2 x[4]) {
+  const float2 A = f2(A4), one = f2(1.0f), m1 = f2(-1.0f);
+  const float2 Q1 = __ffma2_rn(G.hy, hl, __ffma2_rn(G.hx, vb, __fmul2_rn(A, s[0])));
+  const float2 Q2 = __ffma2_rn(G.hy, hr, __fmul2_rn(A, s[1]));
+  const float2 Q3 = __fmul2_rn(A, s[2]);
+  const float2 Q4 = __ffma2_rn(G.hx, vt, __fmul2_rn(A, s[3]));
+
+  const float2 r = frcp2(gamma);
+  const float2 a = __fmul2_rn(G.a, r), b = __fmul2_rn(G.b, r);
+  const float2 c = __ffma2_rn(a, a, __ffma2_rn(b, b, one));
+  const float2 d = __fmul2_rn(__fadd2_rn(a, a), b);
+  const float2 amb = __ffma2_rn(b, m1, a), apb = __fadd2_rn(a, b);
+  const float2 det = __fmul2_rn(__ffma2_rn(amb, amb, one), __ffma2_rn(apb, apb, one));
+  const float2 inv = __fmul2_rn(r, frcp2(det));
+  const float2 nd = __fmul2_rn(d, m1), na = __fmul2_rn(a, m1), nb = __fmul2_rn(b, m1);
+
+  const float2 y1 = __ffma2_rn(d, Q3, __fmul2_rn(c, Q1));
+  const float2 y2 = __ffma2_rn(nd, Q4, __fmul2_rn(c, Q2));
+  const float2 y3 = __ffma2_rn(d, Q1, __fmul2_rn(c, Q3));
+  const float2 y4 = __ffma2_rn(nd, Q2, __fmul2_rn(c, Q4));
+
+  x[0] = __fmul2_rn(__ffma2_rn(nb, y4, __ffma2_rn(na, y2, y1)), inv);
+  x[1] = __fmul2_rn(__ffma2_rn(nb, y3, __ffma2_rn(a, y1, y2)), inv);
+  x[2] = __fmul2_rn(__ffma2_rn(b, y2, __ffma2_rn(a, y4, y3)), inv);
+  x[3] = __fmul2_rn(__ffma2_rn(b, y1, __ffma2_rn(na, y3, y4)), inv);
+}
+#endif
+
 }  // namespace trt

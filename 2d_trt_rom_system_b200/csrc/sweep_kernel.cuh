@@ -493,8 +493,105 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
       Real topL[kLeanFP32 ? 1 : D], topR[kLeanFP32 ? 1 : D];
       const Real kA4 = scb_kA4(dx, dy, kp);
 
+      // FP32 moment products of one direction slot (FP64 lane sums)
+      auto add_moments = [&](int ml, Real x0, Real x1, Real x2, Real x3) {
+        const double Iavg = (double)(((x0 + x1) + (x2 + x3)) * Real(0.25));
+        const double Iv = (double)((x1 + x2) * Real(0.5));
+        const double Ih = (double)((x3 + x2) * Real(0.5));
+        const double ww = wtab[0 * mqc + ml], wxx = wtab[1 * mqc + ml], wyy = wtab[2 * mqc + ml];
+        const double wxy = wtab[3 * mqc + ml], wx = wtab[4 * mqc + ml], wy = wtab[5 * mqc + ml];
+        acc[kCxx] = fma(wxx, Iavg, acc[kCxx]);
+        acc[kCyy] = fma(wyy, Iavg, acc[kCyy]);
+        acc[kCxy] = fma(wxy, Iavg, acc[kCxy]);
+        acc[kCe] = fma(ww, Iavg, acc[kCe]);
+        acc[kVxx] = fma(wxx, Iv, acc[kVxx]);
+        acc[kVxy] = fma(wxy, Iv, acc[kVxy]);
+        acc[kVx] = fma(wx, Iv, acc[kVx]);
+        acc[kVe] = fma(ww, Iv, acc[kVe]);
+        acc[kHyy] = fma(wyy, Ih, acc[kHyy]);
+        acc[kHxy] = fma(wxy, Ih, acc[kHxy]);
+        acc[kHy] = fma(wy, Ih, acc[kHy]);
+        acc[kHx] = fma(wx, Ih, acc[kHx]);
+        acc[kHe] = fma(ww, Ih, acc[kHe]);
+      };
+      // FP32 outputs of one live direction slot: corner state, outflow boundary faces, row handoff
+      auto store_slot = [&](int d, int ml, Real x0, Real x1, Real x2, Real x3) {
+        Real* gb = gnew + gchunk + d * 128;
+        *reinterpret_cast<float4*>(gb + lane * 4) = make_float4((float)x0, (float)x1, (float)x2, (float)x3);
+        if (right_edge) {
+          bVout[ml * 2 * ny + 2 * j + byo] = x1;
+          bVout[ml * 2 * ny + 2 * j + 1 - byo] = x2;
+        }
+        if (top_edge) {
+          bHout[ml * 2 * nx + 2 * i + bxo] = x3;
+          bHout[ml * 2 * nx + 2 * i + 1 - bxo] = x2;
+        }
+        if (last_row) {
+          hand_dst[ml * 2 + 0] = x3;
+          hand_dst[ml * 2 + 1] = x2;
+        }
+      };
+
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+      // FP32: directions d and d+1 of the lane solved together on the packed FP32x2 pipe (bit-identical
+      // to two scalar solves); every lane computes (idle slots and inactive lanes on valid addresses,
+      // results discarded) so the bottom-inflow shuffles run inline.
+      auto pair = [&](int d) {
+        const bool valid1 = (d + 1 < D - 1) || (s < s_last);
+        const int ml0 = d * S + s, ml1 = valid1 ? (d + 1) * S + s : 0;
+        const int ln1 = valid1 ? lane : 0;
+        const bool live1 = active && valid1;
+        const float4 p0 = *reinterpret_cast<const float4*>(sm + d * 128 + lane * 4);
+        const float4 p1 = *reinterpret_cast<const float4*>(sm + (d + 1) * 128 + ln1 * 4);
+        const float2 io[4] = {make_float2(p0.x, p1.x), make_float2(p0.y, p1.y), make_float2(p0.z, p1.z),
+                              make_float2(p0.w, p1.w)};
+        float2 src[4];
+        if (SRC_FULL) {
+          const Real* gs0 = a.srcfull + blk_off + gchunk + d * 128 + lane * 4;
+          const Real* gs1 = a.srcfull + blk_off + gchunk + (d + 1) * 128 + ln1 * 4;
+  #pragma unroll
+          for (int c = 0; c < 4; ++c)
+            src[c] = __ffma2_rn(io[c], f2(rcdt), make_float2(active ? gs0[c] : 0.0f, live1 ? gs1[c] : 0.0f));
+        } else {
+  #pragma unroll
+          for (int c = 0; c < 4; ++c) src[c] = __ffma2_rn(io[c], f2(rcdt), f2(qs));
+        }
+        const ScbGeom2 G2 = scb_geom2(make_float2(dtab[kAx * mqc + ml0], dtab[kAx * mqc + ml1]),
+                                      make_float2(dtab[kAy * mqc + ml0], dtab[kAy * mqc + ml1]), dx, dy);
+        const float2 gam = scb_gamma2(G2, kA4);
+        float2 x[4];
+        scb_solve2(G2, gam, A4, src, make_float2(vb[d], vb[d + 1]), make_float2(vt[d], vt[d + 1]),
+                   make_float2(hl[d], hl[d + 1]), make_float2(hr[d], hr[d + 1]), x);
+        vb[d] = x[1].x;
+        vb[d + 1] = x[1].y;
+        vt[d] = x[2].x;
+        vt[d + 1] = x[2].y;
+        hl[d] = __shfl_up_sync(0xffffffffu, x[3].x, 1);
+        hl[d + 1] = __shfl_up_sync(0xffffffffu, x[3].y, 1);
+        hr[d] = __shfl_up_sync(0xffffffffu, x[2].x, 1);
+        hr[d + 1] = __shfl_up_sync(0xffffffffu, x[2].y, 1);
+        if (active) {
+          store_slot(d, ml0, x[0].x, x[1].x, x[2].x, x[3].x);
+          add_moments(ml0, x[0].x, x[1].x, x[2].x, x[3].x);
+        }
+        if (live1) {
+          store_slot(d + 1, ml1, x[0].y, x[1].y, x[2].y, x[3].y);
+          add_moments(ml1, x[0].y, x[1].y, x[2].y, x[3].y);
+        }
+      };
+#endif
+
   #pragma unroll
       for (int d = 0; d < D; ++d) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+        if constexpr (kLeanFP32) {
+          if (d % 2 == 0 && d + 1 < D) {
+            pair(d);
+            continue;
+          }
+          if (d % 2 == 1) continue;   // second direction of a pair
+        }
+#endif
         const bool valid = (d < D - 1) || (s < s_last);
         // FP32: every lane computes every slot (idle slots and inactive lanes on valid addresses, results
         // discarded) so the bottom-inflow shuffle runs inline; FP64: only live slots compute.
