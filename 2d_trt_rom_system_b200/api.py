@@ -201,6 +201,14 @@ class TransportSweep:
         check(_lib.lib().trt_set_tiling(self._h, int(warps), int(slices), int(stages), int(splits)),
               "trt_set_tiling")
 
+    def autotune(self):
+        """Pick the fastest tiling by timing one sweep per candidate (re-lays out and zeroes the state:
+        call before init_state / put_state).  Returns the tiling and its sweep time in ms."""
+        w, sl, sp, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0), ctypes.c_float(0)
+        check(_lib.lib().trt_autotune(self._h, ctypes.byref(w), ctypes.byref(sl), ctypes.byref(sp), ctypes.byref(ms)),
+              "trt_autotune")
+        return dict(self.tiling(), sweep_ms=ms.value)
+
     def tiling(self):
         v = [ctypes.c_int(0) for _ in range(5)]
         check(_lib.lib().trt_get_tiling(self._h, *[ctypes.byref(x) for x in v]), "trt_get_tiling")

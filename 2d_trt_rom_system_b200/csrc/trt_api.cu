@@ -111,21 +111,14 @@ bool pick_cfg(int ndir, int prec, int S_req, KernelCfg* out) {
 }
 
 template <class Real>
-cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int grid, int block, size_t smem, cudaStream_t st,
-                         const trt::SweepArgs<Real>& a) {
-#define TRT_SWEEP_CASE(S_, D_)                                                                   \
-  if (kc.S == S_ && kc.D == D_) {                                                                \
-    if (src_full) {                                                                              \
-      auto k = trt::scb_sweep_kernel<Real, S_, D_, true>;                                        \
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);           \
-      k<<<grid, block, smem, st>>>(a);                                                           \
-    } else {                                                                                     \
-      auto k = trt::scb_sweep_kernel<Real, S_, D_, false>;                                       \
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);           \
-      k<<<grid, block, smem, st>>>(a);                                                           \
-    }                                                                                            \
-    return cudaGetLastError();                                                                   \
-  }
+using SweepKernel = void (*)(trt::SweepArgs<Real>);
+
+// The compiled sweep kernel of a (slices, directions per lane) configuration (null if none).
+template <class Real>
+SweepKernel<Real> sweep_kernel_for(const KernelCfg& kc, bool src_full) {
+#define TRT_SWEEP_CASE(S_, D_)                                                                         \
+  if (kc.S == S_ && kc.D == D_)                                                                        \
+    return src_full ? trt::scb_sweep_kernel<Real, S_, D_, true> : trt::scb_sweep_kernel<Real, S_, D_, false>;
   TRT_SWEEP_CASE(1, 2)
   TRT_SWEEP_CASE(1, 4)
   TRT_SWEEP_CASE(2, 2)
@@ -149,7 +142,31 @@ cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int grid, int block
   TRT_SWEEP_CASE(32, 1)
   TRT_SWEEP_CASE(32, 2)
 #undef TRT_SWEEP_CASE
-  return cudaErrorInvalidValue;
+  return nullptr;
+}
+
+template <class Real>
+cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int grid, int block, size_t smem, cudaStream_t st,
+                         const trt::SweepArgs<Real>& a) {
+  SweepKernel<Real> k = sweep_kernel_for<Real>(kc, src_full);
+  if (!k) return cudaErrorInvalidValue;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k<<<grid, block, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+// CTAs of a sweep configuration that are resident on one SM at once (0 on failure).
+template <class Real>
+int sweep_ctas_per_sm(const KernelCfg& kc, int block, size_t smem) {
+  SweepKernel<Real> k = sweep_kernel_for<Real>(kc, false);
+  int n = 0;
+  if (!k) return 0;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, block, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
 }
 
 }  // namespace
@@ -1063,6 +1080,75 @@ void trt_destroy(trt_ctx* c) {
   for (void* p : c->allocs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
+}
+
+int trt_autotune(trt_ctx* c, int* warps_out, int* slices_out, int* splits_out, float* ms_out) {
+  if (!c) return TRT_ERR_ARG;
+  const bool had_material = c->have_material;
+  const size_t ncell = (size_t)c->nx * c->ny * c->ng;
+  if (!had_material) {   // trial sweeps on a zero material
+    TRT_CUDA(cudaMemsetAsync(c->d_kap, 0, ncell * c->esz(), c->stream));
+    TRT_CUDA(cudaMemsetAsync(c->d_q, 0, ncell * c->esz(), c->stream));
+  }
+  cudaEvent_t e0, e1;
+  TRT_CUDA(cudaEventCreate(&e0));
+  TRT_CUDA(cudaEventCreate(&e1));
+  const int sms = sm_count();
+  int bestNH = 0, bestW = 0;
+  float best = 0.0f;
+  const int nhs[] = {1, 2, 3, 4}, ws[] = {2, 3, 4, 5, 6, 8};
+  for (int NH : nhs) {
+    if (NH > c->mq) continue;
+    for (int W : ws) {
+      c->NHreq = NH;
+      c->Wreq = W;
+      c->Sreq = 0;
+      c->stages = 2;
+      if (setup_layout(c) != TRT_OK) continue;
+      // only tilings whose CTAs are all resident at once
+      const size_t smem = c->prec == TRT_PREC_FP64
+                              ? trt::sweep_smem_bytes<double>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D)
+                              : trt::sweep_smem_bytes<float>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D);
+      const int per = c->prec == TRT_PREC_FP64 ? sweep_ctas_per_sm<double>(c->kc, 32 * c->t.W, smem)
+                                               : sweep_ctas_per_sm<float>(c->kc, 32 * c->t.W, smem);
+      if (per <= 0 || 4LL * c->ng * NH > (long long)per * sms) continue;
+      c->have_state = true;
+      c->have_material = true;
+      int rc = c->prec == TRT_PREC_FP64 ? sweep_impl<double>(c, 0) : sweep_impl<float>(c, 0);
+      if (rc) continue;
+      TRT_CUDA(cudaEventRecord(e0, c->stream));
+      for (int k = 0; k < 2 && !rc; ++k) rc = c->prec == TRT_PREC_FP64 ? sweep_impl<double>(c, 0) : sweep_impl<float>(c, 0);
+      TRT_CUDA(cudaEventRecord(e1, c->stream));
+      TRT_CUDA(cudaStreamSynchronize(c->stream));
+      if (rc || check_err(c)) continue;
+      float ms = 0.0f;
+      TRT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      ms *= 0.5f;
+      if (bestNH == 0 || ms < best) {
+        best = ms;
+        bestNH = NH;
+        bestW = W;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->NHreq = bestNH;
+  c->Wreq = bestW;
+  c->Sreq = 0;
+  c->stages = 2;
+  int rc = setup_layout(c);
+  c->have_state = false;
+  c->swept = false;
+  c->have_moments = false;
+  c->have_material = had_material;
+  if (rc) return rc;
+  if (!bestNH) return TRT_ERR_UNSUPPORTED;
+  if (warps_out) *warps_out = c->t.W;
+  if (slices_out) *slices_out = c->t.S;
+  if (splits_out) *splits_out = c->t.NH;
+  if (ms_out) *ms_out = best;
+  return TRT_OK;
 }
 
 int trt_set_tiling(trt_ctx* c, int warps_per_cta, int slices, int stages, int splits) {

@@ -51,6 +51,9 @@ def parse():
     p.add_argument("--n", type=int, default=0, help="grid size override (profiling small cases)")
     p.add_argument("--groups", type=int, default=0, help="group count override (profiling small cases)")
     p.add_argument("--tiling-sweep", action="store_true", help="time the sweep kernel over a set of tilings")
+    p.add_argument("--sweep-prec", default="fp64,fp32", help="precisions of --tiling-sweep")
+    p.add_argument("--no-autotune", dest="autotune", action="store_false",
+                   help="use the library's default tiling instead of trt_autotune")
     p.add_argument("--time-steps", type=int, default=10,
                    help="time steps of the transport-only time loop (mixed vs FP64 temperature error); 0 = skip")
     return p.parse_args()
@@ -175,12 +178,12 @@ def run_tiling_sweep(args):
     pkg, prob = build_problem(args.config, args.n, args.groups)
     upd = prob.updates_per_sweep()
     peak, _ = peaks()
-    for prec in ("fp64", "fp32"):
+    for prec in args.sweep_prec.split(","):
         s, _, _ = setup_instance(pkg, prob, "mixed" if prec == "fp32" else "fp64", None)
         seen = set()
         try:
-            for NH in (1, 2, 3, 4):
-                for W in (2, 4, 6, 8, 12, 16):
+            for NH in (1, 2, 3, 4, 5, 6):
+                for W in (2, 3, 4, 5, 6, 8, 12, 16):
                     for S in (0, 2, 4, 8, 16):
                         for st in (2, 3):
                             try:
@@ -253,11 +256,13 @@ def run_time_steps(pkg, torch, prob, steps, conv_type=2, conv_ho=1e-10, maxit=20
     return out
 
 
-def setup_instance(pkg, prob, precision, tiling):
+def setup_instance(pkg, prob, precision, tiling, autotune=False):
     ox, oy, w = prob.directions()
     s = pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng, precision=precision)
     if tiling:
         s.set_tiling(*tiling)
+    elif autotune:
+        s.autotune()
     s.init_state(prob.T0 * 1e3, [t * 1e3 for t in prob.bcT], pkg.problems.COMP_UNIT, prob.nu_eV)
     # a temperature field between the cold initial state and the hot boundary
     x = (np.arange(prob.nx) + 0.5) / prob.nx
@@ -396,7 +401,7 @@ def main():
     precs = ["fp32"] + ([] if args.no_fp64 else ["fp64"])
     clocks = None
     for prec in precs:
-        s, kap, src = setup_instance(pkg, prob, "mixed" if prec == "fp32" else "fp64", tiling)
+        s, kap, src = setup_instance(pkg, prob, "mixed" if prec == "fp32" else "fp64", tiling, autotune=args.autotune)
         try:
             if prec == "fp32":
                 with ClockSampler(local) as cs:

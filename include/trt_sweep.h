@@ -156,6 +156,13 @@ int trt_set_tiling(trt_ctx* ctx, int warps_per_cta, int slices, int stages, int 
 int trt_get_tiling(const trt_ctx* ctx, int* warps_per_cta, int* slices, int* dirs_per_lane, int* stages,
                    int* splits);
 
+/* Autotuner: times one sweep of this handle's problem for each (direction splits 1..4) x (warps per CTA
+ * 2, 3, 4, 5, 6, 8) tiling whose CTAs are all resident at once (CUDA occupancy query), with the
+ * default slices per warp, and keeps the fastest.  Uses the handle's material if set, else a zero
+ * material.  Call before trt_init_state / trt_put_state: it re-lays out (and zeroes) the state.
+ * Outputs (each may be NULL): the chosen warps, slices, splits and its sweep time in ms. */
+int trt_autotune(trt_ctx* ctx, int* warps_per_cta, int* slices, int* splits, float* sweep_ms);
+
 /* Material for the next sweeps: KapE_in(n_x,n_y,n_g) (the opacity before the 1/(c*Delt) term of
  * TRANSPORT_SOLVES.f08:47) and the isotropic corner source src_iso(n_x,n_y,n_g) = KapB*Bg
  * (UPDATES.f08:141-150).  c and Delt as passed to TRANSPORT_SCB; Comp_Unit as passed to

@@ -418,3 +418,20 @@ def test_launch_counter_counts_library_kernels():
     with resident(d) as s:
         s.sweep(moments=True)
     assert pkg.kernel_launches() - before >= 3
+
+
+def test_autotune_picks_a_resident_tiling_and_keeps_results(oracle):
+    prob = pkg.problems.random_small(30, 33, 29, 3, "S16")
+    d = sweep_inputs(prob, seed=30)
+    ref = oracle_full(d, solver=1)
+    nx, ny, ng = len(d["Delx"]), len(d["Dely"]), d["KapE_in"].shape[2]
+    with pkg.TransportSweep(nx, ny, d["Omega_x"], d["Omega_y"], d["w"], d["Delx"], d["Dely"], ng) as s:
+        t = s.autotune()
+        assert t["splits"] in (1, 2, 3, 4) and t["warps"] in (2, 3, 4, 5, 6, 8) and t["sweep_ms"] > 0
+        s.put_state(d["I_crn_old"])
+        s.set_boundary(d["Ic_edgV"], d["Ic_edgH"], (0, 0, 0, 0))
+        s.set_material(d["KapE_in"], d["src_iso"], d["c"], d["dt"], CU)
+        s.sweep(moments=True)
+        assert np.array_equal(s.get_state(), ref["I_crn"])
+        m = s.moments(["Eg_avg", "E_avg"])
+    assert moment_err(m, ref, "Eg_avg") < 1e-13
