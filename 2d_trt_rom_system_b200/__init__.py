@@ -4,7 +4,7 @@ jmc9/2D_TRT_ROM_System (drop-in for MODULE TRANSPORT_SOLVES and the QD-factor ro
 The compute path is libtrt_sweep.so (CUDA, sm_100a) behind the C ABI of include/trt_sweep.h; this
 package is its Python mirror plus the problem and quadrature generators used by tests and the bench.
 """
-from . import problems, quadrature, ranks  # noqa: F401
+from . import problems, quadrature, ranks, serving  # noqa: F401
 from .api import (COLLAPSE_INTENSITIES, GQD_In_Calc, MGQD_In_Calc, RT_BC_UPDATE, TRANSPORT_SCB,  # noqa: F401
                   Bg_planck_calc, Cg_Calc, TransportSweep, fg_Calc, kernel_launches, required_bytes)
 from ._lib import LIB_PATH, TrtError, check, lib  # noqa: F401

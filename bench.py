@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--groups", type=int, default=0, help="group count override (profiling small cases)")
     p.add_argument("--tiling-sweep", action="store_true", help="time the sweep kernel over a set of tilings")
     p.add_argument("--sweep-prec", default="fp64,fp32", help="precisions of --tiling-sweep")
+    p.add_argument("--serving", type=float, default=0.0,
+                   help="arrival window (s) of a config-3 request stream served after the step timing; 0 = skip")
     p.add_argument("--no-autotune", dest="autotune", action="store_false",
                    help="use the library's default tiling instead of trt_autotune")
     p.add_argument("--time-steps", type=int, default=10,
@@ -253,6 +255,20 @@ def run_time_steps(pkg, torch, prob, steps, conv_type=2, conv_ho=1e-10, maxit=20
         out[prec] = {"outer_its": r["its"], "step_ms_p50": float(np.percentile(lat, 50)),
                      "step_ms_p99": float(np.percentile(lat, 99)),
                      "updates_per_s": float(upd * sum(r["its"]) / (lat.sum() * 1e-3))}
+    return out
+
+
+def run_serving(pkg, window_s, rate=200.0, budget_gb=120.0):
+    """Config-3 request stream (Poisson arrivals at `rate`/s, seed 3) over a `window_s` arrival window,
+    admitted against a `budget_gb` HBM budget; mixed and FP64 served separately."""
+    out = {"rate_per_s": rate, "arrival_window_s": window_s, "hbm_budget_gb": budget_gb,
+           "per_request": "10 backward-Euler steps of the transport-only loop, 4 outer iterations per step"}
+    for prec in ("mixed", "fp64"):
+        reqs = pkg.serving.config3_requests(rate=rate, duration=window_s, seed=3, precision=prec)
+        res, log = pkg.serving.Server(hbm_budget=int(budget_gb * 1e9), max_active=64).run(reqs)
+        summ = pkg.serving.latency_summary(res)
+        summ["max_concurrent_gb"] = max(e[2] for e in log) / 1e9
+        out[prec] = summ
     return out
 
 
@@ -461,6 +477,8 @@ def main():
                    "ms_per_step": dt * 1e3, "path": "trt_set_material(host) + trt_sweep + trt_moments(host), pinned"}
     if args.time_steps > 0:
         line["time_steps"] = run_time_steps(pkg, torch, prob, args.time_steps)
+    if args.serving > 0 and ws == 1:
+        line["serving"] = run_serving(pkg, args.serving)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(prob)
     if rank == 0:
