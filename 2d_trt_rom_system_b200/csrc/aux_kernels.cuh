@@ -63,20 +63,16 @@ __global__ void unpack_state_kernel(Geo G, const Real* __restrict__ skew, double
   }
 }
 
-// Fill every slot of a skewed buffer that belongs to a cell with one value per (cell, g)
-// (used to initialise the state to B_g(T_ini) as RT_INIT does, INITIALIZERS.f08:84-92).
+// Fill a whole skewed state with one value per group (used to initialise the state to B_g(T_ini) as
+// RT_INIT does, INITIALIZERS.f08:84-92).  The (g, q, h) blocks of group g are contiguous, so this is a
+// streaming store; slots that hold no (cell, direction) get the value too, which is harmless because
+// the sweep never uses them as data.
 template <class Real>
-__global__ void fill_state_kernel(Geo G, const double* __restrict__ per_g, Real* __restrict__ skew) {
-  const long long n = 4LL * G.nx * G.ny * G.nm * G.ng;
-  const long long nxx = 2LL * G.nx, nyy = 2LL * G.ny;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-    long long r = k;
-    const int ix = (int)(r % nxx); r /= nxx;
-    const int iy = (int)(r % nyy); r /= nyy;
-    const int m = (int)(r % G.nm); r /= G.nm;
-    const int g = (int)r;
-    skew[state_index<Real>(G, ix >> 1, iy >> 1, ix & 1, iy & 1, m, g)] = (Real)per_g[g];
-  }
+__global__ void fill_groups_kernel(long long per_group, int ng, const double* __restrict__ per_g,
+                                   Real* __restrict__ skew) {
+  const long long n = per_group * ng;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    skew[k] = (Real)per_g[k / per_group];
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -657,9 +657,10 @@ int init_state_impl(trt_ctx* c, double Tini, const double* Tb, double cu, const 
   int rc = alloc_t(c, &d_pg, c->ng);
   if (rc) return rc;
   TRT_CUDA(cudaMemcpyAsync(d_pg, per_g.data(), c->ng * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  const long long n = 4LL * c->nx * c->ny * c->nm * c->ng;
+  const long long per_group = 4LL * c->t.NH * c->blk;
   for (int k = 0; k < 2; ++k) {
-    trt::fill_state_kernel<Real><<<grid_for(n), 256, 0, c->stream>>>(c->geo(), d_pg, (Real*)c->d_state[k]);
+    trt::fill_groups_kernel<Real><<<grid_for(per_group * c->ng), 256, 0, c->stream>>>(per_group, c->ng, d_pg,
+                                                                                       (Real*)c->d_state[k]);
     TRT_LAUNCHED();
     TRT_CUDA(cudaGetLastError());
   }

@@ -183,6 +183,7 @@ def latency_summary(results):
     solves = np.array([r.solve_s * 1e3 for r in ok]) if ok else np.zeros(1)
     span = (max(r.finished_s for r in ok) - min(r.arrival_s for r in ok)) if ok else 1.0
     return {"requests": len(results), "failed": len(results) - len(ok),
+            "errors": sorted({r.error for r in results if r.error})[:3],
             "step_ms_p50": float(np.percentile(steps, 50)), "step_ms_p99": float(np.percentile(steps, 99)),
             "solve_ms_p50": float(np.percentile(solves, 50)), "solve_ms_p99": float(np.percentile(solves, 99)),
             "updates_per_s": float(sum(r.updates for r in ok) / span), "span_s": float(span)}
