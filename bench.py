@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--sweep-prec", default="fp64,fp32", help="precisions of --tiling-sweep")
     p.add_argument("--serving", type=float, default=0.0,
                    help="arrival window (s) of a config-3 request stream served after the step timing; 0 = skip")
+    p.add_argument("--batch", type=int, default=0,
+                   help="instances of a config-2 batch run concurrently (mixed) and sequentially (FP64); 0 = skip")
     p.add_argument("--no-autotune", dest="autotune", action="store_false",
                    help="use the library's default tiling instead of trt_autotune")
     p.add_argument("--time-steps", type=int, default=10,
@@ -272,6 +274,24 @@ def run_serving(pkg, window_s, rate=200.0, budget_gb=120.0):
     return out
 
 
+def run_batch(pkg, count, budget_gb=120.0):
+    """Config 2: `count` independent instances (seed 2) all submitted at once, mixed precision, run
+    concurrently under a `budget_gb` HBM budget, against the same instances solved one after another in
+    plain FP64."""
+    out = {"instances": count, "hbm_budget_gb": budget_gb,
+           "per_instance": "10 backward-Euler steps of the transport-only loop, 4 outer iterations per step"}
+    for name, prec, active in (("mixed_concurrent", "mixed", 64), ("fp64_sequential", "fp64", 1)):
+        reqs = pkg.serving.config2_batch(count, precision=prec)
+        t0 = time.perf_counter()
+        res, log = pkg.serving.Server(hbm_budget=int(budget_gb * 1e9), max_active=active).run(reqs, realtime=False)
+        wall = time.perf_counter() - t0
+        summ = pkg.serving.latency_summary(res)
+        summ["wall_s"] = wall
+        out[name] = summ
+    out["speedup_updates_per_s"] = out["mixed_concurrent"]["updates_per_s"] / out["fp64_sequential"]["updates_per_s"]
+    return out
+
+
 def setup_instance(pkg, prob, precision, tiling, autotune=False):
     ox, oy, w = prob.directions()
     s = pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng, precision=precision)
@@ -479,6 +499,8 @@ def main():
         line["time_steps"] = run_time_steps(pkg, torch, prob, args.time_steps)
     if args.serving > 0 and ws == 1:
         line["serving"] = run_serving(pkg, args.serving)
+    if args.batch > 0 and ws == 1:
+        line["batched"] = run_batch(pkg, args.batch)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(prob)
     if rank == 0:
