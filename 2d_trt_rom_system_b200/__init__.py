@@ -6,5 +6,5 @@ package is its Python mirror plus the problem and quadrature generators used by 
 """
 from . import problems, quadrature, ranks, serving  # noqa: F401
 from .api import (COLLAPSE_INTENSITIES, GQD_In_Calc, MGQD_In_Calc, RT_BC_UPDATE, TRANSPORT_SCB,  # noqa: F401
-                  Bg_planck_calc, Cg_Calc, TransportSweep, fg_Calc, kernel_launches, required_bytes)
+                  Batch, Bg_planck_calc, Cg_Calc, TransportSweep, fg_Calc, kernel_launches, required_bytes)
 from ._lib import LIB_PATH, TrtError, check, lib  # noqa: F401

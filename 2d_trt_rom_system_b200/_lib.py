@@ -99,6 +99,11 @@ SIGNATURES = {
     "trt_set_wait_limit_zero": (_i, [_P]),
     "trt_device_output": (_P, [_P, ctypes.c_char_p]),
     "trt_autotune": (_i, [_P, _I, _I, _I, ctypes.POINTER(ctypes.c_float)]),
+    "trt_batch_create": (_P, [ctypes.POINTER(_P), _i, _I]),
+    "trt_batch_destroy": (None, [_P]),
+    "trt_batch_sweep": (_i, [_P, ctypes.c_uint]),
+    "trt_batch_sync": (_i, [_P]),
+    "trt_batch_tstep": (_i, [_P, _I, _D, _D]),
     "trt_tstep_setup": (_i, [_P, _D, _D, _D, _D, _d, _d, _d, _d, _I, _D, _i, _d, _i]),
     "trt_tstep": (_i, [_P, _I, _D, _D]),
     "trt_get_temperature": (_i, [_P, _D]),

@@ -333,3 +333,50 @@ def required_bytes(nx, ny, nm, ng, precision="fp64"):
 
 def kernel_launches():
     return int(_lib.lib().trt_kernel_launches())
+
+
+class Batch:
+    """Many TransportSweep handles stepped together: the sweeps of handles that share a tiling class
+    run as one kernel launch over all their (handle, group, quadrant, split) CTAs.  Results are
+    bit-identical to stepping each handle alone.  The handles stay owned by the caller and must
+    outlive the batch."""
+
+    def __init__(self, sweeps):
+        self.sweeps = list(sweeps)
+        arr = (ctypes.c_void_p * len(self.sweeps))(*[s.handle for s in self.sweeps])
+        st = ctypes.c_int(0)
+        self._b = _lib.lib().trt_batch_create(arr, len(self.sweeps), ctypes.byref(st))
+        if not self._b:
+            raise _lib.TrtError(st.value, "trt_batch_create")
+
+    def close(self):
+        if getattr(self, "_b", None):
+            _lib.lib().trt_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def sweep(self, roll=False, moments=True, sync=True):
+        flags = (_lib.TRT_ROLL_STATE if roll else 0) | (_lib.TRT_MOMENTS if moments else 0)
+        check(_lib.lib().trt_batch_sweep(self._b, flags), "trt_batch_sweep")
+        if sync:
+            check(_lib.lib().trt_batch_sync(self._b), "trt_batch_sync")
+
+    def tstep(self):
+        """One time step of every handle's transport-only loop; returns (iterations, T norms, E norms)."""
+        n = len(self.sweeps)
+        its = np.zeros(n, dtype=np.int32)
+        tn = np.zeros(n)
+        en = np.zeros(n)
+        check(_lib.lib().trt_batch_tstep(self._b, iptr(its), dptr(tn), dptr(en)), "trt_batch_tstep")
+        return its, tn, en

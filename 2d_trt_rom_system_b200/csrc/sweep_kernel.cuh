@@ -126,8 +126,10 @@ __device__ __forceinline__ int slice_reduce_scatter(double (&v)[16], int s, bool
 //    bottom-inflow shuffle runs inline (no per-direction top-face registers);
 //  * FP64: global inflows loaded at the step start, only live slots compute, top faces kept in
 //    registers and shuffled after the direction loop (fits 128 registers without spills).
+// The sweep of one CTA: (group, quadrant, direction split) number `bid` of the instance described by
+// `a` (blockIdx.x for a single-instance launch; the instance-local number in a batched launch).
 template <class Real, int S, int D, bool SRC_FULL>
-__global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a) {
+__device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const int bid) {
   constexpr bool kLeanFP32 = sizeof(Real) == 4;
   constexpr int R = 32 / S;
   constexpr int NV = 16 / (int)sizeof(Real);
@@ -136,7 +138,7 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   const Tiling t = a.t;
   const int W = t.W;
   const int nx = a.nx, ny = a.ny, nm = a.nm, ng = a.ng, mq = a.mq;
-  const int h = blockIdx.x % t.NH, g = (blockIdx.x / t.NH) >> 2, q = (blockIdx.x / t.NH) & 3;
+  const int h = bid % t.NH, g = (bid / t.NH) >> 2, q = (bid / t.NH) & 3;
   const int mqc = t.mqc;                           // chunk width (directions of the largest split)
   const int mo = split_first(mq, t.NH, h);         // first quadrant-local direction of this split
   const int mq_h = split_count(mq, t.NH, h);       // directions of this split
@@ -179,7 +181,7 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
   }
   __syncthreads();
 
-  const long long blk_off = (long long)blockIdx.x * a.blk;
+  const long long blk_off = (long long)bid * a.blk;
   const Real* gold = a.Iold + blk_off;
   Real* gnew = a.Inew + blk_off;
   const int Tsteps = t.Tsteps;
@@ -193,7 +195,7 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
 
   const Real rcdt = a.rcdt;
   const int nxy = nx * ny;
-  Real* wrapc = a.wrap + (size_t)blockIdx.x * nx * mqc * 2;
+  Real* wrapc = a.wrap + (size_t)bid * nx * mqc * 2;
   constexpr int kRec = part_rec<Real>();
   Real* partg = a.part + ((size_t)((q * t.NH + h) * ng + g) * nxy) * kRec;
   const int sideVin = fx ? 1 : 0, sideVout = fx ? 0 : 1;
@@ -780,6 +782,33 @@ __global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a)
     }
     __syncthreads();
   }
+}
+
+template <class Real, int S, int D, bool SRC_FULL>
+__global__ void __launch_bounds__(512) scb_sweep_kernel(const SweepArgs<Real> a) {
+  scb_sweep_body<Real, S, D, SRC_FULL>(a, blockIdx.x);
+}
+
+// One launch over the CTAs of several instances (same precision, slices, directions per lane, warps
+// per CTA and stages): instance k owns CTAs [first[k], first[k+1]).  Its arguments are copied to
+// shared memory once; the block scheduler then drains the (instance, group, quadrant, split) CTAs.
+template <class Real, int S, int D, bool SRC_FULL>
+__global__ void __launch_bounds__(512) scb_sweep_batch_kernel(const SweepArgs<Real>* __restrict__ args,
+                                                              const int* __restrict__ first, int n) {
+  __shared__ SweepArgs<Real> sa;
+  __shared__ int sbid;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (first[mid] <= (int)blockIdx.x) lo = mid;
+      else hi = mid - 1;
+    }
+    sa = args[lo];
+    sbid = (int)blockIdx.x - first[lo];
+  }
+  __syncthreads();
+  scb_sweep_body<Real, S, D, SRC_FULL>(sa, sbid);
 }
 
 }  // namespace trt

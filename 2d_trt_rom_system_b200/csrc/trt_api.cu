@@ -146,6 +146,41 @@ SweepKernel<Real> sweep_kernel_for(const KernelCfg& kc, bool src_full) {
 }
 
 template <class Real>
+using SweepBatchKernel = void (*)(const trt::SweepArgs<Real>*, const int*, int);
+
+// The batched sweep kernel of a configuration (null if none).
+template <class Real>
+SweepBatchKernel<Real> sweep_batch_kernel_for(const KernelCfg& kc, bool src_full) {
+#define TRT_SWEEP_CASE(S_, D_)                                                                         \
+  if (kc.S == S_ && kc.D == D_)                                                                        \
+    return src_full ? trt::scb_sweep_batch_kernel<Real, S_, D_, true> : trt::scb_sweep_batch_kernel<Real, S_, D_, false>;
+  TRT_SWEEP_CASE(1, 2)
+  TRT_SWEEP_CASE(1, 4)
+  TRT_SWEEP_CASE(2, 2)
+  TRT_SWEEP_CASE(2, 3)
+  TRT_SWEEP_CASE(2, 5)
+  TRT_SWEEP_CASE(2, 9)
+  TRT_SWEEP_CASE(4, 1)
+  TRT_SWEEP_CASE(4, 2)
+  TRT_SWEEP_CASE(4, 3)
+  TRT_SWEEP_CASE(4, 5)
+  TRT_SWEEP_CASE(4, 6)
+  TRT_SWEEP_CASE(4, 9)
+  TRT_SWEEP_CASE(8, 1)
+  TRT_SWEEP_CASE(8, 2)
+  TRT_SWEEP_CASE(8, 3)
+  TRT_SWEEP_CASE(8, 4)
+  TRT_SWEEP_CASE(8, 5)
+  TRT_SWEEP_CASE(16, 1)
+  TRT_SWEEP_CASE(16, 2)
+  TRT_SWEEP_CASE(16, 3)
+  TRT_SWEEP_CASE(32, 1)
+  TRT_SWEEP_CASE(32, 2)
+#undef TRT_SWEEP_CASE
+  return nullptr;
+}
+
+template <class Real>
 cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int grid, int block, size_t smem, cudaStream_t st,
                          const trt::SweepArgs<Real>& a) {
   SweepKernel<Real> k = sweep_kernel_for<Real>(kc, src_full);
@@ -483,8 +518,7 @@ int check_err(trt_ctx* c) {
 }
 
 template <class Real>
-int sweep_impl(trt_ctx* c, unsigned flags) {
-  if (flags & TRT_ROLL_STATE) c->cur = 1 - c->cur;   // I_crn_old <- I_crn (ALGORITHMS.f08:397)
+trt::SweepArgs<Real> make_sweep_args(const trt_ctx* c) {
   trt::SweepArgs<Real> a{};
   a.nx = c->nx; a.ny = c->ny; a.nm = c->nm; a.ng = c->ng; a.mq = c->mq;
   a.t = c->t;
@@ -509,12 +543,32 @@ int sweep_impl(trt_ctx* c, unsigned flags) {
   a.err = c->d_err;
   a.max_polls = c->wait_polls;
   a.drain_polls = 1u << 24;
-  const size_t smem = trt::sweep_smem_bytes<Real>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D);
-  cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, 4 * c->ng * c->t.NH, 32 * c->t.W, smem, c->stream, a);
+  return a;
+}
+
+template <class Real>
+size_t sweep_smem(const trt_ctx* c) {
+  return trt::sweep_smem_bytes<Real>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D);
+}
+
+template <class Real>
+int sweep_epilogue(trt_ctx* c, unsigned flags);
+
+template <class Real>
+int sweep_impl(trt_ctx* c, unsigned flags) {
+  if (flags & TRT_ROLL_STATE) c->cur = 1 - c->cur;   // I_crn_old <- I_crn (ALGORITHMS.f08:397)
+  const trt::SweepArgs<Real> a = make_sweep_args<Real>(c);
+  cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, 4 * c->ng * c->t.NH, 32 * c->t.W, sweep_smem<Real>(c),
+                                     c->stream, a);
   TRT_LAUNCHED();
   if (e != cudaSuccess) return TRT_ERR_CUDA;
   c->swept = true;
+  return sweep_epilogue<Real>(c, flags);
+}
 
+// Moments / QD factors and residual norms after a sweep (on the handle's stream).
+template <class Real>
+int sweep_epilogue(trt_ctx* c, unsigned flags) {
   if (flags & TRT_MOMENTS) {
     trt::CombineArgs A{};
     A.nx = c->nx; A.ny = c->ny; A.nm = c->nm; A.ng = c->ng; A.mq = c->mq; A.nh = c->t.NH;
@@ -927,55 +981,74 @@ bool convergence(int conv_type, double eps, const double* r, int its, double* no
   return !(nrm > new_eps);
 }
 
-template <class Real>
-int tstep_impl(trt_ctx* c, int* its_out, double* tnorm_out, double* enorm_out) {
-  const size_t nxy = (size_t)c->nx * c->ny;
-  const size_t bytes = nxy * sizeof(double);
-  // moving last time step data to the _old arrays (ALGORITHMS.f08:395-396) and resetting the
-  // outer-iteration history (:518-521)
+// Phases of one time step of the transport-only loop, shared by the single-handle and batched drivers.
+// Start of a step: Temp_old <- Temp (ALGORITHMS.f08:395-396) and the outer-iteration history reset
+// (:518-521).
+int tstep_begin(trt_ctx* c) {
+  const size_t bytes = (size_t)c->nx * c->ny * sizeof(double);
   TRT_CUDA(cudaMemcpyAsync(c->d_Told, c->d_T, bytes, cudaMemcpyDeviceToDevice, c->stream));
   for (double* p : {c->d_Trt1, c->d_Trt2, c->d_Ert1, c->d_Ert2}) TRT_CUDA(cudaMemsetAsync(p, 0, bytes, c->stream));
+  return TRT_OK;
+}
+
+// After an outer iteration's sweep and moments: RT_BC_UPDATE on reflective sides, MEB_SOLVE with the
+// transport group energies (:666), MATERIAL_UPDATE (:668) and the convergence reductions of T and the
+// transport E (:816-818), whose 10 values are copied to `host` (read after the stream synchronises).
+template <class Real>
+int tstep_after_sweep(trt_ctx* c, unsigned long long* host) {
+  const size_t nxy = (size_t)c->nx * c->ny;
   const bool reflective = c->ts_bc[0] > 0 || c->ts_bc[1] > 0 || c->ts_bc[2] > 0 || c->ts_bc[3] > 0;
+  int rc;
+  if (reflective && (rc = bc_update_impl<Real>(c, c->ts_bc, c->ts_Tb, c->comp_unit, c->ts_nu.data()))) return rc;
+  trt::meb_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>(c->nx, c->ny, c->ng, c->dout.Eg_avg, c->d_kap64,
+                                                                    c->d_Told, c->d_cv, c->dt, c->ts_Kap0,
+                                                                    c->comp_unit, c->d_T);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  if ((rc = material_update_impl<Real>(c))) return rc;
+  static const unsigned long long init[10] = {0, 0, 0, 0x7ff0000000000000ULL, 0, 0, 0, 0, 0x7ff0000000000000ULL, 0};
+  TRT_CUDA(cudaMemcpyAsync(c->d_conv, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+  trt::conv_reduce_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>((long long)nxy, c->d_T, c->d_Trt1,
+                                                                            c->d_Trt2, c->d_conv);
+  TRT_LAUNCHED();
+  trt::conv_reduce_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>((long long)nxy, c->dout.E_avg, c->d_Ert1,
+                                                                            c->d_Ert2, c->d_conv + 5);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  TRT_CUDA(cudaMemcpyAsync(host, c->d_conv, 10 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+  return TRT_OK;
+}
+
+// With the reductions on the host: CONVERGENCE of T and E, then current iterate -> last iterate (:834-837).
+bool tstep_decide(trt_ctx* c, const unsigned long long* host, int its, double* tn, double* en) {
+  double r[10];
+  std::memcpy(r, host, sizeof(r));
+  const bool tconv = convergence(c->ts_conv_type, c->ts_conv_ho, r, its, tn);
+  const bool econv = convergence(c->ts_conv_type, c->ts_conv_ho, r + 5, its, en);
+  const size_t bytes = (size_t)c->nx * c->ny * sizeof(double);
+  cudaMemcpyAsync(c->d_Ert2, c->d_Ert1, bytes, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->d_Ert1, c->dout.E_avg, bytes, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->d_Trt2, c->d_Trt1, bytes, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->d_Trt1, c->d_T, bytes, cudaMemcpyDeviceToDevice, c->stream);
+  return tconv && econv;
+}
+
+template <class Real>
+int tstep_impl(trt_ctx* c, int* its_out, double* tnorm_out, double* enorm_out) {
+  int rc = tstep_begin(c);
+  if (rc) return rc;
   int its = 0;
   bool conv = false;
   double tn = 0.0, en = 0.0;
-  const unsigned long long init[10] = {0, 0, 0, 0x7ff0000000000000ULL, 0, 0, 0, 0, 0x7ff0000000000000ULL, 0};
+  unsigned long long h[10];
   while (!conv && its < c->ts_maxit) {
     ++its;
     // RTE solve with the collapse, fg and Cg (:547-569); I_crn_old <- I_crn only on the first
-    int rc = sweep_impl<Real>(c, (its == 1 ? TRT_ROLL_STATE : 0u) | TRT_MOMENTS);
-    if (rc) return rc;
-    if (reflective && (rc = bc_update_impl<Real>(c, c->ts_bc, c->ts_Tb, c->comp_unit, c->ts_nu.data()))) return rc;
-    // MEB_SOLVE with the transport group energies (:666), then MATERIAL_UPDATE (:668)
-    trt::meb_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>(c->nx, c->ny, c->ng, c->dout.Eg_avg, c->d_kap64,
-                                                                      c->d_Told, c->d_cv, c->dt, c->ts_Kap0,
-                                                                      c->comp_unit, c->d_T);
-    TRT_LAUNCHED();
-    TRT_CUDA(cudaGetLastError());
-    if ((rc = material_update_impl<Real>(c))) return rc;
-    // convergence of T and of the transport E (:816-818)
-    TRT_CUDA(cudaMemcpyAsync(c->d_conv, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
-    trt::conv_reduce_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>((long long)nxy, c->d_T, c->d_Trt1,
-                                                                              c->d_Trt2, c->d_conv);
-    TRT_LAUNCHED();
-    trt::conv_reduce_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>((long long)nxy, c->dout.E_avg,
-                                                                              c->d_Ert1, c->d_Ert2, c->d_conv + 5);
-    TRT_LAUNCHED();
-    TRT_CUDA(cudaGetLastError());
-    unsigned long long h[10];
-    TRT_CUDA(cudaMemcpyAsync(h, c->d_conv, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = sweep_impl<Real>(c, (its == 1 ? TRT_ROLL_STATE : 0u) | TRT_MOMENTS))) return rc;
+    if ((rc = tstep_after_sweep<Real>(c, h))) return rc;
     TRT_CUDA(cudaStreamSynchronize(c->stream));
     if ((rc = check_err(c))) return rc;
-    double r[10];
-    std::memcpy(r, h, sizeof(r));
-    const bool tconv = convergence(c->ts_conv_type, c->ts_conv_ho, r, its, &tn);
-    const bool econv = convergence(c->ts_conv_type, c->ts_conv_ho, r + 5, its, &en);
-    conv = tconv && econv;
-    // current iterate -> last iterate (:834-837)
-    TRT_CUDA(cudaMemcpyAsync(c->d_Ert2, c->d_Ert1, bytes, cudaMemcpyDeviceToDevice, c->stream));
-    TRT_CUDA(cudaMemcpyAsync(c->d_Ert1, c->dout.E_avg, bytes, cudaMemcpyDeviceToDevice, c->stream));
-    TRT_CUDA(cudaMemcpyAsync(c->d_Trt2, c->d_Trt1, bytes, cudaMemcpyDeviceToDevice, c->stream));
-    TRT_CUDA(cudaMemcpyAsync(c->d_Trt1, c->d_T, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    conv = tstep_decide(c, h, its, &tn, &en);
   }
   TRT_CUDA(cudaStreamSynchronize(c->stream));
   if (its_out) *its_out = its;
@@ -986,7 +1059,295 @@ int tstep_impl(trt_ctx* c, int* its_out, double* tnorm_out, double* enorm_out) {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------------------------
+// Batched instances: one sweep launch per tiling class over the CTAs of many handles.
+// ---------------------------------------------------------------------------------------------
+struct trt_batch {
+  std::vector<trt_ctx*> h;
+  cudaStream_t stream = nullptr;             // epilogues and the time-loop kernels of every handle
+  std::vector<cudaStream_t> gstreams;        // one per launch group (their sweeps overlap)
+  std::vector<cudaEvent_t> gevents;
+  cudaEvent_t start = nullptr;
+  void* d_args = nullptr;                    // SweepArgs of every handle, grouped
+  size_t d_args_cap = 0;
+  int* d_first = nullptr;                    // first CTA of each handle in its group's launch
+  size_t d_first_cap = 0;
+  unsigned char* h_args = nullptr;           // pinned staging of d_args / d_first
+  size_t h_args_cap = 0;
+  unsigned long long* h_norms = nullptr;     // pinned, 10 convergence values per handle
+};
+
+namespace {
+
+// Run a handle's own calls on another stream for the lifetime of this object.
+struct StreamSwap {
+  trt_ctx* c;
+  cudaStream_t old;
+  StreamSwap(trt_ctx* ctx, cudaStream_t s) : c(ctx), old(ctx->stream) { c->stream = s; }
+  ~StreamSwap() { c->stream = old; }
+};
+
+template <class Real>
+int batch_group_launch(trt_batch* b, std::vector<trt_ctx*>& grp, size_t args_off, size_t first_off, size_t done,
+                       cudaStream_t gs) {
+  // largest CTAs first: the block scheduler then starts the long sweeps before the short ones
+  std::stable_sort(grp.begin(), grp.end(), [](const trt_ctx* x, const trt_ctx* y) {
+    return (long long)x->t.Tsteps * x->t.D > (long long)y->t.Tsteps * y->t.D;
+  });
+  auto* ha = reinterpret_cast<trt::SweepArgs<Real>*>(b->h_args + args_off);
+  auto* hf = reinterpret_cast<int*>(b->h_args + first_off);
+  long long total = 0;
+  size_t smem = 0;
+  for (size_t k = 0; k < grp.size(); ++k) {
+    ha[k] = make_sweep_args<Real>(grp[k]);
+    hf[k] = (int)total;
+    total += 4LL * grp[k]->ng * grp[k]->t.NH;
+    smem = std::max(smem, sweep_smem<Real>(grp[k]));
+    grp[k]->swept = true;
+  }
+  if (total > (1LL << 30)) return TRT_ERR_ARG;
+  auto* da = reinterpret_cast<trt::SweepArgs<Real>*>(static_cast<unsigned char*>(b->d_args) + args_off);
+  int* df = b->d_first + done;   // the device copy holds only the first-CTA table
+  TRT_CUDA(cudaMemcpyAsync(da, ha, grp.size() * sizeof(trt::SweepArgs<Real>), cudaMemcpyHostToDevice, gs));
+  TRT_CUDA(cudaMemcpyAsync(df, hf, grp.size() * sizeof(int), cudaMemcpyHostToDevice, gs));
+  SweepBatchKernel<Real> k = sweep_batch_kernel_for<Real>(grp[0]->kc, grp[0]->use_srcfull);
+  if (!k) return TRT_ERR_UNSUPPORTED;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k<<<(unsigned)total, 32 * grp[0]->t.W, smem, gs>>>(da, df, (int)grp.size());
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  return TRT_OK;
+}
+
+// Sweep the handles act (rolling the state of those with roll[k]) in one launch per tiling class;
+// on return b->stream is ordered after every sweep.
+int batch_sweep_launch(trt_batch* b, const std::vector<int>& act, const std::vector<char>& roll) {
+  TRT_CUDA(cudaStreamSynchronize(b->stream));   // the staging buffers of the previous launch are free
+  struct Key {
+    int prec, S, D, W, stages, srcfull;
+    bool operator==(const Key& o) const {
+      return prec == o.prec && S == o.S && D == o.D && W == o.W && stages == o.stages && srcfull == o.srcfull;
+    }
+  };
+  std::vector<Key> keys;
+  std::vector<std::vector<trt_ctx*>> groups;
+  for (size_t i = 0; i < act.size(); ++i) {
+    trt_ctx* c = b->h[act[i]];
+    if (roll[i]) c->cur = 1 - c->cur;   // I_crn_old <- I_crn (ALGORITHMS.f08:397)
+    const Key key{c->prec, c->kc.S, c->kc.D, c->t.W, c->stages, c->use_srcfull ? 1 : 0};
+    size_t g = 0;
+    while (g < keys.size() && !(keys[g] == key)) ++g;
+    if (g == keys.size()) {
+      keys.push_back(key);
+      groups.emplace_back();
+    }
+    groups[g].push_back(c);
+  }
+  // staging: args (max of both precisions' struct sizes) then first indices, per group
+  const size_t asz = std::max(sizeof(trt::SweepArgs<double>), sizeof(trt::SweepArgs<float>));
+  const size_t args_bytes = (act.size() * asz + 255) & ~size_t(255);
+  const size_t need = args_bytes + act.size() * sizeof(int) + 256;
+  if (need > b->h_args_cap) {
+    if (b->h_args) cudaFreeHost(b->h_args);
+    b->h_args = nullptr;
+    if (cudaMallocHost((void**)&b->h_args, need) != cudaSuccess) {
+      cudaGetLastError();
+      b->h_args_cap = 0;
+      return TRT_ERR_NOMEM;
+    }
+    b->h_args_cap = need;
+  }
+  if (args_bytes > b->d_args_cap) {
+    if (b->d_args) cudaFree(b->d_args);
+    if (cudaMalloc(&b->d_args, args_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      b->d_args = nullptr;
+      b->d_args_cap = 0;
+      return TRT_ERR_NOMEM;
+    }
+    b->d_args_cap = args_bytes;
+  }
+  if (act.size() * sizeof(int) > b->d_first_cap) {
+    if (b->d_first) cudaFree(b->d_first);
+    if (cudaMalloc((void**)&b->d_first, act.size() * sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      b->d_first = nullptr;
+      b->d_first_cap = 0;
+      return TRT_ERR_NOMEM;
+    }
+    b->d_first_cap = act.size() * sizeof(int);
+  }
+  while (b->gstreams.size() < groups.size()) {
+    cudaStream_t st;
+    cudaEvent_t ev;
+    TRT_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    TRT_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    b->gstreams.push_back(st);
+    b->gevents.push_back(ev);
+  }
+  TRT_CUDA(cudaEventRecord(b->start, b->stream));
+  size_t done = 0;
+  for (size_t g = 0; g < groups.size(); ++g) {
+    cudaStream_t gs = b->gstreams[g];
+    TRT_CUDA(cudaStreamWaitEvent(gs, b->start, 0));
+    const size_t args_off = done * asz, first_off = args_bytes + done * sizeof(int);
+    int rc = keys[g].prec == TRT_PREC_FP64 ? batch_group_launch<double>(b, groups[g], args_off, first_off, done, gs)
+                                           : batch_group_launch<float>(b, groups[g], args_off, first_off, done, gs);
+    if (rc) return rc;
+    done += groups[g].size();
+    TRT_CUDA(cudaEventRecord(b->gevents[g], gs));
+    TRT_CUDA(cudaStreamWaitEvent(b->stream, b->gevents[g], 0));
+  }
+  return TRT_OK;
+}
+
+int batch_prepare(trt_batch* b, bool tstep) {
+  for (trt_ctx* c : b->h) {
+    if (tstep ? !c->ts_ready : !c->have_material) return TRT_ERR_STATE;
+    if (!c->have_state && !c->swept) return TRT_ERR_STATE;
+    TRT_CUDA(cudaStreamSynchronize(c->stream));   // order after the handle's own earlier calls
+  }
+  return TRT_OK;
+}
+
+// Later calls on each handle's own stream wait for the batch's work.
+int batch_release(trt_batch* b) {
+  TRT_CUDA(cudaEventRecord(b->start, b->stream));
+  for (trt_ctx* c : b->h) TRT_CUDA(cudaStreamWaitEvent(c->stream, b->start, 0));
+  return TRT_OK;
+}
+
+int batch_sweep_impl(trt_batch* b, unsigned flags) {
+  int rc = batch_prepare(b, false);
+  if (rc) return rc;
+  std::vector<int> act(b->h.size());
+  for (size_t k = 0; k < act.size(); ++k) act[k] = (int)k;
+  std::vector<char> roll(act.size(), (flags & TRT_ROLL_STATE) ? 1 : 0);
+  if ((rc = batch_sweep_launch(b, act, roll))) return rc;
+  for (trt_ctx* c : b->h) {
+    StreamSwap sw(c, b->stream);
+    rc = c->prec == TRT_PREC_FP64 ? sweep_epilogue<double>(c, flags & ~TRT_ROLL_STATE)
+                                  : sweep_epilogue<float>(c, flags & ~TRT_ROLL_STATE);
+    if (rc) return rc;
+  }
+  return batch_release(b);
+}
+
+int batch_tstep_impl(trt_batch* b, int* its_out, double* tn_out, double* en_out) {
+  int rc = batch_prepare(b, true);
+  if (rc) return rc;
+  const size_t n = b->h.size();
+  std::vector<StreamSwap> swaps;
+  swaps.reserve(n);
+  for (trt_ctx* c : b->h) swaps.emplace_back(c, b->stream);
+  for (trt_ctx* c : b->h)
+    if ((rc = tstep_begin(c))) return rc;
+  std::vector<int> its(n, 0), act(n);
+  std::vector<double> tn(n, 0.0), en(n, 0.0);
+  for (size_t k = 0; k < n; ++k) act[k] = (int)k;
+  while (!act.empty()) {
+    std::vector<char> roll(act.size());
+    for (size_t i = 0; i < act.size(); ++i) roll[i] = (++its[act[i]] == 1) ? 1 : 0;
+    if ((rc = batch_sweep_launch(b, act, roll))) return rc;
+    for (int k : act) {
+      trt_ctx* c = b->h[k];
+      rc = c->prec == TRT_PREC_FP64 ? sweep_epilogue<double>(c, TRT_MOMENTS) : sweep_epilogue<float>(c, TRT_MOMENTS);
+      if (!rc) rc = c->prec == TRT_PREC_FP64 ? tstep_after_sweep<double>(c, b->h_norms + 10 * k)
+                                             : tstep_after_sweep<float>(c, b->h_norms + 10 * k);
+      if (rc) return rc;
+    }
+    TRT_CUDA(cudaStreamSynchronize(b->stream));
+    std::vector<int> next;
+    for (int k : act) {
+      trt_ctx* c = b->h[k];
+      if ((rc = check_err(c))) return rc;
+      const bool conv = tstep_decide(c, b->h_norms + 10 * k, its[k], &tn[k], &en[k]);
+      if (!conv && its[k] < c->ts_maxit) next.push_back(k);
+    }
+    act.swap(next);
+  }
+  TRT_CUDA(cudaStreamSynchronize(b->stream));
+  for (size_t k = 0; k < n; ++k) {
+    if (its_out) its_out[k] = its[k];
+    if (tn_out) tn_out[k] = tn[k];
+    if (en_out) en_out[k] = en[k];
+  }
+  swaps.clear();
+  return batch_release(b);
+}
+
+}  // namespace
+
 extern "C" {
+
+trt_batch* trt_batch_create(trt_ctx* const* handles, int n, int* status) {
+  int dummy;
+  if (!status) status = &dummy;
+  if (!handles || n < 1) {
+    *status = TRT_ERR_ARG;
+    return nullptr;
+  }
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j <= k; ++j)
+      if (!handles[k] || (j < k && handles[j] == handles[k])) {
+        *status = TRT_ERR_ARG;
+        return nullptr;
+      }
+  trt_batch* b = new (std::nothrow) trt_batch();
+  if (!b) {
+    *status = TRT_ERR_NOMEM;
+    return nullptr;
+  }
+  b->h.assign(handles, handles + n);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost((void**)&b->h_norms, (size_t)10 * n * sizeof(unsigned long long)) != cudaSuccess) {
+    cudaGetLastError();
+    trt_batch_destroy(b);
+    *status = TRT_ERR_CUDA;
+    return nullptr;
+  }
+  *status = TRT_OK;
+  return b;
+}
+
+void trt_batch_destroy(trt_batch* b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (cudaStream_t s : b->gstreams) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+  for (cudaEvent_t e : b->gevents) cudaEventDestroy(e);
+  if (b->start) cudaEventDestroy(b->start);
+  if (b->d_args) cudaFree(b->d_args);
+  if (b->d_first) cudaFree(b->d_first);
+  if (b->h_args) cudaFreeHost(b->h_args);
+  if (b->h_norms) cudaFreeHost(b->h_norms);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  cudaGetLastError();
+  delete b;
+}
+
+int trt_batch_sweep(trt_batch* b, unsigned flags) {
+  if (!b) return TRT_ERR_ARG;
+  return batch_sweep_impl(b, flags);
+}
+
+int trt_batch_sync(trt_batch* b) {
+  if (!b) return TRT_ERR_ARG;
+  TRT_CUDA(cudaStreamSynchronize(b->stream));
+  for (trt_ctx* c : b->h) {
+    int rc = check_err(c);
+    if (rc) return rc;
+  }
+  return TRT_OK;
+}
+
+int trt_batch_tstep(trt_batch* b, int* rt_its, double* T_norms, double* E_norms) {
+  if (!b) return TRT_ERR_ARG;
+  return batch_tstep_impl(b, rt_its, T_norms, E_norms);
+}
 
 const char* trt_strerror(int code) {
   switch (code) {

@@ -258,6 +258,24 @@ int trt_get_temperature(trt_ctx* ctx, double* Temp);
 /* Replace the device temperature and recompute the material from it (MATERIAL_UPDATE). */
 int trt_put_temperature(trt_ctx* ctx, const double* Temp);
 
+/* ---- Batched instances ---------------------------------------------------------------------------
+ * Many independent handles (different grids, groups, quadratures, precisions) stepped together: the
+ * sweeps of all handles that share a tiling class (precision, slices, directions per lane, warps per
+ * CTA, stages) run as ONE kernel launch whose CTAs are the (handle, group, quadrant, direction split)
+ * sweeps of every member, largest first; different classes run concurrently.  Config 2's batched
+ * solve (and the serving loop's stepping) drives this instead of one launch per handle.  Every
+ * handle's results are bit-identical to stepping it alone.  A batch does not own its handles; it
+ * orders itself after each handle's earlier calls and each handle's later calls after it.
+ *   trt_batch_sweep: trt_sweep of every handle with the same flags (asynchronous; trt_batch_sync).
+ *   trt_batch_tstep: trt_tstep of every handle (set up with trt_tstep_setup); handles that converge
+ *   stop sweeping while the others iterate; rt_its / T_norms / E_norms receive n values each. */
+typedef struct trt_batch trt_batch;
+trt_batch* trt_batch_create(trt_ctx* const* handles, int n, int* status);
+void trt_batch_destroy(trt_batch* batch);
+int trt_batch_sweep(trt_batch* batch, unsigned flags);
+int trt_batch_sync(trt_batch* batch);
+int trt_batch_tstep(trt_batch* batch, int* rt_its, double* T_norms, double* E_norms);
+
 /* Message for a TRT_ERR_* code. */
 const char* trt_strerror(int code);
 /* Number of kernels this library has launched in this process (instrumentation). */
