@@ -176,6 +176,98 @@ class Server:
         return [results[r.rid] for r in requests], log
 
 
+class BatchedServer:
+    """Continuous batching at time-step granularity: one driver steps every admitted solve together with
+    trt_batch_tstep (one sweep launch per tiling class over all their CTAs); between steps, finished
+    solves leave (their memory returns to the budget) and queued ones that now fit join, in arrival
+    order.  Every member of a batched step sees that step's wall time as its per-step latency."""
+
+    def __init__(self, hbm_budget, max_active=256, sizer=required_bytes):
+        self.budget = int(hbm_budget)
+        self.max_active = int(max_active)
+        self.sizer = sizer
+
+    @staticmethod
+    def _open(req):
+        from . import api
+        p = req.prob
+        ts = P.fc_timestep_setup(p)
+        ox, oy, w = p.directions()
+        s = api.TransportSweep(p.nx, p.ny, ox, oy, w, p.delx, p.dely, p.ng, precision=req.precision,
+                               hbm_budget=required_bytes(req))
+        try:
+            s.init_state(ts.Tini_eV, list(ts.bcT_eV), P.COMP_UNIT, ts.nu_eV)
+            s.tstep_setup(ts.nu_eV, ts.kappa_mult, ts.cv, np.full((p.nx, p.ny), ts.Tini_eV), ts.Kap0, P.COMP_UNIT,
+                          P.C_LIGHT, ts.dt, bcT=ts.bcT_eV, conv_type=2, conv_ho=req.conv_ho, maxit_rte=req.maxit)
+        except Exception:
+            s.close()
+            raise
+        return s
+
+    def run(self, requests, realtime=True):
+        from . import api
+        reqs = sorted(requests, key=lambda r: (r.arrival_s, r.rid))
+        sizes = {r.rid: self.sizer(r) for r in reqs}
+        for r in reqs:
+            if sizes[r.rid] > self.budget:
+                raise ValueError(f"request {r.rid} needs {sizes[r.rid]} bytes, more than the budget {self.budget}")
+        t0 = time.perf_counter()
+        self.stepping_s = 0.0                          # wall time spent in batched steps
+        self.stepped_updates = 0
+        results, log, queue, active = {}, [], [], []   # active: [request, handle, Result]
+        in_use, nxt = 0, 0
+        while len(results) < len(reqs):
+            now = time.perf_counter() - t0
+            while nxt < len(reqs) and (not realtime or reqs[nxt].arrival_s <= now):
+                queue.append(reqs[nxt])
+                nxt += 1
+            while queue and len(active) < self.max_active and in_use + sizes[queue[0].rid] <= self.budget:
+                r = queue.pop(0)
+                res = Result(r.rid, r.arrival_s, time.perf_counter() - t0, 0.0, sizes[r.rid], 0, [], [])
+                try:
+                    h = self._open(r)
+                except Exception as e:
+                    res.error = f"{type(e).__name__}: {e}"
+                    res.finished_s = time.perf_counter() - t0
+                    results[r.rid] = res
+                    continue
+                in_use += sizes[r.rid]
+                active.append([r, h, res])
+                log.append((time.perf_counter() - t0, r.rid, in_use))
+            if not active:
+                if nxt < len(reqs):
+                    time.sleep(max(0.0, reqs[nxt].arrival_s - (time.perf_counter() - t0)))
+                continue
+            a = time.perf_counter()
+            try:
+                with api.Batch([m[1] for m in active]) as b:
+                    its, _, _ = b.tstep()
+                err = ""
+            except Exception as e:   # the whole step failed: report it on every member
+                its, err = [0] * len(active), f"{type(e).__name__}: {e}"
+            ms = (time.perf_counter() - a) * 1e3
+            self.stepping_s += ms * 1e-3
+            self.stepped_updates += sum(int(m[0].prob.updates_per_sweep()) * int(n) for m, n in zip(active, its))
+            keep = []
+            for (r, h, res), n_it in zip(active, its):
+                res.step_ms.append(ms)
+                res.its.append(int(n_it))
+                if err:
+                    res.error = err
+                if err or len(res.its) == r.steps:
+                    if not err:
+                        res.T = h.temperature()
+                    h.close()
+                    in_use -= sizes[r.rid]
+                    res.updates = int(r.prob.updates_per_sweep() * sum(res.its))
+                    res.finished_s = time.perf_counter() - t0
+                    results[r.rid] = res
+                else:
+                    keep.append([r, h, res])
+            active = keep
+        return [results[r.rid] for r in requests], log
+
+
 def latency_summary(results):
     """p50/p99 per-step and per-solve latency, throughput and counts of a served stream."""
     ok = [r for r in results if not r.error]

@@ -87,3 +87,19 @@ def test_budget_limits_concurrency_on_device():
     res, log = S.Server(hbm_budget=2 * one + 1, max_active=8).run(reqs, realtime=False)
     assert all(not r.error for r in res), [r.error for r in res]
     assert max(e[2] for e in log) <= 2 * one + 1
+
+
+@pytest.mark.gpu
+def test_batched_server_matches_solves_alone():
+    """Continuous batching: requests of different sizes, quadratures and precisions, arriving while
+    others run, give the same temperatures as each solved on its own."""
+    reqs = [_req(k, 0.02 * k, n=10 + 3 * k, G=2 + k % 2) for k in range(5)]
+    reqs[1].precision = "fp64"
+    reqs[3].prob = pkg.problems.random_small(203, 9, 11, 2, "S12")
+    alone, _ = S.Server(hbm_budget=1 << 40, max_active=1).run(reqs, realtime=False)
+    batched, log = S.BatchedServer(hbm_budget=1 << 40).run(reqs, realtime=True)
+    assert all(not r.error for r in alone + batched), [r.error for r in alone + batched]
+    for a, b in zip(alone, batched):
+        assert np.array_equal(a.T, b.T)
+        assert a.its == b.its
+    assert len(log) == 5
