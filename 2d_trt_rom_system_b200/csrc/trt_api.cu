@@ -707,25 +707,28 @@ template <class Real>
 int init_state_impl(trt_ctx* c, double Tini, const double* Tb, double cu, const double* nu) {
   std::vector<double> per_g(c->ng);
   for (int g = 0; g < c->ng; ++g) per_g[g] = bg_planck_h(Tini, nu[g], nu[g + 1], cu);
-  double* d_pg = nullptr;
-  int rc = alloc_t(c, &d_pg, c->ng);
-  if (rc) return rc;
+  // per-group values staged in the boundary-value buffer (bc_update_impl below overwrites it later in
+  // stream order), then streaming fills of both states and of every boundary value: RT_INIT sets all of
+  // Ic_edgV/H to Bg(Tini) before the Planck inflow faces
+  double* d_pg = c->d_bval;
   TRT_CUDA(cudaMemcpyAsync(d_pg, per_g.data(), c->ng * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   const long long per_group = 4LL * c->t.NH * c->blk;
   for (int k = 0; k < 2; ++k) {
     trt::fill_groups_kernel<Real><<<grid_for(per_group * c->ng), 256, 0, c->stream>>>(per_group, c->ng, d_pg,
                                                                                        (Real*)c->d_state[k]);
     TRT_LAUNCHED();
-    TRT_CUDA(cudaGetLastError());
   }
-  // every boundary value = Bg(Tini) first (RT_INIT sets all of Ic_edgV/H), then Planck inflow faces
-  std::vector<Real> bV((size_t)2 * c->ng * c->nm * 2 * c->ny), bH((size_t)2 * c->ng * c->nm * 2 * c->nx);
-  for (size_t k = 0; k < bV.size(); ++k) bV[k] = (Real)per_g[(k / ((size_t)c->nm * 2 * c->ny)) % c->ng];
-  for (size_t k = 0; k < bH.size(); ++k) bH[k] = (Real)per_g[(k / ((size_t)c->nm * 2 * c->nx)) % c->ng];
-  TRT_CUDA(cudaMemcpyAsync(c->d_bndV, bV.data(), bV.size() * sizeof(Real), cudaMemcpyHostToDevice, c->stream));
-  TRT_CUDA(cudaMemcpyAsync(c->d_bndH, bH.data(), bH.size() * sizeof(Real), cudaMemcpyHostToDevice, c->stream));
-  TRT_CUDA(cudaStreamSynchronize(c->stream));
-  c->dfree(d_pg, c->ng * sizeof(double));
+  const long long pv = (long long)c->nm * 2 * c->ny, ph = (long long)c->nm * 2 * c->nx;
+  for (int side = 0; side < 2; ++side) {
+    trt::fill_groups_kernel<Real><<<grid_for(pv * c->ng), 256, 0, c->stream>>>(
+        pv, c->ng, d_pg, (Real*)c->d_bndV + (size_t)side * c->ng * pv);
+    TRT_LAUNCHED();
+    trt::fill_groups_kernel<Real><<<grid_for(ph * c->ng), 256, 0, c->stream>>>(
+        ph, c->ng, d_pg, (Real*)c->d_bndH + (size_t)side * c->ng * ph);
+    TRT_LAUNCHED();
+  }
+  TRT_CUDA(cudaGetLastError());
+  int rc;
   const int zero[4] = {0, 0, 0, 0};
   rc = bc_update_impl<Real>(c, zero, Tb, cu, nu);
   if (rc) return rc;
