@@ -1078,6 +1078,9 @@ struct trt_batch {
   unsigned char* h_args = nullptr;           // pinned staging of d_args / d_first
   size_t h_args_cap = 0;
   unsigned long long* h_norms = nullptr;     // pinned, 10 convergence values per handle
+  int* h_err = nullptr;                      // pinned, error word of each handle
+  std::vector<cudaStream_t> estreams;        // the per-handle work after a batched sweep, spread over these
+  std::vector<cudaEvent_t> eevents;
 };
 
 namespace {
@@ -1252,18 +1255,33 @@ int batch_tstep_impl(trt_batch* b, int* its_out, double* tn_out, double* en_out)
     std::vector<char> roll(act.size());
     for (size_t i = 0; i < act.size(); ++i) roll[i] = (++its[act[i]] == 1) ? 1 : 0;
     if ((rc = batch_sweep_launch(b, act, roll))) return rc;
-    for (int k : act) {
+    // each handle's epilogue, MEB, material update and reductions on one of the epilogue streams, so the
+    // small kernels of different handles overlap; one synchronisation for all
+    TRT_CUDA(cudaEventRecord(b->start, b->stream));
+    for (cudaStream_t es : b->estreams) TRT_CUDA(cudaStreamWaitEvent(es, b->start, 0));
+    for (size_t i = 0; i < act.size(); ++i) {
+      const int k = act[i];
       trt_ctx* c = b->h[k];
+      StreamSwap sw(c, b->estreams[i % b->estreams.size()]);
       rc = c->prec == TRT_PREC_FP64 ? sweep_epilogue<double>(c, TRT_MOMENTS) : sweep_epilogue<float>(c, TRT_MOMENTS);
       if (!rc) rc = c->prec == TRT_PREC_FP64 ? tstep_after_sweep<double>(c, b->h_norms + 10 * k)
                                              : tstep_after_sweep<float>(c, b->h_norms + 10 * k);
       if (rc) return rc;
+      TRT_CUDA(cudaMemcpyAsync(b->h_err + k, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    }
+    for (size_t e = 0; e < b->estreams.size(); ++e) {
+      TRT_CUDA(cudaEventRecord(b->eevents[e], b->estreams[e]));
+      TRT_CUDA(cudaStreamWaitEvent(b->stream, b->eevents[e], 0));
     }
     TRT_CUDA(cudaStreamSynchronize(b->stream));
     std::vector<int> next;
     for (int k : act) {
       trt_ctx* c = b->h[k];
-      if ((rc = check_err(c))) return rc;
+      if (b->h_err[k]) {   // a bounded wait of this handle's sweep gave up (see check_err)
+        TRT_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+        TRT_CUDA(cudaStreamSynchronize(c->stream));
+        return TRT_ERR_TIMEOUT;
+      }
       const bool conv = tstep_decide(c, b->h_norms + 10 * k, its[k], &tn[k], &en[k]);
       if (!conv && its[k] < c->ts_maxit) next.push_back(k);
     }
@@ -1304,11 +1322,25 @@ trt_batch* trt_batch_create(trt_ctx* const* handles, int n, int* status) {
   b->h.assign(handles, handles + n);
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming) != cudaSuccess ||
-      cudaMallocHost((void**)&b->h_norms, (size_t)10 * n * sizeof(unsigned long long)) != cudaSuccess) {
+      cudaMallocHost((void**)&b->h_norms, (size_t)10 * n * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMallocHost((void**)&b->h_err, (size_t)n * sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     trt_batch_destroy(b);
     *status = TRT_ERR_CUDA;
     return nullptr;
+  }
+  for (int k = 0; k < 8 && k < n; ++k) {
+    cudaStream_t st;
+    cudaEvent_t ev;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      trt_batch_destroy(b);
+      *status = TRT_ERR_CUDA;
+      return nullptr;
+    }
+    b->estreams.push_back(st);
+    b->eevents.push_back(ev);
   }
   *status = TRT_OK;
   return b;
@@ -1322,6 +1354,12 @@ void trt_batch_destroy(trt_batch* b) {
     cudaStreamDestroy(s);
   }
   for (cudaEvent_t e : b->gevents) cudaEventDestroy(e);
+  for (cudaStream_t s : b->estreams) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+  for (cudaEvent_t e : b->eevents) cudaEventDestroy(e);
+  if (b->h_err) cudaFreeHost(b->h_err);
   if (b->start) cudaEventDestroy(b->start);
   if (b->d_args) cudaFree(b->d_args);
   if (b->d_first) cudaFree(b->d_first);
