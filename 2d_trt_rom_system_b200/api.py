@@ -209,10 +209,17 @@ class TransportSweep:
               "trt_autotune")
         return dict(self.tiling(), sweep_ms=ms.value)
 
+    def set_register_mode(self, mode):
+        """0: kernels for up to 512 threads (<= 128 registers); -1/1: the <= 128-thread, up-to-170-register
+        variant when the whole grid stays resident with it.  Re-lays out (zeroes) the state."""
+        check(_lib.lib().trt_set_register_mode(self._h, int(mode)), "trt_set_register_mode")
+
     def tiling(self):
         v = [ctypes.c_int(0) for _ in range(5)]
         check(_lib.lib().trt_get_tiling(self._h, *[ctypes.byref(x) for x in v]), "trt_get_tiling")
-        return dict(zip(("warps", "slices", "dirs_per_lane", "stages", "splits"), [x.value for x in v]))
+        out = dict(zip(("warps", "slices", "dirs_per_lane", "stages", "splits"), [x.value for x in v]))
+        out["wide_registers"] = int(_lib.lib().trt_get_register_mode(self._h))
+        return out
 
     def set_material(self, KapE_in, src_iso, c, Delt, Comp_Unit):
         K = _f64(KapE_in, (self.nx, self.ny, self.ng))

@@ -113,12 +113,15 @@ bool pick_cfg(int ndir, int prec, int S_req, KernelCfg* out) {
 template <class Real>
 using SweepKernel = void (*)(trt::SweepArgs<Real>);
 
-// The compiled sweep kernel of a (slices, directions per lane) configuration (null if none).
+// The compiled sweep kernel of a (slices, directions per lane) configuration (null if none); `wide`
+// selects the variant for CTAs of at most 128 threads with up to 170 registers per thread.
 template <class Real>
-SweepKernel<Real> sweep_kernel_for(const KernelCfg& kc, bool src_full) {
+SweepKernel<Real> sweep_kernel_for(const KernelCfg& kc, bool src_full, bool wide = false) {
 #define TRT_SWEEP_CASE(S_, D_)                                                                         \
   if (kc.S == S_ && kc.D == D_)                                                                        \
-    return src_full ? trt::scb_sweep_kernel<Real, S_, D_, true> : trt::scb_sweep_kernel<Real, S_, D_, false>;
+    return src_full ? trt::scb_sweep_kernel<Real, S_, D_, true>                                        \
+                    : (wide ? trt::scb_sweep_kernel<Real, S_, D_, false, 128, 3>                       \
+                            : trt::scb_sweep_kernel<Real, S_, D_, false>);
   TRT_SWEEP_CASE(1, 2)
   TRT_SWEEP_CASE(1, 4)
   TRT_SWEEP_CASE(2, 2)
@@ -181,9 +184,9 @@ SweepBatchKernel<Real> sweep_batch_kernel_for(const KernelCfg& kc, bool src_full
 }
 
 template <class Real>
-cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int grid, int block, size_t smem, cudaStream_t st,
-                         const trt::SweepArgs<Real>& a) {
-  SweepKernel<Real> k = sweep_kernel_for<Real>(kc, src_full);
+cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, bool wide, int grid, int block, size_t smem,
+                         cudaStream_t st, const trt::SweepArgs<Real>& a) {
+  SweepKernel<Real> k = sweep_kernel_for<Real>(kc, src_full, wide);
   if (!k) return cudaErrorInvalidValue;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k<<<grid, block, smem, st>>>(a);
@@ -192,8 +195,8 @@ cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int grid, int block
 
 // CTAs of a sweep configuration that are resident on one SM at once (0 on failure).
 template <class Real>
-int sweep_ctas_per_sm(const KernelCfg& kc, int block, size_t smem) {
-  SweepKernel<Real> k = sweep_kernel_for<Real>(kc, false);
+int sweep_ctas_per_sm(const KernelCfg& kc, int block, size_t smem, bool wide = false) {
+  SweepKernel<Real> k = sweep_kernel_for<Real>(kc, false, wide);
   int n = 0;
   if (!k) return 0;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -213,6 +216,8 @@ struct trt_ctx {
   size_t budget = 0, used = 0;
   cudaStream_t stream = nullptr;
   int Wreq = 0, Sreq = 0, NHreq = 0, stages = 2;
+  bool wide = false;                 // sweep with the up-to-170-register variant (set by setup_layout)
+  int wide_req = -1;                 // -1 automatic, 0 never, 1 when it fits
   KernelCfg kc{8, 5};
   trt::Tiling t{};
   long long chunk = 0, blk = 0;
@@ -416,6 +421,14 @@ int setup_layout(trt_ctx* c) {
   c->t = t;
   c->chunk = chunk;
   c->blk = trt::block_elems(t);
+  // the wide-register variant when the CTA has at most 4 warps and the whole grid stays resident with it
+  c->wide = false;
+  if (c->wide_req != 0 && 32 * W <= 128) {
+    const size_t smem = smem_at(stages);
+    const int per = c->prec == TRT_PREC_FP64 ? sweep_ctas_per_sm<double>(c->kc, 32 * W, smem, true)
+                                             : sweep_ctas_per_sm<float>(c->kc, 32 * W, smem, true);
+    c->wide = per > 0 && 4LL * c->ng * NH <= (long long)per * sm_count();
+  }
   const size_t sbytes = (size_t)c->state_elems() * esz;
   for (int k = 0; k < 2; ++k) {
     int rc = c->dalloc(&c->d_state[k], sbytes);
@@ -558,8 +571,8 @@ template <class Real>
 int sweep_impl(trt_ctx* c, unsigned flags) {
   if (flags & TRT_ROLL_STATE) c->cur = 1 - c->cur;   // I_crn_old <- I_crn (ALGORITHMS.f08:397)
   const trt::SweepArgs<Real> a = make_sweep_args<Real>(c);
-  cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, 4 * c->ng * c->t.NH, 32 * c->t.W, sweep_smem<Real>(c),
-                                     c->stream, a);
+  cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, c->wide && !c->use_srcfull, 4 * c->ng * c->t.NH,
+                                     32 * c->t.W, sweep_smem<Real>(c), c->stream, a);
   TRT_LAUNCHED();
   if (e != cudaSuccess) return TRT_ERR_CUDA;
   c->swept = true;
@@ -1512,8 +1525,8 @@ int trt_autotune(trt_ctx* c, int* warps_out, int* slices_out, int* splits_out, f
       const size_t smem = c->prec == TRT_PREC_FP64
                               ? trt::sweep_smem_bytes<double>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D)
                               : trt::sweep_smem_bytes<float>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D);
-      const int per = c->prec == TRT_PREC_FP64 ? sweep_ctas_per_sm<double>(c->kc, 32 * c->t.W, smem)
-                                               : sweep_ctas_per_sm<float>(c->kc, 32 * c->t.W, smem);
+      const int per = c->prec == TRT_PREC_FP64 ? sweep_ctas_per_sm<double>(c->kc, 32 * c->t.W, smem, c->wide)
+                                               : sweep_ctas_per_sm<float>(c->kc, 32 * c->t.W, smem, c->wide);
       if (per <= 0 || 4LL * c->ng * NH > (long long)per * sms) continue;
       c->have_state = true;
       c->have_material = true;
@@ -1564,6 +1577,14 @@ int trt_set_tiling(trt_ctx* c, int warps_per_cta, int slices, int stages, int sp
   c->stages = stages ? stages : 2;
   return setup_layout(c);
 }
+
+int trt_set_register_mode(trt_ctx* c, int mode) {
+  if (!c || mode < -1 || mode > 1) return TRT_ERR_ARG;
+  c->wide_req = mode;
+  return setup_layout(c);
+}
+
+int trt_get_register_mode(const trt_ctx* c) { return c ? (c->wide ? 1 : 0) : TRT_ERR_ARG; }
 
 int trt_get_tiling(const trt_ctx* c, int* W, int* S, int* D, int* stages, int* splits) {
   if (!c) return TRT_ERR_ARG;

@@ -156,6 +156,14 @@ int trt_set_tiling(trt_ctx* ctx, int warps_per_cta, int slices, int stages, int 
 int trt_get_tiling(const trt_ctx* ctx, int* warps_per_cta, int* slices, int* dirs_per_lane, int* stages,
                    int* splits);
 
+/* Register budget of the sweep kernel: mode 0 always uses the variant compiled for up to 512 threads
+ * per CTA (at most 128 registers per thread); mode 1 or -1 (automatic, the default) uses the variant
+ * compiled for up to 128 threads per CTA and 3 CTAs per SM (up to 170 registers per thread) whenever
+ * the CTA has at most 4 warps and the whole grid stays resident with it.  Re-lays out (zeroes) the
+ * state.  trt_get_register_mode returns 1 when the wide variant is in use. */
+int trt_set_register_mode(trt_ctx* ctx, int mode);
+int trt_get_register_mode(const trt_ctx* ctx);
+
 /* Autotuner: times one sweep of this handle's problem for each (direction splits 1..4) x (warps per CTA
  * 2, 3, 4, 5, 6, 8) tiling whose CTAs are all resident at once (CUDA occupancy query), with the
  * default slices per warp, and keeps the fastest.  Uses the handle's material if set, else a zero

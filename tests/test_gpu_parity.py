@@ -435,3 +435,21 @@ def test_autotune_picks_a_resident_tiling_and_keeps_results(oracle):
         assert np.array_equal(s.get_state(), ref["I_crn"])
         m = s.moments(["Eg_avg", "E_avg"])
     assert moment_err(m, ref, "Eg_avg") < 1e-13
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_register_variant_does_not_change_results(precision):
+    """The up-to-170-register kernel variant computes the same operations: bit-identical outputs."""
+    prob = pkg.problems.random_small(31, 40, 36, 4, "S16")
+    d = sweep_inputs(prob, seed=31)
+    out = []
+    for mode in (0, -1):
+        with resident(d, precision=precision, tiling=dict(warps=4)) as s:
+            s.set_register_mode(mode)
+            s.put_state(d["I_crn_old"])
+            s.sweep(moments=True)
+            out.append((s.tiling()["wide_registers"], s.get_state(), s.moments(["Eg_avg", "Fxg_edgV", "Cg_B"])))
+    assert out[0][0] == 0 and out[1][0] == 1
+    assert np.array_equal(out[0][1], out[1][1])
+    for k in out[0][2]:
+        assert np.array_equal(out[0][2][k], out[1][2][k]), k
