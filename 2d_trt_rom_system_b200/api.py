@@ -210,8 +210,8 @@ class TransportSweep:
         return dict(self.tiling(), sweep_ms=ms.value)
 
     def set_register_mode(self, mode):
-        """0: kernels for up to 512 threads (<= 128 registers); -1/1: the <= 128-thread, up-to-170-register
-        variant when the whole grid stays resident with it.  Re-lays out (zeroes) the state."""
+        """Cap the sweep kernel's register level (0: <= 128, 1: <= 170, 2: <= 255 registers per thread);
+        -1 = the highest level that keeps the whole grid resident.  Re-lays out (zeroes) the state."""
         check(_lib.lib().trt_set_register_mode(self._h, int(mode)), "trt_set_register_mode")
 
     def tiling(self):

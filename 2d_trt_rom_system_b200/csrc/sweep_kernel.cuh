@@ -784,9 +784,9 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
   }
 }
 
-// MAXT/MINB: 512/1 fits every tiling (at most 128 registers per thread); 128/3 is the variant for CTAs
-// of at most 4 warps when 3 of them per SM keep the whole grid resident: up to 170 registers per
-// thread, which the solve uses for more independent directions in flight.
+// MAXT/MINB: 512/1 fits every tiling (at most 128 registers per thread); 128/3 and 128/2 are the
+// variants for CTAs of at most 4 warps when 3 or 2 of them per SM keep the whole grid resident: up to
+// 170 or 255 registers per thread, which the solve uses for more independent directions in flight.
 template <class Real, int S, int D, bool SRC_FULL, int MAXT = 512, int MINB = 1>
 __global__ void __launch_bounds__(MAXT, MINB) scb_sweep_kernel(const SweepArgs<Real> a) {
   scb_sweep_body<Real, S, D, SRC_FULL>(a, blockIdx.x);

@@ -113,15 +113,17 @@ bool pick_cfg(int ndir, int prec, int S_req, KernelCfg* out) {
 template <class Real>
 using SweepKernel = void (*)(trt::SweepArgs<Real>);
 
-// The compiled sweep kernel of a (slices, directions per lane) configuration (null if none); `wide`
-// selects the variant for CTAs of at most 128 threads with up to 170 registers per thread.
+// The compiled sweep kernel of a (slices, directions per lane) configuration (null if none).  Register
+// level 0: any CTA size, at most 128 registers per thread; 1: at most 128 threads and 3 CTAs per SM (up to
+// 170 registers); 2: at most 128 threads and 2 CTAs per SM (up to 255 registers).
 template <class Real>
-SweepKernel<Real> sweep_kernel_for(const KernelCfg& kc, bool src_full, bool wide = false) {
+SweepKernel<Real> sweep_kernel_for(const KernelCfg& kc, bool src_full, int level = 0) {
 #define TRT_SWEEP_CASE(S_, D_)                                                                         \
   if (kc.S == S_ && kc.D == D_)                                                                        \
     return src_full ? trt::scb_sweep_kernel<Real, S_, D_, true>                                        \
-                    : (wide ? trt::scb_sweep_kernel<Real, S_, D_, false, 128, 3>                       \
-                            : trt::scb_sweep_kernel<Real, S_, D_, false>);
+                    : (level == 2 ? trt::scb_sweep_kernel<Real, S_, D_, false, 128, 2>                 \
+                                  : (level == 1 ? trt::scb_sweep_kernel<Real, S_, D_, false, 128, 3>     \
+                                                : trt::scb_sweep_kernel<Real, S_, D_, false>));
   TRT_SWEEP_CASE(1, 2)
   TRT_SWEEP_CASE(1, 4)
   TRT_SWEEP_CASE(2, 2)
@@ -184,9 +186,9 @@ SweepBatchKernel<Real> sweep_batch_kernel_for(const KernelCfg& kc, bool src_full
 }
 
 template <class Real>
-cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, bool wide, int grid, int block, size_t smem,
+cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int level, int grid, int block, size_t smem,
                          cudaStream_t st, const trt::SweepArgs<Real>& a) {
-  SweepKernel<Real> k = sweep_kernel_for<Real>(kc, src_full, wide);
+  SweepKernel<Real> k = sweep_kernel_for<Real>(kc, src_full, level);
   if (!k) return cudaErrorInvalidValue;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k<<<grid, block, smem, st>>>(a);
@@ -195,8 +197,8 @@ cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, bool wide, int grid
 
 // CTAs of a sweep configuration that are resident on one SM at once (0 on failure).
 template <class Real>
-int sweep_ctas_per_sm(const KernelCfg& kc, int block, size_t smem, bool wide = false) {
-  SweepKernel<Real> k = sweep_kernel_for<Real>(kc, false, wide);
+int sweep_ctas_per_sm(const KernelCfg& kc, int block, size_t smem, int level = 0) {
+  SweepKernel<Real> k = sweep_kernel_for<Real>(kc, false, level);
   int n = 0;
   if (!k) return 0;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -216,8 +218,8 @@ struct trt_ctx {
   size_t budget = 0, used = 0;
   cudaStream_t stream = nullptr;
   int Wreq = 0, Sreq = 0, NHreq = 0, stages = 2;
-  bool wide = false;                 // sweep with the up-to-170-register variant (set by setup_layout)
-  int wide_req = -1;                 // -1 automatic, 0 never, 1 when it fits
+  int regs = 0;                      // register level of the sweep kernel in use (set by setup_layout)
+  int regs_req = -1;                 // -1: the highest level that keeps the grid resident; 0..2: at most that
   KernelCfg kc{8, 5};
   trt::Tiling t{};
   long long chunk = 0, blk = 0;
@@ -421,13 +423,17 @@ int setup_layout(trt_ctx* c) {
   c->t = t;
   c->chunk = chunk;
   c->blk = trt::block_elems(t);
-  // the wide-register variant when the CTA has at most 4 warps and the whole grid stays resident with it
-  c->wide = false;
-  if (c->wide_req != 0 && 32 * W <= 128) {
+  // the highest register level whose variant keeps the whole grid resident (CTAs of at most 4 warps)
+  c->regs = 0;
+  const int cap = c->regs_req < 0 ? 2 : c->regs_req;
+  for (int level = cap; level >= 1 && 32 * W <= 128; --level) {
     const size_t smem = smem_at(stages);
-    const int per = c->prec == TRT_PREC_FP64 ? sweep_ctas_per_sm<double>(c->kc, 32 * W, smem, true)
-                                             : sweep_ctas_per_sm<float>(c->kc, 32 * W, smem, true);
-    c->wide = per > 0 && 4LL * c->ng * NH <= (long long)per * sm_count();
+    const int per = c->prec == TRT_PREC_FP64 ? sweep_ctas_per_sm<double>(c->kc, 32 * W, smem, level)
+                                             : sweep_ctas_per_sm<float>(c->kc, 32 * W, smem, level);
+    if (per > 0 && 4LL * c->ng * NH <= (long long)per * sm_count()) {
+      c->regs = level;
+      break;
+    }
   }
   const size_t sbytes = (size_t)c->state_elems() * esz;
   for (int k = 0; k < 2; ++k) {
@@ -571,7 +577,7 @@ template <class Real>
 int sweep_impl(trt_ctx* c, unsigned flags) {
   if (flags & TRT_ROLL_STATE) c->cur = 1 - c->cur;   // I_crn_old <- I_crn (ALGORITHMS.f08:397)
   const trt::SweepArgs<Real> a = make_sweep_args<Real>(c);
-  cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, c->wide && !c->use_srcfull, 4 * c->ng * c->t.NH,
+  cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, c->use_srcfull ? 0 : c->regs, 4 * c->ng * c->t.NH,
                                      32 * c->t.W, sweep_smem<Real>(c), c->stream, a);
   TRT_LAUNCHED();
   if (e != cudaSuccess) return TRT_ERR_CUDA;
@@ -1525,8 +1531,8 @@ int trt_autotune(trt_ctx* c, int* warps_out, int* slices_out, int* splits_out, f
       const size_t smem = c->prec == TRT_PREC_FP64
                               ? trt::sweep_smem_bytes<double>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D)
                               : trt::sweep_smem_bytes<float>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D);
-      const int per = c->prec == TRT_PREC_FP64 ? sweep_ctas_per_sm<double>(c->kc, 32 * c->t.W, smem, c->wide)
-                                               : sweep_ctas_per_sm<float>(c->kc, 32 * c->t.W, smem, c->wide);
+      const int per = c->prec == TRT_PREC_FP64 ? sweep_ctas_per_sm<double>(c->kc, 32 * c->t.W, smem, c->regs)
+                                               : sweep_ctas_per_sm<float>(c->kc, 32 * c->t.W, smem, c->regs);
       if (per <= 0 || 4LL * c->ng * NH > (long long)per * sms) continue;
       c->have_state = true;
       c->have_material = true;
@@ -1579,12 +1585,12 @@ int trt_set_tiling(trt_ctx* c, int warps_per_cta, int slices, int stages, int sp
 }
 
 int trt_set_register_mode(trt_ctx* c, int mode) {
-  if (!c || mode < -1 || mode > 1) return TRT_ERR_ARG;
-  c->wide_req = mode;
+  if (!c || mode < -1 || mode > 2) return TRT_ERR_ARG;
+  c->regs_req = mode;
   return setup_layout(c);
 }
 
-int trt_get_register_mode(const trt_ctx* c) { return c ? (c->wide ? 1 : 0) : TRT_ERR_ARG; }
+int trt_get_register_mode(const trt_ctx* c) { return c ? c->regs : TRT_ERR_ARG; }
 
 int trt_get_tiling(const trt_ctx* c, int* W, int* S, int* D, int* stages, int* splits) {
   if (!c) return TRT_ERR_ARG;

@@ -156,11 +156,11 @@ int trt_set_tiling(trt_ctx* ctx, int warps_per_cta, int slices, int stages, int 
 int trt_get_tiling(const trt_ctx* ctx, int* warps_per_cta, int* slices, int* dirs_per_lane, int* stages,
                    int* splits);
 
-/* Register budget of the sweep kernel: mode 0 always uses the variant compiled for up to 512 threads
- * per CTA (at most 128 registers per thread); mode 1 or -1 (automatic, the default) uses the variant
- * compiled for up to 128 threads per CTA and 3 CTAs per SM (up to 170 registers per thread) whenever
- * the CTA has at most 4 warps and the whole grid stays resident with it.  Re-lays out (zeroes) the
- * state.  trt_get_register_mode returns 1 when the wide variant is in use. */
+/* Register budget of the sweep kernel.  Each configuration is compiled at three levels: 0 for any CTA
+ * size (at most 128 registers per thread), 1 for CTAs of at most 128 threads with 3 per SM (up to 170),
+ * 2 for CTAs of at most 128 threads with 2 per SM (up to 255).  mode -1 (the default) uses the highest
+ * level whose variant keeps the whole grid resident at once; mode 0..2 caps the level.  Re-lays out
+ * (zeroes) the state.  trt_get_register_mode returns the level in use. */
 int trt_set_register_mode(trt_ctx* ctx, int mode);
 int trt_get_register_mode(const trt_ctx* ctx);
 

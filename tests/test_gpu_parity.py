@@ -449,7 +449,7 @@ def test_register_variant_does_not_change_results(precision):
             s.put_state(d["I_crn_old"])
             s.sweep(moments=True)
             out.append((s.tiling()["wide_registers"], s.get_state(), s.moments(["Eg_avg", "Fxg_edgV", "Cg_B"])))
-    assert out[0][0] == 0 and out[1][0] == 1
+    assert out[0][0] == 0 and out[1][0] >= 1
     assert np.array_equal(out[0][1], out[1][1])
     for k in out[0][2]:
         assert np.array_equal(out[0][2][k], out[1][2][k]), k
