@@ -795,8 +795,8 @@ __global__ void __launch_bounds__(MAXT, MINB) scb_sweep_kernel(const SweepArgs<R
 // One launch over the CTAs of several instances (same precision, slices, directions per lane, warps
 // per CTA and stages): instance k owns CTAs [first[k], first[k+1]).  Its arguments are copied to
 // shared memory once; the block scheduler then drains the (instance, group, quadrant, split) CTAs.
-template <class Real, int S, int D, bool SRC_FULL>
-__global__ void __launch_bounds__(512) scb_sweep_batch_kernel(const SweepArgs<Real>* __restrict__ args,
+template <class Real, int S, int D, bool SRC_FULL, int MAXT = 512, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB) scb_sweep_batch_kernel(const SweepArgs<Real>* __restrict__ args,
                                                               const int* __restrict__ first, int n) {
   __shared__ SweepArgs<Real> sa;
   __shared__ int sbid;

@@ -153,12 +153,14 @@ SweepKernel<Real> sweep_kernel_for(const KernelCfg& kc, bool src_full, int level
 template <class Real>
 using SweepBatchKernel = void (*)(const trt::SweepArgs<Real>*, const int*, int);
 
-// The batched sweep kernel of a configuration (null if none).
+// The batched sweep kernel of a configuration (null if none); level 1 as for sweep_kernel_for.
 template <class Real>
-SweepBatchKernel<Real> sweep_batch_kernel_for(const KernelCfg& kc, bool src_full) {
+SweepBatchKernel<Real> sweep_batch_kernel_for(const KernelCfg& kc, bool src_full, int level = 0) {
 #define TRT_SWEEP_CASE(S_, D_)                                                                         \
   if (kc.S == S_ && kc.D == D_)                                                                        \
-    return src_full ? trt::scb_sweep_batch_kernel<Real, S_, D_, true> : trt::scb_sweep_batch_kernel<Real, S_, D_, false>;
+    return src_full ? trt::scb_sweep_batch_kernel<Real, S_, D_, true>                                  \
+                    : (level == 1 ? trt::scb_sweep_batch_kernel<Real, S_, D_, false, 128, 3>           \
+                                  : trt::scb_sweep_batch_kernel<Real, S_, D_, false>);
   TRT_SWEEP_CASE(1, 2)
   TRT_SWEEP_CASE(1, 4)
   TRT_SWEEP_CASE(2, 2)
@@ -1135,7 +1137,18 @@ int batch_group_launch(trt_batch* b, std::vector<trt_ctx*>& grp, size_t args_off
   int* df = b->d_first + done;   // the device copy holds only the first-CTA table
   TRT_CUDA(cudaMemcpyAsync(da, ha, grp.size() * sizeof(trt::SweepArgs<Real>), cudaMemcpyHostToDevice, gs));
   TRT_CUDA(cudaMemcpyAsync(df, hf, grp.size() * sizeof(int), cudaMemcpyHostToDevice, gs));
-  SweepBatchKernel<Real> k = sweep_batch_kernel_for<Real>(grp[0]->kc, grp[0]->use_srcfull);
+  // the up-to-170-register variant when every CTA of the launch is resident at once with it
+  int level = 0;
+  if (32 * grp[0]->t.W <= 128 && !grp[0]->use_srcfull) {
+    SweepBatchKernel<Real> k1 = sweep_batch_kernel_for<Real>(grp[0]->kc, false, 1);
+    int per = 0;
+    if (k1 && cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k1, 32 * grp[0]->t.W, smem) == cudaSuccess &&
+        total <= (long long)per * sm_count())
+      level = 1;
+    cudaGetLastError();
+  }
+  SweepBatchKernel<Real> k = sweep_batch_kernel_for<Real>(grp[0]->kc, grp[0]->use_srcfull, level);
   if (!k) return TRT_ERR_UNSUPPORTED;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k<<<(unsigned)total, 32 * grp[0]->t.W, smem, gs>>>(da, df, (int)grp.size());
