@@ -113,6 +113,10 @@ SIGNATURES = {
     "trt_strerror": (ctypes.c_char_p, [_i]),
     "trt_kernel_launches": (ctypes.c_ulonglong, []),
     "trt_transport_residual_noalloc": (_i, [_i, _i, _i, _i] + [_P] * 11 + [_d, _d, _P, _P, _P, _P]),
+    "trt_old_mgqd_coefs": (_i, [_i, _i, _i] + [_D] * 17 + [_d, _d, _d] + [_D] * 5 + [_i]),
+    "trt_mloqd_fv": (_i, [_i, _i, _i] + [_D] * 29 + [_d, _d, _d, _i, _i] + [_D] * 10 + [_I, _d, _d, _d]),
+    "trt_mgqd_set_tolerance": (_i, [_d, _i]),
+    "trt_mgqd_last_stats": (_i, [_D, _I]),
 }
 
 _lib = None

@@ -144,6 +144,65 @@ def RT_BC_UPDATE(BC_Type, bcT_left, bcT_lower, bcT_right, bcT_upper, Comp_Unit, 
     check(rc, "RT_BC_UPDATE")
 
 
+def OLD_MGQD_COEFS(Eg_avg_old, Eg_edgV_old, Eg_edgH_old, Fxg_edgV_old, Fyg_edgH_old, fg_avg_xx_old, fg_avg_yy_old,
+                   fg_edgV_xx_old, fg_edgV_xy_old, fg_edgH_yy_old, fg_edgH_xy_old, KapE_old, KapR_old, Src_old, Delx,
+                   Dely, A, c, Delt, Theta, G_old, Pold_L, Pold_B, Pold_R, Pold_T, Open_Threads):
+    """SUBROUTINE OLD_MGQD_COEFS, MainSrc/MLOQD_SOLVES.f08:12-73."""
+    nx, ny, ng = Eg_avg_old.shape
+    C, V, H = (nx, ny, ng), (nx + 1, ny, ng), (nx, ny + 1, ng)
+    shapes = (C, V, H, V, H, C, C, V, V, H, H, C, C, C, (nx,), (ny,), (nx, ny))
+    ins = [_f64(a, s) for a, s in zip((Eg_avg_old, Eg_edgV_old, Eg_edgH_old, Fxg_edgV_old, Fyg_edgH_old,
+                                       fg_avg_xx_old, fg_avg_yy_old, fg_edgV_xx_old, fg_edgV_xy_old, fg_edgH_yy_old,
+                                       fg_edgH_xy_old, KapE_old, KapR_old, Src_old, Delx, Dely, A), shapes)]
+    outs = [_out(o, C) for o in (G_old, Pold_L, Pold_B, Pold_R, Pold_T)]
+    rc = _lib.lib().trt_old_mgqd_coefs(nx, ny, ng, *[dptr(a) for a in ins], float(c), float(Delt), float(Theta),
+                                       *[dptr(o) for o in outs], int(Open_Threads))
+    check(rc, "OLD_MGQD_COEFS")
+
+
+def MLOQD_FV(Eg_avg, Eg_edgV, Eg_edgH, Fxg_edgV, Fyg_edgH, fg_avg_xx, fg_avg_yy, fg_edgV_xx, fg_edgV_xy, fg_edgH_yy,
+             fg_edgH_xy, Cg_L, Cg_B, Cg_R, Cg_T, Eg_in_L, Eg_in_B, Eg_in_R, Eg_in_T, Fg_in_L, Fg_in_B, Fg_in_R, Fg_in_T,
+             Src, KapE, KapR, Delx, Dely, A, c, Delt, Theta, Open_Threads, Res_Calc, MGQD_Residual, MGQD_BC_Residual,
+             G_old, Pold_L, Pold_B, Pold_R, Pold_T, Eg_avg_old, Fxg_edgV_old, Fyg_edgH_old, MGQD_Kits, Fdt_Weight,
+             Fin_Weight, Ein_Weight):
+    """SUBROUTINE MLOQD_FV, MainSrc/MLOQD_SOLVES.f08:78-362, with QD_FV (QD_SOLVERS.f08:40-538) on the
+    device.  Eg_avg/Eg_edgV/Eg_edgH are the initial guess and are overwritten with the solution;
+    MGQD_Kits must be an int32 array of n_g entries.  Raises TrtError (TRT_ERR_NOCONV) when a group does
+    not converge, after filling the outputs with the last iterate."""
+    nx, ny, ng = Eg_avg.shape
+    C, V, H = (nx, ny, ng), (nx + 1, ny, ng), (nx, ny + 1, ng)
+    for o, s in ((Eg_avg, C), (Eg_edgV, V), (Eg_edgH, H), (Fxg_edgV, V), (Fyg_edgH, H), (MGQD_Residual, (ng, 5, 5)),
+                 (MGQD_BC_Residual, (ng, 4))):
+        _out(o, s)
+    if not (isinstance(MGQD_Kits, np.ndarray) and MGQD_Kits.dtype == np.int32 and MGQD_Kits.shape == (ng,)):
+        raise ValueError("MGQD_Kits must be an int32 array of n_g entries")
+    by, bx = (ny, ng), (nx, ng)
+    ins = [_f64(a, s) for a, s in zip(
+        (fg_avg_xx, fg_avg_yy, fg_edgV_xx, fg_edgV_xy, fg_edgH_yy, fg_edgH_xy, Cg_L, Cg_B, Cg_R, Cg_T, Eg_in_L, Eg_in_B,
+         Eg_in_R, Eg_in_T, Fg_in_L, Fg_in_B, Fg_in_R, Fg_in_T, Src, KapE, KapR, Delx, Dely, A),
+        (C, C, V, V, H, H, by, bx, by, bx, by, bx, by, bx, by, bx, by, bx, C, C, C, (nx,), (ny,), (nx, ny)))]
+    old = [_f64(a, s) for a, s in zip((G_old, Pold_L, Pold_B, Pold_R, Pold_T, Eg_avg_old, Fxg_edgV_old, Fyg_edgH_old),
+                                      (C, C, C, C, C, C, V, H))]
+    rc = _lib.lib().trt_mloqd_fv(nx, ny, ng, dptr(Eg_avg), dptr(Eg_edgV), dptr(Eg_edgH), dptr(Fxg_edgV), dptr(Fyg_edgH),
+                                 *[dptr(a) for a in ins], float(c), float(Delt), float(Theta), int(Open_Threads),
+                                 int(bool(Res_Calc)), dptr(MGQD_Residual), dptr(MGQD_BC_Residual),
+                                 *[dptr(a) for a in old], iptr(MGQD_Kits), float(Fdt_Weight), float(Fin_Weight),
+                                 float(Ein_Weight))
+    check(rc, "MLOQD_FV")
+
+
+def mgqd_set_tolerance(tol=1e-13, maxit=1000):
+    """Convergence settings of MLOQD_FV's device solve (process-wide)."""
+    check(_lib.lib().trt_mgqd_set_tolerance(float(tol), int(maxit)), "mgqd_set_tolerance")
+
+
+def mgqd_last_stats():
+    """(device ms of the last MLOQD_FV solve without its copies, largest iteration count)."""
+    ms, its = ctypes.c_double(0), ctypes.c_int(0)
+    check(_lib.lib().trt_mgqd_last_stats(ctypes.byref(ms), ctypes.byref(its)), "mgqd_last_stats")
+    return ms.value, its.value
+
+
 def Bg_planck_calc(T, nu_low, nu_high, comp_unit):
     """FUNCTION Bg_planck_calc, MainSrc/TEMP_FUNCTIONS.f08:90-108 (host evaluation in the library)."""
     return _lib.lib().trt_bg_planck(float(T), float(nu_low), float(nu_high), float(comp_unit))

@@ -1,0 +1,893 @@
+// Multigroup low-order quasidiffusion (MGQD) solve on the device, FP64 (sm_100a).
+//
+// Replaces the per-group loop of MLOQD_FV (MainSrc/MLOQD_SOLVES.f08:78-362) and its linear solver
+// QD_FV (MainSrc/QD_SOLVERS.f08:40-538: CSR assembly, SPARSKIT2 ILUT + BiCGSTAB).  All groups are
+// solved at once: every kernel runs a (blocks, group) grid and skips groups that have converged.
+//
+// Unknowns of group g, one contiguous segment of nU = 3 nx ny + nx + ny doubles:
+//   [ E_avg (nx*ny, x fastest) | E_edgV ((nx+1)*ny) | E_edgH (nx*(ny+1)) ]
+// The equation of each unknown is the row the reference assembles for it (QD_SOLVERS.f08:66-386):
+// energy balance on the cell, x-momentum balance (or the left/right boundary condition) on the
+// vertical edge, y-momentum balance (or the bottom/top boundary condition) on the horizontal edge.
+// The matrix is never formed: kernels apply it from per-cell coefficient planes.  A "position"
+// (i, j), 0 <= i <= nx, 0 <= j <= ny, owns cell (i, j), vertical edge (i, j) and horizontal edge
+// (i, j) where they exist, so one (nx+1)(ny+1) launch covers every row once.
+//
+// Krylov method: BiCGSTAB with right preconditioning, as the reference (ipar(2) = 2).  The
+// preconditioner replaces ILUT (whose triangular solves are sequential) by a physics-based one:
+//   1. drop the cross-derivative (f_xy) terms of the momentum rows; each edge unknown is then an
+//      explicit combination of its own residual and its two neighbouring cell unknowns;
+//   2. substitute the edges into the energy balance: a 5-point cell-centred operator S;
+//   3. one multigrid V(2,2)-cycle on S (red-black Gauss-Seidel smoothing; coarse operators by
+//      2x2 aggregation with the coupling scaled by 1/2, the cell-centred rediscretisation factor);
+//   4. back-substitute the edges.
+// Groups whose opacity keeps the system diagonally dominant converge in a few iterations; optically
+// thin groups, where the system is a diffusion operator with diffusion number (c dt / dx)^2 / 3,
+// take tens (no growth with the grid beyond the multigrid's).
+//
+// Every reduction has a fixed order (per-block trees, then one warp per group over the block
+// partials in block order), so results are bit-reproducible run to run.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace trt_mgqd {
+
+constexpr int kMaxLevels = 16;
+constexpr int kRedBlock = 256;   // threads of every reducing kernel
+
+struct Dims {
+  int nx, ny, ng;
+  long nC, nV, nH, nU;   // per-group sizes
+  __host__ __device__ long oV() const { return nC; }
+  __host__ __device__ long oH() const { return nC + nV; }
+  __host__ __device__ long npos() const { return (long)(nx + 1) * (ny + 1); }
+};
+
+// Inputs of MLOQD_FV in the reference's Fortran layouts (x fastest, then y, then group).
+struct Inputs {
+  const double *fxx, *fyy, *fVxx, *fVxy, *fHyy, *fHxy;
+  const double *CgL, *CgB, *CgR, *CgT, *EinL, *EinB, *EinR, *EinT, *FinL, *FinB, *FinR, *FinT;
+  const double *Src, *KapE, *KapR, *Delx, *Dely, *A;
+  const double *Gold, *PoldL, *PoldB, *PoldR, *PoldT, *Eold, *Fxold, *Fyold;
+  double c, Delt, Theta, Fdt, Fin, Ein;
+};
+
+// Per-group coefficient planes (cell planes nC per group; edge planes nV / nH per group).
+struct Coefs {
+  double *Xi, *PhL, *PhB, *PhR, *PhT;
+  double *EBL, *EBB, *EBC, *EBR, *EBT;
+  double *MXB, *MXC, *MXT, *MYL, *MYC, *MYR;
+  double *dV, *dH;                      // diagonal of the edge rows (MBx_R / Cp_L / Cp_R; MBy_T / Cp_B / Cp_T)
+  double* b;                            // right-hand side, unknown layout
+  double *aV, *blV, *brV, *aH, *bbH, *btH;   // edge elimination of the preconditioner
+};
+
+struct Level {
+  int mx, my;
+  long n;                                     // cells per group
+  double *sC, *sW, *sE, *sS, *sN, *x, *b;     // [group][cell]
+};
+
+struct Scal {
+  double rho, alpha, omega, beta;
+  double res, xmax;    // last convergence norms
+  int done;            // 0 running, 1 converged, -1 stopped without converging
+  int its;
+};
+
+// ------------------------------------------------------------------------------------------------
+// coefficients (MLOQD_SOLVES.f08:148-220)
+// ------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ double xi_of(const Inputs& in, const Dims& d, int i, int j, int g) {
+  const long k = i + (long)d.nx * j;
+  return in.A[k] * (in.Fdt / (in.Theta * in.c * in.Delt) + in.KapR[k + d.nC * g]) / 2.0;
+}
+__device__ __forceinline__ double phat(double Fdt_A_F, double Pold, const Inputs& in, double xi) {
+  return (Fdt_A_F / (2.0 * in.Theta * in.c * in.Delt) + Pold) / xi;
+}
+
+// Cell coefficients, edge diagonals and the right-hand side.  One thread per position.
+__global__ void coef_kernel(const Inputs in, const Dims d, const Coefs cf) {
+  const int g = blockIdx.y;
+  const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (pos >= d.npos()) return;
+  const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+  const int nx = d.nx, ny = d.ny;
+  const double c = in.c;
+  const long gC = d.nC * g, gV = d.nV * g, gH = d.nH * g;
+  auto V = [&](int ii, int jj) { return gV + ii + (long)(nx + 1) * jj; };
+  auto H = [&](int ii, int jj) { return gH + ii + (long)nx * jj; };
+  auto CI = [&](int ii, int jj) { return ii + (long)nx * jj; };
+  auto PhL = [&](int ii, int jj) {
+    const long k = CI(ii, jj);
+    return phat(in.Fdt * in.A[k] * in.Fxold[V(ii, jj)], in.PoldL[gC + k], in, xi_of(in, d, ii, jj, g));
+  };
+  auto PhR = [&](int ii, int jj) {
+    const long k = CI(ii, jj);
+    return phat(in.Fdt * in.A[k] * in.Fxold[V(ii + 1, jj)], in.PoldR[gC + k], in, xi_of(in, d, ii, jj, g));
+  };
+  auto PhB = [&](int ii, int jj) {
+    const long k = CI(ii, jj);
+    return phat(in.Fdt * in.A[k] * in.Fyold[H(ii, jj)], in.PoldB[gC + k], in, xi_of(in, d, ii, jj, g));
+  };
+  auto PhT = [&](int ii, int jj) {
+    const long k = CI(ii, jj);
+    return phat(in.Fdt * in.A[k] * in.Fyold[H(ii, jj + 1)], in.PoldT[gC + k], in, xi_of(in, d, ii, jj, g));
+  };
+
+  if (i < nx && j < ny) {
+    const long k = CI(i, j), kg = gC + k;
+    const double a = in.A[k], dx = in.Delx[i], dy = in.Dely[j];
+    const double xi = xi_of(in, d, i, j, g);
+    const double pl = PhL(i, j), pb = PhB(i, j), pr = PhR(i, j), pt = PhT(i, j);
+    cf.Xi[kg] = xi;
+    cf.PhL[kg] = pl;
+    cf.PhB[kg] = pb;
+    cf.PhR[kg] = pr;
+    cf.PhT[kg] = pt;
+    cf.b[d.nU * g + k] = a * in.Src[kg] + a * in.Eold[kg] / (in.Theta * in.Delt) + in.Gold[kg] + dy * (pl - pr) +
+                         dx * (pb - pt);
+    cf.EBC[kg] = (a * (1.0 / (in.Theta * in.Delt) + c * in.KapE[kg]) + 2.0 * c * (dy * dy) * in.fxx[kg] / xi +
+                  2.0 * c * (dx * dx) * in.fyy[kg] / xi);
+    cf.EBR[kg] = -c * (dy * dy) * in.fVxx[V(i + 1, j)] / xi;
+    cf.EBL[kg] = -c * (dy * dy) * in.fVxx[V(i, j)] / xi;
+    cf.EBT[kg] = -c * (dx * dx) * in.fHyy[H(i, j + 1)] / xi;
+    cf.EBB[kg] = -c * (dx * dx) * in.fHyy[H(i, j)] / xi;
+    cf.MXC[kg] = c * dy * in.fxx[kg] / xi;
+    cf.MXT[kg] = -c * dx * in.fHxy[H(i, j + 1)] / (2.0 * xi);
+    cf.MXB[kg] = c * dx * in.fHxy[H(i, j)] / (2.0 * xi);
+    cf.MYC[kg] = c * dx * in.fyy[kg] / xi;
+    cf.MYR[kg] = -c * dy * in.fVxy[V(i + 1, j)] / (2.0 * xi);
+    cf.MYL[kg] = c * dy * in.fVxy[V(i, j)] / (2.0 * xi);
+  }
+  if (j < ny) {   // vertical edge (i, j)
+    const double dy = in.Dely[j];
+    const long bj = (long)ny * g + j;
+    double dv, bv;
+    if (i == 0) {
+      dv = c * in.CgL[bj] - c * dy * in.fVxx[V(0, j)] / xi_of(in, d, 0, j, g);
+      bv = in.Ein * c * in.CgL[bj] * in.EinL[bj] - in.Fin * in.FinL[bj] + PhL(0, j);
+    } else if (i == nx) {
+      dv = c * in.CgR[bj] + c * dy * in.fVxx[V(nx, j)] / xi_of(in, d, nx - 1, j, g);
+      bv = in.Ein * c * in.CgR[bj] * in.EinR[bj] - in.Fin * in.FinR[bj] + PhR(nx - 1, j);
+    } else {
+      dv = -(c * dy / xi_of(in, d, i - 1, j, g) + c * dy / xi_of(in, d, i, j, g)) * in.fVxx[V(i, j)];
+      bv = PhL(i, j) - PhR(i - 1, j);
+    }
+    const long e = i + (long)(nx + 1) * j;
+    cf.dV[gV + e] = dv;
+    cf.b[d.nU * g + d.oV() + e] = bv;
+  }
+  if (i < nx) {   // horizontal edge (i, j)
+    const double dx = in.Delx[i];
+    const long bi = (long)nx * g + i;
+    double dh, bh;
+    if (j == 0) {
+      dh = c * in.CgB[bi] - c * dx * in.fHyy[H(i, 0)] / xi_of(in, d, i, 0, g);
+      bh = in.Ein * c * in.CgB[bi] * in.EinB[bi] - in.Fin * in.FinB[bi] + PhB(i, 0);
+    } else if (j == ny) {
+      dh = c * in.CgT[bi] + c * dx * in.fHyy[H(i, ny)] / xi_of(in, d, i, ny - 1, g);
+      bh = in.Ein * c * in.CgT[bi] * in.EinT[bi] - in.Fin * in.FinT[bi] + PhT(i, ny - 1);
+    } else {
+      dh = -(c * dx / xi_of(in, d, i, j - 1, g) + c * dx / xi_of(in, d, i, j, g)) * in.fHyy[H(i, j)];
+      bh = PhB(i, j) - PhT(i, j - 1);
+    }
+    const long e = i + (long)nx * j;
+    cf.dH[gH + e] = dh;
+    cf.b[d.nU * g + d.oH() + e] = bh;
+  }
+}
+
+// Edge-elimination coefficients of vertical edge (i, j): E_V = a r_V + bl E_C(i-1) + br E_C(i).
+__device__ __forceinline__ void edgeV_elim(const Coefs& cf, const Dims& d, int g, int i, int j, double* a,
+                                           double* bl, double* br) {
+  const double dv = cf.dV[d.nV * g + i + (long)(d.nx + 1) * j];
+  const long gC = d.nC * g + (long)d.nx * j;
+  *a = 1.0 / dv;
+  *bl = (i == 0) ? 0.0 : (i == d.nx ? cf.MXC[gC + i - 1] / dv : -cf.MXC[gC + i - 1] / dv);
+  *br = (i == d.nx) ? 0.0 : -cf.MXC[gC + i] / dv;
+}
+__device__ __forceinline__ void edgeH_elim(const Coefs& cf, const Dims& d, int g, int i, int j, double* a,
+                                           double* bb, double* bt) {
+  const double dh = cf.dH[d.nH * g + i + (long)d.nx * j];
+  const long gC = d.nC * g + i;
+  *a = 1.0 / dh;
+  *bb = (j == 0) ? 0.0 : (j == d.ny ? cf.MYC[gC + (long)d.nx * (j - 1)] / dh : -cf.MYC[gC + (long)d.nx * (j - 1)] / dh);
+  *bt = (j == d.ny) ? 0.0 : -cf.MYC[gC + (long)d.nx * j] / dh;
+}
+
+// Preconditioner coefficients: edge elimination planes and the fine cell operator S.
+__global__ void prec_coef_kernel(const Dims d, const Coefs cf, const Level L0) {
+  const int g = blockIdx.y;
+  const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (pos >= d.npos()) return;
+  const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+  if (j < d.ny) {
+    double a, bl, br;
+    edgeV_elim(cf, d, g, i, j, &a, &bl, &br);
+    const long e = d.nV * g + i + (long)(d.nx + 1) * j;
+    cf.aV[e] = a;
+    cf.blV[e] = bl;
+    cf.brV[e] = br;
+  }
+  if (i < d.nx) {
+    double a, bb, bt;
+    edgeH_elim(cf, d, g, i, j, &a, &bb, &bt);
+    const long e = d.nH * g + i + (long)d.nx * j;
+    cf.aH[e] = a;
+    cf.bbH[e] = bb;
+    cf.btH[e] = bt;
+  }
+  if (i < d.nx && j < d.ny) {
+    double aL, blL, brL, aR, blR, brR, aB, bbB, btB, aT, bbT, btT;
+    edgeV_elim(cf, d, g, i, j, &aL, &blL, &brL);
+    edgeV_elim(cf, d, g, i + 1, j, &aR, &blR, &brR);
+    edgeH_elim(cf, d, g, i, j, &aB, &bbB, &btB);
+    edgeH_elim(cf, d, g, i, j + 1, &aT, &bbT, &btT);
+    const long kg = d.nC * g + i + (long)d.nx * j;
+    const double ebl = cf.EBL[kg], ebr = cf.EBR[kg], ebb = cf.EBB[kg], ebt = cf.EBT[kg];
+    L0.sC[kg] = cf.EBC[kg] + ebl * brL + ebr * blR + ebb * btB + ebt * bbT;
+    L0.sW[kg] = ebl * blL;
+    L0.sE[kg] = ebr * brR;
+    L0.sS[kg] = ebb * bbB;
+    L0.sN[kg] = ebt * btT;
+  }
+}
+
+// Coarse operator of level f+1 from level f: 2x2 aggregation; couplings across the coarse cell's
+// faces scaled by alpha = 1/2, the remainder moved to the diagonal (row sums kept).
+__device__ __forceinline__ void coarse_op_cell(const Level& F, const Level& Cs, int g, int I, int J) {
+  constexpr double alpha = 0.5;
+  double D = 0.0, eW = 0.0, eE = 0.0, eS = 0.0, eN = 0.0;
+  for (int dj = 0; dj < 2; ++dj)
+    for (int di = 0; di < 2; ++di) {
+      const int i = 2 * I + di, j = 2 * J + dj;
+      if (i >= F.mx || j >= F.my) continue;
+      const long k = F.n * g + i + (long)F.mx * j;
+      D += F.sC[k];
+      if (di == 1) D += F.sW[k]; else eW += F.sW[k];
+      if (di == 0 && i + 1 < F.mx) D += F.sE[k]; else eE += F.sE[k];
+      if (dj == 1) D += F.sS[k]; else eS += F.sS[k];
+      if (dj == 0 && j + 1 < F.my) D += F.sN[k]; else eN += F.sN[k];
+    }
+  const long kc = Cs.n * g + I + (long)Cs.mx * J;
+  Cs.sC[kc] = D + (1.0 - alpha) * (eW + eE + eS + eN);
+  Cs.sW[kc] = alpha * eW;
+  Cs.sE[kc] = alpha * eE;
+  Cs.sS[kc] = alpha * eS;
+  Cs.sN[kc] = alpha * eN;
+}
+
+__global__ void coarse_op_kernel(const Level F, const Level Cs) {
+  const int g = blockIdx.y;
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p >= Cs.n) return;
+  coarse_op_cell(F, Cs, g, (int)(p % Cs.mx), (int)(p / Cs.mx));
+}
+
+// ------------------------------------------------------------------------------------------------
+// multigrid pieces (cell-centred 5-point operator)
+// ------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ double s_offdiag(const Level& L, long base, int i, int j, long k) {
+  double s = 0.0;
+  if (i > 0) s += L.sW[k] * L.x[k - 1];
+  if (i + 1 < L.mx) s += L.sE[k] * L.x[k + 1];
+  if (j > 0) s += L.sS[k] * L.x[k - L.mx];
+  if (j + 1 < L.my) s += L.sN[k] * L.x[k + L.mx];
+  (void)base;
+  return s;
+}
+
+// One colour of a red-black Gauss-Seidel sweep at cell (i, j); zero_init: the iterate is zero
+// (red cells take b/sC and black cells are cleared).
+__device__ __forceinline__ void smooth_cell(const Level& L, int g, int i, int j, int color, bool zero_init) {
+  const long k = L.n * g + i + (long)L.mx * j;
+  if (((i + j) & 1) != color) {
+    if (zero_init) L.x[k] = 0.0;
+    return;
+  }
+  if (zero_init) {
+    L.x[k] = L.b[k] / L.sC[k];
+    return;
+  }
+  L.x[k] = (L.b[k] - s_offdiag(L, 0, i, j, k)) / L.sC[k];
+}
+
+__device__ __forceinline__ void restrict_cell(const Level& F, const Level& Cs, int g, int I, int J) {
+  double r = 0.0;
+  for (int dj = 0; dj < 2; ++dj)
+    for (int di = 0; di < 2; ++di) {
+      const int i = 2 * I + di, j = 2 * J + dj;
+      if (i >= F.mx || j >= F.my) continue;
+      const long k = F.n * g + i + (long)F.mx * j;
+      r += F.b[k] - F.sC[k] * F.x[k] - s_offdiag(F, 0, i, j, k);
+    }
+  Cs.b[Cs.n * g + I + (long)Cs.mx * J] = r;
+}
+
+__device__ __forceinline__ void prolong_cell(const Level& F, const Level& Cs, int g, int i, int j) {
+  F.x[F.n * g + i + (long)F.mx * j] += Cs.x[Cs.n * g + (i >> 1) + (long)Cs.mx * (j >> 1)];
+}
+
+__global__ void smooth_kernel(const Level L, const int* __restrict__ done, int color, int zero_init) {
+  const int g = blockIdx.y;
+  if (done[g]) return;
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p >= L.n) return;
+  smooth_cell(L, g, (int)(p % L.mx), (int)(p / L.mx), color, zero_init != 0);
+}
+
+__global__ void restrict_kernel(const Level F, const Level Cs, const int* __restrict__ done) {
+  const int g = blockIdx.y;
+  if (done[g]) return;
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p >= Cs.n) return;
+  restrict_cell(F, Cs, g, (int)(p % Cs.mx), (int)(p / Cs.mx));
+}
+
+__global__ void prolong_kernel(const Level F, const Level Cs, const int* __restrict__ done) {
+  const int g = blockIdx.y;
+  if (done[g]) return;
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p >= F.n) return;
+  prolong_cell(F, Cs, g, (int)(p % F.mx), (int)(p / F.mx));
+}
+
+struct LevelSet {
+  Level L[kMaxLevels];
+  int n;
+};
+
+// The V-cycle below level k0 (levels k0 .. n-1, all small) by one CTA per group, __syncthreads
+// between the phases.  Level k0's b is given; its x is returned.
+__global__ void small_vcycle_kernel(const LevelSet ls, int k0, int nu1, int nu2, int coarse_sweeps,
+                                    const int* __restrict__ done) {
+  const int g = blockIdx.x;
+  if (done[g]) return;
+  auto sweep = [&](int k, int color, bool zero) {
+    const Level& L = ls.L[k];
+    for (long p = threadIdx.x; p < L.n; p += blockDim.x) smooth_cell(L, g, (int)(p % L.mx), (int)(p / L.mx), color, zero);
+    __syncthreads();
+  };
+  auto smooth = [&](int k, int sweeps, bool zero) {
+    for (int s = 0; s < sweeps; ++s) {
+      sweep(k, 0, zero && s == 0);
+      sweep(k, 1, false);
+    }
+  };
+  const int last = ls.n - 1;
+  for (int k = k0; k < last; ++k) {
+    smooth(k, nu1, true);
+    const Level &F = ls.L[k], &Cs = ls.L[k + 1];
+    for (long p = threadIdx.x; p < Cs.n; p += blockDim.x) restrict_cell(F, Cs, g, (int)(p % Cs.mx), (int)(p / Cs.mx));
+    __syncthreads();
+  }
+  smooth(last, coarse_sweeps, true);
+  for (int k = last - 1; k >= k0; --k) {
+    const Level &F = ls.L[k], &Cs = ls.L[k + 1];
+    for (long p = threadIdx.x; p < F.n; p += blockDim.x) prolong_cell(F, Cs, g, (int)(p % F.mx), (int)(p / F.mx));
+    __syncthreads();
+    smooth(k, nu2, false);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Krylov pieces
+// ------------------------------------------------------------------------------------------------
+
+// Row of the reduced system owned by a position, applied to x (unknown layout of group g).
+struct RowOut {
+  double yc, yv, yh;
+  bool hc, hv, hh;
+};
+
+__device__ __forceinline__ RowOut apply_rows(const Coefs& cf, const Dims& d, int g, int i, int j, const double* x) {
+  const int nx = d.nx, ny = d.ny;
+  const double* xc = x + d.nU * g;
+  const double* xv = xc + d.oV();
+  const double* xh = xc + d.oH();
+  const long gC = d.nC * g;
+  auto C = [&](int ii, int jj) { return ii + (long)nx * jj; };
+  auto Vx = [&](int ii, int jj) { return xv[ii + (long)(nx + 1) * jj]; };
+  auto Hx = [&](int ii, int jj) { return xh[ii + (long)nx * jj]; };
+  RowOut o{0.0, 0.0, 0.0, false, false, false};
+  if (i < nx && j < ny) {
+    const long k = C(i, j), kg = gC + k;
+    o.yc = cf.EBL[kg] * Vx(i, j) + cf.EBB[kg] * Hx(i, j) + cf.EBC[kg] * xc[k] + cf.EBR[kg] * Vx(i + 1, j) +
+           cf.EBT[kg] * Hx(i, j + 1);
+    o.hc = true;
+  }
+  if (j < ny) {
+    const double dv = cf.dV[d.nV * g + i + (long)(nx + 1) * j] * Vx(i, j);
+    double y;
+    if (i == 0) {
+      const long b = gC + C(0, j);
+      y = dv - cf.MXB[b] * Hx(0, j) + cf.MXC[b] * xc[C(0, j)] - cf.MXT[b] * Hx(0, j + 1);
+    } else if (i == nx) {
+      const long a = gC + C(nx - 1, j);
+      y = dv - cf.MXB[a] * Hx(nx - 1, j) - cf.MXC[a] * xc[C(nx - 1, j)] - cf.MXT[a] * Hx(nx - 1, j + 1);
+    } else {
+      const long a = gC + C(i - 1, j), b = gC + C(i, j);
+      y = cf.MXB[a] * Hx(i - 1, j) + cf.MXC[a] * xc[C(i - 1, j)] + dv + cf.MXT[a] * Hx(i - 1, j + 1) -
+          cf.MXB[b] * Hx(i, j) + cf.MXC[b] * xc[C(i, j)] - cf.MXT[b] * Hx(i, j + 1);
+    }
+    o.yv = y;
+    o.hv = true;
+  }
+  if (i < nx) {
+    const double dh = cf.dH[d.nH * g + i + (long)nx * j] * Hx(i, j);
+    double y;
+    if (j == 0) {
+      const long b = gC + C(i, 0);
+      y = -cf.MYL[b] * Vx(i, 0) + dh + cf.MYC[b] * xc[C(i, 0)] - cf.MYR[b] * Vx(i + 1, 0);
+    } else if (j == ny) {
+      const long a = gC + C(i, ny - 1);
+      y = -cf.MYL[a] * Vx(i, ny - 1) - cf.MYC[a] * xc[C(i, ny - 1)] - cf.MYR[a] * Vx(i + 1, ny - 1) + dh;
+    } else {
+      const long a = gC + C(i, j - 1), b = gC + C(i, j);
+      y = cf.MYL[a] * Vx(i, j - 1) + cf.MYC[a] * xc[C(i, j - 1)] + cf.MYR[a] * Vx(i + 1, j - 1) + dh -
+          cf.MYL[b] * Vx(i, j) + cf.MYC[b] * xc[C(i, j)] - cf.MYR[b] * Vx(i + 1, j);
+    }
+    o.yh = y;
+    o.hh = true;
+  }
+  return o;
+}
+
+// Block reduction of NQ values per thread into part[(g * gridDim.x + blockIdx.x) * NQ + q] (kind 0:
+// sum, kind 1: max): xor-shuffle tree inside each warp, then warp 0 over the warps in warp order.
+template <int NQ>
+__device__ __forceinline__ void block_reduce(double (&v)[NQ], const int (&kind)[NQ], double* part, int g) {
+  constexpr int kWarps = kRedBlock / 32;
+  __shared__ double sh[NQ][kWarps];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double x = v[q];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_xor_sync(0xffffffffu, x, o);
+      x = kind[q] ? fmax(x, y) : x + y;
+    }
+    if (lane == 0) sh[q][warp] = x;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    for (int q = lane; q < NQ; q += 32) {
+      double x = sh[q][0];
+      for (int w = 1; w < kWarps; ++w) x = kind[q] ? fmax(x, sh[q][w]) : x + sh[q][w];
+      part[((long)g * gridDim.x + blockIdx.x) * NQ + q] = x;
+    }
+  }
+}
+
+// Sums (kind 0) or maxima (kind 1) of the block partials of group g by one warp, fixed order.
+template <int NQ>
+__device__ __forceinline__ void warp_finish(const double* part, int nblk, int g, const int (&kind)[NQ],
+                                            double (&out)[NQ]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) out[q] = 0.0;
+  for (int b = lane; b < nblk; b += 32)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const double v = part[((long)g * nblk + b) * NQ + q];
+      out[q] = kind[q] ? fmax(out[q], v) : out[q] + v;
+    }
+#pragma unroll
+  for (int q = 0; q < NQ; ++q)
+    for (int o = 16; o > 0; o >>= 1) {
+      const double w = __shfl_xor_sync(0xffffffffu, out[q], o);
+      out[q] = kind[q] ? fmax(out[q], w) : out[q] + w;
+    }
+}
+
+struct Krylov {
+  double *x, *r, *rh, *p0, *p1, *v, *s, *t, *ph, *sh;
+  Scal* sc;
+  int* done;
+  double* part;      // [ng][nblk][4]
+  double tol;
+  int maxit;
+};
+
+// Jacobi scale of the row of unknown (cell / V edge / H edge) for the convergence norm.
+__device__ __forceinline__ double row_scale(const Coefs& cf, const Dims& d, int g, int kind, long e) {
+  if (kind == 0) return 1.0 / fabs(cf.EBC[d.nC * g + e]);
+  if (kind == 1) return 1.0 / fabs(cf.dV[d.nV * g + e]);
+  return 1.0 / fabs(cf.dH[d.nH * g + e]);
+}
+
+// r = b - A x, rh = r, p0 = p1 = v = 0; partials: (rh.r), max |r| / |diag|, max |x|.
+__global__ void __launch_bounds__(kRedBlock) init_kernel(const Coefs cf, const Dims d, const Krylov K) {
+  const int g = blockIdx.y;
+  const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double v3[3] = {0.0, 0.0, 0.0};
+  if (pos < d.npos()) {
+    const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+    const RowOut o = apply_rows(cf, d, g, i, j, K.x);
+    const long base = d.nU * g;
+    auto emit = [&](bool has, long u, double y, int kind, long e) {
+      if (!has) return;
+      const double r = cf.b[base + u] - y;
+      K.r[base + u] = r;
+      K.rh[base + u] = r;
+      K.p0[base + u] = 0.0;
+      K.p1[base + u] = 0.0;
+      K.v[base + u] = 0.0;
+      v3[0] += r * r;
+      v3[1] = fmax(v3[1], fabs(r) * row_scale(cf, d, g, kind, e));
+      v3[2] = fmax(v3[2], fabs(K.x[base + u]));
+    };
+    emit(o.hc, i + (long)d.nx * j, o.yc, 0, i + (long)d.nx * j);
+    emit(o.hv, d.oV() + i + (long)(d.nx + 1) * j, o.yv, 1, i + (long)(d.nx + 1) * j);
+    emit(o.hh, d.oH() + i + (long)d.nx * j, o.yh, 2, i + (long)d.nx * j);
+  }
+  const int kind[3] = {0, 1, 1};
+  block_reduce<3>(v3, kind, K.part, g);
+}
+
+__global__ void init_finish_kernel(const Krylov K, int nblk) {
+  const int g = blockIdx.x;
+  const int kind[3] = {0, 1, 1};
+  double o[3];
+  warp_finish<3>(K.part, nblk, g, kind, o);
+  if (threadIdx.x == 0) {
+    Scal s;
+    s.rho = o[0];
+    s.alpha = 1.0;
+    s.omega = 1.0;
+    s.beta = 0.0;
+    s.res = o[1];
+    s.xmax = o[2];
+    s.its = 0;
+    s.done = (o[1] <= K.tol * o[2] || o[0] == 0.0) ? 1 : 0;
+    K.sc[g] = s;
+    K.done[g] = s.done;
+  }
+}
+
+// Preconditioner input z and the level-0 right-hand side.  mode 0: z = p_new = r + beta (p_old -
+// omega v), stored into pnew; mode 1: z = s = r - alpha v, stored into s.
+__global__ void elim_kernel(const Coefs cf, const Dims d, const Krylov K, const Level L0, const double* __restrict__ pold,
+                            double* __restrict__ znew, int mode) {
+  const int g = blockIdx.y;
+  if (K.done[g]) return;
+  const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (pos >= d.npos()) return;
+  const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+  const int nx = d.nx, ny = d.ny;
+  const long base = d.nU * g;
+  const Scal sc = K.sc[g];
+  auto z = [&](long u) {
+    return mode == 0 ? K.r[base + u] + sc.beta * (pold[base + u] - sc.omega * K.v[base + u])
+                     : K.r[base + u] - sc.alpha * K.v[base + u];
+  };
+  auto uV = [&](int ii, int jj) { return d.oV() + ii + (long)(nx + 1) * jj; };
+  auto uH = [&](int ii, int jj) { return d.oH() + ii + (long)nx * jj; };
+  if (i < nx && j < ny) {
+    const long uc = i + (long)nx * j;
+    const double zc = z(uc);
+    znew[base + uc] = zc;
+    const long kg = d.nC * g + uc;
+    const long eL = d.nV * g + i + (long)(nx + 1) * j, eB = d.nH * g + i + (long)nx * j;
+    L0.b[kg] = zc - cf.EBL[kg] * (cf.aV[eL] * z(uV(i, j))) - cf.EBR[kg] * (cf.aV[eL + 1] * z(uV(i + 1, j))) -
+               cf.EBB[kg] * (cf.aH[eB] * z(uH(i, j))) - cf.EBT[kg] * (cf.aH[eB + nx] * z(uH(i, j + 1)));
+  }
+  if (j < ny) znew[base + uV(i, j)] = z(uV(i, j));
+  if (i < nx) znew[base + uH(i, j)] = z(uH(i, j));
+}
+
+// Back-substitution of the edges: y = preconditioned z (cells from the level-0 solution).
+__global__ void backsub_kernel(const Coefs cf, const Dims d, const Krylov K, const Level L0,
+                               const double* __restrict__ zin, double* __restrict__ y) {
+  const int g = blockIdx.y;
+  if (K.done[g]) return;
+  const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (pos >= d.npos()) return;
+  const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+  const int nx = d.nx, ny = d.ny;
+  const long base = d.nU * g;
+  const double* xc = L0.x + d.nC * g;
+  if (i < nx && j < ny) y[base + i + (long)nx * j] = xc[i + (long)nx * j];
+  if (j < ny) {
+    const long e = i + (long)(nx + 1) * j, ev = d.nV * g + e;
+    double val = cf.aV[ev] * zin[base + d.oV() + e];
+    if (i > 0) val += cf.blV[ev] * xc[i - 1 + (long)nx * j];
+    if (i < nx) val += cf.brV[ev] * xc[i + (long)nx * j];
+    y[base + d.oV() + e] = val;
+  }
+  if (i < nx) {
+    const long e = i + (long)nx * j, eh = d.nH * g + e;
+    double val = cf.aH[eh] * zin[base + d.oH() + e];
+    if (j > 0) val += cf.bbH[eh] * xc[i + (long)nx * (j - 1)];
+    if (j < ny) val += cf.btH[eh] * xc[i + (long)nx * j];
+    y[base + d.oH() + e] = val;
+  }
+}
+
+// out = A in; partials: mode 0: (rh.out); mode 1: (out.s), (out.out).
+__global__ void __launch_bounds__(kRedBlock) matvec_kernel(const Coefs cf, const Dims d, const Krylov K,
+                                                           const double* __restrict__ in, double* __restrict__ out,
+                                                           int mode) {
+  const int g = blockIdx.y;
+  if (K.done[g]) return;   // uniform over the block: no thread reaches the reduction
+  const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double v2[2] = {0.0, 0.0};
+  if (pos < d.npos()) {
+    const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+    const RowOut o = apply_rows(cf, d, g, i, j, in);
+    const long base = d.nU * g;
+    auto emit = [&](bool has, long u, double y) {
+      if (!has) return;
+      out[base + u] = y;
+      if (mode == 0) {
+        v2[0] += K.rh[base + u] * y;
+      } else {
+        v2[0] += y * K.s[base + u];
+        v2[1] += y * y;
+      }
+    };
+    emit(o.hc, i + (long)d.nx * j, o.yc);
+    emit(o.hv, d.oV() + i + (long)(d.nx + 1) * j, o.yv);
+    emit(o.hh, d.oH() + i + (long)d.nx * j, o.yh);
+  }
+  const int kind[2] = {0, 0};
+  block_reduce<2>(v2, kind, K.part, g);
+}
+
+// alpha = rho / (rh.v)   (mode 0);   omega = (t.s) / (t.t)   (mode 1)
+__global__ void scalar_finish_kernel(const Krylov K, int nblk, int mode) {
+  const int g = blockIdx.x;
+  if (K.done[g]) return;
+  const int kind[2] = {0, 0};
+  double o[2];
+  warp_finish<2>(K.part, nblk, g, kind, o);
+  if (threadIdx.x == 0) {
+    Scal& s = K.sc[g];
+    if (mode == 0) {
+      s.alpha = (o[0] != 0.0) ? s.rho / o[0] : 0.0;
+    } else {
+      s.omega = (o[1] != 0.0) ? o[0] / o[1] : 0.0;
+    }
+  }
+}
+
+// x += alpha ph + omega sh; r = s - omega t; partials: (rh.r), max |r| / |diag|, max |x|.
+__global__ void __launch_bounds__(kRedBlock) update_kernel(const Coefs cf, const Dims d, const Krylov K) {
+  const int g = blockIdx.y;
+  if (K.done[g]) return;
+  const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double v3[3] = {0.0, 0.0, 0.0};
+  if (pos < d.npos()) {
+    const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+    const Scal sc = K.sc[g];
+    const long base = d.nU * g;
+    auto emit = [&](long u, int kind, long e) {
+      const double xn = K.x[base + u] + sc.alpha * K.ph[base + u] + sc.omega * K.sh[base + u];
+      const double rn = K.s[base + u] - sc.omega * K.t[base + u];
+      K.x[base + u] = xn;
+      K.r[base + u] = rn;
+      v3[0] += K.rh[base + u] * rn;
+      v3[1] = fmax(v3[1], fabs(rn) * row_scale(cf, d, g, kind, e));
+      v3[2] = fmax(v3[2], fabs(xn));
+    };
+    if (i < d.nx && j < d.ny) emit(i + (long)d.nx * j, 0, i + (long)d.nx * j);
+    if (j < d.ny) emit(d.oV() + i + (long)(d.nx + 1) * j, 1, i + (long)(d.nx + 1) * j);
+    if (i < d.nx) emit(d.oH() + i + (long)d.nx * j, 2, i + (long)d.nx * j);
+  }
+  const int kind[3] = {0, 1, 1};
+  block_reduce<3>(v3, kind, K.part, g);
+}
+
+// rho_new, beta, convergence test.  done: 1 converged; -1 breakdown or iteration limit.
+__global__ void update_finish_kernel(const Krylov K, int nblk) {
+  const int g = blockIdx.x;
+  if (K.done[g]) return;
+  const int kind[3] = {0, 1, 1};
+  double o[3];
+  warp_finish<3>(K.part, nblk, g, kind, o);
+  if (threadIdx.x == 0) {
+    Scal& s = K.sc[g];
+    s.its += 1;
+    s.res = o[1];
+    s.xmax = o[2];
+    int done = 0;
+    if (o[1] <= K.tol * o[2]) {
+      done = 1;
+    } else if (o[0] == 0.0 || s.omega == 0.0 || s.alpha == 0.0 || !(o[1] == o[1]) || s.its >= K.maxit) {
+      done = -1;
+    } else {
+      s.beta = (o[0] / s.rho) * (s.alpha / s.omega);
+      s.rho = o[0];
+    }
+    s.done = done;
+    K.done[g] = done;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// fluxes and residuals (MLOQD_SOLVES.f08:244-345)
+// ------------------------------------------------------------------------------------------------
+
+struct Outputs {
+  double *Fx, *Fy;   // (nx+1, ny, ng), (nx, ny+1, ng)
+};
+
+__global__ void flux_kernel(const Inputs in, const Dims d, const Coefs cf, const double* __restrict__ x,
+                            const Outputs out) {
+  const int g = blockIdx.y;
+  const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (pos >= d.npos()) return;
+  const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+  const int nx = d.nx, ny = d.ny;
+  const double c = in.c;
+  const double* E = x + d.nU * g;
+  const double* EV = E + d.oV();
+  const double* EH = E + d.oH();
+  const long gC = d.nC * g, gV = d.nV * g, gH = d.nH * g;
+  auto V = [&](int ii, int jj) { return ii + (long)(nx + 1) * jj; };
+  auto H = [&](int ii, int jj) { return ii + (long)nx * jj; };
+  auto C = [&](int ii, int jj) { return ii + (long)nx * jj; };
+  if (j < ny) {
+    // F on vertical edge i: the left half-cell of cell i, or the right half-cell of the last cell
+    const bool last = (i == nx);
+    const int ic = last ? nx - 1 : i;
+    const long k = C(ic, j), kg = gC + k;
+    const double xi = cf.Xi[kg];
+    double f;
+    if (!last)
+      f = -(c * in.Dely[j] / (xi)) * (in.fxx[kg] * E[k] - in.fVxx[gV + V(i, j)] * EV[V(i, j)]) -
+          (c * in.Delx[ic] / (2.0 * xi)) *
+              (in.fHxy[gH + H(ic, j + 1)] * EH[H(ic, j + 1)] - in.fHxy[gH + H(ic, j)] * EH[H(ic, j)]) +
+          cf.PhL[kg];
+    else
+      f = -(c * in.Dely[j] / (xi)) * (in.fVxx[gV + V(nx, j)] * EV[V(nx, j)] - in.fxx[kg] * E[k]) -
+          (c * in.Delx[ic] / (2.0 * xi)) *
+              (in.fHxy[gH + H(ic, j + 1)] * EH[H(ic, j + 1)] - in.fHxy[gH + H(ic, j)] * EH[H(ic, j)]) +
+          cf.PhR[kg];
+    out.Fx[gV + V(i, j)] = f;
+  }
+  if (i < nx) {
+    const bool last = (j == ny);
+    const int jc = last ? ny - 1 : j;
+    const long k = C(i, jc), kg = gC + k;
+    const double xi = cf.Xi[kg];
+    double f;
+    if (!last)
+      f = -(c * in.Delx[i] / (xi)) * (in.fyy[kg] * E[k] - in.fHyy[gH + H(i, j)] * EH[H(i, j)]) -
+          (c * in.Dely[jc] / (2.0 * xi)) *
+              (in.fVxy[gV + V(i + 1, jc)] * EV[V(i + 1, jc)] - in.fVxy[gV + V(i, jc)] * EV[V(i, jc)]) +
+          cf.PhB[kg];
+    else
+      f = -(c * in.Delx[i] / (xi)) * (in.fHyy[gH + H(i, ny)] * EH[H(i, ny)] - in.fyy[kg] * E[k]) -
+          (c * in.Dely[jc] / (2.0 * xi)) *
+              (in.fVxy[gV + V(i + 1, jc)] * EV[V(i + 1, jc)] - in.fVxy[gV + V(i, jc)] * EV[V(i, jc)]) +
+          cf.PhT[kg];
+    out.Fy[gH + H(i, j)] = f;
+  }
+}
+
+// Residuals of the un-reduced equations: 25 per-group values (5 equations x max, sum, sum of
+// squares, area-weighted sum, area-weighted sum of squares) and the 4 boundary maxima.
+constexpr int kNRes = 29;
+__global__ void __launch_bounds__(kRedBlock) residual_kernel(const Inputs in, const Dims d,
+                                                             const double* __restrict__ x, const Outputs out,
+                                                             double* part) {
+  const int g = blockIdx.y;
+  const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double v[kNRes];
+#pragma unroll
+  for (int q = 0; q < kNRes; ++q) v[q] = 0.0;
+  const int nx = d.nx, ny = d.ny;
+  if (pos < d.npos()) {
+    const int i = (int)(pos % (nx + 1)), j = (int)(pos / (nx + 1));
+    const double c = in.c, th = in.Theta, dt = in.Delt;
+    const double* E = x + d.nU * g;
+    const double* EV = E + d.oV();
+    const double* EH = E + d.oH();
+    const long gC = d.nC * g, gV = d.nV * g, gH = d.nH * g;
+    auto V = [&](int ii, int jj) { return ii + (long)(nx + 1) * jj; };
+    auto H = [&](int ii, int jj) { return ii + (long)nx * jj; };
+    const double* Fx = out.Fx + gV;
+    const double* Fy = out.Fy + gH;
+    if (i < nx && j < ny) {
+      const long k = i + (long)nx * j, kg = gC + k;
+      const double a = in.A[k], dx = in.Delx[i], dy = in.Dely[j];
+      double res[5];
+      res[0] = fabs(a * (1.0 / (th * dt) + c * in.KapE[kg]) * E[k] + dy * (Fx[V(i + 1, j)] - Fx[V(i, j)]) +
+                    dx * (Fy[H(i, j + 1)] - Fy[H(i, j)]) -
+                    (a * in.Src[kg] + a * in.Eold[kg] / (th * dt) + in.Gold[kg]));
+      const double xedge = (in.fHxy[gH + H(i, j + 1)] * EH[H(i, j + 1)] - in.fHxy[gH + H(i, j)] * EH[H(i, j)]);
+      const double yedge = (in.fVxy[gV + V(i + 1, j)] * EV[V(i + 1, j)] - in.fVxy[gV + V(i, j)] * EV[V(i, j)]);
+      const double kr = (1.0 / (th * c * dt) + in.KapR[kg]);
+      res[1] = fabs(a * kr * Fx[V(i, j)] / 2.0 + c * dy * (in.fxx[kg] * E[k] - in.fVxx[gV + V(i, j)] * EV[V(i, j)]) +
+                    c * dx * xedge / 2.0 - (a * in.Fxold[gV + V(i, j)] / (2.0 * th * c * dt) + in.PoldL[kg]));
+      res[2] = fabs(a * kr * Fy[H(i, j)] / 2.0 + c * dx * (in.fyy[kg] * E[k] - in.fHyy[gH + H(i, j)] * EH[H(i, j)]) +
+                    c * dy * yedge / 2.0 - (a * in.Fyold[gH + H(i, j)] / (2.0 * th * c * dt) + in.PoldB[kg]));
+      res[3] = fabs(a * kr * Fx[V(i + 1, j)] / 2.0 +
+                    c * dy * (in.fVxx[gV + V(i + 1, j)] * EV[V(i + 1, j)] - in.fxx[kg] * E[k]) + c * dx * xedge / 2.0 -
+                    (a * in.Fxold[gV + V(i + 1, j)] / (2.0 * th * c * dt) + in.PoldR[kg]));
+      res[4] = fabs(a * kr * Fy[H(i, j + 1)] / 2.0 +
+                    c * dx * (in.fHyy[gH + H(i, j + 1)] * EH[H(i, j + 1)] - in.fyy[kg] * E[k]) + c * dy * yedge / 2.0 -
+                    (a * in.Fyold[gH + H(i, j + 1)] / (2.0 * th * c * dt) + in.PoldT[kg]));
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        v[q] = res[q];
+        v[5 + q] = res[q];
+        v[10 + q] = res[q] * res[q];
+        v[15 + q] = a * res[q];
+        v[20 + q] = a * (res[q] * res[q]);
+      }
+    }
+    const long bj = (long)ny * g + j, bi = (long)nx * g + i;
+    if (i == 0 && j < ny)
+      v[25] = fabs(Fx[V(0, j)] - c * in.CgL[bj] * (EV[V(0, j)] - in.EinL[bj]) - in.FinL[bj]);
+    if (i == nx && j < ny)
+      v[27] = fabs(Fx[V(nx, j)] - c * in.CgR[bj] * (EV[V(nx, j)] - in.EinR[bj]) - in.FinR[bj]);
+    if (j == 0 && i < nx)
+      v[26] = fabs(Fy[H(i, 0)] - c * in.CgB[bi] * (EH[H(i, 0)] - in.EinB[bi]) - in.FinB[bi]);
+    if (j == ny && i < nx)
+      v[28] = fabs(Fy[H(i, ny)] - c * in.CgT[bi] * (EH[H(i, ny)] - in.EinT[bi]) - in.FinT[bi]);
+  }
+  int kind[kNRes];
+#pragma unroll
+  for (int q = 0; q < kNRes; ++q) kind[q] = (q < 5 || q >= 25) ? 1 : 0;
+  block_reduce<kNRes>(v, kind, part, g);
+}
+
+// MGQD_Residual(ng,5,5) and MGQD_BC_Residual(ng,4) in the reference's layout.
+__global__ void residual_finish_kernel(const double* part, int nblk, int ng, double* res, double* bcres) {
+  const int g = blockIdx.x;
+  int kind[kNRes];
+#pragma unroll
+  for (int q = 0; q < kNRes; ++q) kind[q] = (q < 5 || q >= 25) ? 1 : 0;
+  double o[kNRes];
+  warp_finish<kNRes>(part, nblk, g, kind, o);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 5; ++k) {
+      res[g + (long)ng * (k + 5 * 0)] = o[k];
+      res[g + (long)ng * (k + 5 * 1)] = o[5 + k];
+      res[g + (long)ng * (k + 5 * 2)] = sqrt(o[10 + k]);
+      res[g + (long)ng * (k + 5 * 3)] = o[15 + k];
+      res[g + (long)ng * (k + 5 * 4)] = sqrt(o[20 + k]);
+    }
+    for (int s = 0; s < 4; ++s) bcres[g + (long)ng * s] = o[25 + s];
+  }
+}
+
+// OLD_MGQD_COEFS (MLOQD_SOLVES.f08:12-73), one thread per cell.
+struct OldIn {
+  const double *E, *EV, *EH, *Fx, *Fy, *fxx, *fyy, *fVxx, *fVxy, *fHyy, *fHxy, *KapE, *KapR, *Src, *Delx, *Dely, *A;
+  double c, Theta;
+};
+struct OldOut {
+  double *G, *PL, *PB, *PR, *PT;
+};
+__global__ void old_coefs_kernel(const OldIn in, const Dims d, const OldOut o) {
+  const int g = blockIdx.y;
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p >= d.nC) return;
+  const int nx = d.nx;
+  const int i = (int)(p % nx), j = (int)(p / nx);
+  const long k = d.nC * g + p;
+  const long v0 = d.nV * g + i + (long)(nx + 1) * j, h0 = d.nH * g + p;
+  const double w = (in.Theta - 1.0) / in.Theta, c = in.c;
+  const double a = in.A[p], dx = in.Delx[i], dy = in.Dely[j];
+  o.G[k] = w * (dy * (in.Fx[v0 + 1] - in.Fx[v0]) + dx * (in.Fy[h0 + nx] - in.Fy[h0]) +
+                a * (c * in.KapE[k] * in.E[k] - in.Src[k]));
+  const double xy_h = (in.fHxy[h0 + nx] * in.EH[h0 + nx] - in.fHxy[h0] * in.EH[h0]);
+  const double xy_v = (in.fVxy[v0 + 1] * in.EV[v0 + 1] - in.fVxy[v0] * in.EV[v0]);
+  o.PL[k] = w * (c * dy * (in.fxx[k] * in.E[k] - in.fVxx[v0] * in.EV[v0]) + c * dx * xy_h / 2.0 +
+                 a * (in.KapR[k] * in.Fx[v0]) / 2.0);
+  o.PB[k] = w * (c * dx * (in.fyy[k] * in.E[k] - in.fHyy[h0] * in.EH[h0]) + c * dy * xy_v / 2.0 +
+                 a * (in.KapR[k] * in.Fy[h0]) / 2.0);
+  o.PR[k] = w * (c * dy * (in.fVxx[v0 + 1] * in.EV[v0 + 1] - in.fxx[k] * in.E[k]) + c * dx * xy_h / 2.0 +
+                 a * (in.KapR[k] * in.Fx[v0 + 1]) / 2.0);
+  o.PT[k] = w * (c * dx * (in.fHyy[h0 + nx] * in.EH[h0 + nx] - in.fyy[k] * in.E[k]) + c * dy * xy_v / 2.0 +
+                 a * (in.KapR[k] * in.Fy[h0 + nx]) / 2.0);
+}
+
+}  // namespace trt_mgqd

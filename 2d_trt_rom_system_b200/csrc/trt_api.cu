@@ -1434,6 +1434,7 @@ const char* trt_strerror(int code) {
     case TRT_ERR_NODEV: return "no CUDA device available";
     case TRT_ERR_UNSUPPORTED: return "shape outside the compiled kernel set";
     case TRT_ERR_SCRATCH: return "problem exceeds the fixed scratch of the no-allocation entry point (n_m*n_g > 65536)";
+    case TRT_ERR_NOCONV: return "the low-order linear solve of a group stopped without converging";
     default: return "unknown error";
   }
 }
@@ -2209,3 +2210,8 @@ extern "C" int trt_transport_residual_noalloc(int n_x, int n_y, int n_m, int n_g
   TRT_CUDA(cudaGetLastError());
   return TRT_OK;
 }
+
+namespace trt_host {
+// launch counter shared with the other translation units of the library
+void add_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace trt_host

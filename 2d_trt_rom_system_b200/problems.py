@@ -238,3 +238,59 @@ def fc_timestep_setup(prob, Tini_eV=None):
     Tini = prob.T0 * KEV if Tini_eV is None else Tini_eV
     return TimeStepSetup(nu_eV=prob.nu_eV, kappa_mult=np.asfortranarray(k0 / k0.min()),
                          cv=fc_cv(max(bcT[0], 1.0)), Kap0=KAP0_FC, Tini_eV=Tini, bcT_eV=bcT, dt=prob.dt)
+
+
+def mgqd_inputs(nx, ny, ng, seed=0, theta=1.0, kap_range=(1e-4, 1e4), xlen=6.0, ylen=6.0, dt=2e-3, uniform=False):
+    """Seeded synthetic inputs of MLOQD_FV / OLD_MGQD_COEFS (MLOQD_SOLVES.f08:12-362) with the value
+    ranges a time step produces: per-group opacities log-uniform over kap_range (thick and thin groups
+    side by side, constant on random rectangles), QD factors near 1/3 with small smooth off-diagonal
+    parts, boundary factors of magnitude 0.3-0.6 with Cg_Calc's signs, positive energies.  Returns (d, c, dt, theta); d holds every
+    input by its reference name (Fortran-ordered) plus Eg_avg/Eg_edgV/Eg_edgH (the initial guess) and
+    G_old/Pold_* from the previous-step fields."""
+    rng = np.random.default_rng(seed)
+    Fo = np.asfortranarray
+    dx = np.full(nx, xlen / nx) if uniform else xlen / nx * rng.uniform(0.7, 1.3, nx)
+    dy = np.full(ny, ylen / ny) if uniform else ylen / ny * rng.uniform(0.7, 1.3, ny)
+    d = {"Delx": dx, "Dely": dy, "A": Fo(np.outer(dx, dy))}
+    lo, hi = math.log10(kap_range[0]), math.log10(kap_range[1])
+    kap = np.empty((nx, ny, ng))
+    for g in range(ng):
+        base = 10 ** (hi - (hi - lo) * (g + 0.5) / ng)
+        field = np.ones((nx, ny))
+        for _ in range(4):
+            x0, y0 = rng.integers(0, nx), rng.integers(0, ny)
+            field[x0:x0 + max(1, nx // 3), y0:y0 + max(1, ny // 3)] = 10 ** rng.uniform(-1, 1)
+        kap[:, :, g] = base * field
+    d["KapE"] = Fo(kap)
+    d["KapR"] = Fo(kap * rng.uniform(0.8, 1.2, (1, 1, ng)))
+    d["Src"] = Fo(kap * rng.uniform(0.5, 2.0, (nx, ny, ng)))
+
+    def smooth(shape, mean, amp):
+        s = [np.linspace(0, np.pi * rng.uniform(1, 3), n) for n in shape[:2]]
+        phase = rng.uniform(0, 2 * np.pi, shape[2])
+        return Fo(mean + amp * np.sin(s[0][:, None, None] + phase) * np.cos(s[1][None, :, None]))
+    V, H, Cc = (nx + 1, ny, ng), (nx, ny + 1, ng), (nx, ny, ng)
+    for suf in ("", "_old"):
+        d["fg_avg_xx" + suf] = smooth(Cc, 1 / 3, 0.05)
+        d["fg_avg_yy" + suf] = smooth(Cc, 1 / 3, 0.05)
+        d["fg_edgV_xx" + suf] = smooth(V, 1 / 3, 0.06)
+        d["fg_edgV_xy" + suf] = smooth(V, 0.0, 0.03)
+        d["fg_edgH_yy" + suf] = smooth(H, 1 / 3, 0.06)
+        d["fg_edgH_xy" + suf] = smooth(H, 0.0, 0.03)
+    for s_ in ("L", "B", "R", "T"):
+        n = ny if s_ in "LR" else nx
+        # Cg_Calc (MLOQD_SOLVES.f08:367-488) weights by the signed direction cosine of the outgoing
+        # directions: negative on the left and bottom faces, positive on the right and top
+        d["Cg_" + s_] = Fo(rng.uniform(0.3, 0.6, (n, ng)) * (-1.0 if s_ in "LB" else 1.0))
+        d["Eg_in_" + s_] = Fo(rng.uniform(0.0, 1.0, (n, ng)) * (s_ == "L"))
+        d["Fg_in_" + s_] = Fo(rng.uniform(0.0, 50.0, (n, ng)) * (s_ == "L"))
+    d["Eg_avg_old"] = Fo(rng.uniform(0.5, 1.5, Cc))
+    d["Eg_edgV_old"] = Fo(rng.uniform(0.5, 1.5, V))
+    d["Eg_edgH_old"] = Fo(rng.uniform(0.5, 1.5, H))
+    d["Fxg_edgV_old"] = Fo(rng.uniform(-20, 20, V))
+    d["Fyg_edgH_old"] = Fo(rng.uniform(-20, 20, H))
+    d["KapE_old"], d["KapR_old"], d["Src_old"] = d["KapE"], d["KapR"], d["Src"]
+    d["Eg_avg"] = d["Eg_avg_old"].copy(order="F")
+    d["Eg_edgV"] = d["Eg_edgV_old"].copy(order="F")
+    d["Eg_edgH"] = d["Eg_edgH_old"].copy(order="F")
+    return d, C_LIGHT, dt, theta

@@ -40,6 +40,7 @@ extern "C" {
 #define TRT_ERR_NODEV (-7)        /* no CUDA device */
 #define TRT_ERR_UNSUPPORTED (-8)  /* shape outside the compiled kernel set (N_m/4 > 64) */
 #define TRT_ERR_SCRATCH (-9)      /* problem larger than the fixed scratch of trt_transport_residual_noalloc */
+#define TRT_ERR_NOCONV (-10)      /* the low-order linear solve of a group stopped without converging */
 
 #define TRT_PREC_FP64 0   /* plain: FP64 state and arithmetic throughout */
 #define TRT_PREC_FP32 1   /* mixed: FP32 state and sweep, FP64 moment combination and QD factors */
@@ -111,6 +112,47 @@ int trt_rt_bc_update(int n_x, int n_y, int n_m, int n_g, const int* BC_Type, dou
 
 /* Bg_planck_calc, MainSrc/TEMP_FUNCTIONS.f08:90-108 (host evaluation, used for boundary values). */
 double trt_bg_planck(double T, double nu_low, double nu_high, double Comp_Unit);
+
+/* Replaces SUBROUTINE OLD_MGQD_COEFS, MainSrc/MLOQD_SOLVES.f08:12-14 (body :15-73).  Cell arrays
+ * (n_x,n_y,n_g), vertical-edge arrays (n_x+1,n_y,n_g), horizontal-edge arrays (n_x,n_y+1,n_g); outputs
+ * G_old, Pold_L/B/R/T (n_x,n_y,n_g). */
+int trt_old_mgqd_coefs(int n_x, int n_y, int n_g, const double* Eg_avg_old, const double* Eg_edgV_old,
+                       const double* Eg_edgH_old, const double* Fxg_edgV_old, const double* Fyg_edgH_old,
+                       const double* fg_avg_xx_old, const double* fg_avg_yy_old, const double* fg_edgV_xx_old,
+                       const double* fg_edgV_xy_old, const double* fg_edgH_yy_old, const double* fg_edgH_xy_old,
+                       const double* KapE_old, const double* KapR_old, const double* Src_old, const double* Delx,
+                       const double* Dely, const double* A, double c, double Delt, double Theta, double* G_old,
+                       double* Pold_L, double* Pold_B, double* Pold_R, double* Pold_T, int Open_Threads);
+
+/* Replaces SUBROUTINE MLOQD_FV, MainSrc/MLOQD_SOLVES.f08:78-82 (body :83-362), including its linear
+ * solver QD_FV (MainSrc/QD_SOLVERS.f08:40-538).  Eg_avg(n_x,n_y,n_g), Eg_edgV(n_x+1,n_y,n_g),
+ * Eg_edgH(n_x,n_y+1,n_g): in (initial guess) / out; Fxg_edgV(n_x+1,n_y,n_g), Fyg_edgH(n_x,n_y+1,n_g): out;
+ * QD factors in the shapes of fg_Calc's outputs; Cg_L/R, Eg_in_L/R, Fg_in_L/R (n_y,n_g); Cg_B/T,
+ * Eg_in_B/T, Fg_in_B/T (n_x,n_g); MGQD_Residual(n_g,5,5) and MGQD_BC_Residual(n_g,4): out when
+ * Res_Calc != 0; MGQD_Kits(n_g): matrix-vector products per group (as SPARSKIT's ipar(7) counts them),
+ * negated for a group that stopped without converging, in which case the call returns TRT_ERR_NOCONV
+ * with the last iterate in the outputs.  All groups are solved on the device at once (FP64 BiCGSTAB,
+ * right-preconditioned like the reference, with an edge-elimination + multigrid preconditioner), to a
+ * Jacobi-scaled residual of at most tol * max|E| per group (trt_mgqd_set_tolerance; default 1e-13). */
+int trt_mloqd_fv(int n_x, int n_y, int n_g, double* Eg_avg, double* Eg_edgV, double* Eg_edgH, double* Fxg_edgV,
+                 double* Fyg_edgH, const double* fg_avg_xx, const double* fg_avg_yy, const double* fg_edgV_xx,
+                 const double* fg_edgV_xy, const double* fg_edgH_yy, const double* fg_edgH_xy, const double* Cg_L,
+                 const double* Cg_B, const double* Cg_R, const double* Cg_T, const double* Eg_in_L,
+                 const double* Eg_in_B, const double* Eg_in_R, const double* Eg_in_T, const double* Fg_in_L,
+                 const double* Fg_in_B, const double* Fg_in_R, const double* Fg_in_T, const double* Src,
+                 const double* KapE, const double* KapR, const double* Delx, const double* Dely, const double* A,
+                 double c, double Delt, double Theta, int Open_Threads, int Res_Calc, double* MGQD_Residual,
+                 double* MGQD_BC_Residual, const double* G_old, const double* Pold_L, const double* Pold_B,
+                 const double* Pold_R, const double* Pold_T, const double* Eg_avg_old, const double* Fxg_edgV_old,
+                 const double* Fyg_edgH_old, int* MGQD_Kits, double Fdt_Weight, double Fin_Weight,
+                 double Ein_Weight);
+
+/* Convergence settings of trt_mloqd_fv (process-wide): tol > 0, maxit >= 1 iterations per group. */
+int trt_mgqd_set_tolerance(double tol, int maxit);
+
+/* Device time (ms, events around the solve, excluding host<->device copies) and the largest
+ * iteration count of the last trt_mloqd_fv call. */
+int trt_mgqd_last_stats(double* device_ms, int* max_iterations);
 
 /* ---------------------------------------------------------------------------------------------
  * Layer 2: resident-state handle.  Replaces the state hand-off of ALGORITHMS.f08:397 and the call

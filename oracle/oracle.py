@@ -34,6 +34,8 @@ _SIG = {
     "oracle_material_update": (_i, [_i, _i, _i, _D, _D, _D, _d, _D, _D, _D]),
     "oracle_meb_solve": (_i, [_i, _i, _i, _D, _D, _D, _D, _d, _D, _d, _d]),
     "oracle_convergence": (_i, [_i, _d, _D, _D, _D, _i, _i, _D, _D]),
+    "oracle_old_mgqd_coefs": (_i, [_i, _i, _i] + [_D] * 17 + [_d, _d, _d] + [_D] * 5),
+    "oracle_mloqd_fv": (_i, [_i, _i, _i] + [_D] * 29 + [_d, _d, _d, _i, _i] + [_D] * 10 + [_I, _d, _d, _d]),
 }
 
 _lib = None
@@ -263,3 +265,44 @@ def tr_no_qd_steps(st, Omega_x, Omega_y, quad_weight, Delx, Dely, Nu_g, kappa_mu
             T_rt2, T_rt1 = T_rt1, st["Temp"].copy(order="F")
         hist.append((st["Temp"].copy(order="F"), m["E_avg"].copy(order="F"), its, tn, en))
     return hist
+
+
+# Low-order (MGQD) solve: argument names of MLOQD_FV / OLD_MGQD_COEFS (MLOQD_SOLVES.f08:12-362).
+MLOQD_FACTORS = ("fg_avg_xx", "fg_avg_yy", "fg_edgV_xx", "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy")
+MLOQD_BOUNDARY = ("Cg_L", "Cg_B", "Cg_R", "Cg_T", "Eg_in_L", "Eg_in_B", "Eg_in_R", "Eg_in_T",
+                  "Fg_in_L", "Fg_in_B", "Fg_in_R", "Fg_in_T")
+MLOQD_MATERIAL = ("Src", "KapE", "KapR", "Delx", "Dely", "A")
+MLOQD_OLD = ("G_old", "Pold_L", "Pold_B", "Pold_R", "Pold_T", "Eg_avg_old", "Fxg_edgV_old", "Fyg_edgH_old")
+OLD_MGQD_IN = ("Eg_avg_old", "Eg_edgV_old", "Eg_edgH_old", "Fxg_edgV_old", "Fyg_edgH_old", "fg_avg_xx_old",
+               "fg_avg_yy_old", "fg_edgV_xx_old", "fg_edgV_xy_old", "fg_edgH_yy_old", "fg_edgH_xy_old", "KapE_old",
+               "KapR_old", "Src_old", "Delx", "Dely", "A")
+
+
+def old_mgqd_coefs(d, c, Delt, Theta):
+    """OLD_MGQD_COEFS (MLOQD_SOLVES.f08:12-73): returns G_old, Pold_L, Pold_B, Pold_R, Pold_T (nx,ny,ng)."""
+    nx, ny, ng = d["Eg_avg_old"].shape
+    out = {k: zeros(nx, ny, ng) for k in ("G_old", "Pold_L", "Pold_B", "Pold_R", "Pold_T")}
+    rc = lib().oracle_old_mgqd_coefs(nx, ny, ng, *[_p(F(d[k])) for k in OLD_MGQD_IN], float(c), float(Delt),
+                                     float(Theta), *[_p(v) for v in out.values()])
+    assert rc == 0
+    return out
+
+
+def mloqd_fv(d, c, Delt, Theta=1.0, res_calc=True, threads=1, Fdt_Weight=1.0, Fin_Weight=1.0, Ein_Weight=1.0):
+    """MLOQD_FV (MLOQD_SOLVES.f08:78-362) solved directly (see mgqd_oracle.cpp).  d holds the
+    subroutine's inputs by name plus Eg_avg/Eg_edgV/Eg_edgH (initial guess).  Returns Eg_avg, Eg_edgV,
+    Eg_edgH, Fxg_edgV, Fyg_edgH, MGQD_Residual (ng,5,5), MGQD_BC_Residual (ng,4), MGQD_Kits (ng)."""
+    nx, ny, ng = d["Eg_avg"].shape
+    o = {k: F(d[k]).copy(order="F") for k in ("Eg_avg", "Eg_edgV", "Eg_edgH")}
+    o["Fxg_edgV"], o["Fyg_edgH"] = zeros(nx + 1, ny, ng), zeros(nx, ny + 1, ng)
+    o["MGQD_Residual"], o["MGQD_BC_Residual"] = zeros(ng, 5, 5), zeros(ng, 4)
+    o["MGQD_Kits"] = np.zeros(ng, dtype=np.int32)
+    rc = lib().oracle_mloqd_fv(
+        nx, ny, ng, *[_p(o[k]) for k in ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH")],
+        *[_p(F(d[k])) for k in MLOQD_FACTORS + MLOQD_BOUNDARY + MLOQD_MATERIAL], float(c), float(Delt),
+        float(Theta), int(threads), int(bool(res_calc)), _p(o["MGQD_Residual"]), _p(o["MGQD_BC_Residual"]),
+        *[_p(F(d[k])) for k in MLOQD_OLD], _p(o["MGQD_Kits"]), float(Fdt_Weight), float(Fin_Weight),
+        float(Ein_Weight))
+    assert rc == 0, rc
+    return o
+

@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_strerror_codes():
     L = pkg.lib()
-    for code in range(0, -9, -1):
+    for code in range(0, -11, -1):
         msg = L.trt_strerror(code).decode()
         assert msg and msg != "unknown error"
     assert L.trt_strerror(-99).decode() == "unknown error"
