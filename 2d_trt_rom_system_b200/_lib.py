@@ -116,7 +116,7 @@ SIGNATURES = {
     "trt_old_mgqd_coefs": (_i, [_i, _i, _i] + [_D] * 17 + [_d, _d, _d] + [_D] * 5 + [_i]),
     "trt_mloqd_fv": (_i, [_i, _i, _i] + [_D] * 29 + [_d, _d, _d, _i, _i] + [_D] * 10 + [_I, _d, _d, _d]),
     "trt_mgqd_set_tolerance": (_i, [_d, _i]),
-    "trt_mgqd_last_stats": (_i, [_D, _I]),
+    "trt_mgqd_last_stats": (_i, [_D, _I, _D]),
 }
 
 _lib = None

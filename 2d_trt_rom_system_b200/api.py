@@ -197,10 +197,11 @@ def mgqd_set_tolerance(tol=1e-13, maxit=1000):
 
 
 def mgqd_last_stats():
-    """(device ms of the last MLOQD_FV solve without its copies, largest iteration count)."""
-    ms, its = ctypes.c_double(0), ctypes.c_int(0)
-    check(_lib.lib().trt_mgqd_last_stats(ctypes.byref(ms), ctypes.byref(its)), "mgqd_last_stats")
-    return ms.value, its.value
+    """(device ms of the last MLOQD_FV solve without its copies, largest iteration count, device ms of
+    its first matrix-vector product)."""
+    ms, its, mv = ctypes.c_double(0), ctypes.c_int(0), ctypes.c_double(0)
+    check(_lib.lib().trt_mgqd_last_stats(ctypes.byref(ms), ctypes.byref(its), ctypes.byref(mv)), "mgqd_last_stats")
+    return ms.value, its.value, mv.value
 
 
 def Bg_planck_calc(T, nu_low, nu_high, comp_unit):

@@ -51,8 +51,8 @@ Settings g_settings;
 struct Solver {
   Dims d{};
   cudaStream_t st = nullptr;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  std::vector<double*> bufs;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, m0 = nullptr, m1 = nullptr;   // solve; first matrix-vector product
+  std::vector<void*> bufs;
   Inputs in{};
   Coefs cf{};
   Krylov K{};
@@ -61,19 +61,21 @@ struct Solver {
   double *Fx = nullptr, *Fy = nullptr, *rpart = nullptr, *res = nullptr, *bcres = nullptr;
   int* h_done = nullptr;
   Scal* h_scal = nullptr;
-  float last_ms = 0.f;
+  float last_ms = 0.f, last_matvec_ms = 0.f;
+  bool matvec_timed = false;
   int last_its = 0;
 
   ~Solver() {
-    for (double* p : bufs) cudaFree(p);
+    for (void* p : bufs) cudaFree(p);
     if (h_done) cudaFreeHost(h_done);
     if (h_scal) cudaFreeHost(h_scal);
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
+    for (cudaEvent_t e : {e0, e1, m0, m1})
+      if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
   }
-  int alloc(double** p, size_t n) {
-    if (cudaMalloc(p, std::max<size_t>(n, 1) * sizeof(double)) != cudaSuccess) {
+  template <class T>
+  int alloc(T** p, size_t n) {
+    if (cudaMalloc(p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
       cudaGetLastError();
       *p = nullptr;
       return TRT_ERR_NOMEM;
@@ -97,6 +99,8 @@ int Solver::init(int nx, int ny, int ng) {
   MG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   MG_CUDA(cudaEventCreate(&e0));
   MG_CUDA(cudaEventCreate(&e1));
+  MG_CUDA(cudaEventCreate(&m0));
+  MG_CUDA(cudaEventCreate(&m1));
   const size_t C = (size_t)d.nC * ng, V = (size_t)d.nV * ng, H = (size_t)d.nH * ng, U = (size_t)d.nU * ng;
   int rc = TRT_OK;
   auto A = [&](const double** p, size_t n) {
@@ -104,7 +108,7 @@ int Solver::init(int nx, int ny, int ng) {
     if (!rc) rc = alloc(&q, n);
     *p = q;
   };
-  auto M = [&](double** p, size_t n) {
+  auto M = [&](auto** p, size_t n) {
     if (!rc) rc = alloc(p, n);
   };
   // inputs
@@ -165,6 +169,7 @@ int Solver::solve(cudaStream_t s) {
   const int ng = d.ng;
   const dim3 gpos(pos_blocks(), ng);
   const int nblk = pos_blocks();
+  matvec_timed = false;
   K.tol = g_settings.tol;
   K.maxit = g_settings.maxit;
   coef_kernel<<<gpos, kRedBlock, 0, s>>>(in, d, cf);
@@ -226,8 +231,11 @@ int Solver::solve(cudaStream_t s) {
     if ((rc = vcycle())) return rc;
     backsub_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, ls.L[0], pnew, K.ph);
     MG_LAUNCHED();
+    matvec_timed = matvec_timed || it == 0;
+    if (it == 0) MG_CUDA(cudaEventRecord(m0, s));
     matvec_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, K.ph, K.v, 0);
     MG_LAUNCHED();
+    if (it == 0) MG_CUDA(cudaEventRecord(m1, s));
     scalar_finish_kernel<<<ng, 32, 0, s>>>(K, nblk, 0);
     MG_LAUNCHED();
     elim_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, ls.L[0], nullptr, K.s, 1);
@@ -299,11 +307,12 @@ int trt_mgqd_set_tolerance(double tol, int maxit) {
   return TRT_OK;
 }
 
-int trt_mgqd_last_stats(double* device_ms, int* max_iterations) {
+int trt_mgqd_last_stats(double* device_ms, int* max_iterations, double* matvec_ms) {
   std::lock_guard<std::mutex> lk(g_cache.mu);
   if (!g_cache.s) return TRT_ERR_STATE;
   if (device_ms) *device_ms = g_cache.s->last_ms;
   if (max_iterations) *max_iterations = g_cache.s->last_its;
+  if (matvec_ms) *matvec_ms = g_cache.s->last_matvec_ms;
   return TRT_OK;
 }
 
@@ -387,6 +396,11 @@ int trt_mloqd_fv(int n_x, int n_y, int n_g, double* Eg_avg, double* Eg_edgV, dou
   MG_CUDA(cudaMemcpyAsync(S->h_scal, S->K.sc, sizeof(Scal) * n_g, cudaMemcpyDeviceToHost, st));
   MG_CUDA(cudaStreamSynchronize(st));
   MG_CUDA(cudaEventElapsedTime(&S->last_ms, S->e0, S->e1));
+  S->last_matvec_ms = 0.f;
+  if (S->matvec_timed && cudaEventElapsedTime(&S->last_matvec_ms, S->m0, S->m1) != cudaSuccess) {
+    cudaGetLastError();
+    S->last_matvec_ms = 0.f;
+  }
   bool conv = true;
   S->last_its = 0;
   for (int g = 0; g < n_g; ++g) {

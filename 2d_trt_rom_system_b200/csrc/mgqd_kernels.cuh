@@ -19,7 +19,10 @@
 //      explicit combination of its own residual and its two neighbouring cell unknowns;
 //   2. substitute the edges into the energy balance: a 5-point cell-centred operator S;
 //   3. one multigrid V(2,2)-cycle on S (red-black Gauss-Seidel smoothing; coarse operators by
-//      2x2 aggregation with the coupling scaled by 1/2, the cell-centred rediscretisation factor);
+//      2x2 aggregation with the coupling scaled by 1/2, the cell-centred rediscretisation factor),
+//      stored and computed in FP32: the preconditioner only steers the FP64 iteration, whose
+//      residual and stopping test stay FP64, and FP32 halves the multigrid's traffic (the fine
+//      level of a 256x256x50 problem then fits the 126 MB L2);
 //   4. back-substitute the edges.
 // Groups whose opacity keeps the system diagonally dominant converge in a few iterations; optically
 // thin groups, where the system is a diffusion operator with diffusion number (c dt / dx)^2 / 3,
@@ -65,8 +68,8 @@ struct Coefs {
 
 struct Level {
   int mx, my;
-  long n;                                     // cells per group
-  double *sC, *sW, *sE, *sS, *sN, *x, *b;     // [group][cell]
+  long n;                                    // cells per group
+  float *sC, *sW, *sE, *sS, *sN, *x, *b;     // [group][cell]
 };
 
 struct Scal {
@@ -228,11 +231,11 @@ __global__ void prec_coef_kernel(const Dims d, const Coefs cf, const Level L0) {
     edgeH_elim(cf, d, g, i, j + 1, &aT, &bbT, &btT);
     const long kg = d.nC * g + i + (long)d.nx * j;
     const double ebl = cf.EBL[kg], ebr = cf.EBR[kg], ebb = cf.EBB[kg], ebt = cf.EBT[kg];
-    L0.sC[kg] = cf.EBC[kg] + ebl * brL + ebr * blR + ebb * btB + ebt * bbT;
-    L0.sW[kg] = ebl * blL;
-    L0.sE[kg] = ebr * brR;
-    L0.sS[kg] = ebb * bbB;
-    L0.sN[kg] = ebt * btT;
+    L0.sC[kg] = (float)(cf.EBC[kg] + ebl * brL + ebr * blR + ebb * btB + ebt * bbT);
+    L0.sW[kg] = (float)(ebl * blL);
+    L0.sE[kg] = (float)(ebr * brR);
+    L0.sS[kg] = (float)(ebb * bbB);
+    L0.sN[kg] = (float)(ebt * btT);
   }
 }
 
@@ -253,11 +256,11 @@ __device__ __forceinline__ void coarse_op_cell(const Level& F, const Level& Cs, 
       if (dj == 0 && j + 1 < F.my) D += F.sN[k]; else eN += F.sN[k];
     }
   const long kc = Cs.n * g + I + (long)Cs.mx * J;
-  Cs.sC[kc] = D + (1.0 - alpha) * (eW + eE + eS + eN);
-  Cs.sW[kc] = alpha * eW;
-  Cs.sE[kc] = alpha * eE;
-  Cs.sS[kc] = alpha * eS;
-  Cs.sN[kc] = alpha * eN;
+  Cs.sC[kc] = (float)(D + (1.0 - alpha) * (eW + eE + eS + eN));
+  Cs.sW[kc] = (float)(alpha * eW);
+  Cs.sE[kc] = (float)(alpha * eE);
+  Cs.sS[kc] = (float)(alpha * eS);
+  Cs.sN[kc] = (float)(alpha * eN);
 }
 
 __global__ void coarse_op_kernel(const Level F, const Level Cs) {
@@ -271,13 +274,12 @@ __global__ void coarse_op_kernel(const Level F, const Level Cs) {
 // multigrid pieces (cell-centred 5-point operator)
 // ------------------------------------------------------------------------------------------------
 
-__device__ __forceinline__ double s_offdiag(const Level& L, long base, int i, int j, long k) {
-  double s = 0.0;
+__device__ __forceinline__ float s_offdiag(const Level& L, int i, int j, long k) {
+  float s = 0.f;
   if (i > 0) s += L.sW[k] * L.x[k - 1];
   if (i + 1 < L.mx) s += L.sE[k] * L.x[k + 1];
   if (j > 0) s += L.sS[k] * L.x[k - L.mx];
   if (j + 1 < L.my) s += L.sN[k] * L.x[k + L.mx];
-  (void)base;
   return s;
 }
 
@@ -286,24 +288,24 @@ __device__ __forceinline__ double s_offdiag(const Level& L, long base, int i, in
 __device__ __forceinline__ void smooth_cell(const Level& L, int g, int i, int j, int color, bool zero_init) {
   const long k = L.n * g + i + (long)L.mx * j;
   if (((i + j) & 1) != color) {
-    if (zero_init) L.x[k] = 0.0;
+    if (zero_init) L.x[k] = 0.f;
     return;
   }
   if (zero_init) {
     L.x[k] = L.b[k] / L.sC[k];
     return;
   }
-  L.x[k] = (L.b[k] - s_offdiag(L, 0, i, j, k)) / L.sC[k];
+  L.x[k] = (L.b[k] - s_offdiag(L, i, j, k)) / L.sC[k];
 }
 
 __device__ __forceinline__ void restrict_cell(const Level& F, const Level& Cs, int g, int I, int J) {
-  double r = 0.0;
+  float r = 0.f;
   for (int dj = 0; dj < 2; ++dj)
     for (int di = 0; di < 2; ++di) {
       const int i = 2 * I + di, j = 2 * J + dj;
       if (i >= F.mx || j >= F.my) continue;
       const long k = F.n * g + i + (long)F.mx * j;
-      r += F.b[k] - F.sC[k] * F.x[k] - s_offdiag(F, 0, i, j, k);
+      r += F.b[k] - F.sC[k] * F.x[k] - s_offdiag(F, i, j, k);
     }
   Cs.b[Cs.n * g + I + (long)Cs.mx * J] = r;
 }
@@ -573,8 +575,8 @@ __global__ void elim_kernel(const Coefs cf, const Dims d, const Krylov K, const 
     znew[base + uc] = zc;
     const long kg = d.nC * g + uc;
     const long eL = d.nV * g + i + (long)(nx + 1) * j, eB = d.nH * g + i + (long)nx * j;
-    L0.b[kg] = zc - cf.EBL[kg] * (cf.aV[eL] * z(uV(i, j))) - cf.EBR[kg] * (cf.aV[eL + 1] * z(uV(i + 1, j))) -
-               cf.EBB[kg] * (cf.aH[eB] * z(uH(i, j))) - cf.EBT[kg] * (cf.aH[eB + nx] * z(uH(i, j + 1)));
+    L0.b[kg] = (float)(zc - cf.EBL[kg] * (cf.aV[eL] * z(uV(i, j))) - cf.EBR[kg] * (cf.aV[eL + 1] * z(uV(i + 1, j))) -
+                       cf.EBB[kg] * (cf.aH[eB] * z(uH(i, j))) - cf.EBT[kg] * (cf.aH[eB + nx] * z(uH(i, j + 1))));
   }
   if (j < ny) znew[base + uV(i, j)] = z(uV(i, j));
   if (i < nx) znew[base + uH(i, j)] = z(uH(i, j));
@@ -590,20 +592,20 @@ __global__ void backsub_kernel(const Coefs cf, const Dims d, const Krylov K, con
   const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
   const int nx = d.nx, ny = d.ny;
   const long base = d.nU * g;
-  const double* xc = L0.x + d.nC * g;
-  if (i < nx && j < ny) y[base + i + (long)nx * j] = xc[i + (long)nx * j];
+  const float* xc = L0.x + d.nC * g;
+  if (i < nx && j < ny) y[base + i + (long)nx * j] = (double)xc[i + (long)nx * j];
   if (j < ny) {
     const long e = i + (long)(nx + 1) * j, ev = d.nV * g + e;
     double val = cf.aV[ev] * zin[base + d.oV() + e];
-    if (i > 0) val += cf.blV[ev] * xc[i - 1 + (long)nx * j];
-    if (i < nx) val += cf.brV[ev] * xc[i + (long)nx * j];
+    if (i > 0) val += cf.blV[ev] * (double)xc[i - 1 + (long)nx * j];
+    if (i < nx) val += cf.brV[ev] * (double)xc[i + (long)nx * j];
     y[base + d.oV() + e] = val;
   }
   if (i < nx) {
     const long e = i + (long)nx * j, eh = d.nH * g + e;
     double val = cf.aH[eh] * zin[base + d.oH() + e];
-    if (j > 0) val += cf.bbH[eh] * xc[i + (long)nx * (j - 1)];
-    if (j < ny) val += cf.btH[eh] * xc[i + (long)nx * j];
+    if (j > 0) val += cf.bbH[eh] * (double)xc[i + (long)nx * (j - 1)];
+    if (j < ny) val += cf.btH[eh] * (double)xc[i + (long)nx * j];
     y[base + d.oH() + e] = val;
   }
 }

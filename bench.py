@@ -58,6 +58,8 @@ def parse():
                    help="instances of a config-2 batch run concurrently (mixed) and sequentially (FP64); 0 = skip")
     p.add_argument("--no-autotune", dest="autotune", action="store_false",
                    help="use the library's default tiling instead of trt_autotune")
+    p.add_argument("--mgqd", type=int, default=3,
+                   help="timed low-order MGQD solves (MLOQD_FV) on the configuration's grid and groups; 0 skips")
     p.add_argument("--time-steps", type=int, default=10,
                    help="time steps of the transport-only time loop (mixed vs FP64 temperature error); 0 = skip")
     return p.parse_args()
@@ -301,6 +303,96 @@ def run_batch(pkg, count, budget_gb=170.0):
     return out
 
 
+def mgqd_matvec_bytes(nx, ny, ng):
+    """Algorithmic bytes of one matrix-vector product of the reduced MGQD system (matvec_kernel): the
+    11 cell coefficient planes, the two edge diagonals, the operand, the product and rh, FP64."""
+    nC, nV, nH = nx * ny, (nx + 1) * ny, nx * (ny + 1)
+    nU = nC + nV + nH
+    return 8 * ng * (11 * nC + nV + nH + 3 * nU)
+
+
+def mgqd_cpu_baseline(pkg, n, ng, budget_s=30.0):
+    """The reference's procedure for MLOQD_FV (its numbering, ILUT(3, 1e-6) + BiCGSTAB, OpenMP over
+    groups) restated in the oracle, on a sample of the groups spread over the opacity range."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    gs = max(1, min(cores, 8, ng))
+    d, c, dt, th = pkg.problems.mgqd_inputs(n, n, ng, seed=1, kap_range=(1e-4, 1e4), uniform=True)
+    sel = np.linspace(0, ng - 1, gs).round().astype(int)
+    ds = {}
+    for k, v in d.items():
+        v = np.asarray(v)
+        ds[k] = np.asfortranarray(v[..., sel]) if v.ndim >= 2 and v.shape[-1] == ng else v
+    ds.update(O.old_mgqd_coefs(ds, c, dt, th))
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < 3 and (time.perf_counter() - t_start) < budget_s:
+        t0 = time.perf_counter()
+        o = O.mloqd_fv(ds, c, dt, th, threads=gs, solver=1)
+        times.append(time.perf_counter() - t0)
+    med = float(np.median(times))
+    return {"value": n * n * gs / med, "unit": "cell*group/s", "cores": gs, "kind": "port",
+            "sample": f"{n}x{n} cells, {gs} of {ng} groups spread over the opacity range (matrix-vector products "
+                      f"{int(o['MGQD_Kits'].min())}-{int(o['MGQD_Kits'].max())}), median of {len(times)} solves, {gs} "
+                      f"threads (OpenMP over groups), g++ -O2 -fopenmp, host has {cores} cores"}
+
+
+def run_mgqd(pkg, solves, n, ng, cpu=True):
+    """MLOQD_FV through the reference-signature entry point (host arrays): device time of the solve
+    (events inside the library, copies excluded) and the whole call."""
+    P = pkg.problems
+    d, c, dt, th = P.mgqd_inputs(n, n, ng, seed=1, kap_range=(1e-4, 1e4), uniform=True)
+    old = {k: np.zeros((n, n, ng), order="F") for k in ("G_old", "Pold_L", "Pold_B", "Pold_R", "Pold_T")}
+    pkg.OLD_MGQD_COEFS(*[d[k] for k in ("Eg_avg_old", "Eg_edgV_old", "Eg_edgH_old", "Fxg_edgV_old", "Fyg_edgH_old",
+                                        "fg_avg_xx_old", "fg_avg_yy_old", "fg_edgV_xx_old", "fg_edgV_xy_old",
+                                        "fg_edgH_yy_old", "fg_edgH_xy_old", "KapE_old", "KapR_old", "Src_old", "Delx",
+                                        "Dely", "A")], c, dt, th, *old.values(), 1)
+    d.update(old)
+    ins = [d[k] for k in ("fg_avg_xx", "fg_avg_yy", "fg_edgV_xx", "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy", "Cg_L",
+                          "Cg_B", "Cg_R", "Cg_T", "Eg_in_L", "Eg_in_B", "Eg_in_R", "Eg_in_T", "Fg_in_L", "Fg_in_B",
+                          "Fg_in_R", "Fg_in_T", "Src", "KapE", "KapR", "Delx", "Dely", "A")]
+    olds = [d[k] for k in ("G_old", "Pold_L", "Pold_B", "Pold_R", "Pold_T", "Eg_avg_old", "Fxg_edgV_old",
+                           "Fyg_edgH_old")]
+    out = {"Fxg_edgV": np.zeros((n + 1, n, ng), order="F"), "Fyg_edgH": np.zeros((n, n + 1, ng), order="F"),
+           "R": np.zeros((ng, 5, 5), order="F"), "RB": np.zeros((ng, 4), order="F"),
+           "K": np.zeros(ng, dtype=np.int32)}
+    rec = []
+    launches0 = pkg.kernel_launches()
+    for k in range(solves + 1):
+        E = {q: d[q].copy(order="F") for q in ("Eg_avg", "Eg_edgV", "Eg_edgH")}
+        t0 = time.perf_counter()
+        pkg.MLOQD_FV(E["Eg_avg"], E["Eg_edgV"], E["Eg_edgH"], out["Fxg_edgV"], out["Fyg_edgH"], *ins, c, dt, th, 1, True,
+                     out["R"], out["RB"], *olds, out["K"], 1.0, 1.0, 1.0)
+        wall = time.perf_counter() - t0
+        if k == 0:
+            launches0 = pkg.kernel_launches()
+            continue
+        ms, its, mv = pkg.mgqd_last_stats()
+        rec.append((ms, wall, its, mv))
+    launches = (pkg.kernel_launches() - launches0) / max(1, solves)
+    ms = float(np.median([r[0] for r in rec]))
+    wall = float(np.median([r[1] for r in rec]))
+    mv = float(np.median([r[3] for r in rec]))
+    h2d = sum(np.asarray(a).nbytes for a in ins + olds) + sum(d[q].nbytes for q in ("Eg_avg", "Eg_edgV", "Eg_edgH"))
+    d2h = sum(d[q].nbytes for q in ("Eg_avg", "Eg_edgV", "Eg_edgH")) + sum(v.nbytes for v in out.values())
+    peak, kind = peaks()
+    mvb = mgqd_matvec_bytes(n, n, ng)
+    res = {"workload": f"MLOQD_FV: {n}x{n} cells, {ng} groups (the configuration's grid and groups), seeded synthetic "
+                       f"QD factors, boundary factors and opacities log-spread over 1e-4..1e4 per group",
+           "metric": "cell*group low-order solves/s", "value": n * n * ng / (ms * 1e-3), "unit": "cell*group/s",
+           "device_ms": ms, "iterations_max": int(rec[-1][2]), "matvec_products": [int(out["K"].min()), int(out["K"].max())],
+           "gpu_launches": launches, "dtype": "f64 (preconditioner f32)",
+           "e2e": {"value": n * n * ng / wall, "unit": "cell*group/s", "ms": wall * 1e3, "h2d_bytes_per_step": int(h2d),
+                   "d2h_bytes_per_step": int(d2h), "path": "trt_mloqd_fv with pageable host arrays (the Fortran call)"},
+           "roofline": {"kernel": "matvec_kernel", "bound": "hbm", "bytes_per_launch": mvb,
+                        "achieved": mvb / (mv * 1e-3) / 1e9 if mv > 0 else None, "peak": peak, "unit": "GB/s",
+                        "frac": (mvb / (mv * 1e-3) / 1e9) / peak if mv > 0 else None, "kernel_ms": mv,
+                        "peak_source": f"{kind} hbm_gbs"}}
+    if cpu:
+        res["cpu_baseline"] = mgqd_cpu_baseline(pkg, n, ng)
+    return res
+
+
 def setup_instance(pkg, prob, precision, tiling, autotune=False):
     ox, oy, w = prob.directions()
     s = pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng, precision=precision)
@@ -506,6 +598,8 @@ def main():
                    "ms_per_step": dt * 1e3, "path": "trt_set_material(host) + trt_sweep + trt_moments(host), pinned"}
     if args.time_steps > 0:
         line["time_steps"] = run_time_steps(pkg, torch, prob, args.time_steps)
+    if args.mgqd > 0 and ws == 1:
+        line["mgqd"] = run_mgqd(pkg, args.mgqd, prob.nx, prob.ng, cpu=rank == 0 and not args.no_cpu_baseline)
     if args.serving > 0 and ws == 1:
         line["serving"] = run_serving(pkg, args.serving)
     if args.batch > 0 and ws == 1:

@@ -150,9 +150,10 @@ int trt_mloqd_fv(int n_x, int n_y, int n_g, double* Eg_avg, double* Eg_edgV, dou
 /* Convergence settings of trt_mloqd_fv (process-wide): tol > 0, maxit >= 1 iterations per group. */
 int trt_mgqd_set_tolerance(double tol, int maxit);
 
-/* Device time (ms, events around the solve, excluding host<->device copies) and the largest
- * iteration count of the last trt_mloqd_fv call. */
-int trt_mgqd_last_stats(double* device_ms, int* max_iterations);
+/* Of the last trt_mloqd_fv call: device time (ms, events around the solve, excluding host<->device
+ * copies), the largest iteration count, and the device time of its first matrix-vector product (ms;
+ * 0 when the initial guess had already converged).  Any pointer may be NULL. */
+int trt_mgqd_last_stats(double* device_ms, int* max_iterations, double* matvec_ms);
 
 /* ---------------------------------------------------------------------------------------------
  * Layer 2: resident-state handle.  Replaces the state hand-off of ALGORITHMS.f08:397 and the call

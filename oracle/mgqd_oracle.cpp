@@ -12,11 +12,19 @@
 // Linear solve.  The reference assembles the reduced system of each group in CSR (QD_SOLVERS.f08:66-386)
 // and solves it with SPARSKIT2's ILUT(fill 3, drop 1e-6) preconditioned BiCGSTAB, relative tolerance
 // 1e-13 and absolute 1e-15 (QD_SOLVERS.f08:415-470), falling back to dense GAUSS_COMPLETE when the
-// iteration fails (:489-497).  SPARSKIT2 is not vendored in the reference tree.  The oracle solves the
-// same equations directly, by banded LU with partial pivoting over a row-by-row numbering of the
-// unknowns (its own numbering: the solution does not depend on it), and so returns the discrete
-// solution that the reference's iteration converges to.  MGQD_Kits is -1 for every group, the value
-// the reference records when it solves directly.
+// iteration fails (:489-497).  SPARSKIT2 is not vendored in the reference tree.  Two solvers:
+//   solver 0 (oracle_mloqd_fv, the checker): the same equations solved directly, by banded LU with
+//     partial pivoting over a row-by-row numbering of the unknowns (its own numbering: the solution
+//     does not depend on it); this is the discrete solution the reference's iteration converges to.
+//     MGQD_Kits is -1 for every group, the value the reference records when it solves directly.
+//   solver 1 (oracle_mloqd_fv_solver(1, ...), the CPU baseline): the reference's own procedure, in the
+//     reference's unknown numbering (QD_SOLVERS.f08:66-77,162-171,219-233) and with its initial guess
+//     (:447-470): ILUT with dual threshold (Saad, "ILUT: a dual threshold incomplete LU
+//     factorization", 1994, as SPARSKIT2 implements it: drop below droptol times the row's mean
+//     absolute value, keep the lfil largest entries of each L and U row besides the diagonal), then
+//     right-preconditioned BiCGSTAB (van der Vorst 1992) stopped on the SPARSKIT criterion ipar(3) = -1
+//     as documented there, ||x_k - x_{k-1}|| <= rtol ||x_k|| + atol, at most 2000 matrix-vector
+//     products, falling back to the direct solve.  MGQD_Kits counts matrix-vector products.
 //
 // Parity status: UNPINNED (no reference outputs exist for this path).  The oracle is checked instead
 // through the reference's own residual formulas (MLOQD_SOLVES.f08:277-345), which are written on the
@@ -91,12 +99,207 @@ bool band_solve(Band& B, std::vector<double>& b) {
 // the horizontal edge's).
 struct Numbering {
   long nx, ny, blk;
-  Numbering(long nx_, long ny_) : nx(nx_), ny(ny_), blk(3 * nx_ + 1) {}
+  bool ref;   // the reference's numbering (QD_SOLVERS.f08:66-77, 162-171, 219-233), 0-based
+  Numbering(long nx_, long ny_, bool ref_ = false) : nx(nx_), ny(ny_), blk(3 * nx_ + 1), ref(ref_) {}
   long n() const { return ny * blk + nx; }
-  long H(long i, long j) const { return j * blk + i; }
-  long V(long i, long j) const { return j * blk + nx + 2 * i; }
-  long C(long i, long j) const { return j * blk + nx + 2 * i + 1; }
+  // reference: row j = 0 holds [E_edgV(0,0), per cell (bottom, centre, right, top)] (4 nx + 1 unknowns),
+  // every later row [E_edgV(0,j), per cell (centre, right, top)] (3 nx + 1)
+  long rstart(long j) const { return 4 * nx + 1 + (j - 1) * (3 * nx + 1); }
+  long H(long i, long j) const {
+    if (!ref) return j * blk + i;
+    if (j == 0) return 4 * i + 1;
+    if (j == 1) return 4 * i + 4;
+    return rstart(j - 1) + 3 * i + 3;
+  }
+  long V(long i, long j) const {
+    if (!ref) return j * blk + nx + 2 * i;
+    if (j == 0) return i == 0 ? 0 : 4 * i - 1;
+    return i == 0 ? rstart(j) : rstart(j) + 3 * i - 1;
+  }
+  long C(long i, long j) const {
+    if (!ref) return j * blk + nx + 2 * i + 1;
+    return j == 0 ? 4 * i + 2 : rstart(j) + 3 * i + 1;
+  }
 };
+
+// Compressed sparse rows, entries of a row in insertion order.
+struct Csr {
+  long n = 0;
+  std::vector<long> ia, ja;
+  std::vector<double> a;
+  void matvec(const double* x, double* y) const {
+    for (long r = 0; r < n; ++r) {
+      double s = 0.0;
+      for (long p = ia[r]; p < ia[r + 1]; ++p) s += a[p] * x[ja[p]];
+      y[r] = s;
+    }
+  }
+};
+
+// ILUT factors: L strictly lower (unit diagonal implied), U upper with the diagonal first in each row.
+struct Ilu {
+  std::vector<long> lia, lja, uia, uja;
+  std::vector<double> la, ua;
+  void solve(const double* x, double* y, long n) const {
+    for (long r = 0; r < n; ++r) {
+      double s = x[r];
+      for (long p = lia[r]; p < lia[r + 1]; ++p) s -= la[p] * y[lja[p]];
+      y[r] = s;
+    }
+    for (long r = n - 1; r >= 0; --r) {
+      double s = y[r];
+      for (long p = uia[r] + 1; p < uia[r + 1]; ++p) s -= ua[p] * y[uja[p]];
+      y[r] = s / ua[uia[r]];
+    }
+  }
+};
+
+// Dual-threshold incomplete LU (Saad 1994): row-wise elimination in increasing column order on a dense
+// work row, dropping multipliers and entries below droptol * mean|a_r|, keeping the lfil largest of
+// each of the L and U parts of a row (the diagonal always; a zero diagonal becomes
+// (1e-4 + droptol) * mean|a_r|).
+void ilut(const Csr& A, int lfil, double droptol, Ilu& F) {
+  const long n = A.n;
+  std::vector<double> w(n, 0.0);
+  std::vector<char> used(n, 0);
+  std::vector<long> lidx, uidx;
+  F.lia.assign(1, 0);
+  F.uia.assign(1, 0);
+  for (long r = 0; r < n; ++r) {
+    double tnorm = 0.0;
+    const long len = A.ia[r + 1] - A.ia[r];
+    lidx.clear();
+    uidx.clear();
+    for (long p = A.ia[r]; p < A.ia[r + 1]; ++p) {
+      const long c = A.ja[p];
+      tnorm += std::fabs(A.a[p]);
+      if (!used[c]) {
+        used[c] = 1;
+        (c < r ? lidx : uidx).push_back(c);
+      }
+      w[c] += A.a[p];
+    }
+    tnorm = len > 0 ? tnorm / (double)len : 1.0;
+    const double thr = droptol * tnorm;
+    if (!used[r]) {
+      used[r] = 1;
+      uidx.push_back(r);
+    }
+    // eliminate the lower part in increasing column order
+    std::vector<long> lkept;
+    size_t done = 0;
+    while (done < lidx.size()) {
+      size_t m = done;
+      for (size_t q = done + 1; q < lidx.size(); ++q)
+        if (lidx[q] < lidx[m]) m = q;
+      std::swap(lidx[done], lidx[m]);
+      const long k = lidx[done++];
+      const double fact = w[k] / F.ua[F.uia[k]];
+      if (std::fabs(fact) <= thr) {
+        w[k] = 0.0;
+        continue;
+      }
+      w[k] = fact;
+      lkept.push_back(k);
+      for (long p = F.uia[k] + 1; p < F.uia[k + 1]; ++p) {
+        const long c = F.uja[p];
+        if (!used[c]) {
+          used[c] = 1;
+          (c < r ? lidx : uidx).push_back(c);
+        }
+        w[c] -= fact * F.ua[p];
+      }
+    }
+    // keep the lfil largest of L and of the off-diagonal U
+    auto keep_largest = [&](std::vector<long>& idx) {
+      std::vector<long> out;
+      for (long c : idx)
+        if (std::fabs(w[c]) > thr) out.push_back(c);
+      if ((long)out.size() > lfil) {
+        std::partial_sort(out.begin(), out.begin() + lfil, out.end(),
+                          [&](long x, long y) { return std::fabs(w[x]) > std::fabs(w[y]); });
+        out.resize(lfil);
+      }
+      std::sort(out.begin(), out.end());
+      return out;
+    };
+    std::vector<long> lsel = keep_largest(lkept);
+    std::vector<long> uoff;
+    for (long c : uidx)
+      if (c != r) uoff.push_back(c);
+    std::vector<long> usel = keep_largest(uoff);
+    for (long c : lsel) {
+      F.lja.push_back(c);
+      F.la.push_back(w[c]);
+    }
+    F.lia.push_back((long)F.lja.size());
+    double diag = w[r];
+    if (diag == 0.0) diag = (1e-4 + droptol) * tnorm;
+    F.uja.push_back(r);
+    F.ua.push_back(diag);
+    for (long c : usel) {
+      F.uja.push_back(c);
+      F.ua.push_back(w[c]);
+    }
+    F.uia.push_back((long)F.uja.size());
+    // clear the work row
+    for (long c : lidx) {
+      w[c] = 0.0;
+      used[c] = 0;
+    }
+    for (long c : uidx) {
+      w[c] = 0.0;
+      used[c] = 0;
+    }
+  }
+}
+
+// Right-preconditioned BiCGSTAB; stops when ||x_k - x_{k-1}||_2 <= rtol ||x_k||_2 + atol.  Returns the
+// matrix-vector products used (initial residual included), or -1 on breakdown / after max_mv products.
+long bicgstab(const Csr& A, const Ilu& M, const std::vector<double>& b, std::vector<double>& x, double rtol,
+              double atol, long max_mv) {
+  const long n = A.n;
+  std::vector<double> r(n), rh(n), p(n, 0.0), v(n, 0.0), s(n), t(n), ph(n), sh(n);
+  auto dot = [&](const std::vector<double>& a, const std::vector<double>& c) {
+    double z = 0.0;
+    for (long k = 0; k < n; ++k) z += a[k] * c[k];
+    return z;
+  };
+  A.matvec(x.data(), r.data());
+  long nmv = 1;
+  for (long k = 0; k < n; ++k) r[k] = b[k] - r[k];
+  rh = r;
+  double rho = 1.0, alpha = 1.0, omega = 1.0;
+  for (;;) {
+    const double rho1 = dot(rh, r);
+    if (rho1 == 0.0) return nmv;   // exact residual zero
+    const double beta = (rho1 / rho) * (alpha / omega);
+    rho = rho1;
+    for (long k = 0; k < n; ++k) p[k] = r[k] + beta * (p[k] - omega * v[k]);
+    M.solve(p.data(), ph.data(), n);
+    A.matvec(ph.data(), v.data());
+    ++nmv;
+    const double rv = dot(rh, v);
+    if (rv == 0.0) return -1;
+    alpha = rho / rv;
+    for (long k = 0; k < n; ++k) s[k] = r[k] - alpha * v[k];
+    M.solve(s.data(), sh.data(), n);
+    A.matvec(sh.data(), t.data());
+    ++nmv;
+    const double tt = dot(t, t);
+    omega = tt != 0.0 ? dot(t, s) / tt : 0.0;
+    double dx2 = 0.0, x2 = 0.0;
+    for (long k = 0; k < n; ++k) {
+      const double dx = alpha * ph[k] + omega * sh[k];
+      x[k] += dx;
+      r[k] = s[k] - omega * t[k];
+      dx2 += dx * dx;
+      x2 += x[k] * x[k];
+    }
+    if (std::sqrt(dx2) <= rtol * std::sqrt(x2) + atol) return nmv;
+    if (omega == 0.0 || nmv >= max_mv) return -1;
+  }
+}
 
 }  // namespace
 
@@ -157,7 +360,8 @@ int oracle_old_mgqd_coefs(int nx, int ny, int ng, const double* Eg_avg_old, cons
 // MGQD_Residual(ng,5,5), MGQD_BC_Residual(ng,4), MGQD_Kits(ng).  Eg_avg/Eg_edgV/Eg_edgH are in/out (the
 // reference uses them as the initial guess; a direct solve does not need one).  Returns 0, or -2 when
 // a group's system is singular.
-int oracle_mloqd_fv(int nx, int ny, int ng, double* Eg_avg, double* Eg_edgV, double* Eg_edgH, double* Fxg_edgV,
+int oracle_mloqd_fv_solver(int solver, int nx, int ny, int ng, double* Eg_avg, double* Eg_edgV, double* Eg_edgH,
+                           double* Fxg_edgV,
                     double* Fyg_edgH, const double* fg_avg_xx, const double* fg_avg_yy, const double* fg_edgV_xx,
                     const double* fg_edgV_xy, const double* fg_edgH_yy, const double* fg_edgH_xy, const double* Cg_L,
                     const double* Cg_B, const double* Cg_R, const double* Cg_T, const double* Eg_in_L,
@@ -239,7 +443,7 @@ int oracle_mloqd_fv(int nx, int ny, int ng, double* Eg_avg, double* Eg_edgV, dou
       }
 
     // the reduced system (QD_SOLVERS.f08:66-386), one row per unknown
-    const Numbering N(nx, ny);
+    const Numbering N(nx, ny, solver == 1);
     const long n = N.n();
     struct Ent {
       long r, c;
@@ -319,16 +523,48 @@ int oracle_mloqd_fv(int nx, int ny, int ng, double* Eg_avg, double* Eg_edgV, dou
           put(r, N.H(i, j + 1), CpT[i]);
         }
       }
-    long kl = 0, ku = 0;
-    for (const Ent& e : ent) {
-      kl = std::max(kl, e.r - e.c);
-      ku = std::max(ku, e.c - e.r);
+    long kits = -1;
+    if (solver == 1) {
+      // QD_SOLVERS.f08:386-497: CSR in row order, ILUT(3, 1e-6), BiCGSTAB from the current E
+      Csr A;
+      A.n = n;
+      std::vector<long> cnt(n + 1, 0);
+      for (const Ent& e : ent) cnt[e.r + 1] += 1;
+      for (long r = 0; r < n; ++r) cnt[r + 1] += cnt[r];
+      A.ia = cnt;
+      A.ja.resize(ent.size());
+      A.a.resize(ent.size());
+      for (const Ent& e : ent) {
+        const long q = cnt[e.r]++;
+        A.ja[q] = e.c;
+        A.a[q] = e.v;
+      }
+      Ilu M;
+      ilut(A, 3, 1e-6, M);
+      std::vector<double> x(n);
+      for (int j = 0; j < ny; ++j) {
+        for (int i = 0; i < nx; ++i) {
+          x[N.C(i, j)] = Eg_avg[C(i, j, g)];
+          x[N.H(i, j)] = Eg_edgH[H(i, j, g)];
+        }
+        for (int i = 0; i <= nx; ++i) x[N.V(i, j)] = Eg_edgV[V(i, j, g)];
+      }
+      for (int i = 0; i < nx; ++i) x[N.H(i, ny)] = Eg_edgH[H(i, ny, g)];
+      kits = bicgstab(A, M, rhs, x, 1e-13, 1e-15, 2000);
+      if (kits > 0) rhs = x;
     }
-    Band B(n, kl, ku);
-    for (const Ent& e : ent) B.at(e.r, e.c) += e.v;
-    if (!band_solve(B, rhs)) {
-      bad += 1;
-      continue;
+    if (kits < 0) {
+      long kl = 0, ku = 0;
+      for (const Ent& e : ent) {
+        kl = std::max(kl, e.r - e.c);
+        ku = std::max(ku, e.c - e.r);
+      }
+      Band B(n, kl, ku);
+      for (const Ent& e : ent) B.at(e.r, e.c) += e.v;
+      if (!band_solve(B, rhs)) {
+        bad += 1;
+        continue;
+      }
     }
     for (int j = 0; j < ny; ++j) {
       for (int i = 0; i < nx; ++i) {
@@ -338,7 +574,7 @@ int oracle_mloqd_fv(int nx, int ny, int ng, double* Eg_avg, double* Eg_edgV, dou
       for (int i = 0; i <= nx; ++i) Eg_edgV[V(i, j, g)] = rhs[N.V(i, j)];
     }
     for (int i = 0; i < nx; ++i) Eg_edgH[H(i, ny, g)] = rhs[N.H(i, ny)];
-    MGQD_Kits[g] = -1;
+    MGQD_Kits[g] = (int)kits;
 
     // fluxes from the auxiliary equations, MLOQD_SOLVES.f08:244-268
     for (int j = 0; j < ny; ++j) {
@@ -449,6 +685,26 @@ int oracle_mloqd_fv(int nx, int ny, int ng, double* Eg_avg, double* Eg_edgV, dou
     }
   }
   return 0;
+}
+
+int oracle_mloqd_fv(int nx, int ny, int ng, double* Eg_avg, double* Eg_edgV, double* Eg_edgH, double* Fxg_edgV,
+                    double* Fyg_edgH, const double* fg_avg_xx, const double* fg_avg_yy, const double* fg_edgV_xx,
+                    const double* fg_edgV_xy, const double* fg_edgH_yy, const double* fg_edgH_xy, const double* Cg_L,
+                    const double* Cg_B, const double* Cg_R, const double* Cg_T, const double* Eg_in_L,
+                    const double* Eg_in_B, const double* Eg_in_R, const double* Eg_in_T, const double* Fg_in_L,
+                    const double* Fg_in_B, const double* Fg_in_R, const double* Fg_in_T, const double* Src,
+                    const double* KapE, const double* KapR, const double* Delx, const double* Dely, const double* A,
+                    double c, double Delt, double Theta, int Open_Threads, int Res_Calc, double* MGQD_Residual,
+                    double* MGQD_BC_Residual, const double* G_old, const double* Pold_L, const double* Pold_B,
+                    const double* Pold_R, const double* Pold_T, const double* Eg_avg_old, const double* Fxg_edgV_old,
+                    const double* Fyg_edgH_old, int* MGQD_Kits, double Fdt_Weight, double Fin_Weight,
+                    double Ein_Weight) {
+  return oracle_mloqd_fv_solver(0, nx, ny, ng, Eg_avg, Eg_edgV, Eg_edgH, Fxg_edgV, Fyg_edgH, fg_avg_xx, fg_avg_yy,
+                                fg_edgV_xx, fg_edgV_xy, fg_edgH_yy, fg_edgH_xy, Cg_L, Cg_B, Cg_R, Cg_T, Eg_in_L,
+                                Eg_in_B, Eg_in_R, Eg_in_T, Fg_in_L, Fg_in_B, Fg_in_R, Fg_in_T, Src, KapE, KapR, Delx,
+                                Dely, A, c, Delt, Theta, Open_Threads, Res_Calc, MGQD_Residual, MGQD_BC_Residual,
+                                G_old, Pold_L, Pold_B, Pold_R, Pold_T, Eg_avg_old, Fxg_edgV_old, Fyg_edgH_old,
+                                MGQD_Kits, Fdt_Weight, Fin_Weight, Ein_Weight);
 }
 
 }  // extern "C"

@@ -36,6 +36,7 @@ _SIG = {
     "oracle_convergence": (_i, [_i, _d, _D, _D, _D, _i, _i, _D, _D]),
     "oracle_old_mgqd_coefs": (_i, [_i, _i, _i] + [_D] * 17 + [_d, _d, _d] + [_D] * 5),
     "oracle_mloqd_fv": (_i, [_i, _i, _i] + [_D] * 29 + [_d, _d, _d, _i, _i] + [_D] * 10 + [_I, _d, _d, _d]),
+    "oracle_mloqd_fv_solver": (_i, [_i, _i, _i, _i] + [_D] * 29 + [_d, _d, _d, _i, _i] + [_D] * 10 + [_I, _d, _d, _d]),
 }
 
 _lib = None
@@ -288,17 +289,20 @@ def old_mgqd_coefs(d, c, Delt, Theta):
     return out
 
 
-def mloqd_fv(d, c, Delt, Theta=1.0, res_calc=True, threads=1, Fdt_Weight=1.0, Fin_Weight=1.0, Ein_Weight=1.0):
-    """MLOQD_FV (MLOQD_SOLVES.f08:78-362) solved directly (see mgqd_oracle.cpp).  d holds the
-    subroutine's inputs by name plus Eg_avg/Eg_edgV/Eg_edgH (initial guess).  Returns Eg_avg, Eg_edgV,
-    Eg_edgH, Fxg_edgV, Fyg_edgH, MGQD_Residual (ng,5,5), MGQD_BC_Residual (ng,4), MGQD_Kits (ng)."""
+def mloqd_fv(d, c, Delt, Theta=1.0, res_calc=True, threads=1, Fdt_Weight=1.0, Fin_Weight=1.0, Ein_Weight=1.0,
+             solver=0):
+    """MLOQD_FV (MLOQD_SOLVES.f08:78-362).  solver 0: the reduced system solved directly (the checker);
+    solver 1: the reference's ILUT + BiCGSTAB procedure in its unknown numbering (the CPU baseline);
+    see mgqd_oracle.cpp.  d holds the subroutine's inputs by name plus Eg_avg/Eg_edgV/Eg_edgH (initial
+    guess).  Returns Eg_avg, Eg_edgV, Eg_edgH, Fxg_edgV, Fyg_edgH, MGQD_Residual (ng,5,5),
+    MGQD_BC_Residual (ng,4), MGQD_Kits (ng)."""
     nx, ny, ng = d["Eg_avg"].shape
     o = {k: F(d[k]).copy(order="F") for k in ("Eg_avg", "Eg_edgV", "Eg_edgH")}
     o["Fxg_edgV"], o["Fyg_edgH"] = zeros(nx + 1, ny, ng), zeros(nx, ny + 1, ng)
     o["MGQD_Residual"], o["MGQD_BC_Residual"] = zeros(ng, 5, 5), zeros(ng, 4)
     o["MGQD_Kits"] = np.zeros(ng, dtype=np.int32)
-    rc = lib().oracle_mloqd_fv(
-        nx, ny, ng, *[_p(o[k]) for k in ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH")],
+    rc = lib().oracle_mloqd_fv_solver(
+        int(solver), nx, ny, ng, *[_p(o[k]) for k in ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH")],
         *[_p(F(d[k])) for k in MLOQD_FACTORS + MLOQD_BOUNDARY + MLOQD_MATERIAL], float(c), float(Delt),
         float(Theta), int(threads), int(bool(res_calc)), _p(o["MGQD_Residual"]), _p(o["MGQD_BC_Residual"]),
         *[_p(F(d[k])) for k in MLOQD_OLD], _p(o["MGQD_Kits"]), float(Fdt_Weight), float(Fin_Weight),

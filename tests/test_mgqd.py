@@ -224,3 +224,16 @@ def test_device_mloqd_fv_on_factors_from_the_sweep(oracle):
     out = call_device(d, c, dt, th)
     for k in ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH"):
         assert rel_err(out[k], ref[k]) < 1e-9, k
+
+
+@pytest.mark.parametrize("case", [(5, 4, 3, 1.0, 1, True), (12, 9, 6, 0.5, 2, False), (1, 6, 2, 1.0, 4, False),
+                                  (7, 1, 2, 0.5, 5, False), (30, 26, 8, 1.0, 15, False)])
+def test_oracle_reference_procedure_matches_the_direct_solve(case, oracle):
+    """The reference's own procedure (its unknown numbering, ILUT(3, 1e-6), BiCGSTAB to 1e-13) lands on
+    the direct solution of the reduced system."""
+    d, c, dt, th = make(*case, oracle)
+    a = oracle.mloqd_fv(d, c, dt, th, threads=2)
+    b = oracle.mloqd_fv(d, c, dt, th, threads=2, solver=1)
+    assert (b["MGQD_Kits"] > 0).all()
+    for k in ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH"):
+        assert rel_err(b[k], a[k]) < 1e-9, k
