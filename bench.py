@@ -60,6 +60,8 @@ def parse():
                    help="use the library's default tiling instead of trt_autotune")
     p.add_argument("--mgqd", type=int, default=3,
                    help="timed low-order MGQD solves (MLOQD_FV) on the configuration's grid and groups; 0 skips")
+    p.add_argument("--mgqd-only", action="store_true",
+                   help="run only the low-order MGQD leg (--mgqd solves) and print its JSON object")
     p.add_argument("--time-steps", type=int, default=10,
                    help="time steps of the transport-only time loop (mixed vs FP64 temperature error); 0 = skip")
     return p.parse_args()
@@ -525,6 +527,10 @@ def main():
         return run_profile(args)
     if args.tiling_sweep:
         return run_tiling_sweep(args)
+    if args.mgqd_only:
+        pkg, prob = build_problem(args.config, args.n, args.groups)
+        print(json.dumps(run_mgqd(pkg, max(1, args.mgqd), prob.nx, prob.ng, cpu=not args.no_cpu_baseline)))
+        return 0
     import torch
     pkg, prob = build_problem(args.config, args.n, args.groups)
     ranks = pkg.ranks
