@@ -116,6 +116,12 @@ SIGNATURES = {
     "trt_old_mgqd_coefs": (_i, [_i, _i, _i] + [_D] * 17 + [_d, _d, _d] + [_D] * 5 + [_i]),
     "trt_mloqd_fv": (_i, [_i, _i, _i] + [_D] * 29 + [_d, _d, _d, _i, _i] + [_D] * 10 + [_I, _d, _d, _d]),
     "trt_mgqd_set_tolerance": (_i, [_d, _i]),
+    "trt_collapse_mg_ef": (_i, [_i, _i, _i] + [_D] * 5 + [_i] + [_D] * 5),
+    "trt_cbar_calc": (_i, [_i, _i, _i] + [_D] * 15),
+    "trt_old_grey_coefs": (_i, [_i, _i, _i, _d, _d, _d, _d] + [_D] * 8),
+    "trt_grey_coefs": (_i, [_i, _i, _i] + [_D] * 14 + [_d, _d, _d] + [_D] * 4 + [_D] * 15 + [_d]),
+    "trt_egp_fv_newt": (_i, [_i, _i] + [_D] * 9 + [_I, _D, _D, _D, _D, _d, _d] + [_D] * 3 + [_D] * 12 + [_D] * 14
+                        + [_D] * 2 + [_d] * 9 + [_i] * 6 + [_I, _d, _d]),
     "trt_mgqd_last_stats": (_i, [_D, _I, _D]),
 }
 

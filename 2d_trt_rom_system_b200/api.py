@@ -191,6 +191,90 @@ def MLOQD_FV(Eg_avg, Eg_edgV, Eg_edgH, Fxg_edgV, Fyg_edgH, fg_avg_xx, fg_avg_yy,
     check(rc, "MLOQD_FV")
 
 
+def COLLAPSE_MG_EF(Eg_avg, Eg_edgV, Eg_edgH, Fxg_edgV, Fyg_edgH, Open_Threads, E_avg, E_edgV, E_edgH, Fx_edgV, Fy_edgH):
+    """SUBROUTINE COLLAPSE_MG_EF, MainSrc/MLOQD_SOLVES.f08:687-730."""
+    nx, ny, ng = Eg_avg.shape
+    ins = [_f64(a, s) for a, s in zip((Eg_avg, Eg_edgV, Eg_edgH, Fxg_edgV, Fyg_edgH),
+                                      ((nx, ny, ng), (nx + 1, ny, ng), (nx, ny + 1, ng), (nx + 1, ny, ng),
+                                       (nx, ny + 1, ng)))]
+    outs = [_out(o, s) for o, s in zip((E_avg, E_edgV, E_edgH, Fx_edgV, Fy_edgH),
+                                       ((nx, ny), (nx + 1, ny), (nx, ny + 1), (nx + 1, ny), (nx, ny + 1)))]
+    check(_lib.lib().trt_collapse_mg_ef(nx, ny, ng, *[dptr(a) for a in ins], int(Open_Threads),
+                                        *[dptr(o) for o in outs]), "COLLAPSE_MG_EF")
+
+
+def Cbar_Calc(Cb_L, Cb_B, Cb_R, Cb_T, Cg_L, Cg_B, Cg_R, Cg_T, Eg_avg, Eg_edgV, Eg_edgH, Eg_in_L, Eg_in_B, Eg_in_R,
+              Eg_in_T):
+    """SUBROUTINE Cbar_Calc, MainSrc/GLOQD_SOLVES.f08:177-231."""
+    nx, ny, ng = Eg_avg.shape
+    outs = [_out(o, s) for o, s in zip((Cb_L, Cb_B, Cb_R, Cb_T), ((ny,), (nx,), (ny,), (nx,)))]
+    by, bx = (ny, ng), (nx, ng)
+    ins = [_f64(a, s) for a, s in zip((Cg_L, Cg_B, Cg_R, Cg_T, Eg_avg, Eg_edgV, Eg_edgH, Eg_in_L, Eg_in_B, Eg_in_R,
+                                       Eg_in_T),
+                                      (by, bx, by, bx, (nx, ny, ng), (nx + 1, ny, ng), (nx, ny + 1, ng), by, bx, by, bx))]
+    check(_lib.lib().trt_cbar_calc(nx, ny, ng, *[dptr(o) for o in outs], *[dptr(a) for a in ins]), "Cbar_Calc")
+
+
+def OLD_GREY_COEFS(c, Delt, Theta, cv, A, Gold, Temp_old, KapE_bar_old, E_avg_old, GQD_Src_old, Gold_Hat, Rhat_old):
+    """SUBROUTINE OLD_GREY_COEFS, MainSrc/GLOQD_SOLVES.f08:12-42."""
+    nx, ny, ng = Gold.shape
+    ins = [_f64(A, (nx, ny)), _f64(Gold, (nx, ny, ng))] + [_f64(a, (nx, ny)) for a in (Temp_old, KapE_bar_old,
+                                                                                       E_avg_old, GQD_Src_old)]
+    outs = [_out(Gold_Hat, (nx, ny)), _out(Rhat_old, (nx, ny))]
+    check(_lib.lib().trt_old_grey_coefs(nx, ny, ng, float(c), float(Delt), float(Theta), float(cv),
+                                        *[dptr(a) for a in ins], *[dptr(o) for o in outs]), "OLD_GREY_COEFS")
+
+
+def GREY_COEFS(Eg_avg, Eg_edgV, Eg_edgH, Fxg_edgV_old, Fyg_edgH_old, fg_avg_xx, fg_avg_yy, fg_edgV_xx, fg_edgV_xy,
+               fg_edgH_yy, fg_edgH_xy, KapE, KapR, A, c, Delt, Theta, Pold_L, Pold_R, Pold_B, Pold_T, KapE_Bar, DC_xx,
+               DL_xx, DR_xx, DC_yy, DB_yy, DT_yy, DL_xy, DR_xy, DB_xy, DT_xy, PL, PR, PB, PT, Fdt_Weight):
+    """SUBROUTINE GREY_COEFS, MainSrc/GLOQD_SOLVES.f08:47-146."""
+    nx, ny, ng = Eg_avg.shape
+    C, V, H = (nx, ny, ng), (nx + 1, ny, ng), (nx, ny + 1, ng)
+    ins = [_f64(a, s) for a, s in zip((Eg_avg, Eg_edgV, Eg_edgH, Fxg_edgV_old, Fyg_edgH_old, fg_avg_xx, fg_avg_yy,
+                                       fg_edgV_xx, fg_edgV_xy, fg_edgH_yy, fg_edgH_xy, KapE, KapR, A),
+                                      (C, V, H, V, H, C, C, V, V, H, H, C, C, (nx, ny)))]
+    olds = [_f64(a, C) for a in (Pold_L, Pold_R, Pold_B, Pold_T)]
+    outs = [_out(o, (nx, ny)) for o in (KapE_Bar, DC_xx, DL_xx, DR_xx, DC_yy, DB_yy, DT_yy, DL_xy, DR_xy, DB_xy, DT_xy,
+                                        PL, PR, PB, PT)]
+    check(_lib.lib().trt_grey_coefs(nx, ny, ng, *[dptr(a) for a in ins], float(c), float(Delt), float(Theta),
+                                    *[dptr(a) for a in olds], *[dptr(o) for o in outs], float(Fdt_Weight)), "GREY_COEFS")
+
+
+def EGP_FV_NEWT(E_avg, E_edgV, E_edgH, Temp, KapE_Bar, Fx_edgV, Fy_edgH, Q_bar, KapE_Bar_dT, Temp_Mold, KapE_bar_Mold,
+                Theta, Delt, Delx, Dely, A, Cb_L, Cb_B, Cb_R, Cb_T, E_in_L, E_in_B, E_in_R, E_in_T, F_in_L, F_in_B,
+                F_in_R, F_in_T, DC_xx, DL_xx, DR_xx, DC_yy, DB_yy, DT_yy, DL_xy, DR_xy, DB_xy, DT_xy, PL, PR, PB, PT,
+                Gold_Hat, Rhat_old, Kap0, cv, Comp_Unit, Chi, line_src, E_Bound_Low, T_Bound_Low, Eps1, Eps2, Maxits,
+                MGQD_It, Use_Line_Search, Use_Safety_Search, Res_Calc, kapE_dT_flag, Fin_Weight, Ein_Weight):
+    """SUBROUTINE EGP_FV_NEWT, MainSrc/GLOQD_SOLVES.f08:305-860, with every linear solve on the device.
+    The INTENT(INOUT)/(OUT) arrays are updated in place; returns (Its, GQD_Kits, Deltas (Its, 6),
+    dresiduals (Its, 6))."""
+    nx, ny = Temp.shape
+    for o, s in ((E_avg, (nx, ny)), (E_edgV, (nx + 1, ny)), (E_edgH, (nx, ny + 1)), (Temp, (nx, ny)),
+                 (KapE_Bar, (nx, ny)), (Fx_edgV, (nx + 1, ny)), (Fy_edgH, (nx, ny + 1)), (Q_bar, (nx, ny)),
+                 (KapE_Bar_dT, (nx, ny))):
+        _out(o, s)
+    its = ctypes.c_int(0)
+    Dl = np.zeros((Maxits, 6), order="F")
+    dr = np.zeros((Maxits, 6), order="F")
+    kits = np.zeros(Maxits, dtype=np.int32)
+    cells = [_f64(a, (nx, ny)) for a in (DC_xx, DL_xx, DR_xx, DC_yy, DB_yy, DT_yy, DL_xy, DR_xy, DB_xy, DT_xy, PL, PR,
+                                         PB, PT, Gold_Hat, Rhat_old)]
+    bnd = [_f64(a, ((ny,) if k % 2 == 0 else (nx,))) for k, a in
+           enumerate((Cb_L, Cb_B, Cb_R, Cb_T, E_in_L, E_in_B, E_in_R, E_in_T, F_in_L, F_in_B, F_in_R, F_in_T))]
+    rc = _lib.lib().trt_egp_fv_newt(
+        nx, ny, *[dptr(o) for o in (E_avg, E_edgV, E_edgH, Temp, KapE_Bar, Fx_edgV, Fy_edgH, Q_bar, KapE_Bar_dT)],
+        ctypes.byref(its), dptr(Dl), dptr(dr), dptr(_f64(Temp_Mold, (nx, ny))), dptr(_f64(KapE_bar_Mold, (nx, ny))),
+        float(Theta), float(Delt), dptr(_f64(Delx, (nx,))), dptr(_f64(Dely, (ny,))), dptr(_f64(A, (nx, ny))),
+        *[dptr(a) for a in bnd], *[dptr(a) for a in cells], float(Kap0), float(cv), float(Comp_Unit), float(Chi),
+        float(line_src), float(E_Bound_Low), float(T_Bound_Low), float(Eps1), float(Eps2), int(Maxits), int(MGQD_It),
+        int(bool(Use_Line_Search)), int(bool(Use_Safety_Search)), int(bool(Res_Calc)), int(bool(kapE_dT_flag)),
+        iptr(kits), float(Fin_Weight), float(Ein_Weight))
+    check(rc, "EGP_FV_NEWT")
+    n = its.value
+    return n, kits[:n], Dl[:n], dr[:n]
+
+
 def mgqd_set_tolerance(tol=1e-13, maxit=1000):
     """Convergence settings of MLOQD_FV's device solve (process-wide)."""
     check(_lib.lib().trt_mgqd_set_tolerance(float(tol), int(maxit)), "mgqd_set_tolerance")

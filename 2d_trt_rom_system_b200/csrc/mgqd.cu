@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "trt_sweep.h"
+#include "gqd_kernels.cuh"
 #include "mgqd_kernels.cuh"
 
 namespace trt_host {
@@ -84,7 +85,8 @@ struct Solver {
     return TRT_OK;
   }
   int init(int nx, int ny, int ng);
-  int solve(cudaStream_t s);
+  int solve(cudaStream_t s);    // MLOQD_FV: coefficients, Krylov solve, fluxes, residuals
+  int krylov(cudaStream_t s);   // the solve of whatever system the coefficient planes hold
   int pos_blocks() const { return (int)((d.npos() + kRedBlock - 1) / kRedBlock); }
 };
 
@@ -164,16 +166,33 @@ int Solver::init(int nx, int ny, int ng) {
 
 int grid1(long n) { return (int)((n + 255) / 256); }
 
-// Right-preconditioned BiCGSTAB over all groups; inputs and the initial guess (K.x) already on the device.
+// MLOQD_FV on the device; inputs and the initial guess (K.x) already uploaded.
 int Solver::solve(cudaStream_t s) {
+  const dim3 gpos(pos_blocks(), d.ng);
+  const int nblk = pos_blocks();
+  coef_kernel<<<gpos, kRedBlock, 0, s>>>(in, d, cf);
+  MG_LAUNCHED();
+  const int rc = krylov(s);
+  if (rc) return rc;
+  const Outputs out{Fx, Fy};
+  flux_kernel<<<gpos, kRedBlock, 0, s>>>(in, d, cf, K.x, out);
+  MG_LAUNCHED();
+  residual_kernel<<<gpos, kRedBlock, 0, s>>>(in, d, K.x, out, rpart);
+  MG_LAUNCHED();
+  residual_finish_kernel<<<d.ng, 32, 0, s>>>(rpart, nblk, d.ng, res, bcres);
+  MG_LAUNCHED();
+  return TRT_OK;
+}
+
+// Right-preconditioned BiCGSTAB over all groups of the system in cf (coefficients, edge diagonals and
+// right-hand side set), from the initial guess in K.x.
+int Solver::krylov(cudaStream_t s) {
   const int ng = d.ng;
   const dim3 gpos(pos_blocks(), ng);
   const int nblk = pos_blocks();
   matvec_timed = false;
   K.tol = g_settings.tol;
   K.maxit = g_settings.maxit;
-  coef_kernel<<<gpos, kRedBlock, 0, s>>>(in, d, cf);
-  MG_LAUNCHED();
   prec_coef_kernel<<<gpos, kRedBlock, 0, s>>>(d, cf, ls.L[0]);
   MG_LAUNCHED();
   for (int k = 0; k + 1 < ls.n; ++k) {
@@ -252,19 +271,13 @@ int Solver::solve(cudaStream_t s) {
     update_finish_kernel<<<ng, 32, 0, s>>>(K, nblk);
     MG_LAUNCHED();
   }
-  const Outputs out{Fx, Fy};
-  flux_kernel<<<gpos, kRedBlock, 0, s>>>(in, d, cf, K.x, out);
-  MG_LAUNCHED();
-  residual_kernel<<<gpos, kRedBlock, 0, s>>>(in, d, K.x, out, rpart);
-  MG_LAUNCHED();
-  residual_finish_kernel<<<ng, 32, 0, s>>>(rpart, nblk, ng, res, bcres);
-  MG_LAUNCHED();
   return TRT_OK;
 }
 
 struct Cache {
   std::mutex mu;
-  std::unique_ptr<Solver> s;
+  std::unique_ptr<Solver> s;       // multigroup shape
+  std::unique_ptr<Solver> grey;    // one-group shape of the grey Newton system
 };
 Cache g_cache;
 
@@ -277,17 +290,55 @@ int device_ok() {
   return TRT_OK;
 }
 
-int get_solver(int nx, int ny, int ng, Solver** out) {
-  Solver* s = g_cache.s.get();
+int get_solver(int nx, int ny, int ng, Solver** out, std::unique_ptr<Solver>& slot = g_cache.s) {
+  Solver* s = slot.get();
   if (!s || s->d.nx != nx || s->d.ny != ny || s->d.ng != ng) {
-    g_cache.s.reset();
+    slot.reset();
     auto fresh = std::make_unique<Solver>();
     const int rc = fresh->init(nx, ny, ng);
     if (rc) return rc;
-    g_cache.s = std::move(fresh);
+    slot = std::move(fresh);
   }
-  *out = g_cache.s.get();
+  *out = slot.get();
   return TRT_OK;
+}
+
+// One device allocation carved into 256-byte aligned pieces (the stateless grey entry points).
+struct Arena {
+  char* base = nullptr;
+  size_t used = 0, cap = 0;
+  ~Arena() {
+    if (base) cudaFree(base);
+  }
+  int reserve(size_t bytes) {
+    cap = bytes;
+    if (cudaMalloc(&base, std::max<size_t>(bytes, 256)) != cudaSuccess) {
+      cudaGetLastError();
+      base = nullptr;
+      return TRT_ERR_NOMEM;
+    }
+    return TRT_OK;
+  }
+  template <class T>
+  T* take(size_t n) {
+    const size_t b = (n * sizeof(T) + 255) & ~(size_t)255;
+    T* p = reinterpret_cast<T*>(base + used);
+    used += b;
+    return p;
+  }
+  static size_t need(size_t n, size_t esz) { return (n * esz + 255) & ~(size_t)255; }
+};
+
+Dims dims_of(int nx, int ny, int ng) {
+  Dims d{};
+  d.nx = nx;
+  d.ny = ny;
+  d.ng = ng;
+  d.nC = (long)nx * ny;
+  d.nV = (long)(nx + 1) * ny;
+  d.nH = (long)nx * (ny + 1);
+  d.nU = d.nC + d.nV + d.nH;
+  return d;
 }
 
 int put(cudaStream_t st, const double* dst, const double* src, size_t n) {
@@ -477,3 +528,330 @@ int trt_old_mgqd_coefs(int n_x, int n_y, int n_g, const double* Eg_avg_old, cons
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Grey low-order side
+// ------------------------------------------------------------------------------------------------
+
+namespace {
+
+// Host arrays to device pieces of one arena, and device pieces back.
+struct HostIn {
+  const double* h;
+  size_t n;
+  const double** d;
+};
+struct HostOut {
+  double* h;
+  size_t n;
+  double** d;
+};
+int stage(Arena& ar, std::initializer_list<HostIn> ins, std::initializer_list<HostOut> outs, size_t extra,
+          cudaStream_t st) {
+  size_t bytes = extra;
+  for (const auto& u : ins) bytes += Arena::need(u.n, sizeof(double));
+  for (const auto& u : outs) bytes += Arena::need(u.n, sizeof(double));
+  int rc = ar.reserve(bytes);
+  if (rc) return rc;
+  for (const auto& u : ins) {
+    double* p = ar.take<double>(u.n);
+    *u.d = p;
+    MG_CUDA(cudaMemcpyAsync(p, u.h, u.n * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  for (const auto& u : outs) *u.d = ar.take<double>(u.n);
+  return TRT_OK;
+}
+int fetch(std::initializer_list<HostOut> outs, cudaStream_t st) {
+  for (const auto& u : outs) MG_CUDA(cudaMemcpyAsync(u.h, *u.d, u.n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaStreamSynchronize(st));
+  return TRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trt_collapse_mg_ef(int n_x, int n_y, int n_g, const double* Eg_avg, const double* Eg_edgV, const double* Eg_edgH,
+                       const double* Fxg_edgV, const double* Fyg_edgH, int Open_Threads, double* E_avg, double* E_edgV,
+                       double* E_edgH, double* Fx_edgV, double* Fy_edgH) {
+  (void)Open_Threads;
+  if (n_x < 1 || n_y < 1 || n_g < 1 || !Eg_avg || !Eg_edgV || !Eg_edgH || !Fxg_edgV || !Fyg_edgH || !E_avg ||
+      !E_edgV || !E_edgH || !Fx_edgV || !Fy_edgH)
+    return TRT_ERR_ARG;
+  int rc = device_ok();
+  if (rc) return rc;
+  const Dims d = dims_of(n_x, n_y, n_g);
+  Arena ar;
+  const double *a, *b, *c, *e, *f;
+  double *o1, *o2, *o3, *o4, *o5;
+  if ((rc = stage(ar, {{Eg_avg, (size_t)d.nC * n_g, &a}, {Eg_edgV, (size_t)d.nV * n_g, &b},
+                       {Eg_edgH, (size_t)d.nH * n_g, &c}, {Fxg_edgV, (size_t)d.nV * n_g, &e},
+                       {Fyg_edgH, (size_t)d.nH * n_g, &f}},
+                  {{E_avg, (size_t)d.nC, &o1}, {E_edgV, (size_t)d.nV, &o2}, {E_edgH, (size_t)d.nH, &o3},
+                   {Fx_edgV, (size_t)d.nV, &o4}, {Fy_edgH, (size_t)d.nH, &o5}},
+                  0, nullptr)))
+    return rc;
+  trt_gqd::collapse_kernel<<<grid1(d.npos()), 256>>>(d, a, b, c, e, f, o1, o2, o3, o4, o5);
+  MG_LAUNCHED();
+  return fetch({{E_avg, (size_t)d.nC, &o1}, {E_edgV, (size_t)d.nV, &o2}, {E_edgH, (size_t)d.nH, &o3},
+                {Fx_edgV, (size_t)d.nV, &o4}, {Fy_edgH, (size_t)d.nH, &o5}},
+               nullptr);
+}
+
+int trt_cbar_calc(int n_x, int n_y, int n_g, double* Cb_L, double* Cb_B, double* Cb_R, double* Cb_T, const double* Cg_L,
+                  const double* Cg_B, const double* Cg_R, const double* Cg_T, const double* Eg_avg,
+                  const double* Eg_edgV, const double* Eg_edgH, const double* Eg_in_L, const double* Eg_in_B,
+                  const double* Eg_in_R, const double* Eg_in_T) {
+  (void)Eg_avg;
+  if (n_x < 1 || n_y < 1 || n_g < 1 || !Cb_L || !Cb_B || !Cb_R || !Cb_T || !Cg_L || !Cg_B || !Cg_R || !Cg_T ||
+      !Eg_edgV || !Eg_edgH || !Eg_in_L || !Eg_in_B || !Eg_in_R || !Eg_in_T)
+    return TRT_ERR_ARG;
+  int rc = device_ok();
+  if (rc) return rc;
+  const Dims d = dims_of(n_x, n_y, n_g);
+  const size_t by = (size_t)n_y * n_g, bx = (size_t)n_x * n_g;
+  Arena ar;
+  trt_gqd::CbarArgs a{};
+  if ((rc = stage(ar, {{Cg_L, by, &a.CgL}, {Cg_B, bx, &a.CgB}, {Cg_R, by, &a.CgR}, {Cg_T, bx, &a.CgT},
+                       {Eg_edgV, (size_t)d.nV * n_g, &a.EgV}, {Eg_edgH, (size_t)d.nH * n_g, &a.EgH},
+                       {Eg_in_L, by, &a.EinL}, {Eg_in_B, bx, &a.EinB}, {Eg_in_R, by, &a.EinR}, {Eg_in_T, bx, &a.EinT}},
+                  {{Cb_L, (size_t)n_y, &a.CbL}, {Cb_B, (size_t)n_x, &a.CbB}, {Cb_R, (size_t)n_y, &a.CbR},
+                   {Cb_T, (size_t)n_x, &a.CbT}},
+                  0, nullptr)))
+    return rc;
+  trt_gqd::cbar_kernel<<<grid1(n_x + n_y), 256>>>(d, a);
+  MG_LAUNCHED();
+  return fetch({{Cb_L, (size_t)n_y, &a.CbL}, {Cb_B, (size_t)n_x, &a.CbB}, {Cb_R, (size_t)n_y, &a.CbR},
+                {Cb_T, (size_t)n_x, &a.CbT}},
+               nullptr);
+}
+
+int trt_old_grey_coefs(int n_x, int n_y, int n_g, double c, double Delt, double Theta, double cv, const double* A,
+                       const double* Gold, const double* Temp_old, const double* KapE_bar_old, const double* E_avg_old,
+                       const double* GQD_Src_old, double* Gold_Hat, double* Rhat_old) {
+  if (n_x < 1 || n_y < 1 || n_g < 1 || !A || !Gold || !Temp_old || !KapE_bar_old || !E_avg_old || !GQD_Src_old ||
+      !Gold_Hat || !Rhat_old || !(Theta != 0.0) || !(Delt > 0.0))
+    return TRT_ERR_ARG;
+  int rc = device_ok();
+  if (rc) return rc;
+  const Dims d = dims_of(n_x, n_y, n_g);
+  const size_t C = (size_t)d.nC;
+  Arena ar;
+  const double *a, *g, *t, *k, *e, *q;
+  double *gh, *rh;
+  if ((rc = stage(ar, {{A, C, &a}, {Gold, C * n_g, &g}, {Temp_old, C, &t}, {KapE_bar_old, C, &k}, {E_avg_old, C, &e},
+                       {GQD_Src_old, C, &q}},
+                  {{Gold_Hat, C, &gh}, {Rhat_old, C, &rh}}, 0, nullptr)))
+    return rc;
+  trt_gqd::old_grey_kernel<<<grid1(d.nC), 256>>>(d, c, Delt, Theta, cv, a, g, t, k, e, q, gh, rh);
+  MG_LAUNCHED();
+  return fetch({{Gold_Hat, C, &gh}, {Rhat_old, C, &rh}}, nullptr);
+}
+
+int trt_grey_coefs(int n_x, int n_y, int n_g, const double* Eg_avg, const double* Eg_edgV, const double* Eg_edgH,
+                   const double* Fxg_edgV_old, const double* Fyg_edgH_old, const double* fg_avg_xx,
+                   const double* fg_avg_yy, const double* fg_edgV_xx, const double* fg_edgV_xy, const double* fg_edgH_yy,
+                   const double* fg_edgH_xy, const double* KapE, const double* KapR, const double* A, double c,
+                   double Delt, double Theta, const double* Pold_L, const double* Pold_R, const double* Pold_B,
+                   const double* Pold_T, double* KapE_Bar, double* DC_xx, double* DL_xx, double* DR_xx, double* DC_yy,
+                   double* DB_yy, double* DT_yy, double* DL_xy, double* DR_xy, double* DB_xy, double* DT_xy,
+                   double* PL, double* PR, double* PB, double* PT, double Fdt_Weight) {
+  const double* ins[] = {Eg_avg, Eg_edgV, Eg_edgH, Fxg_edgV_old, Fyg_edgH_old, fg_avg_xx, fg_avg_yy, fg_edgV_xx,
+                         fg_edgV_xy, fg_edgH_yy, fg_edgH_xy, KapE, KapR, A, Pold_L, Pold_R, Pold_B, Pold_T};
+  double* outs[] = {KapE_Bar, DC_xx, DL_xx, DR_xx, DC_yy, DB_yy, DT_yy, DL_xy, DR_xy, DB_xy, DT_xy, PL, PR, PB, PT};
+  if (n_x < 1 || n_y < 1 || n_g < 1 || !(Theta != 0.0) || !(Delt > 0.0) || !(c > 0.0)) return TRT_ERR_ARG;
+  for (const double* p : ins)
+    if (!p) return TRT_ERR_ARG;
+  for (double* p : outs)
+    if (!p) return TRT_ERR_ARG;
+  int rc = device_ok();
+  if (rc) return rc;
+  const Dims d = dims_of(n_x, n_y, n_g);
+  const size_t C = (size_t)d.nC * n_g, V = (size_t)d.nV * n_g, H = (size_t)d.nH * n_g, c1 = (size_t)d.nC;
+  Arena ar;
+  trt_gqd::GreyIn in{};
+  trt_gqd::GreyOut o{};
+  if ((rc = stage(ar, {{Eg_avg, C, &in.Eg}, {Eg_edgV, V, &in.EgV}, {Eg_edgH, H, &in.EgH}, {Fxg_edgV_old, V, &in.FxOld},
+                       {Fyg_edgH_old, H, &in.FyOld}, {fg_avg_xx, C, &in.fxx}, {fg_avg_yy, C, &in.fyy},
+                       {fg_edgV_xx, V, &in.fVxx}, {fg_edgV_xy, V, &in.fVxy}, {fg_edgH_yy, H, &in.fHyy},
+                       {fg_edgH_xy, H, &in.fHxy}, {KapE, C, &in.KapE}, {KapR, C, &in.KapR}, {A, c1, &in.A},
+                       {Pold_L, C, &in.PoldL}, {Pold_R, C, &in.PoldR}, {Pold_B, C, &in.PoldB}, {Pold_T, C, &in.PoldT}},
+                  {{KapE_Bar, c1, &o.Kb}, {DC_xx, c1, &o.DCxx}, {DL_xx, c1, &o.DLxx}, {DR_xx, c1, &o.DRxx},
+                   {DC_yy, c1, &o.DCyy}, {DB_yy, c1, &o.DByy}, {DT_yy, c1, &o.DTyy}, {DL_xy, c1, &o.DLxy},
+                   {DR_xy, c1, &o.DRxy}, {DB_xy, c1, &o.DBxy}, {DT_xy, c1, &o.DTxy}, {PL, c1, &o.PL}, {PR, c1, &o.PR},
+                   {PB, c1, &o.PB}, {PT, c1, &o.PT}},
+                  0, nullptr)))
+    return rc;
+  in.c = c;
+  in.Delt = Delt;
+  in.Theta = Theta;
+  in.Fdt = Fdt_Weight;
+  trt_gqd::grey_coefs_kernel<<<grid1(d.nC), 256>>>(d, in, o);
+  MG_LAUNCHED();
+  return fetch({{KapE_Bar, c1, &o.Kb}, {DC_xx, c1, &o.DCxx}, {DL_xx, c1, &o.DLxx}, {DR_xx, c1, &o.DRxx},
+                {DC_yy, c1, &o.DCyy}, {DB_yy, c1, &o.DByy}, {DT_yy, c1, &o.DTyy}, {DL_xy, c1, &o.DLxy},
+                {DR_xy, c1, &o.DRxy}, {DB_xy, c1, &o.DBxy}, {DT_xy, c1, &o.DTxy}, {PL, c1, &o.PL}, {PR, c1, &o.PR},
+                {PB, c1, &o.PB}, {PT, c1, &o.PT}},
+               nullptr);
+}
+
+int trt_egp_fv_newt(int n_x, int n_y, double* E_avg, double* E_edgV, double* E_edgH, double* Temp, double* KapE_Bar,
+                    double* Fx_edgV, double* Fy_edgH, double* Q_bar, double* KapE_Bar_dT, int* Its, double* Deltas,
+                    double* dresiduals, const double* Temp_Mold, const double* KapE_bar_Mold, double Theta, double Delt,
+                    const double* Delx, const double* Dely, const double* A, const double* Cb_L, const double* Cb_B,
+                    const double* Cb_R, const double* Cb_T, const double* E_in_L, const double* E_in_B,
+                    const double* E_in_R, const double* E_in_T, const double* F_in_L, const double* F_in_B,
+                    const double* F_in_R, const double* F_in_T, const double* DC_xx, const double* DL_xx,
+                    const double* DR_xx, const double* DC_yy, const double* DB_yy, const double* DT_yy,
+                    const double* DL_xy, const double* DR_xy, const double* DB_xy, const double* DT_xy,
+                    const double* PL, const double* PR, const double* PB, const double* PT, const double* Gold_Hat,
+                    const double* Rhat_old, double Kap0, double cv, double Comp_Unit, double Chi, double line_src,
+                    double E_Bound_Low, double T_Bound_Low, double Eps1, double Eps2, int Maxits, int MGQD_It,
+                    int Use_Line_Search, int Use_Safety_Search, int Res_Calc, int kapE_dT_flag, int* GQD_Kits,
+                    double Fin_Weight, double Ein_Weight) {
+  const double* ins[] = {Temp_Mold, KapE_bar_Mold, Delx, Dely, A, Cb_L, Cb_B, Cb_R, Cb_T, E_in_L, E_in_B, E_in_R,
+                         E_in_T, F_in_L, F_in_B, F_in_R, F_in_T, DC_xx, DL_xx, DR_xx, DC_yy, DB_yy, DT_yy, DL_xy,
+                         DR_xy, DB_xy, DT_xy, PL, PR, PB, PT, Gold_Hat, Rhat_old};
+  double* io[] = {E_avg, E_edgV, E_edgH, Temp, KapE_Bar, Fx_edgV, Fy_edgH, Q_bar, KapE_Bar_dT};
+  if (n_x < 1 || n_y < 1 || Maxits < 1 || !Its || !GQD_Kits || (Res_Calc && (!Deltas || !dresiduals)) ||
+      !(Theta != 0.0) || !(Delt > 0.0) || !(Comp_Unit > 0.0) || (Use_Line_Search && !(line_src > 1.0)) ||
+      (Use_Safety_Search && !(line_src > 1.0)))
+    return TRT_ERR_ARG;
+  for (const double* p : ins)
+    if (!p) return TRT_ERR_ARG;
+  for (double* p : io)
+    if (!p) return TRT_ERR_ARG;
+  int rc = device_ok();
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g_cache.mu);
+  Solver* G = nullptr;
+  if ((rc = get_solver(n_x, n_y, 1, &G, g_cache.grey))) return rc;
+  const Dims d = G->d;
+  cudaStream_t st = G->st;
+  const size_t C = (size_t)d.nC, V = (size_t)d.nV, H = (size_t)d.nH;
+  const int nblk = G->pos_blocks();
+  trt_gqd::Egp e{};
+  e.nx = n_x;
+  e.ny = n_y;
+  Arena ar;
+  const double *cE, *cEV, *cEH, *cT, *cKb, *cFx, *cFy;
+  const size_t extra = Arena::need(C, 8) * 2 + Arena::need(C, 8) * 5 + Arena::need(V, 8) + Arena::need(H, 8) +
+                       Arena::need((size_t)nblk * 6, 8) + Arena::need(8, 8) + Arena::need(18, 8) + 256;
+  if ((rc = stage(ar,
+                  {{E_avg, C, &cE}, {E_edgV, V, &cEV}, {E_edgH, H, &cEH}, {Temp, C, &cT}, {KapE_Bar, C, &cKb},
+                   {Fx_edgV, V, &cFx}, {Fy_edgH, H, &cFy}, {Temp_Mold, C, &e.Tm}, {KapE_bar_Mold, C, &e.Kbm},
+                   {Delx, (size_t)n_x, &e.Delx}, {Dely, (size_t)n_y, &e.Dely}, {A, C, &e.A}, {Cb_L, (size_t)n_y, &e.CbL},
+                   {Cb_B, (size_t)n_x, &e.CbB}, {Cb_R, (size_t)n_y, &e.CbR}, {Cb_T, (size_t)n_x, &e.CbT},
+                   {E_in_L, (size_t)n_y, &e.EinL}, {E_in_B, (size_t)n_x, &e.EinB}, {E_in_R, (size_t)n_y, &e.EinR},
+                   {E_in_T, (size_t)n_x, &e.EinT}, {F_in_L, (size_t)n_y, &e.FinL}, {F_in_B, (size_t)n_x, &e.FinB},
+                   {F_in_R, (size_t)n_y, &e.FinR}, {F_in_T, (size_t)n_x, &e.FinT}, {DC_xx, C, &e.DCxx},
+                   {DL_xx, C, &e.DLxx}, {DR_xx, C, &e.DRxx}, {DC_yy, C, &e.DCyy}, {DB_yy, C, &e.DByy},
+                   {DT_yy, C, &e.DTyy}, {DL_xy, C, &e.DLxy}, {DR_xy, C, &e.DRxy}, {DB_xy, C, &e.DBxy},
+                   {DT_xy, C, &e.DTxy}, {PL, C, &e.PL}, {PR, C, &e.PR}, {PB, C, &e.PB}, {PT, C, &e.PT},
+                   {Gold_Hat, C, &e.Gh}, {Rhat_old, C, &e.Rh}},
+                  {}, extra, st)))
+    return rc;
+  e.E = const_cast<double*>(cE);
+  e.EV = const_cast<double*>(cEV);
+  e.EH = const_cast<double*>(cEH);
+  e.T = const_cast<double*>(cT);
+  e.Kb = const_cast<double*>(cKb);
+  e.Fx = const_cast<double*>(cFx);
+  e.Fy = const_cast<double*>(cFy);
+  e.Q = ar.take<double>(C);
+  e.Kdt = ar.take<double>(C);
+  e.Korg = ar.take<double>(C);
+  e.drT = ar.take<double>(C);
+  e.W = ar.take<double>(C);
+  e.dT = ar.take<double>(C);
+  e.dFx = ar.take<double>(V);
+  e.dFy = ar.take<double>(H);
+  double* part = ar.take<double>((size_t)nblk * 6);
+  double* norms = ar.take<double>(8);
+  e.maxbuf = ar.take<unsigned long long>(18);
+  e.kreq = ar.take<int>(8);
+  if (ar.used > ar.cap + 256) return TRT_ERR_NOMEM;
+  const double h = 6.62613e-19, c = 2.99792458e2, pi = 4.0 * std::atan(1.0), erg = 6.24150934e11;
+  const double sig_R = 2.0 * std::pow(pi, 5) / (15.0 * (c * c) * (h * h * h) * std::pow(erg, 4) * Comp_Unit);
+  e.aR = 4.0 * sig_R / c;
+  e.Theta = Theta;
+  e.Delt = Delt;
+  e.Kap0 = Kap0;
+  e.cv = cv;
+  e.Chi = Chi;
+  e.Fin = Fin_Weight;
+  e.Ein = Ein_Weight;
+  e.damp = (MGQD_It > 1 && kapE_dT_flag) ? 1 : 0;
+
+  const int gp = G->pos_blocks();
+  trt_gqd::egp_dtinit_kernel<<<grid1(d.nC), 256, 0, st>>>(e);
+  MG_LAUNCHED();
+  MG_CUDA(cudaMemsetAsync(G->K.x, 0, sizeof(double) * d.nU, st));   // Delta E of "iteration 0"
+  double hbuf[18];
+  double hn[8];
+  double prev[6] = {0, 0, 0, 0, 0, 0};
+  bool converged = false, noconv = false;
+  int its = 0;
+  while (!converged && its < Maxits) {
+    its += 1;
+    MG_CUDA(cudaMemsetAsync(e.maxbuf, 0, sizeof(unsigned long long) * 18, st));
+    MG_CUDA(cudaMemsetAsync(e.kreq, 0, sizeof(int), st));
+    trt_gqd::egp_coef_kernel<<<gp, kRedBlock, 0, st>>>(e, d, G->cf);
+    MG_LAUNCHED();
+    if ((rc = G->krylov(st))) return rc;
+    trt_gqd::egp_delta_kernel<<<gp, kRedBlock, 0, st>>>(e, d, G->K.x, part);
+    MG_LAUNCHED();
+    trt_gqd::egp_norm_finish_kernel<<<1, 32, 0, st>>>(part, nblk, norms);
+    MG_LAUNCHED();
+    MG_CUDA(cudaMemcpyAsync(hn, norms, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
+    MG_CUDA(cudaMemcpyAsync(G->h_scal, G->K.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+    MG_CUDA(cudaStreamSynchronize(st));
+    GQD_Kits[its - 1] = (G->h_scal[0].done == 1 ? 1 : -1) * (1 + 2 * G->h_scal[0].its);
+    if (G->h_scal[0].done != 1) noconv = true;
+    // line search (GLOQD_SOLVES.f08:604-636): the six quantities in order, each on the deltas as the
+    // earlier ones left them; the deltas are scaled uniformly, so one cumulative factor carries it
+    double S = 1.0;
+    double nrm[6];
+    for (int q = 0; q < 6; ++q) nrm[q] = std::sqrt(hn[q]);
+    if (Use_Line_Search && its > 1) {
+      for (int q = 0; q < 6; ++q) {
+        double LS = 1.0;
+        for (int k = 0; k < 10; ++k) {
+          if (nrm[q] / S / LS > prev[q]) LS = LS * line_src;
+          else break;
+        }
+        if (LS > 1.0) S = S * LS;
+      }
+    }
+    if (Use_Safety_Search) {
+      trt_gqd::egp_safety_kernel<<<gp, kRedBlock, 0, st>>>(e, d, G->K.x, S, line_src, T_Bound_Low, E_Bound_Low);
+      MG_LAUNCHED();
+      int kq = 0;
+      MG_CUDA(cudaMemcpyAsync(&kq, e.kreq, sizeof(int), cudaMemcpyDeviceToHost, st));
+      MG_CUDA(cudaStreamSynchronize(st));
+      for (int k = 0; k < kq; ++k) S = S * line_src;
+    }
+    trt_gqd::egp_update_kernel<<<gp, kRedBlock, 0, st>>>(e, d, G->K.x, S);
+    MG_LAUNCHED();
+    MG_CUDA(cudaMemcpyAsync(hbuf, e.maxbuf, sizeof(double) * 18, cudaMemcpyDeviceToHost, st));
+    MG_CUDA(cudaStreamSynchronize(st));
+    for (int q = 0; q < 6; ++q) prev[q] = nrm[q] / S;
+    converged = true;
+    for (int q = 0; q < 6; ++q)
+      if (hbuf[6 + q] > Eps1 * hbuf[12 + q] + Eps2) converged = false;
+    if (Res_Calc)
+      for (int q = 0; q < 6; ++q) {
+        Deltas[(its - 1) + (long)Maxits * q] = hbuf[6 + q];
+        dresiduals[(its - 1) + (long)Maxits * q] = hbuf[q];
+      }
+  }
+  *Its = its;
+  if ((rc = fetch({{E_avg, C, &e.E}, {E_edgV, V, &e.EV}, {E_edgH, H, &e.EH}, {Temp, C, &e.T}, {KapE_Bar, C, &e.Kb},
+                   {Fx_edgV, V, &e.Fx}, {Fy_edgH, H, &e.Fy}, {Q_bar, C, &e.Q}, {KapE_Bar_dT, C, &e.Kdt}},
+                  st)))
+    return rc;
+  return noconv ? TRT_ERR_NOCONV : TRT_OK;
+}
+
+}  // extern "C"
+

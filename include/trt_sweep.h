@@ -147,6 +147,59 @@ int trt_mloqd_fv(int n_x, int n_y, int n_g, double* Eg_avg, double* Eg_edgV, dou
                  const double* Fyg_edgH_old, int* MGQD_Kits, double Fdt_Weight, double Fin_Weight,
                  double Ein_Weight);
 
+/* Replaces SUBROUTINE COLLAPSE_MG_EF, MainSrc/MLOQD_SOLVES.f08:687 (body :688-730): group sums of the
+ * multigroup E and F into the grey E_avg(n_x,n_y), E_edgV/Fx_edgV(n_x+1,n_y), E_edgH/Fy_edgH(n_x,n_y+1). */
+int trt_collapse_mg_ef(int n_x, int n_y, int n_g, const double* Eg_avg, const double* Eg_edgV, const double* Eg_edgH,
+                       const double* Fxg_edgV, const double* Fyg_edgH, int Open_Threads, double* E_avg, double* E_edgV,
+                       double* E_edgH, double* Fx_edgV, double* Fy_edgH);
+
+/* Replaces SUBROUTINE Cbar_Calc, MainSrc/GLOQD_SOLVES.f08:177 (body :178-231). Cb_L/Cb_R (n_y), Cb_B/Cb_T
+ * (n_x); Cg_* and Eg_in_* in the multigroup boundary shapes. */
+int trt_cbar_calc(int n_x, int n_y, int n_g, double* Cb_L, double* Cb_B, double* Cb_R, double* Cb_T, const double* Cg_L,
+                  const double* Cg_B, const double* Cg_R, const double* Cg_T, const double* Eg_avg,
+                  const double* Eg_edgV, const double* Eg_edgH, const double* Eg_in_L, const double* Eg_in_B,
+                  const double* Eg_in_R, const double* Eg_in_T);
+
+/* Replaces SUBROUTINE OLD_GREY_COEFS, MainSrc/GLOQD_SOLVES.f08:12 (body :13-42). Gold(n_x,n_y,n_g);
+ * the other arrays (n_x,n_y). */
+int trt_old_grey_coefs(int n_x, int n_y, int n_g, double c, double Delt, double Theta, double cv, const double* A,
+                       const double* Gold, const double* Temp_old, const double* KapE_bar_old, const double* E_avg_old,
+                       const double* GQD_Src_old, double* Gold_Hat, double* Rhat_old);
+
+/* Replaces SUBROUTINE GREY_COEFS, MainSrc/GLOQD_SOLVES.f08:47-49 (body :50-146), argument order as the
+ * subroutine (Pold_L, Pold_R, Pold_B, Pold_T in; KapE_Bar, the D's and PL, PR, PB, PT out, (n_x,n_y)). */
+int trt_grey_coefs(int n_x, int n_y, int n_g, const double* Eg_avg, const double* Eg_edgV, const double* Eg_edgH,
+                   const double* Fxg_edgV_old, const double* Fyg_edgH_old, const double* fg_avg_xx,
+                   const double* fg_avg_yy, const double* fg_edgV_xx, const double* fg_edgV_xy, const double* fg_edgH_yy,
+                   const double* fg_edgH_xy, const double* KapE, const double* KapR, const double* A, double c,
+                   double Delt, double Theta, const double* Pold_L, const double* Pold_R, const double* Pold_B,
+                   const double* Pold_T, double* KapE_Bar, double* DC_xx, double* DL_xx, double* DR_xx, double* DC_yy,
+                   double* DB_yy, double* DT_yy, double* DL_xy, double* DR_xy, double* DB_xy, double* DT_xy,
+                   double* PL, double* PR, double* PB, double* PT, double Fdt_Weight);
+
+/* Replaces SUBROUTINE EGP_FV_NEWT, MainSrc/GLOQD_SOLVES.f08:305-309 (body :310-860): Newton iterations of the
+ * effective grey problem, each linear solve on the device (the solver of trt_mloqd_fv, one system).
+ * E_avg/Temp/KapE_Bar (n_x,n_y), E_edgV/Fx_edgV (n_x+1,n_y), E_edgH/Fy_edgH (n_x,n_y+1): in/out; Q_bar,
+ * KapE_Bar_dT (n_x,n_y): out; Its: Newton iterations; GQD_Kits(Maxits): matrix-vector products of each
+ * iteration's solve (negated if it did not converge, and the call then returns TRT_ERR_NOCONV after
+ * finishing the iterations).  Deltas and dresiduals are (Maxits,6) buffers whose first Its rows are filled
+ * when Res_Calc != 0 (the reference allocates them (Its,6)).  Logical arguments are 0/1.  The safety
+ * search makes one pass (the reference's loop at :646-755 has no exit; one pass is the state it reaches). */
+int trt_egp_fv_newt(int n_x, int n_y, double* E_avg, double* E_edgV, double* E_edgH, double* Temp, double* KapE_Bar,
+                    double* Fx_edgV, double* Fy_edgH, double* Q_bar, double* KapE_Bar_dT, int* Its, double* Deltas,
+                    double* dresiduals, const double* Temp_Mold, const double* KapE_bar_Mold, double Theta, double Delt,
+                    const double* Delx, const double* Dely, const double* A, const double* Cb_L, const double* Cb_B,
+                    const double* Cb_R, const double* Cb_T, const double* E_in_L, const double* E_in_B,
+                    const double* E_in_R, const double* E_in_T, const double* F_in_L, const double* F_in_B,
+                    const double* F_in_R, const double* F_in_T, const double* DC_xx, const double* DL_xx,
+                    const double* DR_xx, const double* DC_yy, const double* DB_yy, const double* DT_yy,
+                    const double* DL_xy, const double* DR_xy, const double* DB_xy, const double* DT_xy,
+                    const double* PL, const double* PR, const double* PB, const double* PT, const double* Gold_Hat,
+                    const double* Rhat_old, double Kap0, double cv, double Comp_Unit, double Chi, double line_src,
+                    double E_Bound_Low, double T_Bound_Low, double Eps1, double Eps2, int Maxits, int MGQD_It,
+                    int Use_Line_Search, int Use_Safety_Search, int Res_Calc, int kapE_dT_flag, int* GQD_Kits,
+                    double Fin_Weight, double Ein_Weight);
+
 /* Convergence settings of trt_mloqd_fv (process-wide): tol > 0, maxit >= 1 iterations per group. */
 int trt_mgqd_set_tolerance(double tol, int maxit);
 

@@ -37,6 +37,12 @@ _SIG = {
     "oracle_old_mgqd_coefs": (_i, [_i, _i, _i] + [_D] * 17 + [_d, _d, _d] + [_D] * 5),
     "oracle_mloqd_fv": (_i, [_i, _i, _i] + [_D] * 29 + [_d, _d, _d, _i, _i] + [_D] * 10 + [_I, _d, _d, _d]),
     "oracle_mloqd_fv_solver": (_i, [_i, _i, _i, _i] + [_D] * 29 + [_d, _d, _d, _i, _i] + [_D] * 10 + [_I, _d, _d, _d]),
+    "oracle_collapse_mg_ef": (_i, [_i, _i, _i] + [_D] * 5 + [_i] + [_D] * 5),
+    "oracle_cbar_calc": (_i, [_i, _i, _i] + [_D] * 15),
+    "oracle_old_grey_coefs": (_i, [_i, _i, _i, _d, _d, _d, _d] + [_D] * 8),
+    "oracle_grey_coefs": (_i, [_i, _i, _i] + [_D] * 14 + [_d, _d, _d] + [_D] * 4 + [_D] * 15 + [_d]),
+    "oracle_egp_fv_newt": (_i, [_i, _i] + [_D] * 9 + [_I, _D, _D, _D, _D, _d, _d] + [_D] * 3 + [_D] * 12 + [_D] * 14
+                           + [_D] * 2 + [_d] * 9 + [_i] * 6 + [_I, _d, _d]),
 }
 
 _lib = None
@@ -308,5 +314,88 @@ def mloqd_fv(d, c, Delt, Theta=1.0, res_calc=True, threads=1, Fdt_Weight=1.0, Fi
         *[_p(F(d[k])) for k in MLOQD_OLD], _p(o["MGQD_Kits"]), float(Fdt_Weight), float(Fin_Weight),
         float(Ein_Weight))
     assert rc == 0, rc
+    return o
+
+
+# Grey low-order side (GLOQD_SOLVES.f08, MLOQD_SOLVES.f08:687-730).
+GREY_D = ("DC_xx", "DL_xx", "DR_xx", "DC_yy", "DB_yy", "DT_yy", "DL_xy", "DR_xy", "DB_xy", "DT_xy")
+GREY_P = ("PL", "PR", "PB", "PT")
+SIDES = ("L", "B", "R", "T")
+
+
+def collapse_mg_ef(d):
+    """COLLAPSE_MG_EF: group sums of Eg_avg/Eg_edgV/Eg_edgH/Fxg_edgV/Fyg_edgH."""
+    nx, ny, ng = d["Eg_avg"].shape
+    o = {"E_avg": zeros(nx, ny), "E_edgV": zeros(nx + 1, ny), "E_edgH": zeros(nx, ny + 1),
+         "Fx_edgV": zeros(nx + 1, ny), "Fy_edgH": zeros(nx, ny + 1)}
+    rc = lib().oracle_collapse_mg_ef(nx, ny, ng, *[_p(F(d[k])) for k in ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV",
+                                                                       "Fyg_edgH")], 1, *[_p(v) for v in o.values()])
+    assert rc == 0
+    return o
+
+
+def cbar_calc(d):
+    """Cbar_Calc: Cb_L, Cb_B, Cb_R, Cb_T."""
+    nx, ny, ng = d["Eg_avg"].shape
+    o = {"Cb_" + s: zeros(ny if s in "LR" else nx) for s in SIDES}
+    rc = lib().oracle_cbar_calc(nx, ny, ng, *[_p(v) for v in o.values()], *[_p(F(d["Cg_" + s])) for s in SIDES],
+                                *[_p(F(d[k])) for k in ("Eg_avg", "Eg_edgV", "Eg_edgH")],
+                                *[_p(F(d["Eg_in_" + s])) for s in SIDES])
+    assert rc == 0
+    return o
+
+
+def old_grey_coefs(c, Delt, Theta, cv, A, Gold, Temp_old, KapE_bar_old, E_avg_old, GQD_Src_old):
+    """OLD_GREY_COEFS: (Gold_Hat, Rhat_old)."""
+    nx, ny, ng = Gold.shape
+    gh, rh = zeros(nx, ny), zeros(nx, ny)
+    rc = lib().oracle_old_grey_coefs(nx, ny, ng, float(c), float(Delt), float(Theta), float(cv), _p(F(A)), _p(F(Gold)),
+                                     _p(F(Temp_old)), _p(F(KapE_bar_old)), _p(F(E_avg_old)), _p(F(GQD_Src_old)),
+                                     _p(gh), _p(rh))
+    assert rc == 0
+    return gh, rh
+
+
+def grey_coefs(d, c, Delt, Theta, Fdt_Weight=1.0):
+    """GREY_COEFS: KapE_Bar, the ten D's and the four P's (nx, ny)."""
+    nx, ny, ng = d["Eg_avg"].shape
+    o = {k: zeros(nx, ny) for k in ("KapE_Bar",) + GREY_D + GREY_P}
+    ins = ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV_old", "Fyg_edgH_old", "fg_avg_xx", "fg_avg_yy", "fg_edgV_xx",
+           "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy", "KapE", "KapR", "A")
+    rc = lib().oracle_grey_coefs(nx, ny, ng, *[_p(F(d[k])) for k in ins], float(c), float(Delt), float(Theta),
+                                 *[_p(F(d[k])) for k in ("Pold_L", "Pold_R", "Pold_B", "Pold_T")],
+                                 *[_p(v) for v in o.values()], float(Fdt_Weight))
+    assert rc == 0
+    return o
+
+
+EGP_STATE = ("E_avg", "E_edgV", "E_edgH", "Temp", "KapE_Bar", "Fx_edgV", "Fy_edgH")
+
+
+def egp_fv_newt(g, Theta, Delt, Kap0, cv, Comp_Unit, Chi=0.7, line_src=2.0, E_Bound_Low=0.0, T_Bound_Low=0.0,
+                Eps1=1e-14, Eps2=1e-15, Maxits=10, MGQD_It=1, Use_Line_Search=True, Use_Safety_Search=False,
+                Res_Calc=True, kapE_dT_flag=True, Fin_Weight=1.0, Ein_Weight=1.0):
+    """EGP_FV_NEWT (GLOQD_SOLVES.f08:305-860) on copies of g's state (E_avg, E_edgV, E_edgH, Temp, KapE_Bar,
+    Fx_edgV, Fy_edgH); g also holds Temp_Mold, KapE_bar_Mold, Delx, Dely, A, Cb_*, E_in_*, F_in_*, the D's,
+    the P's, Gold_Hat and Rhat_old.  Returns the new state plus Q_bar, KapE_Bar_dT, Its, GQD_Kits,
+    Deltas (Its, 6), dresiduals (Its, 6)."""
+    nx, ny = g["Temp"].shape
+    o = {k: F(g[k]).copy(order="F") for k in EGP_STATE}
+    o["Q_bar"], o["KapE_Bar_dT"] = zeros(nx, ny), zeros(nx, ny)
+    its = ctypes.c_int(0)
+    Dl, dr = zeros(Maxits, 6), zeros(Maxits, 6)
+    kits = np.zeros(Maxits, dtype=np.int32)
+    rc = lib().oracle_egp_fv_newt(
+        nx, ny, *[_p(o[k]) for k in EGP_STATE], _p(o["Q_bar"]), _p(o["KapE_Bar_dT"]), ctypes.byref(its), _p(Dl),
+        _p(dr), _p(F(g["Temp_Mold"])), _p(F(g["KapE_bar_Mold"])), float(Theta), float(Delt), _p(F(g["Delx"])),
+        _p(F(g["Dely"])), _p(F(g["A"])), *[_p(F(g["Cb_" + s])) for s in SIDES], *[_p(F(g["E_in_" + s])) for s in SIDES],
+        *[_p(F(g["F_in_" + s])) for s in SIDES], *[_p(F(g[k])) for k in GREY_D + GREY_P],
+        _p(F(g["Gold_Hat"])), _p(F(g["Rhat_old"])), float(Kap0), float(cv), float(Comp_Unit), float(Chi),
+        float(line_src), float(E_Bound_Low), float(T_Bound_Low), float(Eps1), float(Eps2), int(Maxits), int(MGQD_It),
+        int(bool(Use_Line_Search)), int(bool(Use_Safety_Search)), int(bool(Res_Calc)), int(bool(kapE_dT_flag)),
+        _p(kits), float(Fin_Weight), float(Ein_Weight))
+    assert rc == 0, rc
+    n = its.value
+    o["Its"], o["GQD_Kits"], o["Deltas"], o["dresiduals"] = n, kits[:n], Dl[:n], dr[:n]
     return o
 
