@@ -61,6 +61,23 @@ def moment_shape(name, nx, ny, ng):
     raise KeyError(name)
 
 
+class MlqdParams(ctypes.Structure):
+    """trt_mlqd_params (include/trt_sweep.h)."""
+    _fields_ = [("conv_lo", ctypes.c_double), ("conv_gr1", ctypes.c_double), ("conv_gr2", ctypes.c_double),
+                ("maxit_mloqd", ctypes.c_int), ("maxit_gloqd", ctypes.c_int), ("chi", ctypes.c_double),
+                ("line_src", ctypes.c_double), ("E_bound_low", ctypes.c_double), ("T_bound_low", ctypes.c_double),
+                ("use_line_search", ctypes.c_int), ("use_safety_search", ctypes.c_int),
+                ("kapE_dT_flag", ctypes.c_int), ("theta", ctypes.c_double)]
+
+
+class MlqdStats(ctypes.Structure):
+    """trt_mlqd_stats (include/trt_sweep.h)."""
+    _fields_ = [("rt_its", ctypes.c_int), ("sweeps", ctypes.c_int), ("mgqd_its", ctypes.c_int),
+                ("egp_its", ctypes.c_int), ("mgqd_nonconv", ctypes.c_int), ("egp_nonconv", ctypes.c_int),
+                ("T_norm", ctypes.c_double), ("E_norm", ctypes.c_double), ("sweep_ms", ctypes.c_double),
+                ("low_order_ms", ctypes.c_double)]
+
+
 # Exported symbols and their ctypes signatures.
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -123,6 +140,10 @@ SIGNATURES = {
     "trt_egp_fv_newt": (_i, [_i, _i] + [_D] * 9 + [_I, _D, _D, _D, _D, _d, _d] + [_D] * 3 + [_D] * 12 + [_D] * 14
                         + [_D] * 2 + [_d] * 9 + [_i] * 6 + [_I, _d, _d]),
     "trt_mgqd_last_stats": (_i, [_D, _I, _D]),
+    "trt_mlqd_setup": (_i, [_P, _d, ctypes.POINTER(MlqdParams)]),
+    "trt_mlqd_step": (_i, [_P, ctypes.POINTER(MlqdStats)]),
+    "trt_mlqd_counts": (_i, [_P, _I, _i, _I, _i, _I, _I]),
+    "trt_mlqd_get": (_i, [_P, ctypes.c_char_p, _D, ctypes.c_longlong]),
 }
 
 _lib = None

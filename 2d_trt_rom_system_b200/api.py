@@ -414,6 +414,48 @@ class TransportSweep:
         check(_lib.lib().trt_tstep(self._h, ctypes.byref(its), ctypes.byref(tn), ctypes.byref(en)), "trt_tstep")
         return its.value, tn.value, en.value
 
+    def mlqd_setup(self, Tini, conv_lo=1e-10, conv_gr1=1e-14, conv_gr2=1e-15, maxit_mloqd=50, maxit_gloqd=20,
+                   chi=0.7, line_src=2.0, E_Bound_Low=0.0, T_Bound_Low=0.0, use_line_search=True,
+                   use_safety_search=False, kapE_dT_flag=True, Theta=1.0):
+        """Device time stepping with the reference's run_type 'mlqd' (after init_state and tstep_setup):
+        the initial low-order state of MGQD_INIT / GQD_INIT at Tini."""
+        p = _lib.MlqdParams(float(conv_lo), float(conv_gr1), float(conv_gr2), int(maxit_mloqd), int(maxit_gloqd),
+                            float(chi), float(line_src), float(E_Bound_Low), float(T_Bound_Low),
+                            int(bool(use_line_search)), int(bool(use_safety_search)), int(bool(kapE_dT_flag)),
+                            float(Theta))
+        check(_lib.lib().trt_mlqd_setup(self._h, float(Tini), ctypes.byref(p)), "trt_mlqd_setup")
+
+    def mlqd_step(self):
+        """One mlqd time step; returns its statistics (dict) with the MGQD iterations of each outer iteration
+        and the EGP iterations of each MGQD iteration."""
+        st = _lib.MlqdStats()
+        check(_lib.lib().trt_mlqd_step(self._h, ctypes.byref(st)), "trt_mlqd_step")
+        out = {k: getattr(st, k) for k, _ in _lib.MlqdStats._fields_}
+        a, b = np.zeros(4096, dtype=np.int32), np.zeros(65536, dtype=np.int32)
+        n1, n2 = ctypes.c_int(0), ctypes.c_int(0)
+        check(_lib.lib().trt_mlqd_counts(self._h, iptr(a), len(a), iptr(b), len(b), ctypes.byref(n1),
+                                         ctypes.byref(n2)), "trt_mlqd_counts")
+        out["mgqd_per_outer"] = a[:n1.value].tolist()
+        out["egp_per_mgqd"] = b[:n2.value].tolist()
+        return out
+
+    def mlqd_field(self, name):
+        """A field of the device mlqd state (trt_mlqd_get), Fortran layout."""
+        nx, ny, ng = self.nx, self.ny, self.ng
+        grey = {"avg": (nx, ny), "edgV": (nx + 1, ny), "edgH": (nx, ny + 1)}
+        if name.startswith("Cb_"):
+            shp = (ny if name[-1] in "LR" else nx,)
+        elif name in ("Temp", "KapE_Bar", "KapE_Bar_dT", "GQD_Src", "MGQD_E_avg", "HO_E_avg"):
+            shp = (nx, ny)
+        elif name == "MGQD_Src":
+            shp = (nx, ny, ng)
+        else:
+            key = [k for k in grey if k in name][0]
+            shp = grey[key] + ((ng,) if name.startswith(("Eg_", "Fxg", "Fyg")) else ())
+        out = np.empty(shp, order="F")
+        check(_lib.lib().trt_mlqd_get(self._h, name.encode(), dptr(out), out.size), "trt_mlqd_get")
+        return out
+
     def temperature(self):
         T = np.empty((self.nx, self.ny), order="F")
         check(_lib.lib().trt_get_temperature(self._h, dptr(T)), "trt_get_temperature")

@@ -95,17 +95,19 @@ __global__ void cbar_kernel(const Dims d, const CbarArgs a) {
 }
 
 // OLD_GREY_COEFS: one thread per cell.
+// cvc: heat capacity per cell, or nullptr for the reference's single value cv.
 __global__ void old_grey_kernel(const Dims d, double c, double Delt, double Theta, double cv,
                                 const double* __restrict__ A, const double* __restrict__ Gold,
                                 const double* __restrict__ Told, const double* __restrict__ Kbold,
                                 const double* __restrict__ Eold, const double* __restrict__ Qold, double* Gh,
-                                double* Rh) {
+                                double* Rh, const double* __restrict__ cvc) {
   const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (k >= d.nC) return;
   double s = 0.0;
   for (int g = 0; g < d.ng; ++g) s = s + Gold[k + d.nC * g];
   Gh[k] = s + A[k] * Eold[k] / (Theta * Delt);
-  Rh[k] = cv / (Theta * Delt) * Told[k] + ((1.0 - Theta) / Theta) * (c * Kbold[k] * Eold[k] - Qold[k]);
+  const double cvk = cvc ? cvc[k] : cv;
+  Rh[k] = cvk / (Theta * Delt) * Told[k] + ((1.0 - Theta) / Theta) * (c * Kbold[k] * Eold[k] - Qold[k]);
 }
 
 // GREY_COEFS: one thread per cell, groups in order.
@@ -190,8 +192,11 @@ struct Egp {
   unsigned long long* maxbuf;   // [0..5] max |dr_*|; [6..11] max |Delta|; [12..17] max |value|
   int* kreq;                    // safety search: steps of line_src required
   double Theta, Delt, Kap0, cv, aR, Chi, Fin, Ein;
+  const double* cvc;            // heat capacity per cell, or nullptr for the single value cv
   int damp;                     // MGQD_It > 1 and kapE_dT_flag
 };
+
+__device__ __forceinline__ double egp_cv(const Egp& e, long k) { return e.cvc ? e.cvc[k] : e.cv; }
 
 __device__ __forceinline__ void atomic_max_abs(unsigned long long* p, double v) {
   atomicMax(p, (unsigned long long)__double_as_longlong(fabs(v)));
@@ -249,17 +254,17 @@ __global__ void egp_coef_kernel(const Egp e, const Dims d, const Coefs cf) {
     double kdt = e.Kdt[k];
     if (e.damp) {
       kdt = e.Korg[k];
-      const double bound = (e.cv / (e.Theta * e.Delt) + Qdt) / (c * e.E[k]);
+      const double bound = (egp_cv(e, k) / (e.Theta * e.Delt) + Qdt) / (c * e.E[k]);
       if (kdt > e.Chi * bound) kdt = e.Chi * bound;
       e.Kdt[k] = kdt;
     }
     const long vL = i + (long)(nx + 1) * j, hB = k;
-    const double drT = e.cv / (e.Theta * e.Delt) * e.T[k] + Q - c * e.Kb[k] * e.E[k] - e.Rh[k];
+    const double drT = egp_cv(e, k) / (e.Theta * e.Delt) * e.T[k] + Q - c * e.Kb[k] * e.E[k] - e.Rh[k];
     const double drB = a * (1.0 / (e.Theta * e.Delt) + c * e.Kb[k]) * e.E[k] + dy * (e.Fx[vL + 1] - e.Fx[vL]) +
                        dx * (e.Fy[hB + nx] - e.Fy[hB]) - a * Q - e.Gh[k];
     const double drML = egp_drML(e, i, j), drMR = egp_drMR(e, i, j), drMB = egp_drMB(e, i, j),
                  drMT = egp_drMT(e, i, j);
-    const double W = e.cv / (e.Theta * e.Delt) + Qdt - c * kdt * e.E[k];
+    const double W = egp_cv(e, k) / (e.Theta * e.Delt) + Qdt - c * kdt * e.E[k];
     e.drT[k] = drT;
     e.W[k] = W;
     atomic_max_abs(&e.maxbuf[0], drT);

@@ -9,11 +9,8 @@
 
 #include "trt_sweep.h"
 #include "gqd_kernels.cuh"
+#include "handle_hooks.h"
 #include "mgqd_kernels.cuh"
-
-namespace trt_host {
-void add_launches(unsigned long long n);   // library-wide launch counter (trt_api.cu)
-}
 
 namespace {
 
@@ -84,13 +81,13 @@ struct Solver {
     bufs.push_back(*p);
     return TRT_OK;
   }
-  int init(int nx, int ny, int ng);
+  int init(int nx, int ny, int ng, bool own_inputs = true);   // own_inputs: allocate the Inputs planes
   int solve(cudaStream_t s);    // MLOQD_FV: coefficients, Krylov solve, fluxes, residuals
   int krylov(cudaStream_t s);   // the solve of whatever system the coefficient planes hold
   int pos_blocks() const { return (int)((d.npos() + kRedBlock - 1) / kRedBlock); }
 };
 
-int Solver::init(int nx, int ny, int ng) {
+int Solver::init(int nx, int ny, int ng, bool own_inputs) {
   d.nx = nx;
   d.ny = ny;
   d.ng = ng;
@@ -113,14 +110,16 @@ int Solver::init(int nx, int ny, int ng) {
   auto M = [&](auto** p, size_t n) {
     if (!rc) rc = alloc(p, n);
   };
-  // inputs
-  A(&in.fxx, C); A(&in.fyy, C); A(&in.fVxx, V); A(&in.fVxy, V); A(&in.fHyy, H); A(&in.fHxy, H);
-  A(&in.CgL, (size_t)ny * ng); A(&in.CgB, (size_t)nx * ng); A(&in.CgR, (size_t)ny * ng); A(&in.CgT, (size_t)nx * ng);
-  A(&in.EinL, (size_t)ny * ng); A(&in.EinB, (size_t)nx * ng); A(&in.EinR, (size_t)ny * ng); A(&in.EinT, (size_t)nx * ng);
-  A(&in.FinL, (size_t)ny * ng); A(&in.FinB, (size_t)nx * ng); A(&in.FinR, (size_t)ny * ng); A(&in.FinT, (size_t)nx * ng);
-  A(&in.Src, C); A(&in.KapE, C); A(&in.KapR, C); A(&in.Delx, nx); A(&in.Dely, ny); A(&in.A, d.nC);
-  A(&in.Gold, C); A(&in.PoldL, C); A(&in.PoldB, C); A(&in.PoldR, C); A(&in.PoldT, C);
-  A(&in.Eold, C); A(&in.Fxold, V); A(&in.Fyold, H);
+  // inputs (a caller that points them at its own device fields skips them)
+  if (own_inputs) {
+    A(&in.fxx, C); A(&in.fyy, C); A(&in.fVxx, V); A(&in.fVxy, V); A(&in.fHyy, H); A(&in.fHxy, H);
+    A(&in.CgL, (size_t)ny * ng); A(&in.CgB, (size_t)nx * ng); A(&in.CgR, (size_t)ny * ng); A(&in.CgT, (size_t)nx * ng);
+    A(&in.EinL, (size_t)ny * ng); A(&in.EinB, (size_t)nx * ng); A(&in.EinR, (size_t)ny * ng); A(&in.EinT, (size_t)nx * ng);
+    A(&in.FinL, (size_t)ny * ng); A(&in.FinB, (size_t)nx * ng); A(&in.FinR, (size_t)ny * ng); A(&in.FinT, (size_t)nx * ng);
+    A(&in.Src, C); A(&in.KapE, C); A(&in.KapR, C); A(&in.Delx, nx); A(&in.Dely, ny); A(&in.A, d.nC);
+    A(&in.Gold, C); A(&in.PoldL, C); A(&in.PoldB, C); A(&in.PoldR, C); A(&in.PoldT, C);
+    A(&in.Eold, C); A(&in.Fxold, V); A(&in.Fyold, H);
+  }
   // coefficients
   M(&cf.Xi, C); M(&cf.PhL, C); M(&cf.PhB, C); M(&cf.PhR, C); M(&cf.PhT, C);
   M(&cf.EBL, C); M(&cf.EBB, C); M(&cf.EBC, C); M(&cf.EBR, C); M(&cf.EBT, C);
@@ -567,6 +566,88 @@ int fetch(std::initializer_list<HostOut> outs, cudaStream_t st) {
   return TRT_OK;
 }
 
+// Options of EGP_FV_NEWT's iteration (GLOQD_SOLVES.f08:305-309).
+struct EgpOpts {
+  double line_src, T_Bound_Low, E_Bound_Low, Eps1, Eps2;
+  int Maxits, Use_Line_Search, Use_Safety_Search, Res_Calc;
+};
+
+// The Newton iterations of EGP_FV_NEWT (GLOQD_SOLVES.f08:393-860) on the device state of e, each linear
+// solve by G's preconditioned BiCGSTAB (one system).  part: nblk*6 doubles, norms: 8 doubles (device).
+// GQD_Kits gets the matrix-vector products of each iteration (negative where the solve did not
+// converge); Deltas / dresiduals (Maxits, 6) when Res_Calc.
+int egp_newton(Solver* G, cudaStream_t st, trt_gqd::Egp& e, const EgpOpts& o, double* part, double* norms,
+               int* its_out, int* GQD_Kits, double* Deltas, double* dresiduals, bool* noconv_out) {
+  const Dims d = G->d;
+  const int nblk = G->pos_blocks();
+  int rc;
+  const int gp = G->pos_blocks();
+  trt_gqd::egp_dtinit_kernel<<<grid1(d.nC), 256, 0, st>>>(e);
+  MG_LAUNCHED();
+  MG_CUDA(cudaMemsetAsync(G->K.x, 0, sizeof(double) * d.nU, st));   // Delta E of "iteration 0"
+  double hbuf[18];
+  double hn[8];
+  double prev[6] = {0, 0, 0, 0, 0, 0};
+  bool converged = false, noconv = false;
+  int its = 0;
+  while (!converged && its < o.Maxits) {
+    its += 1;
+    MG_CUDA(cudaMemsetAsync(e.maxbuf, 0, sizeof(unsigned long long) * 18, st));
+    MG_CUDA(cudaMemsetAsync(e.kreq, 0, sizeof(int), st));
+    trt_gqd::egp_coef_kernel<<<gp, kRedBlock, 0, st>>>(e, d, G->cf);
+    MG_LAUNCHED();
+    if ((rc = G->krylov(st))) return rc;
+    trt_gqd::egp_delta_kernel<<<gp, kRedBlock, 0, st>>>(e, d, G->K.x, part);
+    MG_LAUNCHED();
+    trt_gqd::egp_norm_finish_kernel<<<1, 32, 0, st>>>(part, nblk, norms);
+    MG_LAUNCHED();
+    MG_CUDA(cudaMemcpyAsync(hn, norms, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
+    MG_CUDA(cudaMemcpyAsync(G->h_scal, G->K.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+    MG_CUDA(cudaStreamSynchronize(st));
+    GQD_Kits[its - 1] = (G->h_scal[0].done == 1 ? 1 : -1) * (1 + 2 * G->h_scal[0].its);
+    if (G->h_scal[0].done != 1) noconv = true;
+    // line search (GLOQD_SOLVES.f08:604-636): the six quantities in order, each on the deltas as the
+    // earlier ones left them; the deltas are scaled uniformly, so one cumulative factor carries it
+    double S = 1.0;
+    double nrm[6];
+    for (int q = 0; q < 6; ++q) nrm[q] = std::sqrt(hn[q]);
+    if (o.Use_Line_Search && its > 1) {
+      for (int q = 0; q < 6; ++q) {
+        double LS = 1.0;
+        for (int k = 0; k < 10; ++k) {
+          if (nrm[q] / S / LS > prev[q]) LS = LS * o.line_src;
+          else break;
+        }
+        if (LS > 1.0) S = S * LS;
+      }
+    }
+    if (o.Use_Safety_Search) {
+      trt_gqd::egp_safety_kernel<<<gp, kRedBlock, 0, st>>>(e, d, G->K.x, S, o.line_src, o.T_Bound_Low, o.E_Bound_Low);
+      MG_LAUNCHED();
+      int kq = 0;
+      MG_CUDA(cudaMemcpyAsync(&kq, e.kreq, sizeof(int), cudaMemcpyDeviceToHost, st));
+      MG_CUDA(cudaStreamSynchronize(st));
+      for (int k = 0; k < kq; ++k) S = S * o.line_src;
+    }
+    trt_gqd::egp_update_kernel<<<gp, kRedBlock, 0, st>>>(e, d, G->K.x, S);
+    MG_LAUNCHED();
+    MG_CUDA(cudaMemcpyAsync(hbuf, e.maxbuf, sizeof(double) * 18, cudaMemcpyDeviceToHost, st));
+    MG_CUDA(cudaStreamSynchronize(st));
+    for (int q = 0; q < 6; ++q) prev[q] = nrm[q] / S;
+    converged = true;
+    for (int q = 0; q < 6; ++q)
+      if (hbuf[6 + q] > o.Eps1 * hbuf[12 + q] + o.Eps2) converged = false;
+    if (o.Res_Calc)
+      for (int q = 0; q < 6; ++q) {
+        Deltas[(its - 1) + (long)o.Maxits * q] = hbuf[6 + q];
+        dresiduals[(its - 1) + (long)o.Maxits * q] = hbuf[q];
+      }
+  }
+  *its_out = its;
+  *noconv_out = noconv;
+  return TRT_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -643,7 +724,7 @@ int trt_old_grey_coefs(int n_x, int n_y, int n_g, double c, double Delt, double 
                        {GQD_Src_old, C, &q}},
                   {{Gold_Hat, C, &gh}, {Rhat_old, C, &rh}}, 0, nullptr)))
     return rc;
-  trt_gqd::old_grey_kernel<<<grid1(d.nC), 256>>>(d, c, Delt, Theta, cv, a, g, t, k, e, q, gh, rh);
+  trt_gqd::old_grey_kernel<<<grid1(d.nC), 256>>>(d, c, Delt, Theta, cv, a, g, t, k, e, q, gh, rh, nullptr);
   MG_LAUNCHED();
   return fetch({{Gold_Hat, C, &gh}, {Rhat_old, C, &rh}}, nullptr);
 }
@@ -783,69 +864,10 @@ int trt_egp_fv_newt(int n_x, int n_y, double* E_avg, double* E_edgV, double* E_e
   e.Ein = Ein_Weight;
   e.damp = (MGQD_It > 1 && kapE_dT_flag) ? 1 : 0;
 
-  const int gp = G->pos_blocks();
-  trt_gqd::egp_dtinit_kernel<<<grid1(d.nC), 256, 0, st>>>(e);
-  MG_LAUNCHED();
-  MG_CUDA(cudaMemsetAsync(G->K.x, 0, sizeof(double) * d.nU, st));   // Delta E of "iteration 0"
-  double hbuf[18];
-  double hn[8];
-  double prev[6] = {0, 0, 0, 0, 0, 0};
-  bool converged = false, noconv = false;
-  int its = 0;
-  while (!converged && its < Maxits) {
-    its += 1;
-    MG_CUDA(cudaMemsetAsync(e.maxbuf, 0, sizeof(unsigned long long) * 18, st));
-    MG_CUDA(cudaMemsetAsync(e.kreq, 0, sizeof(int), st));
-    trt_gqd::egp_coef_kernel<<<gp, kRedBlock, 0, st>>>(e, d, G->cf);
-    MG_LAUNCHED();
-    if ((rc = G->krylov(st))) return rc;
-    trt_gqd::egp_delta_kernel<<<gp, kRedBlock, 0, st>>>(e, d, G->K.x, part);
-    MG_LAUNCHED();
-    trt_gqd::egp_norm_finish_kernel<<<1, 32, 0, st>>>(part, nblk, norms);
-    MG_LAUNCHED();
-    MG_CUDA(cudaMemcpyAsync(hn, norms, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
-    MG_CUDA(cudaMemcpyAsync(G->h_scal, G->K.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
-    MG_CUDA(cudaStreamSynchronize(st));
-    GQD_Kits[its - 1] = (G->h_scal[0].done == 1 ? 1 : -1) * (1 + 2 * G->h_scal[0].its);
-    if (G->h_scal[0].done != 1) noconv = true;
-    // line search (GLOQD_SOLVES.f08:604-636): the six quantities in order, each on the deltas as the
-    // earlier ones left them; the deltas are scaled uniformly, so one cumulative factor carries it
-    double S = 1.0;
-    double nrm[6];
-    for (int q = 0; q < 6; ++q) nrm[q] = std::sqrt(hn[q]);
-    if (Use_Line_Search && its > 1) {
-      for (int q = 0; q < 6; ++q) {
-        double LS = 1.0;
-        for (int k = 0; k < 10; ++k) {
-          if (nrm[q] / S / LS > prev[q]) LS = LS * line_src;
-          else break;
-        }
-        if (LS > 1.0) S = S * LS;
-      }
-    }
-    if (Use_Safety_Search) {
-      trt_gqd::egp_safety_kernel<<<gp, kRedBlock, 0, st>>>(e, d, G->K.x, S, line_src, T_Bound_Low, E_Bound_Low);
-      MG_LAUNCHED();
-      int kq = 0;
-      MG_CUDA(cudaMemcpyAsync(&kq, e.kreq, sizeof(int), cudaMemcpyDeviceToHost, st));
-      MG_CUDA(cudaStreamSynchronize(st));
-      for (int k = 0; k < kq; ++k) S = S * line_src;
-    }
-    trt_gqd::egp_update_kernel<<<gp, kRedBlock, 0, st>>>(e, d, G->K.x, S);
-    MG_LAUNCHED();
-    MG_CUDA(cudaMemcpyAsync(hbuf, e.maxbuf, sizeof(double) * 18, cudaMemcpyDeviceToHost, st));
-    MG_CUDA(cudaStreamSynchronize(st));
-    for (int q = 0; q < 6; ++q) prev[q] = nrm[q] / S;
-    converged = true;
-    for (int q = 0; q < 6; ++q)
-      if (hbuf[6 + q] > Eps1 * hbuf[12 + q] + Eps2) converged = false;
-    if (Res_Calc)
-      for (int q = 0; q < 6; ++q) {
-        Deltas[(its - 1) + (long)Maxits * q] = hbuf[6 + q];
-        dresiduals[(its - 1) + (long)Maxits * q] = hbuf[q];
-      }
-  }
-  *Its = its;
+  const EgpOpts opt{line_src, T_Bound_Low, E_Bound_Low, Eps1, Eps2, Maxits, Use_Line_Search, Use_Safety_Search,
+                    Res_Calc};
+  bool noconv = false;
+  if ((rc = egp_newton(G, st, e, opt, part, norms, Its, GQD_Kits, Deltas, dresiduals, &noconv))) return rc;
   if ((rc = fetch({{E_avg, C, &e.E}, {E_edgV, V, &e.EV}, {E_edgH, H, &e.EH}, {Temp, C, &e.T}, {KapE_Bar, C, &e.Kb},
                    {Fx_edgV, V, &e.Fx}, {Fy_edgH, H, &e.Fy}, {Q_bar, C, &e.Q}, {KapE_Bar_dT, C, &e.Kdt}},
                   st)))
@@ -855,3 +877,457 @@ int trt_egp_fv_newt(int n_x, int n_y, double* E_avg, double* E_edgV, double* E_e
 
 }  // extern "C"
 
+
+// ------------------------------------------------------------------------------------------------
+// The mlqd time step on the device: TRT_MLQD_ALGORITHM with run_type 'mlqd', use_grey = 1, HO_Form 0,
+// RT_start_Its 2 and Fdt/Fin/Ein weights 1 (MainSrc/ALGORITHMS.f08:294-302, 389-416, 518-572, 670-836).
+// The handle supplies the sweep, the material and the temperature; everything else lives here.
+// ------------------------------------------------------------------------------------------------
+
+namespace {
+
+struct Mlqd {
+  trt_ctx* h = nullptr;
+  trt_host::HandleView v{};
+  trt_mlqd_params p{};
+  Dims d{};
+  std::unique_ptr<Solver> MG, GR;   // multigroup system (n_g groups) and the grey Newton system
+  Arena ar;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  unsigned long long* h_conv = nullptr;   // pinned, 10 convergence values
+  // multigroup fields, Fortran layouts.  The current solution lives in MG->K.x (unknown layout) and
+  // MG->Fx / MG->Fy; Eg/EgV/EgH are its copies in the reference layout.
+  double *Eg, *EgV, *EgH, *EgO, *EgVO, *EgHO, *FxO, *FyO, *fO[6], *KapO, *Src, *SrcO;
+  double *Gold, *Pold[4];                               // G_old, Pold_L, Pold_B, Pold_R, Pold_T
+  double *EinG[4], *FinG[4];                            // Eg_in_*, Fg_in_* (n_g per boundary point)
+  // grey fields
+  double *E, *EV, *EH, *Fx, *Fy, *MGE, *MGEV, *MGEH, *MGFx, *MGFy, *Eo;
+  double *Kb, *KbO, *KbM, *Kdt, *Korg, *Q, *QO, *Gh, *Rh, *Dc[10], *Pc[4], *Cb[4], *Ein[4], *Fin[4];
+  double *Tm1, *Tm2, *Em1, *Em2, *Tr1, *Tr2, *Er1, *Er2, *Told;
+  double *drT, *W, *dT, *dFx, *dFy, *part, *norms;
+  unsigned long long *maxbuf, *conv;
+  int* kreq;
+  const double* f[6];        // the handle's fg fields (avg_xx, avg_yy, edgV_xx, edgV_xy, edgH_yy, edgH_xy)
+  const double* Cg[4];       // the handle's Cg fields
+  const double* HOE;         // the handle's transport E_avg
+  std::vector<int> mg_counts, egp_counts, kits;
+
+  ~Mlqd() {
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
+    if (h_conv) cudaFreeHost(h_conv);
+  }
+};
+
+void mlqd_release(void* p) { delete static_cast<Mlqd*>(p); }
+
+int d2d(double* dst, const double* src, size_t n, cudaStream_t st) {
+  MG_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return TRT_OK;
+}
+
+int h2d(double* dst, const std::vector<double>& src, cudaStream_t st) {
+  MG_CUDA(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  return TRT_OK;
+}
+
+// MLOQD_FV's solution in the unknown layout <-> the reference layouts (one strided copy per field).
+int unknowns_to_fields(const Mlqd& m, cudaStream_t st) {
+  const Dims& d = m.d;
+  const size_t pitch = (size_t)d.nU * sizeof(double);
+  MG_CUDA(cudaMemcpy2DAsync(m.Eg, d.nC * sizeof(double), m.MG->K.x, pitch, d.nC * sizeof(double), d.ng,
+                            cudaMemcpyDeviceToDevice, st));
+  MG_CUDA(cudaMemcpy2DAsync(m.EgV, d.nV * sizeof(double), m.MG->K.x + d.oV(), pitch, d.nV * sizeof(double), d.ng,
+                            cudaMemcpyDeviceToDevice, st));
+  MG_CUDA(cudaMemcpy2DAsync(m.EgH, d.nH * sizeof(double), m.MG->K.x + d.oH(), pitch, d.nH * sizeof(double), d.ng,
+                            cudaMemcpyDeviceToDevice, st));
+  return TRT_OK;
+}
+
+int fields_to_unknowns(const Mlqd& m, cudaStream_t st) {
+  const Dims& d = m.d;
+  const size_t pitch = (size_t)d.nU * sizeof(double);
+  MG_CUDA(cudaMemcpy2DAsync(m.MG->K.x, pitch, m.Eg, d.nC * sizeof(double), d.nC * sizeof(double), d.ng,
+                            cudaMemcpyDeviceToDevice, st));
+  MG_CUDA(cudaMemcpy2DAsync(m.MG->K.x + d.oV(), pitch, m.EgV, d.nV * sizeof(double), d.nV * sizeof(double), d.ng,
+                            cudaMemcpyDeviceToDevice, st));
+  MG_CUDA(cudaMemcpy2DAsync(m.MG->K.x + d.oH(), pitch, m.EgH, d.nH * sizeof(double), d.nH * sizeof(double), d.ng,
+                            cudaMemcpyDeviceToDevice, st));
+  return TRT_OK;
+}
+
+int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm) {
+  auto m = std::make_unique<Mlqd>();
+  int rc = trt_host::handle_view(h, &m->v);
+  if (rc) return rc;
+  const trt_host::HandleView& v = m->v;
+  m->h = h;
+  m->p = prm;
+  const int nx = v.nx, ny = v.ny, ng = v.ng;
+  m->d = dims_of(nx, ny, ng);
+  const Dims& d = m->d;
+  cudaStream_t st = v.stream;
+  m->MG = std::make_unique<Solver>();
+  if ((rc = m->MG->init(nx, ny, ng, false))) return rc;
+  m->GR = std::make_unique<Solver>();
+  if ((rc = m->GR->init(nx, ny, 1, false))) return rc;
+  const size_t C = (size_t)d.nC * ng, V = (size_t)d.nV * ng, H = (size_t)d.nH * ng;
+  const size_t c1 = d.nC, v1 = d.nV, hh1 = d.nH;
+  const size_t side[4] = {(size_t)ny, (size_t)nx, (size_t)ny, (size_t)nx};   // L, B, R, T
+  const int nblk = m->GR->pos_blocks();
+  // one arena for every field: sizes in the order they are taken below
+  std::vector<std::pair<double**, size_t>> plan = {
+      {&m->Eg, C},    {&m->EgV, V},   {&m->EgH, H},   {&m->EgO, C},   {&m->EgVO, V},  {&m->EgHO, H},
+      {&m->FxO, V},   {&m->FyO, H},   {&m->fO[0], C}, {&m->fO[1], C}, {&m->fO[2], V}, {&m->fO[3], V},
+      {&m->fO[4], H}, {&m->fO[5], H}, {&m->KapO, C},  {&m->Src, C},   {&m->SrcO, C},  {&m->Gold, C},
+      {&m->Pold[0], C}, {&m->Pold[1], C}, {&m->Pold[2], C}, {&m->Pold[3], C},
+      {&m->E, c1},    {&m->EV, v1},   {&m->EH, hh1},  {&m->Fx, v1},   {&m->Fy, hh1},  {&m->MGE, c1},
+      {&m->MGEV, v1}, {&m->MGEH, hh1}, {&m->MGFx, v1}, {&m->MGFy, hh1}, {&m->Eo, c1},  {&m->Kb, c1},
+      {&m->KbO, c1},  {&m->KbM, c1},  {&m->Kdt, c1},  {&m->Korg, c1}, {&m->Q, c1},    {&m->QO, c1},
+      {&m->Gh, c1},   {&m->Rh, c1},   {&m->Tm1, c1},  {&m->Tm2, c1},  {&m->Em1, c1},  {&m->Em2, c1},
+      {&m->Tr1, c1},  {&m->Tr2, c1},  {&m->Er1, c1},  {&m->Er2, c1},  {&m->Told, c1}, {&m->drT, c1},
+      {&m->W, c1},    {&m->dT, c1},   {&m->dFx, v1},  {&m->dFy, hh1}, {&m->part, (size_t)nblk * 6},
+      {&m->norms, 8}};
+  for (int k = 0; k < 10; ++k) plan.push_back({&m->Dc[k], c1});
+  for (int k = 0; k < 4; ++k) {
+    plan.push_back({&m->Pc[k], c1});
+    plan.push_back({&m->Cb[k], side[k]});
+    plan.push_back({&m->Ein[k], side[k]});
+    plan.push_back({&m->Fin[k], side[k]});
+    plan.push_back({&m->EinG[k], side[k] * ng});
+    plan.push_back({&m->FinG[k], side[k] * ng});
+  }
+  size_t bytes = Arena::need(18, 8) + Arena::need(8, 4) + Arena::need(10, 8);
+  for (const auto& q : plan) bytes += Arena::need(q.second, sizeof(double));
+  if ((rc = m->ar.reserve(bytes))) return rc;
+  for (const auto& q : plan) *q.first = m->ar.take<double>(q.second);
+  m->maxbuf = m->ar.take<unsigned long long>(18);
+  m->kreq = m->ar.take<int>(8);
+  m->conv = m->ar.take<unsigned long long>(10);
+  for (cudaEvent_t& e : m->ev) MG_CUDA(cudaEventCreate(&e));
+  MG_CUDA(cudaMallocHost(&m->h_conv, 10 * sizeof(unsigned long long)));
+  static const char* fnames[6] = {"fg_avg_xx", "fg_avg_yy", "fg_edgV_xx", "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy"};
+  static const char* cnames[4] = {"Cg_L", "Cg_B", "Cg_R", "Cg_T"};
+  for (int k = 0; k < 6; ++k)
+    if (!(m->f[k] = trt_device_output(h, fnames[k]))) return TRT_ERR_STATE;
+  for (int k = 0; k < 4; ++k)
+    if (!(m->Cg[k] = trt_device_output(h, cnames[k]))) return TRT_ERR_STATE;
+  if (!(m->HOE = trt_device_output(h, "E_avg"))) return TRT_ERR_STATE;
+
+  // --- initial state at Tini ---
+  const double pi = 4.0 * std::atan(1.0);
+  std::vector<double> eg(ng);
+  for (int g = 0; g < ng; ++g) eg[g] = 4.0 * pi * trt_bg_planck(Tini, v.nu[g], v.nu[g + 1], v.comp_unit) / v.c;
+  double Esum = 0.0;   // the group sum as MGQD_INIT / GQD_INIT / RT_INIT accumulate it
+  for (int g = 0; g < ng; ++g) Esum = Esum + eg[g];
+  auto per_group = [&](size_t plane) {
+    std::vector<double> x(plane * ng);
+    for (int g = 0; g < ng; ++g) std::fill(x.begin() + plane * g, x.begin() + plane * (g + 1), eg[g]);
+    return x;
+  };
+  if ((rc = h2d(m->Eg, per_group(d.nC), st)) || (rc = h2d(m->EgV, per_group(d.nV), st)) ||
+      (rc = h2d(m->EgH, per_group(d.nH), st)))
+    return rc;
+  if ((rc = fields_to_unknowns(*m, st))) return rc;
+  MG_CUDA(cudaMemsetAsync(m->MG->Fx, 0, V * sizeof(double), st));
+  MG_CUDA(cudaMemsetAsync(m->MG->Fy, 0, H * sizeof(double), st));
+  // QD factors of an isotropic field and the vacuum / reflective boundary factors (MGQD_INIT)
+  const double third = 1.0 / 3.0;
+  const size_t fsz[6] = {C, C, V, V, H, H};
+  const double fval[6] = {third, third, third, 0.0, third, 0.0};
+  for (int k = 0; k < 6; ++k)
+    if ((rc = h2d(const_cast<double*>(m->f[k]), std::vector<double>(fsz[k], fval[k]), st))) return rc;
+  const double cval[4] = {-0.5, -0.5, 0.5, 0.5};
+  for (int k = 0; k < 4; ++k) {
+    const double cv0 = v.bc[k] == 0 ? cval[k] : 0.0;
+    if ((rc = h2d(const_cast<double*>(m->Cg[k]), std::vector<double>(side[k] * ng, cv0), st))) return rc;
+    if ((rc = h2d(m->Cb[k], std::vector<double>(side[k], cv0), st))) return rc;
+  }
+  // transport E of RT_INIT
+  if ((rc = h2d(const_cast<double*>(m->HOE), std::vector<double>(c1, Esum), st))) return rc;
+  // grey E, F of GQD_INIT
+  if ((rc = h2d(m->E, std::vector<double>(c1, Esum), st)) || (rc = h2d(m->EV, std::vector<double>(v1, Esum), st)) ||
+      (rc = h2d(m->EH, std::vector<double>(hh1, Esum), st)))
+    return rc;
+  MG_CUDA(cudaMemsetAsync(m->Fx, 0, v1 * sizeof(double), st));
+  MG_CUDA(cudaMemsetAsync(m->Fy, 0, hh1 * sizeof(double), st));
+  for (double* z : {m->Kb, m->Q, m->Kdt})
+    MG_CUDA(cudaMemsetAsync(z, 0, c1 * sizeof(double), st));
+  // MGQD_In_Calc (MLOQD_SOLVES.f08:493-614) on the inflow faces that RT_INIT's RT_BC_UPDATE leaves at
+  // Bg(bcT of the side); reflective sides have none.  These faces keep those values at every later
+  // RT_BC_UPDATE, so the incoming E and F never change.  GQD_In_Calc (GLOQD_SOLVES.f08:263-290) sums
+  // them over groups.
+  const int nm = v.nm;
+  const int range[4][4] = {{0, nm / 4, 3 * nm / 4, nm},   // L: Omega_x > 0
+                           {0, nm / 2, 0, 0},             // B: Omega_y > 0
+                           {nm / 4, 3 * nm / 4, 0, 0},    // R: Omega_x < 0
+                           {nm / 2, nm, 0, 0}};           // T: Omega_y < 0
+  for (int s = 0; s < 4; ++s) {
+    std::vector<double> Eg_in(side[s] * ng, 0.0), Fg_in(side[s] * ng, 0.0), E_in(side[s], 0.0), F_in(side[s], 0.0);
+    for (int g = 0; g < ng; ++g) {
+      const double I = v.bc[s] == 0 ? trt_bg_planck(v.Tb[s], v.nu[g], v.nu[g + 1], v.comp_unit) : 0.0;
+      for (size_t i = 0; i < side[s] && v.bc[s] == 0; ++i) {
+        double e = 0.0, f = 0.0;
+        for (int r = 0; r < 2; ++r)
+          for (int mm = range[s][2 * r]; mm < range[s][2 * r + 1]; ++mm) {
+            const double om = (s == 0 || s == 2) ? v.omx[mm] : v.omy[mm];
+            f = f + om * v.w[mm] * I;
+            e = e + v.w[mm] * I;
+          }
+        Fg_in[i + side[s] * g] = f;
+        Eg_in[i + side[s] * g] = e / v.c;
+      }
+    }
+    for (size_t i = 0; i < side[s]; ++i)
+      for (int g = 0; g < ng; ++g) {
+        E_in[i] = E_in[i] + Eg_in[i + side[s] * g];
+        F_in[i] = F_in[i] + Fg_in[i + side[s] * g];
+      }
+    if ((rc = h2d(m->EinG[s], Eg_in, st)) || (rc = h2d(m->FinG[s], Fg_in, st)) || (rc = h2d(m->Ein[s], E_in, st)) ||
+        (rc = h2d(m->Fin[s], F_in, st)))
+      return rc;
+  }
+  // the material of TEMP_INIT with the low-order source
+  if ((rc = trt_host::handle_material(h, m->Src))) return rc;
+  // MLOQD_FV's inputs point at the live fields
+  Inputs& in = m->MG->in;
+  in.fxx = m->f[0]; in.fyy = m->f[1]; in.fVxx = m->f[2]; in.fVxy = m->f[3]; in.fHyy = m->f[4]; in.fHxy = m->f[5];
+  in.CgL = m->Cg[0]; in.CgB = m->Cg[1]; in.CgR = m->Cg[2]; in.CgT = m->Cg[3];
+  in.EinL = m->EinG[0]; in.EinB = m->EinG[1]; in.EinR = m->EinG[2]; in.EinT = m->EinG[3];
+  in.FinL = m->FinG[0]; in.FinB = m->FinG[1]; in.FinR = m->FinG[2]; in.FinT = m->FinG[3];
+  in.Src = m->Src; in.KapE = v.kap64; in.KapR = v.kap64; in.Delx = v.dx; in.Dely = v.dy; in.A = v.area;
+  in.Gold = m->Gold; in.PoldL = m->Pold[0]; in.PoldB = m->Pold[1]; in.PoldR = m->Pold[2]; in.PoldT = m->Pold[3];
+  in.Eold = m->EgO; in.Fxold = m->FxO; in.Fyold = m->FyO;
+  in.c = v.c; in.Delt = v.dt; in.Theta = prm.theta; in.Fdt = 1.0; in.Fin = 1.0; in.Ein = 1.0;
+  MG_CUDA(cudaStreamSynchronize(st));
+  trt_host::handle_attach(h, m.release(), mlqd_release);
+  return TRT_OK;
+}
+
+// Convergence data of (x vs xo, xo2) and (y vs yo, yo2) to the host; CONVERGENCE of both.
+int conv_pair(Mlqd& m, const double* x, const double* xo, const double* xo2, const double* y, const double* yo,
+              const double* yo2, double eps, int its, double* xn, double* yn, bool* both) {
+  const long long n = m.d.nC;
+  int rc;
+  if ((rc = trt_host::handle_conv_reduce(m.h, n, x, xo, xo2, m.conv))) return rc;
+  if ((rc = trt_host::handle_conv_reduce(m.h, n, y, yo, yo2, m.conv + 5))) return rc;
+  MG_CUDA(cudaMemcpyAsync(m.h_conv, m.conv, 10 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, m.v.stream));
+  MG_CUDA(cudaStreamSynchronize(m.v.stream));
+  double r[10];
+  std::memcpy(r, m.h_conv, sizeof(r));
+  const bool a = trt_host::handle_convergence(m.v.conv_type, eps, r, its, xn);
+  const bool b = trt_host::handle_convergence(m.v.conv_type, eps, r + 5, its, yn);
+  *both = a && b;
+  return TRT_OK;
+}
+
+int mlqd_step_impl(Mlqd& m, trt_mlqd_stats* out) {
+  const trt_host::HandleView& v = m.v;
+  const Dims& d = m.d;
+  const int ng = d.ng;
+  cudaStream_t st = v.stream;
+  const size_t C = (size_t)d.nC * ng, V = (size_t)d.nV * ng, H = (size_t)d.nH * ng;
+  const size_t c1 = d.nC, v1 = d.nV, hh1 = d.nH;
+  const double Theta = m.p.theta;
+  int rc;
+  trt_mlqd_stats S{};
+  m.mg_counts.clear();
+  m.egp_counts.clear();
+  m.kits.assign((size_t)std::max(m.p.maxit_gloqd, 1), 0);
+  MG_CUDA(cudaEventRecord(m.ev[0], st));
+  // last time step's data -> _old (ALGORITHMS.f08:395-413)
+  const size_t fsz[6] = {C, C, V, V, H, H};
+  if ((rc = d2d(m.Told, v.T, c1, st)) || (rc = d2d(m.EgO, m.Eg, C, st)) || (rc = d2d(m.EgVO, m.EgV, V, st)) ||
+      (rc = d2d(m.EgHO, m.EgH, H, st)) || (rc = d2d(m.FxO, m.MG->Fx, V, st)) || (rc = d2d(m.FyO, m.MG->Fy, H, st)) ||
+      (rc = d2d(m.KapO, v.kap64, C, st)) || (rc = d2d(m.SrcO, m.Src, C, st)) || (rc = d2d(m.Eo, m.E, c1, st)) ||
+      (rc = d2d(m.KbO, m.Kb, c1, st)) || (rc = d2d(m.QO, m.Q, c1, st)))
+    return rc;
+  for (int k = 0; k < 6; ++k)
+    if ((rc = d2d(m.fO[k], m.f[k], fsz[k], st))) return rc;
+  // OLD_MGQD_COEFS (KapR_old = KapE_old: MATERIAL_UPDATE sets both to KapB) and OLD_GREY_COEFS
+  const OldIn oi{m.EgO, m.EgVO, m.EgHO, m.FxO, m.FyO, m.fO[0], m.fO[1], m.fO[2], m.fO[3], m.fO[4], m.fO[5],
+                 m.KapO, m.KapO, m.SrcO, v.dx, v.dy, v.area, v.c, Theta};
+  const OldOut oo{m.Gold, m.Pold[0], m.Pold[1], m.Pold[2], m.Pold[3]};
+  old_coefs_kernel<<<dim3(grid1(d.nC), ng), 256, 0, st>>>(oi, d, oo);
+  MG_LAUNCHED();
+  trt_gqd::old_grey_kernel<<<grid1(d.nC), 256, 0, st>>>(d, v.c, v.dt, Theta, 0.0, v.area, m.Gold, m.Told, m.KbO, m.Eo,
+                                                        m.QO, m.Gh, m.Rh, v.cv);
+  MG_LAUNCHED();
+  for (double* z : {m.Tr1, m.Tr2, m.Er1, m.Er2}) MG_CUDA(cudaMemsetAsync(z, 0, c1 * sizeof(double), st));
+
+  // grey Newton state: the grey fields, the handle's temperature, this step's coefficients
+  trt_gqd::Egp e{};
+  e.nx = d.nx;
+  e.ny = d.ny;
+  e.E = m.E; e.EV = m.EV; e.EH = m.EH; e.T = v.T; e.Kb = m.Kb; e.Fx = m.Fx; e.Fy = m.Fy; e.Q = m.Q;
+  e.Kdt = m.Kdt; e.Korg = m.Korg;
+  e.Kbm = m.KbM; e.Delx = v.dx; e.Dely = v.dy; e.A = v.area;
+  e.CbL = m.Cb[0]; e.CbB = m.Cb[1]; e.CbR = m.Cb[2]; e.CbT = m.Cb[3];
+  e.EinL = m.Ein[0]; e.EinB = m.Ein[1]; e.EinR = m.Ein[2]; e.EinT = m.Ein[3];
+  e.FinL = m.Fin[0]; e.FinB = m.Fin[1]; e.FinR = m.Fin[2]; e.FinT = m.Fin[3];
+  e.DCxx = m.Dc[0]; e.DLxx = m.Dc[1]; e.DRxx = m.Dc[2]; e.DCyy = m.Dc[3]; e.DByy = m.Dc[4]; e.DTyy = m.Dc[5];
+  e.DLxy = m.Dc[6]; e.DRxy = m.Dc[7]; e.DBxy = m.Dc[8]; e.DTxy = m.Dc[9];
+  e.PL = m.Pc[0]; e.PR = m.Pc[1]; e.PB = m.Pc[2]; e.PT = m.Pc[3];
+  e.Gh = m.Gh; e.Rh = m.Rh;
+  e.drT = m.drT; e.W = m.W; e.dT = m.dT; e.dFx = m.dFx; e.dFy = m.dFy; e.maxbuf = m.maxbuf; e.kreq = m.kreq;
+  {
+    const double hP = 6.62613e-19, cL = 2.99792458e2, pi = 4.0 * std::atan(1.0), erg = 6.24150934e11;
+    const double sig_R = 2.0 * std::pow(pi, 5) / (15.0 * (cL * cL) * (hP * hP * hP) * std::pow(erg, 4) * v.comp_unit);
+    e.aR = 4.0 * sig_R / cL;
+  }
+  e.Theta = Theta; e.Delt = v.dt; e.Kap0 = v.Kap0; e.cv = 0.0; e.cvc = v.cv; e.Chi = m.p.chi;
+  e.Fin = 1.0; e.Ein = 1.0;
+  const EgpOpts eo{m.p.line_src, m.p.T_bound_low, m.p.E_bound_low, m.p.conv_gr1, m.p.conv_gr2, m.p.maxit_gloqd,
+                   m.p.use_line_search, m.p.use_safety_search, 0};
+
+  float sweep_ms = 0.f;
+  int rt = 0;
+  bool rt_conv = false;
+  double tn = 0.0, en = 0.0;
+  while (!rt_conv && rt < v.maxit_rte) {
+    ++rt;
+    if (rt >= 2) {   // RT_start_Its = 2
+      MG_CUDA(cudaEventRecord(m.ev[2], st));
+      if ((rc = trt_host::handle_outer_sweep(m.h, rt == 2))) return rc;
+      MG_CUDA(cudaEventRecord(m.ev[3], st));
+      ++S.sweeps;
+    }
+    // MGQD iterations (:675-810)
+    if ((rc = d2d(m.Em1, m.HOE, c1, st)) || (rc = d2d(m.Tm1, v.T, c1, st))) return rc;
+    MG_CUDA(cudaMemsetAsync(m.Em2, 0, c1 * sizeof(double), st));
+    MG_CUDA(cudaMemsetAsync(m.Tm2, 0, c1 * sizeof(double), st));
+    int mg = 0;
+    bool mg_conv = false;
+    while (!mg_conv && mg < m.p.maxit_mloqd) {
+      ++mg;
+      if ((rc = m.MG->solve(st))) return rc;   // MLOQD_FV from the previous solution
+      MG_CUDA(cudaMemcpyAsync(m.MG->h_scal, m.MG->K.sc, sizeof(Scal) * ng, cudaMemcpyDeviceToHost, st));
+      if ((rc = unknowns_to_fields(m, st))) return rc;
+      trt_gqd::collapse_kernel<<<grid1(d.npos()), 256, 0, st>>>(d, m.Eg, m.EgV, m.EgH, m.MG->Fx, m.MG->Fy, m.MGE,
+                                                                m.MGEV, m.MGEH, m.MGFx, m.MGFy);
+      MG_LAUNCHED();
+      const trt_gqd::CbarArgs ca{m.Cg[0], m.Cg[1], m.Cg[2], m.Cg[3], m.EgV, m.EgH, m.EinG[0], m.EinG[1], m.EinG[2],
+                                 m.EinG[3], m.Cb[0], m.Cb[1], m.Cb[2], m.Cb[3]};
+      trt_gqd::cbar_kernel<<<grid1(d.nx + d.ny), 256, 0, st>>>(d, ca);
+      MG_LAUNCHED();
+      if ((rc = d2d(m.KbM, m.Kb, c1, st))) return rc;   // KapE_bar_MGQDold = KapE_bar
+      trt_gqd::GreyIn gi{};
+      gi.Eg = m.Eg; gi.EgV = m.EgV; gi.EgH = m.EgH; gi.FxOld = m.FxO; gi.FyOld = m.FyO;
+      gi.fxx = m.f[0]; gi.fyy = m.f[1]; gi.fVxx = m.f[2]; gi.fVxy = m.f[3]; gi.fHyy = m.f[4]; gi.fHxy = m.f[5];
+      gi.KapE = v.kap64; gi.KapR = v.kap64; gi.A = v.area;
+      gi.PoldL = m.Pold[0]; gi.PoldR = m.Pold[2]; gi.PoldB = m.Pold[1]; gi.PoldT = m.Pold[3];
+      gi.c = v.c; gi.Delt = v.dt; gi.Theta = Theta; gi.Fdt = 1.0;
+      const trt_gqd::GreyOut go{m.Kb,    m.Dc[0], m.Dc[1], m.Dc[2], m.Dc[3], m.Dc[4], m.Dc[5], m.Dc[6],
+                                m.Dc[7], m.Dc[8], m.Dc[9], m.Pc[0], m.Pc[1], m.Pc[2], m.Pc[3]};
+      trt_gqd::grey_coefs_kernel<<<grid1(d.nC), 256, 0, st>>>(d, gi, go);
+      MG_LAUNCHED();
+      if ((rc = d2d(m.E, m.MGE, c1, st)) || (rc = d2d(m.EV, m.MGEV, v1, st)) || (rc = d2d(m.EH, m.MGEH, hh1, st)) ||
+          (rc = d2d(m.Fx, m.MGFx, v1, st)) || (rc = d2d(m.Fy, m.MGFy, hh1, st)))
+        return rc;
+      e.Tm = m.Tm2;   // Temp_MGQDold2
+      e.damp = (mg > 1 && m.p.kapE_dT_flag) ? 1 : 0;
+      int its = 0;
+      bool noconv = false;
+      if ((rc = egp_newton(m.GR.get(), st, e, eo, m.part, m.norms, &its, m.kits.data(), nullptr, nullptr, &noconv)))
+        return rc;
+      for (int g = 0; g < ng; ++g)   // h_scal was read before the Newton iteration's synchronisations
+        if (m.MG->h_scal[g].done != 1) ++S.mgqd_nonconv;
+      for (int k = 0; k < its; ++k)
+        if (m.kits[k] < 0) ++S.egp_nonconv;
+      m.egp_counts.push_back(its);
+      S.egp_its += its;
+      if ((rc = trt_host::handle_material(m.h, m.Src))) return rc;   // MATERIAL_UPDATE(Temp)
+      double a = 0.0, b = 0.0;
+      if ((rc = conv_pair(m, v.T, m.Tm1, m.Tm2, m.MGE, m.Em1, m.Em2, m.p.conv_lo, mg, &a, &b, &mg_conv))) return rc;
+      std::swap(m.Em1, m.Em2);
+      std::swap(m.Tm1, m.Tm2);
+      if ((rc = d2d(m.Em1, m.MGE, c1, st)) || (rc = d2d(m.Tm1, v.T, c1, st))) return rc;
+    }
+    m.mg_counts.push_back(mg);
+    S.mgqd_its += mg;
+    if (rt >= 2) {
+      float ms = 0.f;
+      MG_CUDA(cudaEventElapsedTime(&ms, m.ev[2], m.ev[3]));
+      sweep_ms += ms;
+    }
+    if ((rc = conv_pair(m, v.T, m.Tr1, m.Tr2, m.HOE, m.Er1, m.Er2, v.conv_ho, rt, &tn, &en, &rt_conv))) return rc;
+    std::swap(m.Er1, m.Er2);
+    std::swap(m.Tr1, m.Tr2);
+    if ((rc = d2d(m.Er1, m.HOE, c1, st)) || (rc = d2d(m.Tr1, v.T, c1, st))) return rc;
+  }
+  MG_CUDA(cudaEventRecord(m.ev[1], st));
+  if ((rc = trt_host::handle_check(m.h))) return rc;
+  float total = 0.f;
+  MG_CUDA(cudaEventElapsedTime(&total, m.ev[0], m.ev[1]));
+  S.rt_its = rt;
+  S.T_norm = tn;
+  S.E_norm = en;
+  S.sweep_ms = sweep_ms;
+  S.low_order_ms = total - sweep_ms;
+  if (out) *out = S;
+  return (S.mgqd_nonconv || S.egp_nonconv) ? TRT_ERR_NOCONV : TRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trt_mlqd_setup(trt_ctx* ctx, double Tini, const trt_mlqd_params* p) {
+  if (!ctx || !p || !(Tini >= 0.0) || p->maxit_mloqd < 1 || p->maxit_gloqd < 1 || !(p->conv_lo >= 0.0) ||
+      !(p->conv_gr1 >= 0.0) || !(p->conv_gr2 >= 0.0) || !(p->theta > 0.0) ||
+      ((p->use_line_search || p->use_safety_search) && !(p->line_src > 1.0)))
+    return TRT_ERR_ARG;
+  int rc = device_ok();
+  if (rc) return rc;
+  return mlqd_setup_impl(ctx, Tini, *p);
+}
+
+int trt_mlqd_step(trt_ctx* ctx, trt_mlqd_stats* stats) {
+  if (!ctx) return TRT_ERR_ARG;
+  Mlqd* m = static_cast<Mlqd*>(trt_host::handle_attached(ctx));
+  if (!m) return TRT_ERR_STATE;
+  return mlqd_step_impl(*m, stats);
+}
+
+int trt_mlqd_counts(trt_ctx* ctx, int* mgqd_per_outer, int cap_outer, int* egp_per_mgqd, int cap_mgqd, int* n_outer,
+                    int* n_mgqd) {
+  if (!ctx) return TRT_ERR_ARG;
+  const Mlqd* m = static_cast<const Mlqd*>(trt_host::handle_attached(ctx));
+  if (!m) return TRT_ERR_STATE;
+  for (int k = 0; k < cap_outer && k < (int)m->mg_counts.size() && mgqd_per_outer; ++k)
+    mgqd_per_outer[k] = m->mg_counts[k];
+  for (int k = 0; k < cap_mgqd && k < (int)m->egp_counts.size() && egp_per_mgqd; ++k)
+    egp_per_mgqd[k] = m->egp_counts[k];
+  if (n_outer) *n_outer = (int)m->mg_counts.size();
+  if (n_mgqd) *n_mgqd = (int)m->egp_counts.size();
+  return TRT_OK;
+}
+
+int trt_mlqd_get(trt_ctx* ctx, const char* name, double* host, long long count) {
+  if (!ctx || !name || !host) return TRT_ERR_ARG;
+  Mlqd* m = static_cast<Mlqd*>(trt_host::handle_attached(ctx));
+  if (!m) return TRT_ERR_STATE;
+  const Dims& d = m->d;
+  const long long ng = d.ng, C = d.nC, V = d.nV, H = d.nH, nx = d.nx, ny = d.ny;
+  const struct {
+    const char* n;
+    const double* p;
+    long long sz;
+  } tab[] = {{"Temp", m->v.T, C},          {"E_avg", m->E, C},          {"E_edgV", m->EV, V},
+             {"E_edgH", m->EH, H},         {"Fx_edgV", m->Fx, V},       {"Fy_edgH", m->Fy, H},
+             {"KapE_Bar", m->Kb, C},       {"KapE_Bar_dT", m->Kdt, C},  {"GQD_Src", m->Q, C},
+             {"Cb_L", m->Cb[0], ny},       {"Cb_B", m->Cb[1], nx},      {"Cb_R", m->Cb[2], ny},
+             {"Cb_T", m->Cb[3], nx},       {"Eg_avg", m->Eg, C * ng},   {"Eg_edgV", m->EgV, V * ng},
+             {"Eg_edgH", m->EgH, H * ng},  {"Fxg_edgV", m->MG->Fx, V * ng}, {"Fyg_edgH", m->MG->Fy, H * ng},
+             {"MGQD_Src", m->Src, C * ng}, {"MGQD_E_avg", m->MGE, C}, {"HO_E_avg", m->HOE, C}};
+  for (const auto& t : tab)
+    if (std::strcmp(t.n, name) == 0) {
+      if (count < t.sz) return TRT_ERR_ARG;
+      MG_CUDA(cudaMemcpyAsync(host, t.p, (size_t)t.sz * sizeof(double), cudaMemcpyDeviceToHost, m->v.stream));
+      MG_CUDA(cudaStreamSynchronize(m->v.stream));
+      return TRT_OK;
+    }
+  return TRT_ERR_ARG;
+}
+
+}  // extern "C"

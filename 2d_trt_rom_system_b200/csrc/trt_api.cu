@@ -12,6 +12,7 @@
 
 #include "trt_sweep.h"
 #include "aux_kernels.cuh"
+#include "handle_hooks.h"
 #include "dropin_kernels.cuh"
 #include "sweep_kernel.cuh"
 #include "tstep_kernels.cuh"
@@ -261,6 +262,9 @@ struct trt_ctx {
   double ts_Kap0 = 0.0, ts_conv_ho = 0.0, ts_Tb[4] = {0, 0, 0, 0};
   int ts_conv_type = 1, ts_maxit = 1, ts_bc[4] = {0, 0, 0, 0};
   std::vector<double> ts_nu;
+  // low-order (mlqd) state attached by the MGQD side of the library, released with the handle
+  void* lo = nullptr;
+  void (*lo_free)(void*) = nullptr;
 
   size_t esz() const { return prec == TRT_PREC_FP64 ? sizeof(double) : sizeof(float); }
   long long state_elems() const { return 4LL * ng * t.NH * blk; }
@@ -980,11 +984,11 @@ struct DBuf {
 
 // MATERIAL_UPDATE (UPDATES.f08:110-152) from the device temperature into the sweep's material.
 template <class Real>
-int material_update_impl(trt_ctx* c) {
+int material_update_impl(trt_ctx* c, double* mgsrc = nullptr) {
   const long long n = (long long)c->nx * c->ny * c->ng;
   trt::material_update_kernel<Real><<<grid_for(n), 256, 0, c->stream>>>(
       c->nx, c->ny, c->ng, c->d_T, c->d_nu, c->d_kmult, c->comp_unit, c->d_kap64, c->d_q64, (Real*)c->d_kap,
-      (Real*)c->d_q);
+      (Real*)c->d_q, mgsrc);
   TRT_LAUNCHED();
   TRT_CUDA(cudaGetLastError());
   c->use_srcfull = false;
@@ -1513,6 +1517,7 @@ trt_ctx* trt_create(int n_x, int n_y, int n_m, int n_g, const double* Omega_x, c
 void trt_destroy(trt_ctx* c) {
   if (!c) return;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->lo && c->lo_free) c->lo_free(c->lo);
   for (void* p : c->allocs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -2214,4 +2219,90 @@ extern "C" int trt_transport_residual_noalloc(int n_x, int n_y, int n_m, int n_g
 namespace trt_host {
 // launch counter shared with the other translation units of the library
 void add_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace trt_host
+
+// ---------------------------------------------------------------------------------------------
+// Hooks for the low-order time loop of mgqd.cu (handle_hooks.h).
+// ---------------------------------------------------------------------------------------------
+namespace trt_host {
+
+int handle_view(trt_ctx* c, HandleView* v) {
+  if (!c || !v) return TRT_ERR_ARG;
+  if (!c->ts_ready) return TRT_ERR_STATE;
+  v->nx = c->nx;
+  v->ny = c->ny;
+  v->nm = c->nm;
+  v->ng = c->ng;
+  v->prec = c->prec;
+  for (int k = 0; k < 4; ++k) {
+    v->bc[k] = c->ts_bc[k];
+    v->Tb[k] = c->ts_Tb[k];
+  }
+  v->c = c->c;
+  v->dt = c->dt;
+  v->comp_unit = c->comp_unit;
+  v->Kap0 = c->ts_Kap0;
+  v->conv_type = c->ts_conv_type;
+  v->maxit_rte = c->ts_maxit;
+  v->conv_ho = c->ts_conv_ho;
+  v->stream = c->stream;
+  v->dx = c->d_dx;
+  v->dy = c->d_dy;
+  v->area = c->d_area;
+  v->T = c->d_T;
+  v->kap64 = c->d_kap64;
+  v->omx = c->omx.data();
+  v->omy = c->omy.data();
+  v->w = c->w.data();
+  v->nu = c->ts_nu.data();
+  v->cv = c->d_cv;
+  return TRT_OK;
+}
+
+int handle_outer_sweep(trt_ctx* c, bool roll) {
+  const unsigned flags = (roll ? TRT_ROLL_STATE : 0u) | TRT_MOMENTS;
+  const bool reflective = c->ts_bc[0] > 0 || c->ts_bc[1] > 0 || c->ts_bc[2] > 0 || c->ts_bc[3] > 0;
+  int rc;
+  if (c->prec == TRT_PREC_FP64) {
+    if ((rc = sweep_impl<double>(c, flags))) return rc;
+    if (reflective && (rc = bc_update_impl<double>(c, c->ts_bc, c->ts_Tb, c->comp_unit, c->ts_nu.data()))) return rc;
+  } else {
+    if ((rc = sweep_impl<float>(c, flags))) return rc;
+    if (reflective && (rc = bc_update_impl<float>(c, c->ts_bc, c->ts_Tb, c->comp_unit, c->ts_nu.data()))) return rc;
+  }
+  c->have_moments = true;
+  return TRT_OK;
+}
+
+int handle_material(trt_ctx* c, double* mgsrc) {
+  return c->prec == TRT_PREC_FP64 ? material_update_impl<double>(c, mgsrc) : material_update_impl<float>(c, mgsrc);
+}
+
+int handle_conv_reduce(trt_ctx* c, long long n, const double* x, const double* xo, const double* xo2,
+                       unsigned long long* dev_out) {
+  static const unsigned long long init[5] = {0, 0, 0, 0x7ff0000000000000ULL, 0};
+  TRT_CUDA(cudaMemcpyAsync(dev_out, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+  trt::conv_reduce_kernel<<<grid_for(n), 256, 0, c->stream>>>(n, x, xo, xo2, dev_out);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  return TRT_OK;
+}
+
+bool handle_convergence(int conv_type, double eps, const double* r, int its, double* norm) {
+  return convergence(conv_type, eps, r, its, norm);
+}
+
+int handle_check(trt_ctx* c) { return check_err(c); }
+
+void handle_attach(trt_ctx* c, void* obj, void (*release)(void*)) {
+  if (c->lo && c->lo_free) {
+    cudaStreamSynchronize(c->stream);
+    c->lo_free(c->lo);
+  }
+  c->lo = obj;
+  c->lo_free = release;
+}
+
+void* handle_attached(trt_ctx* c) { return c->lo; }
+
 }  // namespace trt_host

@@ -57,12 +57,13 @@ __device__ __forceinline__ double ts_kapb(double T, double nu_low, double nu_hig
 // MATERIAL_UPDATE (UPDATES.f08:110-152) for the sweep: KapE = KapB = kapB_calc(T, nu_g, nu_g+1) *
 // Kappa_Mult(Mat(i,j)) and the isotropic corner source RT_Src = KapB * Bg, one value per (cell, g)
 // (the reference stores it for all 4 corners and N_m directions).  kmult(i,j) = Kappa_Mult(Mat(i,j)).
-// Writes the FP64 copies and the sweep's Real copies.
+// Writes the FP64 copies and the sweep's Real copies; with mgsrc set, also the low-order source
+// MGQD_Src = 4 pi KapB Bg (UPDATES.f08:141).
 template <class Real>
 __global__ void material_update_kernel(int nx, int ny, int ng, const double* __restrict__ T,
                                        const double* __restrict__ nu, const double* __restrict__ kmult,
                                        double comp_unit, double* __restrict__ kap64, double* __restrict__ q64,
-                                       Real* __restrict__ kap, Real* __restrict__ q) {
+                                       Real* __restrict__ kap, Real* __restrict__ q, double* __restrict__ mgsrc) {
   const long long nxy = (long long)nx * ny, n = nxy * ng;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
     const long long cell = k % nxy;
@@ -75,6 +76,7 @@ __global__ void material_update_kernel(int nx, int ny, int ng, const double* __r
     q64[k] = src;
     kap[k] = (Real)kB;
     q[k] = (Real)src;
+    if (mgsrc) mgsrc[k] = ((4.0 * 3.141592653589793) * kB) * Bg;
   }
 }
 

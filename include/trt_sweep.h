@@ -362,6 +362,54 @@ int trt_get_temperature(trt_ctx* ctx, double* Temp);
 /* Replace the device temperature and recompute the material from it (MATERIAL_UPDATE). */
 int trt_put_temperature(trt_ctx* ctx, const double* Temp);
 
+/* ---- The mlqd time step on the device (the reference's run_type 'mlqd', use_grey = 1) -------------
+ * Replaces, for one handle, the time loop of TRT_MLQD_ALGORITHM with HO_Form 0, RT_start_Its 2 and
+ * Fdt/Fin/Ein weights 1 (MainSrc/ALGORITHMS.f08:294-302, 389-416, 518-572, 670-836).  Per time step:
+ * the _old copies (:395-413), OLD_MGQD_COEFS and OLD_GREY_COEFS, then outer iterations, each (from the
+ * second on) one sweep with the fused COLLAPSE_INTENSITIES, fg_Calc and Cg_Calc (RT_BC_UPDATE on reflective
+ * sides), followed by MGQD iterations of
+ *   MLOQD_FV                (the device BiCGSTAB + multigrid solve of trt_mloqd_fv, FP64),
+ *   COLLAPSE_MG_EF, Cbar_Calc, GREY_COEFS,
+ *   EGP_FV_NEWT             (the Newton iteration of trt_egp_fv_newt, FP64),
+ *   MATERIAL_UPDATE and CONVERGENCE(conv_lo) on T and the MGQD E,
+ * and CONVERGENCE(conv_ho) on T and the transport E.  The sweep runs in the handle's precision; every
+ * low-order field, the material and the convergence data are FP64 and stay on the device.
+ * Call order: trt_create -> trt_init_state (RT_INIT) -> trt_tstep_setup (material model, Temp, Delt,
+ * BC_Type, bcT, conv_type, conv_ho, maxit_rte) -> trt_mlqd_setup -> trt_mlqd_step per time step.
+ * trt_mlqd_setup sets the initial low-order state of MGQD_INIT and GQD_INIT (INITIALIZERS.f08:159-427)
+ * at Tini; KapE_Bar and GQD_Src, which the reference leaves unset, start at zero.  The heat capacity is
+ * the per-cell cV of trt_tstep_setup (the reference's scalar cv broadcast). */
+typedef struct trt_mlqd_params {
+  double conv_lo;              /* MGQD-iteration tolerance */
+  double conv_gr1, conv_gr2;   /* EGP Newton tolerances (Eps1 relative, Eps2 absolute) */
+  int maxit_mloqd, maxit_gloqd;
+  double chi, line_src;        /* KapE_Bar_dT bound factor; line-search factor (> 1) */
+  double E_bound_low, T_bound_low;
+  int use_line_search, use_safety_search, kapE_dT_flag;
+  double theta;                /* time-integration weight (1 = backward Euler) */
+} trt_mlqd_params;
+typedef struct trt_mlqd_stats {
+  int rt_its;          /* outer iterations of the step */
+  int sweeps;          /* sweeps run (the first outer iteration of a step has none) */
+  int mgqd_its;        /* MGQD iterations, summed over the outer iterations */
+  int egp_its;         /* EGP Newton iterations, summed over the MGQD iterations */
+  int mgqd_nonconv;    /* group solves of MLOQD_FV that stopped at the iteration limit */
+  int egp_nonconv;     /* Newton linear solves that stopped at the iteration limit */
+  double T_norm, E_norm;   /* norms of the last outer iteration */
+  double sweep_ms, low_order_ms;   /* device time of the sweeps and of everything else in the step */
+} trt_mlqd_stats;
+int trt_mlqd_setup(trt_ctx* ctx, double Tini, const trt_mlqd_params* params);
+int trt_mlqd_step(trt_ctx* ctx, trt_mlqd_stats* stats);
+/* Iteration counts of the last step: MGQD iterations of each outer iteration (n_outer values) and EGP
+ * iterations of each MGQD iteration (n_mgqd values), each copied up to its capacity. */
+int trt_mlqd_counts(trt_ctx* ctx, int* mgqd_per_outer, int cap_outer, int* egp_per_mgqd, int cap_mgqd,
+                    int* n_outer, int* n_mgqd);
+/* Copy a device field of the mlqd state to host memory, Fortran layout: "Temp", the grey "E_avg",
+ * "E_edgV", "E_edgH", "Fx_edgV", "Fy_edgH", "KapE_Bar", "KapE_Bar_dT", "GQD_Src", "Cb_L/B/R/T", the
+ * multigroup "Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH", "MGQD_Src", "MGQD_E_avg", and the
+ * transport "HO_E_avg".  `count` is the number of doubles the caller provides (checked). */
+int trt_mlqd_get(trt_ctx* ctx, const char* name, double* host, long long count);
+
 /* ---- Batched instances ---------------------------------------------------------------------------
  * Many independent handles (different grids, groups, quadratures, precisions) stepped together: the
  * sweeps of all handles that share a tiling class (precision, slices, directions per lane, warps per

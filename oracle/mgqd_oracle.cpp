@@ -811,19 +811,29 @@ int oracle_cbar_calc(int nx, int ny, int ng, double* Cb_L, double* Cb_B, double*
 }
 
 // OLD_GREY_COEFS (GLOQD_SOLVES.f08:12-42).
-int oracle_old_grey_coefs(int nx, int ny, int ng, double c, double Delt, double Theta, double cv, const double* A,
-                          const double* Gold, const double* Temp_old, const double* KapE_bar_old,
-                          const double* E_avg_old, const double* GQD_Src_old, double* Gold_Hat, double* Rhat_old) {
+// cv_cells: heat capacity per cell (the reference passes one value, cv; nullptr means that value).
+int oracle_old_grey_coefs_cells(int nx, int ny, int ng, double c, double Delt, double Theta, double cv,
+                                const double* A, const double* Gold, const double* Temp_old,
+                                const double* KapE_bar_old, const double* E_avg_old, const double* GQD_Src_old,
+                                double* Gold_Hat, double* Rhat_old, const double* cv_cells) {
   const long nC = (long)nx * ny;
   for (long k = 0; k < nC; ++k) Gold_Hat[k] = 0.0;
   for (int g = 0; g < ng; ++g)
     for (long k = 0; k < nC; ++k) Gold_Hat[k] = Gold_Hat[k] + Gold[k + nC * g];
   for (long k = 0; k < nC; ++k) {
     Gold_Hat[k] = Gold_Hat[k] + A[k] * E_avg_old[k] / (Theta * Delt);
-    Rhat_old[k] = cv / (Theta * Delt) * Temp_old[k] +
+    const double cvk = cv_cells ? cv_cells[k] : cv;
+    Rhat_old[k] = cvk / (Theta * Delt) * Temp_old[k] +
                   ((1.0 - Theta) / Theta) * (c * KapE_bar_old[k] * E_avg_old[k] - GQD_Src_old[k]);
   }
   return 0;
+}
+
+int oracle_old_grey_coefs(int nx, int ny, int ng, double c, double Delt, double Theta, double cv, const double* A,
+                          const double* Gold, const double* Temp_old, const double* KapE_bar_old,
+                          const double* E_avg_old, const double* GQD_Src_old, double* Gold_Hat, double* Rhat_old) {
+  return oracle_old_grey_coefs_cells(nx, ny, ng, c, Delt, Theta, cv, A, Gold, Temp_old, KapE_bar_old, E_avg_old,
+                                     GQD_Src_old, Gold_Hat, Rhat_old, nullptr);
 }
 
 // GREY_COEFS (GLOQD_SOLVES.f08:47-146); argument order as the subroutine (Pold_L, Pold_R, Pold_B, Pold_T).
@@ -893,7 +903,7 @@ int oracle_grey_coefs(int nx, int ny, int ng, const double* Eg_avg, const double
 // Res_Calc.  The linear solve of each iteration is QD_FV solved directly.  The safety search
 // (:646-755) loops without an exit in the reference; this restatement makes the single pass that
 // leaves every bounded value at or above its bound, which is the state that loop reaches.
-int oracle_egp_fv_newt(int nx, int ny, double* E_avg, double* E_edgV, double* E_edgH, double* Temp, double* KapE_Bar,
+int oracle_egp_fv_newt_cells(int nx, int ny, double* E_avg, double* E_edgV, double* E_edgH, double* Temp, double* KapE_Bar,
                        double* Fx_edgV, double* Fy_edgH, double* Q_bar, double* KapE_Bar_dT, int* Its,
                        double* Deltas, double* dresiduals, const double* Temp_Mold, const double* KapE_bar_Mold,
                        double Theta, double Delt, const double* Delx, const double* Dely, const double* A,
@@ -906,7 +916,9 @@ int oracle_egp_fv_newt(int nx, int ny, double* E_avg, double* E_edgV, double* E_
                        const double* PT, const double* Gold_Hat, const double* Rhat_old, double Kap0, double cv,
                        double Comp_Unit, double Chi, double line_src, double E_Bound_Low, double T_Bound_Low,
                        double Eps1, double Eps2, int Maxits, int MGQD_It, int Use_Line_Search, int Use_Safety_Search,
-                       int Res_Calc, int kapE_dT_flag, int* GQD_Kits, double Fin_Weight, double Ein_Weight) {
+                       int Res_Calc, int kapE_dT_flag, int* GQD_Kits, double Fin_Weight, double Ein_Weight,
+                       const double* cv_cells) {
+  auto CV = [&](long k) { return cv_cells ? cv_cells[k] : cv; };
   const double h = 6.62613e-19, c = 2.99792458e2, pi = 4.0 * std::atan(1.0), erg = 6.24150934e11;
   const double sig_R = 2.0 * std::pow(pi, 5) / (15.0 * (c * c) * (h * h * h) * std::pow(erg, 4) * Comp_Unit);
   const double aR = 4.0 * sig_R / c;
@@ -942,7 +954,7 @@ int oracle_egp_fv_newt(int nx, int ny, double* E_avg, double* E_edgV, double* E_
     if (MGQD_It > 1 && kapE_dT_flag) {
       for (long k = 0; k < nC; ++k) {
         KapE_Bar_dT[k] = Org[k];
-        const double bound = (cv / (Theta * Delt) + Qdt[k]) / (c * E_avg[k]);
+        const double bound = (CV(k) / (Theta * Delt) + Qdt[k]) / (c * E_avg[k]);
         if (KapE_Bar_dT[k] > Chi * bound) KapE_Bar_dT[k] = Chi * bound;
       }
     }
@@ -950,7 +962,7 @@ int oracle_egp_fv_newt(int nx, int ny, double* E_avg, double* E_edgV, double* E_
       for (int i = 0; i < nx; ++i) {
         const long k = Ci(i, j);
         const double a = A[k], dx = Delx[i], dy = Dely[j];
-        drT[k] = cv / (Theta * Delt) * Temp[k] + Q_bar[k] - c * KapE_Bar[k] * E_avg[k] - Rhat_old[k];
+        drT[k] = CV(k) / (Theta * Delt) * Temp[k] + Q_bar[k] - c * KapE_Bar[k] * E_avg[k] - Rhat_old[k];
         drB[k] = a * (1.0 / (Theta * Delt) + c * KapE_Bar[k]) * E_avg[k] + dy * (Fx_edgV[Vi(i + 1, j)] - Fx_edgV[Vi(i, j)]) +
                  dx * (Fy_edgH[Hi(i, j + 1)] - Fy_edgH[Hi(i, j)]) - a * Q_bar[k] - Gold_Hat[k];
         drML[k] = a * Fx_edgV[Vi(i, j)] / 2.0 + c * dy * (DC_xx[k] * E_avg[k] - DL_xx[k] * E_edgV[Vi(i, j)]) +
@@ -961,7 +973,7 @@ int oracle_egp_fv_newt(int nx, int ny, double* E_avg, double* E_edgV, double* E_
                   c * dy * (DR_xy[k] * E_edgV[Vi(i + 1, j)] - DL_xy[k] * E_edgV[Vi(i, j)]) / 2.0 - PB[k];
         drMT[k] = a * Fy_edgH[Hi(i, j + 1)] / 2.0 + c * dx * (DT_yy[k] * E_edgH[Hi(i, j + 1)] - DC_yy[k] * E_avg[k]) +
                   c * dy * (DR_xy[k] * E_edgV[Vi(i + 1, j)] - DL_xy[k] * E_edgV[Vi(i, j)]) / 2.0 - PT[k];
-        W[k] = cv / (Theta * Delt) + Qdt[k] - c * KapE_Bar_dT[k] * E_avg[k];
+        W[k] = CV(k) / (Theta * Delt) + Qdt[k] - c * KapE_Bar_dT[k] * E_avg[k];
         drG[k] = -drB[k] + drT[k] * (a / W[k]) * (c * KapE_Bar_dT[k] * E_avg[k] - Qdt[k]) +
                  2.0 * dy * (drMR[k] - drML[k]) / a + 2.0 * dx * (drMT[k] - drMB[k]) / a;
         EBC[k] = a * (1.0 / (Theta * Delt) + c * KapE_Bar[k] * (1.0 + (c * KapE_Bar_dT[k] * E_avg[k] - Qdt[k]) / W[k])) +
@@ -1117,6 +1129,29 @@ int oracle_egp_fv_newt(int nx, int ny, double* E_avg, double* E_edgV, double* E_
   }
   *Its = its;
   return 0;
+}
+
+int oracle_egp_fv_newt(int nx, int ny, double* E_avg, double* E_edgV, double* E_edgH, double* Temp, double* KapE_Bar,
+                       double* Fx_edgV, double* Fy_edgH, double* Q_bar, double* KapE_Bar_dT, int* Its,
+                       double* Deltas, double* dresiduals, const double* Temp_Mold, const double* KapE_bar_Mold,
+                       double Theta, double Delt, const double* Delx, const double* Dely, const double* A,
+                       const double* Cb_L, const double* Cb_B, const double* Cb_R, const double* Cb_T,
+                       const double* E_in_L, const double* E_in_B, const double* E_in_R, const double* E_in_T,
+                       const double* F_in_L, const double* F_in_B, const double* F_in_R, const double* F_in_T,
+                       const double* DC_xx, const double* DL_xx, const double* DR_xx, const double* DC_yy,
+                       const double* DB_yy, const double* DT_yy, const double* DL_xy, const double* DR_xy,
+                       const double* DB_xy, const double* DT_xy, const double* PL, const double* PR, const double* PB,
+                       const double* PT, const double* Gold_Hat, const double* Rhat_old, double Kap0, double cv,
+                       double Comp_Unit, double Chi, double line_src, double E_Bound_Low, double T_Bound_Low,
+                       double Eps1, double Eps2, int Maxits, int MGQD_It, int Use_Line_Search, int Use_Safety_Search,
+                       int Res_Calc, int kapE_dT_flag, int* GQD_Kits, double Fin_Weight, double Ein_Weight) {
+  return oracle_egp_fv_newt_cells(nx, ny, E_avg, E_edgV, E_edgH, Temp, KapE_Bar, Fx_edgV, Fy_edgH, Q_bar, KapE_Bar_dT,
+                                  Its, Deltas, dresiduals, Temp_Mold, KapE_bar_Mold, Theta, Delt, Delx, Dely, A, Cb_L,
+                                  Cb_B, Cb_R, Cb_T, E_in_L, E_in_B, E_in_R, E_in_T, F_in_L, F_in_B, F_in_R, F_in_T,
+                                  DC_xx, DL_xx, DR_xx, DC_yy, DB_yy, DT_yy, DL_xy, DR_xy, DB_xy, DT_xy, PL, PR, PB, PT,
+                                  Gold_Hat, Rhat_old, Kap0, cv, Comp_Unit, Chi, line_src, E_Bound_Low, T_Bound_Low,
+                                  Eps1, Eps2, Maxits, MGQD_It, Use_Line_Search, Use_Safety_Search, Res_Calc,
+                                  kapE_dT_flag, GQD_Kits, Fin_Weight, Ein_Weight, nullptr);
 }
 
 }  // extern "C"

@@ -40,9 +40,12 @@ _SIG = {
     "oracle_collapse_mg_ef": (_i, [_i, _i, _i] + [_D] * 5 + [_i] + [_D] * 5),
     "oracle_cbar_calc": (_i, [_i, _i, _i] + [_D] * 15),
     "oracle_old_grey_coefs": (_i, [_i, _i, _i, _d, _d, _d, _d] + [_D] * 8),
+    "oracle_old_grey_coefs_cells": (_i, [_i, _i, _i, _d, _d, _d, _d] + [_D] * 9),
     "oracle_grey_coefs": (_i, [_i, _i, _i] + [_D] * 14 + [_d, _d, _d] + [_D] * 4 + [_D] * 15 + [_d]),
     "oracle_egp_fv_newt": (_i, [_i, _i] + [_D] * 9 + [_I, _D, _D, _D, _D, _d, _d] + [_D] * 3 + [_D] * 12 + [_D] * 14
                            + [_D] * 2 + [_d] * 9 + [_i] * 6 + [_I, _d, _d]),
+    "oracle_egp_fv_newt_cells": (_i, [_i, _i] + [_D] * 9 + [_I, _D, _D, _D, _D, _d, _d] + [_D] * 3 + [_D] * 12
+                                 + [_D] * 14 + [_D] * 2 + [_d] * 9 + [_i] * 6 + [_I, _d, _d, _D]),
 }
 
 _lib = None
@@ -346,12 +349,16 @@ def cbar_calc(d):
 
 
 def old_grey_coefs(c, Delt, Theta, cv, A, Gold, Temp_old, KapE_bar_old, E_avg_old, GQD_Src_old):
-    """OLD_GREY_COEFS: (Gold_Hat, Rhat_old)."""
+    """OLD_GREY_COEFS: (Gold_Hat, Rhat_old).  cv: the reference's scalar, or an (nx, ny) array per cell."""
     nx, ny, ng = Gold.shape
     gh, rh = zeros(nx, ny), zeros(nx, ny)
-    rc = lib().oracle_old_grey_coefs(nx, ny, ng, float(c), float(Delt), float(Theta), float(cv), _p(F(A)), _p(F(Gold)),
-                                     _p(F(Temp_old)), _p(F(KapE_bar_old)), _p(F(E_avg_old)), _p(F(GQD_Src_old)),
-                                     _p(gh), _p(rh))
+    args = [nx, ny, ng, float(c), float(Delt), float(Theta), 0.0 if np.ndim(cv) else float(cv), _p(F(A)), _p(F(Gold)),
+            _p(F(Temp_old)), _p(F(KapE_bar_old)), _p(F(E_avg_old)), _p(F(GQD_Src_old)), _p(gh), _p(rh)]
+    if np.ndim(cv):
+        cvc = F(np.broadcast_to(cv, (nx, ny)))
+        rc = lib().oracle_old_grey_coefs_cells(*args, _p(cvc))
+    else:
+        rc = lib().oracle_old_grey_coefs(*args)
     assert rc == 0
     return gh, rh
 
@@ -378,24 +385,194 @@ def egp_fv_newt(g, Theta, Delt, Kap0, cv, Comp_Unit, Chi=0.7, line_src=2.0, E_Bo
     """EGP_FV_NEWT (GLOQD_SOLVES.f08:305-860) on copies of g's state (E_avg, E_edgV, E_edgH, Temp, KapE_Bar,
     Fx_edgV, Fy_edgH); g also holds Temp_Mold, KapE_bar_Mold, Delx, Dely, A, Cb_*, E_in_*, F_in_*, the D's,
     the P's, Gold_Hat and Rhat_old.  Returns the new state plus Q_bar, KapE_Bar_dT, Its, GQD_Kits,
-    Deltas (Its, 6), dresiduals (Its, 6)."""
+    Deltas (Its, 6), dresiduals (Its, 6).  cv: the reference's scalar, or an (nx, ny) array per cell."""
     nx, ny = g["Temp"].shape
     o = {k: F(g[k]).copy(order="F") for k in EGP_STATE}
     o["Q_bar"], o["KapE_Bar_dT"] = zeros(nx, ny), zeros(nx, ny)
     its = ctypes.c_int(0)
     Dl, dr = zeros(Maxits, 6), zeros(Maxits, 6)
     kits = np.zeros(Maxits, dtype=np.int32)
-    rc = lib().oracle_egp_fv_newt(
+    cvc = F(np.broadcast_to(cv, (nx, ny))) if np.ndim(cv) else None
+    fn = lib().oracle_egp_fv_newt_cells if cvc is not None else lib().oracle_egp_fv_newt
+    extra = (_p(cvc),) if cvc is not None else ()
+    rc = fn(
         nx, ny, *[_p(o[k]) for k in EGP_STATE], _p(o["Q_bar"]), _p(o["KapE_Bar_dT"]), ctypes.byref(its), _p(Dl),
         _p(dr), _p(F(g["Temp_Mold"])), _p(F(g["KapE_bar_Mold"])), float(Theta), float(Delt), _p(F(g["Delx"])),
         _p(F(g["Dely"])), _p(F(g["A"])), *[_p(F(g["Cb_" + s])) for s in SIDES], *[_p(F(g["E_in_" + s])) for s in SIDES],
         *[_p(F(g["F_in_" + s])) for s in SIDES], *[_p(F(g[k])) for k in GREY_D + GREY_P],
-        _p(F(g["Gold_Hat"])), _p(F(g["Rhat_old"])), float(Kap0), float(cv), float(Comp_Unit), float(Chi),
-        float(line_src), float(E_Bound_Low), float(T_Bound_Low), float(Eps1), float(Eps2), int(Maxits), int(MGQD_It),
-        int(bool(Use_Line_Search)), int(bool(Use_Safety_Search)), int(bool(Res_Calc)), int(bool(kapE_dT_flag)),
-        _p(kits), float(Fin_Weight), float(Ein_Weight))
+        _p(F(g["Gold_Hat"])), _p(F(g["Rhat_old"])), float(Kap0), 0.0 if cvc is not None else float(cv),
+        float(Comp_Unit), float(Chi), float(line_src), float(E_Bound_Low), float(T_Bound_Low), float(Eps1), float(Eps2),
+        int(Maxits), int(MGQD_It), int(bool(Use_Line_Search)), int(bool(Use_Safety_Search)), int(bool(Res_Calc)),
+        int(bool(kapE_dT_flag)), _p(kits), float(Fin_Weight), float(Ein_Weight), *extra)
     assert rc == 0, rc
     n = its.value
     o["Its"], o["GQD_Kits"], o["Deltas"], o["dresiduals"] = n, kits[:n], Dl[:n], dr[:n]
     return o
 
+
+
+# ------------------------------------------------------------------------------------------------
+# The mlqd time loop: TRT_MLQD_ALGORITHM with run_type 'mlqd' and use_grey = 1 (HO_Form 0, RT_start_Its 2,
+# Fdt/Fin/Ein weights 1; ALGORITHMS.f08:294-302, 389-416, 518-572, 670-836).
+# ------------------------------------------------------------------------------------------------
+
+def mlqd_init(nx, ny, Omega_x, Omega_y, quad_weight, Nu_g, Tini, comp_unit, c, bc_type=(0, 0, 0, 0),
+              bcT=(0.0, 0.0, 0.0, 0.0)):
+    """The initial state of the mlqd algorithm: RT_INIT (INITIALIZERS.f08:15-109), Temp = Tini (TEMP_INIT,
+    :114-139; the material follows from Temp), MGQD_INIT (:159-321) and GQD_INIT (:326-427).  KapE_Bar and
+    GQD_Src are left unset by the reference (allocated, never written before the first step); they are
+    zero here, and with Theta = 1 they do not enter the first step."""
+    nm, ng = len(Omega_x), len(Nu_g) - 1
+    pi = np.pi
+    bg = np.array([bg_planck(Tini, Nu_g[g], Nu_g[g + 1], comp_unit) for g in range(ng)])
+    st = {}
+    st["I_crn"] = F(np.broadcast_to(bg, (2 * nx, 2 * ny, nm, ng)))
+    I_edgV = F(np.broadcast_to(bg, (nx + 1, ny, nm, ng)))
+    I_edgH = F(np.broadcast_to(bg, (nx, ny + 1, nm, ng)))
+    Ic_edgV = F(np.broadcast_to(bg, (nx + 1, 2 * ny, nm, ng)))
+    Ic_edgH = F(np.broadcast_to(bg, (2 * nx, ny + 1, nm, ng)))
+    st["I_edgV"], st["I_edgH"], st["Ic_edgV"], st["Ic_edgH"] = rt_bc_update(
+        (0, 0, 0, 0), bcT[0], bcT[1], bcT[2], bcT[3], comp_unit, Nu_g, I_edgV, I_edgH, Ic_edgV, Ic_edgH)
+    eg = 4.0 * pi * bg / c
+    E0 = zeros(nx, ny)
+    for g in range(ng):
+        E0 = E0 + eg[g]
+    st["HO_E_avg"] = E0.copy(order="F")
+    st["Temp"] = F(np.full((nx, ny), float(Tini)))
+    st["Eg_avg"] = F(np.broadcast_to(eg, (nx, ny, ng)))
+    st["Eg_edgV"] = F(np.broadcast_to(eg, (nx + 1, ny, ng)))
+    st["Eg_edgH"] = F(np.broadcast_to(eg, (nx, ny + 1, ng)))
+    st["Fxg_edgV"], st["Fyg_edgH"] = zeros(nx + 1, ny, ng), zeros(nx, ny + 1, ng)
+    third = 1.0 / 3.0
+    st["fg_avg_xx"], st["fg_avg_yy"] = F(np.full((nx, ny, ng), third)), F(np.full((nx, ny, ng), third))
+    st["fg_edgV_xx"], st["fg_edgV_xy"] = F(np.full((nx + 1, ny, ng), third)), zeros(nx + 1, ny, ng)
+    st["fg_edgH_yy"], st["fg_edgH_xy"] = F(np.full((nx, ny + 1, ng), third)), zeros(nx, ny + 1, ng)
+    for s, v in zip(SIDES, (-0.5, -0.5, 0.5, 0.5)):
+        n = ny if s in "LR" else nx
+        k = SIDES.index(s)
+        st["Cg_" + s] = F(np.full((n, ng), v if bc_type[k] == 0 else 0.0))
+        st["Cb_" + s] = F(np.full(n, v if bc_type[k] == 0 else 0.0))
+    st.update(mgqd_in_calc(st["I_edgV"], st["I_edgH"], Omega_x, Omega_y, quad_weight, c, comp_unit, bc_type))
+    st.update(gqd_in_calc(st))
+    st["E_avg"] = E0.copy(order="F")
+    st["E_edgV"] = F(np.broadcast_to(E0[:1, :1], (nx + 1, ny)))
+    st["E_edgH"] = F(np.broadcast_to(E0[:1, :1], (nx, ny + 1)))
+    st["Fx_edgV"], st["Fy_edgH"] = zeros(nx + 1, ny), zeros(nx, ny + 1)
+    st["KapE_Bar"], st["GQD_Src"], st["KapE_Bar_dT"] = zeros(nx, ny), zeros(nx, ny), zeros(nx, ny)
+    return st
+
+
+def mlqd_steps(st, Omega_x, Omega_y, quad_weight, Delx, Dely, Nu_g, kappa_mult, cV, Kap0, comp_unit, c, Delt, steps,
+               Theta=1.0, conv_type=2, conv_ho=1e-10, conv_lo=1e-10, conv_gr1=1e-14, conv_gr2=1e-15, maxit_rte=50,
+               maxit_mloqd=50, maxit_gloqd=20, chi=0.7, line_src=2.0, E_Bound_Low=0.0, T_Bound_Low=0.0,
+               use_line_search=True, use_safety_search=False, kapE_dT_flag=True, bc_type=(0, 0, 0, 0),
+               bcT=(0.0, 0.0, 0.0, 0.0), threads=4):
+    """Time steps of TRT_MLQD_ALGORITHM with run_type 'mlqd' (ALGORITHMS.f08:389-416, 518-572, 670-836), on
+    the state dict of mlqd_init (updated in place).  Per step: the _old copies (:395-416), OLD_MGQD_COEFS and
+    OLD_GREY_COEFS; then outer iterations, each (from the second on) TRANSPORT_SCB + COLLAPSE_INTENSITIES
+    (+ RT_BC_UPDATE, MGQD_In_Calc, GQD_In_Calc when a side is reflective) + fg_Calc + Cg_Calc, then MGQD
+    iterations of MLOQD_FV (solved directly), COLLAPSE_MG_EF, Cbar_Calc, GREY_COEFS, EGP_FV_NEWT and
+    MATERIAL_UPDATE with CONVERGENCE(conv_lo) on T and the MGQD E, then CONVERGENCE(conv_ho) on T and the
+    transport E.  cV is a scalar or an (nx, ny) array.  Returns one dict per step (Temp, E_avg, HO_E_avg,
+    RT_Its, MGQD_Its per outer iteration, EGP_Its per MGQD iteration, the last MGQD T/E norms of each outer
+    iteration, the outer T/E norms)."""
+    nx, ny = st["Temp"].shape
+    nm, ng = len(Omega_x), len(Nu_g) - 1
+    A = F(np.outer(Delx, Dely))
+    cv = F(np.broadcast_to(cV, (nx, ny))) if np.ndim(cV) else float(cV)
+    KapE, rt_src, Bg = material_update(st["Temp"], Nu_g, kappa_mult, comp_unit)   # TEMP_INIT
+    MGQD_Src = F(4.0 * np.pi * KapE * Bg)
+    rt_start = 2
+    hist = []
+    for _ in range(steps):
+        Temp_old = st["Temp"].copy(order="F")
+        I_crn_old = st["I_crn"].copy(order="F")
+        od = {k + "_old": F(st[k]).copy(order="F") for k in ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV",
+                                                              "Fyg_edgH") + MLOQD_FACTORS}
+        od.update(KapE_old=KapE.copy(order="F"), KapR_old=KapE.copy(order="F"), Src_old=MGQD_Src.copy(order="F"),
+                  Delx=Delx, Dely=Dely, A=A)
+        E_avg_old, GQD_Src_old, KapE_Bar_old = st["E_avg"].copy(order="F"), st["GQD_Src"].copy(order="F"), \
+            st["KapE_Bar"].copy(order="F")
+        old = old_mgqd_coefs(od, c, Delt, Theta)
+        Gold_Hat, Rhat_old = old_grey_coefs(c, Delt, Theta, cv, A, old["G_old"], Temp_old, KapE_Bar_old, E_avg_old,
+                                            GQD_Src_old)
+        T_rt1, T_rt2, E_rt1, E_rt2 = zeros(nx, ny), zeros(nx, ny), zeros(nx, ny), zeros(nx, ny)
+        rt_its, rt_conv = 0, False
+        mg_hist, egp_hist, lo_norms = [], [], []
+        while not rt_conv and rt_its < maxit_rte:
+            rt_its += 1
+            if rt_its >= rt_start:
+                Src_in = F(np.repeat(np.repeat(rt_src, 2, axis=0), 2, axis=1)[:, :, None, :].repeat(nm, axis=2))
+                s = transport_scb(st["I_edgV"], st["I_edgH"], st["Ic_edgV"], st["Ic_edgH"], Omega_x, Omega_y, Delx,
+                                  Dely, A, KapE, Src_in, I_crn_old, c, Delt, threads=threads, solver=1)
+                for k in ("I_crn", "I_edgV", "I_edgH", "Ic_edgV", "Ic_edgH"):
+                    st[k] = s[k]
+                m = collapse_intensities(s["I_avg"], s["I_edgV"], s["I_edgH"], Omega_x, Omega_y, quad_weight,
+                                         comp_unit, threads=threads)
+                st["HO_E_avg"] = m["E_avg"]
+                if max(bc_type) > 0:
+                    st["I_edgV"], st["I_edgH"], st["Ic_edgV"], st["Ic_edgH"] = rt_bc_update(
+                        bc_type, bcT[0], bcT[1], bcT[2], bcT[3], comp_unit, Nu_g, st["I_edgV"], st["I_edgH"],
+                        st["Ic_edgV"], st["Ic_edgH"])
+                    st.update(mgqd_in_calc(st["I_edgV"], st["I_edgH"], Omega_x, Omega_y, quad_weight, c, comp_unit,
+                                           bc_type))
+                    st.update(gqd_in_calc(st))
+                st.update({k: v for k, v in fg_calc(m, c).items() if k != "fg_avg_xy"})
+                st.update(cg_calc(st["I_edgV"], st["I_edgH"], Omega_x, Omega_y, quad_weight, comp_unit, bc_type))
+            E_mg1, E_mg2 = st["HO_E_avg"].copy(order="F"), zeros(nx, ny)
+            T_mg1, T_mg2 = st["Temp"].copy(order="F"), zeros(nx, ny)
+            mg_its, mg_conv = 0, False
+            while not mg_conv and mg_its < maxit_mloqd:
+                mg_its += 1
+                d = {k: st[k] for k in MLOQD_FACTORS + MLOQD_BOUNDARY + ("Eg_avg", "Eg_edgV", "Eg_edgH")}
+                d.update(Src=MGQD_Src, KapE=KapE, KapR=KapE, Delx=Delx, Dely=Dely, A=A, G_old=old["G_old"],
+                         Pold_L=old["Pold_L"], Pold_B=old["Pold_B"], Pold_R=old["Pold_R"], Pold_T=old["Pold_T"],
+                         Eg_avg_old=od["Eg_avg_old"], Fxg_edgV_old=od["Fxg_edgV_old"], Fyg_edgH_old=od["Fyg_edgH_old"])
+                sol = mloqd_fv(d, c, Delt, Theta, res_calc=False, solver=0)
+                for k in ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH"):
+                    st[k] = sol[k]
+                mg = collapse_mg_ef(st)
+                cb = cbar_calc(st)
+                KapE_bar_MGQDold = st["KapE_Bar"].copy(order="F")
+                gd = dict(st, Fxg_edgV_old=od["Fxg_edgV_old"], Fyg_edgH_old=od["Fyg_edgH_old"], KapE=KapE, KapR=KapE,
+                          A=A, Pold_L=old["Pold_L"], Pold_R=old["Pold_R"], Pold_B=old["Pold_B"], Pold_T=old["Pold_T"])
+                gc = grey_coefs(gd, c, Delt, Theta)
+                g = dict(gc, **cb)
+                for k in ("E_avg", "E_edgV", "E_edgH", "Fx_edgV", "Fy_edgH"):
+                    g[k] = mg[k]
+                for k in ("E_in_", "F_in_"):
+                    for s_ in SIDES:
+                        g[k + s_] = st[k + s_]
+                g.update(Temp=st["Temp"], Temp_Mold=T_mg2, KapE_bar_Mold=KapE_bar_MGQDold, Delx=Delx, Dely=Dely, A=A,
+                         Gold_Hat=Gold_Hat, Rhat_old=Rhat_old)
+                o = egp_fv_newt(g, Theta, Delt, Kap0, cv, comp_unit, Chi=chi, line_src=line_src,
+                                E_Bound_Low=E_Bound_Low, T_Bound_Low=T_Bound_Low, Eps1=conv_gr1, Eps2=conv_gr2,
+                                Maxits=maxit_gloqd, MGQD_It=mg_its, Use_Line_Search=use_line_search,
+                                Use_Safety_Search=use_safety_search, Res_Calc=False, kapE_dT_flag=kapE_dT_flag)
+                for k in EGP_STATE:
+                    st[k] = o[k]
+                st["GQD_Src"], st["KapE_Bar_dT"] = o["Q_bar"], o["KapE_Bar_dT"]
+                st.update({k: gc[k] for k in GREY_D + GREY_P})
+                st.update(cb)
+                st["MGQD_E_avg"] = mg["E_avg"]
+                egp_hist.append(o["Its"])
+                KapE, rt_src, Bg = material_update(st["Temp"], Nu_g, kappa_mult, comp_unit)
+                MGQD_Src = F(4.0 * np.pi * KapE * Bg)
+                tc, tn_lo, _ = convergence(conv_type, conv_lo, st["Temp"], T_mg1, T_mg2, mg_its)
+                ec, en_lo, _ = convergence(conv_type, conv_lo, mg["E_avg"], E_mg1, E_mg2, mg_its)
+                mg_conv = tc and ec
+                E_mg2, E_mg1 = E_mg1, mg["E_avg"].copy(order="F")
+                T_mg2, T_mg1 = T_mg1, st["Temp"].copy(order="F")
+            mg_hist.append(mg_its)
+            lo_norms.append((tn_lo, en_lo))
+            tc, tn, _ = convergence(conv_type, conv_ho, st["Temp"], T_rt1, T_rt2, rt_its)
+            ec, en, _ = convergence(conv_type, conv_ho, st["HO_E_avg"], E_rt1, E_rt2, rt_its)
+            rt_conv = tc and ec
+            E_rt2, E_rt1 = E_rt1, st["HO_E_avg"].copy(order="F")
+            T_rt2, T_rt1 = T_rt1, st["Temp"].copy(order="F")
+        hist.append(dict(Temp=st["Temp"].copy(order="F"), E_avg=st["E_avg"].copy(order="F"),
+                         HO_E_avg=st["HO_E_avg"].copy(order="F"), Eg_avg=st["Eg_avg"].copy(order="F"),
+                         RT_Its=rt_its, MGQD_Its=mg_hist, EGP_Its=egp_hist, T_norm=tn, E_norm=en,
+                         MGQD_norms=lo_norms))
+    st["KapE"], st["MGQD_Src"] = KapE, MGQD_Src
+    return hist
