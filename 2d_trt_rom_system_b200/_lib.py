@@ -74,6 +74,7 @@ class MlqdStats(ctypes.Structure):
     """trt_mlqd_stats (include/trt_sweep.h)."""
     _fields_ = [("rt_its", ctypes.c_int), ("sweeps", ctypes.c_int), ("mgqd_its", ctypes.c_int),
                 ("egp_its", ctypes.c_int), ("mgqd_nonconv", ctypes.c_int), ("egp_nonconv", ctypes.c_int),
+                ("mgqd_krylov_max", ctypes.c_int), ("egp_krylov_max", ctypes.c_int),
                 ("T_norm", ctypes.c_double), ("E_norm", ctypes.c_double), ("sweep_ms", ctypes.c_double),
                 ("low_order_ms", ctypes.c_double)]
 

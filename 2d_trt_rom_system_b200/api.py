@@ -443,15 +443,17 @@ class TransportSweep:
         """A field of the device mlqd state (trt_mlqd_get), Fortran layout."""
         nx, ny, ng = self.nx, self.ny, self.ng
         grey = {"avg": (nx, ny), "edgV": (nx + 1, ny), "edgH": (nx, ny + 1)}
+        keys = [k for k in grey if k in name]
         if name.startswith("Cb_"):
             shp = (ny if name[-1] in "LR" else nx,)
         elif name in ("Temp", "KapE_Bar", "KapE_Bar_dT", "GQD_Src", "MGQD_E_avg", "HO_E_avg"):
             shp = (nx, ny)
         elif name == "MGQD_Src":
             shp = (nx, ny, ng)
+        elif keys:
+            shp = grey[keys[0]] + ((ng,) if name.startswith(("Eg_", "Fxg", "Fyg")) else ())
         else:
-            key = [k for k in grey if k in name][0]
-            shp = grey[key] + ((ng,) if name.startswith(("Eg_", "Fxg", "Fyg")) else ())
+            shp = (1,)   # unknown name: the library rejects it
         out = np.empty(shp, order="F")
         check(_lib.lib().trt_mlqd_get(self._h, name.encode(), dptr(out), out.size), "trt_mlqd_get")
         return out

@@ -1230,10 +1230,14 @@ int mlqd_step_impl(Mlqd& m, trt_mlqd_stats* out) {
       bool noconv = false;
       if ((rc = egp_newton(m.GR.get(), st, e, eo, m.part, m.norms, &its, m.kits.data(), nullptr, nullptr, &noconv)))
         return rc;
-      for (int g = 0; g < ng; ++g)   // h_scal was read before the Newton iteration's synchronisations
+      for (int g = 0; g < ng; ++g) {   // h_scal was read before the Newton iteration's synchronisations
         if (m.MG->h_scal[g].done != 1) ++S.mgqd_nonconv;
-      for (int k = 0; k < its; ++k)
+        S.mgqd_krylov_max = std::max(S.mgqd_krylov_max, m.MG->h_scal[g].its);
+      }
+      for (int k = 0; k < its; ++k) {
         if (m.kits[k] < 0) ++S.egp_nonconv;
+        S.egp_krylov_max = std::max(S.egp_krylov_max, (std::abs(m.kits[k]) - 1) / 2);
+      }
       m.egp_counts.push_back(its);
       S.egp_its += its;
       if ((rc = trt_host::handle_material(m.h, m.Src))) return rc;   // MATERIAL_UPDATE(Temp)
@@ -1265,7 +1269,7 @@ int mlqd_step_impl(Mlqd& m, trt_mlqd_stats* out) {
   S.sweep_ms = sweep_ms;
   S.low_order_ms = total - sweep_ms;
   if (out) *out = S;
-  return (S.mgqd_nonconv || S.egp_nonconv) ? TRT_ERR_NOCONV : TRT_OK;
+  return TRT_OK;
 }
 
 }  // namespace

@@ -62,6 +62,9 @@ def parse():
                    help="timed low-order MGQD solves (MLOQD_FV) on the configuration's grid and groups; 0 skips")
     p.add_argument("--mgqd-only", action="store_true",
                    help="run only the low-order MGQD leg (--mgqd solves) and print its JSON object")
+    p.add_argument("--mlqd-steps", type=int, default=2,
+                   help="time steps of the mlqd algorithm (sweep + MGQD/grey low-order iterations) on the "
+                        "configuration's grid, mixed vs FP64; 0 = skip")
     p.add_argument("--time-steps", type=int, default=10,
                    help="time steps of the transport-only time loop (mixed vs FP64 temperature error); 0 = skip")
     return p.parse_args()
@@ -262,6 +265,63 @@ def run_time_steps(pkg, torch, prob, steps, conv_type=2, conv_ho=1e-10, maxit=20
                      "step_ms_p99": float(np.percentile(lat, 99)),
                      "updates_per_s": float(upd * sum(r["its"]) / (lat.sum() * 1e-3))}
     return out
+
+
+def run_mlqd(pkg, torch, prob, steps, conv_ho=1e-8, conv_lo=1e-9, maxit_rte=10, maxit_mloqd=50):
+    """The reference's mlqd algorithm (TRT_MLQD_ALGORITHM, run_type 'mlqd') on the device, FP64 and mixed from
+    the same initial state: per outer iteration one sweep (from the second on), then MGQD iterations of
+    MLOQD_FV + the grey EGP Newton solve + MATERIAL_UPDATE, all low-order work in FP64.  The material is
+    the Fleck-Cummings opacity with Kappa_Mult = 1: the reference's grey emission (Q_bar with Kap0) leaves
+    Kappa_Mult out, so only a uniform multiplier keeps the grey problem consistent with the multigroup one
+    (with the configuration's rectangles the MGQD iteration does not converge, in the oracle as well).
+    Reports the mixed run's temperature, energy density and flux error against FP64 after every step."""
+    ts = pkg.problems.fc_timestep_setup(prob)
+    CU, C = pkg.problems.COMP_UNIT, pkg.problems.C_LIGHT
+    ox, oy, w = prob.directions()
+    km = np.ones((prob.nx, prob.ny), order="F")
+    fields = ("Temp", "E_avg", "HO_E_avg", "Fx_edgV", "Fy_edgH")
+    res = {}
+    for prec in ("fp64", "fp32"):
+        s = pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng,
+                               precision="mixed" if prec == "fp32" else "fp64")
+        try:
+            s.init_state(ts.Tini_eV, list(ts.bcT_eV), CU, ts.nu_eV)
+            s.tstep_setup(ts.nu_eV, km, ts.cv, np.full((prob.nx, prob.ny), ts.Tini_eV), ts.Kap0, CU, C, ts.dt,
+                          bcT=ts.bcT_eV, conv_type=2, conv_ho=conv_ho, maxit_rte=maxit_rte)
+            s.mlqd_setup(ts.Tini_eV, conv_lo=conv_lo, maxit_mloqd=maxit_mloqd)
+            out, stats, lat = {k: [] for k in fields}, [], []
+            for _ in range(steps):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                st = s.mlqd_step()
+                lat.append((time.perf_counter() - t0) * 1e3)
+                stats.append(st)
+                for k in fields:
+                    out[k].append(s.mlqd_field(k))
+        finally:
+            s.close()
+        res[prec] = dict(out=out, stats=stats, lat=lat)
+    rel = lambda a, b: float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    r = {"algorithm": "mlqd: sweep + fused moments per outer iteration (none in the first), MGQD iterations of "
+                      "MLOQD_FV (BiCGSTAB + multigrid), COLLAPSE_MG_EF, Cbar_Calc, GREY_COEFS, EGP_FV_NEWT, "
+                      "MATERIAL_UPDATE; FP64 low-order in both runs",
+         "problem": f"{prob.nx}x{prob.ny} cells, {prob.ng} groups, {prob.quad} ({prob.nm} directions); "
+                    "Fleck-Cummings opacity, Kappa_Mult 1; T0 10 eV, left boundary 1 keV; dt 2e-3 sh",
+         "steps": steps, "conv_ho": conv_ho, "conv_lo": conv_lo, "maxit_rte": maxit_rte, "maxit_mloqd": maxit_mloqd}
+    for k in fields:
+        r[k + "_rel_err_per_step"] = [rel(a, b) for a, b in zip(res["fp32"]["out"][k], res["fp64"]["out"][k])]
+    r["T_rel_err_max"] = max(r["Temp_rel_err_per_step"])
+    for prec in ("fp64", "fp32"):
+        sts = res[prec]["stats"]
+        lat = np.array(res[prec]["lat"])
+        r[prec] = {"step_ms": [float(x) for x in lat], "rt_its": [x["rt_its"] for x in sts],
+                   "sweeps": [x["sweeps"] for x in sts], "mgqd_its": [x["mgqd_its"] for x in sts],
+                   "egp_its": [x["egp_its"] for x in sts], "sweep_ms": [x["sweep_ms"] for x in sts],
+                   "low_order_ms": [x["low_order_ms"] for x in sts],
+                   "mgqd_nonconv": sum(x["mgqd_nonconv"] for x in sts),
+                   "egp_nonconv": sum(x["egp_nonconv"] for x in sts),
+                   "updates_per_s": float(prob.updates_per_sweep() * sum(x["sweeps"] for x in sts) / (lat.sum() * 1e-3))}
+    return r
 
 
 def run_serving(pkg, window_s, rate=200.0, budget_gb=120.0):
@@ -604,6 +664,11 @@ def main():
                    "ms_per_step": dt * 1e3, "path": "trt_set_material(host) + trt_sweep + trt_moments(host), pinned"}
     if args.time_steps > 0:
         line["time_steps"] = run_time_steps(pkg, torch, prob, args.time_steps)
+    if args.mlqd_steps > 0 and ws == 1:
+        try:
+            line["mlqd"] = run_mlqd(pkg, torch, prob, args.mlqd_steps)
+        except Exception as exc:   # reported, not fatal to the headline line
+            line["mlqd"] = {"error": repr(exc)}
     if args.mgqd > 0 and ws == 1:
         line["mgqd"] = run_mgqd(pkg, args.mgqd, prob.nx, prob.ng, cpu=rank == 0 and not args.no_cpu_baseline)
     if args.serving > 0 and ws == 1:

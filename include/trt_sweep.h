@@ -393,8 +393,11 @@ typedef struct trt_mlqd_stats {
   int sweeps;          /* sweeps run (the first outer iteration of a step has none) */
   int mgqd_its;        /* MGQD iterations, summed over the outer iterations */
   int egp_its;         /* EGP Newton iterations, summed over the MGQD iterations */
-  int mgqd_nonconv;    /* group solves of MLOQD_FV that stopped at the iteration limit */
-  int egp_nonconv;     /* Newton linear solves that stopped at the iteration limit */
+  int mgqd_nonconv;    /* group solves of MLOQD_FV that stopped at the iteration limit (the step goes on
+                          with that iterate; the reference falls back to a direct solve there) */
+  int egp_nonconv;     /* EGP Newton linear solves that stopped at the iteration limit (likewise) */
+  int mgqd_krylov_max; /* most BiCGSTAB iterations of a group solve of MLOQD_FV in the step */
+  int egp_krylov_max;  /* most BiCGSTAB iterations of an EGP Newton linear solve in the step */
   double T_norm, E_norm;   /* norms of the last outer iteration */
   double sweep_ms, low_order_ms;   /* device time of the sweeps and of everything else in the step */
 } trt_mlqd_stats;
