@@ -101,6 +101,8 @@ SIGNATURES = {
     "trt_get_tiling": (_i, [_P, _I, _I, _I, _I, _I]),
     "trt_set_material": (_i, [_P, _D, _D, _d, _d, _d]),
     "trt_set_material_device": (_i, [_P, _P, _P, _d, _d, _d]),
+    "trt_set_material_async": (_i, [_P, _D, _D, _d, _d, _d]),
+    "trt_moments_async": (_i, [_P, ctypes.POINTER(MomentsHost)]),
     "trt_set_source_full": (_i, [_P, _D]),
     "trt_set_boundary": (_i, [_P, _D, _D, _I]),
     "trt_bc_update": (_i, [_P, _I, _d, _d, _d, _d, _d, _D]),

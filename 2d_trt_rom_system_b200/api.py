@@ -371,6 +371,12 @@ class TransportSweep:
         check(_lib.lib().trt_set_material(self._h, dptr(K), dptr(S), float(c), float(Delt), float(Comp_Unit)),
               "trt_set_material")
 
+    def set_material_async(self, KapE_in, src_iso, c, Delt, Comp_Unit):
+        """Enqueue the material upload on the handle's input copy stream (trt_set_material_async).  The
+        arrays must be contiguous float64 (pinned for overlap) and stay unchanged until sync()."""
+        check(_lib.lib().trt_set_material_async(self._h, dptr(KapE_in), dptr(src_iso), float(c), float(Delt),
+                                                float(Comp_Unit)), "trt_set_material_async")
+
     def set_material_device(self, d_kap, d_src, c, Delt, Comp_Unit):
         """Device pointers (ints) to FP64 (nx, ny, ng) Fortran arrays."""
         check(_lib.lib().trt_set_material_device(self._h, ctypes.c_void_p(d_kap), ctypes.c_void_p(d_src), float(c),
@@ -497,6 +503,10 @@ class TransportSweep:
     def moments_into(self, mh):
         """Fill a prepared MomentsHost (pinned buffers) without allocating."""
         check(_lib.lib().trt_moments(self._h, ctypes.byref(mh)), "trt_moments")
+
+    def moments_async(self, mh):
+        """Enqueue the output download into a prepared MomentsHost (trt_moments_async); read after sync()."""
+        check(_lib.lib().trt_moments_async(self._h, ctypes.byref(mh)), "trt_moments_async")
 
     def angular(self, which=("I_avg", "I_edgV", "I_edgH", "Ic_edgV", "Ic_edgH")):
         nx, ny, nm, ng = self.nx, self.ny, self.nm, self.ng

@@ -262,6 +262,12 @@ struct trt_ctx {
   double ts_Kap0 = 0.0, ts_conv_ho = 0.0, ts_Tb[4] = {0, 0, 0, 0};
   int ts_conv_type = 1, ts_maxit = 1, ts_bc[4] = {0, 0, 0, 0};
   std::vector<double> ts_nu;
+  // pipelined stepping (trt_set_material_async / trt_moments_async): a copy stream for each direction,
+  // a staging pair for the next material, and the events that order them against the handle's stream
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaEvent_t ev_staged = nullptr, ev_stage_free = nullptr, ev_epi = nullptr, ev_out = nullptr;
+  double *d_kap_in = nullptr, *d_q_in = nullptr;
+  bool out_pending = false;
   // low-order (mlqd) state attached by the MGQD side of the library, released with the handle
   void* lo = nullptr;
   void (*lo_free)(void*) = nullptr;
@@ -594,6 +600,11 @@ int sweep_impl(trt_ctx* c, unsigned flags) {
 // Moments / QD factors and residual norms after a sweep (on the handle's stream).
 template <class Real>
 int sweep_epilogue(trt_ctx* c, unsigned flags) {
+  if ((flags & TRT_MOMENTS) && c->out_pending) {
+    // the outputs of the previous step are still being copied out (trt_moments_async)
+    TRT_CUDA(cudaStreamWaitEvent(c->stream, c->ev_out, 0));
+    c->out_pending = false;
+  }
   if (flags & TRT_MOMENTS) {
     trt::CombineArgs A{};
     A.nx = c->nx; A.ny = c->ny; A.nm = c->nm; A.ng = c->ng; A.mq = c->mq; A.nh = c->t.NH;
@@ -1517,6 +1528,13 @@ trt_ctx* trt_create(int n_x, int n_y, int n_m, int n_g, const double* Omega_x, c
 void trt_destroy(trt_ctx* c) {
   if (!c) return;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (cudaStream_t q : {c->s_in, c->s_out})
+    if (q) {
+      cudaStreamSynchronize(q);
+      cudaStreamDestroy(q);
+    }
+  for (cudaEvent_t e : {c->ev_staged, c->ev_stage_free, c->ev_epi, c->ev_out})
+    if (e) cudaEventDestroy(e);
   if (c->lo && c->lo_free) c->lo_free(c->lo);
   for (void* p : c->allocs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1712,7 +1730,63 @@ int trt_sweep(trt_ctx* c, unsigned flags) {
 int trt_sync(trt_ctx* c) {
   if (!c) return TRT_ERR_ARG;
   TRT_CUDA(cudaStreamSynchronize(c->stream));
+  for (cudaStream_t q : {c->s_in, c->s_out})
+    if (q) TRT_CUDA(cudaStreamSynchronize(q));
   return check_err(c);
+}
+
+// Copy streams, events and the staging pair of the pipelined calls (first use).
+static int pipe_init(trt_ctx* c) {
+  if (c->s_in) return TRT_OK;
+  const size_t n = (size_t)c->nx * c->ny * c->ng;
+  int rc;
+  if ((rc = alloc_t(c, &c->d_kap_in, n)) || (rc = alloc_t(c, &c->d_q_in, n))) return rc;
+  for (cudaEvent_t* e : {&c->ev_staged, &c->ev_stage_free, &c->ev_epi, &c->ev_out})
+    TRT_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  TRT_CUDA(cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking));
+  TRT_CUDA(cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking));
+  TRT_CUDA(cudaEventRecord(c->ev_stage_free, c->stream));
+  return TRT_OK;
+}
+
+int trt_set_material_async(trt_ctx* c, const double* KapE_in, const double* src_iso, double cl, double Delt,
+                           double Comp_Unit) {
+  if (!c || !KapE_in || !src_iso || !(cl > 0) || !(Delt > 0) || !(Comp_Unit > 0)) return TRT_ERR_ARG;
+  int rc = pipe_init(c);
+  if (rc) return rc;
+  const size_t n = (size_t)c->nx * c->ny * c->ng;
+  // host -> staging on the input stream, once the previous material has left the staging pair
+  TRT_CUDA(cudaStreamWaitEvent(c->s_in, c->ev_stage_free, 0));
+  TRT_CUDA(cudaMemcpyAsync(c->d_kap_in, KapE_in, n * sizeof(double), cudaMemcpyHostToDevice, c->s_in));
+  TRT_CUDA(cudaMemcpyAsync(c->d_q_in, src_iso, n * sizeof(double), cudaMemcpyHostToDevice, c->s_in));
+  TRT_CUDA(cudaEventRecord(c->ev_staged, c->s_in));
+  // staging -> the handle's material, in order on the handle's stream (after every earlier reader)
+  TRT_CUDA(cudaStreamWaitEvent(c->stream, c->ev_staged, 0));
+  c->c = cl; c->dt = Delt; c->comp_unit = Comp_Unit;
+  rc = c->prec == TRT_PREC_FP64 ? set_material_impl<double>(c, c->d_kap_in, c->d_q_in, true)
+                                : set_material_impl<float>(c, c->d_kap_in, c->d_q_in, true);
+  if (rc) return rc;
+  TRT_CUDA(cudaEventRecord(c->ev_stage_free, c->stream));
+  c->have_material = true;
+  return TRT_OK;
+}
+
+int trt_moments_async(trt_ctx* c, const trt_moments_host* out) {
+  if (!c || !out) return TRT_ERR_ARG;
+  if (!c->have_moments) return TRT_ERR_STATE;
+  int rc = pipe_init(c);
+  if (rc) return rc;
+  long long sz[kNOut];
+  output_sizes(c->nx, c->ny, c->ng, sz);
+  TRT_CUDA(cudaEventRecord(c->ev_epi, c->stream));
+  TRT_CUDA(cudaStreamWaitEvent(c->s_out, c->ev_epi, 0));
+  const double* const* h = reinterpret_cast<const double* const*>(out);
+  double* const* d = reinterpret_cast<double* const*>(&c->dout);
+  for (int k = 0; k < kNOut; ++k)
+    if (h[k]) TRT_CUDA(cudaMemcpyAsync((void*)h[k], d[k], sz[k] * sizeof(double), cudaMemcpyDeviceToHost, c->s_out));
+  TRT_CUDA(cudaEventRecord(c->ev_out, c->s_out));
+  c->out_pending = true;
+  return TRT_OK;
 }
 
 int trt_moments(trt_ctx* c, const trt_moments_host* out) {

@@ -10,7 +10,9 @@ The corner state (15 GB FP64 / 7.5 GB FP32) is far larger than L2, so no flush i
   value        mixed precision (FP32 sweep, FP64 moment combination), inputs resident in HBM
   plain_fp64   the same with FP64 throughout
   e2e          through the C ABI with host buffers: H2D of the step's material (KapE, KapB*Bg) from
-               pinned memory, sweep + moments, D2H of fg, Cg, E and the group energies
+               pinned memory, sweep + moments, D2H of fg, Cg, E and the group energies; the asynchronous
+               calls let each step's copies overlap the neighbouring sweeps (e2e.sequential: the
+               synchronous calls, one step after the other)
   roofline     scb_sweep_kernel alone (CUDA events on the library's stream), algorithmic bytes
                B = 8*s + (8*8 + 48*8)/N_m per update (s = 8 FP64 / 4 FP32) over the measured HBM peak
   cpu_baseline the CPU oracle (restatement of TRANSPORT_SCB with its OpenMP-over-groups loop,
@@ -494,8 +496,11 @@ def time_resident(pkg, torch, s, steps, warmup, flags):
     return e0.elapsed_time(e1) / steps, n1 - n0
 
 
-def time_e2e(pkg, torch, s, prob, kap, src, steps, warmup):
-    """Per step: H2D of the material from pinned memory, sweep + moments, D2H of the step's result."""
+def time_e2e(pkg, torch, s, prob, kap, src, steps, warmup, pipelined=True):
+    """Per step: H2D of the material from pinned memory, sweep + moments, D2H of the step's result.
+    pipelined: through trt_set_material_async / trt_moments_async, so that step k+1's upload and step k's
+    download run on copy streams while the sweeps run (every step still copies its own inputs and outputs);
+    otherwise the synchronous calls, one step after the other."""
     import ctypes
     names = ["fg_avg_xx", "fg_avg_yy", "fg_avg_xy", "fg_edgV_xx", "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy",
              "Cg_L", "Cg_B", "Cg_R", "Cg_T", "Eg_avg", "E_avg"]
@@ -513,19 +518,28 @@ def time_e2e(pkg, torch, s, prob, kap, src, steps, warmup):
     flags = pkg._lib.TRT_ROLL_STATE | pkg._lib.TRT_MOMENTS
     C, CU = pkg.problems.C_LIGHT, pkg.problems.COMP_UNIT
 
-    def step():
-        assert L.trt_set_material(s.handle, kp.ctypes.data_as(D), sp.ctypes.data_as(D), C, prob.dt, CU) == 0
-        assert L.trt_sweep(s.handle, flags) == 0
-        assert L.trt_moments(s.handle, ctypes.byref(mh)) == 0
+    if pipelined:
+        def step():   # the step's copies overlap the neighbouring steps' sweeps (two copy streams)
+            assert L.trt_set_material_async(s.handle, kp.ctypes.data_as(D), sp.ctypes.data_as(D), C, prob.dt,
+                                            CU) == 0
+            assert L.trt_sweep(s.handle, flags) == 0
+            assert L.trt_moments_async(s.handle, ctypes.byref(mh)) == 0
+    else:
+        def step():
+            assert L.trt_set_material(s.handle, kp.ctypes.data_as(D), sp.ctypes.data_as(D), C, prob.dt, CU) == 0
+            assert L.trt_sweep(s.handle, flags) == 0
+            assert L.trt_moments(s.handle, ctypes.byref(mh)) == 0
 
     for _ in range(warmup):
         step()
+    assert L.trt_sync(s.handle) == 0
     # host wall clock: the region includes the host<->device copies the C ABI makes
     torch.cuda.synchronize()
     pkg.ranks.barrier()
     t0 = time.perf_counter()
     for _ in range(steps):
         step()
+    assert L.trt_sync(s.handle) == 0
     torch.cuda.synchronize()
     dt = (time.perf_counter() - t0) / steps
     pkg.ranks.barrier()
@@ -616,7 +630,10 @@ def main():
             # sweep kernel alone (no moments, no roll): per-launch duration for the roofline
             ms_k, _ = time_resident(pkg, torch, s, max(3, args.steps // 2), 1, 0)
             ms_k = ranks.reduce_max(ms_k)
-            e2e = time_e2e(pkg, torch, s, prob, kap, src, max(3, args.steps // 4), 1) if prec == "fp32" else None
+            e2e = None
+            if prec == "fp32":
+                e2e = (time_e2e(pkg, torch, s, prob, kap, src, max(3, args.steps // 4), 3, pipelined=True),
+                       time_e2e(pkg, torch, s, prob, kap, src, max(3, args.steps // 8), 3, pipelined=False))
             tl = s.tiling()
         finally:
             s.close()
@@ -658,10 +675,16 @@ def main():
                                            "traffic": traffic_from_profile("fp64")},
                               "tiling": r["tiling"]}
         line["mixed_over_fp64"] = line["value"] / line["plain_fp64"]["value"]
-    dt, h2d, d2h = main_["e2e"]
+    (dt, h2d, d2h), (dt_seq, _, _) = main_["e2e"]
     dt = ranks.reduce_max(dt)
+    dt_seq = ranks.reduce_max(dt_seq)
     line["e2e"] = {"value": ranks.whole_job_rate(upd, dt, ws), "unit": "updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                   "ms_per_step": dt * 1e3, "path": "trt_set_material(host) + trt_sweep + trt_moments(host), pinned"}
+                   "ms_per_step": dt * 1e3,
+                   "path": "trt_set_material_async(pinned host) + trt_sweep + trt_moments_async(pinned host): each step "
+                           "uploads its material and downloads its fg, Cg, Eg, E; the copies of neighbouring steps "
+                           "overlap the sweeps on two copy streams",
+                   "sequential": {"value": ranks.whole_job_rate(upd, dt_seq, ws), "ms_per_step": dt_seq * 1e3,
+                                  "path": "trt_set_material + trt_sweep + trt_moments, one step after the other"}}
     if args.time_steps > 0:
         line["time_steps"] = run_time_steps(pkg, torch, prob, args.time_steps)
     if args.mlqd_steps > 0 and ws == 1:

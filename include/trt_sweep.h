@@ -302,6 +302,20 @@ int trt_sweep(trt_ctx* ctx, unsigned flags);
 int trt_sync(trt_ctx* ctx);
 /* Copy the combined moments / factors of the latest TRT_MOMENTS sweep to host memory. */
 int trt_moments(trt_ctx* ctx, const trt_moments_host* out);
+/* Pipelined stepping (no counterpart in the reference, whose calls are synchronous).  For a caller that
+ * streams many materials through one handle (snapshot generation, parametric runs):
+ *   trt_set_material_async: enqueues the host-to-device copy of KapE_in and src_iso (as trt_set_material) on
+ *     a copy stream into a staging pair, so that it overlaps the sweep already queued; the handle's stream
+ *     takes the new material over in order, before the next trt_sweep.
+ *   trt_moments_async: enqueues the device-to-host copies of the latest TRT_MOMENTS sweep's outputs (as
+ *     trt_moments) on a second copy stream, so that they overlap the next sweep; that sweep's moment
+ *     epilogue waits for them before it overwrites the outputs.
+ * Host buffers should be pinned (pageable ones make the copies synchronous); inputs must stay unchanged and
+ * outputs unread until trt_sync returns, which waits for both copy streams.  A step is then
+ *   trt_set_material_async -> trt_sweep(TRT_ROLL_STATE | TRT_MOMENTS) -> trt_moments_async. */
+int trt_set_material_async(trt_ctx* ctx, const double* KapE_in, const double* src_iso, double c, double Delt,
+                           double Comp_Unit);
+int trt_moments_async(trt_ctx* ctx, const trt_moments_host* out);
 /* Angular intensities of the latest sweep in the reference layouts (any pointer may be NULL). */
 int trt_get_angular(trt_ctx* ctx, double* I_avg, double* I_edgV, double* I_edgH, double* Ic_edgV,
                     double* Ic_edgH);
