@@ -13,7 +13,8 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libtrt_sweep.so")
 SOURCES = ["trt_api.cu", "mgqd.cu"]
-HEADERS = ["aux_kernels.cuh", "dropin_kernels.cuh", "layout.cuh", "mgqd_kernels.cuh", "ptx.cuh", "scb_cell.h",
+HEADERS = ["aux_kernels.cuh", "dropin_kernels.cuh", "gqd_kernels.cuh", "handle_hooks.h", "layout.cuh", "mgqd_kernels.cuh",
+           "ptx.cuh", "scb_cell.h",
            "sweep_kernel.cuh", "tstep_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-shared",
