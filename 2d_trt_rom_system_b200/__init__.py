@@ -6,7 +6,8 @@ package is its Python mirror plus the problem and quadrature generators used by 
 """
 from . import problems, quadrature, ranks, serving  # noqa: F401
 from .api import (COLLAPSE_INTENSITIES, COLLAPSE_MG_EF, EGP_FV_NEWT, GQD_In_Calc, GREY_COEFS,  # noqa: F401
-                  MGQD_In_Calc, MLOQD_FV, OLD_GREY_COEFS, OLD_MGQD_COEFS, RT_BC_UPDATE, TRANSPORT_SCB, Batch,
+                  MGQD_In_Calc, MLOQD_FV, OLD_GREY_COEFS, OLD_MGQD_COEFS, POD_RECONSTRUCT, POD_Calc, RT_BC_UPDATE,
+                  TRANSPORT_SCB, Batch,
                   Bg_planck_calc, Cbar_Calc, Cg_Calc, TransportSweep, fg_Calc, kernel_launches, mgqd_last_stats,
                   mgqd_set_tolerance, required_bytes)
 from ._lib import LIB_PATH, TrtError, check, lib  # noqa: F401

@@ -143,6 +143,12 @@ SIGNATURES = {
     "trt_egp_fv_newt": (_i, [_i, _i] + [_D] * 9 + [_I, _D, _D, _D, _D, _d, _d] + [_D] * 3 + [_D] * 12 + [_D] * 14
                         + [_D] * 2 + [_d] * 9 + [_i] * 6 + [_I, _d, _d]),
     "trt_mgqd_last_stats": (_i, [_D, _I, _D]),
+    "trt_pod_calc": (_i, [_D, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, _D, _D, _D,
+                          _D]),
+    "trt_pod_calc_device": (_i, [_P, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong,
+                                 _P, _P, _P, _P, _P]),
+    "trt_pod_reconstruct": (_i, [_D, _D, _D, _D, _D, _I, _i, _i, _i, _i, _i]),
+    "trt_pod_reconstruct_device": (_i, [_P, _P, _P, _P, _P, _P, _P, _i, _i, _i, _i, _P]),
     "trt_mlqd_setup": (_i, [_P, _d, ctypes.POINTER(MlqdParams)]),
     "trt_mlqd_step": (_i, [_P, ctypes.POINTER(MlqdStats)]),
     "trt_mlqd_counts": (_i, [_P, _I, _i, _I, _i, _I, _I]),

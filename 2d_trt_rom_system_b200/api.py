@@ -288,6 +288,27 @@ def mgqd_last_stats():
     return ms.value, its.value, mv.value
 
 
+def POD_Calc(data, N_t, N_g, clen, g):
+    """POD of block g of data(clen, N_g, N_t) (trt_pod_calc): (center, umat, sig, vtmat), k = min(clen, N_t)."""
+    k = min(clen, N_t)
+    d = np.asarray(data, dtype=np.float64).reshape(-1, order="F")
+    if d.size != clen * max(N_g, 1) * N_t:
+        raise ValueError(f"data holds {d.size} values, expected clen * max(N_g, 1) * N_t")
+    d = np.ascontiguousarray(d)
+    c, u, s, vt = np.empty(clen), np.empty((clen, k), order="F"), np.empty(k), np.empty((k, N_t), order="F")
+    check(_lib.lib().trt_pod_calc(dptr(d), int(N_t), int(N_g), int(clen), int(g), dptr(c), dptr(u), dptr(s),
+                                  dptr(vt)), "trt_pod_calc")
+    return c, u, s, vt
+
+
+def POD_RECONSTRUCT(dat, C, S, U, V, rank, len_, N_g, N_t, t, PODgsum):
+    """trt_pod_reconstruct into dat (float64, len_ values)."""
+    r = np.ascontiguousarray(rank, dtype=np.int32)
+    arrs = [np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1, order="F")) for a in (C, S, U, V)]
+    check(_lib.lib().trt_pod_reconstruct(dptr(dat), *[dptr(a) for a in arrs], iptr(r), int(len_), int(N_g), int(N_t),
+                                         int(t), int(PODgsum)), "trt_pod_reconstruct")
+
+
 def Bg_planck_calc(T, nu_low, nu_high, comp_unit):
     """FUNCTION Bg_planck_calc, MainSrc/TEMP_FUNCTIONS.f08:90-108 (host evaluation in the library)."""
     return _lib.lib().trt_bg_planck(float(T), float(nu_low), float(nu_high), float(comp_unit))

@@ -12,11 +12,12 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libtrt_sweep.so")
-SOURCES = ["trt_api.cu", "mgqd.cu"]
+SOURCES = ["trt_api.cu", "mgqd.cu", "rom.cu"]
 HEADERS = ["aux_kernels.cuh", "dropin_kernels.cuh", "gqd_kernels.cuh", "handle_hooks.h", "layout.cuh", "mgqd_kernels.cuh",
            "ptx.cuh", "scb_cell.h",
            "sweep_kernel.cuh", "tstep_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+LIBS = ["-lcusolver"]   # the SVD of the POD (rom.cu)
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-shared",
               "-diag-suppress", "177"]
 
@@ -42,7 +43,7 @@ def build(force=False, verbose=False):
     if not force and not _stale():
         return LIB
     cmd = [_nvcc()] + NVCC_FLAGS + ARCH + ["-I" + INCLUDE, "-I" + CSRC, "-o", LIB + ".tmp"] + \
-        [os.path.join(CSRC, s) for s in SOURCES]
+        [os.path.join(CSRC, s) for s in SOURCES] + LIBS
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -427,6 +427,30 @@ int trt_mlqd_counts(trt_ctx* ctx, int* mgqd_per_outer, int cap_outer, int* egp_p
  * transport "HO_E_avg".  `count` is the number of doubles the caller provides (checked). */
 int trt_mlqd_get(trt_ctx* ctx, const char* name, double* host, long long count);
 
+/* ---- Reduced-order model: POD of QD-factor snapshots and its reconstruction ----------------------
+ * trt_pod_calc replaces the offline decomposer's POD_Calc with SVD_Calc_Cntr
+ * (Decomposer/DecompSrc/POD_ROUTINES.c:75-120, LA_ROUTINES.c:50-170): data(clen, n_g, n_t) in the decomposer's
+ * layout (one snapshot of n_g blocks of clen values per time level; n_g = 0 for a single block), the POD of
+ * block g (0-based): center(clen) = mean over t, and the thin SVD of the centred (clen x n_t) matrix,
+ * umat(clen, k), sig(k) descending, vtmat(k, n_t) = V^T, k = min(clen, n_t).  The SVD is cuSOLVER's gesvd
+ * (LAPACK's dgesvd in the reference); singular vectors are unique up to sign.  Returns TRT_ERR_NOCONV when the
+ * SVD does not converge.  trt_pod_calc_device takes device pointers (data resident in HBM, e.g. snapshots
+ * stored by a time loop) and enqueues on `stream`. */
+int trt_pod_calc(const double* data, long long n_t, long long n_g, long long clen, long long g, double* center,
+                 double* umat, double* sig, double* vtmat);
+int trt_pod_calc_device(const double* data, long long n_t, long long n_g, long long clen, long long g, double* center,
+                        double* umat, double* sig, double* vtmat, void* stream);
+/* Replaces SUBROUTINE POD_RECONSTRUCT, MainSrc/POD_ROUTINES.f08:372-432 (argument order as the subroutine;
+ * t is 1-based): dat(len) = C + sum_r S U V^T(., t), groupwise (PODgsum = 0: N_g blocks of len/N_g values,
+ * block g with rank(g) modes packed after the earlier blocks' in S, U and V) or over the whole vector
+ * (PODgsum = 1, rank(1) modes).  trt_pod_reconstruct_device takes device pointers and the per-block mode
+ * offsets (sum of the earlier ranks), for a caller that keeps the basis on the device. */
+int trt_pod_reconstruct(double* dat, const double* C, const double* S, const double* U, const double* V,
+                        const int* rank, int len, int N_g, int N_t, int t, int PODgsum);
+int trt_pod_reconstruct_device(double* dat, const double* C, const double* S, const double* U, const double* V,
+                               const int* rank, const long long* offsets, int len, int n_blocks, int N_t, int t,
+                               void* stream);
+
 /* ---- Batched instances ---------------------------------------------------------------------------
  * Many independent handles (different grids, groups, quadratures, precisions) stepped together: the
  * sweeps of all handles that share a tiling class (precision, slices, directions per lane, warps per

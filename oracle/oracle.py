@@ -576,3 +576,50 @@ def mlqd_steps(st, Omega_x, Omega_y, quad_weight, Delx, Dely, Nu_g, kappa_mult, 
                          MGQD_norms=lo_norms))
     st["KapE"], st["MGQD_Src"] = KapE, MGQD_Src
     return hist
+
+
+# ------------------------------------------------------------------------------------------------
+# Reduced-order model: POD of snapshots and its reconstruction.
+# ------------------------------------------------------------------------------------------------
+
+def pod_calc(data, n_t, n_g, clen, g):
+    """POD_Calc with SVD_Calc_Cntr (Decomposer/DecompSrc/POD_ROUTINES.c:75-120, LA_ROUTINES.c:50-170): the
+    columns of block g (gdat_reform, LA_ROUTINES.c:279-294) of data(clen, n_g, n_t) (n_g = 0: one block),
+    centred by their mean over t (summed in t order), then the thin SVD (LAPACK, as dgesvd).  Returns
+    (center(clen), umat(clen, k), sig(k), vtmat(k, n_t)), k = min(clen, n_t)."""
+    ng = max(n_g, 1)
+    d = np.asarray(data, dtype=np.float64).reshape(-1, order="F")
+    X = np.empty((clen, n_t), order="F")
+    for t in range(n_t):
+        p = g * clen + t * ng * clen
+        X[:, t] = d[p:p + clen]
+    center = np.zeros(clen)
+    for t in range(n_t):
+        center = center + X[:, t]
+    center = center / float(n_t)
+    Xc = X - center[:, None]
+    U, S, VT = np.linalg.svd(Xc, full_matrices=False)
+    return center, F(U), S.copy(), F(VT)
+
+
+def pod_reconstruct(C, S, U, V, rank, length, N_g, N_t, t, PODgsum):
+    """POD_RECONSTRUCT (MainSrc/POD_ROUTINES.f08:372-432), with its loop order: modes in order, each term
+    (S U) V added to a zeroed vector, then the centring vector; t is 1-based."""
+    C, S, U, V = (np.asarray(a, dtype=np.float64).reshape(-1, order="F") for a in (C, S, U, V))
+    dat = np.zeros(length)
+    if PODgsum == 0:
+        glen = length // N_g
+        p2 = p3 = 0
+        for g in range(N_g):
+            rg = int(rank[g])
+            p4 = N_t * p3 + (t - 1) * rg
+            for r in range(rg):
+                seg = slice(g * glen, (g + 1) * glen)
+                dat[seg] = dat[seg] + (S[p3 + r] * U[p2:p2 + glen]) * V[p4 + r]
+                p2 += glen
+            p3 += rg
+    else:
+        r1 = int(rank[0])
+        for r in range(r1):
+            dat = dat + (S[r] * U[r * length:(r + 1) * length]) * V[r + (t - 1) * r1]
+    return dat + C

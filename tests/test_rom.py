@@ -1,0 +1,155 @@
+"""Reduced-order model path: the POD of snapshots (the decomposer's POD_Calc with SVD_Calc_Cntr,
+Decomposer/DecompSrc/POD_ROUTINES.c:75-120, LA_ROUTINES.c:50-170) and POD_RECONSTRUCT
+(MainSrc/POD_ROUTINES.f08:372-432), on the device (trt_pod_calc, trt_pod_reconstruct) against the oracle
+(oracle.pod_calc: centring in the decomposer's order + LAPACK SVD; oracle.pod_reconstruct: the Fortran loop).
+
+Singular values agree to 1e-12 of the largest; singular vectors are unique only up to sign (and only where
+the singular values are separated), so they are compared after aligning signs, on well-separated spectra.
+The centring vector and the reconstruction follow the reference's operation order and agree bit for bit.
+"""
+import numpy as np
+import pytest
+
+from common import pkg
+
+
+def snapshots(clen, n_g, n_t, seed, decay=0.5):
+    """data(clen, n_g, n_t): per block a mean field plus modes with geometrically decaying singular values
+    (ratio `decay`, so each is separated from the next); the time coefficients have zero mean, so the
+    centred matrix has exactly these singular values."""
+    rng = np.random.default_rng(seed)
+    out = np.empty((clen, max(n_g, 1), n_t), order="F")
+    for g in range(max(n_g, 1)):
+        k = min(clen, n_t - 1)
+        Q1, _ = np.linalg.qr(rng.standard_normal((clen, k)))
+        Q2, _ = np.linalg.qr(np.hstack([np.ones((n_t, 1)), rng.standard_normal((n_t, k))]))
+        s = 3.0 * decay ** np.arange(k) * (1 + 0.1 * g)
+        out[:, g, :] = 0.3 + rng.standard_normal((clen, 1)) * 0.01 + (Q1 * s) @ Q2[:, 1:k + 1].T
+    return out
+
+
+def align(A, B):
+    """Flip the columns of A to the signs of B."""
+    sgn = np.sign(np.sum(A * B, axis=0))
+    sgn[sgn == 0] = 1.0
+    return A * sgn
+
+
+# ------------------------------------------------------------------------------------------------ CPU
+
+def test_oracle_pod_reproduces_the_snapshots(oracle):
+    data = snapshots(40, 3, 12, 1)
+    for g in range(3):
+        c, u, s, vt = oracle.pod_calc(data, 12, 3, 40, g)
+        assert np.all(np.diff(s) <= 0)
+        np.testing.assert_allclose(c[:, None] + (u * s) @ vt, data[:, g, :], rtol=0, atol=1e-13)
+        for t in range(1, 13):   # full-rank reconstruction of block g at every time level
+            r = oracle.pod_reconstruct(c, s, u, vt, [len(s)], 40, 1, 12, t, 1)
+            np.testing.assert_allclose(r, data[:, g, t - 1], rtol=0, atol=1e-13)
+
+
+def test_oracle_groupwise_reconstruction_layout(oracle):
+    clen, ng, nt, rank = 30, 3, 8, [2, 4, 3]
+    data = snapshots(clen, ng, nt, 2)
+    C, S, U, V = [], [], [], []
+    for g in range(ng):
+        c, u, s, vt = oracle.pod_calc(data, nt, ng, clen, g)
+        C.append(c)
+        S.append(s[:rank[g]])
+        U.append(u[:, :rank[g]].ravel(order="F"))
+        V.append(vt[:rank[g]].ravel(order="F"))
+    for t in (1, 5, 8):
+        r = oracle.pod_reconstruct(np.concatenate(C), np.concatenate(S), np.concatenate(U), np.concatenate(V), rank,
+                                   clen * ng, ng, nt, t, 0)
+        for g in range(ng):
+            c, u, s, vt = oracle.pod_calc(data, nt, ng, clen, g)
+            k = rank[g]
+            np.testing.assert_allclose(r[g * clen:(g + 1) * clen], c + (u[:, :k] * s[:k]) @ vt[:k, t - 1],
+                                       rtol=0, atol=1e-13)
+
+
+# ------------------------------------------------------------------------------------------------ GPU
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(500, 0, 20, 0), (300, 4, 16, 2), (12, 2, 30, 1), (1, 0, 5, 0)])
+def test_device_pod_matches_oracle(oracle, shape):
+    clen, ng, nt, g = shape
+    data = snapshots(clen, ng, nt, 3 + clen)
+    c, u, s, vt = pkg.POD_Calc(data, nt, ng, clen, g)
+    rc, ru, rs, rvt = oracle.pod_calc(data, nt, ng, clen, g)
+    assert np.array_equal(c, rc)
+    np.testing.assert_allclose(s, rs, rtol=0, atol=1e-12 * rs[0])
+    k = int(np.sum(rs > 1e-10 * rs[0]))   # the modes the data carries (the rest are round-off)
+    np.testing.assert_allclose(align(u[:, :k], ru[:, :k]), ru[:, :k], rtol=0, atol=1e-9)
+    np.testing.assert_allclose(align(vt[:k].T, rvt[:k].T), rvt[:k].T, rtol=0, atol=1e-9)
+    # the decomposition reproduces the data
+    blk = data[:, g, :] if ng else data[:, 0, :]
+    np.testing.assert_allclose(c[:, None] + (u * s) @ vt, blk, rtol=0, atol=1e-12 * np.abs(blk).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("gsum", [0, 1])
+def test_device_pod_reconstruct_bit_identical(oracle, gsum):
+    clen, ng, nt = 64, 3, 10
+    data = snapshots(clen, ng, nt, 9)
+    if gsum == 0:
+        rank = [3, 5, 2]
+        parts = [oracle.pod_calc(data, nt, ng, clen, g) for g in range(ng)]
+        C = np.concatenate([p[0] for p in parts])
+        S = np.concatenate([p[2][:r] for p, r in zip(parts, rank)])
+        U = np.concatenate([p[1][:, :r].ravel(order="F") for p, r in zip(parts, rank)])
+        V = np.concatenate([p[3][:r].ravel(order="F") for p, r in zip(parts, rank)])
+        length = clen * ng
+    else:
+        whole = data.reshape(clen * ng, 1, nt, order="F")
+        c, u, s, vt = oracle.pod_calc(whole, nt, 0, clen * ng, 0)
+        rank = [7]
+        C, S, U, V = c, s[:7], u[:, :7].ravel(order="F"), vt[:7].ravel(order="F")
+        length = clen * ng
+    for t in (1, 4, nt):
+        out = np.zeros(length)
+        pkg.POD_RECONSTRUCT(out, C, S, U, V, rank, length, ng, nt, t, gsum)
+        assert np.array_equal(out, oracle.pod_reconstruct(C, S, U, V, rank, length, ng, nt, t, gsum))
+
+
+@pytest.mark.gpu
+def test_rom_of_qd_factor_snapshots_from_the_device_time_loop(oracle):
+    """Snapshots of fg_avg_xx from device time steps (the transport-only loop on a small problem), kept in
+    HBM, decomposed by trt_pod_calc_device; a truncated POD reproduces the snapshots to its tail energy."""
+    import ctypes
+    import torch
+    P = pkg.problems
+    prob = P.random_small(51, 12, 10, 3, "S8")
+    ts = P.fc_timestep_setup(prob)
+    ox, oy, w = prob.directions()
+    nt = 8
+    clen = prob.nx * prob.ny
+    snaps = torch.empty((nt, prob.ng, clen), dtype=torch.float64, device="cuda")
+    with pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng) as s:
+        s.init_state(ts.Tini_eV, list(ts.bcT_eV), P.COMP_UNIT, ts.nu_eV)
+        s.tstep_setup(ts.nu_eV, ts.kappa_mult, ts.cv, np.full((prob.nx, prob.ny), ts.Tini_eV), ts.Kap0, P.COMP_UNIT,
+                      P.C_LIGHT, ts.dt, bcT=ts.bcT_eV, conv_type=2, conv_ho=1e-8, maxit_rte=30)
+        host = []
+        for t in range(nt):
+            s.tstep()
+            f = s.moments(["fg_avg_xx"])["fg_avg_xx"]            # (nx, ny, ng)
+            host.append(f)
+            # the snapshot store: column t of every group, in the decomposer's (clen, n_g, n_t) layout
+            snaps[t].copy_(torch.from_numpy(np.ascontiguousarray(f.reshape(clen, prob.ng, order="F").T)))
+    data = np.stack([h.reshape(clen, prob.ng, order="F") for h in host], axis=2)   # (clen, ng, nt)
+    g = 1
+    k = min(clen, nt)
+    outs = [torch.empty(n, dtype=torch.float64, device="cuda") for n in (clen, clen * k, k, k * nt)]
+    L = pkg.lib()
+    assert L.trt_pod_calc_device(ctypes.c_void_p(snaps.data_ptr()), nt, prob.ng, clen, g,
+                                 *[ctypes.c_void_p(o.data_ptr()) for o in outs], None) == 0
+    torch.cuda.synchronize()
+    c, u, sg, vt = (o.cpu().numpy() for o in outs)
+    u, vt = u.reshape(clen, k, order="F"), vt.reshape(k, nt, order="F")
+    rc, ru, rs, rvt = oracle.pod_calc(data, nt, prob.ng, clen, g)
+    assert np.array_equal(c, rc)
+    np.testing.assert_allclose(sg, rs, rtol=0, atol=1e-12 * rs[0])
+    r = 3
+    X = data[:, g, :]
+    approx = c[:, None] + (u[:, :r] * sg[:r]) @ vt[:r]
+    assert np.linalg.norm(approx - X) == pytest.approx(np.sqrt(np.sum(rs[r:] ** 2)), rel=1e-6, abs=1e-13)
