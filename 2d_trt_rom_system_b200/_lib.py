@@ -67,7 +67,7 @@ class MlqdParams(ctypes.Structure):
                 ("maxit_mloqd", ctypes.c_int), ("maxit_gloqd", ctypes.c_int), ("chi", ctypes.c_double),
                 ("line_src", ctypes.c_double), ("E_bound_low", ctypes.c_double), ("T_bound_low", ctypes.c_double),
                 ("use_line_search", ctypes.c_int), ("use_safety_search", ctypes.c_int),
-                ("kapE_dT_flag", ctypes.c_int), ("theta", ctypes.c_double)]
+                ("kapE_dT_flag", ctypes.c_int), ("theta", ctypes.c_double), ("ho_form", ctypes.c_int)]
 
 
 class MlqdStats(ctypes.Structure):
@@ -153,6 +153,7 @@ SIGNATURES = {
     "trt_mlqd_step": (_i, [_P, ctypes.POINTER(MlqdStats)]),
     "trt_mlqd_counts": (_i, [_P, _I, _i, _I, _i, _I, _I]),
     "trt_mlqd_get": (_i, [_P, ctypes.c_char_p, _D, ctypes.c_longlong]),
+    "trt_mlqd_put": (_i, [_P, ctypes.c_char_p, _P, ctypes.c_longlong, _i]),
 }
 
 _lib = None

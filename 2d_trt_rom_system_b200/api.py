@@ -443,13 +443,13 @@ class TransportSweep:
 
     def mlqd_setup(self, Tini, conv_lo=1e-10, conv_gr1=1e-14, conv_gr2=1e-15, maxit_mloqd=50, maxit_gloqd=20,
                    chi=0.7, line_src=2.0, E_Bound_Low=0.0, T_Bound_Low=0.0, use_line_search=True,
-                   use_safety_search=False, kapE_dT_flag=True, Theta=1.0):
+                   use_safety_search=False, kapE_dT_flag=True, Theta=1.0, ho_form=0):
         """Device time stepping with the reference's run_type 'mlqd' (after init_state and tstep_setup):
         the initial low-order state of MGQD_INIT / GQD_INIT at Tini."""
         p = _lib.MlqdParams(float(conv_lo), float(conv_gr1), float(conv_gr2), int(maxit_mloqd), int(maxit_gloqd),
                             float(chi), float(line_src), float(E_Bound_Low), float(T_Bound_Low),
                             int(bool(use_line_search)), int(bool(use_safety_search)), int(bool(kapE_dT_flag)),
-                            float(Theta))
+                            float(Theta), int(ho_form))
         check(_lib.lib().trt_mlqd_setup(self._h, float(Tini), ctypes.byref(p)), "trt_mlqd_setup")
 
     def mlqd_step(self):
@@ -465,6 +465,12 @@ class TransportSweep:
         out["mgqd_per_outer"] = a[:n1.value].tolist()
         out["egp_per_mgqd"] = b[:n2.value].tolist()
         return out
+
+    def mlqd_put(self, name, values):
+        """Overwrite a QD or boundary factor field (fg_*, Cg_*) from a host array (trt_mlqd_put)."""
+        a = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(-1, order="F"))
+        check(_lib.lib().trt_mlqd_put(self._h, name.encode(), a.ctypes.data_as(ctypes.c_void_p), a.size, 0),
+              "trt_mlqd_put")
 
     def mlqd_field(self, name):
         """A field of the device mlqd state (trt_mlqd_get), Fortran layout."""

@@ -1186,7 +1186,7 @@ int mlqd_step_impl(Mlqd& m, trt_mlqd_stats* out) {
   double tn = 0.0, en = 0.0;
   while (!rt_conv && rt < v.maxit_rte) {
     ++rt;
-    if (rt >= 2) {   // RT_start_Its = 2
+    if (m.p.ho_form == 0 && rt >= 2) {   // RT_start_Its = 2; with ho_form 1 the factors are the caller's
       MG_CUDA(cudaEventRecord(m.ev[2], st));
       if ((rc = trt_host::handle_outer_sweep(m.h, rt == 2))) return rc;
       MG_CUDA(cudaEventRecord(m.ev[3], st));
@@ -1249,7 +1249,7 @@ int mlqd_step_impl(Mlqd& m, trt_mlqd_stats* out) {
     }
     m.mg_counts.push_back(mg);
     S.mgqd_its += mg;
-    if (rt >= 2) {
+    if (m.p.ho_form == 0 && rt >= 2) {
       float ms = 0.f;
       MG_CUDA(cudaEventElapsedTime(&ms, m.ev[2], m.ev[3]));
       sweep_ms += ms;
@@ -1278,6 +1278,7 @@ extern "C" {
 
 int trt_mlqd_setup(trt_ctx* ctx, double Tini, const trt_mlqd_params* p) {
   if (!ctx || !p || !(Tini >= 0.0) || p->maxit_mloqd < 1 || p->maxit_gloqd < 1 || !(p->conv_lo >= 0.0) ||
+      (p->ho_form != 0 && p->ho_form != 1) ||
       !(p->conv_gr1 >= 0.0) || !(p->conv_gr2 >= 0.0) || !(p->theta > 0.0) ||
       ((p->use_line_search || p->use_safety_search) && !(p->line_src > 1.0)))
     return TRT_ERR_ARG;
@@ -1305,6 +1306,28 @@ int trt_mlqd_counts(trt_ctx* ctx, int* mgqd_per_outer, int cap_outer, int* egp_p
   if (n_outer) *n_outer = (int)m->mg_counts.size();
   if (n_mgqd) *n_mgqd = (int)m->egp_counts.size();
   return TRT_OK;
+}
+
+int trt_mlqd_put(trt_ctx* ctx, const char* name, const double* src, long long count, int on_device) {
+  if (!ctx || !name || !src) return TRT_ERR_ARG;
+  Mlqd* m = static_cast<Mlqd*>(trt_host::handle_attached(ctx));
+  if (!m) return TRT_ERR_STATE;
+  const Dims& d = m->d;
+  const long long ng = d.ng;
+  static const char* names[10] = {"fg_avg_xx", "fg_avg_yy", "fg_edgV_xx", "fg_edgV_xy", "fg_edgH_yy",
+                                  "fg_edgH_xy", "Cg_L",      "Cg_B",       "Cg_R",       "Cg_T"};
+  const long long sizes[10] = {d.nC * ng, d.nC * ng, d.nV * ng, d.nV * ng, d.nH * ng,
+                               d.nH * ng, d.ny * ng, d.nx * ng, d.ny * ng, d.nx * ng};
+  for (int k = 0; k < 10; ++k)
+    if (std::strcmp(names[k], name) == 0) {
+      if (count != sizes[k]) return TRT_ERR_ARG;
+      double* dst = const_cast<double*>(k < 6 ? m->f[k] : m->Cg[k - 6]);
+      MG_CUDA(cudaMemcpyAsync(dst, src, (size_t)count * sizeof(double),
+                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, m->v.stream));
+      MG_CUDA(cudaStreamSynchronize(m->v.stream));
+      return TRT_OK;
+    }
+  return TRT_ERR_ARG;
 }
 
 int trt_mlqd_get(trt_ctx* ctx, const char* name, double* host, long long count) {

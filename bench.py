@@ -67,6 +67,9 @@ def parse():
     p.add_argument("--mlqd-steps", type=int, default=2,
                    help="time steps of the mlqd algorithm (sweep + MGQD/grey low-order iterations) on the "
                         "configuration's grid, mixed vs FP64; 0 = skip")
+    p.add_argument("--pod-snapshots", type=int, default=20,
+                   help="time levels of the POD leg (per-group POD of fg-sized snapshots on the configuration's "
+                        "grid and groups, device vs the oracle's LAPACK SVD); 0 = skip")
     p.add_argument("--time-steps", type=int, default=10,
                    help="time steps of the transport-only time loop (mixed vs FP64 temperature error); 0 = skip")
     return p.parse_args()
@@ -323,6 +326,52 @@ def run_mlqd(pkg, torch, prob, steps, conv_ho=1e-8, conv_lo=1e-9, maxit_rte=10, 
                    "mgqd_nonconv": sum(x["mgqd_nonconv"] for x in sts),
                    "egp_nonconv": sum(x["egp_nonconv"] for x in sts),
                    "updates_per_s": float(prob.updates_per_sweep() * sum(x["sweeps"] for x in sts) / (lat.sum() * 1e-3))}
+    return r
+
+
+def run_pod(pkg, torch, prob, nt, cpu_groups=4):
+    """The decomposer's POD (POD_Calc + SVD_Calc_Cntr) of fg-sized snapshots resident in HBM: data
+    (nx*ny, n_g, n_t), every group decomposed by trt_pod_calc_device; the oracle (numpy/LAPACK SVD) on a
+    few groups on the host for the CPU figure.  Synthetic snapshots: a mean field plus decaying modes."""
+    import ctypes
+    clen, ng = prob.nx * prob.ny, prob.ng
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    k = min(clen, nt)
+    modes = torch.randn(clen, 8, device="cuda", dtype=torch.float64, generator=gen)
+    coef = torch.randn(8, ng * nt, device="cuda", dtype=torch.float64, generator=gen) * \
+        (0.3 ** torch.arange(8, device="cuda", dtype=torch.float64))[:, None]
+    # row g + ng * t of this (ng * nt, clen) row-major tensor is column (g, t) of data(clen, ng, nt)
+    data = (1.0 / 3.0 + 1e-2 * (modes @ coef)).T.contiguous()
+    outs = [torch.empty(n, dtype=torch.float64, device="cuda") for n in (clen, clen * k, k, k * nt)]
+    L = pkg.lib()
+    ptrs = [ctypes.c_void_p(o.data_ptr()) for o in outs]
+
+    def one(g):
+        assert L.trt_pod_calc_device(ctypes.c_void_p(data.data_ptr()), nt, ng, clen, g, *ptrs, None) == 0
+
+    one(0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for g in range(ng):
+        one(g)
+    torch.cuda.synchronize()
+    dev_s = (time.perf_counter() - t0) / ng
+    r = {"workload": f"POD per group of {nt} snapshots of {prob.nx}x{prob.ny} values x {ng} groups (fg-sized), "
+                     "resident in HBM", "metric": "group PODs/s", "value": 1.0 / dev_s, "ms_per_group": dev_s * 1e3,
+         "path": "trt_pod_calc_device: centring kernel + cuSOLVER gesvd (m = cells, n = snapshots)"}
+    try:
+        sys.path.insert(0, ROOT)
+        from oracle import oracle as O
+        flat = data.cpu().numpy().reshape(-1)   # memory order = data(clen, ng, nt) in Fortran order
+        O.pod_calc(flat, nt, ng, clen, 0)
+        t0 = time.perf_counter()
+        for g in range(cpu_groups):
+            O.pod_calc(flat, nt, ng, clen, g)
+        cpu_s = (time.perf_counter() - t0) / cpu_groups
+        r["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "group PODs/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"{cpu_groups} groups, numpy centring + LAPACK SVD (threaded BLAS)"}
+    except Exception as exc:   # the CPU figure is context, not the measurement
+        r["cpu_baseline"] = {"error": repr(exc)}
     return r
 
 
@@ -692,6 +741,11 @@ def main():
             line["mlqd"] = run_mlqd(pkg, torch, prob, args.mlqd_steps)
         except Exception as exc:   # reported, not fatal to the headline line
             line["mlqd"] = {"error": repr(exc)}
+    if args.pod_snapshots > 0 and ws == 1:
+        try:
+            line["pod"] = run_pod(pkg, torch, prob, args.pod_snapshots)
+        except Exception as exc:
+            line["pod"] = {"error": repr(exc)}
     if args.mgqd > 0 and ws == 1:
         line["mgqd"] = run_mgqd(pkg, args.mgqd, prob.nx, prob.ng, cpu=rank == 0 and not args.no_cpu_baseline)
     if args.serving > 0 and ws == 1:

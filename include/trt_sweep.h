@@ -401,6 +401,9 @@ typedef struct trt_mlqd_params {
   double E_bound_low, T_bound_low;
   int use_line_search, use_safety_search, kapE_dT_flag;
   double theta;                /* time-integration weight (1 = backward Euler) */
+  int ho_form;                 /* 0: the sweep supplies fg and Cg (run_type 'mlqd', RT_start_Its 2); 1: fg and
+                                  Cg are held as the caller last set them with trt_mlqd_put, no sweep runs
+                                  (HO_Form 1/3/4 with RT_start_Its 1: the POD / DMD / file-driven runs) */
 } trt_mlqd_params;
 typedef struct trt_mlqd_stats {
   int rt_its;          /* outer iterations of the step */
@@ -426,6 +429,11 @@ int trt_mlqd_counts(trt_ctx* ctx, int* mgqd_per_outer, int cap_outer, int* egp_p
  * multigroup "Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH", "MGQD_Src", "MGQD_E_avg", and the
  * transport "HO_E_avg".  `count` is the number of doubles the caller provides (checked). */
 int trt_mlqd_get(trt_ctx* ctx, const char* name, double* host, long long count);
+/* Overwrite a QD-factor or boundary-factor field of the handle ("fg_avg_xx", "fg_avg_yy", "fg_edgV_xx",
+ * "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy", "Cg_L", "Cg_B", "Cg_R", "Cg_T"; Fortran layout, `count` values)
+ * from host memory (on_device = 0) or device memory (1): the factors a ROM reconstructs (POD_RECONSTRUCT_fg,
+ * POD_RECONSTRUCT_BCg, MainSrc/POD_ROUTINES.f08:28-353) before an ho_form = 1 step. */
+int trt_mlqd_put(trt_ctx* ctx, const char* name, const double* src, long long count, int on_device);
 
 /* ---- Reduced-order model: POD of QD-factor snapshots and its reconstruction ----------------------
  * trt_pod_calc replaces the offline decomposer's POD_Calc with SVD_Calc_Cntr

@@ -153,3 +153,49 @@ def test_rom_of_qd_factor_snapshots_from_the_device_time_loop(oracle):
     X = data[:, g, :]
     approx = c[:, None] + (u[:, :r] * sg[:r]) @ vt[:r]
     assert np.linalg.norm(approx - X) == pytest.approx(np.sqrt(np.sum(rs[r:] ** 2)), rel=1e-6, abs=1e-13)
+
+
+FACTORS = ("fg_avg_xx", "fg_avg_yy", "fg_edgV_xx", "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy", "Cg_L", "Cg_B", "Cg_R",
+           "Cg_T")
+
+
+@pytest.mark.gpu
+def test_pod_rom_drives_the_low_order_time_loop():
+    """The reference's POD-ROM run (HO_Form 1: each step's QD and boundary factors from POD_RECONSTRUCT
+    instead of a sweep): factors recorded from a full mlqd run, decomposed per group (trt_pod_calc) and
+    rebuilt at every time level (trt_pod_reconstruct, all modes) drive an ho_form = 1 run, which lands on the
+    full run's temperatures (both converge the same low-order problem to the iteration tolerances)."""
+    from test_mlqd import device, setup_problem
+    prob, ts, km, bcT, cv = setup_problem(8, 6, 10, "S8", 31)
+    kw = dict(conv_ho=1e-9, maxit_rte=40, conv_lo=1e-10, maxit_mloqd=80)
+    nt = 3
+    snaps, T_full = {k: [] for k in FACTORS}, []
+    with device(prob, ts, km, bcT, cv, **kw) as s:
+        for _ in range(nt):
+            s.mlqd_step()
+            m = s.moments(list(FACTORS))
+            for k in FACTORS:
+                snaps[k].append(m[k])
+            T_full.append(s.mlqd_field("Temp"))
+    ng = prob.ng
+    rom = {}
+    for k in FACTORS:
+        data = np.stack([a.reshape(-1, ng, order="F") for a in snaps[k]], axis=2)   # (clen, ng, nt)
+        clen = data.shape[0]
+        parts = [pkg.POD_Calc(data, nt, ng, clen, g) for g in range(ng)]
+        rank = [len(p[2]) for p in parts]
+        rom[k] = (clen * ng, np.concatenate([p[0] for p in parts]), np.concatenate([p[2] for p in parts]),
+                  np.concatenate([p[1].ravel(order="F") for p in parts]),
+                  np.concatenate([p[3].ravel(order="F") for p in parts]), rank)
+    with device(prob, ts, km, bcT, cv, ho_form=1, **kw) as s:
+        for t in range(1, nt + 1):
+            for k in FACTORS:
+                length, C, S, U, V, rank = rom[k]
+                out = np.zeros(length)
+                pkg.POD_RECONSTRUCT(out, C, S, U, V, rank, length, ng, nt, t, 0)
+                assert np.abs(out - snaps[k][t - 1].ravel(order="F")).max() <= 1e-12 * max(1.0, np.abs(out).max())
+                s.mlqd_put(k, out)
+            st = s.mlqd_step()
+            assert st["sweeps"] == 0 and st["mgqd_nonconv"] == 0
+            T = s.mlqd_field("Temp")
+            assert float(np.max(np.abs(T - T_full[t - 1])) / np.max(T_full[t - 1])) < 1e-7
