@@ -9,5 +9,5 @@ from .api import (COLLAPSE_INTENSITIES, COLLAPSE_MG_EF, EGP_FV_NEWT, GQD_In_Calc
                   MGQD_In_Calc, MLOQD_FV, OLD_GREY_COEFS, OLD_MGQD_COEFS, POD_RECONSTRUCT, POD_Calc, RT_BC_UPDATE,
                   TRANSPORT_SCB, Batch,
                   Bg_planck_calc, Cbar_Calc, Cg_Calc, TransportSweep, fg_Calc, kernel_launches, mgqd_last_stats,
-                  mgqd_set_tolerance, required_bytes)
+                  mgqd_set_graphs, mgqd_set_tolerance, required_bytes)
 from ._lib import LIB_PATH, TrtError, check, lib  # noqa: F401

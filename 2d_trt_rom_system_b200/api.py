@@ -280,6 +280,11 @@ def mgqd_set_tolerance(tol=1e-13, maxit=1000):
     check(_lib.lib().trt_mgqd_set_tolerance(float(tol), int(maxit)), "mgqd_set_tolerance")
 
 
+def mgqd_set_graphs(on=True):
+    """Replay the low-order solves' iteration blocks as CUDA graphs (default) or launch kernel by kernel."""
+    check(_lib.lib().trt_mgqd_set_graphs(int(bool(on))), "mgqd_set_graphs")
+
+
 def mgqd_last_stats():
     """(device ms of the last MLOQD_FV solve without its copies, largest iteration count, device ms of
     its first matrix-vector product)."""

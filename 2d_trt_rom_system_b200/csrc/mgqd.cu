@@ -42,6 +42,7 @@ constexpr int kCheckEvery = 4;      // iterations between host checks of the con
 struct Settings {
   double tol = 1e-13;
   int maxit = 1000;
+  bool graphs = true;   // replay BiCGSTAB iteration blocks as CUDA graphs
 };
 Settings g_settings;
 
@@ -61,9 +62,15 @@ struct Solver {
   Scal* h_scal = nullptr;
   float last_ms = 0.f, last_matvec_ms = 0.f;
   bool matvec_timed = false;
+  bool time_matvec = true;          // time the first iteration's matrix-vector product (trt_mgqd_last_stats)
+  bool use_graphs = true;           // replay iteration blocks as a CUDA graph
+  cudaGraphExec_t gexec = nullptr;  // kCheckEvery iterations, recorded on first use
+  int g_nodes = 0, g_maxit = -1;
+  double g_tol = -1.0;
   int last_its = 0;
 
   ~Solver() {
+    if (gexec) cudaGraphExecDestroy(gexec);
     for (void* p : bufs) cudaFree(p);
     if (h_done) cudaFreeHost(h_done);
     if (h_scal) cudaFreeHost(h_scal);
@@ -192,6 +199,7 @@ int Solver::krylov(cudaStream_t s) {
   matvec_timed = false;
   K.tol = g_settings.tol;
   K.maxit = g_settings.maxit;
+  use_graphs = g_settings.graphs;
   prec_coef_kernel<<<gpos, kRedBlock, 0, s>>>(d, cf, ls.L[0]);
   MG_LAUNCHED();
   for (int k = 0; k + 1 < ls.n; ++k) {
@@ -203,36 +211,117 @@ int Solver::krylov(cudaStream_t s) {
   init_finish_kernel<<<ng, 32, 0, s>>>(K, nblk);
   MG_LAUNCHED();
 
+  // Launch bookkeeping: a direct launch is counted at once; a launch recorded into the iteration graph is
+  // counted each time the graph is replayed.
+  int recorded = 0;
+  bool capturing = false;
+  auto launched = [&]() -> int {
+    if (capturing) ++recorded;
+    else trt_host::add_launches(1);
+    MG_CUDA(cudaGetLastError());
+    return TRT_OK;
+  };
   auto vcycle = [&]() -> int {
+    int rc;
     for (int k = 0; k < k0; ++k) {
       const Level& L = ls.L[k];
       const dim3 gl(grid1(L.n), ng);
       for (int sw = 0; sw < kNu1; ++sw) {
         smooth_kernel<<<gl, 256, 0, s>>>(L, K.done, 0, sw == 0 ? 1 : 0);
-        MG_LAUNCHED();
+        if ((rc = launched())) return rc;
         smooth_kernel<<<gl, 256, 0, s>>>(L, K.done, 1, 0);
-        MG_LAUNCHED();
+        if ((rc = launched())) return rc;
       }
       restrict_kernel<<<dim3(grid1(ls.L[k + 1].n), ng), 256, 0, s>>>(L, ls.L[k + 1], K.done);
-      MG_LAUNCHED();
+      if ((rc = launched())) return rc;
     }
     small_vcycle_kernel<<<ng, 256, 0, s>>>(ls, k0, kNu1, kNu2, kCoarseSweeps, K.done);
-    MG_LAUNCHED();
+    if ((rc = launched())) return rc;
     for (int k = k0 - 1; k >= 0; --k) {
       const Level& L = ls.L[k];
       const dim3 gl(grid1(L.n), ng);
       prolong_kernel<<<gl, 256, 0, s>>>(L, ls.L[k + 1], K.done);
-      MG_LAUNCHED();
+      if ((rc = launched())) return rc;
       for (int sw = 0; sw < kNu2; ++sw) {
         smooth_kernel<<<gl, 256, 0, s>>>(L, K.done, 0, 0);
-        MG_LAUNCHED();
+        if ((rc = launched())) return rc;
         smooth_kernel<<<gl, 256, 0, s>>>(L, K.done, 1, 0);
-        MG_LAUNCHED();
+        if ((rc = launched())) return rc;
       }
     }
     return TRT_OK;
   };
+  // One BiCGSTAB iteration; the p vectors alternate with the iteration's parity.  Groups that have
+  // converged (or stopped) skip every kernel, so iterations run past the end leave the result unchanged.
+  auto iteration = [&](int it, bool timed) -> int {
+    int rc;
+    double* pold = (it & 1) ? K.p1 : K.p0;
+    double* pnew = (it & 1) ? K.p0 : K.p1;
+    elim_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, ls.L[0], pold, pnew, 0);
+    if ((rc = launched())) return rc;
+    if ((rc = vcycle())) return rc;
+    backsub_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, ls.L[0], pnew, K.ph);
+    if ((rc = launched())) return rc;
+    if (timed) MG_CUDA(cudaEventRecord(m0, s));
+    matvec_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, K.ph, K.v, 0);
+    if ((rc = launched())) return rc;
+    if (timed) MG_CUDA(cudaEventRecord(m1, s));
+    scalar_finish_kernel<<<ng, 32, 0, s>>>(K, nblk, 0);
+    if ((rc = launched())) return rc;
+    elim_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, ls.L[0], nullptr, K.s, 1);
+    if ((rc = launched())) return rc;
+    if ((rc = vcycle())) return rc;
+    backsub_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, ls.L[0], K.s, K.sh);
+    if ((rc = launched())) return rc;
+    matvec_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, K.sh, K.t, 1);
+    if ((rc = launched())) return rc;
+    scalar_finish_kernel<<<ng, 32, 0, s>>>(K, nblk, 1);
+    if ((rc = launched())) return rc;
+    update_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K);
+    if ((rc = launched())) return rc;
+    update_finish_kernel<<<ng, 32, 0, s>>>(K, nblk);
+    return launched();
+  };
+  // kCheckEvery iterations (an even count, so the parity pattern repeats) recorded once as a CUDA graph and
+  // replayed between the host's convergence checks: the same kernels in the same order, one launch.  The
+  // kernels take the solver's fixed buffers and K by value, so the graph is recorded again only when the
+  // tolerance or the iteration limit in K changes.
+  auto block = [&]() -> int {
+    if (!gexec || g_tol != K.tol || g_maxit != K.maxit) {
+      if (gexec) {
+        cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+      }
+      cudaGraph_t g = nullptr;
+      MG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      capturing = true;
+      recorded = 0;
+      int rc = TRT_OK;
+      for (int k = 0; k < kCheckEvery && !rc; ++k) rc = iteration(k, false);
+      capturing = false;
+      const cudaError_t e = cudaStreamEndCapture(s, &g);
+      if (rc || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return rc ? rc : TRT_ERR_CUDA;
+      }
+      const cudaError_t ei = cudaGraphInstantiate(&gexec, g, 0);
+      cudaGraphDestroy(g);
+      if (ei != cudaSuccess) {
+        gexec = nullptr;
+        cudaGetLastError();
+        return TRT_ERR_CUDA;
+      }
+      g_nodes = recorded;
+      g_tol = K.tol;
+      g_maxit = K.maxit;
+    }
+    MG_CUDA(cudaGraphLaunch(gexec, s));
+    trt_host::add_launches((unsigned long long)g_nodes);
+    return TRT_OK;
+  };
 
+  static_assert(kCheckEvery % 2 == 0, "graph blocks must keep the parity of the p vectors");
   int rc;
   for (int it = 0; it < K.maxit; ++it) {
     if (it % kCheckEvery == 0) {
@@ -241,34 +330,15 @@ int Solver::krylov(cudaStream_t s) {
       bool all = true;
       for (int g = 0; g < ng; ++g) all = all && h_done[g] != 0;
       if (all) break;
+      const bool timed_block = it == 0 && time_matvec;
+      if (use_graphs && !timed_block && it + kCheckEvery <= K.maxit) {
+        if ((rc = block())) return rc;
+        it += kCheckEvery - 1;
+        continue;
+      }
     }
-    double* pold = (it & 1) ? K.p1 : K.p0;
-    double* pnew = (it & 1) ? K.p0 : K.p1;
-    elim_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, ls.L[0], pold, pnew, 0);
-    MG_LAUNCHED();
-    if ((rc = vcycle())) return rc;
-    backsub_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, ls.L[0], pnew, K.ph);
-    MG_LAUNCHED();
-    matvec_timed = matvec_timed || it == 0;
-    if (it == 0) MG_CUDA(cudaEventRecord(m0, s));
-    matvec_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, K.ph, K.v, 0);
-    MG_LAUNCHED();
-    if (it == 0) MG_CUDA(cudaEventRecord(m1, s));
-    scalar_finish_kernel<<<ng, 32, 0, s>>>(K, nblk, 0);
-    MG_LAUNCHED();
-    elim_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, ls.L[0], nullptr, K.s, 1);
-    MG_LAUNCHED();
-    if ((rc = vcycle())) return rc;
-    backsub_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, ls.L[0], K.s, K.sh);
-    MG_LAUNCHED();
-    matvec_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K, K.sh, K.t, 1);
-    MG_LAUNCHED();
-    scalar_finish_kernel<<<ng, 32, 0, s>>>(K, nblk, 1);
-    MG_LAUNCHED();
-    update_kernel<<<gpos, kRedBlock, 0, s>>>(cf, d, K);
-    MG_LAUNCHED();
-    update_finish_kernel<<<ng, 32, 0, s>>>(K, nblk);
-    MG_LAUNCHED();
+    if ((rc = iteration(it, it == 0 && time_matvec))) return rc;
+    matvec_timed = matvec_timed || (it == 0 && time_matvec);
   }
   return TRT_OK;
 }
@@ -354,6 +424,12 @@ int trt_mgqd_set_tolerance(double tol, int maxit) {
   std::lock_guard<std::mutex> lk(g_cache.mu);
   g_settings.tol = tol;
   g_settings.maxit = maxit;
+  return TRT_OK;
+}
+
+int trt_mgqd_set_graphs(int on) {
+  std::lock_guard<std::mutex> lk(g_cache.mu);
+  g_settings.graphs = on != 0;
   return TRT_OK;
 }
 
@@ -971,6 +1047,8 @@ int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm) {
   if ((rc = m->MG->init(nx, ny, ng, false))) return rc;
   m->GR = std::make_unique<Solver>();
   if ((rc = m->GR->init(nx, ny, 1, false))) return rc;
+  m->MG->time_matvec = false;   // every iteration block of the time loop's solves runs as a graph
+  m->GR->time_matvec = false;
   const size_t C = (size_t)d.nC * ng, V = (size_t)d.nV * ng, H = (size_t)d.nH * ng;
   const size_t c1 = d.nC, v1 = d.nV, hh1 = d.nH;
   const size_t side[4] = {(size_t)ny, (size_t)nx, (size_t)ny, (size_t)nx};   // L, B, R, T

@@ -202,6 +202,10 @@ int trt_egp_fv_newt(int n_x, int n_y, double* E_avg, double* E_edgV, double* E_e
 
 /* Convergence settings of trt_mloqd_fv (process-wide): tol > 0, maxit >= 1 iterations per group. */
 int trt_mgqd_set_tolerance(double tol, int maxit);
+/* No counterpart in the reference.  The low-order BiCGSTAB solves (MLOQD_FV, the EGP Newton steps, the mlqd
+ * time step) replay each block of iterations between two host convergence checks as one CUDA graph (on, the
+ * default) or launch its kernels one by one (0); the kernels and their order are the same either way. */
+int trt_mgqd_set_graphs(int on);
 
 /* Of the last trt_mloqd_fv call: device time (ms, events around the solve, excluding host<->device
  * copies), the largest iteration count, and the device time of its first matrix-vector product (ms;

@@ -166,6 +166,23 @@ def test_device_mloqd_fv_is_reproducible_and_guess_independent(oracle):
 
 
 @pytest.mark.gpu
+def test_graph_replayed_iterations_are_bit_identical(oracle):
+    """The iteration blocks replayed as CUDA graphs run the same kernels in the same order as direct launches."""
+    d, c, dt, th = make(48, 40, 6, 1.0, 14, False, oracle)
+    try:
+        pkg.mgqd_set_graphs(False)
+        a = call_device(d, c, dt, th)
+        pkg.mgqd_set_graphs(True)
+        b = call_device(d, c, dt, th)
+        c2 = call_device(d, c, dt, th)   # the recorded graph replayed again
+    finally:
+        pkg.mgqd_set_graphs(True)
+    assert (a["MGQD_Kits"] > 9).any()    # more than one block of iterations
+    for k in ("Eg_avg", "Eg_edgV", "Fxg_edgV", "MGQD_Residual", "MGQD_Kits"):
+        assert np.array_equal(a[k], b[k]) and np.array_equal(b[k], c2[k]), k
+
+
+@pytest.mark.gpu
 def test_device_mloqd_fv_reports_non_convergence(oracle):
     d, c, dt, th = make(16, 16, 3, 1.0, 13, True, oracle)
     try:
