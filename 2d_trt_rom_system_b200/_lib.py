@@ -150,6 +150,9 @@ SIGNATURES = {
                                  _P, _P, _P, _P, _P]),
     "trt_pod_reconstruct": (_i, [_D, _D, _D, _D, _D, _I, _i, _i, _i, _i, _i]),
     "trt_pod_reconstruct_device": (_i, [_P, _P, _P, _P, _P, _P, _P, _i, _i, _i, _i, _P]),
+    "trt_dmd_reconstruct": (_i, [_D, _D, _D, _D, _D, _I, _i, _i, _i, _d]),
+    "trt_dmd_calc": (_i, [_D, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, _i, _d, _d,
+                          ctypes.POINTER(ctypes.c_longlong)] + [_D] * 8),
     "trt_mlqd_setup": (_i, [_P, _d, ctypes.POINTER(MlqdParams)]),
     "trt_mlqd_step": (_i, [_P, ctypes.POINTER(MlqdStats)]),
     "trt_mlqd_counts": (_i, [_P, _I, _i, _I, _i, _I, _I]),

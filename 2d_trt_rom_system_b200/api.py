@@ -314,6 +314,38 @@ def POD_RECONSTRUCT(dat, C, S, U, V, rank, len_, N_g, N_t, t, PODgsum):
                                          int(t), int(PODgsum)), "trt_pod_reconstruct")
 
 
+def DMD_Calc(data, N_t, N_g, clen, g, base_subtract=0, svd_eps=-1.0, delt=1.0):
+    """DMD of block g of data(clen, N_g, N_t) (trt_dmd_calc).  Returns a dict with lambda, omega, b (xr),
+    wmat, wmat_proj (clen, xr) complex, umat (clen, xr), wmat_tild (xr, xr) complex, cvec (clen)."""
+    shift = 2 if base_subtract else 1
+    k = min(clen, N_t - shift)
+    d = np.ascontiguousarray(np.asarray(data, dtype=np.float64).reshape(-1, order="F"))
+    if d.size != clen * max(N_g, 1) * N_t:
+        raise ValueError("data holds the wrong number of values")
+    lam, om, b = (np.zeros(k, dtype=np.complex128) for _ in range(3))
+    wm, wp = np.zeros(clen * k, dtype=np.complex128), np.zeros(clen * k, dtype=np.complex128)
+    um, wt, cv = np.zeros(clen * k), np.zeros(k * k, dtype=np.complex128), np.zeros(clen)
+    nm = ctypes.c_longlong(0)
+    f = lambda a: a.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    check(_lib.lib().trt_dmd_calc(dptr(d), int(N_t), int(N_g), int(clen), int(g), int(bool(base_subtract)),
+                                  float(svd_eps), float(delt), ctypes.byref(nm), f(lam), f(om), f(b), f(wm), f(wp),
+                                  dptr(um), f(wt), dptr(cv)), "trt_dmd_calc")
+    xr = nm.value
+    return dict(lambda_=lam[:xr], omega=om[:xr], b=b[:xr], wmat=wm[:clen * xr].reshape(clen, xr, order="F"),
+                wmat_proj=wp[:clen * xr].reshape(clen, xr, order="F"), umat=um[:clen * xr].reshape(clen, xr, order="F"),
+                wmat_tild=wt[:xr * xr].reshape(xr, xr, order="F"), cvec=cv)
+
+
+def DMD_RECONSTRUCT(dat, L, B, W, C, rank, len_, N_g, DMDgsum, Time):
+    """trt_dmd_reconstruct into dat (float64, len_ values); L, B, W complex."""
+    r = np.ascontiguousarray(rank, dtype=np.int32)
+    cplx = [np.ascontiguousarray(np.asarray(a, dtype=np.complex128).reshape(-1, order="F")).view(np.float64)
+            for a in (L, B, W)]
+    c = np.ascontiguousarray(np.asarray(C, dtype=np.float64).reshape(-1, order="F"))
+    check(_lib.lib().trt_dmd_reconstruct(dptr(dat), *[dptr(a) for a in cplx], dptr(c), iptr(r), int(len_), int(N_g),
+                                         int(DMDgsum), float(Time)), "trt_dmd_reconstruct")
+
+
 def Bg_planck_calc(T, nu_low, nu_high, comp_unit):
     """FUNCTION Bg_planck_calc, MainSrc/TEMP_FUNCTIONS.f08:90-108 (host evaluation in the library)."""
     return _lib.lib().trt_bg_planck(float(T), float(nu_low), float(nu_high), float(comp_unit))

@@ -17,7 +17,7 @@ HEADERS = ["aux_kernels.cuh", "dropin_kernels.cuh", "gqd_kernels.cuh", "handle_h
            "ptx.cuh", "scb_cell.h",
            "sweep_kernel.cuh", "tstep_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-LIBS = ["-lcusolver"]   # the SVD of the POD (rom.cu)
+LIBS = ["-lcusolver", "-lcublas"]   # the SVD / eigenpairs / products of POD and DMD (rom.cu)
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-shared",
               "-diag-suppress", "177"]
 

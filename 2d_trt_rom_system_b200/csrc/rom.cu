@@ -2,10 +2,15 @@
 // decomposer computes (POD_Calc with SVD_Calc_Cntr, Decomposer/DecompSrc/POD_ROUTINES.c:75-120 and
 // LA_ROUTINES.c:50-170) and the online reconstruction of a snapshot from it (POD_RECONSTRUCT,
 // MainSrc/POD_ROUTINES.f08:372-432).  Declarations and contracts: include/trt_sweep.h.
+#include <cublas_v2.h>
+#include <cuComplex.h>
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
 #include <vector>
 
 #include "trt_sweep.h"
@@ -69,6 +74,32 @@ __global__ void pod_reconstruct_kernel(long long glen, int n_blocks, int n_t, in
     double acc = 0.0;
     for (int r = 0; r < rg; ++r) acc = acc + (S[o + r] * Ug[i + glen * r]) * Vg[r];
     dat[k] = acc + C[k];
+  }
+}
+
+// DMD_RECONSTRUCT: dat(i) = Re( sum_r B(r) W(i, r) exp(L(r) Time) ) + C(i), modes in order, each term formed as
+// (B W) e with the complex products written out as the reference's COMPLEX*16 arithmetic does (re = ac - bd,
+// im = ad + bc).  e(r) = exp(L(r) Time) is computed once per mode by the host and passed in.  Groupwise
+// (n_blocks > 1): block g has rank(g) modes packed after the earlier blocks' (offsets off[g]).
+__global__ void dmd_reconstruct_kernel(long long glen, int n_blocks, const int* __restrict__ rank,
+                                       const long long* __restrict__ off, const double* __restrict__ C,
+                                       const double2* __restrict__ B, const double2* __restrict__ W,
+                                       const double2* __restrict__ E, double* __restrict__ dat) {
+  const long long n = glen * n_blocks;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int g = (int)(k / glen);
+    const long long i = k % glen;
+    const long long o = off[g];
+    const double2* Wg = W + glen * o;
+    double re = 0.0, im = 0.0;
+    for (int r = 0; r < rank[g]; ++r) {
+      const double2 b = B[o + r], w = Wg[i + glen * r], e = E[o + r];
+      const double pr = b.x * w.x - b.y * w.y, pi = b.x * w.y + b.y * w.x;   // B W
+      const double tr = pr * e.x - pi * e.y, ti = pr * e.y + pi * e.x;       // (B W) e
+      re = re + tr;
+      im = im + ti;
+    }
+    dat[k] = re + C[k];
   }
 }
 
@@ -245,6 +276,323 @@ int trt_pod_reconstruct_device(double* dat, const double* C, const double* S, co
   trt_host::add_launches(1);
   ROM_CUDA(cudaGetLastError());
   ROM_CUDA(cudaStreamSynchronize(st));
+  return TRT_OK;
+}
+
+int trt_dmd_reconstruct(double* dat, const double* L, const double* B, const double* W, const double* C,
+                        const int* rank, int len, int N_g, int DMDgsum, double Time) {
+  if (!dat || !L || !B || !W || !C || !rank || len < 1 || (DMDgsum != 0 && DMDgsum != 1) ||
+      (DMDgsum == 0 && (N_g < 1 || len % N_g != 0)))
+    return TRT_ERR_ARG;
+  int rc = device_present();
+  if (rc) return rc;
+  const int nb = DMDgsum == 0 ? N_g : 1;
+  const long long glen = len / nb;
+  std::vector<long long> off(nb);
+  long long tot = 0;
+  for (int g = 0; g < nb; ++g) {
+    if (rank[g] < 0) return TRT_ERR_ARG;
+    off[g] = tot;
+    tot += rank[g];
+  }
+  // exp(L(r) Time) once per mode (the reference evaluates it once per mode too, before the value loop)
+  std::vector<double> E(2 * (size_t)tot);
+  for (long long r = 0; r < tot; ++r) {
+    const double zr = L[2 * r] * Time, zi = L[2 * r + 1] * Time;
+    const double m = std::exp(zr);
+    E[2 * r] = m * std::cos(zi);
+    E[2 * r + 1] = m * std::sin(zi);
+  }
+  Dev dv;
+  double *dC, *dB, *dW, *dE, *dd;
+  int* dr;
+  long long* doff;
+  if ((rc = dv.get(&dC, (size_t)len)) || (rc = dv.get(&dB, 2 * (size_t)tot)) ||
+      (rc = dv.get(&dW, 2 * (size_t)(glen * tot))) || (rc = dv.get(&dE, 2 * (size_t)tot)) ||
+      (rc = dv.get(&dd, (size_t)len)) || (rc = dv.get(&dr, (size_t)nb)) || (rc = dv.get(&doff, (size_t)nb)))
+    return rc;
+  ROM_CUDA(cudaMemcpy(dC, C, (size_t)len * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dB, B, 2 * (size_t)tot * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dW, W, 2 * (size_t)(glen * tot) * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dE, E.data(), E.size() * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dr, rank, (size_t)nb * sizeof(int), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(doff, off.data(), (size_t)nb * sizeof(long long), cudaMemcpyHostToDevice));
+  dmd_reconstruct_kernel<<<grid_of(len), 256>>>(glen, nb, dr, doff, dC, reinterpret_cast<const double2*>(dB),
+                                               reinterpret_cast<const double2*>(dW),
+                                               reinterpret_cast<const double2*>(dE), dd);
+  trt_host::add_launches(1);
+  ROM_CUDA(cudaGetLastError());
+  ROM_CUDA(cudaMemcpy(dat, dd, (size_t)len * sizeof(double), cudaMemcpyDeviceToHost));
+  return TRT_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// DMD of snapshots: DMD_Calc, Coef_Calc and Omega_Calc (Decomposer/DecompSrc/DMD_ROUTINES.c:100-470).
+// ------------------------------------------------------------------------------------------------
+
+namespace {
+
+using cplx = std::complex<double>;
+
+// dst = (double2) src for n values.
+__global__ void to_complex_kernel(long long n, const double* __restrict__ src, double2* __restrict__ dst) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    dst[k] = make_double2(src[k], 0.0);
+}
+
+// Column j of the (rows x cols) complex matrix M divided by lam(j) (complex division as C's operator/).
+__global__ void divide_columns_kernel(long long rows, int cols, double2* __restrict__ M, const double2* __restrict__ lam) {
+  const long long n = rows * cols;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const double2 l = lam[k / rows];
+    M[k] = cuCdiv(M[k], l);
+  }
+}
+
+// SVD_Rank_Calc (LA_ROUTINES.c:178-208) with opt = 1: the first i whose tail energy sqrt(sum_{j>=i} s_j^2),
+// relative to the total, is at most svd_eps.
+long long svd_rank(long long frank, double svd_eps, const double* s) {
+  double fsum = 0.0;
+  for (long long i = 0; i < frank; ++i) fsum = fsum + std::pow(s[i], 2);
+  fsum = std::sqrt(fsum);
+  for (long long i = 0; i < frank; ++i) {
+    double sum = 0.0;
+    for (long long j = i; j < frank; ++j) sum = sum + std::pow(s[j], 2);
+    sum = std::sqrt(sum) / fsum;
+    if (sum <= svd_eps) return i;
+  }
+  return frank;
+}
+
+// Omega_Calc (DMD_ROUTINES.c:100-152): the continuous-time exponent log(lambda)/delt with the reference's
+// branch choices for the argument.
+cplx omega_of(cplx lam, double delt) {
+  const double pi = 4.0 * std::atan(1.0);
+  const double clam = lam.imag(), rlam = lam.real();
+  if (clam == 0.0) {
+    if (rlam > 0.0) return cplx(std::log(std::fabs(rlam)) / delt, 0.0);
+    if (rlam < 0.0) return cplx(std::log(std::fabs(rlam)), pi) / delt;
+    return cplx(0.0, 0.0);   // the reference leaves this entry unset
+  }
+  if (rlam == 0.0) {
+    if (clam > 0.0) return cplx(std::log(std::fabs(clam)), pi / 2.0) / delt;
+    return cplx(std::log(std::fabs(clam)), 3.0 * pi / 2.0) / delt;
+  }
+  double theta = std::atan(std::fabs(clam) / std::fabs(rlam));
+  const double radius = std::sqrt(std::pow(rlam, 2) + std::pow(clam, 2));
+  if (rlam < 0.0 && clam > 0.0) theta = pi - theta;
+  else if (rlam < 0.0 && clam < 0.0) theta += pi;
+  else if (rlam > 0.0 && clam < 0.0) theta = 2.0 * pi - theta;
+  return cplx(std::log(radius), theta) / delt;
+}
+
+// A x = b by LU with partial pivoting (the zgesv of cGaussElim, DMD_ROUTINES.c); A column-major n x n.
+int lu_solve(int n, std::vector<cplx> A, std::vector<cplx>& b) {
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    for (int i = k + 1; i < n; ++i)
+      if (std::abs(A[i + (size_t)n * k]) > std::abs(A[p + (size_t)n * k])) p = i;
+    if (A[p + (size_t)n * k] == cplx(0.0, 0.0)) return TRT_ERR_NOCONV;
+    if (p != k) {
+      for (int j = 0; j < n; ++j) std::swap(A[k + (size_t)n * j], A[p + (size_t)n * j]);
+      std::swap(b[k], b[p]);
+    }
+    for (int i = k + 1; i < n; ++i) {
+      const cplx f = A[i + (size_t)n * k] / A[k + (size_t)n * k];
+      for (int j = k; j < n; ++j) A[i + (size_t)n * j] -= f * A[k + (size_t)n * j];
+      b[i] -= f * b[k];
+    }
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    cplx s = b[k];
+    for (int j = k + 1; j < n; ++j) s -= A[k + (size_t)n * j] * b[j];
+    b[k] = s / A[k + (size_t)n * k];
+  }
+  return TRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trt_dmd_calc(const double* data, long long N_t, long long N_g, long long clen, long long g, int base_subtract,
+                 double svd_eps, double delt, long long* N_modes, double* lambda, double* omega, double* b,
+                 double* wmat, double* wmat_proj, double* umat, double* wmat_tild, double* cvec) {
+  const long long shift = base_subtract ? 2 : 1;
+  if (!data || !N_modes || !lambda || !omega || !b || !wmat || !wmat_proj || !umat || !wmat_tild || !cvec ||
+      clen < 1 || N_g < 0 || g < 0 || (N_g > 0 && g >= N_g) || N_t - shift < 1 || N_t > 65535 || !(delt > 0.0) ||
+      clen > 0x7fffffffLL)
+    return TRT_ERR_ARG;
+  int rc = device_present();
+  if (rc) return rc;
+  const long long ng = N_g > 0 ? N_g : 1, n = N_t - shift, k = std::min(clen, n);
+  // block g (gdat_reform), the base vector, X = columns 0..n-1 and Y = columns 1..n, less the base
+  auto col = [&](long long t) { return data + (size_t)(g * clen + t * ng * clen); };
+  for (long long i = 0; i < clen; ++i) cvec[i] = base_subtract ? col(N_t - 1)[i] : 0.0;
+  std::vector<double> X((size_t)clen * n), Y((size_t)clen * n);
+  for (long long t = 0; t < n; ++t)
+    for (long long i = 0; i < clen; ++i) {
+      X[(size_t)(i + clen * t)] = col(t)[i] - cvec[i];
+      Y[(size_t)(i + clen * t)] = col(t + 1)[i] - cvec[i];
+    }
+  Dev dv;
+  double *dX, *dY, *dc, *dU, *dS, *dVT;
+  if ((rc = dv.get(&dX, X.size())) || (rc = dv.get(&dY, Y.size())) || (rc = dv.get(&dc, (size_t)clen)) ||
+      (rc = dv.get(&dU, (size_t)(clen * k))) || (rc = dv.get(&dS, (size_t)k)) || (rc = dv.get(&dVT, (size_t)(k * n))))
+    return rc;
+  ROM_CUDA(cudaMemcpy(dX, X.data(), X.size() * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dY, Y.data(), Y.size() * sizeof(double), cudaMemcpyHostToDevice));
+  // thin SVD of X itself (DMD does not centre; SVD_Calc, LA_ROUTINES.c:95-130)
+  cusolverDnHandle_t sh = nullptr;
+  if (cusolverDnCreate(&sh) != CUSOLVER_STATUS_SUCCESS) return TRT_ERR_CUDA;
+  cublasHandle_t bh = nullptr;
+  if (cublasCreate(&bh) != CUBLAS_STATUS_SUCCESS) {
+    cusolverDnDestroy(sh);
+    return TRT_ERR_CUDA;
+  }
+  struct Guard {
+    cusolverDnHandle_t s;
+    cublasHandle_t b;
+    ~Guard() {
+      cublasDestroy(b);
+      cusolverDnDestroy(s);
+    }
+  } guard{sh, bh};
+  {
+    const bool tall = clen >= n;
+    const int m = (int)(tall ? clen : n), nn = (int)(tall ? n : clen);
+    double* A = dX;
+    if (!tall) {
+      if ((rc = dv.get(&A, X.size()))) return rc;
+      transpose_kernel<<<grid_of(clen * n), 256>>>(clen, n, dX, A);
+      trt_host::add_launches(1);
+    }
+    double *Um, *VT, *work;
+    int* info;
+    int lwork = 0;
+    if ((rc = dv.get(&Um, (size_t)m * nn)) || (rc = dv.get(&VT, (size_t)nn * nn)) || (rc = dv.get(&info, 1))) return rc;
+    if (cusolverDnDgesvd_bufferSize(sh, m, nn, &lwork) != CUSOLVER_STATUS_SUCCESS) return TRT_ERR_CUDA;
+    if ((rc = dv.get(&work, (size_t)lwork))) return rc;
+    if (cusolverDnDgesvd(sh, 'S', 'S', m, nn, A, m, dS, Um, m, VT, nn, work, lwork, nullptr, info) !=
+        CUSOLVER_STATUS_SUCCESS)
+      return TRT_ERR_CUDA;
+    int hinfo = 0;
+    ROM_CUDA(cudaMemcpy(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hinfo != 0) return hinfo > 0 ? TRT_ERR_NOCONV : TRT_ERR_ARG;
+    if (tall) {
+      ROM_CUDA(cudaMemcpy(dU, Um, sizeof(double) * (size_t)(clen * k), cudaMemcpyDeviceToDevice));
+      ROM_CUDA(cudaMemcpy(dVT, VT, sizeof(double) * (size_t)(k * n), cudaMemcpyDeviceToDevice));
+    } else {
+      transpose_kernel<<<grid_of((long long)nn * nn), 256>>>(nn, nn, VT, dU);
+      transpose_kernel<<<grid_of((long long)m * nn), 256>>>(m, nn, Um, dVT);
+      trt_host::add_launches(2);
+    }
+    ROM_CUDA(cudaDeviceSynchronize());
+  }
+  std::vector<double> S((size_t)k), VTh((size_t)(k * n));
+  ROM_CUDA(cudaMemcpy(S.data(), dS, S.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  ROM_CUDA(cudaMemcpy(VTh.data(), dVT, VTh.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  const long long xr = svd_eps < 0.0 ? k : svd_rank(k, svd_eps, S.data());
+  if (xr < 1) return TRT_ERR_ARG;
+  // XV = V(:, 1:xr) S^-1 (n x xr), as the reference scales the transposed V^T
+  std::vector<double> XV((size_t)(n * xr));
+  for (long long i = 0; i < xr; ++i)
+    for (long long j = 0; j < n; ++j) XV[(size_t)(j + n * i)] = VTh[(size_t)(i + k * j)] / S[(size_t)i];
+  double *dXV, *dXm, *dAt;
+  if ((rc = dv.get(&dXV, XV.size())) || (rc = dv.get(&dXm, (size_t)(clen * xr))) ||
+      (rc = dv.get(&dAt, (size_t)(xr * xr))))
+    return rc;
+  ROM_CUDA(cudaMemcpy(dXV, XV.data(), XV.size() * sizeof(double), cudaMemcpyHostToDevice));
+  const double one = 1.0, zero = 0.0;
+  // Xm = Y XV (clen x xr); A~ = U(:, 1:xr)^T Xm (xr x xr)
+  if (cublasDgemm(bh, CUBLAS_OP_N, CUBLAS_OP_N, (int)clen, (int)xr, (int)n, &one, dY, (int)clen, dXV, (int)n, &zero, dXm,
+                  (int)clen) != CUBLAS_STATUS_SUCCESS ||
+      cublasDgemm(bh, CUBLAS_OP_T, CUBLAS_OP_N, (int)xr, (int)xr, (int)clen, &one, dU, (int)clen, dXm, (int)clen, &zero,
+                  dAt, (int)xr) != CUBLAS_STATUS_SUCCESS)
+    return TRT_ERR_CUDA;
+  // eigenpairs of A~ (EIG_Calc; complex arithmetic throughout, right eigenvectors of unit norm)
+  double2 *dAc, *dW, *dVR;
+  if ((rc = dv.get(&dAc, (size_t)(xr * xr))) || (rc = dv.get(&dW, (size_t)xr)) || (rc = dv.get(&dVR, (size_t)(xr * xr))))
+    return rc;
+  to_complex_kernel<<<grid_of(xr * xr), 256>>>(xr * xr, dAt, dAc);
+  trt_host::add_launches(1);
+  ROM_CUDA(cudaGetLastError());
+  cusolverDnParams_t prm = nullptr;
+  if (cusolverDnCreateParams(&prm) != CUSOLVER_STATUS_SUCCESS) return TRT_ERR_CUDA;
+  size_t wd = 0, wh = 0;
+  cusolverStatus_t es = cusolverDnXgeev_bufferSize(sh, prm, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_MODE_VECTOR, xr,
+                                                   CUDA_C_64F, dAc, xr, CUDA_C_64F, dW, CUDA_C_64F, nullptr, 1,
+                                                   CUDA_C_64F, dVR, xr, CUDA_C_64F, &wd, &wh);
+  if (es != CUSOLVER_STATUS_SUCCESS) {
+    cusolverDnDestroyParams(prm);
+    return TRT_ERR_UNSUPPORTED;
+  }
+  char* dwork = nullptr;
+  int* dinfo = nullptr;
+  if ((rc = dv.get(&dwork, wd)) || (rc = dv.get(&dinfo, 1))) {
+    cusolverDnDestroyParams(prm);
+    return rc;
+  }
+  std::vector<char> hwork(std::max<size_t>(wh, 1));
+  es = cusolverDnXgeev(sh, prm, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_MODE_VECTOR, xr, CUDA_C_64F, dAc, xr,
+                       CUDA_C_64F, dW, CUDA_C_64F, nullptr, 1, CUDA_C_64F, dVR, xr, CUDA_C_64F, dwork, wd, hwork.data(),
+                       wh, dinfo);
+  cusolverDnDestroyParams(prm);
+  if (es != CUSOLVER_STATUS_SUCCESS) return TRT_ERR_UNSUPPORTED;
+  int hinfo = 0;
+  ROM_CUDA(cudaMemcpy(&hinfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost));
+  if (hinfo != 0) return hinfo > 0 ? TRT_ERR_NOCONV : TRT_ERR_ARG;
+  // modes: wmat = Xm W~ / lambda, wmat_proj = U W~
+  double2 *dXmc, *dUc, *dWm, *dWp;
+  if ((rc = dv.get(&dXmc, (size_t)(clen * xr))) || (rc = dv.get(&dUc, (size_t)(clen * xr))) ||
+      (rc = dv.get(&dWm, (size_t)(clen * xr))) || (rc = dv.get(&dWp, (size_t)(clen * xr))))
+    return rc;
+  to_complex_kernel<<<grid_of(clen * xr), 256>>>(clen * xr, dXm, dXmc);
+  to_complex_kernel<<<grid_of(clen * xr), 256>>>(clen * xr, dU, dUc);
+  trt_host::add_launches(2);
+  const cuDoubleComplex c1 = make_cuDoubleComplex(1.0, 0.0), c0 = make_cuDoubleComplex(0.0, 0.0);
+  if (cublasZgemm(bh, CUBLAS_OP_N, CUBLAS_OP_N, (int)clen, (int)xr, (int)xr, &c1, dXmc, (int)clen, dVR, (int)xr, &c0, dWm,
+                  (int)clen) != CUBLAS_STATUS_SUCCESS ||
+      cublasZgemm(bh, CUBLAS_OP_N, CUBLAS_OP_N, (int)clen, (int)xr, (int)xr, &c1, dUc, (int)clen, dVR, (int)xr, &c0, dWp,
+                  (int)clen) != CUBLAS_STATUS_SUCCESS)
+    return TRT_ERR_CUDA;
+  divide_columns_kernel<<<grid_of(clen * xr), 256>>>(clen, (int)xr, dWm, dW);
+  trt_host::add_launches(1);
+  ROM_CUDA(cudaGetLastError());
+  ROM_CUDA(cudaDeviceSynchronize());
+  std::vector<cplx> lam((size_t)xr), Wt((size_t)(xr * xr));
+  ROM_CUDA(cudaMemcpy(lam.data(), dW, lam.size() * sizeof(cplx), cudaMemcpyDeviceToHost));
+  ROM_CUDA(cudaMemcpy(Wt.data(), dVR, Wt.size() * sizeof(cplx), cudaMemcpyDeviceToHost));
+  ROM_CUDA(cudaMemcpy(wmat, dWm, (size_t)(clen * xr) * sizeof(cplx), cudaMemcpyDeviceToHost));
+  ROM_CUDA(cudaMemcpy(wmat_proj, dWp, (size_t)(clen * xr) * sizeof(cplx), cudaMemcpyDeviceToHost));
+  ROM_CUDA(cudaMemcpy(umat, dU, (size_t)(clen * xr) * sizeof(double), cudaMemcpyDeviceToHost));
+  std::memcpy(wmat_tild, Wt.data(), Wt.size() * sizeof(cplx));
+  // Coef_Calc: b solves W~ b = U^T a0, a0 the first snapshot (less the base only for an undivided data set,
+  // as the reference does)
+  std::vector<double> Uh((size_t)(clen * xr));
+  std::memcpy(Uh.data(), umat, Uh.size() * sizeof(double));
+  std::vector<cplx> rhs((size_t)xr, cplx(0.0, 0.0));
+  for (long long r = 0; r < xr; ++r) {
+    cplx sacc(0.0, 0.0);
+    for (long long i = 0; i < clen; ++i) {
+      const double a0 = N_g > 0 ? col(0)[i] : col(0)[i] - cvec[i];
+      sacc += cplx(Uh[(size_t)(i + clen * r)], 0.0) * cplx(a0, 0.0);
+    }
+    rhs[(size_t)r] = sacc;
+  }
+  if ((rc = lu_solve((int)xr, Wt, rhs))) return rc;
+  for (long long r = 0; r < xr; ++r) {
+    b[2 * r] = rhs[(size_t)r].real();
+    b[2 * r + 1] = rhs[(size_t)r].imag();
+    lambda[2 * r] = lam[(size_t)r].real();
+    lambda[2 * r + 1] = lam[(size_t)r].imag();
+    const cplx om = omega_of(lam[(size_t)r], delt);
+    omega[2 * r] = om.real();
+    omega[2 * r + 1] = om.imag();
+  }
+  *N_modes = xr;
   return TRT_OK;
 }
 

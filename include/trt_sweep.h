@@ -462,6 +462,26 @@ int trt_pod_reconstruct(double* dat, const double* C, const double* S, const dou
 int trt_pod_reconstruct_device(double* dat, const double* C, const double* S, const double* U, const double* V,
                                const int* rank, const long long* offsets, int len, int n_blocks, int N_t, int t,
                                void* stream);
+/* Replaces the offline decomposer's DMD of one block (DMD_Calc, Coef_Calc and Omega_Calc,
+ * Decomposer/DecompSrc/DMD_ROUTINES.c:100-470): from data(clen, n_g, n_t) (layout as trt_pod_calc), the base
+ * vector cvec (the last snapshot when base_subtract, else zero), X and Y = the snapshots 0..n-1 and 1..n less
+ * cvec (n = N_t - 1, or N_t - 2 when base_subtract), the thin SVD X = U S V^T truncated to xr modes (all when
+ * svd_eps < 0, else SVD_Rank_Calc's tail-energy rule), A~ = U^T Y V S^-1, its eigenpairs (lambda, W~), the
+ * modes wmat = Y V S^-1 W~ / lambda and wmat_proj = U W~, the amplitudes b solving W~ b = U^T a0 (a0 the first
+ * snapshot, less cvec only for an undivided data set, as the reference does) and omega = log(lambda) / delt
+ * with Omega_Calc's branches.  Complex outputs are interleaved (re, im); the caller sizes them for
+ * k = min(clen, n) modes: lambda, omega, b (2k), wmat, wmat_proj (2 clen k), umat (clen k), wmat_tild (2 k k),
+ * cvec (clen); N_modes gets xr.  SVD by cuSOLVER gesvd, products by cuBLAS, eigenpairs by cuSOLVER's geev in
+ * complex arithmetic (the reference: LAPACK dgeev); eigenvectors have unit norm, unique up to a phase. */
+int trt_dmd_calc(const double* data, long long N_t, long long N_g, long long clen, long long g, int base_subtract,
+                 double svd_eps, double delt, long long* N_modes, double* lambda, double* omega, double* b,
+                 double* wmat, double* wmat_proj, double* umat, double* wmat_tild, double* cvec);
+/* Replaces SUBROUTINE DMD_RECONSTRUCT, MainSrc/DMD_ROUTINES.f08:28-109 (argument order as the subroutine;
+ * the COMPLEX*16 arrays L (eigenvalue exponents), B (mode amplitudes) and W (modes) as interleaved (re, im)
+ * doubles): dat(len) = Re(sum_r B(r) W(., r) exp(L(r) Time)) + C, groupwise (DMDgsum = 0: N_g blocks, block g
+ * with rank(g) modes packed after the earlier blocks') or over the whole vector (DMDgsum = 1). */
+int trt_dmd_reconstruct(double* dat, const double* L, const double* B, const double* W, const double* C,
+                        const int* rank, int len, int N_g, int DMDgsum, double Time);
 
 /* ---- Batched instances ---------------------------------------------------------------------------
  * Many independent handles (different grids, groups, quadratures, precisions) stepped together: the

@@ -623,3 +623,88 @@ def pod_reconstruct(C, S, U, V, rank, length, N_g, N_t, t, PODgsum):
         for r in range(r1):
             dat = dat + (S[r] * U[r * length:(r + 1) * length]) * V[r + (t - 1) * r1]
     return dat + C
+
+
+def dmd_reconstruct(L, B, W, C, rank, length, N_g, DMDgsum, Time):
+    """DMD_RECONSTRUCT (MainSrc/DMD_ROUTINES.f08:28-109): dat = Re(sum_r B(r) W(., r) exp(L(r) Time)) + C, modes
+    in order, each term (B W) e with the complex products written out (re = ac - bd, im = ad + bc) and
+    e = exp(L Time) evaluated once per mode (with the host's libm, as the library does)."""
+    import math
+    L, B, W = (np.asarray(a, dtype=np.complex128).reshape(-1, order="F") for a in (L, B, W))
+    C = np.asarray(C, dtype=np.float64).reshape(-1, order="F")
+    nb = N_g if DMDgsum == 0 else 1
+    glen = length // nb
+    re, im = np.zeros(length), np.zeros(length)
+    p3 = 0
+    for g in range(nb):
+        for r in range(int(rank[g])):
+            b, lam = B[p3 + r], L[p3 + r]
+            zr, zi = lam.real * Time, lam.imag * Time
+            m = math.exp(zr)
+            er, ei = m * math.cos(zi), m * math.sin(zi)
+            w = W[glen * (p3 + r):glen * (p3 + r + 1)]
+            pr = b.real * w.real - b.imag * w.imag
+            pi = b.real * w.imag + b.imag * w.real
+            seg = slice(g * glen, (g + 1) * glen)
+            re[seg] = re[seg] + (pr * er - pi * ei)
+            im[seg] = im[seg] + (pr * ei + pi * er)
+        p3 += int(rank[g])
+    return re + C
+
+
+def _omega(lam, delt):
+    """Omega_Calc (DMD_ROUTINES.c:100-152): log(lambda)/delt with the reference's argument branches."""
+    import math
+    pi = 4.0 * math.atan(1.0)
+    c, r = lam.imag, lam.real
+    if c == 0.0:
+        if r > 0.0:
+            return complex(math.log(abs(r)) / delt, 0.0)
+        if r < 0.0:
+            return complex(math.log(abs(r)), pi) / delt
+        return 0j
+    if r == 0.0:
+        return complex(math.log(abs(c)), pi / 2.0 if c > 0.0 else 3.0 * pi / 2.0) / delt
+    theta = math.atan(abs(c) / abs(r))
+    radius = math.sqrt(r ** 2 + c ** 2)
+    if r < 0.0 < c:
+        theta = pi - theta
+    elif r < 0.0 and c < 0.0:
+        theta += pi
+    elif r > 0.0 > c:
+        theta = 2.0 * pi - theta
+    return complex(math.log(radius), theta) / delt
+
+
+def dmd_calc(data, N_t, N_g, clen, g, base_subtract=0, svd_eps=-1.0, delt=1.0):
+    """DMD_Calc, Coef_Calc and Omega_Calc (Decomposer/DecompSrc/DMD_ROUTINES.c:100-470) restated with numpy/LAPACK:
+    X, Y (snapshots 0..n-1 and 1..n less the base vector), thin SVD of X truncated by SVD_Rank_Calc's rule,
+    A~ = U^T Y V S^-1, eig(A~), modes Y V S^-1 W~ / lambda and U W~, amplitudes W~ b = U^T a0, omega."""
+    ng = max(N_g, 1)
+    d = np.asarray(data, dtype=np.float64).reshape(-1, order="F")
+    col = lambda t: d[g * clen + t * ng * clen:g * clen + t * ng * clen + clen]
+    shift = 2 if base_subtract else 1
+    n = N_t - shift
+    cvec = col(N_t - 1).copy() if base_subtract else np.zeros(clen)
+    X = np.stack([col(t) - cvec for t in range(n)], axis=1)
+    Y = np.stack([col(t + 1) - cvec for t in range(n)], axis=1)
+    U, S, VT = np.linalg.svd(X, full_matrices=False)
+    k = len(S)
+    xr = k
+    if svd_eps >= 0.0:
+        fsum = np.sqrt(np.sum(S ** 2))
+        for i in range(k):
+            if np.sqrt(np.sum(S[i:] ** 2)) / fsum <= svd_eps:
+                xr = i
+                break
+    Ur = U[:, :xr]
+    XV = VT[:xr].T / S[:xr]
+    Xm = Y @ XV
+    At = Ur.T @ Xm
+    lam, Wt = np.linalg.eig(At)
+    wmat = (Xm @ Wt) / lam
+    wmat_proj = Ur @ Wt
+    a0 = col(0) if N_g > 0 else col(0) - cvec
+    b = np.linalg.solve(Wt, Ur.T @ a0)
+    omega = np.array([_omega(x, delt) for x in lam])
+    return dict(lambda_=lam, omega=omega, b=b, wmat=wmat, wmat_proj=wmat_proj, umat=Ur, wmat_tild=Wt, cvec=cvec)

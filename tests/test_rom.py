@@ -199,3 +199,108 @@ def test_pod_rom_drives_the_low_order_time_loop():
             assert st["sweeps"] == 0 and st["mgqd_nonconv"] == 0
             T = s.mlqd_field("Temp")
             assert float(np.max(np.abs(T - T_full[t - 1])) / np.max(T_full[t - 1])) < 1e-7
+
+
+def dmd_model(clen, n_blocks, ranks, seed):
+    """Modes, amplitudes and complex exponents of a DMD expansion (conjugate pairs, as a real signal has)."""
+    rng = np.random.default_rng(seed)
+    L, B, W = [], [], []
+    for g in range(n_blocks):
+        for _ in range(ranks[g]):
+            L.append(complex(rng.uniform(-5, 1), rng.uniform(-40, 40)))
+            B.append(complex(rng.standard_normal(), rng.standard_normal()))
+            W.append(rng.standard_normal(clen) + 1j * rng.standard_normal(clen))
+    return np.array(L), np.array(B), np.concatenate(W), rng.standard_normal(clen * n_blocks)
+
+
+def test_oracle_dmd_reconstruct_is_the_expansion(oracle):
+    clen, ranks = 25, [3, 2]
+    L, B, W, C = dmd_model(clen, 2, ranks, 4)
+    t = 0.037
+    r = oracle.dmd_reconstruct(L, B, W, C, ranks, 2 * clen, 2, 0, t)
+    ref = np.empty(2 * clen)
+    o = 0
+    for g in range(2):
+        Wg = W[clen * o:clen * (o + ranks[g])].reshape(clen, ranks[g], order="F")
+        ref[g * clen:(g + 1) * clen] = (Wg @ (B[o:o + ranks[g]] * np.exp(L[o:o + ranks[g]] * t))).real + \
+            C[g * clen:(g + 1) * clen]
+        o += ranks[g]
+    np.testing.assert_allclose(r, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("gsum", [0, 1])
+def test_device_dmd_reconstruct_bit_identical(oracle, gsum):
+    clen, ng = 300, 3
+    ranks = [4, 2, 6] if gsum == 0 else [9]
+    nb = ng if gsum == 0 else 1
+    L, B, W, C = dmd_model(clen * (1 if gsum == 0 else ng), nb, ranks, 8)
+    length = clen * ng
+    for t in (0.0, 0.013, 0.2):
+        out = np.zeros(length)
+        pkg.DMD_RECONSTRUCT(out, L, B, W, C, ranks, length, ng, gsum, t)
+        assert np.array_equal(out, oracle.dmd_reconstruct(L, B, W, C, ranks, length, ng, gsum, t))
+
+
+def dmd_data(clen, n_g, n_t, seed, base=0.0):
+    """Snapshots that are an exact sum of a few discrete-time modes: one real decaying mode and two
+    conjugate oscillating pairs per block, plus a constant base vector."""
+    rng = np.random.default_rng(seed)
+    out = np.empty((clen, max(n_g, 1), n_t), order="F")
+    mus = [0.93, 0.97 * np.exp(0.3j), 0.85 * np.exp(1.1j)]
+    for g in range(max(n_g, 1)):
+        field = base * rng.standard_normal(clen)
+        modes = [rng.standard_normal(clen) + 1j * rng.standard_normal(clen) for _ in mus]
+        for t in range(n_t):
+            x = field.copy()
+            for mu, phi in zip(mus, modes):
+                x = x + (phi * mu ** t).real if mu.imag else x + phi.real * mu.real ** t
+            out[:, g, t] = x
+    return out
+
+
+def match(a, b):
+    """Order of the entries of b that pairs them with a (nearest, one to one)."""
+    used, idx = set(), []
+    for x in a:
+        j = min((j for j in range(len(b)) if j not in used), key=lambda j: abs(b[j] - x))
+        used.add(j)
+        idx.append(j)
+    return np.array(idx)
+
+
+def test_oracle_dmd_recovers_the_modes(oracle):
+    data = dmd_data(60, 2, 14, 3)
+    o = oracle.dmd_calc(data, 14, 2, 60, 1, svd_eps=1e-10, delt=0.1)
+    assert len(o["lambda_"]) == 5
+    mus = np.array([0.93, 0.97 * np.exp(0.3j), 0.97 * np.exp(-0.3j), 0.85 * np.exp(1.1j), 0.85 * np.exp(-1.1j)])
+    np.testing.assert_allclose(o["lambda_"][match(mus, o["lambda_"])], mus, atol=1e-10)
+    for t in (0, 5, 12):   # the expansion reproduces the snapshots (DMD_RECONSTRUCT's formula at Time = t delt)
+        x = (o["wmat"] @ (o["b"] * np.exp(o["omega"] * 0.1 * t))).real + o["cvec"]
+        np.testing.assert_allclose(x, data[:, 1, t], atol=1e-9 * np.abs(data).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [(80, 0, 16, 0, 0), (50, 3, 12, 2, 0), (40, 0, 15, 0, 1)])
+def test_device_dmd_matches_oracle(oracle, case):
+    clen, ng, nt, g, base = case
+    data = dmd_data(clen, ng, nt, 11 + clen, base=1.0 if base else 0.0)
+    dev = pkg.DMD_Calc(data, nt, ng, clen, g, base_subtract=base, svd_eps=1e-10, delt=0.05)
+    ref = oracle.dmd_calc(data, nt, ng, clen, g, base_subtract=base, svd_eps=1e-10, delt=0.05)
+    assert len(dev["lambda_"]) == len(ref["lambda_"])
+    idx = match(ref["lambda_"], dev["lambda_"])
+    np.testing.assert_allclose(dev["lambda_"][idx], ref["lambda_"], atol=1e-10)
+    np.testing.assert_allclose(dev["omega"][idx], ref["omega"], atol=1e-8)
+    np.testing.assert_array_equal(dev["cvec"], ref["cvec"])
+    # the eigenvectors are unique up to a phase, which the amplitudes b absorb: compare the products
+    np.testing.assert_allclose(dev["wmat"][:, idx] * dev["b"][idx], ref["wmat"] * ref["b"], rtol=0,
+                               atol=1e-8 * np.abs(ref["wmat"] * ref["b"]).max())
+    if base:   # with the last snapshot as base the affine part is outside a linear fit: no exact expansion
+        return
+    # and the device expansion, evaluated by DMD_RECONSTRUCT on the device, reproduces the snapshots
+    blk = data[:, g, :] if ng else data[:, 0, :]
+    xr = len(dev["lambda_"])
+    for t in (1, nt // 2, nt - 2):
+        out = np.zeros(clen)
+        pkg.DMD_RECONSTRUCT(out, dev["omega"], dev["b"], dev["wmat"], dev["cvec"], [xr], clen, 1, 1, 0.05 * t)
+        np.testing.assert_allclose(out, blk[:, t], rtol=0, atol=1e-8 * np.abs(blk).max())
