@@ -583,6 +583,12 @@ int trt_dmd_calc(const double* data, long long N_t, long long N_g, long long cle
     rhs[(size_t)r] = sacc;
   }
   if ((rc = lu_solve((int)xr, Wt, rhs))) return rc;
+  // A~ is real: dgeev returns its real eigenvalues with a zero imaginary part, the complex solver with one at
+  // round-off level, which would move Omega_Calc onto the 2 pi branch.  Such parts are set to zero.
+  double lam_max = 0.0;
+  for (const cplx& l : lam) lam_max = std::max(lam_max, std::abs(l));
+  for (cplx& l : lam)
+    if (std::fabs(l.imag()) <= 1e-13 * lam_max) l = cplx(l.real(), 0.0);
   for (long long r = 0; r < xr; ++r) {
     b[2 * r] = rhs[(size_t)r].real();
     b[2 * r + 1] = rhs[(size_t)r].imag();
