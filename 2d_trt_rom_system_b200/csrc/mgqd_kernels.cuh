@@ -77,7 +77,13 @@ struct Scal {
   double res, xmax;    // last convergence norms
   int done;            // 0 running, 1 converged, -1 stopped without converging
   int its;
+  double best;         // smallest residual norm so far that halved the one before it
+  int best_it;         // the iteration that reached it
 };
+
+// Iterations without halving the best residual after which a solve counts as stagnated (it stops, reported as
+// not converged): a residual at the round-off floor of its right-hand side cannot reach the tolerance.
+constexpr int kStagnation = 150;
 
 // ------------------------------------------------------------------------------------------------
 // coefficients (MLOQD_SOLVES.f08:148-220)
@@ -545,6 +551,8 @@ __global__ void init_finish_kernel(const Krylov K, int nblk) {
     s.res = o[1];
     s.xmax = o[2];
     s.its = 0;
+    s.best = o[1];
+    s.best_it = 0;
     s.done = (o[1] <= K.tol * o[2] || o[0] == 0.0) ? 1 : 0;
     K.sc[g] = s;
     K.done[g] = s.done;
@@ -697,9 +705,14 @@ __global__ void update_finish_kernel(const Krylov K, int nblk) {
     s.res = o[1];
     s.xmax = o[2];
     int done = 0;
+    if (o[1] < 0.5 * s.best) {
+      s.best = o[1];
+      s.best_it = s.its;
+    }
     if (o[1] <= K.tol * o[2]) {
       done = 1;
-    } else if (o[0] == 0.0 || s.omega == 0.0 || s.alpha == 0.0 || !(o[1] == o[1]) || s.its >= K.maxit) {
+    } else if (o[0] == 0.0 || s.omega == 0.0 || s.alpha == 0.0 || !(o[1] == o[1]) || s.its >= K.maxit ||
+               s.its - s.best_it >= kStagnation) {
       done = -1;
     } else {
       s.beta = (o[0] / s.rho) * (s.alpha / s.omega);
