@@ -969,7 +969,7 @@ struct Mlqd {
   Dims d{};
   std::unique_ptr<Solver> MG, GR;   // multigroup system (n_g groups) and the grey Newton system
   Arena ar;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   unsigned long long* h_conv = nullptr;   // pinned, 10 convergence values
   // multigroup fields, Fortran layouts.  The current solution lives in MG->K.x (unknown layout) and
   // MG->Fx / MG->Fy; Eg/EgV/EgH are its copies in the reference layout.
@@ -1278,7 +1278,9 @@ int mlqd_step_impl(Mlqd& m, trt_mlqd_stats* out) {
     bool mg_conv = false;
     while (!mg_conv && mg < m.p.maxit_mloqd) {
       ++mg;
+      MG_CUDA(cudaEventRecord(m.ev[4], st));
       if ((rc = m.MG->solve(st))) return rc;   // MLOQD_FV from the previous solution
+      MG_CUDA(cudaEventRecord(m.ev[5], st));
       MG_CUDA(cudaMemcpyAsync(m.MG->h_scal, m.MG->K.sc, sizeof(Scal) * ng, cudaMemcpyDeviceToHost, st));
       if ((rc = unknowns_to_fields(m, st))) return rc;
       trt_gqd::collapse_kernel<<<grid1(d.npos()), 256, 0, st>>>(d, m.Eg, m.EgV, m.EgH, m.MG->Fx, m.MG->Fy, m.MGE,
@@ -1306,8 +1308,10 @@ int mlqd_step_impl(Mlqd& m, trt_mlqd_stats* out) {
       e.damp = (mg > 1 && m.p.kapE_dT_flag) ? 1 : 0;
       int its = 0;
       bool noconv = false;
+      MG_CUDA(cudaEventRecord(m.ev[6], st));
       if ((rc = egp_newton(m.GR.get(), st, e, eo, m.part, m.norms, &its, m.kits.data(), nullptr, nullptr, &noconv)))
         return rc;
+      MG_CUDA(cudaEventRecord(m.ev[7], st));
       for (int g = 0; g < ng; ++g) {   // h_scal was read before the Newton iteration's synchronisations
         if (m.MG->h_scal[g].done != 1) ++S.mgqd_nonconv;
         S.mgqd_krylov_max = std::max(S.mgqd_krylov_max, m.MG->h_scal[g].its);
@@ -1321,6 +1325,13 @@ int mlqd_step_impl(Mlqd& m, trt_mlqd_stats* out) {
       if ((rc = trt_host::handle_material(m.h, m.Src))) return rc;   // MATERIAL_UPDATE(Temp)
       double a = 0.0, b = 0.0;
       if ((rc = conv_pair(m, v.T, m.Tm1, m.Tm2, m.MGE, m.Em1, m.Em2, m.p.conv_lo, mg, &a, &b, &mg_conv))) return rc;
+      {   // the stream has synchronised: both intervals are complete
+        float t1 = 0.f, t2 = 0.f;
+        MG_CUDA(cudaEventElapsedTime(&t1, m.ev[4], m.ev[5]));
+        MG_CUDA(cudaEventElapsedTime(&t2, m.ev[6], m.ev[7]));
+        S.mgqd_solve_ms += t1;
+        S.egp_ms += t2;
+      }
       std::swap(m.Em1, m.Em2);
       std::swap(m.Tm1, m.Tm2);
       if ((rc = d2d(m.Em1, m.MGE, c1, st)) || (rc = d2d(m.Tm1, v.T, c1, st))) return rc;

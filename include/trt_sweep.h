@@ -421,6 +421,7 @@ typedef struct trt_mlqd_stats {
   int egp_krylov_max;  /* most BiCGSTAB iterations of an EGP Newton linear solve in the step */
   double T_norm, E_norm;   /* norms of the last outer iteration */
   double sweep_ms, low_order_ms;   /* device time of the sweeps and of everything else in the step */
+  double mgqd_solve_ms, egp_ms;    /* of low_order_ms: the MLOQD_FV solves and the EGP Newton iterations */
 } trt_mlqd_stats;
 int trt_mlqd_setup(trt_ctx* ctx, double Tini, const trt_mlqd_params* params);
 int trt_mlqd_step(trt_ctx* ctx, trt_mlqd_stats* stats);
