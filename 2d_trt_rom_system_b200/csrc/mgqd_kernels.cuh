@@ -83,7 +83,7 @@ struct Scal {
 
 // Iterations without halving the best residual after which a solve counts as stagnated (it stops, reported as
 // not converged): a residual at the round-off floor of its right-hand side cannot reach the tolerance.
-constexpr int kStagnation = 150;
+constexpr int kStagnation = 50;
 
 // ------------------------------------------------------------------------------------------------
 // coefficients (MLOQD_SOLVES.f08:148-220)
