@@ -101,6 +101,20 @@ def test_mlqd_step_fp64_matches_oracle_fixed_iterations(oracle, shape):
 
 
 @pytest.mark.gpu
+def test_mlqd_step_theta_half_matches_oracle(oracle):
+    """Theta = 0.5 brings in every old-time term of OLD_MGQD_COEFS and OLD_GREY_COEFS (with Theta = 1 they
+    vanish), including the KapE_Bar and GQD_Src that the reference leaves unset before the first step."""
+    prob, ts, km, bcT, cv = setup_problem(7, 6, 4, "S8", 39)
+    kw = dict(conv_lo=0.0, maxit_mloqd=3, Theta=0.5)
+    st, ref = oracle_run(oracle, prob, ts, km, bcT, cv, 2, conv_ho=0.0, maxit_rte=3, **kw)
+    with device(prob, ts, km, bcT, cv, conv_ho=0.0, maxit_rte=3, **kw) as s:
+        for r in ref:
+            s.mlqd_step()
+            assert rel(s.mlqd_field("Temp"), r["Temp"]) < 1e-9
+            assert rel(s.mlqd_field("E_avg"), r["E_avg"]) < 1e-9
+
+
+@pytest.mark.gpu
 def test_mlqd_convergence_path_matches_oracle(oracle):
     prob, ts, km, bcT, cv = setup_problem(8, 6, 10, "S8", 31)
     kw = dict(conv_lo=1e-8, maxit_mloqd=60)
