@@ -114,6 +114,8 @@ SIGNATURES = {
     "trt_moments": (_i, [_P, ctypes.POINTER(MomentsHost)]),
     "trt_get_angular": (_i, [_P, _D, _D, _D, _D, _D]),
     "trt_get_residual": (_i, [_P, _D, _I, _I]),
+    "trt_snapshot_angular": (_i, [_P, _P]),
+    "trt_snapshot_output": (_i, [_P, ctypes.c_char_p, _P]),
     "trt_stream": (_P, [_P]),
     "trt_set_wait_limit": (_i, [_P, ctypes.c_uint]),
     "trt_set_wait_limit_zero": (_i, [_P]),

@@ -1812,6 +1812,34 @@ int trt_get_angular(trt_ctx* c, double* I_avg, double* I_edgV, double* I_edgH, d
                                   : get_angular_impl<float>(c, I_avg, I_edgV, I_edgH, Ic_edgV, Ic_edgH);
 }
 
+int trt_snapshot_angular(trt_ctx* c, float* I_avg_device) {
+  if (!c || !I_avg_device) return TRT_ERR_ARG;
+  if (!c->have_state && !c->swept) return TRT_ERR_STATE;
+  const void* st = c->d_state[c->swept ? 1 - c->cur : c->cur];
+  const long long n = (long long)c->nx * c->ny * c->nm * c->ng;
+  if (c->prec == TRT_PREC_FP64)
+    trt::snapshot_avg_kernel<double><<<grid_for(n), 256, 0, c->stream>>>(c->geo(), (const double*)st, I_avg_device);
+  else
+    trt::snapshot_avg_kernel<float><<<grid_for(n), 256, 0, c->stream>>>(c->geo(), (const float*)st, I_avg_device);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  return TRT_OK;
+}
+
+int trt_snapshot_output(trt_ctx* c, const char* name, double* dst_device) {
+  if (!c || !name || !dst_device) return TRT_ERR_ARG;
+  if (!c->have_moments) return TRT_ERR_STATE;
+  long long sz[kNOut];
+  output_sizes(c->nx, c->ny, c->ng, sz);
+  double* const* d = reinterpret_cast<double* const*>(&c->dout);
+  for (int k = 0; k < kNOut; ++k)
+    if (std::strcmp(kOutNames[k], name) == 0) {
+      TRT_CUDA(cudaMemcpyAsync(dst_device, d[k], sz[k] * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+      return TRT_OK;
+    }
+  return TRT_ERR_ARG;
+}
+
 int trt_get_residual(trt_ctx* c, double* RT_Residual, int* RT_ResLoc_x, int* RT_ResLoc_y) {
   if (!c || !RT_Residual || !RT_ResLoc_x || !RT_ResLoc_y) return TRT_ERR_ARG;
   if (!c->have_res) return TRT_ERR_STATE;

@@ -323,6 +323,14 @@ int trt_moments_async(trt_ctx* ctx, const trt_moments_host* out);
 /* Angular intensities of the latest sweep in the reference layouts (any pointer may be NULL). */
 int trt_get_angular(trt_ctx* ctx, double* I_avg, double* I_edgV, double* I_edgH, double* Ic_edgV,
                     double* Ic_edgH);
+/* Snapshot output on the device (the I_out / fg / Cg writes of a snapshot-generating run, Tgen_QDf,
+ * MainSrc/ALGORITHMS.f08:1046-1095, into a caller's device store instead of a netCDF file):
+ * trt_snapshot_angular writes the latest I_avg(n_x,n_y,n_m,n_g) (mean of the corner intensities) as 4-byte
+ * floats to I_avg_device; trt_snapshot_output copies a combined output (name as in trt_moments_host) of the
+ * latest TRT_MOMENTS sweep to dst_device.  Both are enqueued on the handle's stream (trt_sync to wait) and
+ * allocate nothing; a time-last store (snapshot t at offset t * size) is the layout trt_pod_calc_device reads. */
+int trt_snapshot_angular(trt_ctx* ctx, float* I_avg_device);
+int trt_snapshot_output(trt_ctx* ctx, const char* name, double* dst_device);
 /* Residual norms of the latest TRT_RES_CALC sweep: RT_Residual(4,n_g,5), RT_ResLoc_x/y(4,n_g,5). */
 int trt_get_residual(trt_ctx* ctx, double* RT_Residual, int* RT_ResLoc_x, int* RT_ResLoc_y);
 

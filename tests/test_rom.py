@@ -114,8 +114,9 @@ def test_device_pod_reconstruct_bit_identical(oracle, gsum):
 
 @pytest.mark.gpu
 def test_rom_of_qd_factor_snapshots_from_the_device_time_loop(oracle):
-    """Snapshots of fg_avg_xx from device time steps (the transport-only loop on a small problem), kept in
-    HBM, decomposed by trt_pod_calc_device; a truncated POD reproduces the snapshots to its tail energy."""
+    """Snapshots of fg_avg_xx from device time steps (the transport-only loop on a small problem), stored in
+    HBM by trt_snapshot_output (with FP32 I_avg snapshots from trt_snapshot_angular), decomposed by
+    trt_pod_calc_device; a truncated POD reproduces the snapshots to its tail energy."""
     import ctypes
     import torch
     P = pkg.problems
@@ -130,12 +131,20 @@ def test_rom_of_qd_factor_snapshots_from_the_device_time_loop(oracle):
         s.tstep_setup(ts.nu_eV, ts.kappa_mult, ts.cv, np.full((prob.nx, prob.ny), ts.Tini_eV), ts.Kap0, P.COMP_UNIT,
                       P.C_LIGHT, ts.dt, bcT=ts.bcT_eV, conv_type=2, conv_ho=1e-8, maxit_rte=30)
         host = []
+        nm = len(ox)
+        iavg = torch.empty((nt, clen * nm * prob.ng), dtype=torch.float32, device="cuda")
         for t in range(nt):
             s.tstep()
-            f = s.moments(["fg_avg_xx"])["fg_avg_xx"]            # (nx, ny, ng)
+            # the snapshot store on the device: slot t of a time-last (clen, n_g, n_t) array, and the FP32
+            # angular snapshot beside it
+            assert pkg.lib().trt_snapshot_output(s.handle, b"fg_avg_xx", ctypes.c_void_p(snaps[t].data_ptr())) == 0
+            assert pkg.lib().trt_snapshot_angular(s.handle, ctypes.c_void_p(iavg[t].data_ptr())) == 0
+            s.sync()
+            f = s.moments(["fg_avg_xx"])["fg_avg_xx"]            # (nx, ny, ng), for the host-side check
             host.append(f)
-            # the snapshot store: column t of every group, in the decomposer's (clen, n_g, n_t) layout
-            snaps[t].copy_(torch.from_numpy(np.ascontiguousarray(f.reshape(clen, prob.ng, order="F").T)))
+            assert np.array_equal(snaps[t].cpu().numpy().reshape(-1), f.reshape(-1, order="F"))
+            I = s.angular(("I_avg",))["I_avg"]
+            assert np.array_equal(iavg[t].cpu().numpy(), I.reshape(-1, order="F").astype(np.float32))
     data = np.stack([h.reshape(clen, prob.ng, order="F") for h in host], axis=2)   # (clen, ng, nt)
     g = 1
     k = min(clen, nt)
