@@ -130,6 +130,39 @@ int device_present() {
   return TRT_OK;
 }
 
+// cuSOLVER / cuBLAS handles, created once per host thread and device (creating them costs milliseconds) and
+// kept until the process exits: destroying them from a thread-exit hook could run after the CUDA runtime has
+// been torn down.
+struct Handles {
+  int device = -1;
+  cusolverDnHandle_t s = nullptr;
+  cublasHandle_t b = nullptr;
+};
+int handles(cusolverDnHandle_t* s, cublasHandle_t* b) {
+  thread_local Handles h;
+  int dev = 0;
+  ROM_CUDA(cudaGetDevice(&dev));
+  if (h.device != dev) {
+    if (h.b) cublasDestroy(h.b);
+    if (h.s) cusolverDnDestroy(h.s);
+    h.s = nullptr;
+    h.b = nullptr;
+    h.device = -1;
+    if (cusolverDnCreate(&h.s) != CUSOLVER_STATUS_SUCCESS) {
+      h.s = nullptr;
+      return TRT_ERR_CUDA;
+    }
+    if (cublasCreate(&h.b) != CUBLAS_STATUS_SUCCESS) {
+      h.b = nullptr;
+      return TRT_ERR_CUDA;
+    }
+    h.device = dev;
+  }
+  *s = h.s;
+  if (b) *b = h.b;
+  return TRT_OK;
+}
+
 // Centring + thin SVD of the (clen x n_t) matrix whose column t starts at X + t * col_stride (device).
 // Outputs on the device: center(clen), umat(clen, k), sig(k), vtmat(k, n_t), k = min(clen, n_t).
 int pod_device(const double* X, long long col_stride, long long clen, int n_t, double* center, double* umat,
@@ -143,11 +176,7 @@ int pod_device(const double* X, long long col_stride, long long clen, int n_t, d
   trt_host::add_launches(1);
   ROM_CUDA(cudaGetLastError());
   cusolverDnHandle_t h = nullptr;
-  if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) return TRT_ERR_CUDA;
-  struct Guard {
-    cusolverDnHandle_t h;
-    ~Guard() { cusolverDnDestroy(h); }
-  } guard{h};
+  if ((rc = handles(&h, nullptr))) return rc;
   if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return TRT_ERR_CUDA;
   // cuSOLVER's gesvd wants rows >= columns: a wide matrix is decomposed through its transpose
   const bool tall = clen >= n_t;
@@ -446,20 +475,10 @@ int trt_dmd_calc(const double* data, long long N_t, long long N_g, long long cle
   ROM_CUDA(cudaMemcpy(dY, Y.data(), Y.size() * sizeof(double), cudaMemcpyHostToDevice));
   // thin SVD of X itself (DMD does not centre; SVD_Calc, LA_ROUTINES.c:95-130)
   cusolverDnHandle_t sh = nullptr;
-  if (cusolverDnCreate(&sh) != CUSOLVER_STATUS_SUCCESS) return TRT_ERR_CUDA;
   cublasHandle_t bh = nullptr;
-  if (cublasCreate(&bh) != CUBLAS_STATUS_SUCCESS) {
-    cusolverDnDestroy(sh);
+  if ((rc = handles(&sh, &bh))) return rc;
+  if (cusolverDnSetStream(sh, nullptr) != CUSOLVER_STATUS_SUCCESS || cublasSetStream(bh, nullptr) != CUBLAS_STATUS_SUCCESS)
     return TRT_ERR_CUDA;
-  }
-  struct Guard {
-    cusolverDnHandle_t s;
-    cublasHandle_t b;
-    ~Guard() {
-      cublasDestroy(b);
-      cusolverDnDestroy(s);
-    }
-  } guard{sh, bh};
   {
     const bool tall = clen >= n;
     const int m = (int)(tall ? clen : n), nn = (int)(tall ? n : clen);

@@ -66,3 +66,27 @@ def test_no_device_is_reported_not_emulated():
     p = one.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     h = L.trt_create(4, 4, 8, 1, p, p, p, p, p, 0, 0, ctypes.byref(st))
     assert not h and st.value == pkg._lib.TRT_ERR_NODEV
+
+
+def test_rom_entry_points_need_a_device():
+    """The POD / DMD entry points check their arguments, then report a missing device (no CPU path)."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    data = np.random.default_rng(0).standard_normal((6, 2, 5))
+    with pytest.raises(pkg.TrtError) as e:
+        pkg.POD_Calc(data, 5, 2, 6, 1)
+    assert e.value.code == pkg._lib.TRT_ERR_NODEV
+    with pytest.raises(pkg.TrtError) as e:
+        pkg.POD_Calc(data, 5, 2, 6, 2)                      # block index out of range
+    assert e.value.code == pkg._lib.TRT_ERR_ARG
+    with pytest.raises(pkg.TrtError) as e:
+        pkg.DMD_Calc(data, 5, 2, 6, 0, delt=0.1)
+    assert e.value.code == pkg._lib.TRT_ERR_NODEV
+    out = np.zeros(12)
+    with pytest.raises(pkg.TrtError) as e:
+        pkg.POD_RECONSTRUCT(out, np.zeros(12), np.ones(2), np.ones(12), np.ones(10), [1, 1], 12, 2, 5, 6, 0)
+    assert e.value.code == pkg._lib.TRT_ERR_ARG            # t beyond N_t
+    with pytest.raises(pkg.TrtError) as e:
+        pkg.DMD_RECONSTRUCT(out, np.ones(2), np.ones(2), np.ones(12), np.zeros(12), [1, 1], 12, 2, 0, 0.5)
+    assert e.value.code == pkg._lib.TRT_ERR_NODEV
