@@ -163,6 +163,55 @@ int handles(cusolverDnHandle_t* s, cublasHandle_t* b) {
   return TRT_OK;
 }
 
+// R(n x n) = the upper triangle of the first n rows of A (column-major, leading dimension lda), zero below.
+__global__ void upper_kernel(int n, long long lda, const double* __restrict__ A, double* __restrict__ R) {
+  const long long nn = (long long)n * n;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn; k += (long long)gridDim.x * blockDim.x) {
+    const long long i = k % n, j = k / n;
+    R[k] = i <= j ? A[i + lda * j] : 0.0;
+  }
+}
+
+// Thin SVD of a tall (m >= n) column-major matrix A, which is overwritten: A = Q R (geqrf), R = U_R S V^T
+// (gesvd of the n x n triangle), U = Q [U_R; 0] (ormqr).  Both routes are backward stable; for m >> n this one
+// runs the SVD on an n x n matrix instead of the m x n one.  Outputs U (m x n), S (n), VT (n x n).
+int thin_svd_tall(cusolverDnHandle_t h, cudaStream_t st, Dev& dv, double* A, int m, int n, double* U, double* S,
+                  double* VT) {
+  int rc;
+  double *tau, *R, *UR, *work;
+  int* info;
+  if ((rc = dv.get(&tau, (size_t)n)) || (rc = dv.get(&R, (size_t)n * n)) || (rc = dv.get(&UR, (size_t)n * n)) ||
+      (rc = dv.get(&info, 3)))
+    return rc;
+  int l1 = 0, l2 = 0, l3 = 0;
+  if (cusolverDnDgeqrf_bufferSize(h, m, n, A, m, &l1) != CUSOLVER_STATUS_SUCCESS ||
+      cusolverDnDgesvd_bufferSize(h, n, n, &l2) != CUSOLVER_STATUS_SUCCESS ||
+      cusolverDnDormqr_bufferSize(h, CUBLAS_SIDE_LEFT, CUBLAS_OP_N, m, n, n, A, m, tau, U, m, &l3) !=
+          CUSOLVER_STATUS_SUCCESS)
+    return TRT_ERR_CUDA;
+  const int lw = std::max(l1, std::max(l2, l3));
+  if ((rc = dv.get(&work, (size_t)lw))) return rc;
+  if (cusolverDnDgeqrf(h, m, n, A, m, tau, work, lw, info) != CUSOLVER_STATUS_SUCCESS) return TRT_ERR_CUDA;
+  upper_kernel<<<grid_of((long long)n * n), 256, 0, st>>>(n, m, A, R);
+  trt_host::add_launches(1);
+  ROM_CUDA(cudaGetLastError());
+  if (cusolverDnDgesvd(h, 'S', 'S', n, n, R, n, S, UR, n, VT, n, work, lw, nullptr, info + 1) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return TRT_ERR_CUDA;
+  ROM_CUDA(cudaMemsetAsync(U, 0, sizeof(double) * (size_t)m * n, st));
+  ROM_CUDA(cudaMemcpy2DAsync(U, sizeof(double) * (size_t)m, UR, sizeof(double) * (size_t)n, sizeof(double) * (size_t)n,
+                             n, cudaMemcpyDeviceToDevice, st));
+  if (cusolverDnDormqr(h, CUBLAS_SIDE_LEFT, CUBLAS_OP_N, m, n, n, A, m, tau, U, m, work, lw, info + 2) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return TRT_ERR_CUDA;
+  int hinfo[3] = {0, 0, 0};
+  ROM_CUDA(cudaMemcpyAsync(hinfo, info, sizeof(hinfo), cudaMemcpyDeviceToHost, st));
+  ROM_CUDA(cudaStreamSynchronize(st));
+  if (hinfo[1] > 0) return TRT_ERR_NOCONV;
+  if (hinfo[0] || hinfo[1] || hinfo[2]) return TRT_ERR_ARG;
+  return TRT_OK;
+}
+
 // Centring + thin SVD of the (clen x n_t) matrix whose column t starts at X + t * col_stride (device).
 // Outputs on the device: center(clen), umat(clen, k), sig(k), vtmat(k, n_t), k = min(clen, n_t).
 int pod_device(const double* X, long long col_stride, long long clen, int n_t, double* center, double* umat,
@@ -178,6 +227,11 @@ int pod_device(const double* X, long long col_stride, long long clen, int n_t, d
   cusolverDnHandle_t h = nullptr;
   if ((rc = handles(&h, nullptr))) return rc;
   if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return TRT_ERR_CUDA;
+  if (clen >= 2LL * n_t) {   // tall-skinny (the usual snapshot block): QR first
+    if ((rc = thin_svd_tall(h, st, dv, Xc, (int)clen, n_t, umat, sig, vtmat))) return rc;
+    ROM_CUDA(cudaStreamSynchronize(st));
+    return TRT_OK;
+  }
   // cuSOLVER's gesvd wants rows >= columns: a wide matrix is decomposed through its transpose
   const bool tall = clen >= n_t;
   const int m = (int)(tall ? clen : n_t), n = (int)(tall ? n_t : clen);
