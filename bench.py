@@ -359,7 +359,8 @@ def run_pod(pkg, torch, prob, nt, cpu_groups=4):
     dev_s = (time.perf_counter() - t0) / ng
     r = {"workload": f"POD per group of {nt} snapshots of {prob.nx}x{prob.ny} values x {ng} groups (fg-sized), "
                      "resident in HBM", "metric": "group PODs/s", "value": 1.0 / dev_s, "ms_per_group": dev_s * 1e3,
-         "path": "trt_pod_calc_device: centring kernel + cuSOLVER gesvd (m = cells, n = snapshots)"}
+         "path": "trt_pod_calc_device: centring kernel, then QR (cuSOLVER geqrf), SVD of the small triangle "
+                 "(gesvd) and U = Q U_R (ormqr)"}
     try:
         sys.path.insert(0, ROOT)
         from oracle import oracle as O
