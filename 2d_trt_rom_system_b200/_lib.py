@@ -153,6 +153,8 @@ SIGNATURES = {
     "trt_pod_reconstruct": (_i, [_D, _D, _D, _D, _D, _I, _i, _i, _i, _i, _i]),
     "trt_pod_reconstruct_device": (_i, [_P, _P, _P, _P, _P, _P, _P, _i, _i, _i, _i, _P]),
     "trt_dmd_reconstruct": (_i, [_D, _D, _D, _D, _D, _I, _i, _i, _i, _d]),
+    "trt_fmap": (_i, [_D, _D, _D, _D, _I, _I, _i, _i, _i, _i]),
+    "trt_linear_interpolation": (_i, [_D, _D, _d, _d, _d, _i]),
     "trt_dmd_calc": (_i, [_D, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, _i, _d, _d,
                           ctypes.POINTER(ctypes.c_longlong)] + [_D] * 8),
     "trt_mlqd_setup": (_i, [_P, _d, ctypes.POINTER(MlqdParams)]),

@@ -346,6 +346,26 @@ def DMD_RECONSTRUCT(dat, L, B, W, C, rank, len_, N_g, DMDgsum, Time):
                                          int(DMDgsum), float(Time)), "trt_dmd_reconstruct")
 
 
+def FMAP(f1, Grid1, Grid2, GMap, VMap, Glen1, Glen2, flen2):
+    """trt_fmap: returns f2 (flen2 values) mapped from f1 on grid 1 to grid 2."""
+    a = np.ascontiguousarray(np.asarray(f1, dtype=np.float64).reshape(-1, order="F"))
+    g1 = np.ascontiguousarray(Grid1, dtype=np.float64)
+    g2 = np.ascontiguousarray(Grid2, dtype=np.float64)
+    gm = np.ascontiguousarray(np.asarray(GMap).reshape(-1, order="F"), dtype=np.int32)
+    vm = np.ascontiguousarray(np.asarray(VMap).reshape(-1, order="F"), dtype=np.int32)
+    f2 = np.zeros(flen2)
+    check(_lib.lib().trt_fmap(dptr(a), dptr(f2), dptr(g1), dptr(g2), iptr(gm), iptr(vm), int(Glen1), int(Glen2),
+                              int(a.size), int(flen2)), "trt_fmap")
+    return f2
+
+
+def LINEAR_INTERPOLATION(v1, v2, xm, x1, x2, len_):
+    """trt_linear_interpolation, in place on v1 (float64)."""
+    b = np.ascontiguousarray(np.asarray(v2, dtype=np.float64).reshape(-1))
+    check(_lib.lib().trt_linear_interpolation(dptr(v1), dptr(b), float(xm), float(x1), float(x2), int(len_)),
+          "trt_linear_interpolation")
+
+
 def Bg_planck_calc(T, nu_low, nu_high, comp_unit):
     """FUNCTION Bg_planck_calc, MainSrc/TEMP_FUNCTIONS.f08:90-108 (host evaluation in the library)."""
     return _lib.lib().trt_bg_planck(float(T), float(nu_low), float(nu_high), float(comp_unit))

@@ -676,3 +676,101 @@ int trt_dmd_calc(const double* data, long long N_t, long long N_g, long long cle
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Grid and time mapping of reconstructed data: FMAP with BILINEAR_INTERPOLATE and LINEAR_INTERPOLATION
+// (MainSrc/GRID_FUNCTIONS.f08:14-44, 366-401, 819-836).
+// ------------------------------------------------------------------------------------------------
+
+namespace {
+
+// BILINEAR_INTERPOLATE, its branches and operation order.
+__device__ __forceinline__ double bilinear(double f11, double f12, double f21, double f22, double x, double x1, double x2,
+                                           double y, double y1, double y2) {
+  if ((x2 - x1) == 0.0) {
+    if ((y2 - y1) == 0.0) return f11;
+    const double yy1 = y - y1, yy2 = y2 - y;
+    return (f11 * yy2 + f12 * yy1) / (y2 - y1);
+  }
+  if ((y2 - y1) == 0.0) {
+    const double xx1 = x - x1, xx2 = x2 - x;
+    return (f11 * xx2 + f21 * xx1) / (x2 - x1);
+  }
+  const double xx1 = x - x1, xx2 = x2 - x, yy1 = y - y1, yy2 = y2 - y;
+  return (f11 * xx2 * yy2 + f21 * xx1 * yy2 + f12 * xx2 * yy1 + f22 * xx1 * yy1) / ((x2 - x1) * (y2 - y1));
+}
+
+// FMAP: for each of the flen2 / Glen2 blocks (groups), every point j of grid 2 from the four grid-1 values that
+// VMap names (1-based, within the block) and the corner coordinates GMap names (1-based index of an x, its y
+// following).  One thread per output value.
+__global__ void fmap_kernel(const double* __restrict__ f1, double* __restrict__ f2, const double* __restrict__ G1,
+                            const double* __restrict__ G2, const int* __restrict__ GMap, const int* __restrict__ VMap,
+                            int Glen1, int Glen2, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const long long blk = k / Glen2;
+    const int j = (int)(k % Glen2);
+    const double* f = f1 + blk * (long long)Glen1 - 1;   // 1-based within the block
+    const int* vm = VMap + 4 * j;
+    const int* gm = GMap + 4 * j;
+    f2[k] = bilinear(f[vm[0]], f[vm[2]], f[vm[1]], f[vm[3]], G2[2 * j], G1[gm[0] - 1], G1[gm[3] - 1], G2[2 * j + 1],
+                     G1[gm[0]], G1[gm[3]]);
+  }
+}
+
+// LINEAR_INTERPOLATION: v1 = v1 + (xm - x1) (v2 - v1) / (x2 - x1), value by value.
+__global__ void linear_interpolation_kernel(double* __restrict__ v1, const double* __restrict__ v2, double xm, double x1,
+                                            double x2, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    v1[k] = v1[k] + (xm - x1) * (v2[k] - v1[k]) / (x2 - x1);
+}
+
+}  // namespace
+
+extern "C" {
+
+int trt_fmap(const double* f1, double* f2, const double* Grid1, const double* Grid2, const int* GMap, const int* VMap,
+             int Glen1, int Glen2, int flen1, int flen2) {
+  if (!f1 || !f2 || !Grid1 || !Grid2 || !GMap || !VMap || Glen1 < 1 || Glen2 < 1 || flen2 % Glen2 != 0 ||
+      (long long)(flen2 / Glen2) * Glen1 > flen1)
+    return TRT_ERR_ARG;
+  // every map entry must name a value of the block and a coordinate pair of grid 1 (checked before any launch)
+  for (long long j = 0; j < 4LL * Glen2; ++j)
+    if (VMap[j] < 1 || VMap[j] > Glen1 || GMap[j] < 1 || GMap[j] > 2 * Glen1 - 1) return TRT_ERR_ARG;
+  int rc = device_present();
+  if (rc) return rc;
+  Dev dv;
+  double *d1, *d2, *g1, *g2;
+  int *gm, *vm;
+  if ((rc = dv.get(&d1, (size_t)flen1)) || (rc = dv.get(&d2, (size_t)flen2)) || (rc = dv.get(&g1, 2 * (size_t)Glen1)) ||
+      (rc = dv.get(&g2, 2 * (size_t)Glen2)) || (rc = dv.get(&gm, 4 * (size_t)Glen2)) || (rc = dv.get(&vm, 4 * (size_t)Glen2)))
+    return rc;
+  ROM_CUDA(cudaMemcpy(d1, f1, (size_t)flen1 * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(g1, Grid1, 2 * (size_t)Glen1 * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(g2, Grid2, 2 * (size_t)Glen2 * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(gm, GMap, 4 * (size_t)Glen2 * sizeof(int), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(vm, VMap, 4 * (size_t)Glen2 * sizeof(int), cudaMemcpyHostToDevice));
+  fmap_kernel<<<grid_of(flen2), 256>>>(d1, d2, g1, g2, gm, vm, Glen1, Glen2, (long long)flen2);
+  trt_host::add_launches(1);
+  ROM_CUDA(cudaGetLastError());
+  ROM_CUDA(cudaMemcpy(f2, d2, (size_t)flen2 * sizeof(double), cudaMemcpyDeviceToHost));
+  return TRT_OK;
+}
+
+int trt_linear_interpolation(double* v1, const double* v2, double xm, double x1, double x2, int len) {
+  if (!v1 || !v2 || len < 0 || !(x2 != x1)) return TRT_ERR_ARG;
+  if (len == 0) return TRT_OK;
+  int rc = device_present();
+  if (rc) return rc;
+  Dev dv;
+  double *a, *b;
+  if ((rc = dv.get(&a, (size_t)len)) || (rc = dv.get(&b, (size_t)len))) return rc;
+  ROM_CUDA(cudaMemcpy(a, v1, (size_t)len * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(b, v2, (size_t)len * sizeof(double), cudaMemcpyHostToDevice));
+  linear_interpolation_kernel<<<grid_of(len), 256>>>(a, b, xm, x1, x2, len);
+  trt_host::add_launches(1);
+  ROM_CUDA(cudaGetLastError());
+  ROM_CUDA(cudaMemcpy(v1, a, (size_t)len * sizeof(double), cudaMemcpyDeviceToHost));
+  return TRT_OK;
+}
+
+}  // extern "C"

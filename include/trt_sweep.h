@@ -485,6 +485,16 @@ int trt_pod_reconstruct_device(double* dat, const double* C, const double* S, co
 int trt_dmd_calc(const double* data, long long N_t, long long N_g, long long clen, long long g, int base_subtract,
                  double svd_eps, double delt, long long* N_modes, double* lambda, double* omega, double* b,
                  double* wmat, double* wmat_proj, double* umat, double* wmat_tild, double* cvec);
+/* Replaces SUBROUTINE FMAP, MainSrc/GRID_FUNCTIONS.f08:14-44 (with BILINEAR_INTERPOLATE, :366-401): data f1 on grid 1
+ * (flen1 values, blocks of Glen1) to grid 2 (f2, flen2 values, blocks of Glen2) by bilinear interpolation.
+ * Grid1 / Grid2 hold (x, y) pairs; VMap(4, Glen2) names the four grid-1 values (1-based within a block) and
+ * GMap(4, Glen2) the 1-based x index of the corner coordinates, as GENERATE_GRIDS builds them.  Map entries out
+ * of range are rejected (TRT_ERR_ARG) before anything runs. */
+int trt_fmap(const double* f1, double* f2, const double* Grid1, const double* Grid2, const int* GMap, const int* VMap,
+             int Glen1, int Glen2, int flen1, int flen2);
+/* Replaces SUBROUTINE LINEAR_INTERPOLATION, MainSrc/GRID_FUNCTIONS.f08:819-829 (LINEAR_INTERPOLATE, :831-836):
+ * v1 = v1 + (xm - x1) (v2 - v1) / (x2 - x1), the time interpolation between two reconstructed data levels. */
+int trt_linear_interpolation(double* v1, const double* v2, double xm, double x1, double x2, int len);
 /* Replaces SUBROUTINE DMD_RECONSTRUCT, MainSrc/DMD_ROUTINES.f08:28-109 (argument order as the subroutine;
  * the COMPLEX*16 arrays L (eigenvalue exponents), B (mode amplitudes) and W (modes) as interleaved (re, im)
  * doubles): dat(len) = Re(sum_r B(r) W(., r) exp(L(r) Time)) + C, groupwise (DMDgsum = 0: N_g blocks, block g

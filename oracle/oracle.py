@@ -708,3 +708,39 @@ def dmd_calc(data, N_t, N_g, clen, g, base_subtract=0, svd_eps=-1.0, delt=1.0):
     b = np.linalg.solve(Wt, Ur.T @ a0)
     omega = np.array([_omega(x, delt) for x in lam])
     return dict(lambda_=lam, omega=omega, b=b, wmat=wmat, wmat_proj=wmat_proj, umat=Ur, wmat_tild=Wt, cvec=cvec)
+
+
+def _bilinear(f11, f12, f21, f22, x, x1, x2, y, y1, y2):
+    """BILINEAR_INTERPOLATE (MainSrc/GRID_FUNCTIONS.f08:366-401), its branches and operation order."""
+    if (x2 - x1) == 0.0:
+        if (y2 - y1) == 0.0:
+            return f11
+        yy1, yy2 = y - y1, y2 - y
+        return (f11 * yy2 + f12 * yy1) / (y2 - y1)
+    if (y2 - y1) == 0.0:
+        xx1, xx2 = x - x1, x2 - x
+        return (f11 * xx2 + f21 * xx1) / (x2 - x1)
+    xx1, xx2, yy1, yy2 = x - x1, x2 - x, y - y1, y2 - y
+    return (f11 * xx2 * yy2 + f21 * xx1 * yy2 + f12 * xx2 * yy1 + f22 * xx1 * yy1) / ((x2 - x1) * (y2 - y1))
+
+
+def fmap(f1, Grid1, Grid2, GMap, VMap, Glen1, Glen2, flen2):
+    """FMAP (MainSrc/GRID_FUNCTIONS.f08:14-44), the Fortran loop with 1-based maps."""
+    f1 = np.asarray(f1, dtype=np.float64).reshape(-1, order="F")
+    G1, G2 = np.asarray(Grid1, dtype=np.float64), np.asarray(Grid2, dtype=np.float64)
+    GM, VM = np.asarray(GMap).reshape(-1, order="F"), np.asarray(VMap).reshape(-1, order="F")
+    f2 = np.zeros(flen2)
+    for i in range(flen2 // Glen2):
+        p1 = i * Glen1
+        for j in range(1, Glen2 + 1):
+            f2[i * Glen2 + j - 1] = _bilinear(
+                f1[p1 + VM[4 * j - 4] - 1], f1[p1 + VM[4 * j - 2] - 1], f1[p1 + VM[4 * j - 3] - 1],
+                f1[p1 + VM[4 * j - 1] - 1], G2[2 * j - 2], G1[GM[4 * j - 4] - 1], G1[GM[4 * j - 1] - 1], G2[2 * j - 1],
+                G1[GM[4 * j - 4]], G1[GM[4 * j - 1]])
+    return f2
+
+
+def linear_interpolation(v1, v2, xm, x1, x2):
+    """LINEAR_INTERPOLATION (MainSrc/GRID_FUNCTIONS.f08:819-836): v1 + (xm - x1) (v2 - v1) / (x2 - x1)."""
+    v1, v2 = np.asarray(v1, dtype=np.float64), np.asarray(v2, dtype=np.float64)
+    return v1 + (xm - x1) * (v2 - v1) / (x2 - x1)

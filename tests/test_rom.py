@@ -313,3 +313,56 @@ def test_device_dmd_matches_oracle(oracle, case):
         out = np.zeros(clen)
         pkg.DMD_RECONSTRUCT(out, dev["omega"], dev["b"], dev["wmat"], dev["cvec"], [xr], clen, 1, 1, 0.05 * t)
         np.testing.assert_allclose(out, blk[:, t], rtol=0, atol=1e-8 * np.abs(blk).max())
+
+
+def grid_maps(nx1, ny1, nx2, ny2, seed):
+    """A coarse data grid (grid 1) and a finer simulation grid (grid 2) on [0, 6]^2 with the four-corner maps
+    FMAP reads (1-based): the grid-1 cells that bracket each grid-2 point; points on a grid-1 line collapse
+    the bracket (the degenerate branches of BILINEAR_INTERPOLATE)."""
+    x1, y1 = np.linspace(0, 6, nx1), np.linspace(0, 6, ny1)
+    rng = np.random.default_rng(seed)
+    x2 = np.sort(np.concatenate([rng.uniform(0, 6, nx2 - 2), [x1[1], 6.0]]))
+    y2 = np.sort(np.concatenate([rng.uniform(0, 6, ny2 - 2), [y1[2], 0.0]]))
+    G1 = np.array([[x, y] for y in y1 for x in x1]).reshape(-1)       # point p = ix + nx1 * iy, (x, y) pairs
+    G2 = np.array([[x, y] for y in y2 for x in x2]).reshape(-1)
+    pt = lambda ix, iy: ix + nx1 * iy
+    GM, VM = [], []
+    for y in y2:
+        for x in x2:
+            ia = min(np.searchsorted(x1, x, side="right") - 1, nx1 - 1)
+            ja = min(np.searchsorted(y1, y, side="right") - 1, ny1 - 1)
+            ib = ia if x1[ia] == x else min(ia + 1, nx1 - 1)
+            jb = ja if y1[ja] == y else min(ja + 1, ny1 - 1)
+            corners = [pt(ia, ja), pt(ia, jb), pt(ib, ja), pt(ib, jb)]           # f11, f12, f21, f22
+            VM += [corners[0] + 1, corners[2] + 1, corners[1] + 1, corners[3] + 1]   # VMap order: 11, 21, 12, 22
+            GM += [2 * corners[0] + 1, 0, 0, 2 * corners[3] + 1]
+    GM = np.array(GM)
+    GM[1::4], GM[2::4] = GM[0::4], GM[3::4]
+    return G1, G2, GM, np.array(VM)
+
+
+def test_oracle_fmap_reproduces_a_bilinear_field(oracle):
+    G1, G2, GM, VM = grid_maps(7, 6, 11, 9, 1)
+    n1, n2 = len(G1) // 2, len(G2) // 2
+    f = lambda g: 1.0 + 2.0 * g[0::2] - 0.5 * g[1::2] + 0.25 * g[0::2] * g[1::2]
+    f1 = np.concatenate([f(G1), 3.0 * f(G1)])                       # two blocks (groups)
+    f2 = oracle.fmap(f1, G1, G2, GM, VM, n1, n2, 2 * n2)
+    np.testing.assert_allclose(f2, np.concatenate([f(G2), 3.0 * f(G2)]), rtol=1e-13, atol=1e-13)
+
+
+@pytest.mark.gpu
+def test_device_fmap_and_time_interpolation_bit_identical(oracle):
+    G1, G2, GM, VM = grid_maps(9, 8, 23, 17, 2)
+    n1, n2 = len(G1) // 2, len(G2) // 2
+    rng = np.random.default_rng(3)
+    f1 = rng.standard_normal(3 * n1)
+    f2 = pkg.FMAP(f1, G1, G2, GM, VM, n1, n2, 3 * n2)
+    assert np.array_equal(f2, oracle.fmap(f1, G1, G2, GM, VM, n1, n2, 3 * n2))
+    v1, v2 = rng.standard_normal(500), rng.standard_normal(500)
+    out = v1.copy()
+    pkg.LINEAR_INTERPOLATION(out, v2, 0.37, 0.2, 0.9, 500)
+    assert np.array_equal(out, oracle.linear_interpolation(v1, v2, 0.37, 0.2, 0.9))
+    bad = VM.copy()
+    bad[5] = n1 + 1                                                   # a map entry outside grid 1
+    with pytest.raises(pkg.TrtError):
+        pkg.FMAP(f1, G1, G2, GM, bad, n1, n2, 3 * n2)
