@@ -36,10 +36,6 @@ using namespace trt_mgqd;
   } while (0)
 
 constexpr int kSmallCells = 1024;   // levels at or below this many cells run in the one-CTA kernel
-// A one-group system (the grey Newton solves) has a single CTA per launch on its small levels anyway, so more of
-// its hierarchy goes to the one-CTA kernel (with more threads): a 256^2 grid then launches kernels only on its
-// finest level instead of three, and the per-cell arithmetic is the same.
-constexpr int kSmallCellsOneGroup = 16384, kSmallThreadsOneGroup = 1024;
 constexpr int kNu1 = 2, kNu2 = 2, kCoarseSweeps = 16;
 constexpr int kCheckEvery = 4;      // iterations between host checks of the convergence flags
 
@@ -61,7 +57,6 @@ struct Solver {
   Krylov K{};
   LevelSet ls{};
   int k0 = 0;
-  int small_cells = kSmallCells, small_threads = 256;   // the one-CTA part of the hierarchy and its block size
   double *Fx = nullptr, *Fy = nullptr, *rpart = nullptr, *res = nullptr, *bcres = nullptr;
   int* h_done = nullptr;
   Scal* h_scal = nullptr;
@@ -169,9 +164,7 @@ int Solver::init(int nx, int ny, int ng, bool own_inputs) {
     my = (my + 1) / 2;
   }
   k0 = 0;
-  small_cells = ng == 1 ? kSmallCellsOneGroup : kSmallCells;
-  small_threads = ng == 1 ? kSmallThreadsOneGroup : 256;
-  while (ls.L[k0].n > small_cells) ++k0;
+  while (ls.L[k0].n > kSmallCells) ++k0;
   MG_CUDA(cudaMallocHost(&h_done, sizeof(int) * ng));
   MG_CUDA(cudaMallocHost(&h_scal, sizeof(Scal) * ng));
   return TRT_OK;
@@ -242,7 +235,7 @@ int Solver::krylov(cudaStream_t s) {
       restrict_kernel<<<dim3(grid1(ls.L[k + 1].n), ng), 256, 0, s>>>(L, ls.L[k + 1], K.done);
       if ((rc = launched())) return rc;
     }
-    small_vcycle_kernel<<<ng, small_threads, 0, s>>>(ls, k0, kNu1, kNu2, kCoarseSweeps, K.done);
+    small_vcycle_kernel<<<ng, 256, 0, s>>>(ls, k0, kNu1, kNu2, kCoarseSweeps, K.done);
     if ((rc = launched())) return rc;
     for (int k = k0 - 1; k >= 0; --k) {
       const Level& L = ls.L[k];
