@@ -18,6 +18,13 @@ The corner state (15 GB FP64 / 7.5 GB FP32) is far larger than L2, so no flush i
   cpu_baseline the CPU oracle (restatement of TRANSPORT_SCB with its OpenMP-over-groups loop,
                g++ -O2 -fopenmp) on the first G_s groups of C1, one thread per group
 
+Further legs on the same grid (single GPU), each with its own figures:
+  time_steps   the transport-only time loop, mixed vs FP64 temperature error and step latency
+  mlqd         the mlqd time step (sweeps + MGQD and grey Newton low-order iterations), mixed vs FP64
+               errors in T, E and F, and where the step's time goes
+  pod          the POD of fg-sized snapshots resident in HBM against the oracle's LAPACK restatement
+  mgqd         the multigroup low-order solve alone, with its matrix-vector product roofline
+
 --impl reference times that CPU restatement alone (the reference Fortran cannot be built here).
 Multi-GPU (torchrun, one rank per GPU): each rank sweeps its own C1 instance (independent instances,
 no collective on the data path): weak scaling, time = max over ranks.
