@@ -276,7 +276,7 @@ extern "C" {
 int trt_pod_calc(const double* data, long long n_t, long long n_g, long long clen, long long g, double* center,
                  double* umat, double* sig, double* vtmat) {
   if (!data || !center || !umat || !sig || !vtmat || n_t < 1 || clen < 1 || n_g < 0 || g < 0 ||
-      (n_g > 0 && g >= n_g) || n_t > 65535)
+      (n_g > 0 && g >= n_g) || n_t > 65535 || clen > 0x7fffffffLL)   // cuSOLVER takes 32-bit extents
     return TRT_ERR_ARG;
   int rc = device_present();
   if (rc) return rc;
@@ -303,7 +303,7 @@ int trt_pod_calc(const double* data, long long n_t, long long n_g, long long cle
 int trt_pod_calc_device(const double* data, long long n_t, long long n_g, long long clen, long long g, double* center,
                         double* umat, double* sig, double* vtmat, void* stream) {
   if (!data || !center || !umat || !sig || !vtmat || n_t < 1 || clen < 1 || n_g < 0 || g < 0 ||
-      (n_g > 0 && g >= n_g) || n_t > 65535)
+      (n_g > 0 && g >= n_g) || n_t > 65535 || clen > 0x7fffffffLL)
     return TRT_ERR_ARG;
   int rc = device_present();
   if (rc) return rc;
