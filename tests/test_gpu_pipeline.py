@@ -61,3 +61,32 @@ def test_async_stepping_matches_synchronous(precision):
         for n in NAMES:
             assert np.array_equal(o[n], r[n]), n
     assert np.array_equal(state, ref_state)
+
+
+def test_async_and_snapshot_call_order():
+    prob = pkg.problems.random_small(42, 5, 4, 2, "S8")
+    d = sweep_inputs(prob, seed=5)
+    with make(d, "fp64") as s:
+        mh = pkg._lib.MomentsHost()
+        with pytest.raises(pkg.TrtError):
+            s.moments_async(mh)                                   # no moments yet
+        dst = np.zeros(1)
+        L = pkg.lib()
+        assert L.trt_snapshot_output(s.handle, b"fg_avg_xx", ctypes.c_void_p(dst.ctypes.data)) == \
+            pkg._lib.TRT_ERR_STATE
+        s.set_material(d["KapE_in"], d["src_iso"], d["c"], d["dt"], CU)
+        s.sweep(roll=True, moments=True)
+        assert L.trt_snapshot_output(s.handle, b"no_such_output", ctypes.c_void_p(dst.ctypes.data)) == \
+            pkg._lib.TRT_ERR_ARG
+        assert L.trt_snapshot_angular(s.handle, None) == pkg._lib.TRT_ERR_ARG
+        # a synchronous call after asynchronous ones sees their effect
+        kap, src = materials(d, 1)[0]
+        s.set_material_async(kap, src, d["c"], d["dt"], CU)
+        s.sweep(roll=False, moments=True, sync=False)
+        o = s.moments(["E_avg"])["E_avg"]
+        with make(d, "fp64") as r:
+            r.set_material(d["KapE_in"], d["src_iso"], d["c"], d["dt"], CU)
+            r.sweep(roll=True, moments=True)
+            r.set_material(kap, src, d["c"], d["dt"], CU)
+            r.sweep(roll=False, moments=True)
+            assert np.array_equal(o, r.moments(["E_avg"])["E_avg"])

@@ -178,3 +178,9 @@ def test_mlqd_call_order_and_arguments():
             s.mlqd_field("no_such_field")
         s.mlqd_setup(ts.Tini_eV, maxit_mloqd=2)   # a second setup replaces the first
         assert s.mlqd_step()["rt_its"] >= 1
+        with pytest.raises(pkg.TrtError):
+            s.mlqd_put("fg_avg_xx", np.ones(3))                # wrong size
+        with pytest.raises(pkg.TrtError):
+            s.mlqd_put("no_such_factor", np.ones(16 * prob.ng))
+        s.mlqd_put("fg_avg_xx", np.full(16 * prob.ng, 0.3))
+        assert np.array_equal(s.moments(["fg_avg_xx"])["fg_avg_xx"], np.full((4, 4, prob.ng), 0.3))
