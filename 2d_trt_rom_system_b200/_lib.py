@@ -76,7 +76,8 @@ class MlqdStats(ctypes.Structure):
                 ("egp_its", ctypes.c_int), ("mgqd_nonconv", ctypes.c_int), ("egp_nonconv", ctypes.c_int),
                 ("mgqd_krylov_max", ctypes.c_int), ("egp_krylov_max", ctypes.c_int),
                 ("T_norm", ctypes.c_double), ("E_norm", ctypes.c_double), ("sweep_ms", ctypes.c_double),
-                ("low_order_ms", ctypes.c_double), ("mgqd_solve_ms", ctypes.c_double), ("egp_ms", ctypes.c_double)]
+                ("low_order_ms", ctypes.c_double), ("mgqd_solve_ms", ctypes.c_double), ("egp_ms", ctypes.c_double),
+                ("mgqd_krylov_sum", ctypes.c_longlong), ("egp_krylov_sum", ctypes.c_longlong)]
 
 
 # Exported symbols and their ctypes signatures.

@@ -1312,13 +1312,18 @@ int mlqd_step_impl(Mlqd& m, trt_mlqd_stats* out) {
       if ((rc = egp_newton(m.GR.get(), st, e, eo, m.part, m.norms, &its, m.kits.data(), nullptr, nullptr, &noconv)))
         return rc;
       MG_CUDA(cudaEventRecord(m.ev[7], st));
+      int slowest = 0;
       for (int g = 0; g < ng; ++g) {   // h_scal was read before the Newton iteration's synchronisations
         if (m.MG->h_scal[g].done != 1) ++S.mgqd_nonconv;
-        S.mgqd_krylov_max = std::max(S.mgqd_krylov_max, m.MG->h_scal[g].its);
+        slowest = std::max(slowest, m.MG->h_scal[g].its);
       }
+      S.mgqd_krylov_max = std::max(S.mgqd_krylov_max, slowest);
+      S.mgqd_krylov_sum += slowest;
       for (int k = 0; k < its; ++k) {
         if (m.kits[k] < 0) ++S.egp_nonconv;
-        S.egp_krylov_max = std::max(S.egp_krylov_max, (std::abs(m.kits[k]) - 1) / 2);
+        const int ki = (std::abs(m.kits[k]) - 1) / 2;
+        S.egp_krylov_max = std::max(S.egp_krylov_max, ki);
+        S.egp_krylov_sum += ki;
       }
       m.egp_counts.push_back(its);
       S.egp_its += its;

@@ -331,6 +331,8 @@ def run_mlqd(pkg, torch, prob, steps, conv_ho=1e-8, conv_lo=1e-9, maxit_rte=10, 
                    "egp_its": [x["egp_its"] for x in sts], "sweep_ms": [x["sweep_ms"] for x in sts],
                    "low_order_ms": [x["low_order_ms"] for x in sts],
                    "mgqd_solve_ms": [x["mgqd_solve_ms"] for x in sts], "egp_ms": [x["egp_ms"] for x in sts],
+                   "mgqd_krylov_sum": [x["mgqd_krylov_sum"] for x in sts],
+                   "egp_krylov_sum": [x["egp_krylov_sum"] for x in sts],
                    "mgqd_nonconv": sum(x["mgqd_nonconv"] for x in sts),
                    "egp_nonconv": sum(x["egp_nonconv"] for x in sts),
                    "updates_per_s": float(prob.updates_per_sweep() * sum(x["sweeps"] for x in sts) / (lat.sum() * 1e-3))}

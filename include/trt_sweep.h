@@ -430,6 +430,8 @@ typedef struct trt_mlqd_stats {
   double T_norm, E_norm;   /* norms of the last outer iteration */
   double sweep_ms, low_order_ms;   /* device time of the sweeps and of everything else in the step */
   double mgqd_solve_ms, egp_ms;    /* of low_order_ms: the MLOQD_FV solves and the EGP Newton iterations */
+  long long mgqd_krylov_sum;       /* BiCGSTAB iterations of the MLOQD_FV solves (slowest group of each) */
+  long long egp_krylov_sum;        /* BiCGSTAB iterations of the EGP Newton linear solves */
 } trt_mlqd_stats;
 int trt_mlqd_setup(trt_ctx* ctx, double Tini, const trt_mlqd_params* params);
 int trt_mlqd_step(trt_ctx* ctx, trt_mlqd_stats* stats);
