@@ -64,8 +64,9 @@ struct Solver {
   bool matvec_timed = false;
   bool time_matvec = true;          // time the first iteration's matrix-vector product (trt_mgqd_last_stats)
   bool use_graphs = true;           // replay iteration blocks as a CUDA graph
+  bool rel_initial = false;         // stopping test also relative to the initial residual (Krylov::rel_initial)
   cudaGraphExec_t gexec = nullptr;  // kCheckEvery iterations, recorded on first use
-  int g_nodes = 0, g_maxit = -1;
+  int g_nodes = 0, g_maxit = -1, g_rel = -1;
   double g_tol = -1.0;
   int last_its = 0;
 
@@ -199,6 +200,7 @@ int Solver::krylov(cudaStream_t s) {
   matvec_timed = false;
   K.tol = g_settings.tol;
   K.maxit = g_settings.maxit;
+  K.rel_initial = rel_initial ? 1 : 0;
   use_graphs = g_settings.graphs;
   prec_coef_kernel<<<gpos, kRedBlock, 0, s>>>(d, cf, ls.L[0]);
   MG_LAUNCHED();
@@ -287,7 +289,7 @@ int Solver::krylov(cudaStream_t s) {
   // kernels take the solver's fixed buffers and K by value, so the graph is recorded again only when the
   // tolerance or the iteration limit in K changes.
   auto block = [&]() -> int {
-    if (!gexec || g_tol != K.tol || g_maxit != K.maxit) {
+    if (!gexec || g_tol != K.tol || g_maxit != K.maxit || g_rel != K.rel_initial) {
       if (gexec) {
         cudaGraphExecDestroy(gexec);
         gexec = nullptr;
@@ -315,6 +317,7 @@ int Solver::krylov(cudaStream_t s) {
       g_nodes = recorded;
       g_tol = K.tol;
       g_maxit = K.maxit;
+      g_rel = K.rel_initial;
     }
     MG_CUDA(cudaGraphLaunch(gexec, s));
     trt_host::add_launches((unsigned long long)g_nodes);
@@ -1049,6 +1052,7 @@ int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm) {
   if ((rc = m->GR->init(nx, ny, 1, false))) return rc;
   m->MG->time_matvec = false;   // every iteration block of the time loop's solves runs as a graph
   m->GR->time_matvec = false;
+  m->GR->rel_initial = true;    // Newton corrections: the reference's initial-residual test
   const size_t C = (size_t)d.nC * ng, V = (size_t)d.nV * ng, H = (size_t)d.nH * ng;
   const size_t c1 = d.nC, v1 = d.nV, hh1 = d.nH;
   const size_t side[4] = {(size_t)ny, (size_t)nx, (size_t)ny, (size_t)nx};   // L, B, R, T

@@ -79,6 +79,7 @@ struct Scal {
   int its;
   double best;         // smallest residual norm so far that halved the one before it
   int best_it;         // the iteration that reached it
+  double res0;         // residual norm of the initial guess
 };
 
 // Iterations without halving the best residual after which a solve counts as stagnated (it stops, reported as
@@ -499,7 +500,15 @@ struct Krylov {
   double* part;      // [ng][nblk][4]
   double tol;
   int maxit;
+  // 0: stop when the scaled residual is at most tol * max|x|.  1: or at most tol * the initial one, whichever is
+  // looser -- the form of SPARSKIT's test that the reference's QD_FV uses (QD_SOLVERS.f08:444), which a Newton
+  // correction far smaller than its starting guess needs.
+  int rel_initial;
 };
+
+__device__ __forceinline__ double krylov_bound(const Krylov& K, const Scal& s, double xmax) {
+  return K.tol * (K.rel_initial ? fmax(xmax, s.res0) : xmax);
+}
 
 // Jacobi scale of the row of unknown (cell / V edge / H edge) for the convergence norm.
 __device__ __forceinline__ double row_scale(const Coefs& cf, const Dims& d, int g, int kind, long e) {
@@ -553,6 +562,7 @@ __global__ void init_finish_kernel(const Krylov K, int nblk) {
     s.its = 0;
     s.best = o[1];
     s.best_it = 0;
+    s.res0 = o[1];
     s.done = (o[1] <= K.tol * o[2] || o[0] == 0.0) ? 1 : 0;
     K.sc[g] = s;
     K.done[g] = s.done;
@@ -709,7 +719,7 @@ __global__ void update_finish_kernel(const Krylov K, int nblk) {
       s.best = o[1];
       s.best_it = s.its;
     }
-    if (o[1] <= K.tol * o[2]) {
+    if (o[1] <= krylov_bound(K, s, o[2])) {
       done = 1;
     } else if (o[0] == 0.0 || s.omega == 0.0 || s.alpha == 0.0 || !(o[1] == o[1]) || s.its >= K.maxit ||
                s.its - s.best_it >= kStagnation) {
