@@ -156,6 +156,8 @@ SIGNATURES = {
     "trt_dmd_reconstruct": (_i, [_D, _D, _D, _D, _D, _I, _i, _i, _i, _d]),
     "trt_fmap": (_i, [_D, _D, _D, _D, _I, _I, _i, _i, _i, _i]),
     "trt_linear_interpolation": (_i, [_D, _D, _d, _d, _d, _i]),
+    "trt_gridmap_gen": (_i, [_i, _D, _D, _i, _i, _D]),
+    "trt_map_grids": (_i, [_I, _D, _D, _i, _i, _i, _I]),
     "trt_dmd_calc": (_i, [_D, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, _i, _d, _d,
                           ctypes.POINTER(ctypes.c_longlong)] + [_D] * 8),
     "trt_mlqd_setup": (_i, [_P, _d, ctypes.POINTER(MlqdParams)]),

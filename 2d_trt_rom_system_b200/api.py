@@ -359,6 +359,25 @@ def FMAP(f1, Grid1, Grid2, GMap, VMap, Glen1, Glen2, flen2):
     return f2
 
 
+def GRIDMAP_GEN(kind, Delx, Dely, N_x, N_y):
+    """trt_gridmap_gen: (x, y) pairs of cell centres (kind 0), vertical edges (1) or horizontal edges (2)."""
+    out = np.zeros(2 * N_x * N_y)
+    check(_lib.lib().trt_gridmap_gen(int(kind), dptr(_f64(Delx)), dptr(_f64(Dely)), int(N_x), int(N_y), dptr(out)),
+          "trt_gridmap_gen")
+    return out
+
+
+def MAP_GRIDS(Grid1, Grid2, xlen1):
+    """trt_map_grids: (GMap, VMap) of every Grid2 point's four bracketing Grid1 points (1-based)."""
+    g1 = np.ascontiguousarray(Grid1, dtype=np.float64)
+    g2 = np.ascontiguousarray(Grid2, dtype=np.float64)
+    gm = np.zeros(2 * g2.size, dtype=np.int32)
+    vm = np.zeros(2 * g2.size, dtype=np.int32)
+    check(_lib.lib().trt_map_grids(iptr(gm), dptr(g1), dptr(g2), int(g1.size), int(g2.size), int(xlen1), iptr(vm)),
+          "trt_map_grids")
+    return gm, vm
+
+
 def LINEAR_INTERPOLATION(v1, v2, xm, x1, x2, len_):
     """trt_linear_interpolation, in place on v1 (float64)."""
     b = np.ascontiguousarray(np.asarray(v2, dtype=np.float64).reshape(-1))

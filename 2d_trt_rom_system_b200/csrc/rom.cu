@@ -11,6 +11,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #include "trt_sweep.h"
@@ -770,6 +771,93 @@ int trt_linear_interpolation(double* v1, const double* v2, double xm, double x1,
   trt_host::add_launches(1);
   ROM_CUDA(cudaGetLastError());
   ROM_CUDA(cudaMemcpy(v1, a, (size_t)len * sizeof(double), cudaMemcpyDeviceToHost));
+  return TRT_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Grid coordinates and the maps FMAP reads: GRIDMAP_GEN_AVG / _EDGV / _EDGH and MAP_GRIDS
+// (MainSrc/GRID_FUNCTIONS.f08:49-133, 222-351).  Host set-up code (no device work), as in the reference.
+// ------------------------------------------------------------------------------------------------
+
+extern "C" {
+
+int trt_gridmap_gen(int kind, const double* Delx, const double* Dely, int N_x, int N_y, double* GridMap) {
+  if (!Delx || !Dely || !GridMap || N_x < 1 || N_y < 1 || kind < 0 || kind > 2) return TRT_ERR_ARG;
+  std::vector<double> xloc((size_t)N_x);
+  if (kind == 1) {   // vertical edges: x at the cell faces
+    xloc[0] = 0.0;
+    for (int i = 1; i < N_x; ++i) xloc[i] = xloc[i - 1] + Delx[i - 1];
+  } else {           // cell centres (and horizontal edges): x at the cell centres
+    xloc[0] = Delx[0] / 2.0;
+    for (int i = 1; i < N_x; ++i) xloc[i] = xloc[i - 1] + (Delx[i - 1] + Delx[i]) / 2.0;
+  }
+  long long p = 0;
+  double yloc = 0.0;
+  for (int j = 0; j < N_y; ++j) {
+    if (kind != 2) yloc = yloc + Dely[j] / 2.0;
+    for (int i = 0; i < N_x; ++i) {
+      GridMap[p++] = xloc[i];
+      GridMap[p++] = yloc;
+    }
+    if (kind != 2) yloc = yloc + Dely[j] / 2.0;
+    else if (j + 1 < N_y) yloc = yloc + Dely[j];   // horizontal edges: N_y rows of points, N_y - 1 widths used
+  }
+  return TRT_OK;
+}
+
+int trt_map_grids(int* Map, const double* Grid1, const double* Grid2, int len1, int len2, int xlen1, int* Vec_Locs) {
+  if (!Map || !Grid1 || !Grid2 || len1 < 2 || len2 < 2 || len1 % 2 || len2 % 2 || xlen1 < 2 || xlen1 % 2)
+    return TRT_ERR_ARG;
+  auto G1 = [&](long long i) { return Grid1[i - 1]; };   // 1-based, as the reference indexes
+  auto G2 = [&](long long j) { return Grid2[j - 1]; };
+  long long mp = 0;
+  for (long long j = 1; j <= len2; j += 2) {
+    double d = std::numeric_limits<double>::max();   // HUGE(0d0)
+    long long l[4] = {0, 0, 0, 0};
+    for (long long i = 1; i <= len1; i += 2) {   // closest point of grid 1 (DIST), first one on ties
+      const double r = std::fabs(std::sqrt(std::pow(G1(i) - G2(j), 2) + std::pow(G1(i + 1) - G2(j + 1), 2)));
+      if (r < d) {
+        d = r;
+        l[0] = i;
+      }
+    }
+    const double dx = G1(l[0]) - G2(j), dy = G1(l[0] + 1) - G2(j + 1);
+    if (dx < -1e-10) {
+      if (dy < -1e-10) {                 // bottom left
+        l[1] = l[0] + 2; l[2] = l[0] + xlen1; l[3] = l[2] + 2;
+      } else if (dy > 1e-10) {           // top left
+        l[2] = l[0]; l[0] = l[2] - xlen1; l[1] = l[0] + 2; l[3] = l[2] + 2;
+      } else {                           // exact left
+        l[1] = l[0] + 2; l[2] = l[0]; l[3] = l[1];
+      }
+    } else if (dx > 1e-10) {
+      if (dy < -1e-10) {                 // bottom right
+        l[1] = l[0]; l[0] = l[1] - 2; l[2] = l[0] + xlen1; l[3] = l[2] + 2;
+      } else if (dy > 1e-10) {           // top right
+        l[3] = l[0]; l[1] = l[3] - xlen1; l[0] = l[1] - 2; l[2] = l[3] - 2;
+      } else {                           // exact right
+        l[1] = l[0]; l[0] = l[1] - 2; l[2] = l[0]; l[3] = l[1];
+      }
+    } else {
+      if (dy < -1e-10) {                 // exact bottom
+        l[1] = l[0]; l[2] = l[0] + xlen1; l[3] = l[2];
+      } else if (dy > 1e-10) {           // exact top
+        l[2] = l[0]; l[0] = l[2] - xlen1; l[1] = l[0]; l[3] = l[2];
+      } else {                           // exact point
+        l[1] = l[0]; l[2] = l[0]; l[3] = l[0];
+      }
+    }
+    for (int k = 0; k < 4; ++k) {
+      // a grid 2 point outside grid 1's extent has no bracketing cell (the reference reads past its arrays)
+      if (l[k] < 1 || l[k] > len1 - 1) return TRT_ERR_ARG;
+      Map[mp + k] = (int)l[k];
+    }
+    mp += 4;
+  }
+  if (Vec_Locs)
+    for (long long j = 0; j < 2LL * len2; ++j) Vec_Locs[j] = (Map[j] + 1) / 2;
   return TRT_OK;
 }
 

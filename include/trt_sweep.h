@@ -494,6 +494,17 @@ int trt_dmd_calc(const double* data, long long N_t, long long N_g, long long cle
  * of range are rejected (TRT_ERR_ARG) before anything runs. */
 int trt_fmap(const double* f1, double* f2, const double* Grid1, const double* Grid2, const int* GMap, const int* VMap,
              int Glen1, int Glen2, int flen1, int flen2);
+/* Replace SUBROUTINEs GRIDMAP_GEN_AVG (kind 0), GRIDMAP_GEN_EDGV (1) and GRIDMAP_GEN_EDGH (2),
+ * MainSrc/GRID_FUNCTIONS.f08:49-133: the (x, y) pairs of an N_x by N_y set of points (cell centres; vertical edges;
+ * horizontal edges) from the cell widths Delx, Dely, into GridMap(2 N_x N_y).  Host code. */
+int trt_gridmap_gen(int kind, const double* Delx, const double* Dely, int N_x, int N_y, double* GridMap);
+/* Replaces SUBROUTINE MAP_GRIDS, MainSrc/GRID_FUNCTIONS.f08:222-327: for every point of Grid2 (len2 = twice its point
+ * count) the four bracketing points of Grid1 (len1; xlen1 = twice the points of a grid-1 row), as 1-based x indices
+ * into Grid1 (Map(4 len2/2), FMAP's GMap), and, when Vec_Locs is given, as point indices (FMAP's VMap).  The
+ * nearest point is searched with the reference's distance.  A bracket that would reach outside Grid1's arrays is
+ * rejected with TRT_ERR_ARG (the reference would read past them); like the reference, the caller keeps grid 2's
+ * points inside grid 1's extent.  Host code. */
+int trt_map_grids(int* Map, const double* Grid1, const double* Grid2, int len1, int len2, int xlen1, int* Vec_Locs);
 /* Replaces SUBROUTINE LINEAR_INTERPOLATION, MainSrc/GRID_FUNCTIONS.f08:819-829 (LINEAR_INTERPOLATE, :831-836):
  * v1 = v1 + (xm - x1) (v2 - v1) / (x2 - x1), the time interpolation between two reconstructed data levels. */
 int trt_linear_interpolation(double* v1, const double* v2, double xm, double x1, double x2, int len);

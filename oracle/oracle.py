@@ -744,3 +744,66 @@ def linear_interpolation(v1, v2, xm, x1, x2):
     """LINEAR_INTERPOLATION (MainSrc/GRID_FUNCTIONS.f08:819-836): v1 + (xm - x1) (v2 - v1) / (x2 - x1)."""
     v1, v2 = np.asarray(v1, dtype=np.float64), np.asarray(v2, dtype=np.float64)
     return v1 + (xm - x1) * (v2 - v1) / (x2 - x1)
+
+
+def gridmap_gen(kind, Delx, Dely, N_x, N_y):
+    """GRIDMAP_GEN_AVG (kind 0) / _EDGV (1) / _EDGH (2), MainSrc/GRID_FUNCTIONS.f08:49-133: (x, y) pairs."""
+    xloc = [0.0] * N_x
+    if kind == 1:
+        for i in range(1, N_x):
+            xloc[i] = xloc[i - 1] + Delx[i - 1]
+    else:
+        xloc[0] = Delx[0] / 2.0
+        for i in range(1, N_x):
+            xloc[i] = xloc[i - 1] + (Delx[i - 1] + Delx[i]) / 2.0
+    out, yloc = [], 0.0
+    for j in range(N_y):
+        if kind != 2:
+            yloc = yloc + Dely[j] / 2.0
+        for i in range(N_x):
+            out += [xloc[i], yloc]
+        if kind != 2:
+            yloc = yloc + Dely[j] / 2.0
+        elif j + 1 < N_y:
+            yloc = yloc + Dely[j]
+    return np.array(out)
+
+
+def map_grids(Grid1, Grid2, xlen1):
+    """MAP_GRIDS (MainSrc/GRID_FUNCTIONS.f08:222-327): GMap (1-based x indices of the four bracketing points of
+    grid 1 for every grid-2 point) and VMap = (GMap + 1) / 2."""
+    import math
+    G1 = lambda i: Grid1[i - 1]
+    G2 = lambda j: Grid2[j - 1]
+    Map = []
+    for j in range(1, len(Grid2) + 1, 2):
+        d, l1 = np.finfo(np.float64).max, 0
+        for i in range(1, len(Grid1) + 1, 2):
+            r = abs(math.sqrt((G1(i) - G2(j)) ** 2 + (G1(i + 1) - G2(j + 1)) ** 2))
+            if r < d:
+                d, l1 = r, i
+        dx, dy = G1(l1) - G2(j), G1(l1 + 1) - G2(j + 1)
+        if dx < -1e-10:
+            if dy < -1e-10:
+                l = [l1, l1 + 2, l1 + xlen1, l1 + xlen1 + 2]
+            elif dy > 1e-10:
+                l = [l1 - xlen1, l1 - xlen1 + 2, l1, l1 + 2]
+            else:
+                l = [l1, l1 + 2, l1, l1 + 2]
+        elif dx > 1e-10:
+            if dy < -1e-10:
+                l = [l1 - 2, l1, l1 - 2 + xlen1, l1 + xlen1]
+            elif dy > 1e-10:
+                l = [l1 - xlen1 - 2, l1 - xlen1, l1 - 2, l1]
+            else:
+                l = [l1 - 2, l1, l1 - 2, l1]
+        else:
+            if dy < -1e-10:
+                l = [l1, l1, l1 + xlen1, l1 + xlen1]
+            elif dy > 1e-10:
+                l = [l1 - xlen1, l1 - xlen1, l1, l1]
+            else:
+                l = [l1, l1, l1, l1]
+        Map += l
+    Map = np.array(Map, dtype=np.int32)
+    return Map, (Map + 1) // 2

@@ -366,3 +366,28 @@ def test_device_fmap_and_time_interpolation_bit_identical(oracle):
     bad[5] = n1 + 1                                                   # a map entry outside grid 1
     with pytest.raises(pkg.TrtError):
         pkg.FMAP(f1, G1, G2, GM, bad, n1, n2, 3 * n2)
+
+
+def test_grid_coordinates_and_maps_match_oracle(oracle):
+    """GRIDMAP_GEN_* and MAP_GRIDS (host code of the library, no device needed) against their restatements, and
+    the maps they build drive FMAP (the oracle's restatement) to reproduce a bilinear field on the finer grid."""
+    rng = np.random.default_rng(6)
+    dx1, dy1 = rng.uniform(0.5, 1.5, 6), rng.uniform(0.5, 1.5, 5)
+    dx2, dy2 = np.full(13, dx1.sum() / 13), np.full(11, dy1.sum() / 11)
+    for kind, (nx, ny) in ((0, (6, 5)), (1, (7, 5)), (2, (6, 6))):
+        assert np.array_equal(pkg.GRIDMAP_GEN(kind, dx1, dy1, nx, ny), oracle.gridmap_gen(kind, dx1, dy1, nx, ny))
+    # data on the cell-edge lattice of the coarse grid (corners included), mapped to the fine grid's centres
+    xe = np.concatenate([[0.0], np.cumsum(dx1)])
+    ye = np.concatenate([[0.0], np.cumsum(dy1)])
+    G1 = np.array([[x, y] for y in ye for x in xe]).reshape(-1)
+    G2 = pkg.GRIDMAP_GEN(0, dx2, dy2, 13, 11)
+    gm, vm = pkg.MAP_GRIDS(G1, G2, 2 * len(xe))
+    rgm, rvm = oracle.map_grids(G1, G2, 2 * len(xe))
+    assert np.array_equal(gm, rgm) and np.array_equal(vm, rvm)
+    f = lambda g: 2.0 - 0.3 * g[0::2] + 0.7 * g[1::2] + 0.05 * g[0::2] * g[1::2]
+    n1, n2 = len(G1) // 2, len(G2) // 2
+    f2 = oracle.fmap(f(G1), G1, G2, gm, vm, n1, n2, n2)
+    np.testing.assert_allclose(f2, f(G2), rtol=1e-13, atol=1e-13)
+    # a bracket that would reach outside grid 1's arrays is rejected, not read past them
+    with pytest.raises(pkg.TrtError):
+        pkg.MAP_GRIDS(G1, np.array([-1.0, 1.0]), 2 * len(xe))
