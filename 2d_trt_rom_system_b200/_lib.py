@@ -158,6 +158,13 @@ SIGNATURES = {
     "trt_linear_interpolation": (_i, [_D, _D, _d, _d, _d, _i]),
     "trt_gridmap_gen": (_i, [_i, _D, _D, _i, _i, _D]),
     "trt_map_grids": (_i, [_I, _D, _D, _i, _i, _i, _I]),
+    "trt_generate_grids_t": (_i, [_d, _d, _d, _d, _i, _i, _D, _D, _I]),
+    "trt_collect_lr_bnd": (_i, [_D, _D, _i, _i, _i]),
+    "trt_collect_bt_bnd": (_i, [_D, _D, _i, _i, _i]),
+    "trt_collect_crn_bnd": (_i, [_D, _D, _i, _i, _i]),
+    "trt_extnd_bt_bnd": (_i, [_D, _D, _i, _i, _i]),
+    "trt_extnd_lr_bnd": (_i, [_D, _D, _i, _i, _i]),
+    "trt_avg_apnd_bnd": (_i, [_D, _D, _D, _D, _D, _i, _i, _i]),
     "trt_dmd_calc": (_i, [_D, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, _i, _d, _d,
                           ctypes.POINTER(ctypes.c_longlong)] + [_D] * 8),
     "trt_mlqd_setup": (_i, [_P, _d, ctypes.POINTER(MlqdParams)]),

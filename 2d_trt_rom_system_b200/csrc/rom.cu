@@ -862,3 +862,133 @@ int trt_map_grids(int* Map, const double* Grid1, const double* Grid2, int len1, 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Time map and boundary helpers of the ROM reconstruction: GENERATE_GRIDS_T, COLLECT_LR_BND, COLLECT_BT_BND,
+// COLLECT_CRN_BND, EXTND_BT_BND, EXTND_LR_BND, AVG_APND_BND (MainSrc/GRID_FUNCTIONS.f08:406-656, 754-814).
+// Host code; each loop keeps the reference's traversal (pointers advanced in its order, 0-based here).
+// ------------------------------------------------------------------------------------------------
+
+extern "C" {
+
+int trt_generate_grids_t(double Delt_d, double Delt, double Start_Time_d, double Start_Time, int dN_t, int N_t,
+                         double* Sim_TGrid, double* Dat_TGrid, int* TMap) {
+  if (!Sim_TGrid || !Dat_TGrid || !TMap || dN_t < 1 || N_t < 1) return TRT_ERR_ARG;
+  Dat_TGrid[0] = Start_Time_d + Delt_d;
+  for (int j = 1; j < dN_t; ++j) Dat_TGrid[j] = Dat_TGrid[j - 1] + Delt_d;
+  Sim_TGrid[0] = Start_Time + Delt;
+  for (int j = 1; j < N_t; ++j) Sim_TGrid[j] = Sim_TGrid[j - 1] + Delt;
+  int k = 0;
+  for (int i = 0; i < N_t; ++i) {
+    const double ts = Sim_TGrid[i];
+    if (Dat_TGrid[0] >= ts) {
+      TMap[k] = 1;
+      TMap[++k] = 1;
+    } else if (Dat_TGrid[dN_t - 1] <= ts) {
+      TMap[k] = dN_t;
+      TMap[++k] = dN_t;
+    } else {
+      for (int j = 1; j < dN_t; ++j) {   // data levels 2..dN_t (1-based)
+        if (std::fabs(Dat_TGrid[j] - ts) / Dat_TGrid[j] <= 1e-14) {
+          TMap[k] = j + 1;
+          TMap[++k] = j + 1;
+          break;
+        } else if (Dat_TGrid[j] > ts) {
+          TMap[k] = j + 1;
+          TMap[++k] = j;
+          break;
+        }
+      }
+    }
+    ++k;
+  }
+  return TRT_OK;
+}
+
+int trt_collect_lr_bnd(double* bnd, const double* f, int N_g, int N_y, int N_x) {
+  if (!bnd || !f || N_g < 1 || N_y < 1 || N_x < 1) return TRT_ERR_ARG;
+  long long p1 = 0, p2 = 0;   // 1-based positions as the reference advances them
+  for (int g = 0; g < N_g; ++g)
+    for (int j = 0; j < N_y; ++j) {
+      p1 += 1;
+      bnd[p2++] = f[p1 - 1];
+      p1 += N_x - 1;
+      bnd[p2++] = f[p1 - 1];
+    }
+  return TRT_OK;
+}
+
+int trt_collect_bt_bnd(double* bnd, const double* f, int N_g, int N_y, int N_x) {
+  if (!bnd || !f || N_g < 1 || N_y < 2 || N_x < 1) return TRT_ERR_ARG;
+  long long p1 = 0, p2 = 0;
+  for (int g = 0; g < N_g; ++g) {
+    for (int i = 0; i < N_x; ++i) bnd[p2++] = f[p1++];
+    p1 += (long long)(N_y - 2) * N_x;
+    for (int i = 0; i < N_x; ++i) bnd[p2++] = f[p1++];
+  }
+  return TRT_OK;
+}
+
+int trt_collect_crn_bnd(double* bnd, const double* f, int N_g, int N_y, int N_x) {
+  if (!bnd || !f || N_g < 1 || N_y < 2 || N_x < 1) return TRT_ERR_ARG;
+  long long p1 = 0, p2 = 0;
+  for (int g = 0; g < N_g; ++g) {
+    p1 += 1;
+    bnd[p2++] = f[p1 - 1];
+    p1 += N_x - 1;
+    bnd[p2++] = f[p1 - 1];
+    p1 += (long long)(N_y - 2) * N_x + 1;
+    bnd[p2++] = f[p1 - 1];
+    p1 += N_x - 1;
+    bnd[p2++] = f[p1 - 1];
+  }
+  return TRT_OK;
+}
+
+int trt_extnd_bt_bnd(double* f_out, const double* f_in, int N_g, int N_y, int N_x) {
+  if (!f_out || !f_in || N_g < 1 || N_y < 1 || N_x < 1) return TRT_ERR_ARG;
+  long long p1 = 0, p2 = 0;
+  for (int g = 0; g < N_g; ++g) {
+    for (int i = 0; i < N_x; ++i) f_out[p2++] = f_in[p1++];   // bottom row repeated below
+    p1 -= N_x;
+    for (int j = 0; j < N_y; ++j)
+      for (int i = 0; i < N_x; ++i) f_out[p2++] = f_in[p1++];
+    p1 -= N_x;
+    for (int i = 0; i < N_x; ++i) f_out[p2++] = f_in[p1++];   // top row repeated above
+  }
+  return TRT_OK;
+}
+
+int trt_extnd_lr_bnd(double* f_out, const double* f_in, int N_g, int N_y, int N_x) {
+  if (!f_out || !f_in || N_g < 1 || N_y < 1 || N_x < 1) return TRT_ERR_ARG;
+  long long p1 = 0, p2 = 0;
+  for (int g = 0; g < N_g; ++g)
+    for (int j = 0; j < N_y; ++j) {
+      f_out[p2++] = f_in[p1];                                 // first value of the row repeated on the left
+      for (int i = 0; i < N_x; ++i) f_out[p2++] = f_in[p1++];
+      f_out[p2++] = f_in[p1 - 1];                             // last value repeated on the right
+    }
+  return TRT_OK;
+}
+
+int trt_avg_apnd_bnd(double* f_out, const double* f_in, const double* LR_Bnd, const double* BT_Bnd,
+                     const double* Crn_Bnd, int N_g, int N_y, int N_x) {
+  if (!f_out || !f_in || !LR_Bnd || !BT_Bnd || !Crn_Bnd || N_g < 1 || N_y < 1 || N_x < 1) return TRT_ERR_ARG;
+  long long po = 0, pi = 0, plr = 0, pbt = 0, pc = 0;
+  for (int g = 0; g < N_g; ++g) {
+    f_out[po++] = Crn_Bnd[pc++];
+    for (int i = 0; i < N_x; ++i) f_out[po++] = BT_Bnd[pbt++];
+    f_out[po++] = Crn_Bnd[pc++];
+    for (int j = 0; j < N_y; ++j) {
+      f_out[po++] = LR_Bnd[plr++];
+      for (int i = 0; i < N_x; ++i) f_out[po++] = f_in[pi++];
+      f_out[po++] = LR_Bnd[plr++];
+    }
+    f_out[po++] = Crn_Bnd[pc++];
+    for (int i = 0; i < N_x; ++i) f_out[po++] = BT_Bnd[pbt++];
+    f_out[po++] = Crn_Bnd[pc++];
+  }
+  return TRT_OK;
+}
+
+}  // extern "C"

@@ -505,6 +505,23 @@ int trt_gridmap_gen(int kind, const double* Delx, const double* Dely, int N_x, i
  * rejected with TRT_ERR_ARG (the reference would read past them); like the reference, the caller keeps grid 2's
  * points inside grid 1's extent.  Host code. */
 int trt_map_grids(int* Map, const double* Grid1, const double* Grid2, int len1, int len2, int xlen1, int* Vec_Locs);
+/* Replaces SUBROUTINE GENERATE_GRIDS_T, MainSrc/GRID_FUNCTIONS.f08:754-814: the data and simulation time levels and
+ * TMap(2, N_t), for every simulation level the two data levels (1-based) that bracket it (equal when it coincides
+ * with one within 1e-14 relative, or lies outside the data range).  Host code. */
+int trt_generate_grids_t(double Delt_d, double Delt, double Start_Time_d, double Start_Time, int dN_t, int N_t,
+                         double* Sim_TGrid, double* Dat_TGrid, int* TMap);
+/* Replace the boundary helpers of the ROM reconstruction, MainSrc/GRID_FUNCTIONS.f08:406-656 (each with the
+ * reference's arguments and value order; blocks of N_y rows of N_x values, N_g blocks): COLLECT_LR_BND (first and
+ * last value of every row), COLLECT_BT_BND (first and last row), COLLECT_CRN_BND (the four corners),
+ * EXTND_BT_BND (first and last row repeated below and above), EXTND_LR_BND (first and last value repeated left
+ * and right), AVG_APND_BND (a field framed by given edge and corner values).  Host code. */
+int trt_collect_lr_bnd(double* bnd, const double* f, int N_g, int N_y, int N_x);
+int trt_collect_bt_bnd(double* bnd, const double* f, int N_g, int N_y, int N_x);
+int trt_collect_crn_bnd(double* bnd, const double* f, int N_g, int N_y, int N_x);
+int trt_extnd_bt_bnd(double* f_out, const double* f_in, int N_g, int N_y, int N_x);
+int trt_extnd_lr_bnd(double* f_out, const double* f_in, int N_g, int N_y, int N_x);
+int trt_avg_apnd_bnd(double* f_out, const double* f_in, const double* LR_Bnd, const double* BT_Bnd,
+                     const double* Crn_Bnd, int N_g, int N_y, int N_x);
 /* Replaces SUBROUTINE LINEAR_INTERPOLATION, MainSrc/GRID_FUNCTIONS.f08:819-829 (LINEAR_INTERPOLATE, :831-836):
  * v1 = v1 + (xm - x1) (v2 - v1) / (x2 - x1), the time interpolation between two reconstructed data levels. */
 int trt_linear_interpolation(double* v1, const double* v2, double xm, double x1, double x2, int len);

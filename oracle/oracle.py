@@ -807,3 +807,76 @@ def map_grids(Grid1, Grid2, xlen1):
         Map += l
     Map = np.array(Map, dtype=np.int32)
     return Map, (Map + 1) // 2
+
+
+def generate_grids_t(Delt_d, Delt, Start_Time_d, Start_Time, dN_t, N_t):
+    """GENERATE_GRIDS_T (MainSrc/GRID_FUNCTIONS.f08:754-814): (Sim_TGrid, Dat_TGrid, TMap(2 N_t), 1-based)."""
+    dat = [Start_Time_d + Delt_d]
+    for _ in range(1, dN_t):
+        dat.append(dat[-1] + Delt_d)
+    sim = [Start_Time + Delt]
+    for _ in range(1, N_t):
+        sim.append(sim[-1] + Delt)
+    tmap = []
+    for ts in sim:
+        if dat[0] >= ts:
+            tmap += [1, 1]
+        elif dat[-1] <= ts:
+            tmap += [dN_t, dN_t]
+        else:
+            for j in range(1, dN_t):
+                if abs(dat[j] - ts) / dat[j] <= 1e-14:
+                    tmap += [j + 1, j + 1]
+                    break
+                if dat[j] > ts:
+                    tmap += [j + 1, j]
+                    break
+    return np.array(sim), np.array(dat), np.array(tmap, dtype=np.int32)
+
+
+def _blocks(f, N_g, N_y, N_x):
+    return np.asarray(f, dtype=np.float64).reshape(N_g, N_y, N_x)
+
+
+def collect_lr_bnd(f, N_g, N_y, N_x):
+    """COLLECT_LR_BND: first and last value of every row, row by row."""
+    b = _blocks(f, N_g, N_y, N_x)
+    return np.stack([b[:, :, 0], b[:, :, -1]], axis=2).reshape(-1)
+
+
+def collect_bt_bnd(f, N_g, N_y, N_x):
+    """COLLECT_BT_BND: the first and the last row of every block."""
+    b = _blocks(f, N_g, N_y, N_x)
+    return np.concatenate([b[:, 0, :], b[:, -1, :]], axis=1).reshape(-1)
+
+
+def collect_crn_bnd(f, N_g, N_y, N_x):
+    """COLLECT_CRN_BND: the four corners of every block (bottom left, bottom right, top left, top right)."""
+    b = _blocks(f, N_g, N_y, N_x)
+    return np.stack([b[:, 0, 0], b[:, 0, -1], b[:, -1, 0], b[:, -1, -1]], axis=1).reshape(-1)
+
+
+def extnd_bt_bnd(f, N_g, N_y, N_x):
+    """EXTND_BT_BND: the first and last rows repeated below and above."""
+    b = _blocks(f, N_g, N_y, N_x)
+    return np.concatenate([b[:, :1, :], b, b[:, -1:, :]], axis=1).reshape(-1)
+
+
+def extnd_lr_bnd(f, N_g, N_y, N_x):
+    """EXTND_LR_BND: the first and last values of every row repeated left and right."""
+    b = _blocks(f, N_g, N_y, N_x)
+    return np.concatenate([b[:, :, :1], b, b[:, :, -1:]], axis=2).reshape(-1)
+
+
+def avg_apnd_bnd(f, LR, BT, Crn, N_g, N_y, N_x):
+    """AVG_APND_BND: the field framed by its left/right values (2 per row), bottom/top rows and 4 corners."""
+    b = _blocks(f, N_g, N_y, N_x)
+    lr = np.asarray(LR).reshape(N_g, N_y, 2)
+    bt = np.asarray(BT).reshape(N_g, 2, N_x)
+    c = np.asarray(Crn).reshape(N_g, 4)
+    out = np.empty((N_g, N_y + 2, N_x + 2))
+    out[:, 0, 0], out[:, 0, -1], out[:, -1, 0], out[:, -1, -1] = c[:, 0], c[:, 1], c[:, 2], c[:, 3]
+    out[:, 0, 1:-1], out[:, -1, 1:-1] = bt[:, 0], bt[:, 1]
+    out[:, 1:-1, 0], out[:, 1:-1, -1] = lr[:, :, 0], lr[:, :, 1]
+    out[:, 1:-1, 1:-1] = b
+    return out.reshape(-1)

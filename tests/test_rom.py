@@ -391,3 +391,30 @@ def test_grid_coordinates_and_maps_match_oracle(oracle):
     # a bracket that would reach outside grid 1's arrays is rejected, not read past them
     with pytest.raises(pkg.TrtError):
         pkg.MAP_GRIDS(G1, np.array([-1.0, 1.0]), 2 * len(xe))
+
+
+def test_time_map_and_boundary_helpers_match_oracle(oracle):
+    """GENERATE_GRIDS_T and the boundary helpers of the reconstruction (host code of the library, no device)."""
+    import ctypes
+    L = pkg.lib()
+    D, I = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    for args in ((2e-3, 1e-3, 0.0, 0.0, 7, 15), (5e-3, 2e-3, 0.01, 0.0, 6, 20), (1e-3, 1e-3, 0.0, 0.0, 10, 10)):
+        dN_t, N_t = args[4], args[5]
+        sim, dat, tm = np.zeros(N_t), np.zeros(dN_t), np.zeros(2 * N_t, dtype=np.int32)
+        assert L.trt_generate_grids_t(*args, sim.ctypes.data_as(D), dat.ctypes.data_as(D), tm.ctypes.data_as(I)) == 0
+        rs, rd, rt = oracle.generate_grids_t(*args)
+        assert np.array_equal(sim, rs) and np.array_equal(dat, rd) and np.array_equal(tm, rt)
+    ng, ny, nx = 3, 5, 4
+    f = np.random.default_rng(7).standard_normal(ng * ny * nx)
+    fp = f.ctypes.data_as(D)
+    for name, n in (("collect_lr_bnd", ng * ny * 2), ("collect_bt_bnd", ng * 2 * nx), ("collect_crn_bnd", ng * 4),
+                    ("extnd_bt_bnd", ng * (ny + 2) * nx), ("extnd_lr_bnd", ng * ny * (nx + 2))):
+        out = np.zeros(n)
+        assert getattr(L, "trt_" + name)(out.ctypes.data_as(D), fp, ng, ny, nx) == 0
+        assert np.array_equal(out, getattr(oracle, name)(f, ng, ny, nx)), name
+    lr, bt, crn = oracle.collect_lr_bnd(f, ng, ny, nx), oracle.collect_bt_bnd(f, ng, ny, nx), \
+        oracle.collect_crn_bnd(f, ng, ny, nx)
+    out = np.zeros(ng * (ny + 2) * (nx + 2))
+    assert L.trt_avg_apnd_bnd(out.ctypes.data_as(D), fp, lr.ctypes.data_as(D), bt.ctypes.data_as(D),
+                              crn.ctypes.data_as(D), ng, ny, nx) == 0
+    assert np.array_equal(out, oracle.avg_apnd_bnd(f, lr, bt, crn, ng, ny, nx))
