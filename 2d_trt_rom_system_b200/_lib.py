@@ -159,6 +159,8 @@ SIGNATURES = {
     "trt_gridmap_gen": (_i, [_i, _D, _D, _i, _i, _D]),
     "trt_map_grids": (_i, [_I, _D, _D, _i, _i, _i, _I]),
     "trt_generate_grids_t": (_i, [_d, _d, _d, _d, _i, _i, _D, _D, _I]),
+    "trt_gridmap_gen_bnd": (_i, [_i, _D, _d, _i, _D]),
+    "trt_generate_grids_xy": (_i, [_D, _D, _D, _D, _d, _d, _d, _d, _i, _i, _i, _i] + [_D] * 8 + [_I] * 8),
     "trt_collect_lr_bnd": (_i, [_D, _D, _i, _i, _i]),
     "trt_collect_bt_bnd": (_i, [_D, _D, _i, _i, _i]),
     "trt_collect_crn_bnd": (_i, [_D, _D, _i, _i, _i]),

@@ -378,6 +378,33 @@ def MAP_GRIDS(Grid1, Grid2, xlen1):
     return gm, vm
 
 
+def GRIDMAP_GEN_BND(side, Del, pos, N):
+    """trt_gridmap_gen_bnd: the N points of the left/right (side 0, x = pos) or bottom/top (side 1, y = pos) side."""
+    out = np.zeros(2 * N)
+    check(_lib.lib().trt_gridmap_gen_bnd(int(side), dptr(_f64(Del)), float(pos), int(N), dptr(out)),
+          "trt_gridmap_gen_bnd")
+    return out
+
+
+def GENERATE_GRIDS_XY(Delx_d, Dely_d, Delx, Dely, xlen_d, ylen_d, xlen, ylen):
+    """trt_generate_grids_xy: dict of the simulation (Sim_Grid_*) and padded data (Dat_Grid_*) point sets and the
+    maps between them (GMap_xy*, VMap_xy*), keyed by the reference's names."""
+    Delx_d, Dely_d, Delx, Dely = _f64(Delx_d), _f64(Dely_d), _f64(Delx), _f64(Dely)
+    dN_x, dN_y, N_x, N_y = Delx_d.size, Dely_d.size, Delx.size, Dely.size
+    sets = {"Avg": (N_x * N_y, (dN_x + 2) * (dN_y + 2)), "EdgV": ((N_x + 1) * N_y, (dN_x + 1) * (dN_y + 2)),
+            "EdgH": (N_x * (N_y + 1), (dN_x + 2) * (dN_y + 1)), "Bnds": (2 * (N_x + N_y), 2 * (dN_x + dN_y) + 8)}
+    out = {}
+    for k, (ns, nd) in sets.items():
+        out["Sim_Grid_" + k], out["Dat_Grid_" + k] = np.zeros(2 * ns), np.zeros(2 * nd)
+        out["GMap_xy" + k], out["VMap_xy" + k] = np.zeros(4 * ns, dtype=np.int32), np.zeros(4 * ns, dtype=np.int32)
+    args = [dptr(out[p + k]) for p in ("Sim_Grid_", "Dat_Grid_") for k in sets] + \
+        [iptr(out[p + k]) for p in ("GMap_xy", "VMap_xy") for k in sets]
+    check(_lib.lib().trt_generate_grids_xy(dptr(Delx_d), dptr(Dely_d), dptr(Delx), dptr(Dely), float(xlen_d),
+                                           float(ylen_d), float(xlen), float(ylen), dN_x, dN_y, N_x, N_y, *args),
+          "trt_generate_grids_xy")
+    return out
+
+
 def LINEAR_INTERPOLATION(v1, v2, xm, x1, x2, len_):
     """trt_linear_interpolation, in place on v1 (float64)."""
     b = np.ascontiguousarray(np.asarray(v2, dtype=np.float64).reshape(-1))

@@ -807,8 +807,16 @@ int trt_gridmap_gen(int kind, const double* Delx, const double* Dely, int N_x, i
   return TRT_OK;
 }
 
-int trt_map_grids(int* Map, const double* Grid1, const double* Grid2, int len1, int len2, int xlen1, int* Vec_Locs) {
-  if (!Map || !Grid1 || !Grid2 || len1 < 2 || len2 < 2 || len1 % 2 || len2 % 2 || xlen1 < 2 || xlen1 % 2)
+}  // extern "C"
+
+namespace {
+
+// MAP_GRIDS searching the first len1 values of Grid1, whose array holds len1_array >= len1 values: the boundary
+// maps of GENERATE_GRIDS_XY search all but the last point of a side, which a bracket may still reach.
+int map_grids_impl(int* Map, const double* Grid1, const double* Grid2, int len1, long long len1_array, int len2,
+                   int xlen1, int* Vec_Locs) {
+  if (!Map || !Grid1 || !Grid2 || len1 < 2 || len2 < 2 || len1 % 2 || len2 % 2 || xlen1 < 0 || xlen1 % 2 ||
+      len1_array < len1)
     return TRT_ERR_ARG;
   auto G1 = [&](long long i) { return Grid1[i - 1]; };   // 1-based, as the reference indexes
   auto G2 = [&](long long j) { return Grid2[j - 1]; };
@@ -851,13 +859,90 @@ int trt_map_grids(int* Map, const double* Grid1, const double* Grid2, int len1, 
     }
     for (int k = 0; k < 4; ++k) {
       // a grid 2 point outside grid 1's extent has no bracketing cell (the reference reads past its arrays)
-      if (l[k] < 1 || l[k] > len1 - 1) return TRT_ERR_ARG;
+      if (l[k] < 1 || l[k] > len1_array - 1) return TRT_ERR_ARG;
       Map[mp + k] = (int)l[k];
     }
     mp += 4;
   }
   if (Vec_Locs)
     for (long long j = 0; j < 2LL * len2; ++j) Vec_Locs[j] = (Map[j] + 1) / 2;
+  return TRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trt_map_grids(int* Map, const double* Grid1, const double* Grid2, int len1, int len2, int xlen1, int* Vec_Locs) {
+  return map_grids_impl(Map, Grid1, Grid2, len1, len1, len2, xlen1, Vec_Locs);
+}
+
+int trt_gridmap_gen_bnd(int side, const double* Del, double pos, int N, double* GridMap) {
+  if (!Del || !GridMap || N < 1 || (side != 0 && side != 1)) return TRT_ERR_ARG;
+  double loc = 0.0;
+  for (int i = 0; i < N; ++i) {   // GRIDMAP_GEN_LR_BND (side 0: x = pos) / GRIDMAP_GEN_BT_BND (side 1: y = pos)
+    loc = loc + Del[i] / 2.0;
+    GridMap[2 * i] = side == 0 ? pos : loc;
+    GridMap[2 * i + 1] = side == 0 ? loc : pos;
+    loc = loc + Del[i] / 2.0;
+  }
+  return TRT_OK;
+}
+
+int trt_generate_grids_xy(const double* Delx_d, const double* Dely_d, const double* Delx, const double* Dely,
+                          double xlen_d, double ylen_d, double xlen, double ylen, int dN_x, int dN_y, int N_x, int N_y,
+                          double* Sim_Grid_Avg, double* Sim_Grid_EdgV, double* Sim_Grid_EdgH, double* Sim_Grid_Bnds,
+                          double* Dat_Grid_Avg, double* Dat_Grid_EdgV, double* Dat_Grid_EdgH, double* Dat_Grid_Bnds,
+                          int* GMap_xyAvg, int* GMap_xyEdgV, int* GMap_xyEdgH, int* GMap_xyBnds, int* VMap_xyAvg,
+                          int* VMap_xyEdgV, int* VMap_xyEdgH, int* VMap_xyBnds) {
+  const void* ptrs[] = {Delx_d, Dely_d, Delx, Dely, Sim_Grid_Avg, Sim_Grid_EdgV, Sim_Grid_EdgH, Sim_Grid_Bnds,
+                        Dat_Grid_Avg, Dat_Grid_EdgV, Dat_Grid_EdgH, Dat_Grid_Bnds, GMap_xyAvg, GMap_xyEdgV,
+                        GMap_xyEdgH, GMap_xyBnds, VMap_xyAvg, VMap_xyEdgV, VMap_xyEdgH, VMap_xyBnds};
+  for (const void* q : ptrs)
+    if (!q) return TRT_ERR_ARG;
+  if (dN_x < 1 || dN_y < 1 || N_x < 1 || N_y < 1) return TRT_ERR_ARG;
+  // the data grid padded with a zero-width cell on each side
+  std::vector<double> Dx2((size_t)dN_x + 2, 0.0), Dy2((size_t)dN_y + 2, 0.0);
+  std::copy(Delx_d, Delx_d + dN_x, Dx2.begin() + 1);
+  std::copy(Dely_d, Dely_d + dN_y, Dy2.begin() + 1);
+  int rc;
+  if ((rc = trt_gridmap_gen(0, Delx, Dely, N_x, N_y, Sim_Grid_Avg)) ||
+      (rc = trt_gridmap_gen(1, Delx, Dely, N_x + 1, N_y, Sim_Grid_EdgV)) ||
+      (rc = trt_gridmap_gen(2, Delx, Dely, N_x, N_y + 1, Sim_Grid_EdgH)) ||
+      (rc = trt_gridmap_gen_bnd(0, Dely, 0.0, N_y, Sim_Grid_Bnds)) ||
+      (rc = trt_gridmap_gen_bnd(1, Delx, 0.0, N_x, Sim_Grid_Bnds + 2 * N_y)) ||
+      // the reference places the right side at ylen and the top at xlen (equal on its square domains)
+      (rc = trt_gridmap_gen_bnd(0, Dely, ylen, N_y, Sim_Grid_Bnds + 2 * (N_y + N_x))) ||
+      (rc = trt_gridmap_gen_bnd(1, Delx, xlen, N_x, Sim_Grid_Bnds + 4 * N_y + 2 * N_x)))
+    return rc;
+  if ((rc = trt_gridmap_gen(0, Dx2.data(), Dy2.data(), dN_x + 2, dN_y + 2, Dat_Grid_Avg)) ||
+      (rc = trt_gridmap_gen(1, Delx_d, Dy2.data(), dN_x + 1, dN_y + 2, Dat_Grid_EdgV)) ||
+      (rc = trt_gridmap_gen(2, Dx2.data(), Dely_d, dN_x + 2, dN_y + 1, Dat_Grid_EdgH)) ||
+      (rc = trt_gridmap_gen_bnd(0, Dy2.data(), 0.0, dN_y + 2, Dat_Grid_Bnds)) ||
+      (rc = trt_gridmap_gen_bnd(1, Dx2.data(), 0.0, dN_x + 2, Dat_Grid_Bnds + 2 * dN_y + 4)) ||
+      (rc = trt_gridmap_gen_bnd(0, Dy2.data(), ylen_d, dN_y + 2, Dat_Grid_Bnds + 2 * (dN_y + dN_x) + 8)) ||
+      (rc = trt_gridmap_gen_bnd(1, Dx2.data(), xlen_d, dN_x + 2, Dat_Grid_Bnds + 4 * dN_y + 2 * dN_x + 12)))
+    return rc;
+  const int la = 2 * (dN_x + 2) * (dN_y + 2), lv = 2 * (dN_x + 1) * (dN_y + 2), lh = 2 * (dN_x + 2) * (dN_y + 1);
+  if ((rc = map_grids_impl(GMap_xyAvg, Dat_Grid_Avg, Sim_Grid_Avg, la, la, 2 * N_x * N_y, 2 * (dN_x + 2), VMap_xyAvg)) ||
+      (rc = map_grids_impl(GMap_xyEdgV, Dat_Grid_EdgV, Sim_Grid_EdgV, lv, lv, 2 * (N_x + 1) * N_y, 2 * (dN_x + 1),
+                           VMap_xyEdgV)) ||
+      (rc = map_grids_impl(GMap_xyEdgH, Dat_Grid_EdgH, Sim_Grid_EdgH, lh, lh, 2 * N_x * (N_y + 1), 2 * (dN_x + 2),
+                           VMap_xyEdgH)))
+    return rc;
+  // boundary maps: each side's search covers all but its last point set entry (whose array holds one more the
+  // brackets may reach); the reference passes the left side's counts for all four sides, which is the same on
+  // its square grids and reads past its arrays on others
+  const int lby = 2 * dN_y + 2, lbx = 2 * dN_x + 2;
+  if ((rc = map_grids_impl(GMap_xyBnds, Dat_Grid_Bnds, Sim_Grid_Bnds, lby, lby + 2, 2 * N_y, 2, VMap_xyBnds)) ||
+      (rc = map_grids_impl(GMap_xyBnds + 4 * N_y, Dat_Grid_Bnds + 2 * dN_y + 4, Sim_Grid_Bnds + 2 * N_y, lbx,
+                           lbx + 2, 2 * N_x, 0, VMap_xyBnds + 4 * N_y)) ||
+      (rc = map_grids_impl(GMap_xyBnds + 4 * (N_y + N_x), Dat_Grid_Bnds + 2 * (dN_y + dN_x) + 8,
+                           Sim_Grid_Bnds + 2 * (N_y + N_x), lby, lby + 2, 2 * N_y, 2, VMap_xyBnds + 4 * (N_y + N_x))) ||
+      (rc = map_grids_impl(GMap_xyBnds + 8 * N_y + 4 * N_x, Dat_Grid_Bnds + 4 * dN_y + 2 * dN_x + 12,
+                           Sim_Grid_Bnds + 4 * N_y + 2 * N_x, lbx, lbx + 2, 2 * N_x, 0,
+                           VMap_xyBnds + 8 * N_y + 4 * N_x)))
+    return rc;
   return TRT_OK;
 }
 

@@ -505,6 +505,23 @@ int trt_gridmap_gen(int kind, const double* Delx, const double* Dely, int N_x, i
  * rejected with TRT_ERR_ARG (the reference would read past them); like the reference, the caller keeps grid 2's
  * points inside grid 1's extent.  Host code. */
 int trt_map_grids(int* Map, const double* Grid1, const double* Grid2, int len1, int len2, int xlen1, int* Vec_Locs);
+/* Replace SUBROUTINEs GRIDMAP_GEN_LR_BND (side 0) and GRIDMAP_GEN_BT_BND (side 1), MainSrc/GRID_FUNCTIONS.f08:158-200:
+ * the N points of a domain side, at x = pos (side 0, y at the midpoints of Del) or y = pos (side 1, x at the
+ * midpoints of Del), into GridMap(2 N).  Host code. */
+int trt_gridmap_gen_bnd(int side, const double* Del, double pos, int N, double* GridMap);
+/* Replaces SUBROUTINE GENERATE_GRIDS_XY, MainSrc/GRID_FUNCTIONS.f08:689-749: the simulation grid's point sets
+ * (cell centres 2 N_x N_y, vertical edges 2 (N_x+1) N_y, horizontal edges 2 N_x (N_y+1), boundaries 4 (N_x+N_y):
+ * left, bottom, right at x = ylen, top at y = xlen, the reference's placement), the data grid's point sets on its
+ * cells padded with a zero-width cell on each side (2 (dN_x+2)(dN_y+2), 2 (dN_x+1)(dN_y+2), 2 (dN_x+2)(dN_y+1),
+ * 4 (dN_x+dN_y)+16), and MAP_GRIDS of each pair (GMap_/VMap_ with twice the simulation set's values).  Each
+ * boundary map uses its own side's counts, which equals the reference's calls on its square grids (it passes
+ * the left side's counts for all four sides).  Host code. */
+int trt_generate_grids_xy(const double* Delx_d, const double* Dely_d, const double* Delx, const double* Dely,
+                          double xlen_d, double ylen_d, double xlen, double ylen, int dN_x, int dN_y, int N_x, int N_y,
+                          double* Sim_Grid_Avg, double* Sim_Grid_EdgV, double* Sim_Grid_EdgH, double* Sim_Grid_Bnds,
+                          double* Dat_Grid_Avg, double* Dat_Grid_EdgV, double* Dat_Grid_EdgH, double* Dat_Grid_Bnds,
+                          int* GMap_xyAvg, int* GMap_xyEdgV, int* GMap_xyEdgH, int* GMap_xyBnds, int* VMap_xyAvg,
+                          int* VMap_xyEdgV, int* VMap_xyEdgH, int* VMap_xyBnds);
 /* Replaces SUBROUTINE GENERATE_GRIDS_T, MainSrc/GRID_FUNCTIONS.f08:754-814: the data and simulation time levels and
  * TMap(2, N_t), for every simulation level the two data levels (1-based) that bracket it (equal when it coincides
  * with one within 1e-14 relative, or lies outside the data range).  Host code. */

@@ -769,16 +769,19 @@ def gridmap_gen(kind, Delx, Dely, N_x, N_y):
     return np.array(out)
 
 
-def map_grids(Grid1, Grid2, xlen1):
+def map_grids(Grid1, Grid2, xlen1, len1=None, len2=None):
     """MAP_GRIDS (MainSrc/GRID_FUNCTIONS.f08:222-327): GMap (1-based x indices of the four bracketing points of
-    grid 1 for every grid-2 point) and VMap = (GMap + 1) / 2."""
+    grid 1 for every grid-2 point) and VMap = (GMap + 1) / 2.  len1 / len2 (default: the arrays' lengths) are the
+    reference's counts of values searched and mapped, which its boundary maps set below the arrays' lengths."""
     import math
+    len1 = len(Grid1) if len1 is None else len1
+    len2 = len(Grid2) if len2 is None else len2
     G1 = lambda i: Grid1[i - 1]
     G2 = lambda j: Grid2[j - 1]
     Map = []
-    for j in range(1, len(Grid2) + 1, 2):
+    for j in range(1, len2 + 1, 2):
         d, l1 = np.finfo(np.float64).max, 0
-        for i in range(1, len(Grid1) + 1, 2):
+        for i in range(1, len1 + 1, 2):
             r = abs(math.sqrt((G1(i) - G2(j)) ** 2 + (G1(i + 1) - G2(j + 1)) ** 2))
             if r < d:
                 d, l1 = r, i
@@ -807,6 +810,46 @@ def map_grids(Grid1, Grid2, xlen1):
         Map += l
     Map = np.array(Map, dtype=np.int32)
     return Map, (Map + 1) // 2
+
+
+def gridmap_gen_bnd(side, Del, pos, N):
+    """GRIDMAP_GEN_LR_BND (side 0, x = pos) / GRIDMAP_GEN_BT_BND (side 1, y = pos),
+    MainSrc/GRID_FUNCTIONS.f08:158-200: the side's N points at the midpoints of Del."""
+    out, loc = [], 0.0
+    for i in range(N):
+        loc = loc + Del[i] / 2.0
+        out += [pos, loc] if side == 0 else [loc, pos]
+        loc = loc + Del[i] / 2.0
+    return np.array(out)
+
+
+def generate_grids_xy(Delx_d, Dely_d, Delx, Dely, xlen_d, ylen_d, xlen, ylen):
+    """GENERATE_GRIDS_XY (MainSrc/GRID_FUNCTIONS.f08:689-749), its calls in order, on square grids (N_x = N_y,
+    dN_x = dN_y): the reference's boundary maps pass the left side's counts for all four sides and read past the
+    point sets elsewhere.  Returns the dict of point sets and maps keyed by the reference's names."""
+    dN_x, dN_y, N_x, N_y = len(Delx_d), len(Dely_d), len(Delx), len(Dely)
+    assert N_x == N_y and dN_x == dN_y, "the reference's boundary maps are defined on square grids"
+    Dx2, Dy2 = [0.0] + list(Delx_d) + [0.0], [0.0] + list(Dely_d) + [0.0]
+    o = {"Sim_Grid_Avg": gridmap_gen(0, Delx, Dely, N_x, N_y), "Sim_Grid_EdgV": gridmap_gen(1, Delx, Dely, N_x + 1, N_y),
+         "Sim_Grid_EdgH": gridmap_gen(2, Delx, Dely, N_x, N_y + 1),
+         "Sim_Grid_Bnds": np.concatenate([gridmap_gen_bnd(0, Dely, 0.0, N_y), gridmap_gen_bnd(1, Delx, 0.0, N_x),
+                                          gridmap_gen_bnd(0, Dely, ylen, N_y), gridmap_gen_bnd(1, Delx, xlen, N_x)]),
+         "Dat_Grid_Avg": gridmap_gen(0, Dx2, Dy2, dN_x + 2, dN_y + 2),
+         "Dat_Grid_EdgV": gridmap_gen(1, Delx_d, Dy2, dN_x + 1, dN_y + 2),
+         "Dat_Grid_EdgH": gridmap_gen(2, Dx2, Dely_d, dN_x + 2, dN_y + 1),
+         "Dat_Grid_Bnds": np.concatenate([gridmap_gen_bnd(0, Dy2, 0.0, dN_y + 2), gridmap_gen_bnd(1, Dx2, 0.0, dN_x + 2),
+                                          gridmap_gen_bnd(0, Dy2, ylen_d, dN_y + 2),
+                                          gridmap_gen_bnd(1, Dx2, xlen_d, dN_x + 2)])}
+    for k, xl in (("Avg", 2 * (dN_x + 2)), ("EdgV", 2 * (dN_x + 1)), ("EdgH", 2 * (dN_x + 2))):
+        o["GMap_xy" + k], o["VMap_xy" + k] = map_grids(o["Dat_Grid_" + k], o["Sim_Grid_" + k], xl)
+    gm, vm = np.zeros(8 * (N_x + N_y), dtype=np.int32), np.zeros(8 * (N_x + N_y), dtype=np.int32)
+    for go, do, so, xl in ((0, 0, 0, 2), (4 * N_y, 2 * dN_y + 4, 2 * N_y, 0),
+                           (4 * (N_y + N_x), 2 * (dN_y + dN_x) + 8, 2 * (N_y + N_x), 2),
+                           (8 * N_y + 4 * N_x, 4 * dN_y + 2 * dN_x + 12, 4 * N_y + 2 * N_x, 0)):
+        g, v = map_grids(o["Dat_Grid_Bnds"][do:], o["Sim_Grid_Bnds"][so:], xl, 2 * dN_y + 2, 2 * N_y)
+        gm[go:go + g.size], vm[go:go + v.size] = g, v
+    o["GMap_xyBnds"], o["VMap_xyBnds"] = gm, vm
+    return o
 
 
 def generate_grids_t(Delt_d, Delt, Start_Time_d, Start_Time, dN_t, N_t):

@@ -418,3 +418,53 @@ def test_time_map_and_boundary_helpers_match_oracle(oracle):
     assert L.trt_avg_apnd_bnd(out.ctypes.data_as(D), fp, lr.ctypes.data_as(D), bt.ctypes.data_as(D),
                               crn.ctypes.data_as(D), ng, ny, nx) == 0
     assert np.array_equal(out, oracle.avg_apnd_bnd(f, lr, bt, crn, ng, ny, nx))
+
+
+def _map_linear_field(oracle, g, f, dN_x, dN_y, N_x, N_y):
+    """FMAP (the oracle's) of the linear field f from every data point set to the simulation's, the four boundary
+    sides one at a time with their own offsets, as the reconstructions call it (POD_ROUTINES.f08:335-347)."""
+    for k in ("Avg", "EdgV", "EdgH"):
+        G1, G2 = g["Dat_Grid_" + k], g["Sim_Grid_" + k]
+        n1, n2 = G1.size // 2, G2.size // 2
+        f2 = oracle.fmap(f(G1), G1, G2, g["GMap_xy" + k], g["VMap_xy" + k], n1, n2, n2)
+        np.testing.assert_allclose(f2, f(G2), rtol=1e-12, atol=1e-12, err_msg=k)
+    for do, so, mo, n1, n2 in ((0, 0, 0, dN_y + 2, N_y), (2 * dN_y + 4, 2 * N_y, 4 * N_y, dN_x + 2, N_x),
+                               (2 * (dN_y + dN_x) + 8, 2 * (N_y + N_x), 4 * (N_y + N_x), dN_y + 2, N_y),
+                               (4 * dN_y + 2 * dN_x + 12, 4 * N_y + 2 * N_x, 8 * N_y + 4 * N_x, dN_x + 2, N_x)):
+        G1, G2 = g["Dat_Grid_Bnds"][do:do + 2 * n1], g["Sim_Grid_Bnds"][so:so + 2 * n2]
+        f2 = oracle.fmap(f(G1), G1, G2, g["GMap_xyBnds"][mo:mo + 4 * n2], g["VMap_xyBnds"][mo:mo + 4 * n2], n1, n2,
+                         n2)
+        np.testing.assert_allclose(f2, f(G2), rtol=1e-12, atol=1e-12, err_msg="Bnds")
+
+
+@pytest.mark.parametrize("dN,N", [(6, 9), (9, 5), (4, 4)])
+def test_generate_grids_xy_matches_oracle(oracle, dN, N):
+    """GENERATE_GRIDS_XY with GRIDMAP_GEN_LR/BT_BND (host code of the library, no device) against the restatement
+    of the reference's calls on square grids of uneven widths, and the maps drive FMAP (the oracle's) to reproduce
+    a linear field on every point set from the padded data grid."""
+    rng = np.random.default_rng(dN * 10 + N)
+    L = 2.0
+    dxd, dyd = rng.uniform(0.5, 1.5, dN), rng.uniform(0.5, 1.5, dN)
+    dxd, dyd = dxd * (L / dxd.sum()), dyd * (L / dyd.sum())
+    dx, dy = rng.uniform(0.5, 1.5, N), rng.uniform(0.5, 1.5, N)
+    dx, dy = dx * (L / dx.sum()), dy * (L / dy.sum())
+    got = pkg.GENERATE_GRIDS_XY(dxd, dyd, dx, dy, dxd.sum(), dyd.sum(), dx.sum(), dy.sum())
+    ref = oracle.generate_grids_xy(dxd, dyd, dx, dy, dxd.sum(), dyd.sum(), dx.sum(), dy.sum())
+    assert set(got) == set(ref)
+    for k in ref:
+        assert got[k].shape == ref[k].shape and np.array_equal(got[k], ref[k]), k
+    assert np.array_equal(pkg.GRIDMAP_GEN_BND(1, dx, 0.5, N), oracle.gridmap_gen_bnd(1, dx, 0.5, N))
+    _map_linear_field(oracle, got, lambda g: 1.5 + 0.4 * g[0::2] - 0.9 * g[1::2], dN, dN, N, N)
+
+
+def test_generate_grids_xy_rectangular_grids(oracle):
+    """On grids with different x and y counts each boundary map uses its own side's counts (the reference's calls
+    are defined on square grids only): every point set still maps a linear field exactly."""
+    rng = np.random.default_rng(3)
+    dxd, dyd, dx, dy = (rng.uniform(0.5, 1.5, n) for n in (7, 4, 5, 8))
+    dyd, dx, dy = dyd * (dxd.sum() / dyd.sum()), dx * (dxd.sum() / dx.sum()), dy * (dxd.sum() / dy.sum())
+    L = dxd.sum()
+    got = pkg.GENERATE_GRIDS_XY(dxd, dyd, dx, dy, L, L, L, L)
+    _map_linear_field(oracle, got, lambda g: -0.5 + 1.1 * g[0::2] + 0.3 * g[1::2], 7, 4, 5, 8)
+    with pytest.raises(pkg.TrtError):
+        pkg.GENERATE_GRIDS_XY(dxd, dyd, dx[:0], dy, L, L, L, L)
