@@ -405,6 +405,111 @@ def GENERATE_GRIDS_XY(Delx_d, Dely_d, Delx, Dely, xlen_d, ylen_d, xlen, ylen):
     return out
 
 
+_FG_FIELDS = ("avg_xx", "edgV_xx", "avg_yy", "edgH_yy", "edgV_xy", "edgH_xy")   # the decompositions' order
+_FG_OUT = ("fg_avg_xx", "fg_avg_yy", "fg_edgV_xx", "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy")
+
+
+def _fg_out(dN_x, dN_y, N_x, N_y, N_g):
+    na, nv, nh = N_x * N_y * N_g, (N_x + 1) * N_y * N_g, N_x * (N_y + 1) * N_g
+    return {k: np.zeros(n) for k, n in zip(_FG_OUT, (na, na, nv, nv, nh, nh))}
+
+
+def _grid_args(grids, sets):
+    return [dptr(np.ascontiguousarray(grids[p + k], dtype=np.float64)) for p in ("Sim_Grid_", "Dat_Grid_")
+            for k in sets], [iptr(np.ascontiguousarray(grids[p + k], dtype=np.int32)) for p in ("GMap_xy", "VMap_xy")
+                             for k in sets]
+
+
+def _dec_args(parts, n_real):
+    """Pointers of one decomposition: the first n_real arrays float64, the rest complex128 (as interleaved
+    doubles), then the rank array."""
+    keep, ptrs = [], []
+    for i, a in enumerate(parts[:-1]):
+        if i < n_real:
+            v = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1, order="F"))
+        else:
+            v = np.ascontiguousarray(np.asarray(a, dtype=np.complex128).reshape(-1, order="F")).view(np.float64)
+        keep.append(v)
+        ptrs.append(dptr(v))
+    r = np.ascontiguousarray(parts[-1], dtype=np.int32)
+    keep.append(r)
+    return keep, ptrs, iptr(r)
+
+
+def POD_RECONSTRUCT_fg(dec, dN, N, t, PODgsum, grids, tgrids):
+    """trt_pod_reconstruct_fg: dict of the six QD factors on the simulation grid at simulation level t.
+    dec[name] = (C, S, U, V, rank) for name in avg_xx, edgV_xx, avg_yy, edgH_yy, edgV_xy, edgH_xy;
+    dN = (dN_x, dN_y, dN_g, dN_t), N = (N_x, N_y, N_g, N_t); grids from GENERATE_GRIDS_XY; tgrids =
+    (Sim_TGrid, Dat_TGrid, TMap)."""
+    dN_x, dN_y, dN_g, dN_t = dN
+    N_x, N_y, N_g, N_t = N
+    out = _fg_out(dN_x, dN_y, N_x, N_y, N_g)
+    keep, dec_ptrs, ranks = [], [], []
+    for name in _FG_FIELDS:
+        k, p, r = _dec_args(dec[name], 4)
+        keep += k
+        dec_ptrs += p
+        ranks.append(r)
+    g, m = _grid_args(grids, ("Avg", "EdgV", "EdgH"))
+    tg = [np.ascontiguousarray(a, dtype=np.float64) for a in tgrids[:2]]
+    tm = np.ascontiguousarray(tgrids[2], dtype=np.int32)
+    check(_lib.lib().trt_pod_reconstruct_fg(*[dptr(out[k]) for k in _FG_OUT], *dec_ptrs, *ranks, dN_x, dN_y, dN_g,
+                                            dN_t, N_x, N_y, N_g, N_t, int(t), int(PODgsum), *g, *[dptr(a) for a in tg],
+                                            *m, iptr(tm)), "trt_pod_reconstruct_fg")
+    return out
+
+
+def POD_RECONSTRUCT_BCg(dec, dN, N, t, PODgsum, grids, tgrids):
+    """trt_pod_reconstruct_bcg: (Cg_L, Cg_B, Cg_R, Cg_T) at simulation level t; dec = (C, S, U, V, rank)."""
+    dN_x, dN_y, dN_g, dN_t = dN
+    N_x, N_y, N_g, N_t = N
+    out = [np.zeros(N_g * n) for n in (N_y, N_x, N_y, N_x)]
+    keep, p, r = _dec_args(dec, 4)
+    tg = [np.ascontiguousarray(a, dtype=np.float64) for a in tgrids[:2]]
+    tm = np.ascontiguousarray(tgrids[2], dtype=np.int32)
+    gb = [np.ascontiguousarray(grids[k], dtype=np.float64) for k in ("Sim_Grid_Bnds", "Dat_Grid_Bnds")]
+    mb = [np.ascontiguousarray(grids[k], dtype=np.int32) for k in ("GMap_xyBnds", "VMap_xyBnds")]
+    check(_lib.lib().trt_pod_reconstruct_bcg(*[dptr(o) for o in out], *p, r, dN_x, dN_y, dN_g, dN_t, N_x, N_y, N_g,
+                                             N_t, int(t), int(PODgsum), *[dptr(a) for a in gb + tg],
+                                             *[iptr(a) for a in mb], iptr(tm)), "trt_pod_reconstruct_bcg")
+    return tuple(out)
+
+
+def DMD_RECONSTRUCT_fg(dec, dN, N, Time, DMDgsum, grids):
+    """trt_dmd_reconstruct_fg: dict of the six QD factors on the simulation grid at Time.
+    dec[name] = (L, B, W, C, rank) (L, B, W complex); dN = (dN_x, dN_y, dN_g), N = (N_x, N_y, N_g)."""
+    dN_x, dN_y, dN_g = dN
+    N_x, N_y, N_g = N
+    out = _fg_out(dN_x, dN_y, N_x, N_y, N_g)
+    keep, dec_ptrs, ranks = [], [], []
+    for name in _FG_FIELDS:
+        L_, B_, W_, C_, r_ = dec[name]
+        k, p, r = _dec_args((C_, L_, B_, W_, r_), 1)
+        keep += k
+        dec_ptrs += [p[1], p[2], p[3], p[0]]
+        ranks.append(r)
+    g, m = _grid_args(grids, ("Avg", "EdgV", "EdgH"))
+    check(_lib.lib().trt_dmd_reconstruct_fg(*[dptr(out[k]) for k in _FG_OUT], *dec_ptrs, *ranks, dN_x, dN_y, dN_g,
+                                            N_x, N_y, N_g, float(Time), int(DMDgsum), *g, *m),
+          "trt_dmd_reconstruct_fg")
+    return out
+
+
+def DMD_RECONSTRUCT_BCg(dec, dN, N, Time, DMDgsum, grids):
+    """trt_dmd_reconstruct_bcg: (Cg_L, Cg_B, Cg_R, Cg_T) at Time; dec = (L, B, W, C, rank)."""
+    dN_x, dN_y, dN_g = dN
+    N_x, N_y, N_g = N
+    out = [np.zeros(N_g * n) for n in (N_y, N_x, N_y, N_x)]
+    L_, B_, W_, C_, r_ = dec
+    keep, p, r = _dec_args((C_, L_, B_, W_, r_), 1)
+    gb = [np.ascontiguousarray(grids[k], dtype=np.float64) for k in ("Sim_Grid_Bnds", "Dat_Grid_Bnds")]
+    mb = [np.ascontiguousarray(grids[k], dtype=np.int32) for k in ("GMap_xyBnds", "VMap_xyBnds")]
+    check(_lib.lib().trt_dmd_reconstruct_bcg(*[dptr(o) for o in out], p[1], p[2], p[3], p[0], r, dN_x, dN_y, dN_g,
+                                             N_x, N_y, N_g, float(Time), int(DMDgsum), *[dptr(a) for a in gb],
+                                             *[iptr(a) for a in mb]), "trt_dmd_reconstruct_bcg")
+    return tuple(out)
+
+
 def LINEAR_INTERPOLATION(v1, v2, xm, x1, x2, len_):
     """trt_linear_interpolation, in place on v1 (float64)."""
     b = np.ascontiguousarray(np.asarray(v2, dtype=np.float64).reshape(-1))

@@ -8,6 +8,7 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -270,6 +271,107 @@ int pod_device(const double* X, long long col_stride, long long clen, int n_t, d
   return TRT_OK;
 }
 
+// LINEAR_INTERPOLATION: v1 = v1 + (xm - x1) (v2 - v1) / (x2 - x1), value by value.
+__global__ void linear_interpolation_kernel(double* __restrict__ v1, const double* __restrict__ v2, double xm, double x1,
+                                            double x2, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    v1[k] = v1[k] + (xm - x1) * (v2[k] - v1[k]) / (x2 - x1);
+}
+
+// Offsets of each block's modes (the sum of the earlier ranks), every rank checked against [0, max_rank].
+int mode_offsets(const int* rank, int nb, long long max_rank, std::vector<long long>& off, long long& tot) {
+  off.assign((size_t)nb, 0);
+  tot = 0;
+  for (int g = 0; g < nb; ++g) {
+    if (rank[g] < 0 || rank[g] > max_rank) return TRT_ERR_ARG;
+    off[g] = tot;
+    tot += rank[g];
+  }
+  return TRT_OK;
+}
+
+// POD_RECONSTRUCT of one field (len values; N_g blocks with PODgsum = 0, one with PODgsum = 1) from host
+// decomposition arrays into device memory dst at data time level a (1-based); when level b differs, also at b,
+// followed by LINEAR_INTERPOLATION(dst, level b, xm, x1, x2), as the reconstruction drivers do.
+int pod_field(Dev& dv, double* dst, const double* C, const double* S, const double* U, const double* V,
+              const int* rank, long long len, int N_g, int N_t, int PODgsum, int a, int b, double xm, double x1,
+              double x2) {
+  if (!C || !S || !U || !V || !rank || len < 1 || N_t < 1 || a < 1 || a > N_t || b < 1 || b > N_t ||
+      (PODgsum != 0 && PODgsum != 1) || (PODgsum == 0 && (N_g < 1 || len % N_g != 0)) || (a != b && !(x2 != x1)))
+    return TRT_ERR_ARG;
+  const int nb = PODgsum == 0 ? N_g : 1;
+  const long long glen = len / nb;
+  std::vector<long long> off;
+  long long tot = 0;
+  int rc = mode_offsets(rank, nb, std::min<long long>(glen, N_t), off, tot);
+  if (rc) return rc;
+  double *dC, *dS, *dU, *dV;
+  int* dr;
+  long long* doff;
+  if ((rc = dv.get(&dC, (size_t)len)) || (rc = dv.get(&dS, (size_t)tot)) || (rc = dv.get(&dU, (size_t)(glen * tot))) ||
+      (rc = dv.get(&dV, (size_t)(N_t * tot))) || (rc = dv.get(&dr, (size_t)nb)) || (rc = dv.get(&doff, (size_t)nb)))
+    return rc;
+  ROM_CUDA(cudaMemcpy(dC, C, (size_t)len * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dS, S, (size_t)tot * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dU, U, (size_t)(glen * tot) * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dV, V, (size_t)(N_t * tot) * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dr, rank, (size_t)nb * sizeof(int), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(doff, off.data(), (size_t)nb * sizeof(long long), cudaMemcpyHostToDevice));
+  pod_reconstruct_kernel<<<grid_of(len), 256>>>(glen, nb, N_t, a - 1, dr, doff, dC, dS, dU, dV, dst);
+  trt_host::add_launches(1);
+  if (b != a) {
+    double* f3;
+    if ((rc = dv.get(&f3, (size_t)len))) return rc;
+    pod_reconstruct_kernel<<<grid_of(len), 256>>>(glen, nb, N_t, b - 1, dr, doff, dC, dS, dU, dV, f3);
+    linear_interpolation_kernel<<<grid_of(len), 256>>>(dst, f3, xm, x1, x2, len);
+    trt_host::add_launches(2);
+  }
+  ROM_CUDA(cudaGetLastError());
+  return TRT_OK;
+}
+
+// DMD_RECONSTRUCT of one field (len values; N_g blocks with DMDgsum = 0) at time Time from host arrays (L, B, W
+// as interleaved complex doubles) into device memory dst.
+int dmd_field(Dev& dv, double* dst, const double* L, const double* B, const double* W, const double* C,
+              const int* rank, long long len, int N_g, int DMDgsum, double Time) {
+  if (!L || !B || !W || !C || !rank || len < 1 || (DMDgsum != 0 && DMDgsum != 1) ||
+      (DMDgsum == 0 && (N_g < 1 || len % N_g != 0)))
+    return TRT_ERR_ARG;
+  const int nb = DMDgsum == 0 ? N_g : 1;
+  const long long glen = len / nb;
+  std::vector<long long> off;
+  long long tot = 0;
+  int rc = mode_offsets(rank, nb, std::numeric_limits<int>::max(), off, tot);
+  if (rc) return rc;
+  // exp(L(r) Time) once per mode (the reference evaluates it once per mode too, before the value loop)
+  std::vector<double> E(2 * (size_t)tot);
+  for (long long r = 0; r < tot; ++r) {
+    const double zr = L[2 * r] * Time, zi = L[2 * r + 1] * Time;
+    const double m = std::exp(zr);
+    E[2 * r] = m * std::cos(zi);
+    E[2 * r + 1] = m * std::sin(zi);
+  }
+  double *dC, *dB, *dW, *dE;
+  int* dr;
+  long long* doff;
+  if ((rc = dv.get(&dC, (size_t)len)) || (rc = dv.get(&dB, 2 * (size_t)tot)) ||
+      (rc = dv.get(&dW, 2 * (size_t)(glen * tot))) || (rc = dv.get(&dE, 2 * (size_t)tot)) ||
+      (rc = dv.get(&dr, (size_t)nb)) || (rc = dv.get(&doff, (size_t)nb)))
+    return rc;
+  ROM_CUDA(cudaMemcpy(dC, C, (size_t)len * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dB, B, 2 * (size_t)tot * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dW, W, 2 * (size_t)(glen * tot) * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dE, E.data(), E.size() * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(dr, rank, (size_t)nb * sizeof(int), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(doff, off.data(), (size_t)nb * sizeof(long long), cudaMemcpyHostToDevice));
+  dmd_reconstruct_kernel<<<grid_of(len), 256>>>(glen, nb, dr, doff, dC, reinterpret_cast<const double2*>(dB),
+                                               reinterpret_cast<const double2*>(dW),
+                                               reinterpret_cast<const double2*>(dE), dst);
+  trt_host::add_launches(1);
+  ROM_CUDA(cudaGetLastError());
+  return TRT_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -320,30 +422,11 @@ int trt_pod_reconstruct(double* dat, const double* C, const double* S, const dou
     return TRT_ERR_ARG;
   int rc = device_present();
   if (rc) return rc;
-  const int nb = PODgsum == 0 ? N_g : 1;
-  const long long glen = len / nb;
-  std::vector<long long> off(nb);
-  long long tot = 0;
-  for (int g = 0; g < nb; ++g) {
-    if (rank[g] < 0 || rank[g] > std::min<long long>(glen, N_t)) return TRT_ERR_ARG;
-    off[g] = tot;
-    tot += rank[g];
-  }
   Dev dv;
-  double *dC, *dS, *dU, *dV, *dd;
-  int* dr;
-  long long* doff;
-  if ((rc = dv.get(&dC, (size_t)len)) || (rc = dv.get(&dS, (size_t)tot)) || (rc = dv.get(&dU, (size_t)(glen * tot))) ||
-      (rc = dv.get(&dV, (size_t)(N_t * tot))) || (rc = dv.get(&dd, (size_t)len)) || (rc = dv.get(&dr, (size_t)nb)) ||
-      (rc = dv.get(&doff, (size_t)nb)))
+  double* dd;
+  if ((rc = dv.get(&dd, (size_t)std::max(len, 1))) ||
+      (rc = pod_field(dv, dd, C, S, U, V, rank, len, N_g, N_t, PODgsum, t, t, 0.0, 0.0, 0.0)))
     return rc;
-  ROM_CUDA(cudaMemcpy(dC, C, (size_t)len * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(dS, S, (size_t)tot * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(dU, U, (size_t)(glen * tot) * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(dV, V, (size_t)(N_t * tot) * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(dr, rank, (size_t)nb * sizeof(int), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(doff, off.data(), (size_t)nb * sizeof(long long), cudaMemcpyHostToDevice));
-  if ((rc = trt_pod_reconstruct_device(dd, dC, dS, dU, dV, dr, doff, len, nb, N_t, t, nullptr))) return rc;
   ROM_CUDA(cudaMemcpy(dat, dd, (size_t)len * sizeof(double), cudaMemcpyDeviceToHost));
   return TRT_OK;
 }
@@ -370,42 +453,11 @@ int trt_dmd_reconstruct(double* dat, const double* L, const double* B, const dou
     return TRT_ERR_ARG;
   int rc = device_present();
   if (rc) return rc;
-  const int nb = DMDgsum == 0 ? N_g : 1;
-  const long long glen = len / nb;
-  std::vector<long long> off(nb);
-  long long tot = 0;
-  for (int g = 0; g < nb; ++g) {
-    if (rank[g] < 0) return TRT_ERR_ARG;
-    off[g] = tot;
-    tot += rank[g];
-  }
-  // exp(L(r) Time) once per mode (the reference evaluates it once per mode too, before the value loop)
-  std::vector<double> E(2 * (size_t)tot);
-  for (long long r = 0; r < tot; ++r) {
-    const double zr = L[2 * r] * Time, zi = L[2 * r + 1] * Time;
-    const double m = std::exp(zr);
-    E[2 * r] = m * std::cos(zi);
-    E[2 * r + 1] = m * std::sin(zi);
-  }
   Dev dv;
-  double *dC, *dB, *dW, *dE, *dd;
-  int* dr;
-  long long* doff;
-  if ((rc = dv.get(&dC, (size_t)len)) || (rc = dv.get(&dB, 2 * (size_t)tot)) ||
-      (rc = dv.get(&dW, 2 * (size_t)(glen * tot))) || (rc = dv.get(&dE, 2 * (size_t)tot)) ||
-      (rc = dv.get(&dd, (size_t)len)) || (rc = dv.get(&dr, (size_t)nb)) || (rc = dv.get(&doff, (size_t)nb)))
+  double* dd;
+  if ((rc = dv.get(&dd, (size_t)std::max(len, 1))) ||
+      (rc = dmd_field(dv, dd, L, B, W, C, rank, len, N_g, DMDgsum, Time)))
     return rc;
-  ROM_CUDA(cudaMemcpy(dC, C, (size_t)len * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(dB, B, 2 * (size_t)tot * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(dW, W, 2 * (size_t)(glen * tot) * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(dE, E.data(), E.size() * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(dr, rank, (size_t)nb * sizeof(int), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(doff, off.data(), (size_t)nb * sizeof(long long), cudaMemcpyHostToDevice));
-  dmd_reconstruct_kernel<<<grid_of(len), 256>>>(glen, nb, dr, doff, dC, reinterpret_cast<const double2*>(dB),
-                                               reinterpret_cast<const double2*>(dW),
-                                               reinterpret_cast<const double2*>(dE), dd);
-  trt_host::add_launches(1);
-  ROM_CUDA(cudaGetLastError());
   ROM_CUDA(cudaMemcpy(dat, dd, (size_t)len * sizeof(double), cudaMemcpyDeviceToHost));
   return TRT_OK;
 }
@@ -716,13 +768,6 @@ __global__ void fmap_kernel(const double* __restrict__ f1, double* __restrict__ 
     f2[k] = bilinear(f[vm[0]], f[vm[2]], f[vm[1]], f[vm[3]], G2[2 * j], G1[gm[0] - 1], G1[gm[3] - 1], G2[2 * j + 1],
                      G1[gm[0]], G1[gm[3]]);
   }
-}
-
-// LINEAR_INTERPOLATION: v1 = v1 + (xm - x1) (v2 - v1) / (x2 - x1), value by value.
-__global__ void linear_interpolation_kernel(double* __restrict__ v1, const double* __restrict__ v2, double xm, double x1,
-                                            double x2, long long n) {
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-    v1[k] = v1[k] + (xm - x1) * (v2[k] - v1[k]) / (x2 - x1);
 }
 
 }  // namespace
@@ -1074,6 +1119,337 @@ int trt_avg_apnd_bnd(double* f_out, const double* f_in, const double* LR_Bnd, co
     f_out[po++] = Crn_Bnd[pc++];
   }
   return TRT_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Online reconstruction drivers: POD_RECONSTRUCT_fg / _BCg (MainSrc/POD_ROUTINES.f08:28-353) and
+// DMD_RECONSTRUCT_fg / _BCg (MainSrc/DMD_ROUTINES.f08:131-424).  Every field is reconstructed on the data grid
+// (POD: at one data time level, or at the two that bracket the step with the linear time interpolation between
+// them; DMD: at the step's time), padded with the values the reference appends for the mapping (EXTND_BT_BND,
+// EXTND_LR_BND, AVG_APND_BND of COLLECT_*_BND values; the boundary factors' end values repeated) and mapped to
+// the simulation grid by FMAP, all on the device.  The padding only moves values, so every output equals the
+// reference's sequence of calls.
+// ------------------------------------------------------------------------------------------------
+
+namespace {
+
+enum PadKind { PAD_BT = 0, PAD_LR = 1, PAD_AVG_XX = 2, PAD_AVG_YY = 3 };
+
+__device__ __forceinline__ int clamp_to(int v, int hi) { return v < 0 ? 0 : (v > hi ? hi : v); }
+
+// One padded field per group from an ny x nx field f.  PAD_BT: EXTND_BT_BND (first and last rows repeated below
+// and above; ny + 2 rows).  PAD_LR: EXTND_LR_BND (first and last columns repeated; nx + 2 columns).  PAD_AVG_XX
+// / PAD_AVG_YY: AVG_APND_BND (ny + 2 by nx + 2) of a cell field framed by its own first/last rows, columns and
+// corners, except the left/right columns, which XX takes from the first and last columns of the vertical-edge
+// field side (ny by nx + 1), and the bottom/top rows, which YY takes from the first and last rows of the
+// horizontal-edge field side (ny + 1 by nx).
+__global__ void pad_kernel(int kind, const double* __restrict__ f, const double* __restrict__ side, int n_g, int ny,
+                           int nx, double* __restrict__ out) {
+  const long long R = kind == PAD_LR ? ny : ny + 2, Cc = kind == PAD_BT ? nx : nx + 2;
+  const long long n = (long long)n_g * R * Cc;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const long long g = k / (R * Cc), rem = k % (R * Cc);
+    const int r = (int)(rem / Cc), c = (int)(rem % Cc);
+    const double* fg = f + g * ny * nx;
+    double v;
+    if (kind == PAD_BT)
+      v = fg[(long long)clamp_to(r - 1, ny - 1) * nx + c];
+    else if (kind == PAD_LR)
+      v = fg[(long long)r * nx + clamp_to(c - 1, nx - 1)];
+    else if (kind == PAD_AVG_XX && r >= 1 && r <= ny && (c == 0 || c == nx + 1))
+      v = side[g * ny * (nx + 1) + (long long)(r - 1) * (nx + 1) + (c == 0 ? 0 : nx)];
+    else if (kind == PAD_AVG_YY && c >= 1 && c <= nx && (r == 0 || r == ny + 1))
+      v = side[g * (ny + 1) * nx + (long long)(r == 0 ? 0 : ny) * nx + (c - 1)];
+    else
+      v = fg[(long long)clamp_to(r - 1, ny - 1) * nx + clamp_to(c - 1, nx - 1)];
+    out[k] = v;
+  }
+}
+
+// One boundary factor side per group (the CL2 / CB2 / CR2 / CT2 of the BCg drivers): the side's n values at
+// offset off of each group's block of blk values, with the first repeated before and the last after.
+__global__ void side_pad_kernel(const double* __restrict__ BC, int n_g, long long blk, long long off, int n,
+                                double* __restrict__ out) {
+  const long long m = (long long)n_g * (n + 2);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x) {
+    const long long g = k / (n + 2);
+    const int j = (int)(k % (n + 2));
+    out[k] = BC[g * blk + off + clamp_to(j - 1, n - 1)];
+  }
+}
+
+// A point-set pair with its maps (host arrays): the data grid (glen1 points), the simulation grid (glen2) and
+// GMap / VMap (4 glen2 entries each).
+struct MapSet {
+  const double* dat;
+  const double* sim;
+  const int* gmap;
+  const int* vmap;
+  long long glen1, glen2;
+};
+
+struct DevSet {
+  double *dat, *sim;
+  int *gmap, *vmap;
+  int glen1, glen2;
+};
+
+// Checks a set's maps on the host (every VMap entry a value of the block, every GMap entry an x of grid 1), then
+// uploads the grids and maps.
+int upload_set(Dev& dv, const MapSet& s, DevSet& d) {
+  if (!s.dat || !s.sim || !s.gmap || !s.vmap || s.glen1 < 1 || s.glen2 < 1 || 2 * s.glen1 > INT_MAX ||
+      4 * s.glen2 > INT_MAX)
+    return TRT_ERR_ARG;
+  for (long long j = 0; j < 4 * s.glen2; ++j)
+    if (s.vmap[j] < 1 || s.vmap[j] > s.glen1 || s.gmap[j] < 1 || s.gmap[j] > 2 * s.glen1 - 1) return TRT_ERR_ARG;
+  int rc;
+  if ((rc = dv.get(&d.dat, 2 * (size_t)s.glen1)) || (rc = dv.get(&d.sim, 2 * (size_t)s.glen2)) ||
+      (rc = dv.get(&d.gmap, 4 * (size_t)s.glen2)) || (rc = dv.get(&d.vmap, 4 * (size_t)s.glen2)))
+    return rc;
+  ROM_CUDA(cudaMemcpy(d.dat, s.dat, 2 * (size_t)s.glen1 * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(d.sim, s.sim, 2 * (size_t)s.glen2 * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(d.gmap, s.gmap, 4 * (size_t)s.glen2 * sizeof(int), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(d.vmap, s.vmap, 4 * (size_t)s.glen2 * sizeof(int), cudaMemcpyHostToDevice));
+  d.glen1 = (int)s.glen1;
+  d.glen2 = (int)s.glen2;
+  return TRT_OK;
+}
+
+// FMAP of n_g blocks of the padded device field f2 (glen1 values each) into the host array out (n_g glen2).
+int map_out(Dev& dv, const DevSet& d, const double* f2, int n_g, double* out) {
+  if (!out) return TRT_ERR_ARG;
+  const long long n = (long long)n_g * d.glen2;
+  double* o;
+  int rc = dv.get(&o, (size_t)n);
+  if (rc) return rc;
+  fmap_kernel<<<grid_of(n), 256>>>(f2, o, d.dat, d.sim, d.gmap, d.vmap, d.glen1, d.glen2, n);
+  trt_host::add_launches(1);
+  ROM_CUDA(cudaGetLastError());
+  ROM_CUDA(cudaMemcpy(out, o, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+  return TRT_OK;
+}
+
+int pad(Dev& dv, int kind, const double* f, const double* side, int n_g, int ny, int nx, double** out) {
+  const long long n = (long long)n_g * (kind == PAD_LR ? ny : ny + 2) * (kind == PAD_BT ? nx : nx + 2);
+  int rc = dv.get(out, (size_t)n);
+  if (rc) return rc;
+  pad_kernel<<<grid_of(n), 256>>>(kind, f, side, n_g, ny, nx, *out);
+  trt_host::add_launches(1);
+  ROM_CUDA(cudaGetLastError());
+  return TRT_OK;
+}
+
+bool grid_dims_ok(int dN_x, int dN_y, int dN_g, int N_x, int N_y, int N_g) {
+  // the drivers map group g of the data to group g of the simulation
+  return dN_x >= 1 && dN_y >= 1 && dN_g >= 1 && N_x >= 1 && N_y >= 1 && N_g == dN_g &&
+         (long long)(dN_x + 2) * (dN_y + 2) * dN_g <= INT_MAX && (long long)(N_x + 1) * (N_y + 1) * N_g <= INT_MAX;
+}
+
+// The data levels bracketing simulation level t (TMap(2t-1), TMap(2t)) and the times of the interpolation.
+int time_levels(const int* TMap, const double* Sim_TGrid, const double* Dat_TGrid, int dN_t, int N_t, int t, int& a,
+                int& b, double& xm, double& x1, double& x2) {
+  if (!TMap || !Sim_TGrid || !Dat_TGrid || dN_t < 1 || t < 1 || t > N_t) return TRT_ERR_ARG;
+  a = TMap[2 * t - 2];
+  b = TMap[2 * t - 1];
+  if (a < 1 || a > dN_t || b < 1 || b > dN_t) return TRT_ERR_ARG;
+  xm = Sim_TGrid[t - 1];
+  x1 = Dat_TGrid[a - 1];
+  x2 = Dat_TGrid[b - 1];
+  if (a != b && !(x2 != x1)) return TRT_ERR_ARG;
+  if (a == b) x1 = x2 = xm = 0.0;
+  return TRT_OK;
+}
+
+// Reconstructs field k on the data grid (len values) into device memory; fields in the order of the
+// decompositions' arguments: 0 avg_xx, 1 edgV_xx, 2 avg_yy, 3 edgH_yy, 4 edgV_xy, 5 edgH_xy.
+template <class Rec>
+int fg_driver(Dev& dv, const Rec& rec, double* const out[6], int dN_x, int dN_y, int dN_g, int N_x, int N_y, int N_g,
+              const double* const sim[3], const double* const dat[3], const int* const gmap[3],
+              const int* const vmap[3]) {
+  const long long la = (long long)dN_x * dN_y * dN_g, lv = (long long)(dN_x + 1) * dN_y * dN_g,
+                  lh = (long long)dN_x * (dN_y + 1) * dN_g;
+  const long long lens[6] = {la, lv, la, lh, lv, lh};
+  double* f[6];
+  int rc;
+  for (int k = 0; k < 6; ++k)
+    if ((rc = dv.get(&f[k], (size_t)lens[k])) || (rc = rec(k, lens[k], f[k]))) return rc;
+  // sets 0 cell averages, 1 vertical edges, 2 horizontal edges
+  const MapSet ms[3] = {{dat[0], sim[0], gmap[0], vmap[0], (long long)(dN_x + 2) * (dN_y + 2), (long long)N_x * N_y},
+                        {dat[1], sim[1], gmap[1], vmap[1], (long long)(dN_x + 1) * (dN_y + 2), (long long)(N_x + 1) * N_y},
+                        {dat[2], sim[2], gmap[2], vmap[2], (long long)(dN_x + 2) * (dN_y + 1), (long long)N_x * (N_y + 1)}};
+  DevSet ds[3];
+  for (int i = 0; i < 3; ++i)
+    if ((rc = upload_set(dv, ms[i], ds[i]))) return rc;
+  double* p;
+  // outputs: 0 avg_xx, 1 avg_yy, 2 edgV_xx, 3 edgV_xy, 4 edgH_yy, 5 edgH_xy
+  if ((rc = pad(dv, PAD_BT, f[1], nullptr, dN_g, dN_y, dN_x + 1, &p)) || (rc = map_out(dv, ds[1], p, N_g, out[2])) ||
+      (rc = pad(dv, PAD_BT, f[4], nullptr, dN_g, dN_y, dN_x + 1, &p)) || (rc = map_out(dv, ds[1], p, N_g, out[3])) ||
+      (rc = pad(dv, PAD_LR, f[3], nullptr, dN_g, dN_y + 1, dN_x, &p)) || (rc = map_out(dv, ds[2], p, N_g, out[4])) ||
+      (rc = pad(dv, PAD_LR, f[5], nullptr, dN_g, dN_y + 1, dN_x, &p)) || (rc = map_out(dv, ds[2], p, N_g, out[5])) ||
+      (rc = pad(dv, PAD_AVG_XX, f[0], f[1], dN_g, dN_y, dN_x, &p)) || (rc = map_out(dv, ds[0], p, N_g, out[0])) ||
+      (rc = pad(dv, PAD_AVG_YY, f[2], f[3], dN_g, dN_y, dN_x, &p)) || (rc = map_out(dv, ds[0], p, N_g, out[1])))
+    return rc;
+  return TRT_OK;
+}
+
+// The four boundary factors from the device vector BC (per group: left dN_y, bottom dN_x, right dN_y, top dN_x
+// values), each padded and mapped with its side's slice of the boundary point sets and maps.
+int bcg_driver(Dev& dv, const double* BC, double* const out[4], int dN_x, int dN_y, int dN_g, int N_x, int N_y,
+               int N_g, const double* Sim_Grid_Bnds, const double* Dat_Grid_Bnds, const int* GMap, const int* VMap) {
+  if (!Sim_Grid_Bnds || !Dat_Grid_Bnds || !GMap || !VMap) return TRT_ERR_ARG;
+  const long long blk = 2LL * (dN_x + dN_y);
+  const int n[4] = {dN_y, dN_x, dN_y, dN_x}, m[4] = {N_y, N_x, N_y, N_x};
+  const long long off[4] = {0, dN_y, (long long)dN_y + dN_x, 2LL * dN_y + dN_x};
+  const long long dat_off[4] = {0, 2LL * dN_y + 4, 2LL * (dN_y + dN_x) + 8, 4LL * dN_y + 2LL * dN_x + 12};
+  const long long sim_off[4] = {0, 2LL * N_y, 2LL * (N_y + N_x), 4LL * N_y + 2LL * N_x};
+  const long long map_off[4] = {0, 4LL * N_y, 4LL * (N_y + N_x), 8LL * N_y + 4LL * N_x};
+  int rc;
+  for (int s = 0; s < 4; ++s) {
+    const MapSet ms = {Dat_Grid_Bnds + dat_off[s], Sim_Grid_Bnds + sim_off[s], GMap + map_off[s], VMap + map_off[s],
+                       n[s] + 2, m[s]};
+    DevSet ds;
+    double* p;
+    if ((rc = upload_set(dv, ms, ds)) || (rc = dv.get(&p, (size_t)dN_g * (n[s] + 2)))) return rc;
+    side_pad_kernel<<<grid_of((long long)dN_g * (n[s] + 2)), 256>>>(BC, dN_g, blk, off[s], n[s], p);
+    trt_host::add_launches(1);
+    ROM_CUDA(cudaGetLastError());
+    if ((rc = map_out(dv, ds, p, N_g, out[s]))) return rc;
+  }
+  return TRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trt_pod_reconstruct_fg(
+    double* fg_avg_xx, double* fg_avg_yy, double* fg_edgV_xx, double* fg_edgV_xy, double* fg_edgH_yy,
+    double* fg_edgH_xy, const double* C_fg_avg_xx, const double* S_fg_avg_xx, const double* U_fg_avg_xx,
+    const double* V_fg_avg_xx, const double* C_fg_edgV_xx, const double* S_fg_edgV_xx, const double* U_fg_edgV_xx,
+    const double* V_fg_edgV_xx, const double* C_fg_avg_yy, const double* S_fg_avg_yy, const double* U_fg_avg_yy,
+    const double* V_fg_avg_yy, const double* C_fg_edgH_yy, const double* S_fg_edgH_yy, const double* U_fg_edgH_yy,
+    const double* V_fg_edgH_yy, const double* C_fg_edgV_xy, const double* S_fg_edgV_xy, const double* U_fg_edgV_xy,
+    const double* V_fg_edgV_xy, const double* C_fg_edgH_xy, const double* S_fg_edgH_xy, const double* U_fg_edgH_xy,
+    const double* V_fg_edgH_xy, const int* rrank_fg_avg_xx, const int* rrank_fg_edgV_xx, const int* rrank_fg_avg_yy,
+    const int* rrank_fg_edgH_yy, const int* rrank_fg_edgV_xy, const int* rrank_fg_edgH_xy, int dN_x, int dN_y,
+    int dN_g, int dN_t, int N_x, int N_y, int N_g, int N_t, int t, int PODgsum, const double* Sim_Grid_Avg,
+    const double* Sim_Grid_EdgV, const double* Sim_Grid_EdgH, const double* Dat_Grid_Avg, const double* Dat_Grid_EdgV,
+    const double* Dat_Grid_EdgH, const double* Sim_TGrid, const double* Dat_TGrid, const int* GMap_xyAvg,
+    const int* GMap_xyEdgV, const int* GMap_xyEdgH, const int* VMap_xyAvg, const int* VMap_xyEdgV,
+    const int* VMap_xyEdgH, const int* TMap) {
+  double* const out[6] = {fg_avg_xx, fg_avg_yy, fg_edgV_xx, fg_edgV_xy, fg_edgH_yy, fg_edgH_xy};
+  const double* const C[6] = {C_fg_avg_xx, C_fg_edgV_xx, C_fg_avg_yy, C_fg_edgH_yy, C_fg_edgV_xy, C_fg_edgH_xy};
+  const double* const S[6] = {S_fg_avg_xx, S_fg_edgV_xx, S_fg_avg_yy, S_fg_edgH_yy, S_fg_edgV_xy, S_fg_edgH_xy};
+  const double* const U[6] = {U_fg_avg_xx, U_fg_edgV_xx, U_fg_avg_yy, U_fg_edgH_yy, U_fg_edgV_xy, U_fg_edgH_xy};
+  const double* const V[6] = {V_fg_avg_xx, V_fg_edgV_xx, V_fg_avg_yy, V_fg_edgH_yy, V_fg_edgV_xy, V_fg_edgH_xy};
+  const int* const rr[6] = {rrank_fg_avg_xx, rrank_fg_edgV_xx, rrank_fg_avg_yy,
+                            rrank_fg_edgH_yy, rrank_fg_edgV_xy, rrank_fg_edgH_xy};
+  for (int k = 0; k < 6; ++k)
+    if (!out[k] || !C[k] || !S[k] || !U[k] || !V[k] || !rr[k]) return TRT_ERR_ARG;
+  if (!grid_dims_ok(dN_x, dN_y, dN_g, N_x, N_y, N_g) || dN_t < 1 || (PODgsum != 0 && PODgsum != 1)) return TRT_ERR_ARG;
+  int a, b;
+  double xm, x1, x2;
+  int rc = time_levels(TMap, Sim_TGrid, Dat_TGrid, dN_t, N_t, t, a, b, xm, x1, x2);
+  if (rc) return rc;
+  if ((rc = device_present())) return rc;
+  const double* const sim[3] = {Sim_Grid_Avg, Sim_Grid_EdgV, Sim_Grid_EdgH};
+  const double* const dat[3] = {Dat_Grid_Avg, Dat_Grid_EdgV, Dat_Grid_EdgH};
+  const int* const gm[3] = {GMap_xyAvg, GMap_xyEdgV, GMap_xyEdgH};
+  const int* const vm[3] = {VMap_xyAvg, VMap_xyEdgV, VMap_xyEdgH};
+  Dev dv;
+  auto rec = [&](int k, long long len, double* dst) {
+    return pod_field(dv, dst, C[k], S[k], U[k], V[k], rr[k], len, dN_g, dN_t, PODgsum, a, b, xm, x1, x2);
+  };
+  return fg_driver(dv, rec, out, dN_x, dN_y, dN_g, N_x, N_y, N_g, sim, dat, gm, vm);
+}
+
+int trt_pod_reconstruct_bcg(double* Cg_L, double* Cg_B, double* Cg_R, double* Cg_T, const double* C_BCg,
+                            const double* S_BCg, const double* U_BCg, const double* V_BCg, const int* rrank_BCg,
+                            int dN_x, int dN_y, int dN_g, int dN_t, int N_x, int N_y, int N_g, int N_t, int t,
+                            int PODgsum, const double* Sim_Grid_Bnds, const double* Dat_Grid_Bnds,
+                            const double* Sim_TGrid, const double* Dat_TGrid, const int* GMap_xyBnds,
+                            const int* VMap_xyBnds, const int* TMap) {
+  double* const out[4] = {Cg_L, Cg_B, Cg_R, Cg_T};
+  for (double* o : out)
+    if (!o) return TRT_ERR_ARG;
+  if (!C_BCg || !S_BCg || !U_BCg || !V_BCg || !rrank_BCg || !grid_dims_ok(dN_x, dN_y, dN_g, N_x, N_y, N_g) ||
+      dN_t < 1 || (PODgsum != 0 && PODgsum != 1))
+    return TRT_ERR_ARG;
+  int a, b;
+  double xm, x1, x2;
+  int rc = time_levels(TMap, Sim_TGrid, Dat_TGrid, dN_t, N_t, t, a, b, xm, x1, x2);
+  if (rc) return rc;
+  if ((rc = device_present())) return rc;
+  Dev dv;
+  const long long len = 2LL * dN_g * (dN_x + dN_y);
+  double* BC;
+  if ((rc = dv.get(&BC, (size_t)len)) ||
+      (rc = pod_field(dv, BC, C_BCg, S_BCg, U_BCg, V_BCg, rrank_BCg, len, dN_g, dN_t, PODgsum, a, b, xm, x1, x2)))
+    return rc;
+  return bcg_driver(dv, BC, out, dN_x, dN_y, dN_g, N_x, N_y, N_g, Sim_Grid_Bnds, Dat_Grid_Bnds, GMap_xyBnds,
+                    VMap_xyBnds);
+}
+
+int trt_dmd_reconstruct_fg(
+    double* fg_avg_xx, double* fg_avg_yy, double* fg_edgV_xx, double* fg_edgV_xy, double* fg_edgH_yy,
+    double* fg_edgH_xy, const double* L_fg_avg_xx, const double* B_fg_avg_xx, const double* W_fg_avg_xx,
+    const double* C_fg_avg_xx, const double* L_fg_edgV_xx, const double* B_fg_edgV_xx, const double* W_fg_edgV_xx,
+    const double* C_fg_edgV_xx, const double* L_fg_avg_yy, const double* B_fg_avg_yy, const double* W_fg_avg_yy,
+    const double* C_fg_avg_yy, const double* L_fg_edgH_yy, const double* B_fg_edgH_yy, const double* W_fg_edgH_yy,
+    const double* C_fg_edgH_yy, const double* L_fg_edgV_xy, const double* B_fg_edgV_xy, const double* W_fg_edgV_xy,
+    const double* C_fg_edgV_xy, const double* L_fg_edgH_xy, const double* B_fg_edgH_xy, const double* W_fg_edgH_xy,
+    const double* C_fg_edgH_xy, const int* rrank_fg_avg_xx, const int* rrank_fg_edgV_xx, const int* rrank_fg_avg_yy,
+    const int* rrank_fg_edgH_yy, const int* rrank_fg_edgV_xy, const int* rrank_fg_edgH_xy, int dN_x, int dN_y,
+    int dN_g, int N_x, int N_y, int N_g, double Time, int DMDgsum, const double* Sim_Grid_Avg,
+    const double* Sim_Grid_EdgV, const double* Sim_Grid_EdgH, const double* Dat_Grid_Avg, const double* Dat_Grid_EdgV,
+    const double* Dat_Grid_EdgH, const int* GMap_xyAvg, const int* GMap_xyEdgV, const int* GMap_xyEdgH,
+    const int* VMap_xyAvg, const int* VMap_xyEdgV, const int* VMap_xyEdgH) {
+  double* const out[6] = {fg_avg_xx, fg_avg_yy, fg_edgV_xx, fg_edgV_xy, fg_edgH_yy, fg_edgH_xy};
+  const double* const L[6] = {L_fg_avg_xx, L_fg_edgV_xx, L_fg_avg_yy, L_fg_edgH_yy, L_fg_edgV_xy, L_fg_edgH_xy};
+  const double* const B[6] = {B_fg_avg_xx, B_fg_edgV_xx, B_fg_avg_yy, B_fg_edgH_yy, B_fg_edgV_xy, B_fg_edgH_xy};
+  const double* const W[6] = {W_fg_avg_xx, W_fg_edgV_xx, W_fg_avg_yy, W_fg_edgH_yy, W_fg_edgV_xy, W_fg_edgH_xy};
+  const double* const C[6] = {C_fg_avg_xx, C_fg_edgV_xx, C_fg_avg_yy, C_fg_edgH_yy, C_fg_edgV_xy, C_fg_edgH_xy};
+  const int* const rr[6] = {rrank_fg_avg_xx, rrank_fg_edgV_xx, rrank_fg_avg_yy,
+                            rrank_fg_edgH_yy, rrank_fg_edgV_xy, rrank_fg_edgH_xy};
+  for (int k = 0; k < 6; ++k)
+    if (!out[k] || !L[k] || !B[k] || !W[k] || !C[k] || !rr[k]) return TRT_ERR_ARG;
+  if (!grid_dims_ok(dN_x, dN_y, dN_g, N_x, N_y, N_g) || (DMDgsum != 0 && DMDgsum != 1)) return TRT_ERR_ARG;
+  int rc = device_present();
+  if (rc) return rc;
+  const double* const sim[3] = {Sim_Grid_Avg, Sim_Grid_EdgV, Sim_Grid_EdgH};
+  const double* const dat[3] = {Dat_Grid_Avg, Dat_Grid_EdgV, Dat_Grid_EdgH};
+  const int* const gm[3] = {GMap_xyAvg, GMap_xyEdgV, GMap_xyEdgH};
+  const int* const vm[3] = {VMap_xyAvg, VMap_xyEdgV, VMap_xyEdgH};
+  Dev dv;
+  auto rec = [&](int k, long long len, double* dst) {
+    return dmd_field(dv, dst, L[k], B[k], W[k], C[k], rr[k], len, N_g, DMDgsum, Time);
+  };
+  return fg_driver(dv, rec, out, dN_x, dN_y, dN_g, N_x, N_y, N_g, sim, dat, gm, vm);
+}
+
+int trt_dmd_reconstruct_bcg(double* Cg_L, double* Cg_B, double* Cg_R, double* Cg_T, const double* L_BCg,
+                            const double* B_BCg, const double* W_BCg, const double* C_BCg, const int* rrank_BCg,
+                            int dN_x, int dN_y, int dN_g, int N_x, int N_y, int N_g, double Time, int DMDgsum,
+                            const double* Sim_Grid_Bnds, const double* Dat_Grid_Bnds, const int* GMap_xyBnds,
+                            const int* VMap_xyBnds) {
+  double* const out[4] = {Cg_L, Cg_B, Cg_R, Cg_T};
+  for (double* o : out)
+    if (!o) return TRT_ERR_ARG;
+  if (!L_BCg || !B_BCg || !W_BCg || !C_BCg || !rrank_BCg || !grid_dims_ok(dN_x, dN_y, dN_g, N_x, N_y, N_g) ||
+      (DMDgsum != 0 && DMDgsum != 1))
+    return TRT_ERR_ARG;
+  int rc = device_present();
+  if (rc) return rc;
+  Dev dv;
+  const long long len = 2LL * dN_g * (dN_x + dN_y);
+  double* BC;
+  if ((rc = dv.get(&BC, (size_t)len)) ||
+      (rc = dmd_field(dv, BC, L_BCg, B_BCg, W_BCg, C_BCg, rrank_BCg, len, N_g, DMDgsum, Time)))
+    return rc;
+  return bcg_driver(dv, BC, out, dN_x, dN_y, dN_g, N_x, N_y, N_g, Sim_Grid_Bnds, Dat_Grid_Bnds, GMap_xyBnds,
+                    VMap_xyBnds);
 }
 
 }  // extern "C"

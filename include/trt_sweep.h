@@ -522,6 +522,56 @@ int trt_generate_grids_xy(const double* Delx_d, const double* Dely_d, const doub
                           double* Dat_Grid_Avg, double* Dat_Grid_EdgV, double* Dat_Grid_EdgH, double* Dat_Grid_Bnds,
                           int* GMap_xyAvg, int* GMap_xyEdgV, int* GMap_xyEdgH, int* GMap_xyBnds, int* VMap_xyAvg,
                           int* VMap_xyEdgV, int* VMap_xyEdgH, int* VMap_xyBnds);
+/* Replace SUBROUTINEs POD_RECONSTRUCT_fg and POD_RECONSTRUCT_BCg, MainSrc/POD_ROUTINES.f08:28-353, and
+ * DMD_RECONSTRUCT_fg and DMD_RECONSTRUCT_BCg, MainSrc/DMD_ROUTINES.f08:131-424 (arguments in the reference's order,
+ * without Open_Threads; COMPLEX*16 arrays as interleaved (re, im) doubles).  Each field is reconstructed on the data
+ * grid (POD: at data level TMap(2t-1), and when TMap(2t) differs also there with LINEAR_INTERPOLATION between them;
+ * DMD: at Time), padded as the reference pads it for the mapping (EXTND_BT_BND for the vertical-edge factors,
+ * EXTND_LR_BND for the horizontal-edge ones, AVG_APND_BND for the cell averages with the left/right values of
+ * fg_edgV_xx and the bottom/top values of fg_edgH_yy, each boundary factor side with its end values repeated) and
+ * mapped to the simulation grid by FMAP with the point sets and maps of trt_generate_grids_xy and the time map of
+ * trt_generate_grids_t.  Host arrays in and out; the work runs on the device.  N_g must equal dN_g; the maps are
+ * checked on the host before any launch. */
+int trt_pod_reconstruct_fg(
+    double* fg_avg_xx, double* fg_avg_yy, double* fg_edgV_xx, double* fg_edgV_xy, double* fg_edgH_yy,
+    double* fg_edgH_xy, const double* C_fg_avg_xx, const double* S_fg_avg_xx, const double* U_fg_avg_xx,
+    const double* V_fg_avg_xx, const double* C_fg_edgV_xx, const double* S_fg_edgV_xx, const double* U_fg_edgV_xx,
+    const double* V_fg_edgV_xx, const double* C_fg_avg_yy, const double* S_fg_avg_yy, const double* U_fg_avg_yy,
+    const double* V_fg_avg_yy, const double* C_fg_edgH_yy, const double* S_fg_edgH_yy, const double* U_fg_edgH_yy,
+    const double* V_fg_edgH_yy, const double* C_fg_edgV_xy, const double* S_fg_edgV_xy, const double* U_fg_edgV_xy,
+    const double* V_fg_edgV_xy, const double* C_fg_edgH_xy, const double* S_fg_edgH_xy, const double* U_fg_edgH_xy,
+    const double* V_fg_edgH_xy, const int* rrank_fg_avg_xx, const int* rrank_fg_edgV_xx, const int* rrank_fg_avg_yy,
+    const int* rrank_fg_edgH_yy, const int* rrank_fg_edgV_xy, const int* rrank_fg_edgH_xy, int dN_x, int dN_y,
+    int dN_g, int dN_t, int N_x, int N_y, int N_g, int N_t, int t, int PODgsum, const double* Sim_Grid_Avg,
+    const double* Sim_Grid_EdgV, const double* Sim_Grid_EdgH, const double* Dat_Grid_Avg, const double* Dat_Grid_EdgV,
+    const double* Dat_Grid_EdgH, const double* Sim_TGrid, const double* Dat_TGrid, const int* GMap_xyAvg,
+    const int* GMap_xyEdgV, const int* GMap_xyEdgH, const int* VMap_xyAvg, const int* VMap_xyEdgV,
+    const int* VMap_xyEdgH, const int* TMap);
+int trt_pod_reconstruct_bcg(double* Cg_L, double* Cg_B, double* Cg_R, double* Cg_T, const double* C_BCg,
+                            const double* S_BCg, const double* U_BCg, const double* V_BCg, const int* rrank_BCg,
+                            int dN_x, int dN_y, int dN_g, int dN_t, int N_x, int N_y, int N_g, int N_t, int t,
+                            int PODgsum, const double* Sim_Grid_Bnds, const double* Dat_Grid_Bnds,
+                            const double* Sim_TGrid, const double* Dat_TGrid, const int* GMap_xyBnds,
+                            const int* VMap_xyBnds, const int* TMap);
+int trt_dmd_reconstruct_fg(
+    double* fg_avg_xx, double* fg_avg_yy, double* fg_edgV_xx, double* fg_edgV_xy, double* fg_edgH_yy,
+    double* fg_edgH_xy, const double* L_fg_avg_xx, const double* B_fg_avg_xx, const double* W_fg_avg_xx,
+    const double* C_fg_avg_xx, const double* L_fg_edgV_xx, const double* B_fg_edgV_xx, const double* W_fg_edgV_xx,
+    const double* C_fg_edgV_xx, const double* L_fg_avg_yy, const double* B_fg_avg_yy, const double* W_fg_avg_yy,
+    const double* C_fg_avg_yy, const double* L_fg_edgH_yy, const double* B_fg_edgH_yy, const double* W_fg_edgH_yy,
+    const double* C_fg_edgH_yy, const double* L_fg_edgV_xy, const double* B_fg_edgV_xy, const double* W_fg_edgV_xy,
+    const double* C_fg_edgV_xy, const double* L_fg_edgH_xy, const double* B_fg_edgH_xy, const double* W_fg_edgH_xy,
+    const double* C_fg_edgH_xy, const int* rrank_fg_avg_xx, const int* rrank_fg_edgV_xx, const int* rrank_fg_avg_yy,
+    const int* rrank_fg_edgH_yy, const int* rrank_fg_edgV_xy, const int* rrank_fg_edgH_xy, int dN_x, int dN_y,
+    int dN_g, int N_x, int N_y, int N_g, double Time, int DMDgsum, const double* Sim_Grid_Avg,
+    const double* Sim_Grid_EdgV, const double* Sim_Grid_EdgH, const double* Dat_Grid_Avg, const double* Dat_Grid_EdgV,
+    const double* Dat_Grid_EdgH, const int* GMap_xyAvg, const int* GMap_xyEdgV, const int* GMap_xyEdgH,
+    const int* VMap_xyAvg, const int* VMap_xyEdgV, const int* VMap_xyEdgH);
+int trt_dmd_reconstruct_bcg(double* Cg_L, double* Cg_B, double* Cg_R, double* Cg_T, const double* L_BCg,
+                            const double* B_BCg, const double* W_BCg, const double* C_BCg, const int* rrank_BCg,
+                            int dN_x, int dN_y, int dN_g, int N_x, int N_y, int N_g, double Time, int DMDgsum,
+                            const double* Sim_Grid_Bnds, const double* Dat_Grid_Bnds, const int* GMap_xyBnds,
+                            const int* VMap_xyBnds);
 /* Replaces SUBROUTINE GENERATE_GRIDS_T, MainSrc/GRID_FUNCTIONS.f08:754-814: the data and simulation time levels and
  * TMap(2, N_t), for every simulation level the two data levels (1-based) that bracket it (equal when it coincides
  * with one within 1e-14 relative, or lies outside the data range).  Host code. */

@@ -923,3 +923,113 @@ def avg_apnd_bnd(f, LR, BT, Crn, N_g, N_y, N_x):
     out[:, 1:-1, 0], out[:, 1:-1, -1] = lr[:, :, 0], lr[:, :, 1]
     out[:, 1:-1, 1:-1] = b
     return out.reshape(-1)
+
+
+# ------------------------------------------------------------------------------------------------------------
+# Online reconstruction drivers: POD_RECONSTRUCT_fg / _BCg (MainSrc/POD_ROUTINES.f08:28-353) and
+# DMD_RECONSTRUCT_fg / _BCg (MainSrc/DMD_ROUTINES.f08:131-424), their calls in order.  dec maps a field name
+# (avg_xx, edgV_xx, avg_yy, edgH_yy, edgV_xy, edgH_xy, BCg) to its decomposition; grids is the dict of
+# generate_grids_xy; tgrids = (Sim_TGrid, Dat_TGrid, TMap) of generate_grids_t.
+# ------------------------------------------------------------------------------------------------------------
+FG_FIELDS = ("avg_xx", "edgV_xx", "avg_yy", "edgH_yy", "edgV_xy", "edgH_xy")
+
+
+def _pod_at_step(d, length, dN_g, dN_t, t, PODgsum, tgrids):
+    """POD_RECONSTRUCT at data level TMap(2t) when TMap(2t-1) equals it, else at both levels with
+    LINEAR_INTERPOLATION between them (the drivers' time handling)."""
+    C, S, U, V, rank = d
+    sim_t, dat_t, tmap = tgrids
+    a, b = int(tmap[2 * t - 2]), int(tmap[2 * t - 1])
+    if a == b:
+        return pod_reconstruct(C, S, U, V, rank, length, dN_g, dN_t, b, PODgsum)
+    f = pod_reconstruct(C, S, U, V, rank, length, dN_g, dN_t, a, PODgsum)
+    f3 = pod_reconstruct(C, S, U, V, rank, length, dN_g, dN_t, b, PODgsum)
+    return linear_interpolation(f, f3, sim_t[t - 1], dat_t[a - 1], dat_t[b - 1])
+
+
+def _fg_map(rec, dN_x, dN_y, dN_g, N_x, N_y, N_g, grids):
+    out = {}
+    G = grids
+    nv1, nv2 = (dN_x + 1) * (dN_y + 2), (N_x + 1) * N_y
+    f = rec("edgV_xx", (dN_x + 1) * dN_y * dN_g)
+    xxbnd = collect_lr_bnd(f, dN_g, dN_y, dN_x + 1)
+    f2 = extnd_bt_bnd(f, dN_g, dN_y, dN_x + 1)
+    out["fg_edgV_xx"] = fmap(f2, G["Dat_Grid_EdgV"], G["Sim_Grid_EdgV"], G["GMap_xyEdgV"], G["VMap_xyEdgV"], nv1, nv2,
+                             nv2 * N_g)
+    f = rec("edgV_xy", (dN_x + 1) * dN_y * dN_g)
+    f2 = extnd_bt_bnd(f, dN_g, dN_y, dN_x + 1)
+    out["fg_edgV_xy"] = fmap(f2, G["Dat_Grid_EdgV"], G["Sim_Grid_EdgV"], G["GMap_xyEdgV"], G["VMap_xyEdgV"], nv1, nv2,
+                             nv2 * N_g)
+    nh1, nh2 = (dN_x + 2) * (dN_y + 1), N_x * (N_y + 1)
+    f = rec("edgH_yy", dN_x * (dN_y + 1) * dN_g)
+    yybnd = collect_bt_bnd(f, dN_g, dN_y + 1, dN_x)
+    f2 = extnd_lr_bnd(f, dN_g, dN_y + 1, dN_x)
+    out["fg_edgH_yy"] = fmap(f2, G["Dat_Grid_EdgH"], G["Sim_Grid_EdgH"], G["GMap_xyEdgH"], G["VMap_xyEdgH"], nh1, nh2,
+                             nh2 * N_g)
+    f = rec("edgH_xy", dN_x * (dN_y + 1) * dN_g)
+    f2 = extnd_lr_bnd(f, dN_g, dN_y + 1, dN_x)
+    out["fg_edgH_xy"] = fmap(f2, G["Dat_Grid_EdgH"], G["Sim_Grid_EdgH"], G["GMap_xyEdgH"], G["VMap_xyEdgH"], nh1, nh2,
+                             nh2 * N_g)
+    na1, na2 = (dN_x + 2) * (dN_y + 2), N_x * N_y
+    f = rec("avg_xx", dN_x * dN_y * dN_g)
+    f2 = avg_apnd_bnd(f, xxbnd, collect_bt_bnd(f, dN_g, dN_y, dN_x), collect_crn_bnd(f, dN_g, dN_y, dN_x), dN_g, dN_y,
+                      dN_x)
+    out["fg_avg_xx"] = fmap(f2, G["Dat_Grid_Avg"], G["Sim_Grid_Avg"], G["GMap_xyAvg"], G["VMap_xyAvg"], na1, na2,
+                            na2 * N_g)
+    f = rec("avg_yy", dN_x * dN_y * dN_g)
+    f2 = avg_apnd_bnd(f, collect_lr_bnd(f, dN_g, dN_y, dN_x), yybnd, collect_crn_bnd(f, dN_g, dN_y, dN_x), dN_g, dN_y,
+                      dN_x)
+    out["fg_avg_yy"] = fmap(f2, G["Dat_Grid_Avg"], G["Sim_Grid_Avg"], G["GMap_xyAvg"], G["VMap_xyAvg"], na1, na2,
+                            na2 * N_g)
+    return out
+
+
+def _bcg_map(BC, dN_x, dN_y, dN_g, N_x, N_y, N_g, grids):
+    """The BCg drivers' side vectors CL2, CB2, CR2, CT2 (each side with its end values repeated) and their FMAPs."""
+    sides = ([], [], [], [])
+    p = 0
+    for _ in range(dN_g):
+        for s, n in enumerate((dN_y, dN_x, dN_y, dN_x)):
+            sides[s].append(BC[p])
+            for _i in range(n):
+                p += 1
+                sides[s].append(BC[p - 1])
+            sides[s].append(BC[p - 1])
+    G = grids
+    out = []
+    for s, (do, so, mo, n1, n2) in enumerate(((0, 0, 0, dN_y + 2, N_y),
+                                              (2 * dN_y + 4, 2 * N_y, 4 * N_y, dN_x + 2, N_x),
+                                              (2 * (dN_y + dN_x) + 8, 2 * (N_y + N_x), 4 * (N_y + N_x), dN_y + 2, N_y),
+                                              (4 * dN_y + 2 * dN_x + 12, 4 * N_y + 2 * N_x, 8 * N_y + 4 * N_x, dN_x + 2,
+                                               N_x))):
+        out.append(fmap(np.array(sides[s]), G["Dat_Grid_Bnds"][do:], G["Sim_Grid_Bnds"][so:], G["GMap_xyBnds"][mo:],
+                        G["VMap_xyBnds"][mo:], n1, n2, N_g * n2))
+    return tuple(out)
+
+
+def pod_reconstruct_fg(dec, dN, N, t, PODgsum, grids, tgrids):
+    """POD_RECONSTRUCT_fg: dN = (dN_x, dN_y, dN_g, dN_t), N = (N_x, N_y, N_g); dec[name] = (C, S, U, V, rank)."""
+    dN_x, dN_y, dN_g, dN_t = dN
+    rec = lambda name, length: _pod_at_step(dec[name], length, dN_g, dN_t, t, PODgsum, tgrids)
+    return _fg_map(rec, dN_x, dN_y, dN_g, *N, grids)
+
+
+def pod_reconstruct_bcg(dec, dN, N, t, PODgsum, grids, tgrids):
+    """POD_RECONSTRUCT_BCg: (Cg_L, Cg_B, Cg_R, Cg_T); dec = (C, S, U, V, rank) of the boundary factors."""
+    dN_x, dN_y, dN_g, dN_t = dN
+    BC = _pod_at_step(dec, dN_g * 2 * (dN_x + dN_y), dN_g, dN_t, t, PODgsum, tgrids)
+    return _bcg_map(BC, dN_x, dN_y, dN_g, *N, grids)
+
+
+def dmd_reconstruct_fg(dec, dN, N, Time, DMDgsum, grids):
+    """DMD_RECONSTRUCT_fg: dN = (dN_x, dN_y, dN_g), N = (N_x, N_y, N_g); dec[name] = (L, B, W, C, rank)."""
+    dN_x, dN_y, dN_g = dN
+    rec = lambda name, length: dmd_reconstruct(*dec[name], length, N[2], DMDgsum, Time)
+    return _fg_map(rec, dN_x, dN_y, dN_g, *N, grids)
+
+
+def dmd_reconstruct_bcg(dec, dN, N, Time, DMDgsum, grids):
+    """DMD_RECONSTRUCT_BCg: (Cg_L, Cg_B, Cg_R, Cg_T); dec = (L, B, W, C, rank) of the boundary factors."""
+    dN_x, dN_y, dN_g = dN
+    BC = dmd_reconstruct(*dec, dN_g * 2 * (dN_x + dN_y), N[2], DMDgsum, Time)
+    return _bcg_map(BC, dN_x, dN_y, dN_g, *N, grids)

@@ -468,3 +468,112 @@ def test_generate_grids_xy_rectangular_grids(oracle):
     _map_linear_field(oracle, got, lambda g: -0.5 + 1.1 * g[0::2] + 0.3 * g[1::2], 7, 4, 5, 8)
     with pytest.raises(pkg.TrtError):
         pkg.GENERATE_GRIDS_XY(dxd, dyd, dx[:0], dy, L, L, L, L)
+
+
+# ------------------------------------------------------------------------------------------------------------
+# Reconstruction drivers POD_RECONSTRUCT_fg / _BCg, DMD_RECONSTRUCT_fg / _BCg
+# ------------------------------------------------------------------------------------------------------------
+def _widths(rng, n, length=1.0):
+    d = rng.uniform(0.6, 1.4, n)
+    return d * (length / d.sum())
+
+
+def _driver_setup(oracle, dN, N, dN_g, seed):
+    """Grids of trt_generate_grids_xy for a dN x dN data grid and an N x N simulation grid of uneven widths."""
+    rng = np.random.default_rng(seed)
+    dxd, dyd, dx, dy = _widths(rng, dN), _widths(rng, dN), _widths(rng, N), _widths(rng, N)
+    if N == dN:
+        dx, dy = dxd, dyd
+    return pkg.GENERATE_GRIDS_XY(dxd, dyd, dx, dy, 1.0, 1.0, 1.0, 1.0)
+
+
+def _pod_dec(rng, length, n_g, n_t, gsum):
+    nb = n_g if gsum == 0 else 1
+    glen = length // nb
+    rank = rng.integers(1, min(4, n_t, glen) + 1, nb).astype(np.int32)
+    tot = int(rank.sum())
+    return (rng.standard_normal(length), rng.uniform(0.1, 1.0, tot), rng.standard_normal(glen * tot),
+            rng.standard_normal(n_t * tot), rank)
+
+
+def _dmd_dec(rng, length, n_g, gsum):
+    nb = n_g if gsum == 0 else 1
+    rank = rng.integers(1, 4, nb)
+    L, B, W, C = dmd_model(length // nb, nb, rank, int(rng.integers(1 << 30)))
+    return L, B, W, C, rank.astype(np.int32)
+
+
+def _fg_lengths(dN_x, dN_y, dN_g):
+    la, lv, lh = dN_x * dN_y * dN_g, (dN_x + 1) * dN_y * dN_g, dN_x * (dN_y + 1) * dN_g
+    return {"avg_xx": la, "edgV_xx": lv, "avg_yy": la, "edgH_yy": lh, "edgV_xy": lv, "edgH_xy": lh}
+
+
+def test_oracle_reconstruction_drivers_on_the_data_grid(oracle):
+    """With the simulation grid equal to the data grid every mapped point coincides with a data point, so the
+    drivers' padding and FMAP hand back the reconstructions themselves: at a data level, between two levels
+    (linear time interpolation), and for the boundary factors side by side."""
+    dN, dN_g, dN_t = 5, 3, 6
+    g = _driver_setup(oracle, dN, dN, dN_g, 11)
+    rng = np.random.default_rng(12)
+    lens = _fg_lengths(dN, dN, dN_g)
+    dec = {k: _pod_dec(rng, n, dN_g, dN_t, 0) for k, n in lens.items()}
+    tg = oracle.generate_grids_t(2e-3, 1e-3, 0.0, 0.0, dN_t, 2 * dN_t)
+    names = {"fg_avg_xx": "avg_xx", "fg_avg_yy": "avg_yy", "fg_edgV_xx": "edgV_xx", "fg_edgV_xy": "edgV_xy",
+             "fg_edgH_yy": "edgH_yy", "fg_edgH_xy": "edgH_xy"}
+    for t in (4, 5):                                   # level 4 sits on data level 2; level 5 between 2 and 3
+        out = oracle.pod_reconstruct_fg(dec, (dN, dN, dN_g, dN_t), (dN, dN, dN_g), t, 0, g, tg)
+        a, b = tg[2][2 * t - 2], tg[2][2 * t - 1]
+        assert (a == b) == (t == 4)
+        for o, k in names.items():
+            f = oracle.pod_reconstruct(*dec[k][:4], dec[k][4], lens[k], dN_g, dN_t, a, 0)
+            if a != b:
+                f3 = oracle.pod_reconstruct(*dec[k][:4], dec[k][4], lens[k], dN_g, dN_t, b, 0)
+                f = oracle.linear_interpolation(f, f3, tg[0][t - 1], tg[1][a - 1], tg[1][b - 1])
+            assert np.array_equal(out[o], f), o
+    bdec = _pod_dec(rng, dN_g * 4 * dN, dN_g, dN_t, 1)
+    sides = oracle.pod_reconstruct_bcg(bdec, (dN, dN, dN_g, dN_t), (dN, dN, dN_g), 4, 1, g, tg)
+    BC = oracle.pod_reconstruct(*bdec[:4], bdec[4], dN_g * 4 * dN, dN_g, dN_t, 2, 1).reshape(dN_g, 4, dN)
+    for s in range(4):
+        assert np.array_equal(sides[s], BC[:, s, :].reshape(-1))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("gsum,t", [(0, 4), (0, 5), (1, 7)])
+def test_device_pod_reconstruct_drivers_bit_identical(oracle, gsum, t):
+    """trt_pod_reconstruct_fg / _bcg against the oracle's restatement of the drivers, data grid 6 x 6 to a
+    simulation grid 9 x 9 of other widths, 3 groups, bit for bit."""
+    dN, N, dN_g, dN_t = 6, 9, 3, 5
+    g = _driver_setup(oracle, dN, N, dN_g, 21)
+    rng = np.random.default_rng(22 + t)
+    dec = {k: _pod_dec(rng, n, dN_g, dN_t, gsum) for k, n in _fg_lengths(dN, dN, dN_g).items()}
+    tg = oracle.generate_grids_t(2e-3, 1e-3, 0.0, 0.0, dN_t, 2 * dN_t)
+    got = pkg.POD_RECONSTRUCT_fg(dec, (dN, dN, dN_g, dN_t), (N, N, dN_g, 2 * dN_t), t, gsum, g, tg)
+    ref = oracle.pod_reconstruct_fg(dec, (dN, dN, dN_g, dN_t), (N, N, dN_g), t, gsum, g, tg)
+    for k in ref:
+        assert got[k].shape == ref[k].shape and np.array_equal(got[k], ref[k]), k
+    bdec = _pod_dec(rng, dN_g * 4 * dN, dN_g, dN_t, gsum)
+    got = pkg.POD_RECONSTRUCT_BCg(bdec, (dN, dN, dN_g, dN_t), (N, N, dN_g, 2 * dN_t), t, gsum, g, tg)
+    ref = oracle.pod_reconstruct_bcg(bdec, (dN, dN, dN_g, dN_t), (N, N, dN_g), t, gsum, g, tg)
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
+    with pytest.raises(pkg.TrtError):                  # a simulation level beyond the time map
+        pkg.POD_RECONSTRUCT_BCg(bdec, (dN, dN, dN_g, dN_t), (N, N, dN_g, 2 * dN_t), 2 * dN_t + 1, gsum, g, tg)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("gsum", [0, 1])
+def test_device_dmd_reconstruct_drivers_bit_identical(oracle, gsum):
+    """trt_dmd_reconstruct_fg / _bcg against the oracle's restatement of the drivers, bit for bit."""
+    dN, N, dN_g = 5, 8, 2
+    g = _driver_setup(oracle, dN, N, dN_g, 31)
+    rng = np.random.default_rng(32 + gsum)
+    dec = {k: _dmd_dec(rng, n, dN_g, gsum) for k, n in _fg_lengths(dN, dN, dN_g).items()}
+    got = pkg.DMD_RECONSTRUCT_fg(dec, (dN, dN, dN_g), (N, N, dN_g), 0.037, gsum, g)
+    ref = oracle.dmd_reconstruct_fg(dec, (dN, dN, dN_g), (N, N, dN_g), 0.037, gsum, g)
+    for k in ref:
+        assert got[k].shape == ref[k].shape and np.array_equal(got[k], ref[k]), k
+    bdec = _dmd_dec(rng, dN_g * 4 * dN, dN_g, gsum)
+    got = pkg.DMD_RECONSTRUCT_BCg(bdec, (dN, dN, dN_g), (N, N, dN_g), 0.037, gsum, g)
+    ref = oracle.dmd_reconstruct_bcg(bdec, (dN, dN, dN_g), (N, N, dN_g), 0.037, gsum, g)
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
