@@ -405,6 +405,15 @@ def GENERATE_GRIDS_XY(Delx_d, Dely_d, Delx, Dely, xlen_d, ylen_d, xlen, ylen):
     return out
 
 
+def GENERATE_GRIDS_T(Delt_d, Delt, Start_Time_d, Start_Time, dN_t, N_t):
+    """trt_generate_grids_t: (Sim_TGrid, Dat_TGrid, TMap) with TMap's data levels 1-based."""
+    sim, dat, tmap = np.zeros(N_t), np.zeros(dN_t), np.zeros(2 * N_t, dtype=np.int32)
+    check(_lib.lib().trt_generate_grids_t(float(Delt_d), float(Delt), float(Start_Time_d), float(Start_Time),
+                                          int(dN_t), int(N_t), dptr(sim), dptr(dat), iptr(tmap)),
+          "trt_generate_grids_t")
+    return sim, dat, tmap
+
+
 _FG_FIELDS = ("avg_xx", "edgV_xx", "avg_yy", "edgH_yy", "edgV_xy", "edgH_xy")   # the decompositions' order
 _FG_OUT = ("fg_avg_xx", "fg_avg_yy", "fg_edgV_xx", "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy")
 

@@ -577,3 +577,54 @@ def test_device_dmd_reconstruct_drivers_bit_identical(oracle, gsum):
     ref = oracle.dmd_reconstruct_bcg(bdec, (dN, dN, dN_g), (N, N, dN_g), 0.037, gsum, g)
     for a, b in zip(got, ref):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_pod_rom_through_the_reconstruction_drivers():
+    """The reference's POD-ROM run through its own drivers: per-group PODs of the recorded factors (the boundary
+    factors as one vector per group, left, bottom, right, top, as the drivers read them), rebuilt at every step by
+    trt_pod_reconstruct_fg / _bcg on the simulation's own grids and time levels (the maps then name the data
+    points themselves), drive an ho_form = 1 run to the full run's temperatures."""
+    from test_mlqd import device, setup_problem
+    prob, ts, km, bcT, cv = setup_problem(8, 6, 10, "S8", 31)
+    kw = dict(conv_ho=1e-9, maxit_rte=40, conv_lo=1e-10, maxit_mloqd=80)
+    nt, nx, ny, ng = 3, prob.nx, prob.ny, prob.ng
+    snaps, T_full = {k: [] for k in FACTORS}, []
+    with device(prob, ts, km, bcT, cv, **kw) as s:
+        for _ in range(nt):
+            s.mlqd_step()
+            m = s.moments(list(FACTORS))
+            for k in FACTORS:
+                snaps[k].append(m[k])
+            T_full.append(s.mlqd_field("Temp"))
+
+    def pod_of(data):                                   # data (clen, ng, nt) -> (C, S, U, V, rank), groupwise
+        parts = [pkg.POD_Calc(data, nt, ng, data.shape[0], g) for g in range(ng)]
+        return (np.concatenate([p[0] for p in parts]), np.concatenate([p[2] for p in parts]),
+                np.concatenate([p[1].ravel(order="F") for p in parts]),
+                np.concatenate([p[3].ravel(order="F") for p in parts]),
+                np.array([len(p[2]) for p in parts], dtype=np.int32))
+
+    dec = {k[3:]: pod_of(np.stack([a.reshape(-1, ng, order="F") for a in snaps[k]], axis=2)) for k in FACTORS[:6]}
+    bc = np.stack([np.concatenate([snaps[k][t].reshape(-1, ng, order="F") for k in FACTORS[6:]], axis=0)
+                   for t in range(nt)], axis=2)
+    bdec = pod_of(bc)
+    dx, dy = np.asarray(prob.delx, dtype=np.float64), np.asarray(prob.dely, dtype=np.float64)
+    grids = pkg.GENERATE_GRIDS_XY(dx, dy, dx, dy, dx.sum(), dy.sum(), dx.sum(), dy.sum())
+    tgrids = pkg.GENERATE_GRIDS_T(ts.dt, ts.dt, 0.0, 0.0, nt, nt)
+    assert np.array_equal(tgrids[2], np.repeat(np.arange(1, nt + 1), 2))
+    dims = (nx, ny, ng, nt)
+    with device(prob, ts, km, bcT, cv, ho_form=1, **kw) as s:
+        for t in range(1, nt + 1):
+            fg = pkg.POD_RECONSTRUCT_fg(dec, dims, dims, t, 0, grids, tgrids)
+            cg = dict(zip(FACTORS[6:], pkg.POD_RECONSTRUCT_BCg(bdec, dims, dims, t, 0, grids, tgrids)))
+            for k in FACTORS:
+                out = fg[k] if k in fg else cg[k]
+                ref = snaps[k][t - 1].ravel(order="F")
+                assert out.shape == ref.shape
+                assert np.abs(out - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()), k
+                s.mlqd_put(k, out)
+            st = s.mlqd_step()
+            assert st["sweeps"] == 0 and st["mgqd_nonconv"] == 0
+            T = s.mlqd_field("Temp")
+            assert float(np.max(np.abs(T - T_full[t - 1])) / np.max(T_full[t - 1])) < 1e-7
