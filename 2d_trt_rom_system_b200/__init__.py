@@ -7,7 +7,7 @@ package is its Python mirror plus the problem and quadrature generators used by 
 from . import problems, quadrature, ranks, serving  # noqa: F401
 from .api import (COLLAPSE_INTENSITIES, COLLAPSE_MG_EF, DMD_Calc, DMD_RECONSTRUCT, EGP_FV_NEWT, FMAP,  # noqa: F401
                   GENERATE_GRIDS_T, GENERATE_GRIDS_XY, GRIDMAP_GEN, GRIDMAP_GEN_BND, MAP_GRIDS, GQD_In_Calc, GREY_COEFS,
-                  DMD_RECONSTRUCT_BCg, DMD_RECONSTRUCT_fg, POD_RECONSTRUCT_BCg, POD_RECONSTRUCT_fg,
+                  DMD_RECONSTRUCT_BCg, DMD_RECONSTRUCT_fg, POD_RECONSTRUCT_BCg, POD_RECONSTRUCT_fg, POD_TRUNCATE, RRANK_CALC,
                   MGQD_In_Calc, MLOQD_FV, OLD_GREY_COEFS, OLD_MGQD_COEFS, POD_RECONSTRUCT, POD_Calc, RT_BC_UPDATE,
                   LINEAR_INTERPOLATION, TRANSPORT_SCB, Batch,
                   Bg_planck_calc, Cbar_Calc, Cg_Calc, TransportSweep, fg_Calc, kernel_launches, mgqd_last_stats,

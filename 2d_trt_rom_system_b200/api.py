@@ -405,6 +405,31 @@ def GENERATE_GRIDS_XY(Delx_d, Dely_d, Delx, Dely, xlen_d, ylen_d, xlen, ylen):
     return out
 
 
+def RRANK_CALC(sig, eps):
+    """trt_rrank_calc: the reduced rank of the singular values sig for the error level eps."""
+    s = _f64(sig)
+    r = ctypes.c_int(0)
+    check(_lib.lib().trt_rrank_calc(dptr(s), float(eps), int(s.size), ctypes.byref(r)), "trt_rrank_calc")
+    return r.value
+
+
+def POD_TRUNCATE(parts, eps):
+    """Packs per-group decompositions [(center, U (clen x k), sig (k), Vt (k x N_t)), ...] (POD_Calc's outputs)
+    into the drivers' (C, S, U, V, rank) arrays, each group truncated to RRANK_CALC(sig, eps) modes and appended
+    after the earlier groups' as READ_POD_GPART (MainSrc/POD_ROUTINES.f08:700-774) assembles them: U the first
+    columns, V the first rows of Vt."""
+    C, S, U, V, rank = [], [], [], [], []
+    for c, u, sig, vt in parts:
+        r = RRANK_CALC(sig, eps)
+        C.append(np.asarray(c, dtype=np.float64).reshape(-1))
+        S.append(np.asarray(sig[:r], dtype=np.float64))
+        U.append(np.asarray(u)[:, :r].reshape(-1, order="F"))
+        V.append(np.asarray(vt)[:r, :].reshape(-1, order="F"))
+        rank.append(r)
+    return (np.concatenate(C), np.concatenate(S), np.concatenate(U), np.concatenate(V),
+            np.array(rank, dtype=np.int32))
+
+
 def GENERATE_GRIDS_T(Delt_d, Delt, Start_Time_d, Start_Time, dN_t, N_t):
     """trt_generate_grids_t: (Sim_TGrid, Dat_TGrid, TMap) with TMap's data levels 1-based."""
     sim, dat, tmap = np.zeros(N_t), np.zeros(dN_t), np.zeros(2 * N_t, dtype=np.int32)

@@ -1453,3 +1453,24 @@ int trt_dmd_reconstruct_bcg(double* Cg_L, double* Cg_B, double* Cg_R, double* Cg
 }
 
 }  // extern "C"
+
+extern "C" {
+
+int trt_rrank_calc(const double* sig, double eps, int len, int* rank) {
+  if (!sig || !rank || len < 1) return TRT_ERR_ARG;
+  double sum1 = 0.0;
+  for (int i = 0; i < len; ++i) sum1 = sum1 + sig[i] * sig[i];
+  const double eps2 = eps * std::sqrt(sum1);
+  *rank = len;
+  for (int i = 1; i <= len; ++i) {   // the first i whose discarded tail sig(i+1:len) has norm <= eps2
+    double sum2 = 0.0;
+    for (int j = i + 1; j <= len; ++j) sum2 = sum2 + sig[j - 1] * sig[j - 1];
+    if (std::sqrt(sum2) <= eps2) {
+      *rank = i;
+      break;
+    }
+  }
+  return TRT_OK;
+}
+
+}  // extern "C"

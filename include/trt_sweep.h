@@ -572,6 +572,10 @@ int trt_dmd_reconstruct_bcg(double* Cg_L, double* Cg_B, double* Cg_R, double* Cg
                             int dN_x, int dN_y, int dN_g, int N_x, int N_y, int N_g, double Time, int DMDgsum,
                             const double* Sim_Grid_Bnds, const double* Dat_Grid_Bnds, const int* GMap_xyBnds,
                             const int* VMap_xyBnds);
+/* Replaces SUBROUTINE RRANK_CALC, MainSrc/POD_ROUTINES.f08:791-819: the smallest rank whose discarded singular
+ * values sig(rank+1:len) have a norm at most eps times the norm of all of them (len when none qualifies before
+ * the last), the truncation READ_POD_FULL / READ_POD_GPART apply to a stored decomposition.  Host code. */
+int trt_rrank_calc(const double* sig, double eps, int len, int* rank);
 /* Replaces SUBROUTINE GENERATE_GRIDS_T, MainSrc/GRID_FUNCTIONS.f08:754-814: the data and simulation time levels and
  * TMap(2, N_t), for every simulation level the two data levels (1-based) that bracket it (equal when it coincides
  * with one within 1e-14 relative, or lies outside the data range).  Host code. */

@@ -1007,6 +1007,24 @@ def _bcg_map(BC, dN_x, dN_y, dN_g, N_x, N_y, N_g, grids):
     return tuple(out)
 
 
+def rrank_calc(sig, eps):
+    """RRANK_CALC (MainSrc/POD_ROUTINES.f08:791-819): sums of squares in index order, the first i whose tail
+    norm is at most eps times the total norm."""
+    import math
+    n = len(sig)
+    sum1 = 0.0
+    for v in sig:
+        sum1 = sum1 + v * v
+    eps2 = eps * math.sqrt(sum1)
+    for i in range(1, n + 1):
+        sum2 = 0.0
+        for j in range(i + 1, n + 1):
+            sum2 = sum2 + sig[j - 1] * sig[j - 1]
+        if math.sqrt(sum2) <= eps2:
+            return i
+    return n
+
+
 def pod_reconstruct_fg(dec, dN, N, t, PODgsum, grids, tgrids):
     """POD_RECONSTRUCT_fg: dN = (dN_x, dN_y, dN_g, dN_t), N = (N_x, N_y, N_g); dec[name] = (C, S, U, V, rank)."""
     dN_x, dN_y, dN_g, dN_t = dN

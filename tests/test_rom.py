@@ -628,3 +628,32 @@ def test_pod_rom_through_the_reconstruction_drivers():
             assert st["sweeps"] == 0 and st["mgqd_nonconv"] == 0
             T = s.mlqd_field("Temp")
             assert float(np.max(np.abs(T - T_full[t - 1])) / np.max(T_full[t - 1])) < 1e-7
+
+
+def test_rrank_calc_matches_oracle(oracle):
+    """RRANK_CALC (host code of the library) against the restatement: decaying spectra over error levels, the
+    edge levels (0 keeps every mode, 1 keeps one) and trailing zeros; POD_TRUNCATE packs the truncated groups."""
+    rng = np.random.default_rng(41)
+    for n in (1, 2, 7, 20):
+        sig = np.sort(rng.uniform(0.0, 1.0, n) ** 3)[::-1]
+        for eps in (0.0, 1e-12, 1e-3, 0.05, 0.3, 1.0):
+            assert pkg.RRANK_CALC(sig, eps) == oracle.rrank_calc(list(sig), eps), (n, eps)
+        assert pkg.RRANK_CALC(sig, 1.0) == 1
+    assert pkg.RRANK_CALC(np.array([3.0, 2.0, 0.0, 0.0]), 0.0) == 2
+    assert pkg.RRANK_CALC(np.array([1.0, 1e-9, 1e-12]), 0.0) == 3
+    with pytest.raises(pkg.TrtError):
+        pkg.RRANK_CALC(np.zeros(0), 0.1)
+    clen, nt = 9, 5
+    parts = []
+    for _ in range(3):
+        u, sig, vt = rng.standard_normal((clen, nt)), np.array([4.0, 1.0, 0.1, 0.01, 0.001]), rng.standard_normal((nt, nt))
+        parts.append((rng.standard_normal(clen), u, sig, vt))
+    C, S, U, V, rank = pkg.POD_TRUNCATE(parts, 0.02)
+    r = oracle.rrank_calc([4.0, 1.0, 0.1, 0.01, 0.001], 0.02)
+    assert list(rank) == [r] * 3 and S.size == 3 * r and U.size == 3 * clen * r and V.size == 3 * nt * r
+    # the packed arrays reconstruct what the truncated factors give, group by group (POD_RECONSTRUCT's layout)
+    for t in (1, nt):
+        dat = oracle.pod_reconstruct(C, S, U, V, rank, 3 * clen, 3, nt, t, 0)
+        for g, (c, u, sig, vt) in enumerate(parts):
+            ref = c + (u[:, :r] * sig[:r]) @ vt[:r, t - 1]
+            np.testing.assert_allclose(dat[g * clen:(g + 1) * clen], ref, rtol=1e-13, atol=1e-13)
