@@ -161,6 +161,8 @@ SIGNATURES = {
     "trt_generate_grids_t": (_i, [_d, _d, _d, _d, _i, _i, _D, _D, _I]),
     "trt_gridmap_gen_bnd": (_i, [_i, _D, _d, _i, _D]),
     "trt_rrank_calc": (_i, [_D, _d, _i, _I]),
+    "trt_pod_reconstruct_fg_device": (_i, [_P] * 30 + [_I] * 6 + [_i] * 10 + [_P] * 6 + [_D] * 2 + [_P] * 6 + [_I, _P]),
+    "trt_pod_reconstruct_bcg_device": (_i, [_P] * 8 + [_I] + [_i] * 10 + [_P] * 2 + [_D] * 2 + [_P] * 2 + [_I, _P]),
     "trt_pod_reconstruct_fg": (_i, [_D] * 30 + [_I] * 6 + [_i] * 10 + [_D] * 8 + [_I] * 7),
     "trt_pod_reconstruct_bcg": (_i, [_D] * 8 + [_I] + [_i] * 10 + [_D] * 4 + [_I] * 3),
     "trt_dmd_reconstruct_fg": (_i, [_D] * 30 + [_I] * 6 + [_i] * 6 + [_d, _i] + [_D] * 6 + [_I] * 6),

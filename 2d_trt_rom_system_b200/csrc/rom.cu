@@ -290,12 +290,13 @@ int mode_offsets(const int* rank, int nb, long long max_rank, std::vector<long l
   return TRT_OK;
 }
 
-// POD_RECONSTRUCT of one field (len values; N_g blocks with PODgsum = 0, one with PODgsum = 1) from host
-// decomposition arrays into device memory dst at data time level a (1-based); when level b differs, also at b,
-// followed by LINEAR_INTERPOLATION(dst, level b, xm, x1, x2), as the reconstruction drivers do.
+// POD_RECONSTRUCT of one field (len values; N_g blocks with PODgsum = 0, one with PODgsum = 1) into device memory
+// dst at data time level a (1-based); when level b differs, also at b, followed by LINEAR_INTERPOLATION(dst,
+// level b, xm, x1, x2), as the reconstruction drivers do.  C, S, U, V are host arrays (uploaded here), or device
+// arrays when resident; rank is a host array; the launches go to stream st.
 int pod_field(Dev& dv, double* dst, const double* C, const double* S, const double* U, const double* V,
               const int* rank, long long len, int N_g, int N_t, int PODgsum, int a, int b, double xm, double x1,
-              double x2) {
+              double x2, bool resident = false, cudaStream_t st = nullptr) {
   if (!C || !S || !U || !V || !rank || len < 1 || N_t < 1 || a < 1 || a > N_t || b < 1 || b > N_t ||
       (PODgsum != 0 && PODgsum != 1) || (PODgsum == 0 && (N_g < 1 || len % N_g != 0)) || (a != b && !(x2 != x1)))
     return TRT_ERR_ARG;
@@ -305,25 +306,33 @@ int pod_field(Dev& dv, double* dst, const double* C, const double* S, const doub
   long long tot = 0;
   int rc = mode_offsets(rank, nb, std::min<long long>(glen, N_t), off, tot);
   if (rc) return rc;
-  double *dC, *dS, *dU, *dV;
+  const double *dC = C, *dS = S, *dU = U, *dV = V;
   int* dr;
   long long* doff;
-  if ((rc = dv.get(&dC, (size_t)len)) || (rc = dv.get(&dS, (size_t)tot)) || (rc = dv.get(&dU, (size_t)(glen * tot))) ||
-      (rc = dv.get(&dV, (size_t)(N_t * tot))) || (rc = dv.get(&dr, (size_t)nb)) || (rc = dv.get(&doff, (size_t)nb)))
-    return rc;
-  ROM_CUDA(cudaMemcpy(dC, C, (size_t)len * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(dS, S, (size_t)tot * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(dU, U, (size_t)(glen * tot) * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(dV, V, (size_t)(N_t * tot) * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(dr, rank, (size_t)nb * sizeof(int), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(doff, off.data(), (size_t)nb * sizeof(long long), cudaMemcpyHostToDevice));
-  pod_reconstruct_kernel<<<grid_of(len), 256>>>(glen, nb, N_t, a - 1, dr, doff, dC, dS, dU, dV, dst);
+  if ((rc = dv.get(&dr, (size_t)nb)) || (rc = dv.get(&doff, (size_t)nb))) return rc;
+  if (!resident) {
+    double *hC, *hS, *hU, *hV;
+    if ((rc = dv.get(&hC, (size_t)len)) || (rc = dv.get(&hS, (size_t)tot)) ||
+        (rc = dv.get(&hU, (size_t)(glen * tot))) || (rc = dv.get(&hV, (size_t)(N_t * tot))))
+      return rc;
+    ROM_CUDA(cudaMemcpy(hC, C, (size_t)len * sizeof(double), cudaMemcpyHostToDevice));
+    ROM_CUDA(cudaMemcpy(hS, S, (size_t)tot * sizeof(double), cudaMemcpyHostToDevice));
+    ROM_CUDA(cudaMemcpy(hU, U, (size_t)(glen * tot) * sizeof(double), cudaMemcpyHostToDevice));
+    ROM_CUDA(cudaMemcpy(hV, V, (size_t)(N_t * tot) * sizeof(double), cudaMemcpyHostToDevice));
+    dC = hC;
+    dS = hS;
+    dU = hU;
+    dV = hV;
+  }
+  ROM_CUDA(cudaMemcpyAsync(dr, rank, (size_t)nb * sizeof(int), cudaMemcpyHostToDevice, st));
+  ROM_CUDA(cudaMemcpyAsync(doff, off.data(), (size_t)nb * sizeof(long long), cudaMemcpyHostToDevice, st));
+  pod_reconstruct_kernel<<<grid_of(len), 256, 0, st>>>(glen, nb, N_t, a - 1, dr, doff, dC, dS, dU, dV, dst);
   trt_host::add_launches(1);
   if (b != a) {
     double* f3;
     if ((rc = dv.get(&f3, (size_t)len))) return rc;
-    pod_reconstruct_kernel<<<grid_of(len), 256>>>(glen, nb, N_t, b - 1, dr, doff, dC, dS, dU, dV, f3);
-    linear_interpolation_kernel<<<grid_of(len), 256>>>(dst, f3, xm, x1, x2, len);
+    pod_reconstruct_kernel<<<grid_of(len), 256, 0, st>>>(glen, nb, N_t, b - 1, dr, doff, dC, dS, dU, dV, f3);
+    linear_interpolation_kernel<<<grid_of(len), 256, 0, st>>>(dst, f3, xm, x1, x2, len);
     trt_host::add_launches(2);
   }
   ROM_CUDA(cudaGetLastError());
@@ -1191,10 +1200,38 @@ struct MapSet {
 };
 
 struct DevSet {
-  double *dat, *sim;
-  int *gmap, *vmap;
+  const double *dat, *sim;
+  const int *gmap, *vmap;
   int glen1, glen2;
 };
+
+// Flags a map entry outside grid 1 (VMap outside [1, glen1], GMap outside [1, 2 glen1 - 1]).
+__global__ void check_maps_kernel(const int* __restrict__ gmap, const int* __restrict__ vmap, long long n, int glen1,
+                                  int* __restrict__ bad) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    if (vmap[k] < 1 || vmap[k] > glen1 || gmap[k] < 1 || gmap[k] > 2 * glen1 - 1) atomicOr(bad, 1);
+}
+
+// A set whose grids and maps already live on the device: its maps are checked on the device (one pass, the
+// verdict read back) before any FMAP reads through them.
+int device_set(Dev& dv, const MapSet& s, DevSet& d, cudaStream_t st) {
+  if (!s.dat || !s.sim || !s.gmap || !s.vmap || s.glen1 < 1 || s.glen2 < 1 || 2 * s.glen1 > INT_MAX ||
+      4 * s.glen2 > INT_MAX)
+    return TRT_ERR_ARG;
+  int* bad;
+  int rc = dv.get(&bad, 1);
+  if (rc) return rc;
+  ROM_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), st));
+  check_maps_kernel<<<grid_of(4 * s.glen2), 256, 0, st>>>(s.gmap, s.vmap, 4 * s.glen2, (int)s.glen1, bad);
+  trt_host::add_launches(1);
+  ROM_CUDA(cudaGetLastError());
+  int hbad = 0;
+  ROM_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+  ROM_CUDA(cudaStreamSynchronize(st));
+  if (hbad) return TRT_ERR_ARG;
+  d = {s.dat, s.sim, s.gmap, s.vmap, (int)s.glen1, (int)s.glen2};
+  return TRT_OK;
+}
 
 // Checks a set's maps on the host (every VMap entry a value of the block, every GMap entry an x of grid 1), then
 // uploads the grids and maps.
@@ -1205,37 +1242,46 @@ int upload_set(Dev& dv, const MapSet& s, DevSet& d) {
   for (long long j = 0; j < 4 * s.glen2; ++j)
     if (s.vmap[j] < 1 || s.vmap[j] > s.glen1 || s.gmap[j] < 1 || s.gmap[j] > 2 * s.glen1 - 1) return TRT_ERR_ARG;
   int rc;
-  if ((rc = dv.get(&d.dat, 2 * (size_t)s.glen1)) || (rc = dv.get(&d.sim, 2 * (size_t)s.glen2)) ||
-      (rc = dv.get(&d.gmap, 4 * (size_t)s.glen2)) || (rc = dv.get(&d.vmap, 4 * (size_t)s.glen2)))
+  double *dat, *sim;
+  int *gmap, *vmap;
+  if ((rc = dv.get(&dat, 2 * (size_t)s.glen1)) || (rc = dv.get(&sim, 2 * (size_t)s.glen2)) ||
+      (rc = dv.get(&gmap, 4 * (size_t)s.glen2)) || (rc = dv.get(&vmap, 4 * (size_t)s.glen2)))
     return rc;
-  ROM_CUDA(cudaMemcpy(d.dat, s.dat, 2 * (size_t)s.glen1 * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(d.sim, s.sim, 2 * (size_t)s.glen2 * sizeof(double), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(d.gmap, s.gmap, 4 * (size_t)s.glen2 * sizeof(int), cudaMemcpyHostToDevice));
-  ROM_CUDA(cudaMemcpy(d.vmap, s.vmap, 4 * (size_t)s.glen2 * sizeof(int), cudaMemcpyHostToDevice));
-  d.glen1 = (int)s.glen1;
-  d.glen2 = (int)s.glen2;
+  ROM_CUDA(cudaMemcpy(dat, s.dat, 2 * (size_t)s.glen1 * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(sim, s.sim, 2 * (size_t)s.glen2 * sizeof(double), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(gmap, s.gmap, 4 * (size_t)s.glen2 * sizeof(int), cudaMemcpyHostToDevice));
+  ROM_CUDA(cudaMemcpy(vmap, s.vmap, 4 * (size_t)s.glen2 * sizeof(int), cudaMemcpyHostToDevice));
+  d = {dat, sim, gmap, vmap, (int)s.glen1, (int)s.glen2};
   return TRT_OK;
 }
 
-// FMAP of n_g blocks of the padded device field f2 (glen1 values each) into the host array out (n_g glen2).
-int map_out(Dev& dv, const DevSet& d, const double* f2, int n_g, double* out) {
+// Host sets are checked and uploaded; resident ones are checked on the device.
+int make_set(Dev& dv, const MapSet& s, DevSet& d, bool resident, cudaStream_t st) {
+  return resident ? device_set(dv, s, d, st) : upload_set(dv, s, d);
+}
+
+// FMAP of n_g blocks of the padded device field f2 (glen1 values each) into out (n_g glen2 values): a device
+// array when resident, else a host array (through a device buffer).
+int map_out(Dev& dv, const DevSet& d, const double* f2, int n_g, double* out, bool resident = false,
+            cudaStream_t st = nullptr) {
   if (!out) return TRT_ERR_ARG;
   const long long n = (long long)n_g * d.glen2;
-  double* o;
-  int rc = dv.get(&o, (size_t)n);
-  if (rc) return rc;
-  fmap_kernel<<<grid_of(n), 256>>>(f2, o, d.dat, d.sim, d.gmap, d.vmap, d.glen1, d.glen2, n);
+  double* o = out;
+  int rc;
+  if (!resident && (rc = dv.get(&o, (size_t)n))) return rc;
+  fmap_kernel<<<grid_of(n), 256, 0, st>>>(f2, o, d.dat, d.sim, d.gmap, d.vmap, d.glen1, d.glen2, n);
   trt_host::add_launches(1);
   ROM_CUDA(cudaGetLastError());
-  ROM_CUDA(cudaMemcpy(out, o, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (!resident) ROM_CUDA(cudaMemcpy(out, o, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
   return TRT_OK;
 }
 
-int pad(Dev& dv, int kind, const double* f, const double* side, int n_g, int ny, int nx, double** out) {
+int pad(Dev& dv, int kind, const double* f, const double* side, int n_g, int ny, int nx, double** out,
+        cudaStream_t st) {
   const long long n = (long long)n_g * (kind == PAD_LR ? ny : ny + 2) * (kind == PAD_BT ? nx : nx + 2);
   int rc = dv.get(out, (size_t)n);
   if (rc) return rc;
-  pad_kernel<<<grid_of(n), 256>>>(kind, f, side, n_g, ny, nx, *out);
+  pad_kernel<<<grid_of(n), 256, 0, st>>>(kind, f, side, n_g, ny, nx, *out);
   trt_host::add_launches(1);
   ROM_CUDA(cudaGetLastError());
   return TRT_OK;
@@ -1263,45 +1309,51 @@ int time_levels(const int* TMap, const double* Sim_TGrid, const double* Dat_TGri
 }
 
 // Reconstructs field k on the data grid (len values) into device memory; fields in the order of the
-// decompositions' arguments: 0 avg_xx, 1 edgV_xx, 2 avg_yy, 3 edgH_yy, 4 edgV_xy, 5 edgH_xy.
+// decompositions' arguments: 0 avg_xx, 1 edgV_xx, 2 avg_yy, 3 edgH_yy, 4 edgV_xy, 5 edgH_xy.  Outputs: 0 avg_xx,
+// 1 avg_yy, 2 edgV_xx, 3 edgV_xy, 4 edgH_yy, 5 edgH_xy; host arrays, or device arrays (grids and maps too) when
+// resident, with the launches on stream st.
 template <class Rec>
 int fg_driver(Dev& dv, const Rec& rec, double* const out[6], int dN_x, int dN_y, int dN_g, int N_x, int N_y, int N_g,
               const double* const sim[3], const double* const dat[3], const int* const gmap[3],
-              const int* const vmap[3]) {
+              const int* const vmap[3], bool resident = false, cudaStream_t st = nullptr) {
   const long long la = (long long)dN_x * dN_y * dN_g, lv = (long long)(dN_x + 1) * dN_y * dN_g,
                   lh = (long long)dN_x * (dN_y + 1) * dN_g;
   const long long lens[6] = {la, lv, la, lh, lv, lh};
-  double* f[6];
-  int rc;
-  for (int k = 0; k < 6; ++k)
-    if ((rc = dv.get(&f[k], (size_t)lens[k])) || (rc = rec(k, lens[k], f[k]))) return rc;
-  // sets 0 cell averages, 1 vertical edges, 2 horizontal edges
+  // sets 0 cell averages, 1 vertical edges, 2 horizontal edges, checked before any reconstruction
   const MapSet ms[3] = {{dat[0], sim[0], gmap[0], vmap[0], (long long)(dN_x + 2) * (dN_y + 2), (long long)N_x * N_y},
                         {dat[1], sim[1], gmap[1], vmap[1], (long long)(dN_x + 1) * (dN_y + 2), (long long)(N_x + 1) * N_y},
                         {dat[2], sim[2], gmap[2], vmap[2], (long long)(dN_x + 2) * (dN_y + 1), (long long)N_x * (N_y + 1)}};
   DevSet ds[3];
+  int rc;
   for (int i = 0; i < 3; ++i)
-    if ((rc = upload_set(dv, ms[i], ds[i]))) return rc;
+    if ((rc = make_set(dv, ms[i], ds[i], resident, st))) return rc;
+  double* f[6];
+  for (int k = 0; k < 6; ++k)
+    if ((rc = dv.get(&f[k], (size_t)lens[k])) || (rc = rec(k, lens[k], f[k]))) return rc;
   double* p;
-  // outputs: 0 avg_xx, 1 avg_yy, 2 edgV_xx, 3 edgV_xy, 4 edgH_yy, 5 edgH_xy
-  if ((rc = pad(dv, PAD_BT, f[1], nullptr, dN_g, dN_y, dN_x + 1, &p)) || (rc = map_out(dv, ds[1], p, N_g, out[2])) ||
-      (rc = pad(dv, PAD_BT, f[4], nullptr, dN_g, dN_y, dN_x + 1, &p)) || (rc = map_out(dv, ds[1], p, N_g, out[3])) ||
-      (rc = pad(dv, PAD_LR, f[3], nullptr, dN_g, dN_y + 1, dN_x, &p)) || (rc = map_out(dv, ds[2], p, N_g, out[4])) ||
-      (rc = pad(dv, PAD_LR, f[5], nullptr, dN_g, dN_y + 1, dN_x, &p)) || (rc = map_out(dv, ds[2], p, N_g, out[5])) ||
-      (rc = pad(dv, PAD_AVG_XX, f[0], f[1], dN_g, dN_y, dN_x, &p)) || (rc = map_out(dv, ds[0], p, N_g, out[0])) ||
-      (rc = pad(dv, PAD_AVG_YY, f[2], f[3], dN_g, dN_y, dN_x, &p)) || (rc = map_out(dv, ds[0], p, N_g, out[1])))
+  if ((rc = pad(dv, PAD_BT, f[1], nullptr, dN_g, dN_y, dN_x + 1, &p, st)) ||
+      (rc = map_out(dv, ds[1], p, N_g, out[2], resident, st)) ||
+      (rc = pad(dv, PAD_BT, f[4], nullptr, dN_g, dN_y, dN_x + 1, &p, st)) ||
+      (rc = map_out(dv, ds[1], p, N_g, out[3], resident, st)) ||
+      (rc = pad(dv, PAD_LR, f[3], nullptr, dN_g, dN_y + 1, dN_x, &p, st)) ||
+      (rc = map_out(dv, ds[2], p, N_g, out[4], resident, st)) ||
+      (rc = pad(dv, PAD_LR, f[5], nullptr, dN_g, dN_y + 1, dN_x, &p, st)) ||
+      (rc = map_out(dv, ds[2], p, N_g, out[5], resident, st)) ||
+      (rc = pad(dv, PAD_AVG_XX, f[0], f[1], dN_g, dN_y, dN_x, &p, st)) ||
+      (rc = map_out(dv, ds[0], p, N_g, out[0], resident, st)) ||
+      (rc = pad(dv, PAD_AVG_YY, f[2], f[3], dN_g, dN_y, dN_x, &p, st)) ||
+      (rc = map_out(dv, ds[0], p, N_g, out[1], resident, st)))
     return rc;
   return TRT_OK;
 }
 
 // The four boundary factors from the device vector BC (per group: left dN_y, bottom dN_x, right dN_y, top dN_x
-// values), each padded and mapped with its side's slice of the boundary point sets and maps.
-int bcg_driver(Dev& dv, const double* BC, double* const out[4], int dN_x, int dN_y, int dN_g, int N_x, int N_y,
-               int N_g, const double* Sim_Grid_Bnds, const double* Dat_Grid_Bnds, const int* GMap, const int* VMap) {
+// values), each padded and mapped with its side's slice of the boundary point sets and maps (host arrays, or
+// device arrays when resident, like the outputs).
+int bcg_sets(Dev& dv, DevSet ds[4], int dN_x, int dN_y, int N_x, int N_y, const double* Sim_Grid_Bnds,
+             const double* Dat_Grid_Bnds, const int* GMap, const int* VMap, bool resident, cudaStream_t st) {
   if (!Sim_Grid_Bnds || !Dat_Grid_Bnds || !GMap || !VMap) return TRT_ERR_ARG;
-  const long long blk = 2LL * (dN_x + dN_y);
   const int n[4] = {dN_y, dN_x, dN_y, dN_x}, m[4] = {N_y, N_x, N_y, N_x};
-  const long long off[4] = {0, dN_y, (long long)dN_y + dN_x, 2LL * dN_y + dN_x};
   const long long dat_off[4] = {0, 2LL * dN_y + 4, 2LL * (dN_y + dN_x) + 8, 4LL * dN_y + 2LL * dN_x + 12};
   const long long sim_off[4] = {0, 2LL * N_y, 2LL * (N_y + N_x), 4LL * N_y + 2LL * N_x};
   const long long map_off[4] = {0, 4LL * N_y, 4LL * (N_y + N_x), 8LL * N_y + 4LL * N_x};
@@ -1309,13 +1361,24 @@ int bcg_driver(Dev& dv, const double* BC, double* const out[4], int dN_x, int dN
   for (int s = 0; s < 4; ++s) {
     const MapSet ms = {Dat_Grid_Bnds + dat_off[s], Sim_Grid_Bnds + sim_off[s], GMap + map_off[s], VMap + map_off[s],
                        n[s] + 2, m[s]};
-    DevSet ds;
+    if ((rc = make_set(dv, ms, ds[s], resident, st))) return rc;
+  }
+  return TRT_OK;
+}
+
+int bcg_driver(Dev& dv, const double* BC, double* const out[4], int dN_x, int dN_y, int dN_g, int N_g,
+               const DevSet ds[4], bool resident = false, cudaStream_t st = nullptr) {
+  const long long blk = 2LL * (dN_x + dN_y);
+  const int n[4] = {dN_y, dN_x, dN_y, dN_x};
+  const long long off[4] = {0, dN_y, (long long)dN_y + dN_x, 2LL * dN_y + dN_x};
+  int rc;
+  for (int s = 0; s < 4; ++s) {
     double* p;
-    if ((rc = upload_set(dv, ms, ds)) || (rc = dv.get(&p, (size_t)dN_g * (n[s] + 2)))) return rc;
-    side_pad_kernel<<<grid_of((long long)dN_g * (n[s] + 2)), 256>>>(BC, dN_g, blk, off[s], n[s], p);
+    if ((rc = dv.get(&p, (size_t)dN_g * (n[s] + 2)))) return rc;
+    side_pad_kernel<<<grid_of((long long)dN_g * (n[s] + 2)), 256, 0, st>>>(BC, dN_g, blk, off[s], n[s], p);
     trt_host::add_launches(1);
     ROM_CUDA(cudaGetLastError());
-    if ((rc = map_out(dv, ds, p, N_g, out[s]))) return rc;
+    if ((rc = map_out(dv, ds[s], p, N_g, out[s], resident, st))) return rc;
   }
   return TRT_OK;
 }
@@ -1385,11 +1448,90 @@ int trt_pod_reconstruct_bcg(double* Cg_L, double* Cg_B, double* Cg_R, double* Cg
   Dev dv;
   const long long len = 2LL * dN_g * (dN_x + dN_y);
   double* BC;
-  if ((rc = dv.get(&BC, (size_t)len)) ||
+  DevSet ds[4];
+  if ((rc = bcg_sets(dv, ds, dN_x, dN_y, N_x, N_y, Sim_Grid_Bnds, Dat_Grid_Bnds, GMap_xyBnds, VMap_xyBnds, false,
+                     nullptr)) ||
+      (rc = dv.get(&BC, (size_t)len)) ||
       (rc = pod_field(dv, BC, C_BCg, S_BCg, U_BCg, V_BCg, rrank_BCg, len, dN_g, dN_t, PODgsum, a, b, xm, x1, x2)))
     return rc;
-  return bcg_driver(dv, BC, out, dN_x, dN_y, dN_g, N_x, N_y, N_g, Sim_Grid_Bnds, Dat_Grid_Bnds, GMap_xyBnds,
-                    VMap_xyBnds);
+  return bcg_driver(dv, BC, out, dN_x, dN_y, dN_g, N_g, ds);
+}
+
+int trt_pod_reconstruct_fg_device(
+    double* fg_avg_xx, double* fg_avg_yy, double* fg_edgV_xx, double* fg_edgV_xy, double* fg_edgH_yy,
+    double* fg_edgH_xy, const double* C_fg_avg_xx, const double* S_fg_avg_xx, const double* U_fg_avg_xx,
+    const double* V_fg_avg_xx, const double* C_fg_edgV_xx, const double* S_fg_edgV_xx, const double* U_fg_edgV_xx,
+    const double* V_fg_edgV_xx, const double* C_fg_avg_yy, const double* S_fg_avg_yy, const double* U_fg_avg_yy,
+    const double* V_fg_avg_yy, const double* C_fg_edgH_yy, const double* S_fg_edgH_yy, const double* U_fg_edgH_yy,
+    const double* V_fg_edgH_yy, const double* C_fg_edgV_xy, const double* S_fg_edgV_xy, const double* U_fg_edgV_xy,
+    const double* V_fg_edgV_xy, const double* C_fg_edgH_xy, const double* S_fg_edgH_xy, const double* U_fg_edgH_xy,
+    const double* V_fg_edgH_xy, const int* rrank_fg_avg_xx, const int* rrank_fg_edgV_xx, const int* rrank_fg_avg_yy,
+    const int* rrank_fg_edgH_yy, const int* rrank_fg_edgV_xy, const int* rrank_fg_edgH_xy, int dN_x, int dN_y,
+    int dN_g, int dN_t, int N_x, int N_y, int N_g, int N_t, int t, int PODgsum, const double* Sim_Grid_Avg,
+    const double* Sim_Grid_EdgV, const double* Sim_Grid_EdgH, const double* Dat_Grid_Avg, const double* Dat_Grid_EdgV,
+    const double* Dat_Grid_EdgH, const double* Sim_TGrid, const double* Dat_TGrid, const int* GMap_xyAvg,
+    const int* GMap_xyEdgV, const int* GMap_xyEdgH, const int* VMap_xyAvg, const int* VMap_xyEdgV,
+    const int* VMap_xyEdgH, const int* TMap, void* stream) {
+  double* const out[6] = {fg_avg_xx, fg_avg_yy, fg_edgV_xx, fg_edgV_xy, fg_edgH_yy, fg_edgH_xy};
+  const double* const C[6] = {C_fg_avg_xx, C_fg_edgV_xx, C_fg_avg_yy, C_fg_edgH_yy, C_fg_edgV_xy, C_fg_edgH_xy};
+  const double* const S[6] = {S_fg_avg_xx, S_fg_edgV_xx, S_fg_avg_yy, S_fg_edgH_yy, S_fg_edgV_xy, S_fg_edgH_xy};
+  const double* const U[6] = {U_fg_avg_xx, U_fg_edgV_xx, U_fg_avg_yy, U_fg_edgH_yy, U_fg_edgV_xy, U_fg_edgH_xy};
+  const double* const V[6] = {V_fg_avg_xx, V_fg_edgV_xx, V_fg_avg_yy, V_fg_edgH_yy, V_fg_edgV_xy, V_fg_edgH_xy};
+  const int* const rr[6] = {rrank_fg_avg_xx, rrank_fg_edgV_xx, rrank_fg_avg_yy,
+                            rrank_fg_edgH_yy, rrank_fg_edgV_xy, rrank_fg_edgH_xy};
+  for (int k = 0; k < 6; ++k)
+    if (!out[k] || !C[k] || !S[k] || !U[k] || !V[k] || !rr[k]) return TRT_ERR_ARG;
+  if (!grid_dims_ok(dN_x, dN_y, dN_g, N_x, N_y, N_g) || dN_t < 1 || (PODgsum != 0 && PODgsum != 1)) return TRT_ERR_ARG;
+  int a, b;
+  double xm, x1, x2;
+  int rc = time_levels(TMap, Sim_TGrid, Dat_TGrid, dN_t, N_t, t, a, b, xm, x1, x2);
+  if (rc) return rc;
+  if ((rc = device_present())) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const double* const sim[3] = {Sim_Grid_Avg, Sim_Grid_EdgV, Sim_Grid_EdgH};
+  const double* const dat[3] = {Dat_Grid_Avg, Dat_Grid_EdgV, Dat_Grid_EdgH};
+  const int* const gm[3] = {GMap_xyAvg, GMap_xyEdgV, GMap_xyEdgH};
+  const int* const vm[3] = {VMap_xyAvg, VMap_xyEdgV, VMap_xyEdgH};
+  Dev dv;
+  auto rec = [&](int k, long long len, double* dst) {
+    return pod_field(dv, dst, C[k], S[k], U[k], V[k], rr[k], len, dN_g, dN_t, PODgsum, a, b, xm, x1, x2, true, st);
+  };
+  if ((rc = fg_driver(dv, rec, out, dN_x, dN_y, dN_g, N_x, N_y, N_g, sim, dat, gm, vm, true, st))) return rc;
+  ROM_CUDA(cudaStreamSynchronize(st));
+  return TRT_OK;
+}
+
+int trt_pod_reconstruct_bcg_device(double* Cg_L, double* Cg_B, double* Cg_R, double* Cg_T, const double* C_BCg,
+                                   const double* S_BCg, const double* U_BCg, const double* V_BCg,
+                                   const int* rrank_BCg, int dN_x, int dN_y, int dN_g, int dN_t, int N_x, int N_y,
+                                   int N_g, int N_t, int t, int PODgsum, const double* Sim_Grid_Bnds,
+                                   const double* Dat_Grid_Bnds, const double* Sim_TGrid, const double* Dat_TGrid,
+                                   const int* GMap_xyBnds, const int* VMap_xyBnds, const int* TMap, void* stream) {
+  double* const out[4] = {Cg_L, Cg_B, Cg_R, Cg_T};
+  for (double* o : out)
+    if (!o) return TRT_ERR_ARG;
+  if (!C_BCg || !S_BCg || !U_BCg || !V_BCg || !rrank_BCg || !grid_dims_ok(dN_x, dN_y, dN_g, N_x, N_y, N_g) ||
+      dN_t < 1 || (PODgsum != 0 && PODgsum != 1))
+    return TRT_ERR_ARG;
+  int a, b;
+  double xm, x1, x2;
+  int rc = time_levels(TMap, Sim_TGrid, Dat_TGrid, dN_t, N_t, t, a, b, xm, x1, x2);
+  if (rc) return rc;
+  if ((rc = device_present())) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  Dev dv;
+  const long long len = 2LL * dN_g * (dN_x + dN_y);
+  double* BC;
+  DevSet ds[4];
+  if ((rc = bcg_sets(dv, ds, dN_x, dN_y, N_x, N_y, Sim_Grid_Bnds, Dat_Grid_Bnds, GMap_xyBnds, VMap_xyBnds, true,
+                     st)) ||
+      (rc = dv.get(&BC, (size_t)len)) ||
+      (rc = pod_field(dv, BC, C_BCg, S_BCg, U_BCg, V_BCg, rrank_BCg, len, dN_g, dN_t, PODgsum, a, b, xm, x1, x2, true,
+                      st)) ||
+      (rc = bcg_driver(dv, BC, out, dN_x, dN_y, dN_g, N_g, ds, true, st)))
+    return rc;
+  ROM_CUDA(cudaStreamSynchronize(st));
+  return TRT_OK;
 }
 
 int trt_dmd_reconstruct_fg(
@@ -1445,11 +1587,13 @@ int trt_dmd_reconstruct_bcg(double* Cg_L, double* Cg_B, double* Cg_R, double* Cg
   Dev dv;
   const long long len = 2LL * dN_g * (dN_x + dN_y);
   double* BC;
-  if ((rc = dv.get(&BC, (size_t)len)) ||
+  DevSet ds[4];
+  if ((rc = bcg_sets(dv, ds, dN_x, dN_y, N_x, N_y, Sim_Grid_Bnds, Dat_Grid_Bnds, GMap_xyBnds, VMap_xyBnds, false,
+                     nullptr)) ||
+      (rc = dv.get(&BC, (size_t)len)) ||
       (rc = dmd_field(dv, BC, L_BCg, B_BCg, W_BCg, C_BCg, rrank_BCg, len, N_g, DMDgsum, Time)))
     return rc;
-  return bcg_driver(dv, BC, out, dN_x, dN_y, dN_g, N_x, N_y, N_g, Sim_Grid_Bnds, Dat_Grid_Bnds, GMap_xyBnds,
-                    VMap_xyBnds);
+  return bcg_driver(dv, BC, out, dN_x, dN_y, dN_g, N_g, ds);
 }
 
 }  // extern "C"

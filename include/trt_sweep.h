@@ -572,6 +572,31 @@ int trt_dmd_reconstruct_bcg(double* Cg_L, double* Cg_B, double* Cg_R, double* Cg
                             int dN_x, int dN_y, int dN_g, int N_x, int N_y, int N_g, double Time, int DMDgsum,
                             const double* Sim_Grid_Bnds, const double* Dat_Grid_Bnds, const int* GMap_xyBnds,
                             const int* VMap_xyBnds);
+/* Device-resident forms of trt_pod_reconstruct_fg / trt_pod_reconstruct_bcg for a caller that keeps the
+ * decomposition in HBM (an online ROM run): the outputs, the decomposition arrays (C, S, U, V), the point sets and
+ * the maps are device arrays; the ranks, the time grids and TMap are host arrays.  The maps are checked on the
+ * device before any mapping reads through them; the work runs on the given stream and is complete on return. */
+int trt_pod_reconstruct_fg_device(
+    double* fg_avg_xx, double* fg_avg_yy, double* fg_edgV_xx, double* fg_edgV_xy, double* fg_edgH_yy,
+    double* fg_edgH_xy, const double* C_fg_avg_xx, const double* S_fg_avg_xx, const double* U_fg_avg_xx,
+    const double* V_fg_avg_xx, const double* C_fg_edgV_xx, const double* S_fg_edgV_xx, const double* U_fg_edgV_xx,
+    const double* V_fg_edgV_xx, const double* C_fg_avg_yy, const double* S_fg_avg_yy, const double* U_fg_avg_yy,
+    const double* V_fg_avg_yy, const double* C_fg_edgH_yy, const double* S_fg_edgH_yy, const double* U_fg_edgH_yy,
+    const double* V_fg_edgH_yy, const double* C_fg_edgV_xy, const double* S_fg_edgV_xy, const double* U_fg_edgV_xy,
+    const double* V_fg_edgV_xy, const double* C_fg_edgH_xy, const double* S_fg_edgH_xy, const double* U_fg_edgH_xy,
+    const double* V_fg_edgH_xy, const int* rrank_fg_avg_xx, const int* rrank_fg_edgV_xx, const int* rrank_fg_avg_yy,
+    const int* rrank_fg_edgH_yy, const int* rrank_fg_edgV_xy, const int* rrank_fg_edgH_xy, int dN_x, int dN_y,
+    int dN_g, int dN_t, int N_x, int N_y, int N_g, int N_t, int t, int PODgsum, const double* Sim_Grid_Avg,
+    const double* Sim_Grid_EdgV, const double* Sim_Grid_EdgH, const double* Dat_Grid_Avg, const double* Dat_Grid_EdgV,
+    const double* Dat_Grid_EdgH, const double* Sim_TGrid, const double* Dat_TGrid, const int* GMap_xyAvg,
+    const int* GMap_xyEdgV, const int* GMap_xyEdgH, const int* VMap_xyAvg, const int* VMap_xyEdgV,
+    const int* VMap_xyEdgH, const int* TMap, void* stream);
+int trt_pod_reconstruct_bcg_device(double* Cg_L, double* Cg_B, double* Cg_R, double* Cg_T, const double* C_BCg,
+                                   const double* S_BCg, const double* U_BCg, const double* V_BCg,
+                                   const int* rrank_BCg, int dN_x, int dN_y, int dN_g, int dN_t, int N_x, int N_y,
+                                   int N_g, int N_t, int t, int PODgsum, const double* Sim_Grid_Bnds,
+                                   const double* Dat_Grid_Bnds, const double* Sim_TGrid, const double* Dat_TGrid,
+                                   const int* GMap_xyBnds, const int* VMap_xyBnds, const int* TMap, void* stream);
 /* Replaces SUBROUTINE RRANK_CALC, MainSrc/POD_ROUTINES.f08:791-819: the smallest rank whose discarded singular
  * values sig(rank+1:len) have a norm at most eps times the norm of all of them (len when none qualifies before
  * the last), the truncation READ_POD_FULL / READ_POD_GPART apply to a stored decomposition.  Host code. */

@@ -7,6 +7,8 @@ Singular values agree to 1e-12 of the largest; singular vectors are unique only 
 the singular values are separated), so they are compared after aligning signs, on well-separated spectra.
 The centring vector and the reconstruction follow the reference's operation order and agree bit for bit.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -614,16 +616,43 @@ def test_pod_rom_through_the_reconstruction_drivers():
     tgrids = pkg.GENERATE_GRIDS_T(ts.dt, ts.dt, 0.0, 0.0, nt, nt)
     assert np.array_equal(tgrids[2], np.repeat(np.arange(1, nt + 1), 2))
     dims = (nx, ny, ng, nt)
+    # the device-resident forms: decompositions, point sets, maps and outputs in HBM
+    import torch
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    P = lambda x: ctypes.c_void_p(x.data_ptr())
+    tg = [np.ascontiguousarray(a, dtype=np.float64) for a in tgrids[:2]]
+    tm = np.ascontiguousarray(tgrids[2], dtype=np.int32)
+    D = ctypes.POINTER(ctypes.c_double)
+    I = ctypes.POINTER(ctypes.c_int)
+    names = ("avg_xx", "edgV_xx", "avg_yy", "edgH_yy", "edgV_xy", "edgH_xy")
+    ddec = {k: [dev(a) for a in dec[k][:4]] for k in names}
+    dgr = {k: dev(v) for k, v in grids.items()}
+    bd = [dev(a) for a in bdec[:4]]
     with device(prob, ts, km, bcT, cv, ho_form=1, **kw) as s:
         for t in range(1, nt + 1):
             fg = pkg.POD_RECONSTRUCT_fg(dec, dims, dims, t, 0, grids, tgrids)
             cg = dict(zip(FACTORS[6:], pkg.POD_RECONSTRUCT_BCg(bdec, dims, dims, t, 0, grids, tgrids)))
+            dout = {k: torch.zeros(snaps[k][0].size, dtype=torch.float64, device="cuda") for k in FACTORS}
+            rc = pkg.lib().trt_pod_reconstruct_fg_device(
+                *[P(dout[k]) for k in FACTORS[:6]], *[P(a) for k in names for a in ddec[k]],
+                *[dec[k][4].ctypes.data_as(I) for k in names], nx, ny, ng, nt, nx, ny, ng, nt, t, 0,
+                *[P(dgr[p + k]) for p in ("Sim_Grid_", "Dat_Grid_") for k in ("Avg", "EdgV", "EdgH")],
+                *[a.ctypes.data_as(D) for a in tg],
+                *[P(dgr[p + k]) for p in ("GMap_xy", "VMap_xy") for k in ("Avg", "EdgV", "EdgH")], tm.ctypes.data_as(I),
+                None)
+            assert rc == 0
+            rc = pkg.lib().trt_pod_reconstruct_bcg_device(
+                *[P(dout[k]) for k in FACTORS[6:]], *[P(a) for a in bd], bdec[4].ctypes.data_as(I), nx, ny, ng, nt,
+                nx, ny, ng, nt, t, 0, P(dgr["Sim_Grid_Bnds"]), P(dgr["Dat_Grid_Bnds"]), *[a.ctypes.data_as(D) for a in tg],
+                P(dgr["GMap_xyBnds"]), P(dgr["VMap_xyBnds"]), tm.ctypes.data_as(I), None)
+            assert rc == 0
             for k in FACTORS:
                 out = fg[k] if k in fg else cg[k]
                 ref = snaps[k][t - 1].ravel(order="F")
                 assert out.shape == ref.shape
                 assert np.abs(out - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()), k
-                s.mlqd_put(k, out)
+                assert np.array_equal(dout[k].cpu().numpy(), out), k      # resident form = host form, bit for bit
+                assert pkg.lib().trt_mlqd_put(s.handle, k.encode(), P(dout[k]), out.size, 1) == 0
             st = s.mlqd_step()
             assert st["sweeps"] == 0 and st["mgqd_nonconv"] == 0
             T = s.mlqd_field("Temp")
