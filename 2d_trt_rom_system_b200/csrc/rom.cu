@@ -879,7 +879,9 @@ int map_grids_impl(int* Map, const double* Grid1, const double* Grid2, int len1,
     double d = std::numeric_limits<double>::max();   // HUGE(0d0)
     long long l[4] = {0, 0, 0, 0};
     for (long long i = 1; i <= len1; i += 2) {   // closest point of grid 1 (DIST), first one on ties
-      const double r = std::fabs(std::sqrt(std::pow(G1(i) - G2(j), 2) + std::pow(G1(i + 1) - G2(j + 1), 2)));
+      // DIST's integer powers (xp1 - xp2)**2 are products
+      const double ddx = G1(i) - G2(j), ddy = G1(i + 1) - G2(j + 1);
+      const double r = std::fabs(std::sqrt(ddx * ddx + ddy * ddy));
       if (r < d) {
         d = r;
         l[0] = i;

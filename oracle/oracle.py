@@ -782,7 +782,8 @@ def map_grids(Grid1, Grid2, xlen1, len1=None, len2=None):
     for j in range(1, len2 + 1, 2):
         d, l1 = np.finfo(np.float64).max, 0
         for i in range(1, len1 + 1, 2):
-            r = abs(math.sqrt((G1(i) - G2(j)) ** 2 + (G1(i + 1) - G2(j + 1)) ** 2))
+            ddx, ddy = G1(i) - G2(j), G1(i + 1) - G2(j + 1)   # DIST's integer powers are products
+            r = abs(math.sqrt(ddx * ddx + ddy * ddy))
             if r < d:
                 d, l1 = r, i
         dx, dy = G1(l1) - G2(j), G1(l1 + 1) - G2(j + 1)
