@@ -90,3 +90,44 @@ def test_rom_entry_points_need_a_device():
     with pytest.raises(pkg.TrtError) as e:
         pkg.DMD_RECONSTRUCT(out, np.ones(2), np.ones(2), np.ones(12), np.zeros(12), [1, 1], 12, 2, 0, 0.5)
     assert e.value.code == pkg._lib.TRT_ERR_NODEV
+
+
+def test_reconstruction_drivers_check_arguments_before_the_device():
+    """The ROM drivers reject inconsistent calls on the host (group counts that differ, a simulation level or a
+    time-map entry out of range, two bracketing data levels at one time) and only then look for a device."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    dN, N, ng, nt = 3, 4, 2, 3
+    d = np.full(dN, 1.0 / dN)
+    s = np.full(N, 1.0 / N)
+    grids = pkg.GENERATE_GRIDS_XY(d, d, s, s, 1.0, 1.0, 1.0, 1.0)
+    tgrids = pkg.GENERATE_GRIDS_T(1e-3, 1e-3, 0.0, 0.0, nt, nt)
+    rank = np.ones(ng, dtype=np.int32)
+
+    def dec(n):
+        return (np.zeros(n), np.ones(ng), np.ones(n), np.ones(nt * ng), rank)
+
+    la, lv, lh = dN * dN * ng, (dN + 1) * dN * ng, dN * (dN + 1) * ng
+    fg = {k: dec(n) for k, n in zip(("avg_xx", "edgV_xx", "avg_yy", "edgH_yy", "edgV_xy", "edgH_xy"),
+                                    (la, lv, la, lh, lv, lh))}
+    bc = dec(ng * 4 * dN)
+
+    def code(fn, *a):
+        with pytest.raises(pkg.TrtError) as e:
+            fn(*a)
+        return e.value.code
+
+    ARG, NODEV = pkg._lib.TRT_ERR_ARG, pkg._lib.TRT_ERR_NODEV
+    assert code(pkg.POD_RECONSTRUCT_fg, fg, (dN, dN, ng, nt), (N, N, ng, nt), 2, 0, grids, tgrids) == NODEV
+    assert code(pkg.POD_RECONSTRUCT_BCg, bc, (dN, dN, ng, nt), (N, N, ng, nt), 2, 0, grids, tgrids) == NODEV
+    assert code(pkg.POD_RECONSTRUCT_fg, fg, (dN, dN, ng, nt), (N, N, ng + 1, nt), 2, 0, grids, tgrids) == ARG
+    assert code(pkg.POD_RECONSTRUCT_BCg, bc, (dN, dN, ng, nt), (N, N, ng, nt), nt + 1, 0, grids, tgrids) == ARG
+    bad_map = (tgrids[0], tgrids[1], np.array([1, 1, nt + 1, nt + 1, 3, 3], dtype=np.int32))
+    assert code(pkg.POD_RECONSTRUCT_BCg, bc, (dN, dN, ng, nt), (N, N, ng, nt), 2, 0, grids, bad_map) == ARG
+    same_time = (tgrids[0], np.array([1e-3, 1e-3, 3e-3]), np.array([1, 1, 2, 1, 3, 3], dtype=np.int32))
+    assert code(pkg.POD_RECONSTRUCT_BCg, bc, (dN, dN, ng, nt), (N, N, ng, nt), 2, 0, grids, same_time) == ARG
+    dmd = {k: (np.ones(ng, dtype=complex), np.ones(ng, dtype=complex), np.ones(v[0].size, dtype=complex), v[0], rank)
+           for k, v in fg.items()}
+    assert code(pkg.DMD_RECONSTRUCT_fg, dmd, (dN, dN, ng), (N, N, ng), 0.1, 0, grids) == NODEV
+    assert code(pkg.DMD_RECONSTRUCT_fg, dmd, (dN, dN, ng), (N, N, ng), 0.1, 2, grids) == ARG
