@@ -26,6 +26,8 @@ TRT_PREC_FP64 = 0
 TRT_PREC_FP32 = 1
 
 TRT_ROLL_STATE = 1
+TRT_LAW_FLECK_CUMMINGS = 0   # material laws of the time loops (trt_tstep_set_law)
+TRT_LAW_CONFIG = 1
 TRT_MOMENTS = 2
 TRT_RES_CALC = 4
 
@@ -131,6 +133,7 @@ SIGNATURES = {
     "trt_batch_tstep": (_i, [_P, _I, _D, _D]),
     "trt_tstep_setup": (_i, [_P, _D, _D, _D, _D, _d, _d, _d, _d, _I, _D, _i, _d, _i]),
     "trt_tstep": (_i, [_P, _I, _D, _D]),
+    "trt_tstep_set_law": (_i, [_P, _i]),
     "trt_get_temperature": (_i, [_P, _D]),
     "trt_put_temperature": (_i, [_P, _D]),
     "trt_strerror": (ctypes.c_char_p, [_i]),

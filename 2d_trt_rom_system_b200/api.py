@@ -665,10 +665,13 @@ class TransportSweep:
                                         dptr(_f64(Nu_g, (self.ng + 1,)))), "trt_init_state")
 
     def tstep_setup(self, Nu_g, kappa_mult, cV, Temp, Kap0, Comp_Unit, c, Delt, BC_Type=(0, 0, 0, 0),
-                    bcT=(0.0, 0.0, 0.0, 0.0), conv_type=2, conv_ho=1e-12, maxit_rte=150):
+                    bcT=(0.0, 0.0, 0.0, 0.0), conv_type=2, conv_ho=1e-12, maxit_rte=150, law=0):
         """Device time stepping with the reference's run_type 'tr_no_qd' (temperatures in eV);
-        kappa_mult(i,j) = Kappa_Mult(Mat(i,j)); cV per cell or a scalar."""
+        kappa_mult(i,j) = Kappa_Mult(Mat(i,j)); cV per cell or a scalar.  law 0: the reference's
+        Fleck-Cummings material and MEB_SOLVE; law 1 (TRT_LAW_CONFIG): the configurations' opacity law
+        with kappa_mult = kappa0(i,j) and the T^4-linearised energy balance (Kap0 unused)."""
         shp = (self.nx, self.ny)
+        check(_lib.lib().trt_tstep_set_law(self._h, int(law)), "trt_tstep_set_law")
         cv = _f64(np.broadcast_to(np.asarray(cV, dtype=np.float64), shp), shp)
         bc = np.ascontiguousarray(BC_Type, dtype=np.int32)
         bt = np.ascontiguousarray(bcT, dtype=np.float64)

@@ -18,8 +18,8 @@ HEADERS = ["aux_kernels.cuh", "dropin_kernels.cuh", "gqd_kernels.cuh", "handle_h
            "sweep_kernel.cuh", "tstep_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIBS = ["-lcusolver", "-lcublas"]   # the SVD / eigenpairs / products of POD and DMD (rom.cu)
-NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-shared",
-              "-diag-suppress", "177"]
+NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-diag-suppress", "177"]
+OBJDIR = os.path.join(HERE, "_build")
 
 
 def _nvcc():
@@ -39,14 +39,26 @@ def _stale():
 
 
 def build(force=False, verbose=False):
-    """Compile the library if a source is newer than it.  Returns the path of the .so."""
+    """Compile the library if a source is newer than it: the translation units in parallel, then one
+    link.  Returns the path of the .so."""
     if not force and not _stale():
         return LIB
-    cmd = [_nvcc()] + NVCC_FLAGS + ARCH + ["-I" + INCLUDE, "-I" + CSRC, "-o", LIB + ".tmp"] + \
-        [os.path.join(CSRC, s) for s in SOURCES] + LIBS
+    from concurrent.futures import ThreadPoolExecutor
+    os.makedirs(OBJDIR, exist_ok=True)
+    objs = [os.path.join(OBJDIR, os.path.splitext(s)[0] + ".o") for s in SOURCES]
+    cmds = [[_nvcc()] + NVCC_FLAGS + ARCH + ["-I" + INCLUDE, "-I" + CSRC, "-c", "-o", o, os.path.join(CSRC, s)]
+            for s, o in zip(SOURCES, objs)]
     if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
+        for c in cmds:
+            print(" ".join(c), file=sys.stderr)
+    with ThreadPoolExecutor(len(cmds)) as ex:
+        procs = list(ex.map(lambda c: subprocess.run(c), cmds))
+    if any(p.returncode for p in procs):
+        raise subprocess.CalledProcessError(1, "nvcc")
+    link = [_nvcc(), "-shared"] + ARCH + ["-o", LIB + ".tmp"] + objs + LIBS
+    if verbose:
+        print(" ".join(link), file=sys.stderr)
+    subprocess.run(link, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

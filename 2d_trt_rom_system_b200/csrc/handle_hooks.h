@@ -26,6 +26,9 @@ struct HandleView {
   const double *omx, *omy, *w;      // direction set (host)
   const double* nu;                 // group edges Nu_g (host, n_g + 1)
   const double* cv;                 // heat capacity per cell (device)
+  int law;                          // material law (TRT_LAW_*)
+  const double* kmult;              // Kappa_Mult(Mat(i,j)), or kappa0(i,j) of the configurations' law (device)
+  const double* nu_dev;             // group edges Nu_g (device, n_g + 1)
 };
 
 // Requires trt_tstep_setup to have run on the handle.

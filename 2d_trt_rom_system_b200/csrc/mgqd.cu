@@ -1040,6 +1040,7 @@ int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm) {
   int rc = trt_host::handle_view(h, &m->v);
   if (rc) return rc;
   const trt_host::HandleView& v = m->v;
+  if (v.law != TRT_LAW_FLECK_CUMMINGS) return TRT_ERR_ARG;   // the grey emission below is the reference's
   m->h = h;
   m->p = prm;
   const int nx = v.nx, ny = v.ny, ng = v.ng;

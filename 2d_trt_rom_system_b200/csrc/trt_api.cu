@@ -261,6 +261,7 @@ struct trt_ctx {
   unsigned long long* d_conv = nullptr;   // [2][5] convergence reductions (T, E)
   double ts_Kap0 = 0.0, ts_conv_ho = 0.0, ts_Tb[4] = {0, 0, 0, 0};
   int ts_conv_type = 1, ts_maxit = 1, ts_bc[4] = {0, 0, 0, 0};
+  int ts_law = trt::kLawFleckCummings;   // material law of the time loops (trt_tstep_set_law)
   std::vector<double> ts_nu;
   // pipelined stepping (trt_set_material_async / trt_moments_async): a copy stream for each direction,
   // a staging pair for the next material, and the events that order them against the handle's stream
@@ -999,7 +1000,7 @@ int material_update_impl(trt_ctx* c, double* mgsrc = nullptr) {
   const long long n = (long long)c->nx * c->ny * c->ng;
   trt::material_update_kernel<Real><<<grid_for(n), 256, 0, c->stream>>>(
       c->nx, c->ny, c->ng, c->d_T, c->d_nu, c->d_kmult, c->comp_unit, c->d_kap64, c->d_q64, (Real*)c->d_kap,
-      (Real*)c->d_q, mgsrc);
+      (Real*)c->d_q, mgsrc, c->ts_law);
   TRT_LAUNCHED();
   TRT_CUDA(cudaGetLastError());
   c->use_srcfull = false;
@@ -1039,9 +1040,14 @@ int tstep_after_sweep(trt_ctx* c, unsigned long long* host) {
   const bool reflective = c->ts_bc[0] > 0 || c->ts_bc[1] > 0 || c->ts_bc[2] > 0 || c->ts_bc[3] > 0;
   int rc;
   if (reflective && (rc = bc_update_impl<Real>(c, c->ts_bc, c->ts_Tb, c->comp_unit, c->ts_nu.data()))) return rc;
-  trt::meb_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>(c->nx, c->ny, c->ng, c->dout.Eg_avg, c->d_kap64,
-                                                                    c->d_Told, c->d_cv, c->dt, c->ts_Kap0,
-                                                                    c->comp_unit, c->d_T);
+  if (c->ts_law == trt::kLawConfig)
+    trt::meb_law_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>(c->nx, c->ny, c->ng, c->dout.Eg_avg,
+                                                                          c->d_kap64, c->d_Told, c->d_cv, c->d_nu,
+                                                                          c->dt, c->comp_unit, c->c, c->d_T);
+  else
+    trt::meb_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>(c->nx, c->ny, c->ng, c->dout.Eg_avg, c->d_kap64,
+                                                                      c->d_Told, c->d_cv, c->dt, c->ts_Kap0,
+                                                                      c->comp_unit, c->d_T);
   TRT_LAUNCHED();
   TRT_CUDA(cudaGetLastError());
   if ((rc = material_update_impl<Real>(c))) return rc;
@@ -1904,6 +1910,20 @@ int trt_tstep_setup(trt_ctx* c, const double* Nu_g, const double* kappa_mult, co
   return TRT_OK;
 }
 
+static_assert(TRT_LAW_FLECK_CUMMINGS == trt::kLawFleckCummings && TRT_LAW_CONFIG == trt::kLawConfig,
+              "material law numbering");
+
+int trt_tstep_set_law(trt_ctx* c, int law) {
+  if (!c || (law != trt::kLawFleckCummings && law != trt::kLawConfig)) return TRT_ERR_ARG;
+  c->ts_law = law;
+  if (c->ts_ready) {   // the material follows the law at once
+    int rc = c->prec == TRT_PREC_FP64 ? material_update_impl<double>(c) : material_update_impl<float>(c);
+    if (rc) return rc;
+    TRT_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return TRT_OK;
+}
+
 int trt_tstep(trt_ctx* c, int* rt_its, double* T_norm, double* E_norm) {
   if (!c) return TRT_ERR_ARG;
   if (!c->ts_ready || (!c->have_state && !c->swept)) return TRT_ERR_STATE;
@@ -2358,6 +2378,9 @@ int handle_view(trt_ctx* c, HandleView* v) {
   v->w = c->w.data();
   v->nu = c->ts_nu.data();
   v->cv = c->d_cv;
+  v->law = c->ts_law;
+  v->kmult = c->d_kmult;
+  v->nu_dev = c->d_nu;
   return TRT_OK;
 }
 

@@ -54,23 +54,54 @@ __device__ __forceinline__ double ts_kapb(double T, double nu_low, double nu_hig
   return sig0 * (exp(-nu_low / T) - exp(-nu_high / T)) / (t3 * sig);
 }
 
+// Opacity law of the synthetic configurations, in place of kapB_calc:
+//   kappa_g(T) = kappa0 (1 - exp(-nu_g/T)) / (nu_g^3 sqrt(T)),  nu_g = sqrt(nu_low nu_high),
+// T and nu in keV (the arguments are in eV, as everywhere else).
+__device__ __forceinline__ double ts_law_kappa(double T, double nu_low, double nu_high, double kappa0) {
+  const double nb = sqrt(nu_low * nu_high) * 1e-3;
+  const double tk = T * 1e-3;
+  return kappa0 * (-expm1(-nb / tk)) / (((nb * nb) * nb) * sqrt(tk));
+}
+
+// dBg/dT of Bg_planck_calc, Bg = 2 T^4 (sigint(nu_high/T) - sigint(nu_low/T)) / K, with the exact
+// derivative of the Planck integral, d sigint(z)/dz = z^3/(e^z - 1):
+//   dBg/dT = 2 T^3 (4 (sigint(z_h) - sigint(z_l)) - z_h^4/(e^z_h - 1) + z_l^4/(e^z_l - 1)) / K.
+__device__ __forceinline__ double ts_bg_planck_dT(double T, double nu_low, double nu_high, double comp_unit) {
+  if (T <= 1e-15) return 0.0;
+  const double zh = nu_high / T, zl = nu_low / T;
+  const double s = ts_sigint(zh) - ts_sigint(zl);
+  const double ph = zh > 700.0 ? 0.0 : (((zh * zh) * (zh * zh)) / expm1(zh));
+  const double pl = zl > 700.0 ? 0.0 : (((zl * zl) * (zl * zl)) / expm1(zl));
+  const double h3 = (kTsH * kTsH) * kTsH, c2 = kTsC * kTsC, e2 = kTsErg * kTsErg;
+  const double K = ((h3 * c2) * (e2 * e2)) * comp_unit;
+  const double t3 = (T * T) * T;
+  return ((2.0 * t3) * (((4.0 * s) - ph) + pl)) / K;
+}
+
+// Material laws of the time loops: the reference's Fleck-Cummings opacity with MEB_SOLVE, or the
+// configurations' opacity law with the T^4-linearised energy balance (meb_law_kernel).
+enum MaterialLaw { kLawFleckCummings = 0, kLawConfig = 1 };
+
 // MATERIAL_UPDATE (UPDATES.f08:110-152) for the sweep: KapE = KapB = kapB_calc(T, nu_g, nu_g+1) *
 // Kappa_Mult(Mat(i,j)) and the isotropic corner source RT_Src = KapB * Bg, one value per (cell, g)
-// (the reference stores it for all 4 corners and N_m directions).  kmult(i,j) = Kappa_Mult(Mat(i,j)).
+// (the reference stores it for all 4 corners and N_m directions).  kmult(i,j) = Kappa_Mult(Mat(i,j)),
+// or kappa0(i,j) of the configurations' law (law = kLawConfig).
 // Writes the FP64 copies and the sweep's Real copies; with mgsrc set, also the low-order source
 // MGQD_Src = 4 pi KapB Bg (UPDATES.f08:141).
 template <class Real>
 __global__ void material_update_kernel(int nx, int ny, int ng, const double* __restrict__ T,
                                        const double* __restrict__ nu, const double* __restrict__ kmult,
                                        double comp_unit, double* __restrict__ kap64, double* __restrict__ q64,
-                                       Real* __restrict__ kap, Real* __restrict__ q, double* __restrict__ mgsrc) {
+                                       Real* __restrict__ kap, Real* __restrict__ q, double* __restrict__ mgsrc,
+                                       int law) {
   const long long nxy = (long long)nx * ny, n = nxy * ng;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
     const long long cell = k % nxy;
     const int g = (int)(k / nxy);
     const double Tc = T[cell];
     const double Bg = ts_bg_planck(Tc, nu[g], nu[g + 1], comp_unit);
-    const double kB = ts_kapb(Tc, nu[g], nu[g + 1]) * kmult[cell];
+    const double kB = law == kLawConfig ? ts_law_kappa(Tc, nu[g], nu[g + 1], kmult[cell])
+                                        : ts_kapb(Tc, nu[g], nu[g + 1]) * kmult[cell];
     const double src = kB * Bg;
     kap64[k] = kB;
     q64[k] = src;
@@ -104,6 +135,31 @@ __global__ void meb_kernel(int nx, int ny, int ng, const double* __restrict__ Eg
     const double cvk = cv[k];
     const double coef = c2h3 / (((c2h3 * cvk) * comp_unit) + lin);
     T[k] = (coef * ((((Delt * kTsC) * kb) * E) + cvk * T_old[k])) * comp_unit;
+  }
+}
+
+// Energy balance of the configurations' material (in place of MEB_SOLVE), backward Euler per cell,
+//   cv (T - T_old)/Delt = sum_g KapE_g (c Eg - 4 pi Bg(T)),
+// with the emission linearised about the current iterate T* (one Newton step per outer iteration):
+//   T = (cv T_old/Delt + sum_g KapE_g (c Eg - 4 pi Bg(T*) + 4 pi Bg'(T*) T*)) / (cv/Delt + 4 pi sum_g KapE_g Bg'(T*)).
+// T holds T* on entry.  Eg are the transport group energies (HO_Eg_avg), KapE the material at T*.
+__global__ void meb_law_kernel(int nx, int ny, int ng, const double* __restrict__ Eg, const double* __restrict__ kapE,
+                               const double* __restrict__ T_old, const double* __restrict__ cv,
+                               const double* __restrict__ nu, double Delt, double comp_unit, double c,
+                               double* __restrict__ T) {
+  const long long nxy = (long long)nx * ny;
+  const double fp = 4.0 * 3.141592653589793;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nxy; k += (long long)gridDim.x * blockDim.x) {
+    const double ts = T[k];
+    double num = (cv[k] * T_old[k]) / Delt, den = cv[k] / Delt;
+    for (int g = 0; g < ng; ++g) {
+      const double kap = kapE[k + nxy * g];
+      const double B = ts_bg_planck(ts, nu[g], nu[g + 1], comp_unit);
+      const double dB = ts_bg_planck_dT(ts, nu[g], nu[g + 1], comp_unit);
+      num = num + kap * (((c * Eg[k + nxy * g]) - (fp * B)) + ((fp * dB) * ts));
+      den = den + (fp * kap) * dB;
+    }
+    T[k] = num / den;
   }
 }
 

@@ -240,6 +240,18 @@ def fc_timestep_setup(prob, Tini_eV=None):
                          cv=fc_cv(max(bcT[0], 1.0)), Kap0=KAP0_FC, Tini_eV=Tini, bcT_eV=bcT, dt=prob.dt)
 
 
+def config_timestep_setup(prob, Tini_eV=None):
+    """Inputs of trt_tstep_setup for a Problem with its own physics (TRT_LAW_CONFIG): the opacity law
+    kappa0 (1 - exp(-nu/T)) / (nu^3 sqrt(T)) with kappa0 passed as kappa_mult, the per-cell c_v (given per
+    kT_ref = 1 keV in the radiation-energy unit of the reference's Comp_Unit scaling, converted here to per
+    eV, the library's temperature unit), T0 and the boundary temperatures in eV.  Kap0 is unused."""
+    bcT = tuple(t * KEV for t in prob.bcT)
+    Tini = prob.T0 * KEV if Tini_eV is None else Tini_eV
+    return TimeStepSetup(nu_eV=prob.nu_eV, kappa_mult=np.asfortranarray(np.asarray(prob.kappa0, dtype=np.float64)),
+                         cv=np.asfortranarray(np.asarray(prob.cv, dtype=np.float64) / KEV), Kap0=0.0, Tini_eV=Tini,
+                         bcT_eV=bcT, dt=prob.dt)
+
+
 def mgqd_inputs(nx, ny, ng, seed=0, theta=1.0, kap_range=(1e-4, 1e4), xlen=6.0, ylen=6.0, dt=2e-3, uniform=False):
     """Seeded synthetic inputs of MLOQD_FV / OLD_MGQD_COEFS (MLOQD_SOLVES.f08:12-362) with the value
     ranges a time step produces: per-group opacities log-uniform over kap_range (thick and thin groups

@@ -384,6 +384,20 @@ int trt_tstep_setup(trt_ctx* ctx, const double* Nu_g, const double* kappa_mult, 
                     double Kap0, double Comp_Unit, double c, double Delt, const int* BC_Type, const double* bcT,
                     int conv_type, double conv_ho, int maxit_rte);
 int trt_tstep(trt_ctx* ctx, int* rt_its, double* T_norm, double* E_norm);
+/* Material law of the time loops (trt_tstep, trt_batch_tstep, trt_mlqd_step).
+ *   TRT_LAW_FLECK_CUMMINGS (default): the reference's material, KapE = kapB_calc(T) * Kappa_Mult
+ *     (TEMP_FUNCTIONS.f08:11-32, UPDATES.f08:130-150) and MEB_SOLVE (UPDATES.f08:185-230).
+ *   TRT_LAW_CONFIG: the synthetic configurations' opacity law in place of kapB_calc,
+ *     KapE = kappa0(i,j) (1 - exp(-nu_g/T)) / (nu_g^3 sqrt(T)), nu_g = sqrt(Nu_g(g) Nu_g(g+1)), T and nu in
+ *     keV (the arguments stay in eV), with kappa0 passed as trt_tstep_setup's kappa_mult; MEB_SOLVE is
+ *     replaced by the backward-Euler balance cv (T - T_old)/Delt = sum_g KapE_g (c Eg - 4 pi Bg(T)) with
+ *     the emission linearised about the current iterate (one Newton step per outer iteration); Kap0 is
+ *     unused.  The reference has no such material (it is not expressible in its input); MATERIAL_UPDATE
+ *     is the template.
+ * May be called before or after trt_tstep_setup; after it, the material is recomputed at once. */
+#define TRT_LAW_FLECK_CUMMINGS 0
+#define TRT_LAW_CONFIG 1
+int trt_tstep_set_law(trt_ctx* ctx, int law);
 int trt_get_temperature(trt_ctx* ctx, double* Temp);
 /* Replace the device temperature and recompute the material from it (MATERIAL_UPDATE). */
 int trt_put_temperature(trt_ctx* ctx, const double* Temp);

@@ -33,6 +33,8 @@ _SIG = {
     "oracle_openmp_max_threads": (_i, []),
     "oracle_material_update": (_i, [_i, _i, _i, _D, _D, _D, _d, _D, _D, _D]),
     "oracle_meb_solve": (_i, [_i, _i, _i, _D, _D, _D, _D, _d, _D, _d, _d]),
+    "oracle_material_update_law": (_i, [_i, _i, _i, _D, _D, _D, _d, _D, _D, _D]),
+    "oracle_meb_solve_law": (_i, [_i, _i, _i, _D, _D, _D, _D, _d, _D, _D, _d, _d]),
     "oracle_convergence": (_i, [_i, _d, _D, _D, _D, _i, _i, _D, _D]),
     "oracle_old_mgqd_coefs": (_i, [_i, _i, _i] + [_D] * 17 + [_d, _d, _d] + [_D] * 5),
     "oracle_mloqd_fv": (_i, [_i, _i, _i] + [_D] * 29 + [_d, _d, _d, _i, _i] + [_D] * 10 + [_I, _d, _d, _d]),
@@ -227,6 +229,29 @@ def meb_solve(Temp_old, Eg_HO, KapE, Delt, cV, Kap0, comp_unit):
     return T
 
 
+def material_update_law(Temp, Nu_g, kappa0, comp_unit):
+    """The configurations' opacity law in place of kapB_calc (MATERIAL_UPDATE's template,
+    UPDATES.f08:130-150): KapE = kappa0 (1 - exp(-nu/T)) / (nu^3 sqrt(T)) (keV), src = KapE * Bg, Bg."""
+    nx, ny = Temp.shape
+    ng = len(Nu_g) - 1
+    K, S, B = zeros(nx, ny, ng), zeros(nx, ny, ng), zeros(nx, ny, ng)
+    rc = lib().oracle_material_update_law(nx, ny, ng, _p(F(Temp)), _p(F(Nu_g)), _p(F(kappa0)), float(comp_unit),
+                                          _p(K), _p(S), _p(B))
+    assert rc == 0
+    return K, S, B
+
+
+def meb_solve_law(Temp, Temp_old, Eg_HO, KapE, Delt, cV, Nu_g, comp_unit, c):
+    """Backward-Euler energy balance of the configurations with the emission linearised about Temp (one
+    Newton step); returns the new Temp."""
+    nx, ny, ng = Eg_HO.shape
+    T = F(Temp).copy(order="F")
+    rc = lib().oracle_meb_solve_law(nx, ny, ng, _p(T), _p(F(Eg_HO)), _p(F(KapE)), _p(F(Temp_old)), float(Delt),
+                                    _p(F(np.broadcast_to(cV, (nx, ny)))), _p(F(Nu_g)), float(comp_unit), float(c))
+    assert rc == 0
+    return T
+
+
 def convergence(conv_type, eps, x, x_old, x_old2, its):
     """CONVERGENCE (CONVERGENCE_CHECKS.f08:7-44): (converged, norm, rho)."""
     n = int(np.asarray(x).size)
@@ -238,13 +263,18 @@ def convergence(conv_type, eps, x, x_old, x_old2, its):
 
 def tr_no_qd_steps(st, Omega_x, Omega_y, quad_weight, Delx, Dely, Nu_g, kappa_mult, cV, Kap0, comp_unit, c, Delt,
                    steps, conv_type=2, conv_ho=1e-12, maxit=150, bc_type=(0, 0, 0, 0), bcT=(0.0, 0.0, 0.0, 0.0),
-                   threads=4):
+                   threads=4, solver=1, law=0, record=None):
     """Time steps of TRT_MLQD_ALGORITHM with run_type 'tr_no_qd' (ALGORITHMS.f08:389-421, 518-572,
     662-668, 816-836).  st: dict with I_crn, Ic_edgV, Ic_edgH, I_edgV, I_edgH, Temp (updated in place).
+    solver: the sweep's cell solve (0 = SCB_BGEN + Gaussian elimination, the reference's form; 1 = the
+    closed form).  law 0: the reference's material (kapB_calc * kappa_mult, MEB_SOLVE); law 1: the
+    configurations' opacity law with kappa_mult = kappa0 and the T^4-linearised energy balance.
+    record: optional list; after every step a dict of the step's fg factors and corner state is appended.
     Returns one (Temp, HO_E_avg, outer iterations, T norm, E norm) tuple per step."""
     A = F(np.outer(Delx, Dely))
     nm = len(Omega_x)
-    KapE, src, _ = material_update(st["Temp"], Nu_g, kappa_mult, comp_unit)   # INITIALIZERS.f08:137
+    mat = material_update_law if law == 1 else material_update
+    KapE, src, _ = mat(st["Temp"], Nu_g, kappa_mult, comp_unit)   # INITIALIZERS.f08:137
     hist = []
     for _ in range(steps):
         Temp_old = st["Temp"].copy(order="F")
@@ -257,7 +287,7 @@ def tr_no_qd_steps(st, Omega_x, Omega_y, quad_weight, Delx, Dely, Nu_g, kappa_mu
             its += 1
             Src_in = F(np.repeat(np.repeat(src, 2, axis=0), 2, axis=1)[:, :, None, :].repeat(nm, axis=2))
             s = transport_scb(st["I_edgV"], st["I_edgH"], st["Ic_edgV"], st["Ic_edgH"], Omega_x, Omega_y, Delx, Dely,
-                              A, KapE, Src_in, I_crn_old, c, Delt, threads=threads, solver=1)
+                              A, KapE, Src_in, I_crn_old, c, Delt, threads=threads, solver=solver)
             for k in ("I_crn", "I_edgV", "I_edgH", "Ic_edgV", "Ic_edgH"):
                 st[k] = s[k]
             m = collapse_intensities(s["I_avg"], s["I_edgV"], s["I_edgH"], Omega_x, Omega_y, quad_weight, comp_unit,
@@ -266,14 +296,20 @@ def tr_no_qd_steps(st, Omega_x, Omega_y, quad_weight, Delx, Dely, Nu_g, kappa_mu
                 st["I_edgV"], st["I_edgH"], st["Ic_edgV"], st["Ic_edgH"] = rt_bc_update(
                     bc_type, bcT[0], bcT[1], bcT[2], bcT[3], comp_unit, Nu_g, st["I_edgV"], st["I_edgH"],
                     st["Ic_edgV"], st["Ic_edgH"])
-            st["Temp"] = meb_solve(Temp_old, m["Eg_avg"], KapE, Delt, cV, Kap0, comp_unit)
-            KapE, src, _ = material_update(st["Temp"], Nu_g, kappa_mult, comp_unit)
+            if law == 1:
+                st["Temp"] = meb_solve_law(st["Temp"], Temp_old, m["Eg_avg"], KapE, Delt, cV, Nu_g, comp_unit, c)
+            else:
+                st["Temp"] = meb_solve(Temp_old, m["Eg_avg"], KapE, Delt, cV, Kap0, comp_unit)
+            KapE, src, _ = mat(st["Temp"], Nu_g, kappa_mult, comp_unit)
             tc, tn, _ = convergence(conv_type, conv_ho, st["Temp"], T_rt1, T_rt2, its)
             ec, en, _ = convergence(conv_type, conv_ho, m["E_avg"], E_rt1, E_rt2, its)
             conv = tc and ec
             E_rt2, E_rt1 = E_rt1, m["E_avg"].copy(order="F")
             T_rt2, T_rt1 = T_rt1, st["Temp"].copy(order="F")
         hist.append((st["Temp"].copy(order="F"), m["E_avg"].copy(order="F"), its, tn, en))
+        if record is not None:
+            f = fg_calc(m, c, threads=threads)
+            record.append(dict(f, I_crn=st["I_crn"].copy(order="F"), Eg_avg=m["Eg_avg"].copy(order="F")))
     return hist
 
 

@@ -18,6 +18,9 @@
 //   kapB_calc                MainSrc/TEMP_FUNCTIONS.f08:11-32      -> oracle_kapb
 //   MATERIAL_UPDATE          MainSrc/UPDATES.f08:110-152           -> oracle_material_update
 //   MEB_SOLVE                MainSrc/UPDATES.f08:185-230           -> oracle_meb_solve
+//   (the configurations' opacity law and T^4-linearised energy balance, in place of kapB_calc and
+//    MEB_SOLVE)                                                  -> oracle_material_update_law,
+//                                                                   oracle_meb_solve_law
 //   CONVERGENCE              MainSrc/CONVERGENCE_CHECKS.f08:7-44   -> oracle_convergence
 //
 // Third-party arithmetic: the reference solves each 4x4 corner system with GAUSS_COMPLETE from the
@@ -789,6 +792,74 @@ int oracle_meb_solve(int nx, int ny, int ng, double* Temp, const double* Eg_HO, 
       kb = kb / E;
       const double coef = c2h3 / (((c2h3 * cV[c]) * Comp_Unit) + lin);
       Temp[c] = (coef * ((((Delt * kC) * kb) * E) + cV[c] * Temp_old[c])) * Comp_Unit;
+    }
+  return 0;
+}
+
+// ---- Material of the synthetic configurations (not the reference's material) ---------------------
+// The configurations replace kapB_calc with the opacity law
+//   kappa_g(T) = kappa0(i,j) (1 - exp(-nu_g/T)) / (nu_g^3 sqrt(T)),  nu_g = sqrt(Nu_g(g) Nu_g(g+1)),
+// T and nu in keV (Temp and Nu_g are passed in eV, as everywhere else), and the Fleck-Cummings
+// MEB_SOLVE with a backward-Euler energy balance per cell,
+//   cv (T - T_old)/Delt = sum_g KapE_g (c Eg - 4 pi Bg(T)),
+// whose emission is linearised about the current iterate T* (one Newton step per outer iteration):
+//   T = (cv T_old/Delt + sum_g KapE_g (c Eg - 4 pi Bg(T*) + 4 pi Bg'(T*) T*)) / (cv/Delt + 4 pi sum_g KapE_g Bg'(T*)).
+// MATERIAL_UPDATE (UPDATES.f08:130-150) is the template: KapE = KapB, src = KapB * Bg.
+double law_kappa(double Temp, double nu_low, double nu_high, double kappa0) {
+  const double nb = std::sqrt(nu_low * nu_high) * 1e-3;
+  const double tk = Temp * 1e-3;
+  return kappa0 * (-std::expm1(-nb / tk)) / (((nb * nb) * nb) * std::sqrt(tk));
+}
+
+// dBg/dT of Bg_planck_calc: Bg = 2 T^4 (sigint(nu_h/T) - sigint(nu_l/T)) / K, with the exact derivative
+// of the Planck integral, d sigint(z)/dz = z^3/(e^z - 1):
+//   dBg/dT = 2 T^3 (4 (sigint(z_h) - sigint(z_l)) - z_h^4/(e^z_h - 1) + z_l^4/(e^z_l - 1)) / K.
+double bg_planck_dT(double Tin, double nu_low, double nu_high, double comp_unit) {
+  if (Tin <= 1e-15) return 0.0;
+  const double zh = nu_high / Tin, zl = nu_low / Tin;
+  const double s = sigint(zh) - sigint(zl);
+  const double ph = zh > 700.0 ? 0.0 : (((zh * zh) * (zh * zh)) / std::expm1(zh));
+  const double pl = zl > 700.0 ? 0.0 : (((zl * zl) * (zl * zl)) / std::expm1(zl));
+  const double h3 = (kH * kH) * kH, c2 = kC * kC, e2 = kErg * kErg;
+  const double K = ((h3 * c2) * (e2 * e2)) * comp_unit;
+  const double t3 = (Tin * Tin) * Tin;
+  return ((2.0 * t3) * (((4.0 * s) - ph) + pl)) / K;
+}
+
+int oracle_material_update_law(int nx, int ny, int ng, const double* Temp, const double* Nu_g, const double* kappa0,
+                               double Comp_Unit, double* KapE, double* src, double* Bg) {
+  for (int g = 0; g < ng; ++g)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const size_t c = (size_t)i + (size_t)nx * j, k = c + (size_t)nx * ny * g;
+        const double B = bg_planck(Temp[c], Nu_g[g], Nu_g[g + 1], Comp_Unit);
+        const double kB = law_kappa(Temp[c], Nu_g[g], Nu_g[g + 1], kappa0[c]);
+        if (Bg) Bg[k] = B;
+        KapE[k] = kB;
+        src[k] = kB * B;
+      }
+  return 0;
+}
+
+// Temp holds the current iterate T* on entry and the new temperature on return.
+int oracle_meb_solve_law(int nx, int ny, int ng, double* Temp, const double* Eg_HO, const double* KapE,
+                         const double* Temp_old, double Delt, const double* cV, const double* Nu_g, double Comp_Unit,
+                         double c) {
+  const double fp = 4.0 * (4.0 * std::atan(1.0));
+  const size_t nxy = (size_t)nx * ny;
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const size_t k = (size_t)i + (size_t)nx * j;
+      const double ts = Temp[k];
+      double num = (cV[k] * Temp_old[k]) / Delt, den = cV[k] / Delt;
+      for (int g = 0; g < ng; ++g) {
+        const double kap = KapE[k + nxy * g];
+        const double B = bg_planck(ts, Nu_g[g], Nu_g[g + 1], Comp_Unit);
+        const double dB = bg_planck_dT(ts, Nu_g[g], Nu_g[g + 1], Comp_Unit);
+        num = num + kap * (((c * Eg_HO[k + nxy * g]) - (fp * B)) + ((fp * dB) * ts));
+        den = den + (fp * kap) * dB;
+      }
+      Temp[k] = num / den;
     }
   return 0;
 }

@@ -453,3 +453,82 @@ def test_register_variant_does_not_change_results(precision):
     assert np.array_equal(out[0][1], out[1][1])
     for k in out[0][2]:
         assert np.array_equal(out[0][2][k], out[1][2][k]), k
+
+
+@pytest.mark.parametrize("name,make", SHAPES[:5], ids=[s[0] for s in SHAPES[:5]])
+def test_resident_sweep_matches_gaussian_elimination_oracle(oracle, name, make):
+    """The resident sweep with the isotropic per-cell source (the kernel the benchmark times) against the
+    oracle's SCB_BGEN + Gaussian-elimination form (solver 0), which shares no code with the library:
+    corner state, group energies and QD/boundary factors within 1e-12."""
+    d = sweep_inputs(make(), seed=13)
+    r0 = oracle_full(d, solver=0)
+    with resident(d) as s:
+        s.sweep(moments=True)
+        I = s.get_state()
+        m = s.moments()
+    assert rel_err_per_group(I, r0["I_crn"]) <= 1e-12
+    for k in ("Eg_avg", "Eg_edgV", "Eg_edgH"):
+        assert rel_err_per_group(m[k], r0[k]) <= 1e-12, k
+    for k in FG_KEYS + ("Cg_L", "Cg_B", "Cg_R", "Cg_T"):
+        assert np.max(np.abs(m[k] - r0[k])) <= 1e-12, k
+
+
+def _c1_group_inputs(prob, sel, T):
+    """Reference-layout sweep inputs of config C1 restricted to the groups `sel`, in the state the
+    benchmark's handle starts from (trt_init_state: every corner at Bg(T0), Planck inflow on the left)
+    and with the material at temperature field T."""
+    from oracle import oracle as O
+    ox, oy, w = prob.directions()
+    nx, ny, nm = prob.nx, prob.ny, len(ox)
+    kap, src = prob.material(T)
+    nu = prob.nu_eV
+    ns = len(sel)
+    Bg0 = np.array([pkg.problems.bg_planck(prob.T0 * 1e3, nu[g], nu[g + 1]) for g in sel])
+    I_old = np.asfortranarray(np.broadcast_to(Bg0, (2 * nx, 2 * ny, nm, ns)).copy())
+    src_s = np.asfortranarray(src[:, :, sel])
+    Src_in = np.asfortranarray(np.repeat(np.repeat(src_s, 2, axis=0), 2, axis=1)[:, :, None, :].repeat(nm, axis=2))
+    faces = [np.zeros((nx + 1, 2 * ny, nm, ns), order="F"), np.zeros((2 * nx, ny + 1, nm, ns), order="F"),
+             np.zeros((nx + 1, ny, nm, ns), order="F"), np.zeros((nx, ny + 1, nm, ns), order="F")]
+    bT = [t * 1e3 for t in prob.bcT]
+    for k, g in enumerate(sel):   # RT_INIT's boundary update, one group at a time (edges g, g+1)
+        b = Bg0[k]
+        IcV = np.full((nx + 1, 2 * ny, nm, 1), b, order="F")
+        IcH = np.full((2 * nx, ny + 1, nm, 1), b, order="F")
+        IV = np.full((nx + 1, ny, nm, 1), b, order="F")
+        IH = np.full((nx, ny + 1, nm, 1), b, order="F")
+        IV, IH, IcV, IcH = O.rt_bc_update((0, 0, 0, 0), bT[0], bT[1], bT[2], bT[3], CU, nu[g:g + 2], IV, IH, IcV, IcH)
+        for f, v in zip(faces, (IcV, IcH, IV, IH)):
+            f[..., k] = v[..., 0]
+    return dict(Omega_x=ox, Omega_y=oy, w=w, Delx=prob.delx, Dely=prob.dely, A=np.asfortranarray(np.outer(prob.delx,
+                prob.dely)), KapE_in=np.asfortranarray(kap[:, :, sel]), src_iso=src_s, Src_in=Src_in, I_crn_old=I_old,
+                Ic_edgV=faces[0], Ic_edgH=faces[1], I_edgV=faces[2], I_edgH=faces[3], c=C, dt=prob.dt)
+
+
+def test_c1_full_size_sweep_matches_gaussian_elimination_oracle(oracle):
+    """Config C1 at full size (256x256 cells, 50 groups, S16) through the resident handle with the
+    benchmark's set-up (initial state, material at the benchmark's temperature field): the group
+    energies, QD factors and boundary factors of 8 groups spread over the group range (opacities from
+    optically thin to thick) against the oracle's Gaussian-elimination sweep of those groups, within
+    1e-12."""
+    prob = pkg.problems.config1()
+    ox, oy, w = prob.directions()
+    x = (np.arange(prob.nx) + 0.5) / prob.nx
+    T = np.asfortranarray(np.broadcast_to((prob.T0 + 0.5 * np.exp(-8 * x))[:, None], (prob.nx, prob.ny)))
+    kap, src = prob.material(T)
+    s = pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng, precision="fp64")
+    try:
+        s.init_state(prob.T0 * 1e3, [t * 1e3 for t in prob.bcT], CU, prob.nu_eV)
+        s.set_material(kap, src, C, prob.dt, CU)
+        s.sweep(roll=True, moments=True)
+        m = s.moments(("Eg_avg", "Eg_edgV", "Eg_edgH") + FG_KEYS + ("Cg_L", "Cg_B", "Cg_R", "Cg_T"))
+    finally:
+        s.close()
+    sel = [int(g) for g in np.linspace(0, prob.ng - 1, 8).round()]
+    for chunk in (sel[0:2], sel[2:4], sel[4:6], sel[6:8]):
+        d = _c1_group_inputs(prob, chunk, T)
+        r0 = oracle_full(d, solver=0, threads=2)
+        for k in ("Eg_avg", "Eg_edgV", "Eg_edgH"):
+            assert rel_err_per_group(m[k][..., chunk], r0[k]) <= 1e-12, (k, chunk)
+        for k in FG_KEYS + ("Cg_L", "Cg_B", "Cg_R", "Cg_T"):
+            assert np.max(np.abs(m[k][..., chunk] - r0[k])) <= 1e-12, (k, chunk)
+        del d, r0
