@@ -124,6 +124,8 @@ SIGNATURES = {
     "trt_set_wait_limit_zero": (_i, [_P]),
     "trt_device_output": (_P, [_P, ctypes.c_char_p]),
     "trt_set_register_mode": (_i, [_P, _i]),
+    "trt_set_bands": (_i, [_P, _i]),
+    "trt_get_bands": (_i, [_P]),
     "trt_get_register_mode": (_i, [_P]),
     "trt_autotune": (_i, [_P, _I, _I, _I, ctypes.POINTER(ctypes.c_float)]),
     "trt_batch_create": (_P, [ctypes.POINTER(_P), _i, _I]),

@@ -616,6 +616,11 @@ class TransportSweep:
               "trt_autotune")
         return dict(self.tiling(), sweep_ms=ms.value)
 
+    def set_bands(self, bands):
+        """Band CTAs per (group, quadrant, split) sweep (spatial row tiles on a tile-diagonal wavefront,
+        one thread-block cluster each); 0/1 = one CTA per sweep.  Re-lays out (zeroes) the state."""
+        check(_lib.lib().trt_set_bands(self._h, int(bands)), "trt_set_bands")
+
     def set_register_mode(self, mode):
         """Cap the sweep kernel's register level (0: <= 128, 1: <= 170, 2: <= 255 registers per thread);
         -1 = the highest level that keeps the whole grid resident.  Re-lays out (zeroes) the state."""
@@ -626,6 +631,7 @@ class TransportSweep:
         check(_lib.lib().trt_get_tiling(self._h, *[ctypes.byref(x) for x in v]), "trt_get_tiling")
         out = dict(zip(("warps", "slices", "dirs_per_lane", "stages", "splits"), [x.value for x in v]))
         out["wide_registers"] = int(_lib.lib().trt_get_register_mode(self._h))
+        out["bands"] = int(_lib.lib().trt_get_bands(self._h))
         return out
 
     def set_material(self, KapE_in, src_iso, c, Delt, Comp_Unit):

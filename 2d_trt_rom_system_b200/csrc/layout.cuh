@@ -21,6 +21,15 @@
 // a cell's left inflow comes from the same lane one step earlier, its bottom inflow from the row
 // below one step earlier.
 //
+// Spatial tiles.  With NB > 1 the rounds of one (g, q, h) sweep are dealt round-robin to NB CTAs
+// (one thread-block cluster): CTA b sweeps rounds n = b, b + NB, b + 2 NB, ... one after the other
+// (local round k = n / NB starts at local step k*P), and round n's first row takes its bottom inflow
+// from round n-1's top outflow, written by the neighbouring CTA of the cluster into the L2-resident
+// wrap buffer.  The CTAs run as a pipeline of row tiles on a tile-diagonal wavefront, each about H
+// steps behind the one below.  Every step index below is local to a CTA: cell (i', j') of round n
+// sits at step T = (n % NB) * Tb + (n / NB) * P + i' + rho of its (g, q, h) block, where Tb (steps
+// per band) is the local step count of the band with the most rounds.
+//
 // Skewed state layout.  For each (g, q, h) a block of Tsteps*W chunks; chunk (T, w) holds the cells
 // the lanes of warp w touch at step T, as D sub-blocks (one per d) of nl_d lanes
 // (nl_d = R*min(S, mqc - d*S), mqc = ceil(mq/NH)); a lane's 4 corners are stored as 16-byte vectors ("pairs" for
@@ -50,12 +59,14 @@ struct Tiling {
   int H;       // rows per round = W * R
   int P;       // period = max(nx, H + 1)
   int nr;      // rounds = ceil(ny / H)
-  int Tsteps;  // steps of one (g, q) sweep = (nr-1)*P + nx + H - 1
+  int NB;      // band CTAs per (g, q, h) sweep (rounds dealt round-robin); 1 = one CTA sweeps every round
+  int Tb;      // local steps of a band CTA with the most rounds = (ceil(nr/NB)-1)*P + nx + H - 1
+  int Tsteps;  // steps of one (g, q, h) block = NB * Tb
 };
 
 TRT_LHD int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
-TRT_LHD Tiling make_tiling(int nx, int ny, int mq, int W, int S, int NH) {
+TRT_LHD Tiling make_tiling(int nx, int ny, int mq, int W, int S, int NH, int NB = 1) {
   Tiling t;
   t.W = W;
   t.S = S;
@@ -66,9 +77,15 @@ TRT_LHD Tiling make_tiling(int nx, int ny, int mq, int W, int S, int NH) {
   t.H = W * t.R;
   t.P = nx > t.H ? nx : t.H + 1;   // P > H: a round's wrap entry is written a step before it is prefetched
   t.nr = ceil_div(ny, t.H);
-  t.Tsteps = (t.nr - 1) * t.P + nx + t.H - 1;
+  t.NB = NB < 1 ? 1 : (NB > t.nr ? t.nr : NB);
+  t.Tb = (ceil_div(t.nr, t.NB) - 1) * t.P + nx + t.H - 1;
+  t.Tsteps = t.NB * t.Tb;
   return t;
 }
+
+// Rounds of band b (n = b, b + NB, ...) and its local step count.
+TRT_LHD int band_rounds(const Tiling& t, int b) { return ceil_div(t.nr - b, t.NB); }
+TRT_LHD int band_steps(const Tiling& t, int nx, int b) { return (band_rounds(t, b) - 1) * t.P + nx + t.H - 1; }
 
 // Direction split h of a quadrant: first quadrant-local direction and count (floor/ceil(mq/NH)).
 TRT_LHD int split_first(int mq, int NH, int h) { return h * (mq / NH) + (h < mq % NH ? h : mq % NH); }
@@ -104,7 +121,7 @@ TRT_LHD SweepPos sweep_pos(int nx, int ny, const Tiling& t, int q, int i, int j)
   const int jp = fy ? ny - 1 - j : j;
   const int n = jp / t.H, rho = jp % t.H;
   SweepPos p;
-  p.T = n * t.P + ip + rho;
+  p.T = (n % t.NB) * t.Tb + (n / t.NB) * t.P + ip + rho;
   p.w = rho / t.R;
   p.r = rho % t.R;
   return p;

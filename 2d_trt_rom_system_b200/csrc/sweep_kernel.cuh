@@ -72,13 +72,16 @@ struct SweepArgs {
 
 constexpr int kErrTmaTimeout = 1;
 
+// Dynamic shared memory of one sweep CTA: the TMA ring, its mbarriers, the row handoff, the direction
+// table and the moment-weight table (FP32 sweep: float2 pairs of direction slots, 6 rows).
 template <class Real>
-__host__ __device__ inline size_t sweep_smem_bytes(int W, long long chunk, int stages, int mqc, int D) {
+__host__ __device__ inline size_t sweep_smem_bytes(int W, long long chunk, int stages, int mqc, int D, int S) {
+  (void)mqc;
   size_t ring = (size_t)stages * W * chunk * sizeof(Real);
   size_t bars = (size_t)stages * sizeof(uint64_t);
   size_t hand = (size_t)2 * W * mqc * 2 * sizeof(Real);
   size_t dtab = (size_t)kNDirRow * mqc * sizeof(Real);
-  size_t wtab = (size_t)6 * mqc * sizeof(double) + 16;
+  size_t wtab = (size_t)6 * ((D + 1) / 2) * S * sizeof(float2) + 16;
   return ring + bars + hand + dtab + wtab + 32;
 }
 
@@ -138,7 +141,12 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
   const Tiling t = a.t;
   const int W = t.W;
   const int nx = a.nx, ny = a.ny, nm = a.nm, ng = a.ng, mq = a.mq;
-  const int h = bid % t.NH, g = (bid / t.NH) >> 2, q = (bid / t.NH) & 3;
+  // band CTAs of one (g, q, h) sweep are consecutive blocks (one cluster); band = rank in the cluster
+  const int NB = t.NB;
+  const int band = NB > 1 ? bid % NB : 0;
+  const int gqh = NB > 1 ? bid / NB : bid;
+  const int prod = (band + NB - 1) % NB;   // the band CTA that sweeps the round below each of ours
+  const int h = gqh % t.NH, g = (gqh / t.NH) >> 2, q = (gqh / t.NH) & 3;
   const int mqc = t.mqc;                           // chunk width (directions of the largest split)
   const int mo = split_first(mq, t.NH, h);         // first quadrant-local direction of this split
   const int mq_h = split_count(mq, t.NH, h);       // directions of this split
@@ -158,7 +166,10 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + (size_t)stages * stage_bytes);
   Real* hand = reinterpret_cast<Real*>(mbar + stages);
   Real* dtab = hand + 2 * W * mqc * 2;
-  double* wtab = reinterpret_cast<double*>(
+  // FP32 moment weights w, w Ox^2, w Oy^2, w Ox Oy, w Ox, w Oy as float2 pairs: row k, pair p, slice s holds
+  // the weights of the lane's direction slots 2p (.x) and 2p+1 (.y); slots without a direction hold 0
+  constexpr int NP = (D + 1) / 2;
+  float2* wt2 = reinterpret_cast<float2*>(
       (reinterpret_cast<uintptr_t>(dtab + kNDirRow * mqc) + 15) & ~static_cast<uintptr_t>(15));
 
   // direction table of this split: row k of split-local direction ml at dtab[k * mqc + ml]
@@ -168,23 +179,33 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
     if (row < 2) v = v * Real(0.25);   // |Omega| / 4 for the corner-matrix geometry
     dtab[k] = v;
   }
-  // moment weights w, w Ox^2, w Oy^2, w Ox Oy, w Ox, w Oy of the split's directions, FP64
   if constexpr (kLeanFP32) {
-    for (int k = threadIdx.x; k < 6 * mqc; k += blockDim.x) {
-      const int row = k / mqc, col = k % mqc;
-      wtab[k] = col < mq_h ? a.dir64[(size_t)(kW + row) * nm + q * mq + mo + col] : 0.0;
+    for (int k = threadIdx.x; k < 6 * NP * S; k += blockDim.x) {
+      const int row = k / (NP * S), p = (k / S) % NP, sl = k % S;
+      const int m0 = (2 * p) * S + sl, m1 = (2 * p + 1) * S + sl;   // split-local directions of the two slots
+      const double* wr = a.dir64 + (size_t)(kW + row) * nm + q * mq + mo;
+      wt2[k] = make_float2(2 * p < D && m0 < mq_h ? (float)wr[m0] : 0.0f,
+                           2 * p + 1 < D && m1 < mq_h ? (float)wr[m1] : 0.0f);
     }
   }
   if (threadIdx.x == 0) {
     for (int k = 0; k < stages; ++k) mbar_init(&mbar[k], 1);
     fence_mbar_init();
   }
+  // Band handoff (NB > 1): band_prog holds the local steps the producer band has completed; the producer
+  // writes it into this CTA's shared memory with a cluster-scope release after each step that the
+  // rounds above it still need (publication stops once the last of those steps is out, so no CTA writes
+  // into a CTA that may have left).  Every CTA initialises its slot before any CTA publishes.
+  __shared__ int band_prog;
+  if (NB > 1 && threadIdx.x == 0) band_prog = 0;
   __syncthreads();
+  if (NB > 1) cluster_sync_all();
 
-  const long long blk_off = (long long)bid * a.blk;
+  // this band's steps inside the (g, q, h) block of the skewed state
+  const long long blk_off = (long long)gqh * a.blk + (long long)band * t.Tb * W * chunk;
   const Real* gold = a.Iold + blk_off;
   Real* gnew = a.Inew + blk_off;
-  const int Tsteps = t.Tsteps;
+  const int Tsteps = band_steps(t, nx, band);
 
   if (threadIdx.x == 0) {
     for (int k = 0; k < stages && k < Tsteps; ++k) {
@@ -195,7 +216,7 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
 
   const Real rcdt = a.rcdt;
   const int nxy = nx * ny;
-  Real* wrapc = a.wrap + (size_t)bid * nx * mqc * 2;
+  Real* wrapc = a.wrap + (size_t)gqh * nx * mqc * 2;
   constexpr int kRec = part_rec<Real>();
   Real* partg = a.part + ((size_t)((q * t.NH + h) * ng + g) * nxy) * kRec;
   const int sideVin = fx ? 1 : 0, sideVout = fx ? 0 : 1;
@@ -214,7 +235,37 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
   for (int d = 0; d < D; ++d) vb[d] = vt[d] = hl[d] = hr[d] = Real(0);
 
   // lane position: column ip of round n (ip < 0 before the lane starts); advanced incrementally
-  int ip = -rho, n = 0;
+  int ip = -rho, n = band;
+  bool timed_out = false;
+  // Producer side: publish after every local step up to the end of the last round that has a round
+  // above it (round band + ks*NB <= nr - 2, its top row done with column nx-1).
+  const int ks = (t.nr - 2 - band) >= 0 ? (t.nr - 2 - band) / NB : -1;
+  const int pub_stop = ks >= 0 ? ks * t.P + nx + t.H - 1 : 0;
+  const uint32_t prog_remote = NB > 1 ? cluster_map(&band_prog, (uint32_t)((band + 1) % NB)) : 0u;
+  // Consumer side (warp 0, whose first row reads the wrap buffer): before the first row of round nn > 0
+  // takes the bottom inflow of column ipn, the producer must have finished that column in round nn - 1
+  // (its local round (nn-1-prod)/NB), i.e. completed local step k'P + ipn + H - 1.  Bounded wait: false
+  // when the producer did not get there within max_polls polls.
+  int seen = 0;
+  auto band_wait = [&](int ipn, int nn) -> bool {
+    if (NB == 1 || nn <= 0 || nn >= t.nr || ipn < 0 || ipn >= nx) return true;
+    const int need = ((nn - 1 - prod) / NB) * t.P + ipn + t.H;
+    int ok = 1;
+    if (lane == 0 && seen < need) {
+      for (unsigned k = 0;; ++k) {
+        seen = ld_acquire_cluster(&band_prog);
+        if (seen >= need) break;
+        if (k >= a.max_polls) {
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    return ok != 0;
+  };
   // material of the lane's cell at the current step, loaded one step ahead
   Real mdx = Real(0), mdy = Real(0), mA4 = Real(0), mkp = Real(0), mqs = Real(0);
   auto load_material = [&](int ipn, int nn) {
@@ -259,18 +310,18 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
           if (nn == 0) {
             hl[d] = bHin[ml * 2 * nx + 2 * in + bxo];
             hr[d] = bHin[ml * 2 * nx + 2 * in + 1 - bxo];
-          } else {
-            hl[d] = wrapc[(ipn * mqc + ml) * 2 + 0];
-            hr[d] = wrapc[(ipn * mqc + ml) * 2 + 1];
+          } else {   // written by another band CTA (or this one): read through L2
+            hl[d] = __ldcg(wrapc + (ipn * mqc + ml) * 2 + 0);
+            hr[d] = __ldcg(wrapc + (ipn * mqc + ml) * 2 + 1);
           }
         }
       }
     }
   };
   load_material(ip, n);
+  if (warp == 0 && !band_wait(ip, n)) timed_out = true;
   if (kLeanFP32) load_inflow(ip, n);
 
-  bool timed_out = false;
   int stage = 0;
   uint32_t phase = 0;
   int T_break = Tsteps;
@@ -311,25 +362,24 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
           for (int d = 0; d < D; ++d) {
             const int ml = d * S + s;
             if (d < D - 1 || s < s_last) {
-              const Real* src;
-              int o0, o1;
-              if (rho == 0) {
-                if (n == 0) {
+              if (rho == 0 && n > 0) {   // wrap buffer, possibly written by another band CTA: through L2
+                hl[d] = __ldcg(wrapc + (ip * mqc + ml) * 2);
+                hr[d] = __ldcg(wrapc + (ip * mqc + ml) * 2 + 1);
+              } else {
+                const Real* src;
+                int o0, o1;
+                if (rho == 0) {
                   src = bHin + ml * 2 * nx + 2 * i;
                   o0 = bxo;
                   o1 = 1 - bxo;
                 } else {
-                  src = wrapc + (ip * mqc + ml) * 2;
+                  src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mqc + ml) * 2;
                   o0 = 0;
                   o1 = 1;
                 }
-              } else {
-                src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mqc + ml) * 2;
-                o0 = 0;
-                o1 = 1;
+                hl[d] = src[o0];
+                hr[d] = src[o1];
               }
-              hl[d] = src[o0];
-              hr[d] = src[o1];
             }
           }
         }
@@ -443,35 +493,6 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
       j = fy ? ny - 1 - jp : jp;
       const Real dx = mdx, dy = mdy, A4 = mA4, kp = mkp, qs = mqs;
 
-      if (!kLeanFP32 && active) {
-        // global-memory inflows: the sweep-left boundary face at the start of a round, and for the
-        // CTA's first row the sweep-bottom boundary face (round 0) or the wrap buffer
-        if (ip == 0) {
-  #pragma unroll
-          for (int d = 0; d < D; ++d) {
-            const int ml = d * S + s;
-            if (d < D - 1 || s < s_last) {
-              vb[d] = bVin[ml * 2 * ny + 2 * j + byo];
-              vt[d] = bVin[ml * 2 * ny + 2 * j + 1 - byo];
-            }
-          }
-        }
-        if (rho == 0) {
-  #pragma unroll
-          for (int d = 0; d < D; ++d) {
-            const int ml = d * S + s;
-            if (d < D - 1 || s < s_last) {
-              if (n == 0) {
-                hl[d] = bHin[ml * 2 * nx + 2 * i + bxo];
-                hr[d] = bHin[ml * 2 * nx + 2 * i + 1 - bxo];
-              } else {
-                hl[d] = wrapc[(ip * mqc + ml) * 2 + 0];
-                hr[d] = wrapc[(ip * mqc + ml) * 2 + 1];
-              }
-            }
-          }
-        }
-      }
       // bottom inflow of a warp's first row from the warp below (shared memory, written last step)
       if (active && r == 0 && warp > 0) {
   #pragma unroll
@@ -490,31 +511,65 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
       const bool last_row = active && (r == R - 1) && (warp < W - 1 || t.nr > 1);
       Real* hand_dst = (warp < W - 1) ? hand + ((T & 1) * W + warp) * mqc * 2 : wrapc + ip * mqc * 2;
 
+      // FP32 moment lane sums: acc2[v].x sums the lane's even direction slots, .y its odd ones (at most
+      // ceil(D/2) terms each, one FP32 rounding per fused multiply-add); the two are added in FP64 at the
+      // end of the step, before the slice reduction, so each lane sum carries a relative error of at most
+      // ceil(D/2) units of FP32 rounding.
+      float2 acc2[13];
   #pragma unroll
-      for (int v = 0; v < 13; ++v) acc[v] = 0.0;
+      for (int v = 0; v < 13; ++v) acc2[v] = make_float2(0.0f, 0.0f);
       Real topL[kLeanFP32 ? 1 : D], topR[kLeanFP32 ? 1 : D];
       const Real kA4 = scb_kA4(dx, dy, kp);
 
-      // FP32 moment products of one direction slot (FP64 lane sums)
-      auto add_moments = [&](int ml, Real x0, Real x1, Real x2, Real x3) {
-        const double Iavg = (double)(((x0 + x1) + (x2 + x3)) * Real(0.25));
-        const double Iv = (double)((x1 + x2) * Real(0.5));
-        const double Ih = (double)((x3 + x2) * Real(0.5));
-        const double ww = wtab[0 * mqc + ml], wxx = wtab[1 * mqc + ml], wyy = wtab[2 * mqc + ml];
-        const double wxy = wtab[3 * mqc + ml], wx = wtab[4 * mqc + ml], wy = wtab[5 * mqc + ml];
-        acc[kCxx] = fma(wxx, Iavg, acc[kCxx]);
-        acc[kCyy] = fma(wyy, Iavg, acc[kCyy]);
-        acc[kCxy] = fma(wxy, Iavg, acc[kCxy]);
-        acc[kCe] = fma(ww, Iavg, acc[kCe]);
-        acc[kVxx] = fma(wxx, Iv, acc[kVxx]);
-        acc[kVxy] = fma(wxy, Iv, acc[kVxy]);
-        acc[kVx] = fma(wx, Iv, acc[kVx]);
-        acc[kVe] = fma(ww, Iv, acc[kVe]);
-        acc[kHyy] = fma(wyy, Ih, acc[kHyy]);
-        acc[kHxy] = fma(wxy, Ih, acc[kHxy]);
-        acc[kHy] = fma(wy, Ih, acc[kHy]);
-        acc[kHx] = fma(wx, Ih, acc[kHx]);
-        acc[kHe] = fma(ww, Ih, acc[kHe]);
+      // moment products of the direction slots 2p (.x) and 2p+1 (.y) of the lane, packed FP32x2
+      auto add_moments2 = [&](int p, float2 x0, float2 x1, float2 x2, float2 x3) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+        const float2 Iavg = __fmul2_rn(__fadd2_rn(__fadd2_rn(x0, x1), __fadd2_rn(x2, x3)), f2(0.25f));
+        const float2 Iv = __fmul2_rn(__fadd2_rn(x1, x2), f2(0.5f));
+        const float2 Ih = __fmul2_rn(__fadd2_rn(x3, x2), f2(0.5f));
+        const float2* wp = wt2 + p * S + s;
+        const float2 ww = wp[0 * NP * S], wxx = wp[1 * NP * S], wyy = wp[2 * NP * S];
+        const float2 wxy = wp[3 * NP * S], wx = wp[4 * NP * S], wy = wp[5 * NP * S];
+        acc2[kCxx] = __ffma2_rn(wxx, Iavg, acc2[kCxx]);
+        acc2[kCyy] = __ffma2_rn(wyy, Iavg, acc2[kCyy]);
+        acc2[kCxy] = __ffma2_rn(wxy, Iavg, acc2[kCxy]);
+        acc2[kCe] = __ffma2_rn(ww, Iavg, acc2[kCe]);
+        acc2[kVxx] = __ffma2_rn(wxx, Iv, acc2[kVxx]);
+        acc2[kVxy] = __ffma2_rn(wxy, Iv, acc2[kVxy]);
+        acc2[kVx] = __ffma2_rn(wx, Iv, acc2[kVx]);
+        acc2[kVe] = __ffma2_rn(ww, Iv, acc2[kVe]);
+        acc2[kHyy] = __ffma2_rn(wyy, Ih, acc2[kHyy]);
+        acc2[kHxy] = __ffma2_rn(wxy, Ih, acc2[kHxy]);
+        acc2[kHy] = __ffma2_rn(wy, Ih, acc2[kHy]);
+        acc2[kHx] = __ffma2_rn(wx, Ih, acc2[kHx]);
+        acc2[kHe] = __ffma2_rn(ww, Ih, acc2[kHe]);
+#endif
+      };
+      // moment products of one direction slot d (component d & 1 of pair d / 2)
+      auto add_moments = [&](int d, float x0, float x1, float x2, float x3) {
+        const float Iavg = ((x0 + x1) + (x2 + x3)) * 0.25f;
+        const float Iv = (x1 + x2) * 0.5f;
+        const float Ih = (x3 + x2) * 0.5f;
+        const float2* wp = wt2 + (d / 2) * S + s;
+        const bool hi = (d & 1) != 0;
+        auto w = [&](int row) { const float2 v = wp[row * NP * S]; return hi ? v.y : v.x; };
+        auto acc = [&](int k, float wv, float I) {
+          if (hi) acc2[k].y = fmaf(wv, I, acc2[k].y);
+          else acc2[k].x = fmaf(wv, I, acc2[k].x);
+        };
+        acc(kCxx, w(1), Iavg);
+        acc(kCyy, w(2), Iavg);
+        acc(kCxy, w(3), Iavg);
+        acc(kCe, w(0), Iavg);
+        acc(kVxx, w(1), Iv);
+        acc(kVxy, w(3), Iv);
+        acc(kVx, w(4), Iv);
+        acc(kVe, w(0), Iv);
+        acc(kHyy, w(2), Ih);
+        acc(kHxy, w(3), Ih);
+        acc(kHy, w(5), Ih);
+        acc(kHx, w(4), Ih);
+        acc(kHe, w(0), Ih);
       };
       // FP32 outputs of one live direction slot: corner state, outflow boundary faces, row handoff
       auto store_slot = [&](int d, int ml, Real x0, Real x1, Real x2, Real x3) {
@@ -572,19 +627,20 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
         hl[d + 1] = __shfl_up_sync(0xffffffffu, x[3].y, 1);
         hr[d] = __shfl_up_sync(0xffffffffu, x[2].x, 1);
         hr[d + 1] = __shfl_up_sync(0xffffffffu, x[2].y, 1);
-        if (active) {
-          store_slot(d, ml0, x[0].x, x[1].x, x[2].x, x[3].x);
-          add_moments(ml0, x[0].x, x[1].x, x[2].x, x[3].x);
-        }
-        if (live1) {
-          store_slot(d + 1, ml1, x[0].y, x[1].y, x[2].y, x[3].y);
-          add_moments(ml1, x[0].y, x[1].y, x[2].y, x[3].y);
-        }
+        if (active) store_slot(d, ml0, x[0].x, x[1].x, x[2].x, x[3].x);
+        if (live1) store_slot(d + 1, ml1, x[0].y, x[1].y, x[2].y, x[3].y);
+        if (live1) add_moments2(d / 2, x[0], x[1], x[2], x[3]);
+        else if (active) add_moments(d, x[0].x, x[1].x, x[2].x, x[3].x);
       };
 #endif
 
+      // a warp none of whose lanes has a cell at this step (wavefront fill and drain) skips the solve:
+      // a row that starts at the next step takes its inflows from the boundary, the wrap buffer or the
+      // handoff, never from the shuffles of this step
+      const bool warp_live = __any_sync(0xffffffffu, active);
   #pragma unroll
       for (int d = 0; d < D; ++d) {
+        if (!warp_live) break;
 #if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
         if constexpr (kLeanFP32) {
           if (d % 2 == 0 && d + 1 < D) {
@@ -660,24 +716,7 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
               hand_dst[ml * 2 + 1] = x[2];
             }
           }
-          const double Iavg = (double)(((x[0] + x[1]) + (x[2] + x[3])) * Real(0.25));
-          const double Iv = (double)((x[1] + x[2]) * Real(0.5));
-          const double Ih = (double)((x[3] + x[2]) * Real(0.5));
-          const double ww = wtab[0 * mqc + ml], wxx = wtab[1 * mqc + ml], wyy = wtab[2 * mqc + ml];
-          const double wxy = wtab[3 * mqc + ml], wx = wtab[4 * mqc + ml], wy = wtab[5 * mqc + ml];
-          acc[kCxx] = fma(wxx, Iavg, acc[kCxx]);
-          acc[kCyy] = fma(wyy, Iavg, acc[kCyy]);
-          acc[kCxy] = fma(wxy, Iavg, acc[kCxy]);
-          acc[kCe] = fma(ww, Iavg, acc[kCe]);
-          acc[kVxx] = fma(wxx, Iv, acc[kVxx]);
-          acc[kVxy] = fma(wxy, Iv, acc[kVxy]);
-          acc[kVx] = fma(wx, Iv, acc[kVx]);
-          acc[kVe] = fma(ww, Iv, acc[kVe]);
-          acc[kHyy] = fma(wyy, Ih, acc[kHyy]);
-          acc[kHxy] = fma(wxy, Ih, acc[kHxy]);
-          acc[kHy] = fma(wy, Ih, acc[kHy]);
-          acc[kHx] = fma(wx, Ih, acc[kHx]);
-          acc[kHe] = fma(ww, Ih, acc[kHe]);
+          add_moments(d, (float)x[0], (float)x[1], (float)x[2], (float)x[3]);
         }
       }
 
@@ -710,7 +749,8 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
           hr[d] = __shfl_up_sync(0xffffffffu, topR[kLeanFP32 ? 0 : d], 1);
         }
       }
-
+  #pragma unroll
+      for (int v = 0; v < 13; ++v) acc[v] = (double)acc2[v].x + (double)acc2[v].y;
     }
 
     // moments: reduce-scatter over the S slices of each row, then each lane writes its slots
@@ -750,9 +790,10 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
     ++ip;
     if (ip == t.P) {
       ip = 0;
-      ++n;
+      n += NB;
     }
     load_material(ip, n);
+    if (warp == 0 && !band_wait(ip, n)) timed_out = true;
     if (kLeanFP32) load_inflow(ip, n);
 
     const int any_timeout = __syncthreads_or(timed_out ? 1 : 0);
@@ -761,6 +802,8 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
       T_break = T;
       break;
     }
+    // the step's wrap-buffer writes (top rows, before the barrier) go out with the progress count
+    if (NB > 1 && threadIdx.x == 0 && T + 1 <= pub_stop) st_release_cluster(prog_remote, T + 1);
     if (threadIdx.x == 0 && T + stages < Tsteps) {
       mbar_arrive_expect_tx(&mbar[stage], stage_bytes);
       tma_bulk_g2s(ring + (size_t)stage * W * chunk, gold + (long long)(T + stages) * W * chunk, stage_bytes,
@@ -782,6 +825,8 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
     }
     __syncthreads();
   }
+  // no band CTA leaves while another may still write into its shared memory
+  if (NB > 1) cluster_sync_all();
 }
 
 // MAXT/MINB: 512/1 fits every tiling (at most 128 registers per thread); 128/3 and 128/2 are the

@@ -188,14 +188,36 @@ SweepBatchKernel<Real> sweep_batch_kernel_for(const KernelCfg& kc, bool src_full
   return nullptr;
 }
 
+// Launch a sweep kernel; with NB band CTAs per (group, quadrant, split) sweep, every NB consecutive CTAs
+// form one thread-block cluster (co-scheduled, so a band never waits for a CTA that is not running).
+template <class K, class... Args>
+cudaError_t launch_banded(K k, int NB, int grid, int block, size_t smem, cudaStream_t st, Args... args) {
+  if (NB <= 1) {
+    k<<<grid, block, smem, st>>>(args...);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid, 1, 1);
+  cfg.blockDim = dim3((unsigned)block, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)NB;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <class Real>
 cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int level, int grid, int block, size_t smem,
                          cudaStream_t st, const trt::SweepArgs<Real>& a) {
   SweepKernel<Real> k = sweep_kernel_for<Real>(kc, src_full, level);
   if (!k) return cudaErrorInvalidValue;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k<<<grid, block, smem, st>>>(a);
-  return cudaGetLastError();
+  return launch_banded(k, a.t.NB, grid, block, smem, st, a);
 }
 
 // CTAs of a sweep configuration that are resident on one SM at once (0 on failure).
@@ -220,7 +242,7 @@ struct trt_ctx {
   int nx = 0, ny = 0, nm = 0, ng = 0, mq = 0, prec = 0;
   size_t budget = 0, used = 0;
   cudaStream_t stream = nullptr;
-  int Wreq = 0, Sreq = 0, NHreq = 0, stages = 2;
+  int Wreq = 0, Sreq = 0, NHreq = 0, NBreq = 0, stages = 2;   // NBreq: band CTAs per sweep (0: default)
   int regs = 0;                      // register level of the sweep kernel in use (set by setup_layout)
   int regs_req = -1;                 // -1: the highest level that keeps the grid resident; 0..2: at most that
   KernelCfg kc{8, 5};
@@ -408,12 +430,15 @@ int setup_layout(trt_ctx* c) {
   const size_t sbytes_old = c->blk ? (size_t)c->state_elems() * esz : 0;
   const size_t src_old = sbytes_old;
   const size_t wrap_old = c->blk ? wrap_bytes(c) : 0, part_old = c->blk ? part_bytes(c) : 0;
-  const trt::Tiling t = trt::make_tiling(c->nx, c->ny, c->mq, W, c->kc.S, NH);
+  // band CTAs per sweep: requested (trt_set_bands, trt_autotune), else one
+  int NB = c->NBreq > 0 ? c->NBreq : 1;
+  if (NB > 8) return TRT_ERR_ARG;
+  const trt::Tiling t = trt::make_tiling(c->nx, c->ny, c->mq, W, c->kc.S, NH, NB);
   // pipeline depth limited by shared memory
   const long long chunk = trt::chunk_elems(t);
   auto smem_at = [&](int st) {
-    return c->prec == TRT_PREC_FP64 ? trt::sweep_smem_bytes<double>(W, chunk, st, t.mqc, t.D)
-                                    : trt::sweep_smem_bytes<float>(W, chunk, st, t.mqc, t.D);
+    return c->prec == TRT_PREC_FP64 ? trt::sweep_smem_bytes<double>(W, chunk, st, t.mqc, t.D, t.S)
+                                    : trt::sweep_smem_bytes<float>(W, chunk, st, t.mqc, t.D, t.S);
   };
   int stages = c->stages;
   while (stages > 1 && smem_at(stages) > (size_t)200 * 1024) stages--;
@@ -443,7 +468,7 @@ int setup_layout(trt_ctx* c) {
     const size_t smem = smem_at(stages);
     const int per = c->prec == TRT_PREC_FP64 ? sweep_ctas_per_sm<double>(c->kc, 32 * W, smem, level)
                                              : sweep_ctas_per_sm<float>(c->kc, 32 * W, smem, level);
-    if (per > 0 && 4LL * c->ng * NH <= (long long)per * sm_count()) {
+    if (per > 0 && 4LL * c->ng * NH * t.NB <= (long long)per * sm_count()) {
       c->regs = level;
       break;
     }
@@ -580,7 +605,7 @@ trt::SweepArgs<Real> make_sweep_args(const trt_ctx* c) {
 
 template <class Real>
 size_t sweep_smem(const trt_ctx* c) {
-  return trt::sweep_smem_bytes<Real>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D);
+  return trt::sweep_smem_bytes<Real>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D, c->t.S);
 }
 
 template <class Real>
@@ -590,8 +615,8 @@ template <class Real>
 int sweep_impl(trt_ctx* c, unsigned flags) {
   if (flags & TRT_ROLL_STATE) c->cur = 1 - c->cur;   // I_crn_old <- I_crn (ALGORITHMS.f08:397)
   const trt::SweepArgs<Real> a = make_sweep_args<Real>(c);
-  cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, c->use_srcfull ? 0 : c->regs, 4 * c->ng * c->t.NH,
-                                     32 * c->t.W, sweep_smem<Real>(c), c->stream, a);
+  cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, c->use_srcfull ? 0 : c->regs,
+                                     4 * c->ng * c->t.NH * c->t.NB, 32 * c->t.W, sweep_smem<Real>(c), c->stream, a);
   TRT_LAUNCHED();
   if (e != cudaSuccess) return TRT_ERR_CUDA;
   c->swept = true;
@@ -1140,7 +1165,7 @@ int batch_group_launch(trt_batch* b, std::vector<trt_ctx*>& grp, size_t args_off
                        cudaStream_t gs) {
   // largest CTAs first: the block scheduler then starts the long sweeps before the short ones
   std::stable_sort(grp.begin(), grp.end(), [](const trt_ctx* x, const trt_ctx* y) {
-    return (long long)x->t.Tsteps * x->t.D > (long long)y->t.Tsteps * y->t.D;
+    return (long long)x->t.Tb * x->t.D > (long long)y->t.Tb * y->t.D;
   });
   auto* ha = reinterpret_cast<trt::SweepArgs<Real>*>(b->h_args + args_off);
   auto* hf = reinterpret_cast<int*>(b->h_args + first_off);
@@ -1149,7 +1174,7 @@ int batch_group_launch(trt_batch* b, std::vector<trt_ctx*>& grp, size_t args_off
   for (size_t k = 0; k < grp.size(); ++k) {
     ha[k] = make_sweep_args<Real>(grp[k]);
     hf[k] = (int)total;
-    total += 4LL * grp[k]->ng * grp[k]->t.NH;
+    total += 4LL * grp[k]->ng * grp[k]->t.NH * grp[k]->t.NB;
     smem = std::max(smem, sweep_smem<Real>(grp[k]));
     grp[k]->swept = true;
   }
@@ -1172,9 +1197,9 @@ int batch_group_launch(trt_batch* b, std::vector<trt_ctx*>& grp, size_t args_off
   SweepBatchKernel<Real> k = sweep_batch_kernel_for<Real>(grp[0]->kc, grp[0]->use_srcfull, level);
   if (!k) return TRT_ERR_UNSUPPORTED;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k<<<(unsigned)total, 32 * grp[0]->t.W, smem, gs>>>(da, df, (int)grp.size());
+  TRT_CUDA(launch_banded(k, grp[0]->t.NB, (int)total, 32 * grp[0]->t.W, smem, gs, (const trt::SweepArgs<Real>*)da,
+                         (const int*)df, (int)grp.size()));
   TRT_LAUNCHED();
-  TRT_CUDA(cudaGetLastError());
   return TRT_OK;
 }
 
@@ -1183,9 +1208,10 @@ int batch_group_launch(trt_batch* b, std::vector<trt_ctx*>& grp, size_t args_off
 int batch_sweep_launch(trt_batch* b, const std::vector<int>& act, const std::vector<char>& roll) {
   TRT_CUDA(cudaStreamSynchronize(b->stream));   // the staging buffers of the previous launch are free
   struct Key {
-    int prec, S, D, W, stages, srcfull;
+    int prec, S, D, W, stages, srcfull, NB;
     bool operator==(const Key& o) const {
-      return prec == o.prec && S == o.S && D == o.D && W == o.W && stages == o.stages && srcfull == o.srcfull;
+      return prec == o.prec && S == o.S && D == o.D && W == o.W && stages == o.stages && srcfull == o.srcfull &&
+             NB == o.NB;
     }
   };
   std::vector<Key> keys;
@@ -1193,7 +1219,7 @@ int batch_sweep_launch(trt_batch* b, const std::vector<int>& act, const std::vec
   for (size_t i = 0; i < act.size(); ++i) {
     trt_ctx* c = b->h[act[i]];
     if (roll[i]) c->cur = 1 - c->cur;   // I_crn_old <- I_crn (ALGORITHMS.f08:397)
-    const Key key{c->prec, c->kc.S, c->kc.D, c->t.W, c->stages, c->use_srcfull ? 1 : 0};
+    const Key key{c->prec, c->kc.S, c->kc.D, c->t.W, c->stages, c->use_srcfull ? 1 : 0, c->t.NB};
     size_t g = 0;
     while (g < keys.size() && !(keys[g] == key)) ++g;
     if (g == keys.size()) {
@@ -1559,24 +1585,26 @@ int trt_autotune(trt_ctx* c, int* warps_out, int* slices_out, int* splits_out, f
   TRT_CUDA(cudaEventCreate(&e0));
   TRT_CUDA(cudaEventCreate(&e1));
   const int sms = sm_count();
-  int bestNH = 0, bestW = 0;
+  int bestNH = 0, bestW = 0, bestNB = 1;
   float best = 0.0f;
-  const int nhs[] = {1, 2, 3, 4}, ws[] = {2, 3, 4, 5, 6, 8};
+  const int nhs[] = {1, 2, 3, 4}, ws[] = {2, 3, 4, 5, 6, 8}, nbs[] = {1, 2, 4};
   for (int NH : nhs) {
     if (NH > c->mq) continue;
-    for (int W : ws) {
+    for (int W : ws)
+    for (int NB : nbs) {
       c->NHreq = NH;
       c->Wreq = W;
+      c->NBreq = NB;
       c->Sreq = 0;
       c->stages = 2;
-      if (setup_layout(c) != TRT_OK) continue;
+      if (setup_layout(c) != TRT_OK || c->t.NB != NB) continue;
       // only tilings whose CTAs are all resident at once
       const size_t smem = c->prec == TRT_PREC_FP64
-                              ? trt::sweep_smem_bytes<double>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D)
-                              : trt::sweep_smem_bytes<float>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D);
+                              ? trt::sweep_smem_bytes<double>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D, c->t.S)
+                              : trt::sweep_smem_bytes<float>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D, c->t.S);
       const int per = c->prec == TRT_PREC_FP64 ? sweep_ctas_per_sm<double>(c->kc, 32 * c->t.W, smem, c->regs)
                                                : sweep_ctas_per_sm<float>(c->kc, 32 * c->t.W, smem, c->regs);
-      if (per <= 0 || 4LL * c->ng * NH > (long long)per * sms) continue;
+      if (per <= 0 || 4LL * c->ng * NH * c->t.NB > (long long)per * sms) continue;
       c->have_state = true;
       c->have_material = true;
       int rc = c->prec == TRT_PREC_FP64 ? sweep_impl<double>(c, 0) : sweep_impl<float>(c, 0);
@@ -1593,6 +1621,7 @@ int trt_autotune(trt_ctx* c, int* warps_out, int* slices_out, int* splits_out, f
         best = ms;
         bestNH = NH;
         bestW = W;
+        bestNB = NB;
       }
     }
   }
@@ -1600,6 +1629,7 @@ int trt_autotune(trt_ctx* c, int* warps_out, int* slices_out, int* splits_out, f
   cudaEventDestroy(e1);
   c->NHreq = bestNH;
   c->Wreq = bestW;
+  c->NBreq = bestNB;
   c->Sreq = 0;
   c->stages = 2;
   int rc = setup_layout(c);
@@ -1626,6 +1656,14 @@ int trt_set_tiling(trt_ctx* c, int warps_per_cta, int slices, int stages, int sp
   c->stages = stages ? stages : 2;
   return setup_layout(c);
 }
+
+int trt_set_bands(trt_ctx* c, int bands) {
+  if (!c || bands < 0 || bands > 8) return TRT_ERR_ARG;
+  c->NBreq = bands;
+  return setup_layout(c);
+}
+
+int trt_get_bands(const trt_ctx* c) { return c ? c->t.NB : TRT_ERR_ARG; }
 
 int trt_set_register_mode(trt_ctx* c, int mode) {
   if (!c || mode < -1 || mode > 2) return TRT_ERR_ARG;

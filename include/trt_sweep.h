@@ -256,6 +256,17 @@ int trt_set_tiling(trt_ctx* ctx, int warps_per_cta, int slices, int stages, int 
 int trt_get_tiling(const trt_ctx* ctx, int* warps_per_cta, int* slices, int* dirs_per_lane, int* stages,
                    int* splits);
 
+/* Spatial tiles of the sweep: the rounds (row tiles of warps x rows-per-warp rows) of every (group,
+ * quadrant, split) sweep are dealt round-robin to `bands` CTAs (1..8) that run as one thread-block
+ * cluster, each a row tile behind the one below on a tile-diagonal wavefront; a round's bottom inflow is
+ * the round below's top outflow, handed over through an L2-resident buffer with a cluster-scope
+ * release/acquire progress count per step (bounded waits; a wait that runs out sets the timeout error).
+ * 0 or 1 = one CTA sweeps every round.  Capped at the number of rounds.  Results are bit-identical for
+ * every band count.  Re-lays out (zeroes) the state.  trt_get_bands returns the count in use.
+ * (TRANSPORT_SOLVES.f08:54-242 sweeps each (m, g) over the whole grid in one thread.) */
+int trt_set_bands(trt_ctx* ctx, int bands);
+int trt_get_bands(const trt_ctx* ctx);
+
 /* Register budget of the sweep kernel.  Each configuration is compiled at three levels: 0 for any CTA
  * size (at most 128 registers per thread), 1 for CTAs of at most 128 threads with 3 per SM (up to 170),
  * 2 for CTAs of at most 128 threads with 2 per SM (up to 255).  mode -1 (the default) uses the highest
@@ -265,8 +276,8 @@ int trt_set_register_mode(trt_ctx* ctx, int mode);
 int trt_get_register_mode(const trt_ctx* ctx);
 
 /* Autotuner: times one sweep of this handle's problem for each (direction splits 1..4) x (warps per CTA
- * 2, 3, 4, 5, 6, 8) tiling whose CTAs are all resident at once (CUDA occupancy query), with the
- * default slices per warp, and keeps the fastest.  Uses the handle's material if set, else a zero
+ * 2, 3, 4, 5, 6, 8) x (bands 1, 2, 4) tiling whose CTAs are all resident at once (CUDA occupancy query),
+ * with the default slices per warp, and keeps the fastest.  Uses the handle's material if set, else a zero
  * material.  Call before trt_init_state / trt_put_state: it re-lays out (and zeroes) the state.
  * Outputs (each may be NULL): the chosen warps, slices, splits and its sweep time in ms. */
 int trt_autotune(trt_ctx* ctx, int* warps_per_cta, int* slices, int* splits, float* sweep_ms);

@@ -53,11 +53,13 @@ def dropin_sweep(d, res_calc=False):
     return out
 
 
-def resident(d, precision="fp64", tiling=None, bc_type=(0, 0, 0, 0)):
+def resident(d, precision="fp64", tiling=None, bc_type=(0, 0, 0, 0), bands=0):
     nx, ny, ng = len(d["Delx"]), len(d["Dely"]), d["KapE_in"].shape[2]
     s = pkg.TransportSweep(nx, ny, d["Omega_x"], d["Omega_y"], d["w"], d["Delx"], d["Dely"], ng, precision=precision)
     if tiling:
         s.set_tiling(**tiling)
+    if bands:
+        s.set_bands(bands)
     s.put_state(d["I_crn_old"])
     s.set_boundary(d["Ic_edgV"], d["Ic_edgH"], bc_type)
     s.set_material(d["KapE_in"], d["src_iso"], d["c"], d["dt"], CU)
@@ -532,3 +534,54 @@ def test_c1_full_size_sweep_matches_gaussian_elimination_oracle(oracle):
         for k in FG_KEYS + ("Cg_L", "Cg_B", "Cg_R", "Cg_T"):
             assert np.max(np.abs(m[k][..., chunk] - r0[k])) <= 1e-12, (k, chunk)
         del d, r0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("bands,tiling", [(2, dict(warps=1, slices=4)), (3, dict(warps=2, slices=8)),
+                                          (4, dict(warps=1, slices=8)), (8, dict(warps=1, slices=8, splits=2))],
+                         ids=["b2", "b3", "b4", "b8"])
+def test_band_ctas_bit_identical(precision, bands, tiling):
+    """Spatial row tiles: the rounds of each sweep dealt to `bands` CTAs of one cluster, handed over
+    through the L2 wrap buffer, give the same corner state and moments as one CTA per sweep, bit for bit,
+    over two rolled steps."""
+    prob = pkg.problems.random_small(8, 33, 29, 2, "S16")
+    d = sweep_inputs(prob, seed=5)
+    out = []
+    for nb in (0, bands):
+        with resident(d, precision=precision, tiling=tiling, bands=nb) as s:
+            t = s.tiling()
+            s.sweep(moments=True)
+            s.sweep(roll=True, moments=True)
+            out.append((t, s.get_state(), s.moments(["Eg_avg", "fg_avg_xy", "fg_edgV_xx", "Cg_T", "Eg_in_L"])))
+    (t0, I0, m0), (t1, I1, m1) = out
+    assert t0["bands"] == 1 and t1["bands"] > 1
+    assert np.array_equal(I0, I1)
+    for k in m0:
+        assert np.array_equal(m0[k], m1[k]), k
+
+
+def test_band_ctas_time_loop_matches_single_cta():
+    """The config-0 time loop (three steps of the transport-only iteration) with band CTAs equals the
+    default tiling bit for bit."""
+    from test_gpu_tstep import _device
+    prob = pkg.problems.config0()
+    ts = pkg.problems.config_timestep_setup(prob)
+    res = []
+    for nb in (1, 3):
+        s = _device(prob, ts, "fp64", 2, 0.0, 5, law=1)
+        try:
+            if nb > 1:
+                s.set_tiling(warps=1, slices=8)
+                s.set_bands(nb)
+                s.init_state(ts.Tini_eV, list(ts.bcT_eV), CU, ts.nu_eV)
+            else:
+                s.set_tiling(warps=1, slices=8)
+                s.init_state(ts.Tini_eV, list(ts.bcT_eV), CU, ts.nu_eV)
+            Ts = [(s.tstep(), s.temperature()) for _ in range(3)]
+            res.append((s.tiling()["bands"], Ts, s.get_state()))
+        finally:
+            s.close()
+    assert res[0][0] == 1 and res[1][0] == 3
+    for (_, Ta), (_, Tb) in zip(res[0][1], res[1][1]):
+        assert np.array_equal(Ta, Tb)
+    assert np.array_equal(res[0][2], res[1][2])
