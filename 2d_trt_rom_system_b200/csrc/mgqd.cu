@@ -64,7 +64,7 @@ struct Solver {
   bool matvec_timed = false;
   bool time_matvec = true;          // time the first iteration's matrix-vector product (trt_mgqd_last_stats)
   bool use_graphs = true;           // replay iteration blocks as a CUDA graph
-  bool rel_initial = false;         // stopping test also relative to the initial residual (Krylov::rel_initial)
+  bool update_test = false;         // SPARSKIT's solution-update stopping test (Krylov::update_test)
   cudaGraphExec_t gexec = nullptr;  // kCheckEvery iterations, recorded on first use
   int g_nodes = 0, g_maxit = -1, g_rel = -1;
   double g_tol = -1.0;
@@ -138,7 +138,7 @@ int Solver::init(int nx, int ny, int ng, bool own_inputs) {
   M(&K.x, U); M(&K.r, U); M(&K.rh, U); M(&K.p0, U); M(&K.p1, U); M(&K.v, U); M(&K.s, U); M(&K.t, U);
   M(&K.ph, U); M(&K.sh, U);
   const int nblk = pos_blocks();
-  M(&K.part, (size_t)ng * nblk * 4);
+  M(&K.part, (size_t)ng * nblk * 5);
   M(&rpart, (size_t)ng * nblk * kNRes);
   M(&Fx, V); M(&Fy, H); M(&res, (size_t)ng * 25); M(&bcres, (size_t)ng * 4);
   double* sc = nullptr;
@@ -200,7 +200,8 @@ int Solver::krylov(cudaStream_t s) {
   matvec_timed = false;
   K.tol = g_settings.tol;
   K.maxit = g_settings.maxit;
-  K.rel_initial = rel_initial ? 1 : 0;
+  K.update_test = update_test ? 1 : 0;
+  K.atol = 1e-15;   // fpar(2) of QD_SOLVERS.f08:445
   use_graphs = g_settings.graphs;
   prec_coef_kernel<<<gpos, kRedBlock, 0, s>>>(d, cf, ls.L[0]);
   MG_LAUNCHED();
@@ -289,7 +290,7 @@ int Solver::krylov(cudaStream_t s) {
   // kernels take the solver's fixed buffers and K by value, so the graph is recorded again only when the
   // tolerance or the iteration limit in K changes.
   auto block = [&]() -> int {
-    if (!gexec || g_tol != K.tol || g_maxit != K.maxit || g_rel != K.rel_initial) {
+    if (!gexec || g_tol != K.tol || g_maxit != K.maxit || g_rel != K.update_test) {
       if (gexec) {
         cudaGraphExecDestroy(gexec);
         gexec = nullptr;
@@ -317,7 +318,7 @@ int Solver::krylov(cudaStream_t s) {
       g_nodes = recorded;
       g_tol = K.tol;
       g_maxit = K.maxit;
-      g_rel = K.rel_initial;
+      g_rel = K.update_test;
     }
     MG_CUDA(cudaGraphLaunch(gexec, s));
     trt_host::add_launches((unsigned long long)g_nodes);
@@ -1053,7 +1054,7 @@ int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm) {
   if ((rc = m->GR->init(nx, ny, 1, false))) return rc;
   m->MG->time_matvec = false;   // every iteration block of the time loop's solves runs as a graph
   m->GR->time_matvec = false;
-  m->GR->rel_initial = true;    // Newton corrections: the reference's initial-residual test
+  m->GR->update_test = true;    // Newton corrections: the reference's stopping test (ipar(3) = -1)
   const size_t C = (size_t)d.nC * ng, V = (size_t)d.nV * ng, H = (size_t)d.nH * ng;
   const size_t c1 = d.nC, v1 = d.nV, hh1 = d.nH;
   const size_t side[4] = {(size_t)ny, (size_t)nx, (size_t)ny, (size_t)nx};   // L, B, R, T

@@ -500,15 +500,12 @@ struct Krylov {
   double* part;      // [ng][nblk][4]
   double tol;
   int maxit;
-  // 0: stop when the scaled residual is at most tol * max|x|.  1: or at most tol * the initial one, whichever is
-  // looser -- the form of SPARSKIT's test that the reference's QD_FV uses (QD_SOLVERS.f08:444), which a Newton
-  // correction far smaller than its starting guess needs.
-  int rel_initial;
+  // 0: stop when the Jacobi-scaled residual is at most tol * max|x|.  1: SPARSKIT's test with ipar(3) = -1, the
+  // one the reference's QD_FV sets (QD_SOLVERS.f08:439-445): stop when the solution update of an iteration is
+  // small, ||x_i - x_(i-1)||_2 <= tol * ||x_i||_2 + atol (fpar(1) = tol, fpar(2) = atol).
+  int update_test;
+  double atol;
 };
-
-__device__ __forceinline__ double krylov_bound(const Krylov& K, const Scal& s, double xmax) {
-  return K.tol * (K.rel_initial ? fmax(xmax, s.res0) : xmax);
-}
 
 // Jacobi scale of the row of unknown (cell / V edge / H edge) for the convergence norm.
 __device__ __forceinline__ double row_scale(const Coefs& cf, const Dims& d, int g, int kind, long e) {
@@ -563,7 +560,8 @@ __global__ void init_finish_kernel(const Krylov K, int nblk) {
     s.best = o[1];
     s.best_it = 0;
     s.res0 = o[1];
-    s.done = (o[1] <= K.tol * o[2] || o[0] == 0.0) ? 1 : 0;
+    // the update test needs an iteration; a zero (rh.r) means the guess solves the system exactly
+    s.done = (o[0] == 0.0 || (!K.update_test && o[1] <= K.tol * o[2])) ? 1 : 0;
     K.sc[g] = s;
     K.done[g] = s.done;
   }
@@ -675,40 +673,44 @@ __global__ void scalar_finish_kernel(const Krylov K, int nblk, int mode) {
   }
 }
 
-// x += alpha ph + omega sh; r = s - omega t; partials: (rh.r), max |r| / |diag|, max |x|.
+// x += alpha ph + omega sh; r = s - omega t; partials: (rh.r), max |r| / |diag|, max |x|, sum (x_i - x_(i-1))^2,
+// sum x_i^2.
 __global__ void __launch_bounds__(kRedBlock) update_kernel(const Coefs cf, const Dims d, const Krylov K) {
   const int g = blockIdx.y;
   if (K.done[g]) return;
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  double v3[3] = {0.0, 0.0, 0.0};
+  double v5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   if (pos < d.npos()) {
     const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
     const Scal sc = K.sc[g];
     const long base = d.nU * g;
     auto emit = [&](long u, int kind, long e) {
-      const double xn = K.x[base + u] + sc.alpha * K.ph[base + u] + sc.omega * K.sh[base + u];
+      const double dx = sc.alpha * K.ph[base + u] + sc.omega * K.sh[base + u];
+      const double xn = K.x[base + u] + dx;
       const double rn = K.s[base + u] - sc.omega * K.t[base + u];
       K.x[base + u] = xn;
       K.r[base + u] = rn;
-      v3[0] += K.rh[base + u] * rn;
-      v3[1] = fmax(v3[1], fabs(rn) * row_scale(cf, d, g, kind, e));
-      v3[2] = fmax(v3[2], fabs(xn));
+      v5[0] += K.rh[base + u] * rn;
+      v5[1] = fmax(v5[1], fabs(rn) * row_scale(cf, d, g, kind, e));
+      v5[2] = fmax(v5[2], fabs(xn));
+      v5[3] += dx * dx;
+      v5[4] += xn * xn;
     };
     if (i < d.nx && j < d.ny) emit(i + (long)d.nx * j, 0, i + (long)d.nx * j);
     if (j < d.ny) emit(d.oV() + i + (long)(d.nx + 1) * j, 1, i + (long)(d.nx + 1) * j);
     if (i < d.nx) emit(d.oH() + i + (long)d.nx * j, 2, i + (long)d.nx * j);
   }
-  const int kind[3] = {0, 1, 1};
-  block_reduce<3>(v3, kind, K.part, g);
+  const int kind[5] = {0, 1, 1, 0, 0};
+  block_reduce<5>(v5, kind, K.part, g);
 }
 
 // rho_new, beta, convergence test.  done: 1 converged; -1 breakdown or iteration limit.
 __global__ void update_finish_kernel(const Krylov K, int nblk) {
   const int g = blockIdx.x;
   if (K.done[g]) return;
-  const int kind[3] = {0, 1, 1};
-  double o[3];
-  warp_finish<3>(K.part, nblk, g, kind, o);
+  const int kind[5] = {0, 1, 1, 0, 0};
+  double o[5];
+  warp_finish<5>(K.part, nblk, g, kind, o);
   if (threadIdx.x == 0) {
     Scal& s = K.sc[g];
     s.its += 1;
@@ -719,7 +721,8 @@ __global__ void update_finish_kernel(const Krylov K, int nblk) {
       s.best = o[1];
       s.best_it = s.its;
     }
-    if (o[1] <= krylov_bound(K, s, o[2])) {
+    const bool conv = K.update_test ? (sqrt(o[3]) <= K.tol * sqrt(o[4]) + K.atol) : (o[1] <= K.tol * o[2]);
+    if (conv) {
       done = 1;
     } else if (o[0] == 0.0 || s.omega == 0.0 || s.alpha == 0.0 || !(o[1] == o[1]) || s.its >= K.maxit ||
                s.its - s.best_it >= kStagnation) {
