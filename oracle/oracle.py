@@ -502,7 +502,7 @@ def mlqd_steps(st, Omega_x, Omega_y, quad_weight, Delx, Dely, Nu_g, kappa_mult, 
                Theta=1.0, conv_type=2, conv_ho=1e-10, conv_lo=1e-10, conv_gr1=1e-14, conv_gr2=1e-15, maxit_rte=50,
                maxit_mloqd=50, maxit_gloqd=20, chi=0.7, line_src=2.0, E_Bound_Low=0.0, T_Bound_Low=0.0,
                use_line_search=True, use_safety_search=False, kapE_dT_flag=True, bc_type=(0, 0, 0, 0),
-               bcT=(0.0, 0.0, 0.0, 0.0), threads=4):
+               bcT=(0.0, 0.0, 0.0, 0.0), threads=4, solver=1):
     """Time steps of TRT_MLQD_ALGORITHM with run_type 'mlqd' (ALGORITHMS.f08:389-416, 518-572, 670-836), on
     the state dict of mlqd_init (updated in place).  Per step: the _old copies (:395-416), OLD_MGQD_COEFS and
     OLD_GREY_COEFS; then outer iterations, each (from the second on) TRANSPORT_SCB + COLLAPSE_INTENSITIES
@@ -511,7 +511,8 @@ def mlqd_steps(st, Omega_x, Omega_y, quad_weight, Delx, Dely, Nu_g, kappa_mult, 
     MATERIAL_UPDATE with CONVERGENCE(conv_lo) on T and the MGQD E, then CONVERGENCE(conv_ho) on T and the
     transport E.  cV is a scalar or an (nx, ny) array.  Returns one dict per step (Temp, E_avg, HO_E_avg,
     RT_Its, MGQD_Its per outer iteration, EGP_Its per MGQD iteration, the last MGQD T/E norms of each outer
-    iteration, the outer T/E norms)."""
+    iteration, the outer T/E norms).  solver: the sweep's cell solve (0 = Gaussian elimination, 1 = closed
+    form)."""
     nx, ny = st["Temp"].shape
     nm, ng = len(Omega_x), len(Nu_g) - 1
     A = F(np.outer(Delx, Dely))
@@ -540,7 +541,7 @@ def mlqd_steps(st, Omega_x, Omega_y, quad_weight, Delx, Dely, Nu_g, kappa_mult, 
             if rt_its >= rt_start:
                 Src_in = F(np.repeat(np.repeat(rt_src, 2, axis=0), 2, axis=1)[:, :, None, :].repeat(nm, axis=2))
                 s = transport_scb(st["I_edgV"], st["I_edgH"], st["Ic_edgV"], st["Ic_edgH"], Omega_x, Omega_y, Delx,
-                                  Dely, A, KapE, Src_in, I_crn_old, c, Delt, threads=threads, solver=1)
+                                  Dely, A, KapE, Src_in, I_crn_old, c, Delt, threads=threads, solver=solver)
                 for k in ("I_crn", "I_edgV", "I_edgH", "Ic_edgV", "Ic_edgH"):
                     st[k] = s[k]
                 m = collapse_intensities(s["I_avg"], s["I_edgV"], s["I_edgH"], Omega_x, Omega_y, quad_weight,
