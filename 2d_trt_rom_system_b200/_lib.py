@@ -125,6 +125,11 @@ SIGNATURES = {
     "trt_device_output": (_P, [_P, ctypes.c_char_p]),
     "trt_set_register_mode": (_i, [_P, _i]),
     "trt_set_bands": (_i, [_P, _i]),
+    "trt_set_inplace": (_i, [_P, _i]),
+    "trt_state_bytes": (ctypes.c_size_t, [_P]),
+    "trt_bind_state": (_i, [_P, ctypes.c_void_p, ctypes.c_size_t]),
+    "trt_state_written": (_i, [_P]),
+    "trt_snapshot_angular_groups": (_i, [_P, _i, _i, ctypes.c_void_p]),
     "trt_get_bands": (_i, [_P]),
     "trt_get_register_mode": (_i, [_P]),
     "trt_autotune": (_i, [_P, _I, _I, _I, ctypes.POINTER(ctypes.c_float)]),

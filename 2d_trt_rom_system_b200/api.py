@@ -621,6 +621,32 @@ class TransportSweep:
         one thread-block cluster each); 0/1 = one CTA per sweep.  Re-lays out (zeroes) the state."""
         check(_lib.lib().trt_set_bands(self._h, int(bands)), "trt_set_bands")
 
+    def set_inplace(self, on=True):
+        """One corner-state buffer swept in place (each sweep consumes I_crn_old: the next sweep must roll).
+        Re-lays out (zeroes) the state."""
+        check(_lib.lib().trt_set_inplace(self._h, 1 if on else 0), "trt_set_inplace")
+
+    def state_bytes(self):
+        return int(_lib.lib().trt_state_bytes(self._h))
+
+    def bind_state(self, device_ptr, nbytes):
+        """In-place handles: sweep a caller-owned device buffer (raw state bytes of this layout)."""
+        check(_lib.lib().trt_bind_state(self._h, ctypes.c_void_p(int(device_ptr)), ctypes.c_size_t(int(nbytes))),
+              "trt_bind_state")
+
+    def state_written(self):
+        """The bound state now holds I_crn_old (raw bytes copied in by the caller)."""
+        check(_lib.lib().trt_state_written(self._h), "trt_state_written")
+
+    def snapshot_angular(self, device_ptr):
+        """FP32 I_avg of every group into device memory (n_x, n_y, n_m, n_g), on the handle's stream."""
+        check(_lib.lib().trt_snapshot_angular(self._h, ctypes.c_void_p(int(device_ptr))), "trt_snapshot_angular")
+
+    def snapshot_angular_groups(self, g0, n_groups, device_ptr):
+        """FP32 I_avg of groups g0..g0+n_groups-1 into device memory (n_x, n_y, n_m, n_groups), on the stream."""
+        check(_lib.lib().trt_snapshot_angular_groups(self._h, int(g0), int(n_groups), ctypes.c_void_p(int(device_ptr))),
+              "trt_snapshot_angular_groups")
+
     def set_register_mode(self, mode):
         """Cap the sweep kernel's register level (0: <= 128, 1: <= 170, 2: <= 255 registers per thread);
         -1 = the highest level that keeps the whole grid resident.  Re-lays out (zeroes) the state."""

@@ -112,15 +112,16 @@ __device__ __forceinline__ Real icH_value(const Geo& G, const Real* st, const Re
 // arrays (the reference keeps the caller's values there; the host layer restores them).
 // Snapshot of the cell-average angular intensity I_avg(nx, ny, nm, ng) = mean of the four corner values
 // (TRANSPORT_SOLVES.f08 forms I_avg so), written as 4-byte floats into a caller's device store.
+// Groups g0 .. g0+ngs-1 only (out holds those groups, group-slowest).
 template <class Real>
-__global__ void snapshot_avg_kernel(Geo G, const Real* __restrict__ st, float* __restrict__ out) {
-  const long long nA = (long long)G.nx * G.ny * G.nm * G.ng;
+__global__ void snapshot_avg_kernel(Geo G, const Real* __restrict__ st, float* __restrict__ out, int g0, int ngs) {
+  const long long nA = (long long)G.nx * G.ny * G.nm * ngs;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nA; k += (long long)gridDim.x * blockDim.x) {
     long long r = k;
     const int i = (int)(r % G.nx); r /= G.nx;
     const int j = (int)(r % G.ny); r /= G.ny;
     const int m = (int)(r % G.nm);
-    const int g = (int)(r / G.nm);
+    const int g = g0 + (int)(r / G.nm);
     const double lb = (double)st[state_index<Real>(G, i, j, 0, 0, m, g)];
     const double rb = (double)st[state_index<Real>(G, i, j, 1, 0, m, g)];
     const double rt = (double)st[state_index<Real>(G, i, j, 1, 1, m, g)];

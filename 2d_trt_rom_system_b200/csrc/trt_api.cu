@@ -260,6 +260,8 @@ struct trt_ctx {
   void *d_kap = nullptr, *d_q = nullptr;
   void* d_state[2] = {nullptr, nullptr};
   int cur = 0;                  // d_state[cur] = I_crn_old, d_state[1-cur] = I_crn
+  bool inplace = false;         // one state buffer, swept in place (each sweep consumes I_crn_old)
+  void* ext_state = nullptr;    // caller-provided device memory holding the in-place state (trt_bind_state)
   void* d_srcfull = nullptr;
   bool use_srcfull = false;
   void *d_bndV = nullptr, *d_bndH = nullptr;
@@ -443,6 +445,11 @@ int setup_layout(trt_ctx* c) {
   int stages = c->stages;
   while (stages > 1 && smem_at(stages) > (size_t)200 * 1024) stages--;
   if (smem_at(stages) > (size_t)220 * 1024) return TRT_ERR_ARG;   // tiling does not fit an SM
+  if (c->ext_state) {   // a bound external state is dropped with the layout it was sized for
+    c->d_state[0] = c->d_state[1] = nullptr;
+    c->ext_state = nullptr;
+  }
+  if (c->d_state[1] == c->d_state[0]) c->d_state[1] = nullptr;   // in place: one buffer
   for (int k = 0; k < 2; ++k) {
     c->dfree(c->d_state[k], sbytes_old);
     c->d_state[k] = nullptr;
@@ -474,11 +481,12 @@ int setup_layout(trt_ctx* c) {
     }
   }
   const size_t sbytes = (size_t)c->state_elems() * esz;
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < (c->inplace ? 1 : 2); ++k) {
     int rc = c->dalloc(&c->d_state[k], sbytes);
     if (rc) return rc;
     TRT_CUDA(cudaMemsetAsync(c->d_state[k], 0, sbytes, c->stream));
   }
+  if (c->inplace) c->d_state[1] = c->d_state[0];
   int rc = c->dalloc(&c->d_wrap, wrap_bytes(c));
   if (rc) return rc;
   if ((rc = c->dalloc(&c->d_part, part_bytes(c)))) return rc;
@@ -613,6 +621,9 @@ int sweep_epilogue(trt_ctx* c, unsigned flags);
 
 template <class Real>
 int sweep_impl(trt_ctx* c, unsigned flags) {
+  // in place, a sweep overwrites I_crn_old: the next one must start a new step (roll) and the residuals,
+  // which read I_crn_old after the sweep, are not available
+  if (c->inplace && ((c->swept && !(flags & TRT_ROLL_STATE)) || (flags & TRT_RES_CALC))) return TRT_ERR_STATE;
   if (flags & TRT_ROLL_STATE) c->cur = 1 - c->cur;   // I_crn_old <- I_crn (ALGORITHMS.f08:397)
   const trt::SweepArgs<Real> a = make_sweep_args<Real>(c);
   cudaError_t e = launch_sweep<Real>(c->kc, c->use_srcfull, c->use_srcfull ? 0 : c->regs,
@@ -795,6 +806,7 @@ int init_state_impl(trt_ctx* c, double Tini, const double* Tb, double cu, const 
   rc = bc_update_impl<Real>(c, zero, Tb, cu, nu);
   if (rc) return rc;
   c->have_state = true;
+  c->swept = false;
   return TRT_OK;
 }
 
@@ -1607,10 +1619,12 @@ int trt_autotune(trt_ctx* c, int* warps_out, int* slices_out, int* splits_out, f
       if (per <= 0 || 4LL * c->ng * NH * c->t.NB > (long long)per * sms) continue;
       c->have_state = true;
       c->have_material = true;
-      int rc = c->prec == TRT_PREC_FP64 ? sweep_impl<double>(c, 0) : sweep_impl<float>(c, 0);
+      const unsigned tf = TRT_ROLL_STATE;   // trial data: rolling changes nothing measured, and in place it must
+      int rc = c->prec == TRT_PREC_FP64 ? sweep_impl<double>(c, tf) : sweep_impl<float>(c, tf);
       if (rc) continue;
       TRT_CUDA(cudaEventRecord(e0, c->stream));
-      for (int k = 0; k < 2 && !rc; ++k) rc = c->prec == TRT_PREC_FP64 ? sweep_impl<double>(c, 0) : sweep_impl<float>(c, 0);
+      for (int k = 0; k < 2 && !rc; ++k)
+        rc = c->prec == TRT_PREC_FP64 ? sweep_impl<double>(c, tf) : sweep_impl<float>(c, tf);
       TRT_CUDA(cudaEventRecord(e1, c->stream));
       TRT_CUDA(cudaStreamSynchronize(c->stream));
       if (rc || check_err(c)) continue;
@@ -1655,6 +1669,61 @@ int trt_set_tiling(trt_ctx* c, int warps_per_cta, int slices, int stages, int sp
   c->NHreq = splits;
   c->stages = stages ? stages : 2;
   return setup_layout(c);
+}
+
+int trt_set_inplace(trt_ctx* c, int on) {
+  if (!c || (on != 0 && on != 1)) return TRT_ERR_ARG;
+  if (c->inplace == (on == 1)) return TRT_OK;
+  // release the current buffers under the current mode, then lay out again under the new one
+  const size_t sbytes = c->blk ? (size_t)c->state_elems() * c->esz() : 0;
+  if (c->ext_state) {
+    c->d_state[0] = c->d_state[1] = nullptr;
+    c->ext_state = nullptr;
+  }
+  if (c->d_state[1] == c->d_state[0]) c->d_state[1] = nullptr;
+  for (int k = 0; k < 2; ++k) {
+    c->dfree(c->d_state[k], sbytes);
+    c->d_state[k] = nullptr;
+  }
+  c->inplace = on == 1;
+  return setup_layout(c);
+}
+
+size_t trt_state_bytes(const trt_ctx* c) { return c ? (size_t)c->state_elems() * c->esz() : 0; }
+
+int trt_bind_state(trt_ctx* c, void* device_state, size_t bytes) {
+  if (!c || !device_state || !c->inplace || bytes < trt_state_bytes(c) ||
+      (reinterpret_cast<uintptr_t>(device_state) & 127))
+    return TRT_ERR_ARG;
+  if (!c->ext_state) c->dfree(c->d_state[0], trt_state_bytes(c));
+  c->d_state[0] = c->d_state[1] = device_state;
+  c->ext_state = device_state;
+  c->have_state = false;
+  c->swept = false;
+  return TRT_OK;
+}
+
+int trt_state_written(trt_ctx* c) {
+  if (!c) return TRT_ERR_ARG;
+  c->have_state = true;
+  c->swept = false;
+  return TRT_OK;
+}
+
+int trt_snapshot_angular_groups(trt_ctx* c, int g0, int n_groups, float* I_avg_device) {
+  if (!c || !I_avg_device || g0 < 0 || n_groups < 1 || g0 + n_groups > c->ng) return TRT_ERR_ARG;
+  if (!c->have_state && !c->swept) return TRT_ERR_STATE;
+  const void* st = c->d_state[c->swept ? 1 - c->cur : c->cur];
+  const long long n = (long long)c->nx * c->ny * c->nm * n_groups;
+  if (c->prec == TRT_PREC_FP64)
+    trt::snapshot_avg_kernel<double><<<grid_for(n), 256, 0, c->stream>>>(c->geo(), (const double*)st, I_avg_device, g0,
+                                                                         n_groups);
+  else
+    trt::snapshot_avg_kernel<float><<<grid_for(n), 256, 0, c->stream>>>(c->geo(), (const float*)st, I_avg_device, g0,
+                                                                        n_groups);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  return TRT_OK;
 }
 
 int trt_set_bands(trt_ctx* c, int bands) {
@@ -1862,9 +1931,11 @@ int trt_snapshot_angular(trt_ctx* c, float* I_avg_device) {
   const void* st = c->d_state[c->swept ? 1 - c->cur : c->cur];
   const long long n = (long long)c->nx * c->ny * c->nm * c->ng;
   if (c->prec == TRT_PREC_FP64)
-    trt::snapshot_avg_kernel<double><<<grid_for(n), 256, 0, c->stream>>>(c->geo(), (const double*)st, I_avg_device);
+    trt::snapshot_avg_kernel<double><<<grid_for(n), 256, 0, c->stream>>>(c->geo(), (const double*)st, I_avg_device, 0,
+                                                                         c->ng);
   else
-    trt::snapshot_avg_kernel<float><<<grid_for(n), 256, 0, c->stream>>>(c->geo(), (const float*)st, I_avg_device);
+    trt::snapshot_avg_kernel<float><<<grid_for(n), 256, 0, c->stream>>>(c->geo(), (const float*)st, I_avg_device, 0,
+                                                                        c->ng);
   TRT_LAUNCHED();
   TRT_CUDA(cudaGetLastError());
   return TRT_OK;
@@ -1965,6 +2036,7 @@ int trt_tstep_set_law(trt_ctx* c, int law) {
 int trt_tstep(trt_ctx* c, int* rt_its, double* T_norm, double* E_norm) {
   if (!c) return TRT_ERR_ARG;
   if (!c->ts_ready || (!c->have_state && !c->swept)) return TRT_ERR_STATE;
+  if (c->inplace && c->ts_maxit > 1) return TRT_ERR_STATE;   // later outer iterations re-read I_crn_old
   return c->prec == TRT_PREC_FP64 ? tstep_impl<double>(c, rt_its, T_norm, E_norm)
                                   : tstep_impl<float>(c, rt_its, T_norm, E_norm);
 }

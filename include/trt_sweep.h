@@ -267,6 +267,27 @@ int trt_get_tiling(const trt_ctx* ctx, int* warps_per_cta, int* slices, int* dir
 int trt_set_bands(trt_ctx* ctx, int bands);
 int trt_get_bands(const trt_ctx* ctx);
 
+/* In-place state (on = 1): one corner-state buffer instead of two.  The sweep reads each cell's I_crn_old
+ * from the skewed layout before it writes I_crn to the same place, so the state takes half the device
+ * memory (the 1024^2 x 64-group x S16 instance fits in FP32 only this way).  A sweep then consumes
+ * I_crn_old: after a sweep, the next one must roll (TRT_ROLL_STATE, a new time step), TRT_RES_CALC is
+ * refused, and trt_tstep / trt_mlqd_step allow a single outer iteration per step (TRT_ERR_STATE otherwise).
+ * Re-lays out (zeroes) the state.  (The reference keeps I_crn and I_crn_old, ALGORITHMS.f08:397.) */
+int trt_set_inplace(trt_ctx* ctx, int on);
+/* Bytes of the handle's corner state in its current layout (one buffer). */
+size_t trt_state_bytes(const trt_ctx* ctx);
+/* In-place handles only: use caller-provided device memory (at least trt_state_bytes, 128-byte aligned) for
+ * the state, so that a host driver can stream group slabs of a state larger than the device through a few
+ * device buffers (the bytes are the handle's private layout; copy them whole).  The handle's own buffer is
+ * released; the binding ends with the next re-layout.  The bound state must be put (trt_put_state,
+ * trt_init_state or raw bytes copied in by the caller, then trt_state_written) before the next sweep. */
+int trt_bind_state(trt_ctx* ctx, void* device_state, size_t bytes);
+/* The bound or own state holds a valid I_crn_old (after the caller copied raw state bytes in). */
+int trt_state_written(trt_ctx* ctx);
+/* Snapshot of groups g0 .. g0+n_groups-1 of the cell-average angular intensity (as trt_snapshot_angular,
+ * FP32, (n_x, n_y, n_m, n_groups) Fortran order) into a caller's device store, on the handle's stream. */
+int trt_snapshot_angular_groups(trt_ctx* ctx, int g0, int n_groups, float* I_avg_device);
+
 /* Register budget of the sweep kernel.  Each configuration is compiled at three levels: 0 for any CTA
  * size (at most 128 registers per thread), 1 for CTAs of at most 128 threads with 3 per SM (up to 170),
  * 2 for CTAs of at most 128 threads with 2 per SM (up to 255).  mode -1 (the default) uses the highest
