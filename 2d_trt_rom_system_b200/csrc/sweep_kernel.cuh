@@ -246,13 +246,15 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
   // takes the bottom inflow of column ipn, the producer must have finished that column in round nn - 1
   // (its local round (nn-1-prod)/NB), i.e. completed local step k'P + ipn + H - 1.  Bounded wait: false
   // when the producer did not get there within max_polls polls.
+  // Called by every lane of warp 0 with its own position; lane 0 is row 0 of the band (the lanes that read
+  // the wrap buffer are the slices of that row, at the same position), so its position decides.
   int seen = 0;
   auto band_wait = [&](int ipn, int nn) -> bool {
-    if (NB == 1 || nn <= 0 || nn >= t.nr || ipn < 0 || ipn >= nx) return true;
-    const int need = ((nn - 1 - prod) / NB) * t.P + ipn + t.H;
+    if (NB == 1) return true;
     int ok = 1;
-    if (lane == 0 && seen < need) {
-      for (unsigned k = 0;; ++k) {
+    if (lane == 0 && nn > 0 && nn < t.nr && ipn >= 0 && ipn < nx) {
+      const int need = ((nn - 1 - prod) / NB) * t.P + ipn + t.H;
+      for (unsigned k = 0; seen < need; ++k) {
         seen = ld_acquire_cluster(&band_prog);
         if (seen >= need) break;
         if (k >= a.max_polls) {
