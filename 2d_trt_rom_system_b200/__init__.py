@@ -4,7 +4,7 @@ jmc9/2D_TRT_ROM_System (drop-in for MODULE TRANSPORT_SOLVES and the QD-factor ro
 The compute path is libtrt_sweep.so (CUDA, sm_100a) behind the C ABI of include/trt_sweep.h; this
 package is its Python mirror plus the problem and quadrature generators used by tests and the bench.
 """
-from . import problems, quadrature, ranks, serving  # noqa: F401
+from . import problems, quadrature, ranks, serving, sharded  # noqa: F401
 from .api import (COLLAPSE_INTENSITIES, COLLAPSE_MG_EF, DMD_Calc, DMD_RECONSTRUCT, EGP_FV_NEWT, FMAP,  # noqa: F401
                   GENERATE_GRIDS_T, GENERATE_GRIDS_XY, GRIDMAP_GEN, GRIDMAP_GEN_BND, MAP_GRIDS, GQD_In_Calc, GREY_COEFS,
                   DMD_RECONSTRUCT_BCg, DMD_RECONSTRUCT_fg, POD_RECONSTRUCT_BCg, POD_RECONSTRUCT_fg, POD_TRUNCATE, RRANK_CALC,

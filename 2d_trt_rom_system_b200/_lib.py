@@ -141,6 +141,10 @@ SIGNATURES = {
     "trt_tstep_setup": (_i, [_P, _D, _D, _D, _D, _d, _d, _d, _d, _I, _D, _i, _d, _i]),
     "trt_tstep": (_i, [_P, _I, _D, _D]),
     "trt_tstep_set_law": (_i, [_P, _i]),
+    "trt_tstep_begin": (_i, [_P]),
+    "trt_tstep_sweep": (_i, [_P, _i]),
+    "trt_tstep_partials": (_i, [_P, ctypes.c_void_p]),
+    "trt_tstep_finish": (_i, [_P, ctypes.c_void_p, _i, _I, _D, _D]),
     "trt_get_temperature": (_i, [_P, _D]),
     "trt_put_temperature": (_i, [_P, _D]),
     "trt_strerror": (ctypes.c_char_p, [_i]),

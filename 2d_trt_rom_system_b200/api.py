@@ -712,6 +712,25 @@ class TransportSweep:
                                          float(Delt), iptr(bc), dptr(bt), int(conv_type), float(conv_ho),
                                          int(maxit_rte)), "trt_tstep_setup")
 
+    # group-split time step (sharded.ShardedTimeLoop): the phases of trt_tstep for a handle that holds a
+    # range of the instance's groups
+    def tstep_begin(self):
+        check(_lib.lib().trt_tstep_begin(self._h), "trt_tstep_begin")
+
+    def tstep_sweep(self, its):
+        check(_lib.lib().trt_tstep_sweep(self._h, int(its)), "trt_tstep_sweep")
+
+    def tstep_partials(self, buf):
+        """Group sums of the energy balance (3 n_x n_y doubles) into the device tensor `buf`."""
+        check(_lib.lib().trt_tstep_partials(self._h, ctypes.c_void_p(buf.data_ptr())), "trt_tstep_partials")
+
+    def tstep_finish(self, total, its):
+        """Temperature, material and convergence from the summed partials (device tensor `total`)."""
+        conv, tn, en = ctypes.c_int(0), ctypes.c_double(0), ctypes.c_double(0)
+        check(_lib.lib().trt_tstep_finish(self._h, ctypes.c_void_p(total.data_ptr()), int(its), ctypes.byref(conv),
+                                          ctypes.byref(tn), ctypes.byref(en)), "trt_tstep_finish")
+        return bool(conv.value), tn.value, en.value
+
     def tstep(self):
         """One backward-Euler time step; returns (outer iterations, T norm, E norm)."""
         its, tn, en = ctypes.c_int(0), ctypes.c_double(0), ctypes.c_double(0)

@@ -1115,6 +1115,46 @@ bool tstep_decide(trt_ctx* c, const unsigned long long* host, int its, double* t
   return tconv && econv;
 }
 
+// Group-partial time step (trt_tstep_partials / trt_tstep_finish): the energy balance from group sums that
+// the caller has added over every handle that holds a share of the groups.
+int tstep_partials_impl(trt_ctx* c, double* part) {
+  const size_t nxy = (size_t)c->nx * c->ny;
+  trt::meb_partial_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>(c->nx, c->ny, c->ng, c->ts_law,
+                                                                            c->dout.Eg_avg, c->d_kap64, c->d_T,
+                                                                            c->d_nu, c->comp_unit, c->c, part);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  return TRT_OK;
+}
+
+template <class Real>
+int tstep_finish_impl(trt_ctx* c, const double* sum, int its, int* conv_out, double* tn, double* en) {
+  const size_t nxy = (size_t)c->nx * c->ny;
+  trt::meb_finish_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>(c->nx, c->ny, c->ts_law, sum, c->d_Told,
+                                                                           c->d_cv, c->dt, c->ts_Kap0, c->comp_unit,
+                                                                           c->d_T, c->dout.E_avg);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  int rc = material_update_impl<Real>(c);
+  if (rc) return rc;
+  static const unsigned long long init[10] = {0, 0, 0, 0x7ff0000000000000ULL, 0, 0, 0, 0, 0x7ff0000000000000ULL, 0};
+  TRT_CUDA(cudaMemcpyAsync(c->d_conv, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+  trt::conv_reduce_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>((long long)nxy, c->d_T, c->d_Trt1,
+                                                                            c->d_Trt2, c->d_conv);
+  TRT_LAUNCHED();
+  trt::conv_reduce_kernel<<<grid_for((long long)nxy), 256, 0, c->stream>>>((long long)nxy, c->dout.E_avg, c->d_Ert1,
+                                                                            c->d_Ert2, c->d_conv + 5);
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
+  unsigned long long h[10];
+  TRT_CUDA(cudaMemcpyAsync(h, c->d_conv, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  TRT_CUDA(cudaStreamSynchronize(c->stream));
+  if ((rc = check_err(c))) return rc;
+  const bool conv = tstep_decide(c, h, its, tn, en);
+  if (conv_out) *conv_out = conv ? 1 : 0;
+  return TRT_OK;
+}
+
 template <class Real>
 int tstep_impl(trt_ctx* c, int* its_out, double* tnorm_out, double* enorm_out) {
   int rc = tstep_begin(c);
@@ -2021,6 +2061,39 @@ int trt_tstep_setup(trt_ctx* c, const double* Nu_g, const double* kappa_mult, co
 
 static_assert(TRT_LAW_FLECK_CUMMINGS == trt::kLawFleckCummings && TRT_LAW_CONFIG == trt::kLawConfig,
               "material law numbering");
+
+int trt_tstep_begin(trt_ctx* c) {
+  if (!c) return TRT_ERR_ARG;
+  if (!c->ts_ready || (!c->have_state && !c->swept)) return TRT_ERR_STATE;
+  return tstep_begin(c);
+}
+
+int trt_tstep_sweep(trt_ctx* c, int its) {
+  if (!c || its < 1) return TRT_ERR_ARG;
+  if (!c->ts_ready || (!c->have_state && !c->swept)) return TRT_ERR_STATE;
+  const unsigned flags = (its == 1 ? TRT_ROLL_STATE : 0u) | TRT_MOMENTS;
+  const bool reflective = c->ts_bc[0] > 0 || c->ts_bc[1] > 0 || c->ts_bc[2] > 0 || c->ts_bc[3] > 0;
+  int rc = c->prec == TRT_PREC_FP64 ? sweep_impl<double>(c, flags) : sweep_impl<float>(c, flags);
+  if (rc) return rc;
+  if (reflective)
+    rc = c->prec == TRT_PREC_FP64 ? bc_update_impl<double>(c, c->ts_bc, c->ts_Tb, c->comp_unit, c->ts_nu.data())
+                                  : bc_update_impl<float>(c, c->ts_bc, c->ts_Tb, c->comp_unit, c->ts_nu.data());
+  c->have_moments = true;
+  return rc;
+}
+
+int trt_tstep_partials(trt_ctx* c, double* part_device) {
+  if (!c || !part_device) return TRT_ERR_ARG;
+  if (!c->ts_ready || !c->have_moments) return TRT_ERR_STATE;
+  return tstep_partials_impl(c, part_device);
+}
+
+int trt_tstep_finish(trt_ctx* c, const double* sum_device, int its, int* converged, double* T_norm, double* E_norm) {
+  if (!c || !sum_device || its < 1) return TRT_ERR_ARG;
+  if (!c->ts_ready || !c->have_moments) return TRT_ERR_STATE;
+  return c->prec == TRT_PREC_FP64 ? tstep_finish_impl<double>(c, sum_device, its, converged, T_norm, E_norm)
+                                  : tstep_finish_impl<float>(c, sum_device, its, converged, T_norm, E_norm);
+}
 
 int trt_tstep_set_law(trt_ctx* c, int law) {
   if (!c || (law != trt::kLawFleckCummings && law != trt::kLawConfig)) return TRT_ERR_ARG;

@@ -151,7 +151,7 @@ __global__ void meb_law_kernel(int nx, int ny, int ng, const double* __restrict_
   const double fp = 4.0 * 3.141592653589793;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nxy; k += (long long)gridDim.x * blockDim.x) {
     const double ts = T[k];
-    double num = (cv[k] * T_old[k]) / Delt, den = cv[k] / Delt;
+    double num = 0.0, den = 0.0;
     for (int g = 0; g < ng; ++g) {
       const double kap = kapE[k + nxy * g];
       const double B = ts_bg_planck(ts, nu[g], nu[g + 1], comp_unit);
@@ -159,7 +159,66 @@ __global__ void meb_law_kernel(int nx, int ny, int ng, const double* __restrict_
       num = num + kap * (((c * Eg[k + nxy * g]) - (fp * B)) + ((fp * dB) * ts));
       den = den + (fp * kap) * dB;
     }
-    T[k] = num / den;
+    T[k] = (((cv[k] * T_old[k]) / Delt) + num) / ((cv[k] / Delt) + den);
+  }
+}
+
+// Group-partial form of the energy balances, for time loops whose groups are split over several handles
+// (ranks of a multi-GPU run, or group slabs streamed through one device): per cell the group sums each
+// balance needs, over this handle's groups, into part[0..2][cell]; the sums over all handles then give the
+// new temperature in meb_finish_kernel.  Fleck-Cummings (MEB_SOLVE): {sum KapE Eg, sum Eg, sum Eg};
+// configurations' law: {sum KapE (c Eg - 4 pi Bg + 4 pi Bg' T*), sum 4 pi KapE Bg', sum Eg}.  The third is
+// the handle's part of the transport E (HO_E_avg), whose sum the convergence test reads.
+__global__ void meb_partial_kernel(int nx, int ny, int ng, int law, const double* __restrict__ Eg,
+                                   const double* __restrict__ kapE, const double* __restrict__ T,
+                                   const double* __restrict__ nu, double comp_unit, double c,
+                                   double* __restrict__ part) {
+  const long long nxy = (long long)nx * ny;
+  const double fp = 4.0 * 3.141592653589793;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nxy; k += (long long)gridDim.x * blockDim.x) {
+    double p0 = 0.0, p1 = 0.0, p2 = 0.0;
+    const double ts = T[k];
+    for (int g = 0; g < ng; ++g) {
+      const double e = Eg[k + nxy * g];
+      const double kap = kapE[k + nxy * g];
+      if (law == kLawConfig) {
+        const double B = ts_bg_planck(ts, nu[g], nu[g + 1], comp_unit);
+        const double dB = ts_bg_planck_dT(ts, nu[g], nu[g + 1], comp_unit);
+        p0 = p0 + kap * (((c * e) - (fp * B)) + ((fp * dB) * ts));
+        p1 = p1 + (fp * kap) * dB;
+      } else {
+        p0 = p0 + kap * e;
+        p1 = p1 + e;
+      }
+      p2 = p2 + e;
+    }
+    part[k] = p0;
+    part[k + nxy] = p1;
+    part[k + 2 * nxy] = p2;
+  }
+}
+
+// The new temperature from the group sums over all handles (the expressions of meb_kernel and
+// meb_law_kernel with their group sums replaced by the totals), and E_avg = the summed transport E.
+__global__ void meb_finish_kernel(int nx, int ny, int law, const double* __restrict__ sum,
+                                  const double* __restrict__ T_old, const double* __restrict__ cv, double Delt,
+                                  double Kap0, double comp_unit, double* __restrict__ T, double* __restrict__ E_avg) {
+  const long long nxy = (long long)nx * ny;
+  const double pi = 3.141592653589793;
+  const double c2h3 = (kTsC * kTsC) * ((kTsH * kTsH) * kTsH);
+  const double e2 = kTsErg * kTsErg;
+  const double lin = (((8.0 * pi) * Delt) * Kap0) / (e2 * e2);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nxy; k += (long long)gridDim.x * blockDim.x) {
+    const double p0 = sum[k], p1 = sum[k + nxy];
+    if (law == kLawConfig) {
+      T[k] = (((cv[k] * T_old[k]) / Delt) + p0) / ((cv[k] / Delt) + p1);
+    } else {
+      const double kb = p0 / p1;
+      const double cvk = cv[k];
+      const double coef = c2h3 / (((c2h3 * cvk) * comp_unit) + lin);
+      T[k] = (coef * ((((Delt * kTsC) * kb) * p1) + cvk * T_old[k])) * comp_unit;
+    }
+    E_avg[k] = sum[k + 2 * nxy];
   }
 }
 

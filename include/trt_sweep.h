@@ -416,6 +416,23 @@ int trt_tstep_setup(trt_ctx* ctx, const double* Nu_g, const double* kappa_mult, 
                     double Kap0, double Comp_Unit, double c, double Delt, const int* BC_Type, const double* bcT,
                     int conv_type, double conv_ho, int maxit_rte);
 int trt_tstep(trt_ctx* ctx, int* rt_its, double* T_norm, double* E_norm);
+/* The same time step with the groups split over several handles (the ranks of a multi-GPU run, each with
+ * its own group range, or group slabs of one instance streamed through one device).  The only coupling
+ * between groups is in the energy balance (MEB_SOLVE, UPDATES.f08:185-230, or its T^4-linearised form) and
+ * in the convergence test on the transport E (ALGORITHMS.f08:816-818), both per-cell sums over groups.
+ * Per outer iteration its = 1, 2, ... every handle runs
+ *   trt_tstep_sweep(its)        sweep (rolling I_crn_old <- I_crn when its == 1) + moments + RT_BC_UPDATE;
+ *   trt_tstep_partials(part)    its group sums, 3 n_x n_y doubles in device memory, on the handle's stream;
+ * the caller adds the partials of all handles (an all-reduce across ranks), and every handle then runs
+ *   trt_tstep_finish(sum, its, &converged, &T_norm, &E_norm)
+ * which forms the temperature from the sums (identical on every handle), the material of its own groups
+ * and the convergence test; E_avg becomes the summed transport E.  trt_tstep_begin starts a step
+ * (Temp_old <- Temp).  With one handle holding every group, this is trt_tstep. */
+int trt_tstep_begin(trt_ctx* ctx);
+int trt_tstep_sweep(trt_ctx* ctx, int its);
+int trt_tstep_partials(trt_ctx* ctx, double* part_device);
+int trt_tstep_finish(trt_ctx* ctx, const double* sum_device, int its, int* converged, double* T_norm,
+                     double* E_norm);
 /* Material law of the time loops (trt_tstep, trt_batch_tstep, trt_mlqd_step).
  *   TRT_LAW_FLECK_CUMMINGS (default): the reference's material, KapE = kapB_calc(T) * Kappa_Mult
  *     (TEMP_FUNCTIONS.f08:11-32, UPDATES.f08:130-150) and MEB_SOLVE (UPDATES.f08:185-230).

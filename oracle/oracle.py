@@ -35,6 +35,8 @@ _SIG = {
     "oracle_meb_solve": (_i, [_i, _i, _i, _D, _D, _D, _D, _d, _D, _d, _d]),
     "oracle_material_update_law": (_i, [_i, _i, _i, _D, _D, _D, _d, _D, _D, _D]),
     "oracle_meb_solve_law": (_i, [_i, _i, _i, _D, _D, _D, _D, _d, _D, _D, _d, _d]),
+    "oracle_meb_partial": (_i, [_i, _i, _i, _i, _i, _i, _D, _D, _D, _D, _d, _d, _D]),
+    "oracle_meb_finish": (_i, [_i, _i, _i, _D, _D, _D, _d, _d, _d, _D, _D]),
     "oracle_convergence": (_i, [_i, _d, _D, _D, _D, _i, _i, _D, _D]),
     "oracle_old_mgqd_coefs": (_i, [_i, _i, _i] + [_D] * 17 + [_d, _d, _d] + [_D] * 5),
     "oracle_mloqd_fv": (_i, [_i, _i, _i] + [_D] * 29 + [_d, _d, _d, _i, _i] + [_D] * 10 + [_I, _d, _d, _d]),
@@ -250,6 +252,28 @@ def meb_solve_law(Temp, Temp_old, Eg_HO, KapE, Delt, cV, Nu_g, comp_unit, c):
                                     _p(F(np.broadcast_to(cV, (nx, ny)))), _p(F(Nu_g)), float(comp_unit), float(c))
     assert rc == 0
     return T
+
+
+def meb_partial(Eg_HO, KapE, Temp, Nu_g, comp_unit, c, g0, g1, law=0):
+    """Group sums over groups [g0, g1) of the energy balance, (nx, ny, 3) Fortran-ordered: the split form of
+    MEB_SOLVE (law 0) or of the configurations' balance (law 1)."""
+    nx, ny, ng = Eg_HO.shape
+    part = zeros(nx, ny, 3)
+    rc = lib().oracle_meb_partial(nx, ny, ng, int(g0), int(g1), int(law), _p(F(Eg_HO)), _p(F(KapE)), _p(F(Temp)),
+                                  _p(F(Nu_g)), float(comp_unit), float(c), _p(part))
+    assert rc == 0
+    return part
+
+
+def meb_finish(sums, Temp_old, cV, Delt, Kap0, comp_unit, law=0):
+    """Temperature and transport E from the group sums over all ranges (sums: (nx, ny, 3) Fortran-ordered)."""
+    nx, ny = Temp_old.shape
+    sums = F(sums)
+    T, E = zeros(nx, ny), zeros(nx, ny)
+    rc = lib().oracle_meb_finish(nx, ny, int(law), _p(sums), _p(F(Temp_old)), _p(F(np.broadcast_to(cV, (nx, ny)))),
+                                 float(Delt), float(Kap0), float(comp_unit), _p(T), _p(E))
+    assert rc == 0
+    return T, E
 
 
 def convergence(conv_type, eps, x, x_old, x_old2, its):

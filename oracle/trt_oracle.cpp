@@ -851,7 +851,7 @@ int oracle_meb_solve_law(int nx, int ny, int ng, double* Temp, const double* Eg_
     for (int i = 0; i < nx; ++i) {
       const size_t k = (size_t)i + (size_t)nx * j;
       const double ts = Temp[k];
-      double num = (cV[k] * Temp_old[k]) / Delt, den = cV[k] / Delt;
+      double num = 0.0, den = 0.0;
       for (int g = 0; g < ng; ++g) {
         const double kap = KapE[k + nxy * g];
         const double B = bg_planck(ts, Nu_g[g], Nu_g[g + 1], Comp_Unit);
@@ -859,8 +859,62 @@ int oracle_meb_solve_law(int nx, int ny, int ng, double* Temp, const double* Eg_
         num = num + kap * (((c * Eg_HO[k + nxy * g]) - (fp * B)) + ((fp * dB) * ts));
         den = den + (fp * kap) * dB;
       }
-      Temp[k] = num / den;
+      Temp[k] = (((cV[k] * Temp_old[k]) / Delt) + num) / ((cV[k] / Delt) + den);
     }
+  return 0;
+}
+
+// The energy balances split over group ranges (the device's trt_tstep_partials / trt_tstep_finish):
+// per cell the group sums over groups [g0, g1) of the arrays (nx, ny, ng) ...
+//   law 0 (MEB_SOLVE): {sum KapE Eg, sum Eg, sum Eg};  law 1: {sum KapE (c Eg - 4 pi Bg + 4 pi Bg' T*),
+//   sum 4 pi KapE Bg', sum Eg}   -> part (3, nx, ny)
+// ... and the temperature from the sums over all ranges (and E_avg = the summed transport E).
+int oracle_meb_partial(int nx, int ny, int ng, int g0, int g1, int law, const double* Eg_HO, const double* KapE,
+                       const double* Temp, const double* Nu_g, double Comp_Unit, double c, double* part) {
+  (void)ng;
+  const double fp = 4.0 * (4.0 * std::atan(1.0));
+  const size_t nxy = (size_t)nx * ny;
+  for (size_t k = 0; k < nxy; ++k) {
+    double p0 = 0.0, p1 = 0.0, p2 = 0.0;
+    const double ts = Temp[k];
+    for (int g = g0; g < g1; ++g) {
+      const double e = Eg_HO[k + nxy * g], kap = KapE[k + nxy * g];
+      if (law == 1) {
+        const double B = bg_planck(ts, Nu_g[g], Nu_g[g + 1], Comp_Unit);
+        const double dB = bg_planck_dT(ts, Nu_g[g], Nu_g[g + 1], Comp_Unit);
+        p0 = p0 + kap * (((c * e) - (fp * B)) + ((fp * dB) * ts));
+        p1 = p1 + (fp * kap) * dB;
+      } else {
+        p0 = p0 + kap * e;
+        p1 = p1 + e;
+      }
+      p2 = p2 + e;
+    }
+    part[k] = p0;
+    part[k + nxy] = p1;
+    part[k + 2 * nxy] = p2;
+  }
+  return 0;
+}
+
+int oracle_meb_finish(int nx, int ny, int law, const double* sum, const double* Temp_old, const double* cV,
+                      double Delt, double Kap0, double Comp_Unit, double* Temp, double* E_avg) {
+  const double pi = 4.0 * std::atan(1.0);
+  const double c2h3 = (kC * kC) * ((kH * kH) * kH);
+  const double e2 = kErg * kErg;
+  const double lin = (((8.0 * pi) * Delt) * Kap0) / (e2 * e2);
+  const size_t nxy = (size_t)nx * ny;
+  for (size_t k = 0; k < nxy; ++k) {
+    const double p0 = sum[k], p1 = sum[k + nxy];
+    if (law == 1) {
+      Temp[k] = (((cV[k] * Temp_old[k]) / Delt) + p0) / ((cV[k] / Delt) + p1);
+    } else {
+      const double kb = p0 / p1;
+      const double coef = c2h3 / (((c2h3 * cV[k]) * Comp_Unit) + lin);
+      Temp[k] = (coef * ((((Delt * kC) * kb) * p1) + cV[k] * Temp_old[k])) * Comp_Unit;
+    }
+    E_avg[k] = sum[k + 2 * nxy];
+  }
   return 0;
 }
 
