@@ -125,6 +125,7 @@ SIGNATURES = {
     "trt_device_output": (_P, [_P, ctypes.c_char_p]),
     "trt_set_register_mode": (_i, [_P, _i]),
     "trt_set_bands": (_i, [_P, _i]),
+    "trt_batch_set_persistent": (_i, [_P, _i]),
     "trt_set_inplace": (_i, [_P, _i]),
     "trt_state_bytes": (ctypes.c_size_t, [_P]),
     "trt_bind_state": (_i, [_P, ctypes.c_void_p, ctypes.c_size_t]),

@@ -894,6 +894,10 @@ class Batch:
     def __exit__(self, *exc):
         self.close()
 
+    def set_persistent(self, on=True):
+        """Persistent work-queue launches (default) or one CTA per sweep; results are identical."""
+        check(_lib.lib().trt_batch_set_persistent(self._b, 1 if on else 0), "trt_batch_set_persistent")
+
     def sweep(self, roll=False, moments=True, sync=True):
         flags = (_lib.TRT_ROLL_STATE if roll else 0) | (_lib.TRT_MOMENTS if moments else 0)
         check(_lib.lib().trt_batch_sweep(self._b, flags), "trt_batch_sweep")

@@ -24,6 +24,12 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
                : "memory");
 }
 
+// Invalidate an mbarrier whose phases have all completed, so that its shared memory can be initialised
+// again (the persistent sweep reuses it for the next task).
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // Global -> shared bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned),
 // completion signalled on `bar` as transaction bytes.
 __device__ __forceinline__ void tma_bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {

@@ -132,7 +132,7 @@ __device__ __forceinline__ int slice_reduce_scatter(double (&v)[16], int s, bool
 // The sweep of one CTA: (group, quadrant, direction split) number `bid` of the instance described by
 // `a` (blockIdx.x for a single-instance launch; the instance-local number in a batched launch).
 template <class Real, int S, int D, bool SRC_FULL>
-__device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const int bid) {
+__device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const int bid) {
   constexpr bool kLeanFP32 = sizeof(Real) == 4;
   constexpr int R = 32 / S;
   constexpr int NV = 16 / (int)sizeof(Real);
@@ -829,6 +829,11 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
   }
   // no band CTA leaves while another may still write into its shared memory
   if (NB > 1) cluster_sync_all();
+  // every copy has landed (or the bounded drain gave up): the barriers can be set up again by a next task
+  if (threadIdx.x == 0 && !timed_out)
+    for (int k = 0; k < stages; ++k) mbar_inval(&mbar[k]);
+  __syncthreads();
+  return timed_out;
 }
 
 // MAXT/MINB: 512/1 fits every tiling (at most 128 registers per thread); 128/3 and 128/2 are the
@@ -837,6 +842,36 @@ __device__ __forceinline__ void scb_sweep_body(const SweepArgs<Real>& a, const i
 template <class Real, int S, int D, bool SRC_FULL, int MAXT = 512, int MINB = 1>
 __global__ void __launch_bounds__(MAXT, MINB) scb_sweep_kernel(const SweepArgs<Real> a) {
   scb_sweep_body<Real, S, D, SRC_FULL>(a, blockIdx.x);
+}
+
+// Persistent form of the batched sweep: a grid of at most one wave of resident CTAs drains the queue of
+// (instance, group, quadrant, split) sweeps, each CTA taking the next task from a global counter (reset
+// before the launch) until none is left; tasks are ordered as the first-CTA table orders the instances
+// (largest sweeps first).  One CTA per task (no band CTAs).  A CTA whose sweep timed out stops.
+template <class Real, int S, int D, bool SRC_FULL, int MAXT = 512, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB) scb_sweep_queue_kernel(const SweepArgs<Real>* __restrict__ args,
+                                                              const int* __restrict__ first, int n, int total,
+                                                              int* queue) {
+  __shared__ SweepArgs<Real> sa;
+  __shared__ int sbid, stask;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      stask = atomicAdd(queue, 1);
+      if (stask < total) {
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (first[mid] <= stask) lo = mid;
+          else hi = mid - 1;
+        }
+        sa = args[lo];
+        sbid = stask - first[lo];
+      }
+    }
+    __syncthreads();
+    if (stask >= total) break;
+    if (scb_sweep_body<Real, S, D, SRC_FULL>(sa, sbid)) break;
+  }
 }
 
 // One launch over the CTAs of several instances (same precision, slices, directions per lane, warps

@@ -212,6 +212,43 @@ cudaError_t launch_banded(K k, int NB, int grid, int block, size_t smem, cudaStr
 }
 
 template <class Real>
+using SweepQueueKernel = void (*)(const trt::SweepArgs<Real>*, const int*, int, int, int*);
+
+// The persistent (work-queue) batched sweep of a configuration (null if none); level 1 as above.
+template <class Real>
+SweepQueueKernel<Real> sweep_queue_kernel_for(const KernelCfg& kc, bool src_full, int level = 0) {
+#define TRT_SWEEP_CASE(S_, D_)                                                                         \
+  if (kc.S == S_ && kc.D == D_)                                                                        \
+    return src_full ? trt::scb_sweep_queue_kernel<Real, S_, D_, true>                                  \
+                    : (level == 1 ? trt::scb_sweep_queue_kernel<Real, S_, D_, false, 128, 3>           \
+                                  : trt::scb_sweep_queue_kernel<Real, S_, D_, false>);
+  TRT_SWEEP_CASE(1, 2)
+  TRT_SWEEP_CASE(1, 4)
+  TRT_SWEEP_CASE(2, 2)
+  TRT_SWEEP_CASE(2, 3)
+  TRT_SWEEP_CASE(2, 5)
+  TRT_SWEEP_CASE(2, 9)
+  TRT_SWEEP_CASE(4, 1)
+  TRT_SWEEP_CASE(4, 2)
+  TRT_SWEEP_CASE(4, 3)
+  TRT_SWEEP_CASE(4, 5)
+  TRT_SWEEP_CASE(4, 6)
+  TRT_SWEEP_CASE(4, 9)
+  TRT_SWEEP_CASE(8, 1)
+  TRT_SWEEP_CASE(8, 2)
+  TRT_SWEEP_CASE(8, 3)
+  TRT_SWEEP_CASE(8, 4)
+  TRT_SWEEP_CASE(8, 5)
+  TRT_SWEEP_CASE(16, 1)
+  TRT_SWEEP_CASE(16, 2)
+  TRT_SWEEP_CASE(16, 3)
+  TRT_SWEEP_CASE(32, 1)
+  TRT_SWEEP_CASE(32, 2)
+#undef TRT_SWEEP_CASE
+  return nullptr;
+}
+
+template <class Real>
 cudaError_t launch_sweep(const KernelCfg& kc, bool src_full, int level, int grid, int block, size_t smem,
                          cudaStream_t st, const trt::SweepArgs<Real>& a) {
   SweepKernel<Real> k = sweep_kernel_for<Real>(kc, src_full, level);
@@ -1194,6 +1231,9 @@ struct trt_batch {
   size_t d_args_cap = 0;
   int* d_first = nullptr;                    // first CTA of each handle in its group's launch
   size_t d_first_cap = 0;
+  bool persistent = true;                    // classes without band CTAs: one wave of CTAs drains a task queue
+  int* d_queue = nullptr;                    // task counter of each launch group
+  size_t d_queue_cap = 0;
   unsigned char* h_args = nullptr;           // pinned staging of d_args / d_first
   size_t h_args_cap = 0;
   unsigned long long* h_norms = nullptr;     // pinned, 10 convergence values per handle
@@ -1214,7 +1254,7 @@ struct StreamSwap {
 
 template <class Real>
 int batch_group_launch(trt_batch* b, std::vector<trt_ctx*>& grp, size_t args_off, size_t first_off, size_t done,
-                       cudaStream_t gs) {
+                       cudaStream_t gs, size_t qslot) {
   // largest CTAs first: the block scheduler then starts the long sweeps before the short ones
   std::stable_sort(grp.begin(), grp.end(), [](const trt_ctx* x, const trt_ctx* y) {
     return (long long)x->t.Tb * x->t.D > (long long)y->t.Tb * y->t.D;
@@ -1245,6 +1285,24 @@ int batch_group_launch(trt_batch* b, std::vector<trt_ctx*>& grp, size_t args_off
         total <= (long long)per * sm_count())
       level = 1;
     cudaGetLastError();
+  }
+  if (b->persistent && grp[0]->t.NB == 1) {
+    // one wave of resident CTAs that drains the (instance, group, quadrant, split) queue in the table's order
+    SweepQueueKernel<Real> kq = sweep_queue_kernel_for<Real>(grp[0]->kc, grp[0]->use_srcfull, level);
+    if (!kq) return TRT_ERR_UNSUPPORTED;
+    cudaFuncSetAttribute(kq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kq, 32 * grp[0]->t.W, smem) != cudaSuccess || per < 1) {
+      cudaGetLastError();
+      per = 1;
+    }
+    const long long grid = std::min<long long>(total, (long long)per * sm_count());
+    int* q = b->d_queue + qslot;
+    TRT_CUDA(cudaMemsetAsync(q, 0, sizeof(int), gs));
+    kq<<<(unsigned)grid, 32 * grp[0]->t.W, smem, gs>>>(da, df, (int)grp.size(), (int)total, q);
+    TRT_LAUNCHED();
+    TRT_CUDA(cudaGetLastError());
+    return TRT_OK;
   }
   SweepBatchKernel<Real> k = sweep_batch_kernel_for<Real>(grp[0]->kc, grp[0]->use_srcfull, level);
   if (!k) return TRT_ERR_UNSUPPORTED;
@@ -1314,6 +1372,16 @@ int batch_sweep_launch(trt_batch* b, const std::vector<int>& act, const std::vec
     }
     b->d_first_cap = act.size() * sizeof(int);
   }
+  if (groups.size() > b->d_queue_cap) {
+    if (b->d_queue) cudaFree(b->d_queue);
+    if (cudaMalloc((void**)&b->d_queue, groups.size() * sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      b->d_queue = nullptr;
+      b->d_queue_cap = 0;
+      return TRT_ERR_NOMEM;
+    }
+    b->d_queue_cap = groups.size();
+  }
   while (b->gstreams.size() < groups.size()) {
     cudaStream_t st;
     cudaEvent_t ev;
@@ -1328,8 +1396,8 @@ int batch_sweep_launch(trt_batch* b, const std::vector<int>& act, const std::vec
     cudaStream_t gs = b->gstreams[g];
     TRT_CUDA(cudaStreamWaitEvent(gs, b->start, 0));
     const size_t args_off = done * asz, first_off = args_bytes + done * sizeof(int);
-    int rc = keys[g].prec == TRT_PREC_FP64 ? batch_group_launch<double>(b, groups[g], args_off, first_off, done, gs)
-                                           : batch_group_launch<float>(b, groups[g], args_off, first_off, done, gs);
+    int rc = keys[g].prec == TRT_PREC_FP64 ? batch_group_launch<double>(b, groups[g], args_off, first_off, done, gs, g)
+                                           : batch_group_launch<float>(b, groups[g], args_off, first_off, done, gs, g);
     if (rc) return rc;
     done += groups[g].size();
     TRT_CUDA(cudaEventRecord(b->gevents[g], gs));
@@ -1493,6 +1561,7 @@ void trt_batch_destroy(trt_batch* b) {
   if (b->h_err) cudaFreeHost(b->h_err);
   if (b->start) cudaEventDestroy(b->start);
   if (b->d_args) cudaFree(b->d_args);
+  if (b->d_queue) cudaFree(b->d_queue);
   if (b->d_first) cudaFree(b->d_first);
   if (b->h_args) cudaFreeHost(b->h_args);
   if (b->h_norms) cudaFreeHost(b->h_norms);
@@ -1504,6 +1573,12 @@ void trt_batch_destroy(trt_batch* b) {
 int trt_batch_sweep(trt_batch* b, unsigned flags) {
   if (!b) return TRT_ERR_ARG;
   return batch_sweep_impl(b, flags);
+}
+
+int trt_batch_set_persistent(trt_batch* b, int on) {
+  if (!b || (on != 0 && on != 1)) return TRT_ERR_ARG;
+  b->persistent = on == 1;
+  return TRT_OK;
 }
 
 int trt_batch_sync(trt_batch* b) {

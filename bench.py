@@ -74,6 +74,8 @@ def parse():
                    help="use the library's default tiling instead of trt_autotune")
     p.add_argument("--mgqd", type=int, default=3,
                    help="timed low-order MGQD solves (MLOQD_FV) on the configuration's grid and groups; 0 skips")
+    p.add_argument("--c4", type=int, default=0,
+                   help="run only config 4 (1024^2, 64 groups, S16, in-place FP32 state) for this many time steps")
     p.add_argument("--mgqd-only", action="store_true",
                    help="run only the low-order MGQD leg (--mgqd solves) and print its JSON object")
     p.add_argument("--mlqd-steps", type=int, default=2,
@@ -389,6 +391,81 @@ def run_pod(pkg, torch, prob, nt, cpu_groups=4):
     except Exception as exc:   # the CPU figure is context, not the measurement
         r["cpu_baseline"] = {"error": repr(exc)}
     return r
+
+
+def run_config4(pkg, torch, steps, snapshots=True, n=1024):
+    """Config 4: 1024^2 cells, 64 groups, S16 (9.66e9 updates per sweep), 8 material rectangles (seed 4),
+    mixed precision.  The FP32 corner state alone is 155 GB, so the handle sweeps it in place (one state
+    buffer); each time step is one sweep of the transport-only loop (trt_tstep with one outer iteration:
+    sweep, moments, the configurations' energy balance, material update).  With `snapshots`, the FP32
+    cell-average angular intensity of each 8-group slab is derived from the state and streamed to pinned
+    host memory (38.7 GB per step), the copies overlapping the next slab's snapshot kernel."""
+    prob = pkg.problems.config4(n=n)
+    ts = pkg.problems.config_timestep_setup(prob)
+    ox, oy, w = prob.directions()
+    upd = prob.updates_per_sweep()
+    out = {"workload": f"C4: {prob.nx}x{prob.ny} cells, {prob.ng} log-spaced groups, {prob.quad} ({prob.nm} "
+                       f"directions), 8 seeded material rectangles", "updates_per_sweep": upd,
+           "step": "one sweep of the transport-only loop per time step (trt_tstep, maxit_rte 1), in-place FP32 state"}
+    s = pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng, precision="mixed")
+    try:
+        s.set_inplace(True)
+        s.init_state(ts.Tini_eV, list(ts.bcT_eV), pkg.problems.COMP_UNIT, ts.nu_eV)
+        s.tstep_setup(ts.nu_eV, ts.kappa_mult, ts.cv, np.full((prob.nx, prob.ny), ts.Tini_eV), ts.Kap0,
+                      pkg.problems.COMP_UNIT, pkg.problems.C_LIGHT, ts.dt, bcT=ts.bcT_eV, conv_type=2, conv_ho=0.0,
+                      maxit_rte=1, law=1)
+        free, total = torch.cuda.mem_get_info()
+        out["state_gb"] = s.state_bytes() / 1e9
+        out["device_gb_used"] = (total - free) / 1e9
+        out["tiling"] = s.tiling()
+        lat = []
+        for _ in range(steps):
+            s.sync()
+            t0 = time.perf_counter()
+            s.tstep()
+            s.sync()
+            lat.append(time.perf_counter() - t0)
+        T = s.temperature()
+        out["step_s"] = lat
+        out["updates_per_s"] = upd * len(lat) / sum(lat)
+        ms_k, _ = time_resident(pkg, torch, s, 3, 1, pkg._lib.TRT_ROLL_STATE)   # the sweep kernel alone
+        peak, kind = peaks()
+        B = bytes_per_update(prob.nm, "fp32")
+        out["roofline"] = {"kernel": "scb_sweep_kernel<float>", "kernel_ms": ms_k, "bytes_per_update": B,
+                           "achieved": upd * B / (ms_k * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                           "frac": upd * B / (ms_k * 1e-3) / 1e9 / peak, "peak_source": f"{kind} hbm_gbs"}
+        out["T_min_max_eV"] = [float(T.min()), float(T.max())]
+        if snapshots:
+            slab = 8
+            per = prob.nx * prob.ny * prob.nm * slab
+            dev = [torch.empty(per, dtype=torch.float32, device="cuda") for _ in range(2)]
+            host = [torch.empty(per, dtype=torch.float32, pin_memory=True) for _ in range(2)]
+            copy = torch.cuda.Stream()
+            hs = torch.cuda.ExternalStream(s.stream())
+            ev = [torch.cuda.Event() for _ in range(2)]
+            s.sync()
+            t0 = time.perf_counter()
+            for k, g0 in enumerate(range(0, prob.ng, slab)):
+                b = k % 2
+                if k >= 2:
+                    ev[b].synchronize()   # the copy out of this buffer two slabs ago is done
+                s.snapshot_angular_groups(g0, slab, dev[b].data_ptr())
+                e = torch.cuda.Event()
+                e.record(hs)
+                copy.wait_event(e)
+                with torch.cuda.stream(copy):
+                    host[b].copy_(dev[b], non_blocking=True)
+                ev[b].record(copy)
+            copy.synchronize()
+            snap_s = time.perf_counter() - t0
+            nbytes = prob.nx * prob.ny * prob.nm * prob.ng * 4
+            out["snapshot"] = {"bytes": nbytes, "seconds": snap_s, "gb_per_s": nbytes / snap_s / 1e9,
+                               "path": "trt_snapshot_angular_groups per 8-group slab into two device buffers, "
+                                       "copied to pinned host memory on a copy stream"}
+            out["step_with_snapshot_s"] = float(np.median(lat)) + snap_s
+    finally:
+        s.close()
+    return out
 
 
 def run_serving(pkg, window_s, rate=200.0, budget_gb=120.0):
@@ -729,6 +806,12 @@ def main():
         return run_profile(args)
     if args.tiling_sweep:
         return run_tiling_sweep(args)
+    if args.c4:
+        import torch
+        torch.cuda.set_device(0)
+        pkg, _ = build_problem(args.config)
+        print(json.dumps({"config4": run_config4(pkg, torch, max(1, args.c4))}))
+        return 0
     if args.mgqd_only:
         pkg, prob = build_problem(args.config, args.n, args.groups)
         print(json.dumps(run_mgqd(pkg, max(1, args.mgqd), prob.nx, prob.ng, cpu=not args.no_cpu_baseline)))

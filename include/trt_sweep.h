@@ -707,6 +707,11 @@ trt_batch* trt_batch_create(trt_ctx* const* handles, int n, int* status);
 void trt_batch_destroy(trt_batch* batch);
 int trt_batch_sweep(trt_batch* batch, unsigned flags);
 int trt_batch_sync(trt_batch* batch);
+/* Launch form of the batched sweep.  on = 1 (default): for each tiling class without band CTAs, one
+ * persistent launch of at most one wave of resident CTAs that take (instance, group, quadrant, split)
+ * sweeps from a device work queue, largest instances first, until it is empty.  on = 0: one CTA per sweep,
+ * drained by the block scheduler.  Results are bit-identical either way. */
+int trt_batch_set_persistent(trt_batch* batch, int on);
 int trt_batch_tstep(trt_batch* batch, int* rt_its, double* T_norms, double* E_norms);
 
 /* Message for a TRT_ERR_* code. */

@@ -22,7 +22,8 @@ def _resident(k, nx, ny, G, quad, prec):
     return s
 
 
-def test_batched_sweep_matches_single_sweeps():
+@pytest.mark.parametrize("persistent", [True, False], ids=["queue", "grid"])
+def test_batched_sweep_matches_single_sweeps(persistent):
     alone, batched = [], []
     for k, sh in enumerate(SHAPES):
         with _resident(k, *sh) as s:
@@ -34,6 +35,7 @@ def test_batched_sweep_matches_single_sweeps():
     hs[2].put_state(_state_of(2))
     try:
         with pkg.Batch(hs) as b:
+            b.set_persistent(persistent)
             b.sweep(roll=True)
             b.sweep(roll=False)
         for s in hs:
