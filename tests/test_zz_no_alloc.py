@@ -35,9 +35,10 @@ def existing_entry_point(d):
     return out
 
 
-def no_alloc_entry_point(torch, d, sweep):
-    """Device copies (allocated here, by the caller) of the arrays TRANSPORT_SCB used and produced."""
-    nx, ny, nm, ng = len(d["Delx"]), len(d["Dely"]), len(d["Omega_x"]), d["KapE_in"].shape[2]
+def device_arrays(torch, d, sweep):
+    """Device copies (allocated here, by the caller) of the arrays TRANSPORT_SCB used and produced, and the
+    outputs (norms and their locations)."""
+    ng = d["KapE_in"].shape[2]
     dev = lambda a, dt=torch.float64: torch.from_numpy(np.ascontiguousarray(np.asarray(a).ravel(order="F"))).to(
         device="cuda", dtype=dt)
     ins = [dev(sweep["I_crn"]), dev(sweep["Ic_edgV"]), dev(sweep["Ic_edgH"]), dev(d["Omega_x"]), dev(d["Omega_y"]),
@@ -45,6 +46,12 @@ def no_alloc_entry_point(torch, d, sweep):
     res = torch.zeros(4 * ng * 5, dtype=torch.float64, device="cuda")
     lx = torch.full((4 * ng * 5,), LOC0, dtype=torch.int32, device="cuda")
     ly = torch.full((4 * ng * 5,), LOC0, dtype=torch.int32, device="cuda")
+    return ins, res, lx, ly
+
+
+def call(torch, d, arrays):
+    nx, ny, nm, ng = len(d["Delx"]), len(d["Dely"]), len(d["Omega_x"]), d["KapE_in"].shape[2]
+    ins, res, lx, ly = arrays
     stream = torch.cuda.current_stream()
     rc = pkg.lib().trt_transport_residual_noalloc(nx, ny, nm, ng, *[ctypes.c_void_p(t.data_ptr()) for t in ins],
                                                   float(d["c"]), float(d["dt"]), ctypes.c_void_p(res.data_ptr()),
@@ -52,6 +59,13 @@ def no_alloc_entry_point(torch, d, sweep):
                                                   ctypes.c_void_p(stream.cuda_stream))
     assert rc == 0, pkg.lib().trt_strerror(rc)
     torch.cuda.synchronize()
+
+
+def no_alloc_entry_point(torch, d, sweep):
+    ng = d["KapE_in"].shape[2]
+    arrays = device_arrays(torch, d, sweep)
+    call(torch, d, arrays)
+    _, res, lx, ly = arrays
     shape = (4, ng, 5)
     return (res.cpu().numpy().reshape(shape, order="F"), lx.cpu().numpy().reshape(shape, order="F"),
             ly.cpu().numpy().reshape(shape, order="F"))
@@ -79,3 +93,16 @@ def test_no_alloc_rejects_problems_beyond_its_scratch():
     rc = pkg.lib().trt_transport_residual_noalloc(2, 2, 8, 8193, *[p] * 11, 1.0, 1.0, p, p, p, None)
     assert rc == pkg._lib.TRT_ERR_SCRATCH
     assert "scratch" in pkg.lib().trt_strerror(rc).decode()
+
+
+def test_no_alloc_call_takes_no_device_memory():
+    """After a first call (which looks up the scratch array's device address), a call leaves the device's
+    free memory exactly as it was: nothing is allocated, by the library or by any library it calls."""
+    torch = pytest.importorskip("torch")
+    d = sweep_inputs(pkg.problems.random_small(33, 7, 8, 3, "S8"), seed=7)
+    arrays = device_arrays(torch, d, existing_entry_point(d))
+    call(torch, d, arrays)
+    free0 = torch.cuda.mem_get_info()[0]
+    call(torch, d, arrays)
+    call(torch, d, arrays)
+    assert torch.cuda.mem_get_info()[0] == free0
