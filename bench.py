@@ -215,9 +215,10 @@ def run_tiling_sweep(args):
             for NH in (1, 2, 3, 4, 5, 6):
                 for W in (2, 3, 4, 5, 6, 8, 12, 16):
                     for S in (0, 2, 4, 8, 16):
-                        for st in (2, 3):
+                        for st, NB in ((2, 1), (3, 1), (2, 2), (2, 4)):
                             try:
                                 s.set_tiling(W, S, st, NH)
+                                s.set_bands(NB)
                             except pkg.TrtError:
                                 continue
                             tl = s.tiling()
