@@ -293,6 +293,42 @@ def run_time_steps(pkg, torch, prob, steps, conv_type=2, conv_ho=0.0, maxit=8):
     return out
 
 
+def run_group_sharded(pkg, torch, prob, steps, maxit=4):
+    """The transport-only time loop of the workload with its groups split over the ranks (one GPU each): every
+    rank sweeps its group range and one all-reduce of the per-cell group sums per outer iteration gives every
+    rank the same temperature (sharded.ShardedTimeLoop).  Strong scaling of one instance; step time is the
+    maximum over ranks of the device-synchronised wall time."""
+    ws, rank, _ = pkg.ranks.world()
+    ts = pkg.problems.config_timestep_setup(prob)
+    g0, g1 = pkg.sharded.group_ranges(prob.ng, ws)[rank]
+    ox, oy, w = prob.directions()
+    nu = ts.nu_eV[g0:g1 + 1]
+    CU, C = pkg.problems.COMP_UNIT, pkg.problems.C_LIGHT
+    s = pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, g1 - g0, precision="fp64")
+    try:
+        s.init_state(ts.Tini_eV, list(ts.bcT_eV), CU, nu)
+        s.tstep_setup(nu, ts.kappa_mult, ts.cv, np.full((prob.nx, prob.ny), ts.Tini_eV), ts.Kap0, CU, C, ts.dt,
+                      bcT=ts.bcT_eV, conv_type=2, conv_ho=0.0, maxit_rte=maxit, law=1)
+        loop = pkg.sharded.ShardedTimeLoop([s], prob.nx, prob.ny, maxit=maxit,
+                                           allreduce=pkg.sharded.torch_allreduce() if ws > 1 else None)
+        loop.step()   # warm-up
+        lat = []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            pkg.ranks.barrier()
+            t0 = time.perf_counter()
+            loop.step()
+            torch.cuda.synchronize()
+            lat.append(pkg.ranks.reduce_max(time.perf_counter() - t0))
+    finally:
+        s.close()
+    upd = prob.updates_per_sweep() * maxit
+    return {"what": "transport-only time step (configuration's material, FP64), groups split over the ranks, "
+                    "one all-reduce of 3 nx*ny doubles per outer iteration", "ranks": ws, "groups_per_rank": g1 - g0,
+            "outer_its_per_step": maxit, "step_ms": [x * 1e3 for x in lat],
+            "updates_per_s": upd * len(lat) / sum(lat), "scaling": "strong"}
+
+
 def run_mlqd(pkg, torch, prob, steps, conv_ho=1e-8, conv_lo=1e-9, maxit_rte=10, maxit_mloqd=50):
     """The reference's mlqd algorithm (TRT_MLQD_ALGORITHM, run_type 'mlqd') on the device, FP64 and mixed from
     the same initial state: per outer iteration one sweep (from the second on), then MGQD iterations of
@@ -911,6 +947,8 @@ def main():
         line["mixed_over_fp64_e2e"] = line["mixed"]["e2e"]["value"] / line["e2e"]["value"]
     if args.time_steps > 0:
         line["time_steps"] = run_time_steps(pkg, torch, prob, args.time_steps)
+    if ws > 1:
+        line["group_sharded"] = run_group_sharded(pkg, torch, prob, 3)
     if args.mlqd_steps > 0 and ws == 1:
         try:
             line["mlqd"] = run_mlqd(pkg, torch, prob, args.mlqd_steps)
