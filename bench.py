@@ -820,7 +820,9 @@ def workload_config(prob):
             "updates_per_sweep": prob.updates_per_sweep(),
             "step": "one time step of the hot path: I_crn_old <- I_crn, full sweep, angular moments, QD factors fg, "
                     "boundary factors Cg",
-            "precision": "f64 (the reference's REAL*8)"}
+            "precision": "f64 (the reference's REAL*8)",
+            "l2": f"inputs larger than L2 (the corner state of the step: {8 * 4 * prob.updates_per_sweep() / 1e9:.3g} GB "
+                  f"in FP64)"}
 
 
 def run_reference(args):
@@ -913,9 +915,8 @@ def main():
 
     main_ = res["fp64"]
     cfg = workload_config(prob)
-    cfg.update({"l2": "inputs larger than L2 (corner state 15 GB FP64 / 7.5 GB FP32 at C1)",
-                "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"})
     line = {
+        "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
         "metric": "cell-angle-group updates/s",
         "value": ranks.whole_job_rate(upd, main_["ms"] * 1e-3, ws),
         "unit": "updates/s",
