@@ -24,6 +24,7 @@ TRT_ERR_SCRATCH = -9
 
 TRT_PREC_FP64 = 0
 TRT_PREC_FP32 = 1
+TRT_CREATE_INPLACE = 0x10   # OR-ed into trt_create's precision: one in-place state buffer from the start
 
 TRT_ROLL_STATE = 1
 TRT_LAW_FLECK_CUMMINGS = 0   # material laws of the time loops (trt_tstep_set_law)

@@ -568,7 +568,8 @@ class TransportSweep:
         out = s.moments(["fg_avg_xx", ...])
     """
 
-    def __init__(self, nx, ny, Omega_x, Omega_y, quad_weight, Delx, Dely, ng, precision="fp64", hbm_budget=0):
+    def __init__(self, nx, ny, Omega_x, Omega_y, quad_weight, Delx, Dely, ng, precision="fp64", hbm_budget=0,
+                 inplace=False):
         L = _lib.lib()
         self.nx, self.ny, self.ng = int(nx), int(ny), int(ng)
         self.Omega_x, self.Omega_y, self.w = _f64(Omega_x), _f64(Omega_y), _f64(quad_weight)
@@ -576,9 +577,10 @@ class TransportSweep:
         self.Delx, self.Dely = _f64(Delx, (nx,)), _f64(Dely, (ny,))
         self.precision = {"fp64": _lib.TRT_PREC_FP64, "fp32": _lib.TRT_PREC_FP32, "mixed": _lib.TRT_PREC_FP32}[precision]
         st = ctypes.c_int(0)
+        flags = _lib.TRT_CREATE_INPLACE if inplace else 0
         self._h = L.trt_create(self.nx, self.ny, self.nm, self.ng, dptr(self.Omega_x), dptr(self.Omega_y),
-                               dptr(self.w), dptr(self.Delx), dptr(self.Dely), self.precision, int(hbm_budget),
-                               ctypes.byref(st))
+                               dptr(self.w), dptr(self.Delx), dptr(self.Dely), self.precision | flags,
+                               int(hbm_budget), ctypes.byref(st))
         if not self._h:
             raise _lib.TrtError(st.value, "trt_create")
 

@@ -1648,6 +1648,8 @@ trt_ctx* trt_create(int n_x, int n_y, int n_m, int n_g, const double* Omega_x, c
                     size_t hbm_budget, int* status) {
   int dummy;
   if (!status) status = &dummy;
+  const bool inplace = (precision & TRT_CREATE_INPLACE) != 0;
+  precision &= ~TRT_CREATE_INPLACE;
   if (!valid_shape(n_x, n_y, n_m, n_g) || !Omega_x || !Omega_y || !quad_weight || !Delx || !Dely ||
       (precision != TRT_PREC_FP64 && precision != TRT_PREC_FP32)) {
     *status = TRT_ERR_ARG;
@@ -1661,6 +1663,7 @@ trt_ctx* trt_create(int n_x, int n_y, int n_m, int n_g, const double* Omega_x, c
   }
   c->nx = n_x; c->ny = n_y; c->nm = n_m; c->ng = n_g; c->mq = n_m / 4;
   c->prec = precision;
+  c->inplace = inplace;   // one state buffer from the start (an instance whose two buffers would not fit)
   c->budget = hbm_budget;
   c->omx.assign(Omega_x, Omega_x + n_m);
   c->omy.assign(Omega_y, Omega_y + n_m);

@@ -450,9 +450,9 @@ def run_config4(pkg, torch, steps, snapshots=True, n=1024):
     out = {"workload": f"C4: {prob.nx}x{prob.ny} cells, {prob.ng} log-spaced groups, {prob.quad} ({prob.nm} "
                        f"directions), 8 seeded material rectangles", "updates_per_sweep": upd,
            "step": "one sweep of the transport-only loop per time step (trt_tstep, maxit_rte 1), in-place FP32 state"}
-    s = pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng, precision="mixed")
+    s = pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng, precision="mixed",
+                           inplace=True)
     try:
-        s.set_inplace(True)
         s.init_state(ts.Tini_eV, list(ts.bcT_eV), pkg.problems.COMP_UNIT, ts.nu_eV)
         s.tstep_setup(ts.nu_eV, ts.kappa_mult, ts.cv, np.full((prob.nx, prob.ny), ts.Tini_eV), ts.Kap0,
                       pkg.problems.COMP_UNIT, pkg.problems.C_LIGHT, ts.dt, bcT=ts.bcT_eV, conv_type=2, conv_ho=0.0,

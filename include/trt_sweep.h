@@ -44,6 +44,9 @@ extern "C" {
 
 #define TRT_PREC_FP64 0   /* plain: FP64 state and arithmetic throughout */
 #define TRT_PREC_FP32 1   /* mixed: FP32 state and sweep, FP64 moment combination and QD factors */
+/* OR-ed into trt_create's precision: lay the handle out with one (in-place) state buffer from the start, as
+ * trt_set_inplace(ctx, 1) would, without ever allocating the second one. */
+#define TRT_CREATE_INPLACE 0x10
 
 /* trt_sweep flags */
 #define TRT_ROLL_STATE 1u  /* I_crn_old = I_crn before sweeping (start of a time step, ALGORITHMS.f08:397) */

@@ -38,6 +38,25 @@ def test_inplace_steps_bit_identical(precision, bands):
         assert np.array_equal(out[0][1][k], out[1][1][k]), k
 
 
+def test_inplace_from_creation_equals_switched_in_place():
+    prob = pkg.problems.random_small(15, 8, 9, 2, "S8")
+    d = sweep_inputs(prob, seed=8)
+    nx, ny, ng = len(d["Delx"]), len(d["Dely"]), d["KapE_in"].shape[2]
+    out = []
+    for created in (False, True):
+        s = pkg.TransportSweep(nx, ny, d["Omega_x"], d["Omega_y"], d["w"], d["Delx"], d["Dely"], ng, inplace=created)
+        with s:
+            if not created:
+                s.set_inplace(True)
+            s.put_state(d["I_crn_old"])
+            s.set_boundary(d["Ic_edgV"], d["Ic_edgH"], (0, 0, 0, 0))
+            s.set_material(d["KapE_in"], d["src_iso"], d["c"], d["dt"], CU)
+            s.sweep(moments=True)
+            s.sweep(roll=True, moments=True)
+            out.append(s.get_state())
+    assert np.array_equal(out[0], out[1])
+
+
 def test_inplace_refuses_a_second_sweep_of_the_same_step():
     prob = pkg.problems.random_small(13, 6, 5, 2, "S8")
     d = sweep_inputs(prob, seed=4)
