@@ -86,20 +86,27 @@ def required_bytes(req):
     return int(b + 10 * p.nx * p.ny * 8 + 4 * 1024 * 1024)
 
 
+def _setup(s, req):
+    """Initial state and the time loop of a request on handle s: the request's own material (the
+    configurations' opacity law on its rectangles, c_v per cell), its boundary and initial temperature."""
+    p = req.prob
+    ts = P.config_timestep_setup(p)
+    s.init_state(ts.Tini_eV, list(ts.bcT_eV), P.COMP_UNIT, ts.nu_eV)
+    s.tstep_setup(ts.nu_eV, ts.kappa_mult, ts.cv, np.full((p.nx, p.ny), ts.Tini_eV), ts.Kap0, P.COMP_UNIT,
+                  P.C_LIGHT, ts.dt, bcT=ts.bcT_eV, conv_type=2, conv_ho=req.conv_ho, maxit_rte=req.maxit, law=1)
+
+
 def solve(req, t0):
     """Run one request on its own handle, capped at its reserved bytes; returns a Result (times
     relative to t0)."""
     from . import api
     p = req.prob
     res = Result(req.rid, req.arrival_s, time.perf_counter() - t0, 0.0, required_bytes(req), 0, [], [])
-    ts = P.fc_timestep_setup(p)
     ox, oy, w = p.directions()
     try:
         with api.TransportSweep(p.nx, p.ny, ox, oy, w, p.delx, p.dely, p.ng, precision=req.precision,
                                 hbm_budget=res.bytes) as s:
-            s.init_state(ts.Tini_eV, list(ts.bcT_eV), P.COMP_UNIT, ts.nu_eV)
-            s.tstep_setup(ts.nu_eV, ts.kappa_mult, ts.cv, np.full((p.nx, p.ny), ts.Tini_eV), ts.Kap0, P.COMP_UNIT,
-                          P.C_LIGHT, ts.dt, bcT=ts.bcT_eV, conv_type=2, conv_ho=req.conv_ho, maxit_rte=req.maxit)
+            _setup(s, req)
             for _ in range(req.steps):
                 a = time.perf_counter()
                 its, _, _ = s.tstep()
@@ -191,14 +198,11 @@ class BatchedServer:
     def _open(req):
         from . import api
         p = req.prob
-        ts = P.fc_timestep_setup(p)
         ox, oy, w = p.directions()
         s = api.TransportSweep(p.nx, p.ny, ox, oy, w, p.delx, p.dely, p.ng, precision=req.precision,
                                hbm_budget=required_bytes(req))
         try:
-            s.init_state(ts.Tini_eV, list(ts.bcT_eV), P.COMP_UNIT, ts.nu_eV)
-            s.tstep_setup(ts.nu_eV, ts.kappa_mult, ts.cv, np.full((p.nx, p.ny), ts.Tini_eV), ts.Kap0, P.COMP_UNIT,
-                          P.C_LIGHT, ts.dt, bcT=ts.bcT_eV, conv_type=2, conv_ho=req.conv_ho, maxit_rte=req.maxit)
+            _setup(s, req)
         except Exception:
             s.close()
             raise
