@@ -268,20 +268,29 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
     __syncwarp();
     return ok != 0;
   };
-  // material of the lane's cell at the current step, loaded one step ahead
+  // material of the lane's cell at the current step (m*) and at the next one (n*): the next cell's loads are
+  // issued at the top of a step, so that their latency hides behind the step's solve
   Real mdx = Real(0), mdy = Real(0), mA4 = Real(0), mkp = Real(0), mqs = Real(0);
-  auto load_material = [&](int ipn, int nn) {
+  Real ndx = Real(0), ndy = Real(0), nA4 = Real(0), nkp = Real(0), nqs = Real(0);
+  auto fetch_material = [&](int ipn, int nn) {
     const int jpn = nn * t.H + rho;
     if (ipn >= 0 && ipn < nx && nn < t.nr && jpn < ny) {
       const int i = fx ? nx - 1 - ipn : ipn;
       const int j = fy ? ny - 1 - jpn : jpn;
       const int cell = i + nx * j;
-      mdx = a.dx[i];
-      mdy = a.dy[j];
-      mA4 = a.area[cell] * Real(0.25);
-      mkp = kapg[cell] + rcdt;
-      if (!SRC_FULL) mqs = qisog[cell];
+      ndx = a.dx[i];
+      ndy = a.dy[j];
+      nA4 = a.area[cell] * Real(0.25);
+      nkp = kapg[cell] + rcdt;
+      if (!SRC_FULL) nqs = qisog[cell];
     }
+  };
+  auto take_material = [&]() {
+    mdx = ndx;
+    mdy = ndy;
+    mA4 = nA4;
+    mkp = nkp;
+    mqs = nqs;
   };
   // Inflows that come from global memory, loaded one step ahead into the inflow registers: the
   // sweep-left boundary face at the start of a round, and for the CTA's first row the sweep-bottom
@@ -320,7 +329,8 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
       }
     }
   };
-  load_material(ip, n);
+  fetch_material(ip, n);
+  take_material();
   if (warp == 0 && !band_wait(ip, n)) timed_out = true;
   if (kLeanFP32) load_inflow(ip, n);
 
@@ -328,6 +338,10 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
   uint32_t phase = 0;
   int T_break = Tsteps;
   for (int T = 0; T < Tsteps; ++T) {
+    {   // the next cell's material (the lane's position one step on)
+      const bool wrap_round = ip + 1 == t.P;
+      fetch_material(wrap_round ? 0 : ip + 1, wrap_round ? n + NB : n);
+    }
     if (!mbar_wait_bounded(&mbar[stage], phase, a.max_polls)) timed_out = true;
     const Real* sm = ring + (size_t)stage * W * chunk + (size_t)warp * chunk;
     const int gchunk = (T * W + warp) * chunk;
@@ -794,7 +808,7 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
       ip = 0;
       n += NB;
     }
-    load_material(ip, n);
+    take_material();
     if (warp == 0 && !band_wait(ip, n)) timed_out = true;
     if (kLeanFP32) load_inflow(ip, n);
 

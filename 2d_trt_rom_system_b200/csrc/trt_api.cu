@@ -428,13 +428,17 @@ int default_W(int R, int ny, int W = 8) {
   return W;
 }
 
-void default_split(int ng, int mq, int* NH, int* W) {
+// part_bytes_per_split: the moment partial records one split count adds (4 quadrants x cells x groups x record);
+// more splits only balance the SMs, so a split count whose records would take more than 16 GB (an instance
+// large enough to fill the SMs without it, e.g. 1024^2 x 64 groups) is not chosen.
+void default_split(int ng, int mq, int* NH, int* W, size_t part_bytes_per_split = 0) {
   const int sms = sm_count();
   *NH = 1;
   *W = 8;
   double best = 0.0;
   for (int nh = 1; nh <= 4; nh *= 2) {
     if (nh > 1 && mq < 4 * nh) break;   // at least 4 directions per split
+    if (nh > 1 && part_bytes_per_split * nh > ((size_t)16 << 30)) break;
     const long long ctas = 4LL * ng * nh;
     const double busiest = (double)((ctas + sms - 1) / sms) / nh;   // work of the busiest SM
     const double load = (double)ctas / sms / nh / busiest;           // mean / busiest
@@ -457,7 +461,9 @@ size_t wrap_bytes(const trt_ctx* c) { return (size_t)4 * c->ng * c->t.NH * c->nx
 // buffer, moment partials).
 int setup_layout(trt_ctx* c) {
   int NH = 1, Wdef = 8;
-  default_split(c->ng, c->mq, &NH, &Wdef);
+  const size_t rec_bytes = c->prec == TRT_PREC_FP64 ? trt::part_rec<double>() * sizeof(double)
+                                                     : trt::part_rec<float>() * sizeof(float);
+  default_split(c->ng, c->mq, &NH, &Wdef, (size_t)4 * c->ng * c->nx * c->ny * rec_bytes);
   if (c->NHreq) NH = c->NHreq;
   if (NH < 1 || NH > c->mq) return TRT_ERR_ARG;
   const int mqc = (c->mq + NH - 1) / NH;
@@ -1626,7 +1632,7 @@ size_t trt_required_bytes(int n_x, int n_y, int n_m, int n_g, int precision) {
   if (!pick_cfg(mq, precision, 0, &kc)) return 0;
   const size_t esz = precision == TRT_PREC_FP64 ? 8 : 4;
   int NH = 1, W = 8;
-  default_split(n_g, mq, &NH, &W);
+  default_split(n_g, mq, &NH, &W, (size_t)4 * n_g * n_x * n_y * (precision == TRT_PREC_FP64 ? 112 : 64));
   if (!pick_cfg((mq + NH - 1) / NH, precision, 0, &kc)) return 0;
   W = default_W(32 / kc.S, n_y, W);
   const int mqc = (mq + NH - 1) / NH;

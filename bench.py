@@ -450,6 +450,9 @@ def run_config4(pkg, torch, steps, snapshots=True, n=1024):
     out = {"workload": f"C4: {prob.nx}x{prob.ny} cells, {prob.ng} log-spaced groups, {prob.quad} ({prob.nm} "
                        f"directions), 8 seeded material rectangles", "updates_per_sweep": upd,
            "step": "one sweep of the transport-only loop per time step (trt_tstep, maxit_rte 1), in-place FP32 state"}
+    free, total = torch.cuda.mem_get_info()
+    out["device_gb_free_before"] = free / 1e9
+    out["required_gb_two_buffers"] = pkg.required_bytes(prob.nx, prob.ny, prob.nm, prob.ng, "mixed") / 1e9
     s = pkg.TransportSweep(prob.nx, prob.ny, ox, oy, w, prob.delx, prob.dely, prob.ng, precision="mixed",
                            inplace=True)
     try:
