@@ -125,10 +125,12 @@ __device__ __forceinline__ int slice_reduce_scatter(double (&v)[16], int s, bool
 // on this part: measured 7.2 ms with Kahan vs the FP64-accumulating kernel on C1).  Sums over
 // slices, quadrants and groups are FP64 as well.
 // Two variants of the step body, chosen by precision (measured on C1, each the faster for its type):
-//  * FP32: global inflows prefetched one step ahead, every lane computes every direction slot and the
-//    bottom-inflow shuffle runs inline (no per-direction top-face registers);
-//  * FP64: global inflows loaded at the step start, only live slots compute, top faces kept in
-//    registers and shuffled after the direction loop (fits 128 registers without spills).
+//  * FP32: every lane computes every direction slot and the bottom-inflow shuffle runs inline (no
+//    per-direction top-face registers);
+//  * FP64: only live slots compute, top faces kept in registers and shuffled after the direction loop.
+// Both take the inflows that come from global memory (boundary faces, the wrap buffer) and the next cell's
+// material one step ahead, so that no step waits on a global load: the per-step barrier would make the
+// whole CTA wait for the slowest warp's load.
 // The sweep of one CTA: (group, quadrant, direction split) number `bid` of the instance described by
 // `a` (blockIdx.x for a single-instance launch; the instance-local number in a batched launch).
 template <class Real, int S, int D, bool SRC_FULL>
@@ -269,7 +271,9 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
     return ok != 0;
   };
   // material of the lane's cell at the current step (m*) and at the next one (n*): the next cell's loads are
-  // issued at the top of a step, so that their latency hides behind the step's solve
+  // issued at the top of a step and only consumed (scaled by 1/4, 1/(c dt) added) after its solve, so that
+  // their latency hides behind the step; arithmetic on a loaded value right after the load would stall the
+  // warp there (measured on C1: 1700 of 8200 cycles per warp step)
   Real mdx = Real(0), mdy = Real(0), mA4 = Real(0), mkp = Real(0), mqs = Real(0);
   Real ndx = Real(0), ndy = Real(0), nA4 = Real(0), nkp = Real(0), nqs = Real(0);
   auto fetch_material = [&](int ipn, int nn) {
@@ -280,16 +284,16 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
       const int cell = i + nx * j;
       ndx = a.dx[i];
       ndy = a.dy[j];
-      nA4 = a.area[cell] * Real(0.25);
-      nkp = kapg[cell] + rcdt;
+      nA4 = a.area[cell];
+      nkp = kapg[cell];
       if (!SRC_FULL) nqs = qisog[cell];
     }
   };
   auto take_material = [&]() {
     mdx = ndx;
     mdy = ndy;
-    mA4 = nA4;
-    mkp = nkp;
+    mA4 = nA4 * Real(0.25);
+    mkp = nkp + rcdt;
     mqs = nqs;
   };
   // Inflows that come from global memory, loaded one step ahead into the inflow registers: the
@@ -298,7 +302,6 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
   // round n was written at step (n-1)P + ip + H - 1, before the barrier that precedes this prefetch
   // (P > H).
   auto load_inflow = [&](int ipn, int nn) {
-    if constexpr (!kLeanFP32) return;
     const int jpn = nn * t.H + rho;
     if (!(ipn >= 0 && ipn < nx && nn < t.nr && jpn < ny)) return;
     const int in = fx ? nx - 1 - ipn : ipn;
@@ -332,7 +335,7 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
   fetch_material(ip, n);
   take_material();
   if (warp == 0 && !band_wait(ip, n)) timed_out = true;
-  if (kLeanFP32) load_inflow(ip, n);
+  load_inflow(ip, n);
 
   int stage = 0;
   uint32_t phase = 0;
@@ -363,39 +366,14 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
 
       if (active) {
         const Real dx = mdx, dy = mdy, A4 = mA4, kp = mkp, qs = mqs;
-        if (ip == 0) {
+        if (r == 0 && warp > 0) {
   #pragma unroll
           for (int d = 0; d < D; ++d) {
             const int ml = d * S + s;
             if (d < D - 1 || s < s_last) {
-              vb[d] = bVin[ml * 2 * ny + 2 * j + byo];
-              vt[d] = bVin[ml * 2 * ny + 2 * j + 1 - byo];
-            }
-          }
-        }
-        if (r == 0) {
-  #pragma unroll
-          for (int d = 0; d < D; ++d) {
-            const int ml = d * S + s;
-            if (d < D - 1 || s < s_last) {
-              if (rho == 0 && n > 0) {   // wrap buffer, possibly written by another band CTA: through L2
-                hl[d] = __ldcg(wrapc + (ip * mqc + ml) * 2);
-                hr[d] = __ldcg(wrapc + (ip * mqc + ml) * 2 + 1);
-              } else {
-                const Real* src;
-                int o0, o1;
-                if (rho == 0) {
-                  src = bHin + ml * 2 * nx + 2 * i;
-                  o0 = bxo;
-                  o1 = 1 - bxo;
-                } else {
-                  src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mqc + ml) * 2;
-                  o0 = 0;
-                  o1 = 1;
-                }
-                hl[d] = src[o0];
-                hr[d] = src[o1];
-              }
+              const Real* src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mqc + ml) * 2;
+              hl[d] = src[0];
+              hr[d] = src[1];
             }
           }
         }
@@ -810,7 +788,7 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
     }
     take_material();
     if (warp == 0 && !band_wait(ip, n)) timed_out = true;
-    if (kLeanFP32) load_inflow(ip, n);
+    load_inflow(ip, n);
 
     const int any_timeout = __syncthreads_or(timed_out ? 1 : 0);
     if (any_timeout) {
