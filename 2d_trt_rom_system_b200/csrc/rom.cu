@@ -105,19 +105,82 @@ __global__ void dmd_reconstruct_kernel(long long glen, int n_blocks, const int* 
   }
 }
 
-struct Dev {
-  std::vector<void*> p;
-  ~Dev() {
-    for (void* q : p) cudaFree(q);
+// Device scratch of the ROM routines: one arena per host thread, grown by whole blocks, from which every call
+// takes its temporaries in stack order (a Dev gives back what it took when it goes out of scope).  Repeated
+// calls (a POD per group, a reconstruction per time step) then allocate nothing: cudaMalloc and cudaFree cost
+// up to milliseconds each, and cudaFree synchronises the device.  Blocks of at most kKeep bytes are kept for
+// the next call; larger ones are freed when the outermost Dev goes out of scope.
+struct Arena {
+  static constexpr size_t kBlock = size_t(64) << 20, kKeep = size_t(256) << 20;
+  int device = -1;
+  std::vector<std::pair<char*, size_t>> blocks;   // base, capacity
+  size_t blk = 0, off = 0;                          // first free byte: block index, offset in it
+  int depth = 0;                                    // Devs alive
+  void release_large() {   // only with no Dev alive (nothing handed out)
+    for (size_t k = blocks.size(); k-- > 0;) {
+      if (blocks[k].second > kKeep) {
+        cudaFree(blocks[k].first);
+        blocks.erase(blocks.begin() + (long)k);
+      }
+    }
+    blk = off = 0;
   }
+  void release_all() {
+    for (auto& b : blocks) cudaFree(b.first);
+    blocks.clear();
+    blk = off = 0;
+  }
+};
+Arena& arena() {
+  thread_local Arena a;
+  return a;
+}
+
+struct Dev {
+  size_t blk0 = 0, off0 = 0;
+  Dev() {
+    Arena& a = arena();
+    int dev = 0;
+    if (a.depth == 0 && cudaGetDevice(&dev) == cudaSuccess && dev != a.device) {
+      a.release_all();   // blocks of the device this thread used before
+      a.device = dev;
+    }
+    blk0 = a.blk;
+    off0 = a.off;
+    ++a.depth;
+  }
+  ~Dev() {
+    Arena& a = arena();
+    // what this call took may still be read or written by its launches: wait for them, as the cudaFree of a
+    // per-call allocation would
+    if (a.blk != blk0 || a.off != off0) cudaDeviceSynchronize();
+    a.blk = blk0;
+    a.off = off0;
+    if (--a.depth == 0) a.release_large();
+  }
+  Dev(const Dev&) = delete;
+  Dev& operator=(const Dev&) = delete;
   template <class T>
   int get(T** out, size_t n) {
+    Arena& a = arena();
+    const size_t bytes = ((std::max<size_t>(n, 1) * sizeof(T)) + 255) & ~size_t(255);
+    for (; a.blk < a.blocks.size(); ++a.blk, a.off = 0) {
+      if (a.off + bytes <= a.blocks[a.blk].second) {
+        *out = reinterpret_cast<T*>(a.blocks[a.blk].first + a.off);
+        a.off += bytes;
+        return TRT_OK;
+      }
+    }
+    // a new block after the last; a larger one than kKeep is freed again at the end of the outermost call
+    const size_t cap = std::max(bytes, Arena::kBlock);
     void* q = nullptr;
-    if (cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
+    if (cudaMalloc(&q, cap) != cudaSuccess) {
       cudaGetLastError();
       return TRT_ERR_NOMEM;
     }
-    p.push_back(q);
+    a.blocks.emplace_back(static_cast<char*>(q), cap);
+    a.blk = a.blocks.size() - 1;
+    a.off = bytes;
     *out = static_cast<T*>(q);
     return TRT_OK;
   }

@@ -80,7 +80,7 @@ __host__ __device__ inline size_t sweep_smem_bytes(int W, long long chunk, int s
   size_t ring = (size_t)stages * W * chunk * sizeof(Real);
   size_t bars = (size_t)stages * sizeof(uint64_t);
   size_t hand = (size_t)2 * W * mqc * 2 * sizeof(Real);
-  size_t dtab = (size_t)kNDirRow * mqc * sizeof(Real);
+  size_t dtab = (size_t)kNDirRow * D * S * sizeof(Real);
   size_t wtab = (size_t)6 * ((D + 1) / 2) * S * sizeof(float2) + 16;
   return ring + bars + hand + dtab + wtab + 32;
 }
@@ -139,6 +139,7 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
   constexpr int R = 32 / S;
   constexpr int NV = 16 / (int)sizeof(Real);
   constexpr int NSLOT = S >= 16 ? 1 : 16 / S;   // moment slots a lane holds after the reduce-scatter
+  constexpr int DS = D * S;                      // row stride of the direction table
 
   const Tiling t = a.t;
   const int W = t.W;
@@ -172,11 +173,12 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
   // the weights of the lane's direction slots 2p (.x) and 2p+1 (.y); slots without a direction hold 0
   constexpr int NP = (D + 1) / 2;
   float2* wt2 = reinterpret_cast<float2*>(
-      (reinterpret_cast<uintptr_t>(dtab + kNDirRow * mqc) + 15) & ~static_cast<uintptr_t>(15));
+      (reinterpret_cast<uintptr_t>(dtab + kNDirRow * DS) + 15) & ~static_cast<uintptr_t>(15));
 
-  // direction table of this split: row k of split-local direction ml at dtab[k * mqc + ml]
-  for (int k = threadIdx.x; k < kNDirRow * mqc; k += blockDim.x) {
-    const int row = k / mqc, col = k % mqc;
+  // direction table of this split: row k of split-local direction ml at dtab[k * DS + ml] (a compile-time row
+  // stride, so that every table read is a constant offset from one per-lane base)
+  for (int k = threadIdx.x; k < kNDirRow * DS; k += blockDim.x) {
+    const int row = k / DS, col = k % DS;
     Real v = col < mq_h ? a.dirtab[((size_t)q * kNDirRow + row) * mq + mo + col] : Real(0);
     if (row < 2) v = v * Real(0.25);   // |Omega| / 4 for the corner-matrix geometry
     dtab[k] = v;
@@ -209,7 +211,10 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
   Real* gnew = a.Inew + blk_off;
   const int Tsteps = band_steps(t, nx, band);
 
-  if (threadIdx.x == 0) {
+  // the TMA copies are issued by lane 0 of the last warp, whose rows take no inflow from global memory (the
+  // first warp's first row does, and a copy issued behind those loads would wait for them)
+  const bool tma_thread = threadIdx.x == 32 * (W - 1);
+  if (tma_thread) {
     for (int k = 0; k < stages && k < Tsteps; ++k) {
       mbar_arrive_expect_tx(&mbar[k], stage_bytes);
       tma_bulk_g2s(ring + (size_t)k * W * chunk, gold + (long long)k * W * chunk, stage_bytes, &mbar[k]);
@@ -404,7 +409,7 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
   #pragma unroll
               for (int c = 0; c < 4; ++c) src[c] = tfma(io[c], rcdt, qs);
             }
-            const ScbGeom<Real> G = scb_geom(dtab[kAx * mqc + ml], dtab[kAy * mqc + ml], dx, dy);
+            const ScbGeom<Real> G = scb_geom(dtab[kAx * DS + ml], dtab[kAy * DS + ml], dx, dy);
             const Real gam = scb_gamma(G, kA4);
             Real x[4];
             scb_solve(G, gam, A4, src, vb[d], vt[d], hl[d], hr[d], x);
@@ -425,8 +430,8 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
             const Real Iavg = ((x[0] + x[1]) + (x[2] + x[3])) * Real(0.25);
             const Real Iv = (x[1] + x[2]) * Real(0.5);
             const Real Ih = (x[3] + x[2]) * Real(0.5);
-            const Real wxx = dtab[kWxx * mqc + ml], wyy = dtab[kWyy * mqc + ml], wxy = dtab[kWxy * mqc + ml];
-            const Real ww = dtab[kW * mqc + ml], wx = dtab[kWx * mqc + ml], wy = dtab[kWy * mqc + ml];
+            const Real wxx = dtab[kWxx * DS + ml], wyy = dtab[kWyy * DS + ml], wxy = dtab[kWxy * DS + ml];
+            const Real ww = dtab[kW * DS + ml], wx = dtab[kWx * DS + ml], wy = dtab[kWy * DS + ml];
             {
               acc[kCxx] = tfma(wxx, Iavg, acc[kCxx]);
               acc[kCyy] = tfma(wyy, Iavg, acc[kCyy]);
@@ -607,8 +612,8 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
   #pragma unroll
           for (int c = 0; c < 4; ++c) src[c] = __ffma2_rn(io[c], f2(rcdt), f2(qs));
         }
-        const ScbGeom2 G2 = scb_geom2(make_float2(dtab[kAx * mqc + ml0], dtab[kAx * mqc + ml1]),
-                                      make_float2(dtab[kAy * mqc + ml0], dtab[kAy * mqc + ml1]), dx, dy);
+        const ScbGeom2 G2 = scb_geom2(make_float2(dtab[kAx * DS + ml0], dtab[kAx * DS + ml1]),
+                                      make_float2(dtab[kAy * DS + ml0], dtab[kAy * DS + ml1]), dx, dy);
         const float2 gam = scb_gamma2(G2, kA4);
         float2 x[4];
         scb_solve2(G2, gam, A4, src, make_float2(vb[d], vb[d + 1]), make_float2(vt[d], vt[d + 1]),
@@ -672,7 +677,7 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
   #pragma unroll
           for (int c = 0; c < 4; ++c) src[c] = tfma(io[c], rcdt, qs);
         }
-        const ScbGeom<Real> G = scb_geom(dtab[kAx * mqc + ml], dtab[kAy * mqc + ml], dx, dy);
+        const ScbGeom<Real> G = scb_geom(dtab[kAx * DS + ml], dtab[kAy * DS + ml], dx, dy);
         const Real gam = scb_gamma(G, kA4);
         Real x[4];
         scb_solve(G, gam, A4, src, vb[d], vt[d], hl[d], hr[d], x);
@@ -798,7 +803,7 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
     }
     // the step's wrap-buffer writes (top rows, before the barrier) go out with the progress count
     if (NB > 1 && threadIdx.x == 0 && T + 1 <= pub_stop) st_release_cluster(prog_remote, T + 1);
-    if (threadIdx.x == 0 && T + stages < Tsteps) {
+    if (tma_thread && T + stages < Tsteps) {
       mbar_arrive_expect_tx(&mbar[stage], stage_bytes);
       tma_bulk_g2s(ring + (size_t)stage * W * chunk, gold + (long long)(T + stages) * W * chunk, stage_bytes,
                    &mbar[stage]);
