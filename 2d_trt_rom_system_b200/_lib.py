@@ -193,7 +193,17 @@ SIGNATURES = {
     "trt_dmd_calc": (_i, [_D, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, _i, _d, _d,
                           ctypes.POINTER(ctypes.c_longlong)] + [_D] * 8),
     "trt_mlqd_setup": (_i, [_P, _d, ctypes.POINTER(MlqdParams)]),
+    "trt_mlqd_setup_range": (_i, [_P, _d, ctypes.POINTER(MlqdParams), _i, _i, _D]),
     "trt_mlqd_step": (_i, [_P, ctypes.POINTER(MlqdStats)]),
+    "trt_mlqd_exchange_size": (ctypes.c_longlong, [_P]),
+    "trt_mlqd_step_begin": (_i, [_P, _P]),
+    "trt_mlqd_step_begin_finish": (_i, [_P, _P]),
+    "trt_mlqd_outer_begin": (_i, [_P, _i, _P]),
+    "trt_mlqd_outer_begin_finish": (_i, [_P, _P]),
+    "trt_mlqd_mgqd_local": (_i, [_P, _P]),
+    "trt_mlqd_mgqd_finish": (_i, [_P, _i, _P, _I]),
+    "trt_mlqd_outer_end": (_i, [_P, _i, _I]),
+    "trt_mlqd_step_end": (_i, [_P, ctypes.POINTER(MlqdStats)]),
     "trt_mlqd_counts": (_i, [_P, _I, _i, _I, _i, _I, _I]),
     "trt_mlqd_get": (_i, [_P, ctypes.c_char_p, _D, ctypes.c_longlong]),
     "trt_mlqd_put": (_i, [_P, ctypes.c_char_p, _P, ctypes.c_longlong, _i]),

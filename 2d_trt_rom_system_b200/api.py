@@ -741,20 +741,74 @@ class TransportSweep:
 
     def mlqd_setup(self, Tini, conv_lo=1e-10, conv_gr1=1e-14, conv_gr2=1e-15, maxit_mloqd=50, maxit_gloqd=20,
                    chi=0.7, line_src=2.0, E_Bound_Low=0.0, T_Bound_Low=0.0, use_line_search=True,
-                   use_safety_search=False, kapE_dT_flag=True, Theta=1.0, ho_form=0):
+                   use_safety_search=False, kapE_dT_flag=True, Theta=1.0, ho_form=0, group_range=None):
         """Device time stepping with the reference's run_type 'mlqd' (after init_state and tstep_setup):
-        the initial low-order state of MGQD_INIT / GQD_INIT at Tini."""
+        the initial low-order state of MGQD_INIT / GQD_INIT at Tini.  group_range = (g_first, Nu_g of the
+        whole instance): the handle holds groups g_first .. g_first + ng - 1 of it (trt_mlqd_setup_range; the
+        steps then run through the exchange phases, sharded.ShardedMlqd)."""
         p = _lib.MlqdParams(float(conv_lo), float(conv_gr1), float(conv_gr2), int(maxit_mloqd), int(maxit_gloqd),
                             float(chi), float(line_src), float(E_Bound_Low), float(T_Bound_Low),
                             int(bool(use_line_search)), int(bool(use_safety_search)), int(bool(kapE_dT_flag)),
                             float(Theta), int(ho_form))
-        check(_lib.lib().trt_mlqd_setup(self._h, float(Tini), ctypes.byref(p)), "trt_mlqd_setup")
+        self.mlqd_maxit_mloqd = int(maxit_mloqd)
+        if group_range is None:
+            check(_lib.lib().trt_mlqd_setup(self._h, float(Tini), ctypes.byref(p)), "trt_mlqd_setup")
+            return
+        g_first, nu_all = group_range
+        nu_all = np.ascontiguousarray(np.asarray(nu_all, dtype=np.float64))
+        check(_lib.lib().trt_mlqd_setup_range(self._h, float(Tini), ctypes.byref(p), len(nu_all) - 1, int(g_first),
+                                              dptr(nu_all)), "trt_mlqd_setup_range")
+
+    # The phases of an mlqd step for groups split over handles (include/trt_sweep.h); buffers are device
+    # tensors (torch) of mlqd_exchange_size() doubles.
+    def mlqd_exchange_size(self):
+        n = _lib.lib().trt_mlqd_exchange_size(self._h)
+        if n < 0:
+            check(int(n), "trt_mlqd_exchange_size")
+        return int(n)
+
+    def mlqd_step_begin(self, part):
+        check(_lib.lib().trt_mlqd_step_begin(self._h, ctypes.c_void_p(part.data_ptr())), "trt_mlqd_step_begin")
+
+    def mlqd_step_begin_finish(self, tot):
+        check(_lib.lib().trt_mlqd_step_begin_finish(self._h, ctypes.c_void_p(tot.data_ptr())),
+              "trt_mlqd_step_begin_finish")
+
+    def mlqd_outer_begin(self, rt, part):
+        check(_lib.lib().trt_mlqd_outer_begin(self._h, int(rt), ctypes.c_void_p(part.data_ptr())),
+              "trt_mlqd_outer_begin")
+
+    def mlqd_outer_begin_finish(self, tot):
+        check(_lib.lib().trt_mlqd_outer_begin_finish(self._h, ctypes.c_void_p(tot.data_ptr())),
+              "trt_mlqd_outer_begin_finish")
+
+    def mlqd_mgqd_local(self, part):
+        check(_lib.lib().trt_mlqd_mgqd_local(self._h, ctypes.c_void_p(part.data_ptr())), "trt_mlqd_mgqd_local")
+
+    def mlqd_mgqd_finish(self, mg, tot):
+        c = ctypes.c_int(0)
+        check(_lib.lib().trt_mlqd_mgqd_finish(self._h, int(mg), ctypes.c_void_p(tot.data_ptr()), ctypes.byref(c)),
+              "trt_mlqd_mgqd_finish")
+        return bool(c.value)
+
+    def mlqd_outer_end(self, rt):
+        c = ctypes.c_int(0)
+        check(_lib.lib().trt_mlqd_outer_end(self._h, int(rt), ctypes.byref(c)), "trt_mlqd_outer_end")
+        return bool(c.value)
+
+    def mlqd_step_end(self):
+        st = _lib.MlqdStats()
+        check(_lib.lib().trt_mlqd_step_end(self._h, ctypes.byref(st)), "trt_mlqd_step_end")
+        return self._mlqd_stats(st)
 
     def mlqd_step(self):
         """One mlqd time step; returns its statistics (dict) with the MGQD iterations of each outer iteration
         and the EGP iterations of each MGQD iteration."""
         st = _lib.MlqdStats()
         check(_lib.lib().trt_mlqd_step(self._h, ctypes.byref(st)), "trt_mlqd_step")
+        return self._mlqd_stats(st)
+
+    def _mlqd_stats(self, st):
         out = {k: getattr(st, k) for k, _ in _lib.MlqdStats._fields_}
         a, b = np.zeros(4096, dtype=np.int32), np.zeros(65536, dtype=np.int32)
         n1, n2 = ctypes.c_int(0), ctypes.c_int(0)
@@ -777,7 +831,7 @@ class TransportSweep:
         keys = [k for k in grey if k in name]
         if name.startswith("Cb_"):
             shp = (ny if name[-1] in "LR" else nx,)
-        elif name in ("Temp", "KapE_Bar", "KapE_Bar_dT", "GQD_Src", "MGQD_E_avg", "HO_E_avg"):
+        elif name in ("Temp", "KapE_Bar", "KapE_Bar_dT", "GQD_Src", "MGQD_E_avg", "HO_E_avg", "HO_E_avg_own"):
             shp = (nx, ny)
         elif name == "MGQD_Src":
             shp = (nx, ny, ng)

@@ -174,6 +174,168 @@ __global__ void grey_coefs_kernel(const Dims d, const GreyIn in, const GreyOut o
 }
 
 // ------------------------------------------------------------------------------------------------
+// The same group sums split in two, for groups held in several ranges (ranks of a multi-GPU run): each range
+// forms its partial sums (the loops above over its own groups, in order), the partials are added across the
+// ranges (one all-reduce), and the finish kernels form the ratios.  With one range the results are
+// bit-identical to the kernels above: the sums run over the same groups in the same order, and the E, EV, EH
+// sums that GREY_COEFS divides by are the collapse sums themselves (same loops, same order).
+// ------------------------------------------------------------------------------------------------
+
+// Offsets of the per-MGQD-iteration partial sums in one exchange buffer: the collapse sums (E, EV, EH, FV, FH),
+// the boundary sums of Cbar_Calc (per left/right point j: l, s1, r, s2; per bottom/top point i: b, s1, t, s2),
+// and the 15 numerators of GREY_COEFS per cell.
+struct GreyX {
+  long E, EV, EH, FV, FH, cbLR, cbBT, grey, size;
+};
+__host__ __device__ inline GreyX greyx_of(const Dims& d) {
+  GreyX x;
+  x.E = 0;
+  x.EV = x.E + d.nC;
+  x.EH = x.EV + d.nV;
+  x.FV = x.EH + d.nH;
+  x.FH = x.FV + d.nV;
+  x.cbLR = x.FH + d.nH;
+  x.cbBT = x.cbLR + 4L * d.ny;
+  x.grey = x.cbBT + 4L * d.nx;
+  x.size = x.grey + 15L * d.nC;
+  return x;
+}
+
+// OLD_GREY_COEFS's group sum of G_old (partial: this range's groups).
+__global__ void gold_sum_kernel(const Dims d, const double* __restrict__ Gold, double* out) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= d.nC) return;
+  double s = 0.0;
+  for (int g = 0; g < d.ng; ++g) s = s + Gold[k + d.nC * g];
+  out[k] = s;
+}
+
+// OLD_GREY_COEFS from the total group sum of G_old.
+__global__ void old_grey_from_sum_kernel(const Dims d, double c, double Delt, double Theta, double cv,
+                                         const double* __restrict__ A, const double* __restrict__ Gsum,
+                                         const double* __restrict__ Told, const double* __restrict__ Kbold,
+                                         const double* __restrict__ Eold, const double* __restrict__ Qold, double* Gh,
+                                         double* Rh, const double* __restrict__ cvc) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= d.nC) return;
+  Gh[k] = Gsum[k] + A[k] * Eold[k] / (Theta * Delt);
+  const double cvk = cvc ? cvc[k] : cv;
+  Rh[k] = cvk / (Theta * Delt) * Told[k] + ((1.0 - Theta) / Theta) * (c * Kbold[k] * Eold[k] - Qold[k]);
+}
+
+// Cbar_Calc's numerators and weights (partial).
+__global__ void cbar_partial_kernel(const Dims d, const CbarArgs a, double* lr, double* bt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nx = d.nx, ny = d.ny;
+  if (t < ny) {
+    const int j = t;
+    double l = 0.0, r = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int g = 0; g < d.ng; ++g) {
+      double q = a.EgV[(long)(nx + 1) * j + d.nV * g] - a.EinL[j + (long)ny * g];
+      l = l + a.CgL[j + (long)ny * g] * q;
+      s1 = s1 + q;
+      q = a.EgV[nx + (long)(nx + 1) * j + d.nV * g] - a.EinR[j + (long)ny * g];
+      r = r + a.CgR[j + (long)ny * g] * q;
+      s2 = s2 + q;
+    }
+    lr[4 * j] = l;
+    lr[4 * j + 1] = s1;
+    lr[4 * j + 2] = r;
+    lr[4 * j + 3] = s2;
+  } else if (t < ny + nx) {
+    const int i = t - ny;
+    double b = 0.0, tt = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int g = 0; g < d.ng; ++g) {
+      double q = a.EgH[i + d.nH * g] - a.EinB[i + (long)nx * g];
+      b = b + a.CgB[i + (long)nx * g] * q;
+      s1 = s1 + q;
+      q = a.EgH[i + (long)nx * ny + d.nH * g] - a.EinT[i + (long)nx * g];
+      tt = tt + a.CgT[i + (long)nx * g] * q;
+      s2 = s2 + q;
+    }
+    bt[4 * i] = b;
+    bt[4 * i + 1] = s1;
+    bt[4 * i + 2] = tt;
+    bt[4 * i + 3] = s2;
+  }
+}
+
+__global__ void cbar_finish_kernel(const Dims d, const double* __restrict__ lr, const double* __restrict__ bt,
+                                   double* CbL, double* CbB, double* CbR, double* CbT) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < d.ny) {
+    CbL[t] = lr[4 * t] / lr[4 * t + 1];
+    CbR[t] = lr[4 * t + 2] / lr[4 * t + 3];
+  } else if (t < d.ny + d.nx) {
+    const int i = t - d.ny;
+    CbB[i] = bt[4 * i] / bt[4 * i + 1];
+    CbT[i] = bt[4 * i + 2] / bt[4 * i + 3];
+  }
+}
+
+// GREY_COEFS's 15 numerators per cell (partial), planes k + nC * v in the order Kb, DCxx, DLxx, DRxx, DCyy, DByy,
+// DTyy, DLxy, DRxy, DBxy, DTxy, PL, PR, PB, PT.
+__global__ void grey_partial_kernel(const Dims d, const GreyIn in, double* out) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= d.nC) return;
+  const int nx = d.nx;
+  const int i = (int)(k % nx), j = (int)(k / nx);
+  double v[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const double a = in.A[k];
+  for (int g = 0; g < d.ng; ++g) {
+    const long kg = k + d.nC * g;
+    const long vL = i + (long)(nx + 1) * j + d.nV * g, vR = vL + 1;
+    const long hB = k + d.nH * g, hT = hB + nx;
+    const double tk = in.KapR[kg] + in.Fdt / (in.Theta * in.c * in.Delt);
+    v[0] = v[0] + in.KapE[kg] * in.Eg[kg];
+    v[1] = v[1] + in.fxx[kg] * in.Eg[kg] / tk;
+    v[2] = v[2] + in.fVxx[vL] * in.EgV[vL] / tk;
+    v[3] = v[3] + in.fVxx[vR] * in.EgV[vR] / tk;
+    v[4] = v[4] + in.fyy[kg] * in.Eg[kg] / tk;
+    v[5] = v[5] + in.fHyy[hB] * in.EgH[hB] / tk;
+    v[6] = v[6] + in.fHyy[hT] * in.EgH[hT] / tk;
+    v[7] = v[7] + in.fVxy[vL] * in.EgV[vL] / tk;
+    v[8] = v[8] + in.fVxy[vR] * in.EgV[vR] / tk;
+    v[9] = v[9] + in.fHxy[hB] * in.EgH[hB] / tk;
+    v[10] = v[10] + in.fHxy[hT] * in.EgH[hT] / tk;
+    const double w = in.Fdt * a / (2.0 * in.Theta * in.c * in.Delt);
+    v[11] = v[11] + (w * in.FxOld[vL] + in.PoldL[kg]) / tk;
+    v[12] = v[12] + (w * in.FxOld[vR] + in.PoldR[kg]) / tk;
+    v[13] = v[13] + (w * in.FyOld[hB] + in.PoldB[kg]) / tk;
+    v[14] = v[14] + (w * in.FyOld[hT] + in.PoldT[kg]) / tk;
+  }
+#pragma unroll
+  for (int q = 0; q < 15; ++q) out[k + d.nC * q] = v[q];
+}
+
+// GREY_COEFS's ratios from the total numerators and the total group sums of E, EV, EH.
+__global__ void grey_finish_kernel(const Dims d, const double* __restrict__ num, const double* __restrict__ E,
+                                   const double* __restrict__ EV, const double* __restrict__ EH, const GreyOut o) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= d.nC) return;
+  const int nx = d.nx;
+  const int i = (int)(k % nx), j = (int)(k / nx);
+  const double s1 = E[k], s2 = EV[i + (long)(nx + 1) * j], s3 = EV[i + 1 + (long)(nx + 1) * j], s4 = EH[k],
+               s5 = EH[k + nx];
+  auto n = [&](int q) { return num[k + d.nC * q]; };
+  o.Kb[k] = n(0) / s1;
+  o.DCxx[k] = n(1) / s1;
+  o.DLxx[k] = n(2) / s2;
+  o.DRxx[k] = n(3) / s3;
+  o.DCyy[k] = n(4) / s1;
+  o.DByy[k] = n(5) / s4;
+  o.DTyy[k] = n(6) / s5;
+  o.DLxy[k] = n(7) / s2;
+  o.DRxy[k] = n(8) / s3;
+  o.DBxy[k] = n(9) / s4;
+  o.DTxy[k] = n(10) / s5;
+  o.PL[k] = n(11);
+  o.PR[k] = n(12);
+  o.PB[k] = n(13);
+  o.PT[k] = n(14);
+}
+
+// ------------------------------------------------------------------------------------------------
 // EGP_FV_NEWT
 // ------------------------------------------------------------------------------------------------
 

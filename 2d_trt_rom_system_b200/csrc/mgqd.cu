@@ -989,8 +989,17 @@ struct Mlqd {
   int* kreq;
   const double* f[6];        // the handle's fg fields (avg_xx, avg_yy, edgV_xx, edgV_xy, edgH_yy, edgH_xy)
   const double* Cg[4];       // the handle's Cg fields
-  const double* HOE;         // the handle's transport E_avg
+  const double* HOE;         // the handle's transport E_avg (the sum over this handle's groups)
+  double* HOEt = nullptr;    // the transport E_avg summed over every group (= HOE when the handle holds them all)
+  double* xbuf = nullptr;    // group sums of one exchange (trt_gqd::greyx_of), when the caller passes none
+  int ng_total = 0, g_first = 0;   // the groups of the instance and the first one this handle holds
   std::vector<int> mg_counts, egp_counts, kits;
+  // state of the step in progress (the phases below)
+  trt_mlqd_stats S{};
+  float sweep_ms = 0.f;
+  bool swept = false;
+  int mg_cur = 0, rt_cur = 0;
+  double tn = 0.0, en = 0.0;
 
   ~Mlqd() {
     for (cudaEvent_t e : ev)
@@ -1036,7 +1045,11 @@ int fields_to_unknowns(const Mlqd& m, cudaStream_t st) {
   return TRT_OK;
 }
 
-int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm) {
+// ng_total > 0: the handle holds groups g_first .. g_first + ng - 1 of an instance of ng_total groups whose
+// group edges are nu_total (ng_total + 1 values); the initial grey fields and incoming energies are the sums
+// over every group, the handle's own transport E the sum over its groups.
+int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm, int ng_total, int g_first,
+                    const double* nu_total) {
   auto m = std::make_unique<Mlqd>();
   int rc = trt_host::handle_view(h, &m->v);
   if (rc) return rc;
@@ -1045,6 +1058,16 @@ int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm) {
   m->h = h;
   m->p = prm;
   const int nx = v.nx, ny = v.ny, ng = v.ng;
+  if (ng_total <= 0) {
+    ng_total = ng;
+    g_first = 0;
+    nu_total = v.nu;
+  }
+  if (!nu_total || g_first < 0 || g_first + ng > ng_total) return TRT_ERR_ARG;
+  for (int g = 0; g <= ng; ++g)
+    if (nu_total[g_first + g] != v.nu[g]) return TRT_ERR_ARG;   // the handle's groups are that range
+  m->ng_total = ng_total;
+  m->g_first = g_first;
   m->d = dims_of(nx, ny, ng);
   const Dims& d = m->d;
   cudaStream_t st = v.stream;
@@ -1071,7 +1094,7 @@ int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm) {
       {&m->Gh, c1},   {&m->Rh, c1},   {&m->Tm1, c1},  {&m->Tm2, c1},  {&m->Em1, c1},  {&m->Em2, c1},
       {&m->Tr1, c1},  {&m->Tr2, c1},  {&m->Er1, c1},  {&m->Er2, c1},  {&m->Told, c1}, {&m->drT, c1},
       {&m->W, c1},    {&m->dT, c1},   {&m->dFx, v1},  {&m->dFy, hh1}, {&m->part, (size_t)nblk * 6},
-      {&m->norms, 8}};
+      {&m->norms, 8}, {&m->HOEt, c1}, {&m->xbuf, (size_t)trt_gqd::greyx_of(m->d).size}};
   for (int k = 0; k < 10; ++k) plan.push_back({&m->Dc[k], c1});
   for (int k = 0; k < 4; ++k) {
     plan.push_back({&m->Pc[k], c1});
@@ -1100,10 +1123,14 @@ int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm) {
 
   // --- initial state at Tini ---
   const double pi = 4.0 * std::atan(1.0);
-  std::vector<double> eg(ng);
-  for (int g = 0; g < ng; ++g) eg[g] = 4.0 * pi * trt_bg_planck(Tini, v.nu[g], v.nu[g + 1], v.comp_unit) / v.c;
+  std::vector<double> eg_all(ng_total);
+  for (int g = 0; g < ng_total; ++g)
+    eg_all[g] = 4.0 * pi * trt_bg_planck(Tini, nu_total[g], nu_total[g + 1], v.comp_unit) / v.c;
+  const std::vector<double> eg(eg_all.begin() + g_first, eg_all.begin() + g_first + ng);
   double Esum = 0.0;   // the group sum as MGQD_INIT / GQD_INIT / RT_INIT accumulate it
-  for (int g = 0; g < ng; ++g) Esum = Esum + eg[g];
+  for (int g = 0; g < ng_total; ++g) Esum = Esum + eg_all[g];
+  double Esum_own = 0.0;   // over this handle's groups (= Esum when it holds them all)
+  for (int g = 0; g < ng; ++g) Esum_own = Esum_own + eg[g];
   auto per_group = [&](size_t plane) {
     std::vector<double> x(plane * ng);
     for (int g = 0; g < ng; ++g) std::fill(x.begin() + plane * g, x.begin() + plane * (g + 1), eg[g]);
@@ -1127,8 +1154,10 @@ int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm) {
     if ((rc = h2d(const_cast<double*>(m->Cg[k]), std::vector<double>(side[k] * ng, cv0), st))) return rc;
     if ((rc = h2d(m->Cb[k], std::vector<double>(side[k], cv0), st))) return rc;
   }
-  // transport E of RT_INIT
-  if ((rc = h2d(const_cast<double*>(m->HOE), std::vector<double>(c1, Esum), st))) return rc;
+  // transport E of RT_INIT: the handle's own groups, and all of them
+  if ((rc = h2d(const_cast<double*>(m->HOE), std::vector<double>(c1, Esum_own), st)) ||
+      (rc = h2d(m->HOEt, std::vector<double>(c1, Esum), st)))
+    return rc;
   // grey E, F of GQD_INIT
   if ((rc = h2d(m->E, std::vector<double>(c1, Esum), st)) || (rc = h2d(m->EV, std::vector<double>(v1, Esum), st)) ||
       (rc = h2d(m->EH, std::vector<double>(hh1, Esum), st)))
@@ -1147,9 +1176,11 @@ int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm) {
                            {nm / 4, 3 * nm / 4, 0, 0},    // R: Omega_x < 0
                            {nm / 2, nm, 0, 0}};           // T: Omega_y < 0
   for (int s = 0; s < 4; ++s) {
-    std::vector<double> Eg_in(side[s] * ng, 0.0), Fg_in(side[s] * ng, 0.0), E_in(side[s], 0.0), F_in(side[s], 0.0);
-    for (int g = 0; g < ng; ++g) {
-      const double I = v.bc[s] == 0 ? trt_bg_planck(v.Tb[s], v.nu[g], v.nu[g + 1], v.comp_unit) : 0.0;
+    // every group of the instance (the grey sums); the handle keeps its own range
+    std::vector<double> Eg_in(side[s] * ng_total, 0.0), Fg_in(side[s] * ng_total, 0.0), E_in(side[s], 0.0),
+        F_in(side[s], 0.0);
+    for (int g = 0; g < ng_total; ++g) {
+      const double I = v.bc[s] == 0 ? trt_bg_planck(v.Tb[s], nu_total[g], nu_total[g + 1], v.comp_unit) : 0.0;
       for (size_t i = 0; i < side[s] && v.bc[s] == 0; ++i) {
         double e = 0.0, f = 0.0;
         for (int r = 0; r < 2; ++r)
@@ -1163,11 +1194,13 @@ int mlqd_setup_impl(trt_ctx* h, double Tini, const trt_mlqd_params& prm) {
       }
     }
     for (size_t i = 0; i < side[s]; ++i)
-      for (int g = 0; g < ng; ++g) {
+      for (int g = 0; g < ng_total; ++g) {
         E_in[i] = E_in[i] + Eg_in[i + side[s] * g];
         F_in[i] = F_in[i] + Fg_in[i + side[s] * g];
       }
-    if ((rc = h2d(m->EinG[s], Eg_in, st)) || (rc = h2d(m->FinG[s], Fg_in, st)) || (rc = h2d(m->Ein[s], E_in, st)) ||
+    const std::vector<double> own_E(Eg_in.begin() + side[s] * g_first, Eg_in.begin() + side[s] * (g_first + ng));
+    const std::vector<double> own_F(Fg_in.begin() + side[s] * g_first, Fg_in.begin() + side[s] * (g_first + ng));
+    if ((rc = h2d(m->EinG[s], own_E, st)) || (rc = h2d(m->FinG[s], own_F, st)) || (rc = h2d(m->Ein[s], E_in, st)) ||
         (rc = h2d(m->Fin[s], F_in, st)))
       return rc;
   }
@@ -1205,44 +1238,22 @@ int conv_pair(Mlqd& m, const double* x, const double* xo, const double* xo2, con
   return TRT_OK;
 }
 
-int mlqd_step_impl(Mlqd& m, trt_mlqd_stats* out) {
-  const trt_host::HandleView& v = m.v;
-  const Dims& d = m.d;
-  const int ng = d.ng;
-  cudaStream_t st = v.stream;
-  const size_t C = (size_t)d.nC * ng, V = (size_t)d.nV * ng, H = (size_t)d.nH * ng;
-  const size_t c1 = d.nC, v1 = d.nV, hh1 = d.nH;
-  const double Theta = m.p.theta;
-  int rc;
-  trt_mlqd_stats S{};
-  m.mg_counts.clear();
-  m.egp_counts.clear();
-  m.kits.assign((size_t)std::max(m.p.maxit_gloqd, 1), 0);
-  MG_CUDA(cudaEventRecord(m.ev[0], st));
-  // last time step's data -> _old (ALGORITHMS.f08:395-413)
-  const size_t fsz[6] = {C, C, V, V, H, H};
-  if ((rc = d2d(m.Told, v.T, c1, st)) || (rc = d2d(m.EgO, m.Eg, C, st)) || (rc = d2d(m.EgVO, m.EgV, V, st)) ||
-      (rc = d2d(m.EgHO, m.EgH, H, st)) || (rc = d2d(m.FxO, m.MG->Fx, V, st)) || (rc = d2d(m.FyO, m.MG->Fy, H, st)) ||
-      (rc = d2d(m.KapO, v.kap64, C, st)) || (rc = d2d(m.SrcO, m.Src, C, st)) || (rc = d2d(m.Eo, m.E, c1, st)) ||
-      (rc = d2d(m.KbO, m.Kb, c1, st)) || (rc = d2d(m.QO, m.Q, c1, st)))
-    return rc;
-  for (int k = 0; k < 6; ++k)
-    if ((rc = d2d(m.fO[k], m.f[k], fsz[k], st))) return rc;
-  // OLD_MGQD_COEFS (KapR_old = KapE_old: MATERIAL_UPDATE sets both to KapB) and OLD_GREY_COEFS
-  const OldIn oi{m.EgO, m.EgVO, m.EgHO, m.FxO, m.FyO, m.fO[0], m.fO[1], m.fO[2], m.fO[3], m.fO[4], m.fO[5],
-                 m.KapO, m.KapO, m.SrcO, v.dx, v.dy, v.area, v.c, Theta};
-  const OldOut oo{m.Gold, m.Pold[0], m.Pold[1], m.Pold[2], m.Pold[3]};
-  old_coefs_kernel<<<dim3(grid1(d.nC), ng), 256, 0, st>>>(oi, d, oo);
-  MG_LAUNCHED();
-  trt_gqd::old_grey_kernel<<<grid1(d.nC), 256, 0, st>>>(d, v.c, v.dt, Theta, 0.0, v.area, m.Gold, m.Told, m.KbO, m.Eo,
-                                                        m.QO, m.Gh, m.Rh, v.cv);
-  MG_LAUNCHED();
-  for (double* z : {m.Tr1, m.Tr2, m.Er1, m.Er2}) MG_CUDA(cudaMemsetAsync(z, 0, c1 * sizeof(double), st));
+// ---- the mlqd time step in phases -------------------------------------------------------------------
+// A step is: step_begin / step_begin_finish; per outer iteration outer_begin / outer_begin_finish, the MGQD
+// iterations (mgqd_local / mgqd_finish) and outer_end; step_end.  Each *_begin / *_local phase writes the
+// group sums this handle contributes into `part` (a device buffer of greyx_of(d).size doubles), and the next
+// phase reads the sums over every group's handle from `tot`: with one handle holding every group the two are
+// the same buffer (trt_mlqd_step below); with the groups split over handles (ranks) the caller adds the
+// partial buffers (one all-reduce) in between.  The exchanges are the sums behind OLD_GREY_COEFS, the
+// transport E of the convergence test, and per MGQD iteration COLLAPSE_MG_EF, Cbar_Calc and GREY_COEFS; the
+// grey Newton solve then runs on every handle with the same inputs (replicated), and each handle updates the
+// material of its own groups.
 
-  // grey Newton state: the grey fields, the handle's temperature, this step's coefficients
+trt_gqd::Egp egp_state(Mlqd& m) {
+  const trt_host::HandleView& v = m.v;
   trt_gqd::Egp e{};
-  e.nx = d.nx;
-  e.ny = d.ny;
+  e.nx = m.d.nx;
+  e.ny = m.d.ny;
   e.E = m.E; e.EV = m.EV; e.EH = m.EH; e.T = v.T; e.Kb = m.Kb; e.Fx = m.Fx; e.Fy = m.Fy; e.Q = m.Q;
   e.Kdt = m.Kdt; e.Korg = m.Korg;
   e.Kbm = m.KbM; e.Delx = v.dx; e.Dely = v.dy; e.A = v.area;
@@ -1259,132 +1270,274 @@ int mlqd_step_impl(Mlqd& m, trt_mlqd_stats* out) {
     const double sig_R = 2.0 * std::pow(pi, 5) / (15.0 * (cL * cL) * (hP * hP * hP) * std::pow(erg, 4) * v.comp_unit);
     e.aR = 4.0 * sig_R / cL;
   }
-  e.Theta = Theta; e.Delt = v.dt; e.Kap0 = v.Kap0; e.cv = 0.0; e.cvc = v.cv; e.Chi = m.p.chi;
+  e.Theta = m.p.theta; e.Delt = v.dt; e.Kap0 = v.Kap0; e.cv = 0.0; e.cvc = v.cv; e.Chi = m.p.chi;
   e.Fin = 1.0; e.Ein = 1.0;
+  return e;
+}
+
+// The last time step's data -> _old (ALGORITHMS.f08:395-413), OLD_MGQD_COEFS; part[0, nC) = the group sum of
+// G_old over this handle's groups (OLD_GREY_COEFS).
+int ph_step_begin(Mlqd& m, double* part) {
+  const trt_host::HandleView& v = m.v;
+  const Dims& d = m.d;
+  const int ng = d.ng;
+  cudaStream_t st = v.stream;
+  const size_t C = (size_t)d.nC * ng, V = (size_t)d.nV * ng, H = (size_t)d.nH * ng;
+  const size_t c1 = d.nC;
+  int rc;
+  m.S = trt_mlqd_stats{};
+  m.sweep_ms = 0.f;
+  m.rt_cur = m.mg_cur = 0;
+  m.tn = m.en = 0.0;
+  m.mg_counts.clear();
+  m.egp_counts.clear();
+  m.kits.assign((size_t)std::max(m.p.maxit_gloqd, 1), 0);
+  MG_CUDA(cudaEventRecord(m.ev[0], st));
+  const size_t fsz[6] = {C, C, V, V, H, H};
+  if ((rc = d2d(m.Told, v.T, c1, st)) || (rc = d2d(m.EgO, m.Eg, C, st)) || (rc = d2d(m.EgVO, m.EgV, V, st)) ||
+      (rc = d2d(m.EgHO, m.EgH, H, st)) || (rc = d2d(m.FxO, m.MG->Fx, V, st)) || (rc = d2d(m.FyO, m.MG->Fy, H, st)) ||
+      (rc = d2d(m.KapO, v.kap64, C, st)) || (rc = d2d(m.SrcO, m.Src, C, st)) || (rc = d2d(m.Eo, m.E, c1, st)) ||
+      (rc = d2d(m.KbO, m.Kb, c1, st)) || (rc = d2d(m.QO, m.Q, c1, st)))
+    return rc;
+  for (int k = 0; k < 6; ++k)
+    if ((rc = d2d(m.fO[k], m.f[k], fsz[k], st))) return rc;
+  // OLD_MGQD_COEFS (KapR_old = KapE_old: MATERIAL_UPDATE sets both to KapB)
+  const OldIn oi{m.EgO, m.EgVO, m.EgHO, m.FxO, m.FyO, m.fO[0], m.fO[1], m.fO[2], m.fO[3], m.fO[4], m.fO[5],
+                 m.KapO, m.KapO, m.SrcO, v.dx, v.dy, v.area, v.c, m.p.theta};
+  const OldOut oo{m.Gold, m.Pold[0], m.Pold[1], m.Pold[2], m.Pold[3]};
+  old_coefs_kernel<<<dim3(grid1(d.nC), ng), 256, 0, st>>>(oi, d, oo);
+  MG_LAUNCHED();
+  trt_gqd::gold_sum_kernel<<<grid1(d.nC), 256, 0, st>>>(d, m.Gold, part);
+  MG_LAUNCHED();
+  MG_CUDA(cudaStreamSynchronize(st));
+  return TRT_OK;
+}
+
+// OLD_GREY_COEFS from the total group sum of G_old in tot[0, nC).
+int ph_step_begin_finish(Mlqd& m, const double* tot) {
+  const trt_host::HandleView& v = m.v;
+  const Dims& d = m.d;
+  cudaStream_t st = v.stream;
+  trt_gqd::old_grey_from_sum_kernel<<<grid1(d.nC), 256, 0, st>>>(d, v.c, v.dt, m.p.theta, 0.0, v.area, tot, m.Told,
+                                                                 m.KbO, m.Eo, m.QO, m.Gh, m.Rh, v.cv);
+  MG_LAUNCHED();
+  for (double* z : {m.Tr1, m.Tr2, m.Er1, m.Er2}) MG_CUDA(cudaMemsetAsync(z, 0, d.nC * sizeof(double), st));
+  return TRT_OK;
+}
+
+// Outer iteration rt: the sweep (from the second on, RT_start_Its = 2; none with ho_form 1); part[0, nC) = the
+// transport E over this handle's groups.
+int ph_outer_begin(Mlqd& m, int rt, double* part) {
+  cudaStream_t st = m.v.stream;
+  int rc;
+  m.swept = false;
+  m.rt_cur = rt;
+  if (m.p.ho_form == 0 && rt >= 2) {
+    MG_CUDA(cudaEventRecord(m.ev[2], st));
+    if ((rc = trt_host::handle_outer_sweep(m.h, rt == 2))) return rc;
+    MG_CUDA(cudaEventRecord(m.ev[3], st));
+    ++m.S.sweeps;
+    m.swept = true;
+  }
+  if ((rc = d2d(part, m.HOE, m.d.nC, st))) return rc;
+  MG_CUDA(cudaStreamSynchronize(st));
+  return TRT_OK;
+}
+
+// The transport E over every group; the MGQD iterations start (:675-810).
+int ph_outer_begin_finish(Mlqd& m, const double* tot) {
+  cudaStream_t st = m.v.stream;
+  const size_t c1 = m.d.nC;
+  int rc;
+  if ((rc = d2d(m.HOEt, tot, c1, st)) || (rc = d2d(m.Em1, m.HOEt, c1, st)) || (rc = d2d(m.Tm1, m.v.T, c1, st)))
+    return rc;
+  MG_CUDA(cudaMemsetAsync(m.Em2, 0, c1 * sizeof(double), st));
+  MG_CUDA(cudaMemsetAsync(m.Tm2, 0, c1 * sizeof(double), st));
+  m.mg_cur = 0;
+  return TRT_OK;
+}
+
+// MGQD iteration, this handle's part: MLOQD_FV from the previous solution, and the group sums of
+// COLLAPSE_MG_EF, Cbar_Calc and GREY_COEFS over its groups into part (greyx_of layout).
+int ph_mgqd_local(Mlqd& m, double* part) {
+  const trt_host::HandleView& v = m.v;
+  const Dims& d = m.d;
+  const int ng = d.ng;
+  cudaStream_t st = v.stream;
+  int rc;
+  MG_CUDA(cudaEventRecord(m.ev[4], st));
+  if ((rc = m.MG->solve(st))) return rc;
+  MG_CUDA(cudaEventRecord(m.ev[5], st));
+  MG_CUDA(cudaMemcpyAsync(m.MG->h_scal, m.MG->K.sc, sizeof(Scal) * ng, cudaMemcpyDeviceToHost, st));
+  if ((rc = unknowns_to_fields(m, st))) return rc;
+  const trt_gqd::GreyX x = trt_gqd::greyx_of(d);
+  trt_gqd::collapse_kernel<<<grid1(d.npos()), 256, 0, st>>>(d, m.Eg, m.EgV, m.EgH, m.MG->Fx, m.MG->Fy, part + x.E,
+                                                            part + x.EV, part + x.EH, part + x.FV, part + x.FH);
+  MG_LAUNCHED();
+  const trt_gqd::CbarArgs ca{m.Cg[0], m.Cg[1], m.Cg[2], m.Cg[3], m.EgV, m.EgH, m.EinG[0], m.EinG[1], m.EinG[2],
+                             m.EinG[3], m.Cb[0], m.Cb[1], m.Cb[2], m.Cb[3]};
+  trt_gqd::cbar_partial_kernel<<<grid1(d.nx + d.ny), 256, 0, st>>>(d, ca, part + x.cbLR, part + x.cbBT);
+  MG_LAUNCHED();
+  trt_gqd::GreyIn gi{};
+  gi.Eg = m.Eg; gi.EgV = m.EgV; gi.EgH = m.EgH; gi.FxOld = m.FxO; gi.FyOld = m.FyO;
+  gi.fxx = m.f[0]; gi.fyy = m.f[1]; gi.fVxx = m.f[2]; gi.fVxy = m.f[3]; gi.fHyy = m.f[4]; gi.fHxy = m.f[5];
+  gi.KapE = v.kap64; gi.KapR = v.kap64; gi.A = v.area;
+  gi.PoldL = m.Pold[0]; gi.PoldR = m.Pold[2]; gi.PoldB = m.Pold[1]; gi.PoldT = m.Pold[3];
+  gi.c = v.c; gi.Delt = v.dt; gi.Theta = m.p.theta; gi.Fdt = 1.0;
+  trt_gqd::grey_partial_kernel<<<grid1(d.nC), 256, 0, st>>>(d, gi, part + x.grey);
+  MG_LAUNCHED();
+  MG_CUDA(cudaStreamSynchronize(st));
+  return TRT_OK;
+}
+
+// MGQD iteration mg, from the sums over every group in tot: the grey fields, boundary factors and
+// coefficients, EGP_FV_NEWT, MATERIAL_UPDATE of this handle's groups, CONVERGENCE(conv_lo) on T and the MGQD E.
+int ph_mgqd_finish(Mlqd& m, int mg, const double* tot, bool* mg_conv) {
+  const trt_host::HandleView& v = m.v;
+  const Dims& d = m.d;
+  const int ng = d.ng;
+  cudaStream_t st = v.stream;
+  const size_t c1 = d.nC, v1 = d.nV, hh1 = d.nH;
+  int rc;
+  m.mg_cur = mg;
+  const trt_gqd::GreyX x = trt_gqd::greyx_of(d);
+  if ((rc = d2d(m.MGE, tot + x.E, c1, st)) || (rc = d2d(m.MGEV, tot + x.EV, v1, st)) ||
+      (rc = d2d(m.MGEH, tot + x.EH, hh1, st)) || (rc = d2d(m.MGFx, tot + x.FV, v1, st)) ||
+      (rc = d2d(m.MGFy, tot + x.FH, hh1, st)))
+    return rc;
+  trt_gqd::cbar_finish_kernel<<<grid1(d.nx + d.ny), 256, 0, st>>>(d, tot + x.cbLR, tot + x.cbBT, m.Cb[0], m.Cb[1],
+                                                                   m.Cb[2], m.Cb[3]);
+  MG_LAUNCHED();
+  if ((rc = d2d(m.KbM, m.Kb, c1, st))) return rc;   // KapE_bar_MGQDold = KapE_bar
+  const trt_gqd::GreyOut go{m.Kb,    m.Dc[0], m.Dc[1], m.Dc[2], m.Dc[3], m.Dc[4], m.Dc[5], m.Dc[6],
+                            m.Dc[7], m.Dc[8], m.Dc[9], m.Pc[0], m.Pc[1], m.Pc[2], m.Pc[3]};
+  trt_gqd::grey_finish_kernel<<<grid1(d.nC), 256, 0, st>>>(d, tot + x.grey, m.MGE, m.MGEV, m.MGEH, go);
+  MG_LAUNCHED();
+  if ((rc = d2d(m.E, m.MGE, c1, st)) || (rc = d2d(m.EV, m.MGEV, v1, st)) || (rc = d2d(m.EH, m.MGEH, hh1, st)) ||
+      (rc = d2d(m.Fx, m.MGFx, v1, st)) || (rc = d2d(m.Fy, m.MGFy, hh1, st)))
+    return rc;
+  trt_gqd::Egp e = egp_state(m);
+  e.Tm = m.Tm2;   // Temp_MGQDold2
+  e.damp = (mg > 1 && m.p.kapE_dT_flag) ? 1 : 0;
   const EgpOpts eo{m.p.line_src, m.p.T_bound_low, m.p.E_bound_low, m.p.conv_gr1, m.p.conv_gr2, m.p.maxit_gloqd,
                    m.p.use_line_search, m.p.use_safety_search, 0};
+  int its = 0;
+  bool noconv = false;
+  MG_CUDA(cudaEventRecord(m.ev[6], st));
+  if ((rc = egp_newton(m.GR.get(), st, e, eo, m.part, m.norms, &its, m.kits.data(), nullptr, nullptr, &noconv)))
+    return rc;
+  MG_CUDA(cudaEventRecord(m.ev[7], st));
+  trt_mlqd_stats& S = m.S;
+  int slowest = 0;
+  for (int g = 0; g < ng; ++g) {   // h_scal was read before the Newton iteration's synchronisations
+    if (m.MG->h_scal[g].done != 1) ++S.mgqd_nonconv;
+    slowest = std::max(slowest, m.MG->h_scal[g].its);
+  }
+  S.mgqd_krylov_max = std::max(S.mgqd_krylov_max, slowest);
+  S.mgqd_krylov_sum += slowest;
+  for (int k = 0; k < its; ++k) {
+    if (m.kits[k] < 0) ++S.egp_nonconv;
+    const int ki = (std::abs(m.kits[k]) - 1) / 2;
+    S.egp_krylov_max = std::max(S.egp_krylov_max, ki);
+    S.egp_krylov_sum += ki;
+  }
+  m.egp_counts.push_back(its);
+  S.egp_its += its;
+  if ((rc = trt_host::handle_material(m.h, m.Src))) return rc;   // MATERIAL_UPDATE(Temp)
+  double a = 0.0, b = 0.0;
+  if ((rc = conv_pair(m, v.T, m.Tm1, m.Tm2, m.MGE, m.Em1, m.Em2, m.p.conv_lo, mg, &a, &b, mg_conv))) return rc;
+  {   // the stream has synchronised: both intervals are complete
+    float t1 = 0.f, t2 = 0.f;
+    MG_CUDA(cudaEventElapsedTime(&t1, m.ev[4], m.ev[5]));
+    MG_CUDA(cudaEventElapsedTime(&t2, m.ev[6], m.ev[7]));
+    S.mgqd_solve_ms += t1;
+    S.egp_ms += t2;
+  }
+  std::swap(m.Em1, m.Em2);
+  std::swap(m.Tm1, m.Tm2);
+  if ((rc = d2d(m.Em1, m.MGE, c1, st)) || (rc = d2d(m.Tm1, v.T, c1, st))) return rc;
+  return TRT_OK;
+}
 
-  float sweep_ms = 0.f;
+// End of outer iteration rt: CONVERGENCE(conv_ho) on T and the transport E (over every group).
+int ph_outer_end(Mlqd& m, int rt, bool* rt_conv) {
+  const trt_host::HandleView& v = m.v;
+  cudaStream_t st = v.stream;
+  const size_t c1 = m.d.nC;
+  int rc;
+  m.mg_counts.push_back(m.mg_cur);
+  m.S.mgqd_its += m.mg_cur;
+  if (m.swept) {
+    float ms = 0.f;
+    MG_CUDA(cudaEventSynchronize(m.ev[3]));
+    MG_CUDA(cudaEventElapsedTime(&ms, m.ev[2], m.ev[3]));
+    m.sweep_ms += ms;
+  }
+  if ((rc = conv_pair(m, v.T, m.Tr1, m.Tr2, m.HOEt, m.Er1, m.Er2, v.conv_ho, rt, &m.tn, &m.en, rt_conv))) return rc;
+  std::swap(m.Er1, m.Er2);
+  std::swap(m.Tr1, m.Tr2);
+  if ((rc = d2d(m.Er1, m.HOEt, c1, st)) || (rc = d2d(m.Tr1, v.T, c1, st))) return rc;
+  return TRT_OK;
+}
+
+int ph_step_end(Mlqd& m, trt_mlqd_stats* out) {
+  cudaStream_t st = m.v.stream;
+  int rc;
+  MG_CUDA(cudaEventRecord(m.ev[1], st));
+  if ((rc = trt_host::handle_check(m.h))) return rc;
+  MG_CUDA(cudaEventSynchronize(m.ev[1]));
+  float total = 0.f;
+  MG_CUDA(cudaEventElapsedTime(&total, m.ev[0], m.ev[1]));
+  m.S.rt_its = m.rt_cur;
+  m.S.T_norm = m.tn;
+  m.S.E_norm = m.en;
+  m.S.sweep_ms = m.sweep_ms;
+  m.S.low_order_ms = total - m.sweep_ms;
+  if (out) *out = m.S;
+  return TRT_OK;
+}
+
+// One time step with every group on this handle: the phases with the exchange buffer as both the partial
+// and the total sums.
+int mlqd_step_impl(Mlqd& m, trt_mlqd_stats* out) {
+  double* x = m.xbuf;
+  int rc;
+  if ((rc = ph_step_begin(m, x)) || (rc = ph_step_begin_finish(m, x))) return rc;
   int rt = 0;
   bool rt_conv = false;
-  double tn = 0.0, en = 0.0;
-  while (!rt_conv && rt < v.maxit_rte) {
+  while (!rt_conv && rt < m.v.maxit_rte) {
     ++rt;
-    if (m.p.ho_form == 0 && rt >= 2) {   // RT_start_Its = 2; with ho_form 1 the factors are the caller's
-      MG_CUDA(cudaEventRecord(m.ev[2], st));
-      if ((rc = trt_host::handle_outer_sweep(m.h, rt == 2))) return rc;
-      MG_CUDA(cudaEventRecord(m.ev[3], st));
-      ++S.sweeps;
-    }
-    // MGQD iterations (:675-810)
-    if ((rc = d2d(m.Em1, m.HOE, c1, st)) || (rc = d2d(m.Tm1, v.T, c1, st))) return rc;
-    MG_CUDA(cudaMemsetAsync(m.Em2, 0, c1 * sizeof(double), st));
-    MG_CUDA(cudaMemsetAsync(m.Tm2, 0, c1 * sizeof(double), st));
+    if ((rc = ph_outer_begin(m, rt, x)) || (rc = ph_outer_begin_finish(m, x))) return rc;
     int mg = 0;
     bool mg_conv = false;
     while (!mg_conv && mg < m.p.maxit_mloqd) {
       ++mg;
-      MG_CUDA(cudaEventRecord(m.ev[4], st));
-      if ((rc = m.MG->solve(st))) return rc;   // MLOQD_FV from the previous solution
-      MG_CUDA(cudaEventRecord(m.ev[5], st));
-      MG_CUDA(cudaMemcpyAsync(m.MG->h_scal, m.MG->K.sc, sizeof(Scal) * ng, cudaMemcpyDeviceToHost, st));
-      if ((rc = unknowns_to_fields(m, st))) return rc;
-      trt_gqd::collapse_kernel<<<grid1(d.npos()), 256, 0, st>>>(d, m.Eg, m.EgV, m.EgH, m.MG->Fx, m.MG->Fy, m.MGE,
-                                                                m.MGEV, m.MGEH, m.MGFx, m.MGFy);
-      MG_LAUNCHED();
-      const trt_gqd::CbarArgs ca{m.Cg[0], m.Cg[1], m.Cg[2], m.Cg[3], m.EgV, m.EgH, m.EinG[0], m.EinG[1], m.EinG[2],
-                                 m.EinG[3], m.Cb[0], m.Cb[1], m.Cb[2], m.Cb[3]};
-      trt_gqd::cbar_kernel<<<grid1(d.nx + d.ny), 256, 0, st>>>(d, ca);
-      MG_LAUNCHED();
-      if ((rc = d2d(m.KbM, m.Kb, c1, st))) return rc;   // KapE_bar_MGQDold = KapE_bar
-      trt_gqd::GreyIn gi{};
-      gi.Eg = m.Eg; gi.EgV = m.EgV; gi.EgH = m.EgH; gi.FxOld = m.FxO; gi.FyOld = m.FyO;
-      gi.fxx = m.f[0]; gi.fyy = m.f[1]; gi.fVxx = m.f[2]; gi.fVxy = m.f[3]; gi.fHyy = m.f[4]; gi.fHxy = m.f[5];
-      gi.KapE = v.kap64; gi.KapR = v.kap64; gi.A = v.area;
-      gi.PoldL = m.Pold[0]; gi.PoldR = m.Pold[2]; gi.PoldB = m.Pold[1]; gi.PoldT = m.Pold[3];
-      gi.c = v.c; gi.Delt = v.dt; gi.Theta = Theta; gi.Fdt = 1.0;
-      const trt_gqd::GreyOut go{m.Kb,    m.Dc[0], m.Dc[1], m.Dc[2], m.Dc[3], m.Dc[4], m.Dc[5], m.Dc[6],
-                                m.Dc[7], m.Dc[8], m.Dc[9], m.Pc[0], m.Pc[1], m.Pc[2], m.Pc[3]};
-      trt_gqd::grey_coefs_kernel<<<grid1(d.nC), 256, 0, st>>>(d, gi, go);
-      MG_LAUNCHED();
-      if ((rc = d2d(m.E, m.MGE, c1, st)) || (rc = d2d(m.EV, m.MGEV, v1, st)) || (rc = d2d(m.EH, m.MGEH, hh1, st)) ||
-          (rc = d2d(m.Fx, m.MGFx, v1, st)) || (rc = d2d(m.Fy, m.MGFy, hh1, st)))
-        return rc;
-      e.Tm = m.Tm2;   // Temp_MGQDold2
-      e.damp = (mg > 1 && m.p.kapE_dT_flag) ? 1 : 0;
-      int its = 0;
-      bool noconv = false;
-      MG_CUDA(cudaEventRecord(m.ev[6], st));
-      if ((rc = egp_newton(m.GR.get(), st, e, eo, m.part, m.norms, &its, m.kits.data(), nullptr, nullptr, &noconv)))
-        return rc;
-      MG_CUDA(cudaEventRecord(m.ev[7], st));
-      int slowest = 0;
-      for (int g = 0; g < ng; ++g) {   // h_scal was read before the Newton iteration's synchronisations
-        if (m.MG->h_scal[g].done != 1) ++S.mgqd_nonconv;
-        slowest = std::max(slowest, m.MG->h_scal[g].its);
-      }
-      S.mgqd_krylov_max = std::max(S.mgqd_krylov_max, slowest);
-      S.mgqd_krylov_sum += slowest;
-      for (int k = 0; k < its; ++k) {
-        if (m.kits[k] < 0) ++S.egp_nonconv;
-        const int ki = (std::abs(m.kits[k]) - 1) / 2;
-        S.egp_krylov_max = std::max(S.egp_krylov_max, ki);
-        S.egp_krylov_sum += ki;
-      }
-      m.egp_counts.push_back(its);
-      S.egp_its += its;
-      if ((rc = trt_host::handle_material(m.h, m.Src))) return rc;   // MATERIAL_UPDATE(Temp)
-      double a = 0.0, b = 0.0;
-      if ((rc = conv_pair(m, v.T, m.Tm1, m.Tm2, m.MGE, m.Em1, m.Em2, m.p.conv_lo, mg, &a, &b, &mg_conv))) return rc;
-      {   // the stream has synchronised: both intervals are complete
-        float t1 = 0.f, t2 = 0.f;
-        MG_CUDA(cudaEventElapsedTime(&t1, m.ev[4], m.ev[5]));
-        MG_CUDA(cudaEventElapsedTime(&t2, m.ev[6], m.ev[7]));
-        S.mgqd_solve_ms += t1;
-        S.egp_ms += t2;
-      }
-      std::swap(m.Em1, m.Em2);
-      std::swap(m.Tm1, m.Tm2);
-      if ((rc = d2d(m.Em1, m.MGE, c1, st)) || (rc = d2d(m.Tm1, v.T, c1, st))) return rc;
+      if ((rc = ph_mgqd_local(m, x)) || (rc = ph_mgqd_finish(m, mg, x, &mg_conv))) return rc;
     }
-    m.mg_counts.push_back(mg);
-    S.mgqd_its += mg;
-    if (m.p.ho_form == 0 && rt >= 2) {
-      float ms = 0.f;
-      MG_CUDA(cudaEventElapsedTime(&ms, m.ev[2], m.ev[3]));
-      sweep_ms += ms;
-    }
-    if ((rc = conv_pair(m, v.T, m.Tr1, m.Tr2, m.HOE, m.Er1, m.Er2, v.conv_ho, rt, &tn, &en, &rt_conv))) return rc;
-    std::swap(m.Er1, m.Er2);
-    std::swap(m.Tr1, m.Tr2);
-    if ((rc = d2d(m.Er1, m.HOE, c1, st)) || (rc = d2d(m.Tr1, v.T, c1, st))) return rc;
+    if ((rc = ph_outer_end(m, rt, &rt_conv))) return rc;
   }
-  MG_CUDA(cudaEventRecord(m.ev[1], st));
-  if ((rc = trt_host::handle_check(m.h))) return rc;
-  float total = 0.f;
-  MG_CUDA(cudaEventElapsedTime(&total, m.ev[0], m.ev[1]));
-  S.rt_its = rt;
-  S.T_norm = tn;
-  S.E_norm = en;
-  S.sweep_ms = sweep_ms;
-  S.low_order_ms = total - sweep_ms;
-  if (out) *out = S;
-  return TRT_OK;
+  return ph_step_end(m, out);
 }
 
 }  // namespace
 
 extern "C" {
 
-int trt_mlqd_setup(trt_ctx* ctx, double Tini, const trt_mlqd_params* p) {
+int trt_mlqd_setup_range(trt_ctx* ctx, double Tini, const trt_mlqd_params* p, int ng_total, int g_first,
+                         const double* nu_total) {
   if (!ctx || !p || !(Tini >= 0.0) || p->maxit_mloqd < 1 || p->maxit_gloqd < 1 || !(p->conv_lo >= 0.0) ||
       (p->ho_form != 0 && p->ho_form != 1) ||
       !(p->conv_gr1 >= 0.0) || !(p->conv_gr2 >= 0.0) || !(p->theta > 0.0) ||
-      ((p->use_line_search || p->use_safety_search) && !(p->line_src > 1.0)))
+      ((p->use_line_search || p->use_safety_search) && !(p->line_src > 1.0)) || ng_total < 0 ||
+      (ng_total > 0 && !nu_total))
     return TRT_ERR_ARG;
   int rc = device_ok();
   if (rc) return rc;
-  return mlqd_setup_impl(ctx, Tini, *p);
+  return mlqd_setup_impl(ctx, Tini, *p, ng_total, g_first, nu_total);
+}
+
+int trt_mlqd_setup(trt_ctx* ctx, double Tini, const trt_mlqd_params* p) {
+  return trt_mlqd_setup_range(ctx, Tini, p, 0, 0, nullptr);
 }
 
 int trt_mlqd_step(trt_ctx* ctx, trt_mlqd_stats* stats) {
@@ -1392,6 +1545,66 @@ int trt_mlqd_step(trt_ctx* ctx, trt_mlqd_stats* stats) {
   Mlqd* m = static_cast<Mlqd*>(trt_host::handle_attached(ctx));
   if (!m) return TRT_ERR_STATE;
   return mlqd_step_impl(*m, stats);
+}
+
+long long trt_mlqd_exchange_size(trt_ctx* ctx) {
+  if (!ctx) return TRT_ERR_ARG;
+  const Mlqd* m = static_cast<const Mlqd*>(trt_host::handle_attached(ctx));
+  if (!m) return TRT_ERR_STATE;
+  return trt_gqd::greyx_of(m->d).size;
+}
+
+// The phases of a step (see ph_step_begin ... ph_step_end); buffers are device pointers of
+// trt_mlqd_exchange_size doubles, `part` complete when the call returns.
+static Mlqd* mlqd_of(trt_ctx* ctx) { return ctx ? static_cast<Mlqd*>(trt_host::handle_attached(ctx)) : nullptr; }
+
+int trt_mlqd_step_begin(trt_ctx* ctx, double* part) {
+  Mlqd* m = mlqd_of(ctx);
+  if (!m) return ctx ? TRT_ERR_STATE : TRT_ERR_ARG;
+  return part ? ph_step_begin(*m, part) : TRT_ERR_ARG;
+}
+int trt_mlqd_step_begin_finish(trt_ctx* ctx, const double* tot) {
+  Mlqd* m = mlqd_of(ctx);
+  if (!m) return ctx ? TRT_ERR_STATE : TRT_ERR_ARG;
+  return tot ? ph_step_begin_finish(*m, tot) : TRT_ERR_ARG;
+}
+int trt_mlqd_outer_begin(trt_ctx* ctx, int rt, double* part) {
+  Mlqd* m = mlqd_of(ctx);
+  if (!m) return ctx ? TRT_ERR_STATE : TRT_ERR_ARG;
+  return part && rt >= 1 ? ph_outer_begin(*m, rt, part) : TRT_ERR_ARG;
+}
+int trt_mlqd_outer_begin_finish(trt_ctx* ctx, const double* tot) {
+  Mlqd* m = mlqd_of(ctx);
+  if (!m) return ctx ? TRT_ERR_STATE : TRT_ERR_ARG;
+  return tot ? ph_outer_begin_finish(*m, tot) : TRT_ERR_ARG;
+}
+int trt_mlqd_mgqd_local(trt_ctx* ctx, double* part) {
+  Mlqd* m = mlqd_of(ctx);
+  if (!m) return ctx ? TRT_ERR_STATE : TRT_ERR_ARG;
+  return part ? ph_mgqd_local(*m, part) : TRT_ERR_ARG;
+}
+int trt_mlqd_mgqd_finish(trt_ctx* ctx, int mg, const double* tot, int* converged) {
+  Mlqd* m = mlqd_of(ctx);
+  if (!m) return ctx ? TRT_ERR_STATE : TRT_ERR_ARG;
+  if (!tot || !converged || mg < 1) return TRT_ERR_ARG;
+  bool c = false;
+  const int rc = ph_mgqd_finish(*m, mg, tot, &c);
+  *converged = c ? 1 : 0;
+  return rc;
+}
+int trt_mlqd_outer_end(trt_ctx* ctx, int rt, int* converged) {
+  Mlqd* m = mlqd_of(ctx);
+  if (!m) return ctx ? TRT_ERR_STATE : TRT_ERR_ARG;
+  if (!converged || rt < 1) return TRT_ERR_ARG;
+  bool c = false;
+  const int rc = ph_outer_end(*m, rt, &c);
+  *converged = c ? 1 : 0;
+  return rc;
+}
+int trt_mlqd_step_end(trt_ctx* ctx, trt_mlqd_stats* stats) {
+  Mlqd* m = mlqd_of(ctx);
+  if (!m) return ctx ? TRT_ERR_STATE : TRT_ERR_ARG;
+  return ph_step_end(*m, stats);
 }
 
 int trt_mlqd_counts(trt_ctx* ctx, int* mgqd_per_outer, int cap_outer, int* egp_per_mgqd, int cap_mgqd, int* n_outer,
@@ -1446,7 +1659,8 @@ int trt_mlqd_get(trt_ctx* ctx, const char* name, double* host, long long count) 
              {"Cb_L", m->Cb[0], ny},       {"Cb_B", m->Cb[1], nx},      {"Cb_R", m->Cb[2], ny},
              {"Cb_T", m->Cb[3], nx},       {"Eg_avg", m->Eg, C * ng},   {"Eg_edgV", m->EgV, V * ng},
              {"Eg_edgH", m->EgH, H * ng},  {"Fxg_edgV", m->MG->Fx, V * ng}, {"Fyg_edgH", m->MG->Fy, H * ng},
-             {"MGQD_Src", m->Src, C * ng}, {"MGQD_E_avg", m->MGE, C}, {"HO_E_avg", m->HOE, C}};
+             {"MGQD_Src", m->Src, C * ng}, {"MGQD_E_avg", m->MGE, C}, {"HO_E_avg", m->HOEt, C},
+             {"HO_E_avg_own", m->HOE, C}};
   for (const auto& t : tab)
     if (std::strcmp(t.n, name) == 0) {
       if (count < t.sz) return TRT_ERR_ARG;

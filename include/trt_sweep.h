@@ -501,6 +501,38 @@ typedef struct trt_mlqd_stats {
 } trt_mlqd_stats;
 int trt_mlqd_setup(trt_ctx* ctx, double Tini, const trt_mlqd_params* params);
 int trt_mlqd_step(trt_ctx* ctx, trt_mlqd_stats* stats);
+/* Groups split over handles (the ranks of a multi-GPU run; no counterpart in the reference, whose only
+ * parallelism is the OpenMP loop over groups, TRANSPORT_SOLVES.f08:50-53).  The groups of the mlqd algorithm
+ * meet only in group sums: OLD_GREY_COEFS's sum of G_old once per step, the transport E of the outer
+ * convergence test once per outer iteration, and per MGQD iteration the sums of COLLAPSE_MG_EF
+ * (MLOQD_SOLVES.f08:687-730), Cbar_Calc and GREY_COEFS (GLOQD_SOLVES.f08:89-229).
+ * trt_mlqd_setup_range: the handle holds groups g_first .. g_first + n_g - 1 of an instance of ng_total groups
+ * with edges nu_total (ng_total + 1 values, the handle's own edges a sub-range of them); the initial grey
+ * fields and incoming energies are the sums over every group.  A time step is then, on every handle with the
+ * same arguments:
+ *   trt_mlqd_step_begin(part); [add the parts over the handles into tot]; trt_mlqd_step_begin_finish(tot);
+ *   for rt = 1, 2, ... (at most maxit_rte):
+ *     trt_mlqd_outer_begin(rt, part); [add]; trt_mlqd_outer_begin_finish(tot);
+ *     for mg = 1, 2, ... (at most maxit_mloqd):
+ *       trt_mlqd_mgqd_local(part); [add]; trt_mlqd_mgqd_finish(mg, tot, &converged); stop when converged
+ *     trt_mlqd_outer_end(rt, &converged); stop when converged
+ *   trt_mlqd_step_end(stats);
+ * `part` and `tot` are device buffers of trt_mlqd_exchange_size doubles (the sums of one exchange: 16 n_x n_y
+ * + 2 (n_x+1) n_y + 2 n_x (n_y+1) + 4 (n_x + n_y) at most); each *_begin / *_local call has written its part when
+ * it returns, and `tot` must hold the sum over the handles when the next call starts.  The grey Newton solve
+ * runs on every handle with the same totals, so every handle takes the same iterations.  With one handle
+ * holding every group, `tot` = `part` gives trt_mlqd_step bit for bit (trt_mlqd_step is this sequence). */
+int trt_mlqd_setup_range(trt_ctx* ctx, double Tini, const trt_mlqd_params* params, int ng_total, int g_first,
+                         const double* nu_total);
+long long trt_mlqd_exchange_size(trt_ctx* ctx);
+int trt_mlqd_step_begin(trt_ctx* ctx, double* part);
+int trt_mlqd_step_begin_finish(trt_ctx* ctx, const double* tot);
+int trt_mlqd_outer_begin(trt_ctx* ctx, int rt, double* part);
+int trt_mlqd_outer_begin_finish(trt_ctx* ctx, const double* tot);
+int trt_mlqd_mgqd_local(trt_ctx* ctx, double* part);
+int trt_mlqd_mgqd_finish(trt_ctx* ctx, int mg, const double* tot, int* converged);
+int trt_mlqd_outer_end(trt_ctx* ctx, int rt, int* converged);
+int trt_mlqd_step_end(trt_ctx* ctx, trt_mlqd_stats* stats);
 /* Iteration counts of the last step: MGQD iterations of each outer iteration (n_outer values) and EGP
  * iterations of each MGQD iteration (n_mgqd values), each copied up to its capacity. */
 int trt_mlqd_counts(trt_ctx* ctx, int* mgqd_per_outer, int cap_outer, int* egp_per_mgqd, int cap_mgqd,
@@ -508,7 +540,7 @@ int trt_mlqd_counts(trt_ctx* ctx, int* mgqd_per_outer, int cap_outer, int* egp_p
 /* Copy a device field of the mlqd state to host memory, Fortran layout: "Temp", the grey "E_avg",
  * "E_edgV", "E_edgH", "Fx_edgV", "Fy_edgH", "KapE_Bar", "KapE_Bar_dT", "GQD_Src", "Cb_L/B/R/T", the
  * multigroup "Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH", "MGQD_Src", "MGQD_E_avg", and the
- * transport "HO_E_avg".  `count` is the number of doubles the caller provides (checked). */
+ * transport "HO_E_avg" (summed over every group; "HO_E_avg_own": over the handle's groups).  `count` is the number of doubles the caller provides (checked). */
 int trt_mlqd_get(trt_ctx* ctx, const char* name, double* host, long long count);
 /* Overwrite a QD-factor or boundary-factor field of the handle ("fg_avg_xx", "fg_avg_yy", "fg_edgV_xx",
  * "fg_edgV_xy", "fg_edgH_yy", "fg_edgH_xy", "Cg_L", "Cg_B", "Cg_R", "Cg_T"; Fortran layout, `count` values)

@@ -436,6 +436,89 @@ def grey_coefs(d, c, Delt, Theta, Fdt_Weight=1.0):
     return o
 
 
+def grey_sums(d, c, Delt, Theta, Fdt_Weight=1.0):
+    """The group sums behind COLLAPSE_MG_EF (MLOQD_SOLVES.f08:687-730), Cbar_Calc (GLOQD_SOLVES.f08:191-229) and
+    GREY_COEFS (:89-143) over the groups d holds (one range of a split instance), groups added in order, in the
+    exchange layout of the library (trt_mlqd_exchange_size): E (nx,ny), EV (nx+1,ny), EH (nx,ny+1), FV, FH;
+    per left/right point (l, s1, r, s2) and per bottom/top point (b, s1, t, s2) of Cbar_Calc; the 15 numerators
+    of GREY_COEFS (KapE_Bar's, the ten D's, the four P's), each field in Fortran order, concatenated."""
+    Eg, EgV, EgH = F(d["Eg_avg"]), F(d["Eg_edgV"]), F(d["Eg_edgH"])
+    Fx, Fy = F(d["Fxg_edgV"]), F(d["Fyg_edgH"])
+    nx, ny, ng = Eg.shape
+    E, EV, EH, FV, FH = zeros(nx, ny), zeros(nx + 1, ny), zeros(nx, ny + 1), zeros(nx + 1, ny), zeros(nx, ny + 1)
+    for g in range(ng):
+        E = E + Eg[:, :, g]
+        EV = EV + EgV[:, :, g]
+        EH = EH + EgH[:, :, g]
+        FV = FV + Fx[:, :, g]
+        FH = FH + Fy[:, :, g]
+    lr, bt = zeros(4, ny), zeros(4, nx)
+    for g in range(ng):
+        q = EgV[0, :, g] - F(d["Eg_in_L"])[:, g]
+        lr[0] = lr[0] + F(d["Cg_L"])[:, g] * q
+        lr[1] = lr[1] + q
+        q = EgV[nx, :, g] - F(d["Eg_in_R"])[:, g]
+        lr[2] = lr[2] + F(d["Cg_R"])[:, g] * q
+        lr[3] = lr[3] + q
+        q = EgH[:, 0, g] - F(d["Eg_in_B"])[:, g]
+        bt[0] = bt[0] + F(d["Cg_B"])[:, g] * q
+        bt[1] = bt[1] + q
+        q = EgH[:, ny, g] - F(d["Eg_in_T"])[:, g]
+        bt[2] = bt[2] + F(d["Cg_T"])[:, g] * q
+        bt[3] = bt[3] + q
+    num = zeros(nx, ny, 15)
+    A = F(d["A"])
+    fxx, fyy = F(d["fg_avg_xx"]), F(d["fg_avg_yy"])
+    fVxx, fVxy, fHyy, fHxy = F(d["fg_edgV_xx"]), F(d["fg_edgV_xy"]), F(d["fg_edgH_yy"]), F(d["fg_edgH_xy"])
+    FxO, FyO = F(d["Fxg_edgV_old"]), F(d["Fyg_edgH_old"])
+    Pold = [F(d[k]) for k in ("Pold_L", "Pold_R", "Pold_B", "Pold_T")]
+    w = Fdt_Weight * A / (2.0 * Theta * c * Delt)
+    for g in range(ng):
+        tk = F(d["KapR"])[:, :, g] + Fdt_Weight / (Theta * c * Delt)
+        L, R, B, T = (slice(0, nx), slice(None)), (slice(1, nx + 1), slice(None)), (slice(None), slice(0, ny)), \
+            (slice(None), slice(1, ny + 1))
+        terms = [F(d["KapE"])[:, :, g] * Eg[:, :, g],
+                 fxx[:, :, g] * Eg[:, :, g] / tk,
+                 fVxx[L + (g,)] * EgV[L + (g,)] / tk,
+                 fVxx[R + (g,)] * EgV[R + (g,)] / tk,
+                 fyy[:, :, g] * Eg[:, :, g] / tk,
+                 fHyy[B + (g,)] * EgH[B + (g,)] / tk,
+                 fHyy[T + (g,)] * EgH[T + (g,)] / tk,
+                 fVxy[L + (g,)] * EgV[L + (g,)] / tk,
+                 fVxy[R + (g,)] * EgV[R + (g,)] / tk,
+                 fHxy[B + (g,)] * EgH[B + (g,)] / tk,
+                 fHxy[T + (g,)] * EgH[T + (g,)] / tk,
+                 (w * FxO[L + (g,)] + Pold[0][:, :, g]) / tk,
+                 (w * FxO[R + (g,)] + Pold[1][:, :, g]) / tk,
+                 (w * FyO[B + (g,)] + Pold[2][:, :, g]) / tk,
+                 (w * FyO[T + (g,)] + Pold[3][:, :, g]) / tk]
+        for q_, t_ in enumerate(terms):
+            num[:, :, q_] = num[:, :, q_] + t_
+    return np.concatenate([a.reshape(-1, order="F") for a in (E, EV, EH, FV, FH, lr, bt, num)])
+
+
+def grey_from_sums(tot, nx, ny):
+    """The grey fields, Cbar_Calc's boundary factors and GREY_COEFS's coefficients from the group sums of
+    grey_sums added over every range."""
+    sizes = [("E_avg", (nx, ny)), ("E_edgV", (nx + 1, ny)), ("E_edgH", (nx, ny + 1)), ("Fx_edgV", (nx + 1, ny)),
+             ("Fy_edgH", (nx, ny + 1)), ("lr", (4, ny)), ("bt", (4, nx)), ("num", (nx, ny, 15))]
+    out, k = {}, 0
+    for name, shp in sizes:
+        n = int(np.prod(shp))
+        out[name] = F(np.array(tot[k:k + n], dtype=np.float64).reshape(shp, order="F"))
+        k += n
+    lr, bt, num = out.pop("lr"), out.pop("bt"), out.pop("num")
+    out.update(Cb_L=F(lr[0] / lr[1]), Cb_R=F(lr[2] / lr[3]), Cb_B=F(bt[0] / bt[1]), Cb_T=F(bt[2] / bt[3]))
+    E, EV, EH = out["E_avg"], out["E_edgV"], out["E_edgH"]
+    div = [E, E, EV[:nx], EV[1:], E, EH[:, :ny], EH[:, 1:], EV[:nx], EV[1:], EH[:, :ny], EH[:, 1:]]
+    out["KapE_Bar"] = F(num[:, :, 0] / div[0])
+    for q_, name in enumerate(GREY_D):
+        out[name] = F(num[:, :, q_ + 1] / div[q_ + 1])
+    for q_, name in enumerate(GREY_P):
+        out[name] = F(num[:, :, 11 + q_])
+    return out
+
+
 EGP_STATE = ("E_avg", "E_edgV", "E_edgH", "Temp", "KapE_Bar", "Fx_edgV", "Fy_edgH")
 
 
