@@ -36,6 +36,10 @@ using namespace trt_mgqd;
   } while (0)
 
 constexpr int kSmallCells = 1024;   // levels at or below this many cells run in the one-CTA kernel
+// ... or, when every level from the first of at most kSmallCellsSmem cells on fits in kSmemMax bytes of shared
+// memory, in the one-CTA kernel that keeps them in shared memory (64^2 and below on the configurations' grids)
+constexpr int kSmallCellsSmem = 4096;
+constexpr size_t kSmemMax = 200 * 1024;
 constexpr int kNu1 = 2, kNu2 = 2, kCoarseSweeps = 16;
 constexpr int kCheckEvery = 4;      // iterations between host checks of the convergence flags
 
@@ -57,6 +61,8 @@ struct Solver {
   Krylov K{};
   LevelSet ls{};
   int k0 = 0;
+  bool vsmem = false;         // the levels from k0 on run in small_vcycle_smem_kernel
+  size_t vsmem_bytes = 0;
   double *Fx = nullptr, *Fy = nullptr, *rpart = nullptr, *res = nullptr, *bcres = nullptr;
   int* h_done = nullptr;
   Scal* h_scal = nullptr;
@@ -165,7 +171,16 @@ int Solver::init(int nx, int ny, int ng, bool own_inputs) {
     my = (my + 1) / 2;
   }
   k0 = 0;
-  while (ls.L[k0].n > kSmallCells) ++k0;
+  while (ls.L[k0].n > kSmallCellsSmem) ++k0;
+  vsmem_bytes = small_vcycle_smem_bytes(ls, k0);
+  vsmem = vsmem_bytes <= kSmemMax &&
+          cudaFuncSetAttribute(small_vcycle_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kSmemMax) == cudaSuccess;   // one bound for every solver's launches
+  if (!vsmem) {
+    cudaGetLastError();
+    k0 = 0;
+    while (ls.L[k0].n > kSmallCells) ++k0;
+  }
   MG_CUDA(cudaMallocHost(&h_done, sizeof(int) * ng));
   MG_CUDA(cudaMallocHost(&h_scal, sizeof(Scal) * ng));
   return TRT_OK;
@@ -238,7 +253,10 @@ int Solver::krylov(cudaStream_t s) {
       restrict_kernel<<<dim3(grid1(ls.L[k + 1].n), ng), 256, 0, s>>>(L, ls.L[k + 1], K.done);
       if ((rc = launched())) return rc;
     }
-    small_vcycle_kernel<<<ng, 256, 0, s>>>(ls, k0, kNu1, kNu2, kCoarseSweeps, K.done);
+    if (vsmem)
+      small_vcycle_smem_kernel<<<ng, 1024, vsmem_bytes, s>>>(ls, k0, kNu1, kNu2, kCoarseSweeps, K.done);
+    else
+      small_vcycle_kernel<<<ng, 256, 0, s>>>(ls, k0, kNu1, kNu2, kCoarseSweeps, K.done);
     if ((rc = launched())) return rc;
     for (int k = k0 - 1; k >= 0; --k) {
       const Level& L = ls.L[k];

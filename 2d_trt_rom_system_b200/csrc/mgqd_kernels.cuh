@@ -383,6 +383,160 @@ __global__ void small_vcycle_kernel(const LevelSet ls, int k0, int nu1, int nu2,
   }
 }
 
+// The same V-cycle with every level of the CTA's group copied into shared memory first (coefficients of every
+// level, level k0's b), so that each of its ~70 phases costs a shared-memory pass and a barrier instead of an
+// L1/L2 round trip; level k0's x is written back.  The arithmetic is that of small_vcycle_kernel, cell for cell
+// and phase for phase (a colour's cells do not read one another), so the results are identical.
+// Dynamic shared memory: 7 floats per cell of levels k0 .. n-1 (small_vcycle_smem_bytes).
+__host__ __device__ inline size_t small_vcycle_smem_bytes(const LevelSet& ls, int k0) {
+  size_t n = 0;
+  for (int k = k0; k < ls.n; ++k) n += (size_t)ls.L[k].n;
+  return n * 7 * sizeof(float);
+}
+
+// One level of the shared-memory V-cycle: its extents and its arrays in shared memory (cell c = i + mx j).
+struct SLevel {
+  int mx, my, n;
+  float *sC, *sW, *sE, *sS, *sN, *x, *b;
+};
+
+// The operations of smooth_cell / restrict_cell / prolong_cell on a shared-memory level, term for term in the
+// same order (32-bit indices; every phase visits only the cells it writes).
+__device__ __forceinline__ float sl_offdiag(const SLevel& L, int i, int j, int k) {
+  float s = 0.f;
+  if (i > 0) s += L.sW[k] * L.x[k - 1];
+  if (i + 1 < L.mx) s += L.sE[k] * L.x[k + 1];
+  if (j > 0) s += L.sS[k] * L.x[k - L.mx];
+  if (j + 1 < L.my) s += L.sN[k] * L.x[k + L.mx];
+  return s;
+}
+
+__global__ void __launch_bounds__(1024) small_vcycle_smem_kernel(const LevelSet ls, int k0, int nu1, int nu2,
+                                                                 int coarse_sweeps, const int* __restrict__ done) {
+  extern __shared__ float vsm[];
+  __shared__ SLevel S[kMaxLevels];   // levels k0 .. n-1 of this CTA's group, in shared memory
+  const int g = blockIdx.x;
+  if (done[g]) return;
+  const int last = ls.n - 1;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (tid == 0) {
+    float* p = vsm;
+    for (int k = k0; k <= last; ++k) {
+      SLevel& V = S[k];
+      V.mx = ls.L[k].mx;
+      V.my = ls.L[k].my;
+      V.n = (int)ls.L[k].n;
+      float** f[7] = {&V.sC, &V.sW, &V.sE, &V.sS, &V.sN, &V.x, &V.b};
+      for (int q = 0; q < 7; ++q) {
+        *f[q] = p;
+        p += V.n;
+      }
+    }
+  }
+  __syncthreads();
+  for (int k = k0; k <= last; ++k) {
+    const SLevel V = S[k];
+    const Level& L = ls.L[k];
+    const long o = L.n * g;
+    for (int c = tid; c < V.n; c += nt) {
+      V.sC[c] = L.sC[o + c];
+      V.sW[c] = L.sW[o + c];
+      V.sE[c] = L.sE[o + c];
+      V.sS[c] = L.sS[o + c];
+      V.sN[c] = L.sN[o + c];
+      if (k == k0) V.b[c] = L.b[o + c];
+    }
+  }
+  __syncthreads();
+  // The phases over threads [0, n_t) with barrier `bar`: the whole CTA for the larger levels, warp 0 alone
+  // (__syncwarp) for the levels of at most 64 cells and the coarse solve, where a CTA-wide barrier per phase
+  // would cost more than the phase.
+  struct Team {
+    int t, n;
+    bool warp;
+    __device__ void sync() const {
+      if (warp) __syncwarp();
+      else __syncthreads();
+    }
+  };
+  // one colour of a red-black sweep; zero: the iterate is zero (this colour takes b/sC, the other is cleared)
+  auto sweep = [&](const Team& tm, int k, int color, bool zero) {
+    const SLevel L = S[k];
+    if (zero) {
+      for (int c = tm.t; c < L.n; c += tm.n) {
+        const int j = c / L.mx, i = c - j * L.mx;
+        L.x[c] = ((i + j) & 1) == color ? L.b[c] / L.sC[c] : 0.f;
+      }
+    } else {
+      const int hx = (L.mx + 1) >> 1;   // cells of one colour per row, at most
+      for (int q = tm.t; q < hx * L.my; q += tm.n) {
+        const int j = q / hx;
+        const int i = 2 * (q - j * hx) + ((j + color) & 1);
+        if (i >= L.mx) continue;
+        const int c = i + L.mx * j;
+        L.x[c] = (L.b[c] - sl_offdiag(L, i, j, c)) / L.sC[c];
+      }
+    }
+    tm.sync();
+  };
+  auto smooth = [&](const Team& tm, int k, int sweeps, bool zero) {
+    for (int sw = 0; sw < sweeps; ++sw) {
+      sweep(tm, k, 0, zero && sw == 0);
+      sweep(tm, k, 1, false);
+    }
+  };
+  auto restrict_to = [&](const Team& tm, int k) {   // level k's residual -> level k+1's b
+    const SLevel F = S[k], Cs = S[k + 1];
+    for (int c = tm.t; c < Cs.n; c += tm.n) {
+      const int J = c / Cs.mx, I = c - J * Cs.mx;
+      float r = 0.f;
+      for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di) {
+          const int i = 2 * I + di, j = 2 * J + dj;
+          if (i >= F.mx || j >= F.my) continue;
+          const int kf = i + F.mx * j;
+          r += F.b[kf] - F.sC[kf] * F.x[kf] - sl_offdiag(F, i, j, kf);
+        }
+      Cs.b[c] = r;
+    }
+    tm.sync();
+  };
+  auto prolong_from = [&](const Team& tm, int k) {   // level k += level k+1's correction
+    const SLevel F = S[k], Cs = S[k + 1];
+    for (int c = tm.t; c < F.n; c += tm.n) {
+      const int j = c / F.mx, i = c - j * F.mx;
+      F.x[c] += Cs.x[(i >> 1) + Cs.mx * (j >> 1)];
+    }
+    tm.sync();
+  };
+  int kw = last;   // levels kw .. last have at most 64 cells each
+  while (kw > k0 && S[kw - 1].n <= 64) --kw;
+  const Team cta{tid, nt, false}, w0{tid, 32, true};
+  for (int k = k0; k < kw; ++k) {
+    smooth(cta, k, nu1, true);
+    restrict_to(cta, k);
+  }
+  if (tid < 32) {
+    for (int k = kw; k < last; ++k) {
+      smooth(w0, k, nu1, true);
+      restrict_to(w0, k);
+    }
+    smooth(w0, last, coarse_sweeps, true);
+    for (int k = last - 1; k >= kw; --k) {
+      prolong_from(w0, k);
+      smooth(w0, k, nu2, false);
+    }
+  }
+  __syncthreads();
+  for (int k = kw - 1; k >= k0; --k) {
+    prolong_from(cta, k);
+    smooth(cta, k, nu2, false);
+  }
+  const Level& L0 = ls.L[k0];
+  const float* x0 = S[k0].x;
+  for (int c = tid; c < (int)L0.n; c += nt) L0.x[L0.n * g + c] = x0[c];
+}
+
 // ------------------------------------------------------------------------------------------------
 // Krylov pieces
 // ------------------------------------------------------------------------------------------------
