@@ -76,6 +76,9 @@ def parse():
                    help="timed low-order MGQD solves (MLOQD_FV) on the configuration's grid and groups; 0 skips")
     p.add_argument("--c4", type=int, default=0,
                    help="run only config 4 (1024^2, 64 groups, S16, in-place FP32 state) for this many time steps")
+    p.add_argument("--config4-steps", type=int, default=2,
+                   help="time steps of the config-4 leg (1024^2, 64 groups, S16, in-place FP32 state) in the default "
+                        "run; 0 = skip")
     p.add_argument("--mgqd-only", action="store_true",
                    help="run only the low-order MGQD leg (--mgqd solves) and print its JSON object")
     p.add_argument("--mlqd-steps", type=int, default=2,
@@ -974,6 +977,12 @@ def main():
         line["serving"] = run_serving(pkg, args.serving)
     if args.batch > 0 and ws == 1:
         line["batched"] = run_batch(pkg, args.batch)
+    if args.config4_steps > 0 and ws == 1:
+        torch.cuda.empty_cache()   # the leg needs ~171 of the device's ~178 GB
+        try:
+            line["config4"] = run_config4(pkg, torch, args.config4_steps)
+        except Exception as exc:   # reported, not fatal to the headline line
+            line["config4"] = {"error": repr(exc)[:300]}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(prob)
     if rank == 0:
