@@ -192,8 +192,6 @@ SIGNATURES = {
     "trt_avg_apnd_bnd": (_i, [_D, _D, _D, _D, _D, _i, _i, _i]),
     "trt_dmd_calc": (_i, [_D, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, _i, _d, _d,
                           ctypes.POINTER(ctypes.c_longlong)] + [_D] * 8),
-    "trt_set_wrap_ring": (_i, [_P, _i]),
-    "trt_get_wrap_ring": (_i, [_P]),
     "trt_mlqd_setup": (_i, [_P, _d, ctypes.POINTER(MlqdParams)]),
     "trt_mlqd_setup_range": (_i, [_P, _d, ctypes.POINTER(MlqdParams), _i, _i, _D]),
     "trt_mlqd_step": (_i, [_P, ctypes.POINTER(MlqdStats)]),

@@ -623,14 +623,6 @@ class TransportSweep:
         one thread-block cluster each); 0/1 = one CTA per sweep.  Re-lays out (zeroes) the state."""
         check(_lib.lib().trt_set_bands(self._h, int(bands)), "trt_set_bands")
 
-    def set_wrap_ring(self, on=True):
-        """FP32 sweep: the round wrap in a shared-memory ring where it fits (default on; trt_set_wrap_ring).
-        Re-lays out (zeroes) the state."""
-        check(_lib.lib().trt_set_wrap_ring(self._h, 1 if on else 0), "trt_set_wrap_ring")
-
-    def wrap_ring_rows(self):
-        return int(_lib.lib().trt_get_wrap_ring(self._h))
-
     def set_inplace(self, on=True):
         """One corner-state buffer swept in place (each sweep consumes I_crn_old: the next sweep must roll).
         Re-lays out (zeroes) the state."""
@@ -668,7 +660,6 @@ class TransportSweep:
         out = dict(zip(("warps", "slices", "dirs_per_lane", "stages", "splits"), [x.value for x in v]))
         out["wide_registers"] = int(_lib.lib().trt_get_register_mode(self._h))
         out["bands"] = int(_lib.lib().trt_get_bands(self._h))
-        out["wrap_ring"] = int(_lib.lib().trt_get_wrap_ring(self._h))
         return out
 
     def set_material(self, KapE_in, src_iso, c, Delt, Comp_Unit):

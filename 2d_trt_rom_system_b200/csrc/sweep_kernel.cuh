@@ -66,7 +66,6 @@ struct SweepArgs {
   Real* wrap;               // [4 ng][nx][mq][2]  top outflow of the last row of a round
   Real* part;               // [4*NH][ng][ny][nx][part_rec<Real>()]  moment partial records (physical cells)
   int* err;                 // error word (bit 0: TMA wait timed out)
-  int ring_rows;            // > 0: the round wrap kept in a shared-memory ring of this many rows (FP32, one band)
   unsigned max_polls;       // bound on mbarrier polls per wait of the sweep
   unsigned drain_polls;     // bound on the polls that drain outstanding copies after a timeout
 };
@@ -76,16 +75,14 @@ constexpr int kErrTmaTimeout = 1;
 // Dynamic shared memory of one sweep CTA: the TMA ring, its mbarriers, the row handoff, the direction
 // table and the moment-weight table (FP32 sweep: float2 pairs of direction slots, 6 rows).
 template <class Real>
-__host__ __device__ inline size_t sweep_smem_bytes(int W, long long chunk, int stages, int mqc, int D, int S,
-                                                   int ring_rows = 0) {
+__host__ __device__ inline size_t sweep_smem_bytes(int W, long long chunk, int stages, int mqc, int D, int S) {
   (void)mqc;
   size_t ring = (size_t)stages * W * chunk * sizeof(Real);
   size_t bars = (size_t)stages * sizeof(uint64_t);
   size_t hand = (size_t)2 * W * mqc * 2 * sizeof(Real);
   size_t dtab = (size_t)kNDirRow * D * S * sizeof(Real);
   size_t wtab = (size_t)6 * ((D + 1) / 2) * S * sizeof(float2) + 16;
-  size_t wring = ring_rows > 0 ? (size_t)ring_rows * mqc * 2 * sizeof(Real) + 16 : 0;
-  return ring + bars + hand + dtab + wtab + wring + 32;
+  return ring + bars + hand + dtab + wtab + 32;
 }
 
 // Reduce-scatter of the 16 moment slots over the S slices of a row (xor partners R, 2R, ..., 16):
@@ -177,13 +174,6 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
   constexpr int NP = (D + 1) / 2;
   float2* wt2 = reinterpret_cast<float2*>(
       (reinterpret_cast<uintptr_t>(dtab + kNDirRow * DS) + 15) & ~static_cast<uintptr_t>(15));
-  // Round wrap in shared memory (a.ring_rows > 0, FP32 with one band CTA): the top outflow of the band's last row at
-  // step T goes to row T mod L of the ring, and the first row of the next round reads it back P - H + 1 steps later
-  // (row (T - P + H - 1) mod L); with L = P - H + 2 a row is rewritten only after the step that reads it.  The
-  // first row then takes no inflow from global memory in rounds after the first.
-  const int wring_rows = kLeanFP32 ? a.ring_rows : 0;
-  Real* wring = reinterpret_cast<Real*>(
-      (reinterpret_cast<uintptr_t>(wt2 + 6 * NP * S) + 15) & ~static_cast<uintptr_t>(15));
 
   // direction table of this split: row k of split-local direction ml at dtab[k * DS + ml] (a compile-time row
   // stride, so that every table read is a constant offset from one per-lane base)
@@ -339,7 +329,7 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
           if (nn == 0) {
             hl[d] = bHin[ml * 2 * nx + 2 * in + bxo];
             hr[d] = bHin[ml * 2 * nx + 2 * in + 1 - bxo];
-          } else if (wring_rows == 0) {   // written by another band CTA (or this one): read through L2
+          } else {   // written by another band CTA (or this one): read through L2
             hl[d] = __ldcg(wrapc + (ipn * mqc + ml) * 2 + 0);
             hr[d] = __ldcg(wrapc + (ipn * mqc + ml) * 2 + 1);
           }
@@ -502,17 +492,15 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
       j = fy ? ny - 1 - jp : jp;
       const Real dx = mdx, dy = mdy, A4 = mA4, kp = mkp, qs = mqs;
 
-      // bottom inflow of a warp's first row from the warp below (shared memory, written last step), and of the
-      // band's first row in later rounds from the wrap ring
-      if (active && r == 0 && (warp > 0 || (wring_rows > 0 && n > 0))) {
-        const Real* src0 = warp > 0 ? hand + (((T - 1) & 1) * W + (warp - 1)) * mqc * 2
-                                    : wring + (size_t)((T - t.P + t.H - 1) % wring_rows) * mqc * 2;
+      // bottom inflow of a warp's first row from the warp below (shared memory, written last step)
+      if (active && r == 0 && warp > 0) {
   #pragma unroll
         for (int d = 0; d < D; ++d) {
           const int ml = d * S + s;
           if (d < D - 1 || s < s_last) {
-            hl[d] = src0[ml * 2];
-            hr[d] = src0[ml * 2 + 1];
+            const Real* src = hand + ((((T - 1) & 1) * W + (warp - 1)) * mqc + ml) * 2;
+            hl[d] = src[0];
+            hr[d] = src[1];
           }
         }
       }
@@ -520,8 +508,7 @@ __device__ __forceinline__ bool scb_sweep_body(const SweepArgs<Real>& a, const i
       const bool right_edge = active && (ip == nx - 1);
       const bool top_edge = active && (jp == ny - 1);
       const bool last_row = active && (r == R - 1) && (warp < W - 1 || t.nr > 1);
-      Real* hand_dst = (warp < W - 1) ? hand + ((T & 1) * W + warp) * mqc * 2
-                                      : (wring_rows > 0 ? wring + (size_t)(T % wring_rows) * mqc * 2 : wrapc + ip * mqc * 2);
+      Real* hand_dst = (warp < W - 1) ? hand + ((T & 1) * W + warp) * mqc * 2 : wrapc + ip * mqc * 2;
 
       // FP32 moment lane sums: acc2[v].x sums the lane's even direction slots, .y its odd ones (at most
       // ceil(D/2) terms each, one FP32 rounding per fused multiply-add); the two are added in FP64 at the

@@ -281,8 +281,6 @@ struct trt_ctx {
   cudaStream_t stream = nullptr;
   int Wreq = 0, Sreq = 0, NHreq = 0, NBreq = 0, stages = 2;   // NBreq: band CTAs per sweep (0: default)
   int regs = 0;                      // register level of the sweep kernel in use (set by setup_layout)
-  int ring_rows = 0;                 // rows of the shared-memory wrap ring (0: the wrap buffer in global memory)
-  bool ring_enabled = true;          // trt_set_wrap_ring
   int regs_req = -1;                 // -1: the highest level that keeps the grid resident; 0..2: at most that
   KernelCfg kc{8, 5};
   trt::Tiling t{};
@@ -515,7 +513,6 @@ int setup_layout(trt_ctx* c) {
   c->blk = trt::block_elems(t);
   // the highest register level whose variant keeps the whole grid resident (CTAs of at most 4 warps)
   c->regs = 0;
-  c->ring_rows = 0;
   const int cap = c->regs_req < 0 ? 2 : c->regs_req;
   for (int level = cap; level >= 1 && 32 * W <= 128; --level) {
     const size_t smem = smem_at(stages);
@@ -524,16 +521,6 @@ int setup_layout(trt_ctx* c) {
     if (per > 0 && 4LL * c->ng * NH * t.NB <= (long long)per * sm_count()) {
       c->regs = level;
       break;
-    }
-  }
-  // FP32 with one band CTA: the round wrap in a shared-memory ring, when the larger shared memory keeps the
-  // grid resident at the same register level
-  if (c->prec != TRT_PREC_FP64 && t.NB == 1 && t.nr > 1 && c->ring_enabled) {
-    const int L = t.P - t.H + 2;
-    const size_t smem = trt::sweep_smem_bytes<float>(W, chunk, stages, t.mqc, t.D, t.S, L);
-    if (smem <= (size_t)220 * 1024) {
-      const int per = sweep_ctas_per_sm<float>(c->kc, 32 * W, smem, c->regs);
-      if (per > 0 && 4LL * c->ng * NH <= (long long)per * sm_count()) c->ring_rows = L;
     }
   }
   const size_t sbytes = (size_t)c->state_elems() * esz;
@@ -662,7 +649,6 @@ trt::SweepArgs<Real> make_sweep_args(const trt_ctx* c) {
   a.wrap = (Real*)c->d_wrap;
   a.part = (Real*)c->d_part;
   a.err = c->d_err;
-  a.ring_rows = c->ring_rows;
   a.max_polls = c->wait_polls;
   a.drain_polls = 1u << 24;
   return a;
@@ -670,7 +656,7 @@ trt::SweepArgs<Real> make_sweep_args(const trt_ctx* c) {
 
 template <class Real>
 size_t sweep_smem(const trt_ctx* c) {
-  return trt::sweep_smem_bytes<Real>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D, c->t.S, c->ring_rows);
+  return trt::sweep_smem_bytes<Real>(c->t.W, c->chunk, c->stages, c->t.mqc, c->t.D, c->t.S);
 }
 
 template <class Real>
@@ -1285,11 +1271,9 @@ int batch_group_launch(trt_batch* b, std::vector<trt_ctx*>& grp, size_t args_off
   size_t smem = 0;
   for (size_t k = 0; k < grp.size(); ++k) {
     ha[k] = make_sweep_args<Real>(grp[k]);
-    ha[k].ring_rows = 0;   // one shared-memory size for every CTA of the launch: the wrap stays in global memory
     hf[k] = (int)total;
     total += 4LL * grp[k]->ng * grp[k]->t.NH * grp[k]->t.NB;
-    smem = std::max(smem, trt::sweep_smem_bytes<Real>(grp[k]->t.W, grp[k]->chunk, grp[k]->stages, grp[k]->t.mqc,
-                                                      grp[k]->t.D, grp[k]->t.S));
+    smem = std::max(smem, sweep_smem<Real>(grp[k]));
     grp[k]->swept = true;
   }
   if (total > (1LL << 30)) return TRT_ERR_ARG;
@@ -1881,14 +1865,6 @@ int trt_set_register_mode(trt_ctx* c, int mode) {
 }
 
 int trt_get_register_mode(const trt_ctx* c) { return c ? c->regs : TRT_ERR_ARG; }
-
-int trt_set_wrap_ring(trt_ctx* c, int on) {
-  if (!c || (on != 0 && on != 1)) return TRT_ERR_ARG;
-  c->ring_enabled = on != 0;
-  return setup_layout(c);
-}
-
-int trt_get_wrap_ring(const trt_ctx* c) { return c ? c->ring_rows : TRT_ERR_ARG; }
 
 int trt_get_tiling(const trt_ctx* c, int* W, int* S, int* D, int* stages, int* splits) {
   if (!c) return TRT_ERR_ARG;

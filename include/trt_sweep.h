@@ -298,12 +298,6 @@ int trt_snapshot_angular_groups(trt_ctx* ctx, int g0, int n_groups, float* I_avg
  * (zeroes) the state.  trt_get_register_mode returns the level in use. */
 int trt_set_register_mode(trt_ctx* ctx, int mode);
 int trt_get_register_mode(const trt_ctx* ctx);
-/* The round wrap of the FP32 sweep (the top outflow of a band's last row, read by the first row of the next
- * round P - H + 1 steps later) in a shared-memory ring of P - H + 2 rows instead of global memory: on (1, the
- * default) where the sweep has one band CTA and the larger shared memory keeps the whole grid resident.  Results
- * are bit-identical either way.  Re-lays out (zeroes) the state.  trt_get_wrap_ring: the ring's rows (0: off). */
-int trt_set_wrap_ring(trt_ctx* ctx, int on);
-int trt_get_wrap_ring(const trt_ctx* ctx);
 
 /* Autotuner: times one sweep of this handle's problem for each (direction splits 1..4) x (warps per CTA
  * 2, 3, 4, 5, 6, 8) x (bands 1, 2, 4) tiling whose CTAs are all resident at once (CUDA occupancy query),

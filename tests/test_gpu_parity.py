@@ -457,27 +457,6 @@ def test_register_variant_does_not_change_results(precision):
         assert np.array_equal(out[0][2][k], out[1][2][k]), k
 
 
-@pytest.mark.parametrize("shape", [(40, 70, 5, "S16", 4), (96, 200, 3, "S12", 4), (33, 130, 4, "S8", 2)])
-def test_wrap_ring_does_not_change_results(shape):
-    """FP32: the round wrap in the shared-memory ring and in global memory give bit-identical outputs over
-    several rounds (ny well above the band height) and two rolled steps."""
-    nx, ny, G, quad, W = shape
-    prob = pkg.problems.random_small(36, nx, ny, G, quad)
-    d = sweep_inputs(prob, seed=36)
-    out = []
-    for on in (False, True):
-        with resident(d, precision="mixed", tiling=dict(warps=W)) as s:
-            s.set_wrap_ring(on)
-            s.put_state(d["I_crn_old"])
-            s.sweep(moments=True)
-            s.sweep(roll=True, moments=True)
-            out.append((s.wrap_ring_rows(), s.get_state(), s.moments(["Eg_avg", "Fxg_edgV", "Fyg_edgH", "Cg_T"])))
-    assert out[0][0] == 0 and out[1][0] > 0
-    assert np.array_equal(out[0][1], out[1][1])
-    for k in out[0][2]:
-        assert np.array_equal(out[0][2][k], out[1][2][k]), k
-
-
 @pytest.mark.parametrize("name,make", SHAPES[:5], ids=[s[0] for s in SHAPES[:5]])
 def test_resident_sweep_matches_gaussian_elimination_oracle(oracle, name, make):
     """The resident sweep with the isotropic per-cell source (the kernel the benchmark times) against the
