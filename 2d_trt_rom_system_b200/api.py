@@ -285,6 +285,12 @@ def mgqd_set_graphs(on=True):
     check(_lib.lib().trt_mgqd_set_graphs(int(bool(on))), "mgqd_set_graphs")
 
 
+def mgqd_set_fused_levels(on=True):
+    """Run the multigrid preconditioner's fine-level passes as one tiled kernel per level and direction (default)
+    or one kernel per half-sweep; the results are identical."""
+    check(_lib.lib().trt_mgqd_set_fused_levels(int(bool(on))), "mgqd_set_fused_levels")
+
+
 def mgqd_last_stats():
     """(device ms of the last MLOQD_FV solve without its copies, largest iteration count, device ms of
     its first matrix-vector product)."""

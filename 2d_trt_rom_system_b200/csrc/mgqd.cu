@@ -47,6 +47,7 @@ struct Settings {
   double tol = 1e-13;
   int maxit = 1000;
   bool graphs = true;   // replay BiCGSTAB iteration blocks as CUDA graphs
+  bool fused = true;    // one tiled kernel per level and direction of the V-cycle (else one per half-sweep)
 };
 Settings g_settings;
 
@@ -70,6 +71,8 @@ struct Solver {
   bool matvec_timed = false;
   bool time_matvec = true;          // time the first iteration's matrix-vector product (trt_mgqd_last_stats)
   bool use_graphs = true;           // replay iteration blocks as a CUDA graph
+  bool use_fused = true;            // fused tiled level passes in the V-cycle
+  bool g_fused = true;              // the form the recorded graph was made with
   bool update_test = false;         // SPARSKIT's solution-update stopping test (Krylov::update_test)
   cudaGraphExec_t gexec = nullptr;  // kCheckEvery iterations, recorded on first use
   int g_nodes = 0, g_maxit = -1, g_rel = -1;
@@ -218,6 +221,7 @@ int Solver::krylov(cudaStream_t s) {
   K.update_test = update_test ? 1 : 0;
   K.atol = 1e-15;   // fpar(2) of QD_SOLVERS.f08:445
   use_graphs = g_settings.graphs;
+  use_fused = g_settings.fused;
   prec_coef_kernel<<<gpos, kRedBlock, 0, s>>>(d, cf, ls.L[0]);
   MG_LAUNCHED();
   for (int k = 0; k + 1 < ls.n; ++k) {
@@ -239,10 +243,16 @@ int Solver::krylov(cudaStream_t s) {
     MG_CUDA(cudaGetLastError());
     return TRT_OK;
   };
+  static_assert(2 * kNu1 <= kTH && 2 * kNu2 <= kTH, "the tile halo covers the level's half-sweeps");
   auto vcycle = [&]() -> int {
     int rc;
     for (int k = 0; k < k0; ++k) {
       const Level& L = ls.L[k];
+      if (use_fused) {
+        smooth_restrict_tile_kernel<<<dim3(level_tiles(L), ng), kTileThreads, 0, s>>>(L, ls.L[k + 1], K.done, kNu1);
+        if ((rc = launched())) return rc;
+        continue;
+      }
       const dim3 gl(grid1(L.n), ng);
       for (int sw = 0; sw < kNu1; ++sw) {
         smooth_kernel<<<gl, 256, 0, s>>>(L, K.done, 0, sw == 0 ? 1 : 0);
@@ -260,6 +270,11 @@ int Solver::krylov(cudaStream_t s) {
     if ((rc = launched())) return rc;
     for (int k = k0 - 1; k >= 0; --k) {
       const Level& L = ls.L[k];
+      if (use_fused) {
+        prolong_smooth_tile_kernel<<<dim3(level_tiles(L), ng), kTileThreads, 0, s>>>(L, ls.L[k + 1], K.done, kNu2);
+        if ((rc = launched())) return rc;
+        continue;
+      }
       const dim3 gl(grid1(L.n), ng);
       prolong_kernel<<<gl, 256, 0, s>>>(L, ls.L[k + 1], K.done);
       if ((rc = launched())) return rc;
@@ -308,7 +323,7 @@ int Solver::krylov(cudaStream_t s) {
   // kernels take the solver's fixed buffers and K by value, so the graph is recorded again only when the
   // tolerance or the iteration limit in K changes.
   auto block = [&]() -> int {
-    if (!gexec || g_tol != K.tol || g_maxit != K.maxit || g_rel != K.update_test) {
+    if (!gexec || g_tol != K.tol || g_maxit != K.maxit || g_rel != K.update_test || g_fused != use_fused) {
       if (gexec) {
         cudaGraphExecDestroy(gexec);
         gexec = nullptr;
@@ -337,6 +352,7 @@ int Solver::krylov(cudaStream_t s) {
       g_tol = K.tol;
       g_maxit = K.maxit;
       g_rel = K.update_test;
+      g_fused = use_fused;
     }
     MG_CUDA(cudaGraphLaunch(gexec, s));
     trt_host::add_launches((unsigned long long)g_nodes);
@@ -452,6 +468,12 @@ int trt_mgqd_set_tolerance(double tol, int maxit) {
 int trt_mgqd_set_graphs(int on) {
   std::lock_guard<std::mutex> lk(g_cache.mu);
   g_settings.graphs = on != 0;
+  return TRT_OK;
+}
+
+int trt_mgqd_set_fused_levels(int on) {
+  std::lock_guard<std::mutex> lk(g_cache.mu);
+  g_settings.fused = on != 0;
   return TRT_OK;
 }
 

@@ -345,6 +345,127 @@ __global__ void prolong_kernel(const Level F, const Level Cs, const int* __restr
   prolong_cell(F, Cs, g, (int)(p % F.mx), (int)(p / F.mx));
 }
 
+// ---- fused level passes of the V-cycle (tiles with a halo) -------------------------------------------
+// A red-black sweep updates a cell from its four neighbours, so after h half-sweeps a cell's value depends only
+// on cells within h steps of it.  A CTA that holds a tile of kTX x kTY cells plus a halo of kTH cells can therefore
+// run a level's half-sweeps on its own copy, each one on a region one cell narrower than the one before, and end
+// with the exact values of the tile and the ring around it (the halo cells are recomputed by the neighbouring
+// tiles' CTAs).  Every cell is computed with the operations of smooth_cell / restrict_cell / prolong_cell in the
+// same order, so the results equal those of the per-half-sweep kernels bit for bit.  kTH >= 2 nu: the descent's
+// first half-sweep (zero iterate) needs no neighbour, its other 2 nu - 1 and the residual need one ring each; the
+// ascent's 2 nu half-sweeps need one ring each (the prolongation is pointwise).
+constexpr int kTX = 32, kTY = 16, kTH = 4;
+constexpr int kRX = kTX + 2 * kTH, kRY = kTY + 2 * kTH, kRN = kRX * kRY;
+constexpr int kTileThreads = 256;
+
+__host__ __device__ inline int level_tiles(const Level& L) {
+  return (int)(((L.mx + kTX - 1) / kTX) * ((L.my + kTY - 1) / kTY));
+}
+
+// The tile's region (interior plus halo) in shared memory: region cell q = ri + kRX rj is grid cell
+// (i0 + ri, j0 + rj).
+struct TileRegion {
+  float b[kRN], sC[kRN], sW[kRN], sE[kRN], sS[kRN], sN[kRN], x[kRN];
+};
+
+__device__ __forceinline__ float t_offdiag(const TileRegion& R, const Level& L, int i, int j, int q) {
+  float s = 0.f;
+  if (i > 0) s += R.sW[q] * R.x[q - 1];
+  if (i + 1 < L.mx) s += R.sE[q] * R.x[q + 1];
+  if (j > 0) s += R.sS[q] * R.x[q - kRX];
+  if (j + 1 < L.my) s += R.sN[q] * R.x[q + kRX];
+  return s;
+}
+
+// Loads the region's operator and right-hand side (and, for the ascent, the iterate plus the coarse correction).
+__device__ __forceinline__ void tile_load(TileRegion& R, const Level& L, const Level* Cs, int g, int i0, int j0) {
+  const long o = L.n * g;
+  for (int q = threadIdx.x; q < kRN; q += blockDim.x) {
+    const int rj = q / kRX, ri = q - rj * kRX;
+    const int i = i0 + ri, j = j0 + rj;
+    if (i < 0 || i >= L.mx || j < 0 || j >= L.my) continue;
+    const long k = o + i + (long)L.mx * j;
+    R.b[q] = L.b[k];
+    R.sC[q] = L.sC[k];
+    R.sW[q] = L.sW[k];
+    R.sE[q] = L.sE[k];
+    R.sS[q] = L.sS[k];
+    R.sN[q] = L.sN[k];
+    if (Cs) R.x[q] = L.x[k] + Cs->x[Cs->n * g + (i >> 1) + (long)Cs->mx * (j >> 1)];   // prolong_cell
+  }
+}
+
+// One colour of a red-black half-sweep over region cells [lo, kRX - lo) x [lo, kRY - lo) of the grid.
+__device__ __forceinline__ void tile_sweep(TileRegion& R, const Level& L, int i0, int j0, int lo, int color,
+                                           bool zero) {
+  const int w = kRX - 2 * lo, h = kRY - 2 * lo;
+  for (int p = threadIdx.x; p < w * h; p += blockDim.x) {
+    const int rj = lo + p / w, ri = lo + p % w;
+    const int i = i0 + ri, j = j0 + rj;
+    if (i < 0 || i >= L.mx || j < 0 || j >= L.my) continue;
+    const int q = ri + kRX * rj;
+    if (((i + j) & 1) != color) {
+      if (zero) R.x[q] = 0.f;
+      continue;
+    }
+    R.x[q] = zero ? R.b[q] / R.sC[q] : (R.b[q] - t_offdiag(R, L, i, j, q)) / R.sC[q];
+  }
+  __syncthreads();
+}
+
+// Descent on a level: nu pre-smoothing sweeps from a zero iterate, then the residual restricted to the coarse
+// right-hand side; writes the tile's iterate and its coarse cells' b.
+__global__ void __launch_bounds__(kTileThreads) smooth_restrict_tile_kernel(const Level L, const Level Cs,
+                                                                            const int* __restrict__ done, int nu) {
+  const int g = blockIdx.y;
+  if (done[g]) return;
+  __shared__ TileRegion R;
+  const int ntx = (L.mx + kTX - 1) / kTX;
+  const int ti = (int)(blockIdx.x % ntx) * kTX, tj = (int)(blockIdx.x / ntx) * kTY;   // first interior cell
+  const int i0 = ti - kTH, j0 = tj - kTH;
+  tile_load(R, L, nullptr, g, i0, j0);
+  __syncthreads();
+  for (int hs = 0; hs < 2 * nu; ++hs) tile_sweep(R, L, i0, j0, hs, hs & 1, hs == 0);
+  // coarse cells of the tile (kTX, kTY even: their fine cells are interior cells)
+  for (int p = threadIdx.x; p < (kTX / 2) * (kTY / 2); p += blockDim.x) {
+    const int I = ti / 2 + p % (kTX / 2), J = tj / 2 + p / (kTX / 2);
+    if (I >= Cs.mx || J >= Cs.my) continue;
+    float r = 0.f;
+    for (int dj = 0; dj < 2; ++dj)
+      for (int di = 0; di < 2; ++di) {
+        const int i = 2 * I + di, j = 2 * J + dj;
+        if (i >= L.mx || j >= L.my) continue;
+        const int q = (i - i0) + kRX * (j - j0);
+        r += R.b[q] - R.sC[q] * R.x[q] - t_offdiag(R, L, i, j, q);
+      }
+    Cs.b[Cs.n * g + I + (long)Cs.mx * J] = r;
+  }
+  const long o = L.n * g;
+  for (int p = threadIdx.x; p < kTX * kTY; p += blockDim.x) {
+    const int i = ti + p % kTX, j = tj + p / kTX;
+    if (i < L.mx && j < L.my) L.x[o + i + (long)L.mx * j] = R.x[(i - i0) + kRX * (j - j0)];
+  }
+}
+
+// Ascent on a level: the coarse correction added, then nu post-smoothing sweeps; writes the tile's iterate.
+__global__ void __launch_bounds__(kTileThreads) prolong_smooth_tile_kernel(const Level L, const Level Cs,
+                                                                           const int* __restrict__ done, int nu) {
+  const int g = blockIdx.y;
+  if (done[g]) return;
+  __shared__ TileRegion R;
+  const int ntx = (L.mx + kTX - 1) / kTX;
+  const int ti = (int)(blockIdx.x % ntx) * kTX, tj = (int)(blockIdx.x / ntx) * kTY;
+  const int i0 = ti - kTH, j0 = tj - kTH;
+  tile_load(R, L, &Cs, g, i0, j0);
+  __syncthreads();
+  for (int hs = 0; hs < 2 * nu; ++hs) tile_sweep(R, L, i0, j0, hs + 1, hs & 1, false);
+  const long o = L.n * g;
+  for (int p = threadIdx.x; p < kTX * kTY; p += blockDim.x) {
+    const int i = ti + p % kTX, j = tj + p / kTX;
+    if (i < L.mx && j < L.my) L.x[o + i + (long)L.mx * j] = R.x[(i - i0) + kRX * (j - j0)];
+  }
+}
+
 struct LevelSet {
   Level L[kMaxLevels];
   int n;

@@ -209,6 +209,11 @@ int trt_mgqd_set_tolerance(double tol, int maxit);
  * time step) replay each block of iterations between two host convergence checks as one CUDA graph (on, the
  * default) or launch its kernels one by one (0); the kernels and their order are the same either way. */
 int trt_mgqd_set_graphs(int on);
+/* No counterpart in the reference.  The multigrid preconditioner of those solves runs each fine level's
+ * pre-smoothing and restriction, and its prolongation and post-smoothing, as one kernel over tiles with a halo
+ * (on, the default) or as one kernel per half-sweep (0); the cell arithmetic and its order are the same, so the
+ * results are identical. */
+int trt_mgqd_set_fused_levels(int on);
 
 /* Of the last trt_mloqd_fv call: device time (ms, events around the solve, excluding host<->device
  * copies), the largest iteration count, and the device time of its first matrix-vector product (ms;

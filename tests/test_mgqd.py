@@ -116,7 +116,9 @@ def rel_err(a, b):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", CASES + [(48, 40, 12, 1.0, 6, False), (33, 64, 5, 0.5, 7, True)])
+# (100, 72): a fine level above the shared-memory V-cycle, in ragged tiles of the fused level passes
+@pytest.mark.parametrize("case", CASES + [(48, 40, 12, 1.0, 6, False), (33, 64, 5, 0.5, 7, True),
+                                          (100, 72, 3, 1.0, 8, False)])
 def test_device_mloqd_fv_matches_oracle(case, oracle):
     d, c, dt, th = make(*case, oracle)
     ref = oracle.mloqd_fv(d, c, dt, th, res_calc=True, threads=4)
@@ -180,6 +182,24 @@ def test_graph_replayed_iterations_are_bit_identical(oracle):
     assert (a["MGQD_Kits"] > 9).any()    # more than one block of iterations
     for k in ("Eg_avg", "Eg_edgV", "Fxg_edgV", "MGQD_Residual", "MGQD_Kits"):
         assert np.array_equal(a[k], b[k]) and np.array_equal(b[k], c2[k]), k
+
+
+@pytest.mark.gpu
+def test_fused_level_passes_are_bit_identical(oracle):
+    """The V-cycle's fine levels run as one tiled kernel per level and direction (pre-smoothing + restriction,
+    prolongation + post-smoothing) or as one kernel per half-sweep: the same iterates, bit for bit.  300 x 140
+    has two levels above the shared-memory V-cycle (300 x 140, 150 x 70), both in ragged tiles."""
+    d, c, dt, th = make(300, 140, 3, 1.0, 21, False, oracle)
+    try:
+        pkg.mgqd_set_fused_levels(False)
+        a = call_device(d, c, dt, th)
+        pkg.mgqd_set_fused_levels(True)
+        b = call_device(d, c, dt, th)
+    finally:
+        pkg.mgqd_set_fused_levels(True)
+    assert (a["MGQD_Kits"] > 4).all()
+    for k in ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH", "MGQD_Residual", "MGQD_Kits"):
+        assert np.array_equal(a[k], b[k]), k
 
 
 @pytest.mark.gpu
