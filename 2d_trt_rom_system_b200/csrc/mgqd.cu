@@ -168,6 +168,7 @@ int Solver::init(int nx, int ny, int ng, bool own_inputs) {
     L.n = (long)mx * my;
     M(&L.sC, (size_t)L.n * ng); M(&L.sW, (size_t)L.n * ng); M(&L.sE, (size_t)L.n * ng);
     M(&L.sS, (size_t)L.n * ng); M(&L.sN, (size_t)L.n * ng); M(&L.x, (size_t)L.n * ng); M(&L.b, (size_t)L.n * ng);
+    M(&L.xd, (size_t)L.n * ng);
     if (rc) return rc;
     if (mx <= 2 && my <= 2) break;
     mx = (mx + 1) / 2;

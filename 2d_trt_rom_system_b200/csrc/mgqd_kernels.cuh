@@ -70,6 +70,7 @@ struct Level {
   int mx, my;
   long n;                                    // cells per group
   float *sC, *sW, *sE, *sS, *sN, *x, *b;     // [group][cell]
+  float* xd;                                 // [group][cell] the fused descent's iterate (read by the ascent)
 };
 
 struct Scal {
@@ -354,6 +355,8 @@ __global__ void prolong_kernel(const Level F, const Level Cs, const int* __restr
 // same order, so the results equal those of the per-half-sweep kernels bit for bit.  kTH >= 2 nu: the descent's
 // first half-sweep (zero iterate) needs no neighbour, its other 2 nu - 1 and the residual need one ring each; the
 // ascent's 2 nu half-sweeps need one ring each (the prolongation is pointwise).
+// A tile's halo belongs to its neighbours' interiors, which other CTAs of the same launch write: so no pass reads
+// the array it writes.  The descent writes its iterate to xd, and the ascent reads xd and writes x.
 constexpr int kTX = 32, kTY = 16, kTH = 4;
 constexpr int kRX = kTX + 2 * kTH, kRY = kTY + 2 * kTH, kRN = kRX * kRY;
 constexpr int kTileThreads = 256;
@@ -377,7 +380,8 @@ __device__ __forceinline__ float t_offdiag(const TileRegion& R, const Level& L, 
   return s;
 }
 
-// Loads the region's operator and right-hand side (and, for the ascent, the iterate plus the coarse correction).
+// Loads the region's operator and right-hand side (and, for the ascent, the descent's iterate plus the coarse
+// correction).
 __device__ __forceinline__ void tile_load(TileRegion& R, const Level& L, const Level* Cs, int g, int i0, int j0) {
   const long o = L.n * g;
   for (int q = threadIdx.x; q < kRN; q += blockDim.x) {
@@ -391,7 +395,7 @@ __device__ __forceinline__ void tile_load(TileRegion& R, const Level& L, const L
     R.sE[q] = L.sE[k];
     R.sS[q] = L.sS[k];
     R.sN[q] = L.sN[k];
-    if (Cs) R.x[q] = L.x[k] + Cs->x[Cs->n * g + (i >> 1) + (long)Cs->mx * (j >> 1)];   // prolong_cell
+    if (Cs) R.x[q] = L.xd[k] + Cs->x[Cs->n * g + (i >> 1) + (long)Cs->mx * (j >> 1)];   // prolong_cell
   }
 }
 
@@ -414,7 +418,7 @@ __device__ __forceinline__ void tile_sweep(TileRegion& R, const Level& L, int i0
 }
 
 // Descent on a level: nu pre-smoothing sweeps from a zero iterate, then the residual restricted to the coarse
-// right-hand side; writes the tile's iterate and its coarse cells' b.
+// right-hand side; writes the tile's iterate (to xd) and its coarse cells' b.
 __global__ void __launch_bounds__(kTileThreads) smooth_restrict_tile_kernel(const Level L, const Level Cs,
                                                                             const int* __restrict__ done, int nu) {
   const int g = blockIdx.y;
@@ -443,11 +447,12 @@ __global__ void __launch_bounds__(kTileThreads) smooth_restrict_tile_kernel(cons
   const long o = L.n * g;
   for (int p = threadIdx.x; p < kTX * kTY; p += blockDim.x) {
     const int i = ti + p % kTX, j = tj + p / kTX;
-    if (i < L.mx && j < L.my) L.x[o + i + (long)L.mx * j] = R.x[(i - i0) + kRX * (j - j0)];
+    if (i < L.mx && j < L.my) L.xd[o + i + (long)L.mx * j] = R.x[(i - i0) + kRX * (j - j0)];
   }
 }
 
-// Ascent on a level: the coarse correction added, then nu post-smoothing sweeps; writes the tile's iterate.
+// Ascent on a level: the coarse correction added to the descent's iterate (xd), then nu post-smoothing sweeps;
+// writes the tile's iterate (to x).
 __global__ void __launch_bounds__(kTileThreads) prolong_smooth_tile_kernel(const Level L, const Level Cs,
                                                                            const int* __restrict__ done, int nu) {
   const int g = blockIdx.y;

@@ -185,21 +185,25 @@ def test_graph_replayed_iterations_are_bit_identical(oracle):
 
 
 @pytest.mark.gpu
-def test_fused_level_passes_are_bit_identical(oracle):
+@pytest.mark.parametrize("shape", [(300, 140, 3), (512, 384, 4)])
+def test_fused_level_passes_are_bit_identical(shape, oracle):
     """The V-cycle's fine levels run as one tiled kernel per level and direction (pre-smoothing + restriction,
-    prolongation + post-smoothing) or as one kernel per half-sweep: the same iterates, bit for bit.  300 x 140
-    has two levels above the shared-memory V-cycle (300 x 140, 150 x 70), both in ragged tiles."""
-    d, c, dt, th = make(300, 140, 3, 1.0, 21, False, oracle)
+    prolongation + post-smoothing) or as one kernel per half-sweep: the same iterates, bit for bit, and the same
+    again on a repeat (a tile's halo is its neighbours' interior, written by other CTAs of the same launch: no pass
+    may read what it writes).  300 x 140 has two levels above the shared-memory V-cycle in ragged tiles; 512 x 384
+    x 4 groups runs 1536 tiles per launch on its finest level, several waves of CTAs."""
+    d, c, dt, th = make(*shape, 1.0, 21, False, oracle)
     try:
         pkg.mgqd_set_fused_levels(False)
         a = call_device(d, c, dt, th)
         pkg.mgqd_set_fused_levels(True)
         b = call_device(d, c, dt, th)
+        b2 = call_device(d, c, dt, th)
     finally:
         pkg.mgqd_set_fused_levels(True)
     assert (a["MGQD_Kits"] > 4).all()
     for k in ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH", "MGQD_Residual", "MGQD_Kits"):
-        assert np.array_equal(a[k], b[k]), k
+        assert np.array_equal(a[k], b[k]) and np.array_equal(b[k], b2[k]), k
 
 
 @pytest.mark.gpu
