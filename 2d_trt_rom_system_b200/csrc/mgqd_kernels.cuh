@@ -520,20 +520,22 @@ __host__ __device__ inline size_t small_vcycle_smem_bytes(const LevelSet& ls, in
   return n * 7 * sizeof(float);
 }
 
-// One level of the shared-memory V-cycle: its extents and its arrays in shared memory (cell c = i + mx j).
+// One level of the shared-memory V-cycle: its extents and the offsets of its arrays in the dynamic shared array
+// (cell c = i + mx j).  Offsets from the kernel's `extern __shared__` base, not pointers, so that every access is
+// a shared-memory one to the compiler (no generic addressing, and no possible alias with the global loads).
 struct SLevel {
   int mx, my, n;
-  float *sC, *sW, *sE, *sS, *sN, *x, *b;
+  int oC, oW, oE, oS, oN, ox, ob;
 };
 
 // The operations of smooth_cell / restrict_cell / prolong_cell on a shared-memory level, term for term in the
 // same order (32-bit indices; every phase visits only the cells it writes).
-__device__ __forceinline__ float sl_offdiag(const SLevel& L, int i, int j, int k) {
+__device__ __forceinline__ float sl_offdiag(const float* v, const SLevel& L, int i, int j, int k) {
   float s = 0.f;
-  if (i > 0) s += L.sW[k] * L.x[k - 1];
-  if (i + 1 < L.mx) s += L.sE[k] * L.x[k + 1];
-  if (j > 0) s += L.sS[k] * L.x[k - L.mx];
-  if (j + 1 < L.my) s += L.sN[k] * L.x[k + L.mx];
+  if (i > 0) s += v[L.oW + k] * v[L.ox + k - 1];
+  if (i + 1 < L.mx) s += v[L.oE + k] * v[L.ox + k + 1];
+  if (j > 0) s += v[L.oS + k] * v[L.ox + k - L.mx];
+  if (j + 1 < L.my) s += v[L.oN + k] * v[L.ox + k + L.mx];
   return s;
 }
 
@@ -546,13 +548,13 @@ __global__ void __launch_bounds__(1024) small_vcycle_smem_kernel(const LevelSet 
   const int last = ls.n - 1;
   const int tid = threadIdx.x, nt = blockDim.x;
   if (tid == 0) {
-    float* p = vsm;
+    int p = 0;
     for (int k = k0; k <= last; ++k) {
       SLevel& V = S[k];
       V.mx = ls.L[k].mx;
       V.my = ls.L[k].my;
       V.n = (int)ls.L[k].n;
-      float** f[7] = {&V.sC, &V.sW, &V.sE, &V.sS, &V.sN, &V.x, &V.b};
+      int* f[7] = {&V.oC, &V.oW, &V.oE, &V.oS, &V.oN, &V.ox, &V.ob};
       for (int q = 0; q < 7; ++q) {
         *f[q] = p;
         p += V.n;
@@ -560,17 +562,19 @@ __global__ void __launch_bounds__(1024) small_vcycle_smem_kernel(const LevelSet 
     }
   }
   __syncthreads();
+  // copy-in: shared stores cannot alias the global loads, so the loads of a thread's cells go out together
   for (int k = k0; k <= last; ++k) {
     const SLevel V = S[k];
     const Level& L = ls.L[k];
     const long o = L.n * g;
+#pragma unroll 4
     for (int c = tid; c < V.n; c += nt) {
-      V.sC[c] = L.sC[o + c];
-      V.sW[c] = L.sW[o + c];
-      V.sE[c] = L.sE[o + c];
-      V.sS[c] = L.sS[o + c];
-      V.sN[c] = L.sN[o + c];
-      if (k == k0) V.b[c] = L.b[o + c];
+      vsm[V.oC + c] = L.sC[o + c];
+      vsm[V.oW + c] = L.sW[o + c];
+      vsm[V.oE + c] = L.sE[o + c];
+      vsm[V.oS + c] = L.sS[o + c];
+      vsm[V.oN + c] = L.sN[o + c];
+      if (k == k0) vsm[V.ob + c] = L.b[o + c];
     }
   }
   __syncthreads();
@@ -585,34 +589,41 @@ __global__ void __launch_bounds__(1024) small_vcycle_smem_kernel(const LevelSet 
       else __syncthreads();
     }
   };
+  float* v = vsm;
   // one colour of a red-black sweep; zero: the iterate is zero (this colour takes b/sC, the other is cleared)
-  auto sweep = [&](const Team& tm, int k, int color, bool zero) {
-    const SLevel L = S[k];
+  auto sweep = [&](const Team& tm, const SLevel& L, int color, bool zero) {
     if (zero) {
       for (int c = tm.t; c < L.n; c += tm.n) {
         const int j = c / L.mx, i = c - j * L.mx;
-        L.x[c] = ((i + j) & 1) == color ? L.b[c] / L.sC[c] : 0.f;
+        v[L.ox + c] = ((i + j) & 1) == color ? v[L.ob + c] / v[L.oC + c] : 0.f;
       }
     } else {
       const int hx = (L.mx + 1) >> 1;   // cells of one colour per row, at most
-      for (int q = tm.t; q < hx * L.my; q += tm.n) {
-        const int j = q / hx;
-        const int i = 2 * (q - j * hx) + ((j + color) & 1);
-        if (i >= L.mx) continue;
-        const int c = i + L.mx * j;
-        L.x[c] = (L.b[c] - sl_offdiag(L, i, j, c)) / L.sC[c];
+      // q = t, t + n, ... as (row j, position r in the row), advanced without a division per cell
+      const int dj = tm.n / hx, dr = tm.n - dj * hx;
+      int j = tm.t / hx, r = tm.t - j * hx;
+      for (; j < L.my; j += dj) {
+        const int i = 2 * r + ((j + color) & 1);
+        if (i < L.mx) {
+          const int c = i + L.mx * j;
+          v[L.ox + c] = (v[L.ob + c] - sl_offdiag(v, L, i, j, c)) / v[L.oC + c];
+        }
+        r += dr;
+        if (r >= hx) {
+          r -= hx;
+          ++j;
+        }
       }
     }
     tm.sync();
   };
-  auto smooth = [&](const Team& tm, int k, int sweeps, bool zero) {
+  auto smooth = [&](const Team& tm, const SLevel& L, int sweeps, bool zero) {
     for (int sw = 0; sw < sweeps; ++sw) {
-      sweep(tm, k, 0, zero && sw == 0);
-      sweep(tm, k, 1, false);
+      sweep(tm, L, 0, zero && sw == 0);
+      sweep(tm, L, 1, false);
     }
   };
-  auto restrict_to = [&](const Team& tm, int k) {   // level k's residual -> level k+1's b
-    const SLevel F = S[k], Cs = S[k + 1];
+  auto restrict_to = [&](const Team& tm, const SLevel& F, const SLevel& Cs) {   // F's residual -> Cs's b
     for (int c = tm.t; c < Cs.n; c += tm.n) {
       const int J = c / Cs.mx, I = c - J * Cs.mx;
       float r = 0.f;
@@ -621,17 +632,16 @@ __global__ void __launch_bounds__(1024) small_vcycle_smem_kernel(const LevelSet 
           const int i = 2 * I + di, j = 2 * J + dj;
           if (i >= F.mx || j >= F.my) continue;
           const int kf = i + F.mx * j;
-          r += F.b[kf] - F.sC[kf] * F.x[kf] - sl_offdiag(F, i, j, kf);
+          r += v[F.ob + kf] - v[F.oC + kf] * v[F.ox + kf] - sl_offdiag(v, F, i, j, kf);
         }
-      Cs.b[c] = r;
+      v[Cs.ob + c] = r;
     }
     tm.sync();
   };
-  auto prolong_from = [&](const Team& tm, int k) {   // level k += level k+1's correction
-    const SLevel F = S[k], Cs = S[k + 1];
+  auto prolong_from = [&](const Team& tm, const SLevel& F, const SLevel& Cs) {   // F += Cs's correction
     for (int c = tm.t; c < F.n; c += tm.n) {
       const int j = c / F.mx, i = c - j * F.mx;
-      F.x[c] += Cs.x[(i >> 1) + Cs.mx * (j >> 1)];
+      v[F.ox + c] += v[Cs.ox + (i >> 1) + Cs.mx * (j >> 1)];
     }
     tm.sync();
   };
@@ -639,28 +649,32 @@ __global__ void __launch_bounds__(1024) small_vcycle_smem_kernel(const LevelSet 
   while (kw > k0 && S[kw - 1].n <= 64) --kw;
   const Team cta{tid, nt, false}, w0{tid, 32, true};
   for (int k = k0; k < kw; ++k) {
-    smooth(cta, k, nu1, true);
-    restrict_to(cta, k);
+    const SLevel F = S[k], Cs = S[k + 1];
+    smooth(cta, F, nu1, true);
+    restrict_to(cta, F, Cs);
   }
   if (tid < 32) {
     for (int k = kw; k < last; ++k) {
-      smooth(w0, k, nu1, true);
-      restrict_to(w0, k);
+      const SLevel F = S[k], Cs = S[k + 1];
+      smooth(w0, F, nu1, true);
+      restrict_to(w0, F, Cs);
     }
-    smooth(w0, last, coarse_sweeps, true);
+    smooth(w0, S[last], coarse_sweeps, true);
     for (int k = last - 1; k >= kw; --k) {
-      prolong_from(w0, k);
-      smooth(w0, k, nu2, false);
+      const SLevel F = S[k], Cs = S[k + 1];
+      prolong_from(w0, F, Cs);
+      smooth(w0, F, nu2, false);
     }
   }
   __syncthreads();
   for (int k = kw - 1; k >= k0; --k) {
-    prolong_from(cta, k);
-    smooth(cta, k, nu2, false);
+    const SLevel F = S[k], Cs = S[k + 1];
+    prolong_from(cta, F, Cs);
+    smooth(cta, F, nu2, false);
   }
   const Level& L0 = ls.L[k0];
-  const float* x0 = S[k0].x;
-  for (int c = tid; c < (int)L0.n; c += nt) L0.x[L0.n * g + c] = x0[c];
+  const SLevel V0 = S[k0];
+  for (int c = tid; c < (int)L0.n; c += nt) L0.x[L0.n * g + c] = v[V0.ox + c];
 }
 
 // ------------------------------------------------------------------------------------------------
