@@ -11,5 +11,6 @@ from .api import (COLLAPSE_INTENSITIES, COLLAPSE_MG_EF, DMD_Calc, DMD_RECONSTRUC
                   MGQD_In_Calc, MLOQD_FV, OLD_GREY_COEFS, OLD_MGQD_COEFS, POD_RECONSTRUCT, POD_Calc, RT_BC_UPDATE,
                   LINEAR_INTERPOLATION, TRANSPORT_SCB, Batch,
                   Bg_planck_calc, Cbar_Calc, Cg_Calc, TransportSweep, fg_Calc, kernel_launches, mgqd_last_stats,
-                  mgqd_set_fused_levels, mgqd_set_graphs, mgqd_set_tolerance, required_bytes)
+                  mgqd_set_fused_levels, mgqd_set_graphs, mgqd_set_smem_vcycle, mgqd_set_tolerance,
+                  required_bytes)
 from ._lib import LIB_PATH, TrtError, check, lib  # noqa: F401

@@ -157,6 +157,7 @@ SIGNATURES = {
     "trt_mgqd_set_tolerance": (_i, [_d, _i]),
     "trt_mgqd_set_graphs": (_i, [_i]),
     "trt_mgqd_set_fused_levels": (_i, [_i]),
+    "trt_mgqd_set_smem_vcycle": (_i, [_i]),
     "trt_collapse_mg_ef": (_i, [_i, _i, _i] + [_D] * 5 + [_i] + [_D] * 5),
     "trt_cbar_calc": (_i, [_i, _i, _i] + [_D] * 15),
     "trt_old_grey_coefs": (_i, [_i, _i, _i, _d, _d, _d, _d] + [_D] * 8),

@@ -291,6 +291,12 @@ def mgqd_set_fused_levels(on=True):
     check(_lib.lib().trt_mgqd_set_fused_levels(int(bool(on))), "mgqd_set_fused_levels")
 
 
+def mgqd_set_smem_vcycle(on=True):
+    """Run the multigrid levels of at most 64 x 64 cells in the shared-memory kernel (default) or in the tiled
+    level passes and the global-memory one-CTA kernel; the results are identical."""
+    check(_lib.lib().trt_mgqd_set_smem_vcycle(int(bool(on))), "mgqd_set_smem_vcycle")
+
+
 def mgqd_last_stats():
     """(device ms of the last MLOQD_FV solve without its copies, largest iteration count, device ms of
     its first matrix-vector product)."""

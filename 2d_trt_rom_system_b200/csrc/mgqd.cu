@@ -48,6 +48,7 @@ struct Settings {
   int maxit = 1000;
   bool graphs = true;   // replay BiCGSTAB iteration blocks as CUDA graphs
   bool fused = true;    // one tiled kernel per level and direction of the V-cycle (else one per half-sweep)
+  bool smem_vcycle = true;    // levels of at most 64^2 cells in small_vcycle_smem_kernel where they fit
 };
 Settings g_settings;
 
@@ -61,8 +62,10 @@ struct Solver {
   Coefs cf{};
   Krylov K{};
   LevelSet ls{};
-  int k0 = 0;
+  int k0 = 0;                 // first level of the one-CTA kernel in use (kS or kG)
+  int kS = 0, kG = 0;         // first level of small_vcycle_smem_kernel / of small_vcycle_kernel
   bool vsmem = false;         // the levels from k0 on run in small_vcycle_smem_kernel
+  bool vsmem_ok = false;      // they fit in shared memory
   size_t vsmem_bytes = 0;
   double *Fx = nullptr, *Fy = nullptr, *rpart = nullptr, *res = nullptr, *bcres = nullptr;
   int* h_done = nullptr;
@@ -72,7 +75,7 @@ struct Solver {
   bool time_matvec = true;          // time the first iteration's matrix-vector product (trt_mgqd_last_stats)
   bool use_graphs = true;           // replay iteration blocks as a CUDA graph
   bool use_fused = true;            // fused tiled level passes in the V-cycle
-  bool g_fused = true;              // the form the recorded graph was made with
+  bool g_fused = true, g_vsmem = true;   // the forms the recorded graph was made with
   bool update_test = false;         // SPARSKIT's solution-update stopping test (Krylov::update_test)
   cudaGraphExec_t gexec = nullptr;  // kCheckEvery iterations, recorded on first use
   int g_nodes = 0, g_maxit = -1, g_rel = -1;
@@ -174,17 +177,17 @@ int Solver::init(int nx, int ny, int ng, bool own_inputs) {
     mx = (mx + 1) / 2;
     my = (my + 1) / 2;
   }
-  k0 = 0;
-  while (ls.L[k0].n > kSmallCellsSmem) ++k0;
-  vsmem_bytes = small_vcycle_smem_bytes(ls, k0);
-  vsmem = vsmem_bytes <= kSmemMax &&
+  kS = 0;
+  while (ls.L[kS].n > kSmallCellsSmem) ++kS;
+  kG = 0;
+  while (ls.L[kG].n > kSmallCells) ++kG;
+  vsmem_bytes = small_vcycle_smem_bytes(ls, kS);
+  vsmem_ok = vsmem_bytes <= kSmemMax &&
           cudaFuncSetAttribute(small_vcycle_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kSmemMax) == cudaSuccess;   // one bound for every solver's launches
-  if (!vsmem) {
-    cudaGetLastError();
-    k0 = 0;
-    while (ls.L[k0].n > kSmallCells) ++k0;
-  }
+  if (!vsmem_ok) cudaGetLastError();
+  vsmem = vsmem_ok;
+  k0 = vsmem ? kS : kG;
   MG_CUDA(cudaMallocHost(&h_done, sizeof(int) * ng));
   MG_CUDA(cudaMallocHost(&h_scal, sizeof(Scal) * ng));
   return TRT_OK;
@@ -223,6 +226,8 @@ int Solver::krylov(cudaStream_t s) {
   K.atol = 1e-15;   // fpar(2) of QD_SOLVERS.f08:445
   use_graphs = g_settings.graphs;
   use_fused = g_settings.fused;
+  vsmem = vsmem_ok && g_settings.smem_vcycle;
+  k0 = vsmem ? kS : kG;
   prec_coef_kernel<<<gpos, kRedBlock, 0, s>>>(d, cf, ls.L[0]);
   MG_LAUNCHED();
   for (int k = 0; k + 1 < ls.n; ++k) {
@@ -324,7 +329,8 @@ int Solver::krylov(cudaStream_t s) {
   // kernels take the solver's fixed buffers and K by value, so the graph is recorded again only when the
   // tolerance or the iteration limit in K changes.
   auto block = [&]() -> int {
-    if (!gexec || g_tol != K.tol || g_maxit != K.maxit || g_rel != K.update_test || g_fused != use_fused) {
+    if (!gexec || g_tol != K.tol || g_maxit != K.maxit || g_rel != K.update_test || g_fused != use_fused ||
+        g_vsmem != vsmem) {
       if (gexec) {
         cudaGraphExecDestroy(gexec);
         gexec = nullptr;
@@ -354,6 +360,7 @@ int Solver::krylov(cudaStream_t s) {
       g_maxit = K.maxit;
       g_rel = K.update_test;
       g_fused = use_fused;
+      g_vsmem = vsmem;
     }
     MG_CUDA(cudaGraphLaunch(gexec, s));
     trt_host::add_launches((unsigned long long)g_nodes);
@@ -475,6 +482,12 @@ int trt_mgqd_set_graphs(int on) {
 int trt_mgqd_set_fused_levels(int on) {
   std::lock_guard<std::mutex> lk(g_cache.mu);
   g_settings.fused = on != 0;
+  return TRT_OK;
+}
+
+int trt_mgqd_set_smem_vcycle(int on) {
+  std::lock_guard<std::mutex> lk(g_cache.mu);
+  g_settings.smem_vcycle = on != 0;
   return TRT_OK;
 }
 

@@ -590,12 +590,32 @@ __global__ void __launch_bounds__(1024) small_vcycle_smem_kernel(const LevelSet 
     }
   };
   float* v = vsm;
+  // Cells c = t, t + n, ... of a level with mx columns as (column i, row j), advanced by (di, dj) without a
+  // division per cell.
+  struct Walk {
+    int c, i, j, di, dj, mx;
+    __device__ Walk(int t, int n, int mx_) : c(t), mx(mx_) {
+      j = t / mx_;
+      i = t - j * mx_;
+      dj = n / mx_;
+      di = n - dj * mx_;
+    }
+    __device__ void next(int n) {
+      c += n;
+      i += di;
+      j += dj;
+      if (i >= mx) {
+        i -= mx;
+        ++j;
+      }
+    }
+  };
   // one colour of a red-black sweep; zero: the iterate is zero (this colour takes b/sC, the other is cleared)
   auto sweep = [&](const Team& tm, const SLevel& L, int color, bool zero) {
     if (zero) {
-      for (int c = tm.t; c < L.n; c += tm.n) {
-        const int j = c / L.mx, i = c - j * L.mx;
-        v[L.ox + c] = ((i + j) & 1) == color ? v[L.ob + c] / v[L.oC + c] : 0.f;
+      for (Walk w(tm.t, tm.n, L.mx); w.c < L.n; w.next(tm.n)) {
+        const int c = w.c;
+        v[L.ox + c] = ((w.i + w.j) & 1) == color ? v[L.ob + c] / v[L.oC + c] : 0.f;
       }
     } else {
       const int hx = (L.mx + 1) >> 1;   // cells of one colour per row, at most
@@ -624,8 +644,8 @@ __global__ void __launch_bounds__(1024) small_vcycle_smem_kernel(const LevelSet 
     }
   };
   auto restrict_to = [&](const Team& tm, const SLevel& F, const SLevel& Cs) {   // F's residual -> Cs's b
-    for (int c = tm.t; c < Cs.n; c += tm.n) {
-      const int J = c / Cs.mx, I = c - J * Cs.mx;
+    for (Walk w(tm.t, tm.n, Cs.mx); w.c < Cs.n; w.next(tm.n)) {
+      const int c = w.c, J = w.j, I = w.i;
       float r = 0.f;
       for (int dj = 0; dj < 2; ++dj)
         for (int di = 0; di < 2; ++di) {
@@ -639,10 +659,7 @@ __global__ void __launch_bounds__(1024) small_vcycle_smem_kernel(const LevelSet 
     tm.sync();
   };
   auto prolong_from = [&](const Team& tm, const SLevel& F, const SLevel& Cs) {   // F += Cs's correction
-    for (int c = tm.t; c < F.n; c += tm.n) {
-      const int j = c / F.mx, i = c - j * F.mx;
-      v[F.ox + c] += v[Cs.ox + (i >> 1) + Cs.mx * (j >> 1)];
-    }
+    for (Walk w(tm.t, tm.n, F.mx); w.c < F.n; w.next(tm.n)) v[F.ox + w.c] += v[Cs.ox + (w.i >> 1) + Cs.mx * (w.j >> 1)];
     tm.sync();
   };
   int kw = last;   // levels kw .. last have at most 64 cells each
@@ -659,7 +676,36 @@ __global__ void __launch_bounds__(1024) small_vcycle_smem_kernel(const LevelSet 
       smooth(w0, F, nu1, true);
       restrict_to(w0, F, Cs);
     }
-    smooth(w0, S[last], coarse_sweeps, true);
+    const SLevel Lc = S[last];
+    if (Lc.n <= 32) {
+      // The coarsest level (at most 2 x 2 cells) in registers: lane c owns cell c and reads its neighbours'
+      // iterates by shuffles; the half-sweeps take the smem sweep's operations in its order.
+      const int c = tid;
+      const bool own = c < Lc.n;
+      const int j = own ? c / Lc.mx : 0, i = own ? c - j * Lc.mx : 0;
+      const float cC = own ? v[Lc.oC + c] : 1.f, cW = own ? v[Lc.oW + c] : 0.f, cE = own ? v[Lc.oE + c] : 0.f;
+      const float cS = own ? v[Lc.oS + c] : 0.f, cN = own ? v[Lc.oN + c] : 0.f, b = own ? v[Lc.ob + c] : 0.f;
+      const int lw = c >= 1 ? c - 1 : c, le = c + 1 < 32 ? c + 1 : c;
+      const int ls_ = c >= Lc.mx ? c - Lc.mx : c, ln = c + Lc.mx < 32 ? c + Lc.mx : c;
+      float x = own && ((i + j) & 1) == 0 ? b / cC : 0.f;
+      for (int sw = 0; sw < coarse_sweeps; ++sw)
+        for (int color = sw == 0 ? 1 : 0; color < 2; ++color) {
+          const float xW = __shfl_sync(0xffffffffu, x, lw), xE = __shfl_sync(0xffffffffu, x, le);
+          const float xS = __shfl_sync(0xffffffffu, x, ls_), xN = __shfl_sync(0xffffffffu, x, ln);
+          if (own && ((i + j) & 1) == color) {
+            float s = 0.f;
+            if (i > 0) s += cW * xW;
+            if (i + 1 < Lc.mx) s += cE * xE;
+            if (j > 0) s += cS * xS;
+            if (j + 1 < Lc.my) s += cN * xN;
+            x = (b - s) / cC;
+          }
+        }
+      if (own) v[Lc.ox + c] = x;
+      __syncwarp();
+    } else {
+      smooth(w0, Lc, coarse_sweeps, true);
+    }
     for (int k = last - 1; k >= kw; --k) {
       const SLevel F = S[k], Cs = S[k + 1];
       prolong_from(w0, F, Cs);

@@ -1277,24 +1277,28 @@ __global__ void check_maps_kernel(const int* __restrict__ gmap, const int* __res
     if (vmap[k] < 1 || vmap[k] > glen1 || gmap[k] < 1 || gmap[k] > 2 * glen1 - 1) atomicOr(bad, 1);
 }
 
-// A set whose grids and maps already live on the device: its maps are checked on the device (one pass, the
-// verdict read back) before any FMAP reads through them.
-int device_set(Dev& dv, const MapSet& s, DevSet& d, cudaStream_t st) {
-  if (!s.dat || !s.sim || !s.gmap || !s.vmap || s.glen1 < 1 || s.glen2 < 1 || 2 * s.glen1 > INT_MAX ||
-      4 * s.glen2 > INT_MAX)
-    return TRT_ERR_ARG;
+// Sets whose grids and maps already live on the device: their maps are checked on the device (one pass per set,
+// one verdict for all of them read back with a single synchronisation) before any FMAP reads through them.
+int device_sets(Dev& dv, const MapSet* s, DevSet* d, int n, cudaStream_t st) {
+  for (int k = 0; k < n; ++k)
+    if (!s[k].dat || !s[k].sim || !s[k].gmap || !s[k].vmap || s[k].glen1 < 1 || s[k].glen2 < 1 ||
+        2 * s[k].glen1 > INT_MAX || 4 * s[k].glen2 > INT_MAX)
+      return TRT_ERR_ARG;
   int* bad;
   int rc = dv.get(&bad, 1);
   if (rc) return rc;
   ROM_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), st));
-  check_maps_kernel<<<grid_of(4 * s.glen2), 256, 0, st>>>(s.gmap, s.vmap, 4 * s.glen2, (int)s.glen1, bad);
-  trt_host::add_launches(1);
-  ROM_CUDA(cudaGetLastError());
+  for (int k = 0; k < n; ++k) {
+    check_maps_kernel<<<grid_of(4 * s[k].glen2), 256, 0, st>>>(s[k].gmap, s[k].vmap, 4 * s[k].glen2, (int)s[k].glen1,
+                                                               bad);
+    trt_host::add_launches(1);
+    ROM_CUDA(cudaGetLastError());
+  }
   int hbad = 0;
   ROM_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
   ROM_CUDA(cudaStreamSynchronize(st));
   if (hbad) return TRT_ERR_ARG;
-  d = {s.dat, s.sim, s.gmap, s.vmap, (int)s.glen1, (int)s.glen2};
+  for (int k = 0; k < n; ++k) d[k] = {s[k].dat, s[k].sim, s[k].gmap, s[k].vmap, (int)s[k].glen1, (int)s[k].glen2};
   return TRT_OK;
 }
 
@@ -1320,9 +1324,14 @@ int upload_set(Dev& dv, const MapSet& s, DevSet& d) {
   return TRT_OK;
 }
 
-// Host sets are checked and uploaded; resident ones are checked on the device.
-int make_set(Dev& dv, const MapSet& s, DevSet& d, bool resident, cudaStream_t st) {
-  return resident ? device_set(dv, s, d, st) : upload_set(dv, s, d);
+// Host sets are checked and uploaded; resident ones are checked on the device, all n with one synchronisation.
+int make_sets(Dev& dv, const MapSet* s, DevSet* d, int n, bool resident, cudaStream_t st) {
+  if (resident) return device_sets(dv, s, d, n, st);
+  for (int k = 0; k < n; ++k) {
+    const int rc = upload_set(dv, s[k], d[k]);
+    if (rc) return rc;
+  }
+  return TRT_OK;
 }
 
 // FMAP of n_g blocks of the padded device field f2 (glen1 values each) into out (n_g glen2 values): a device
@@ -1390,8 +1399,7 @@ int fg_driver(Dev& dv, const Rec& rec, double* const out[6], int dN_x, int dN_y,
                         {dat[2], sim[2], gmap[2], vmap[2], (long long)(dN_x + 2) * (dN_y + 1), (long long)N_x * (N_y + 1)}};
   DevSet ds[3];
   int rc;
-  for (int i = 0; i < 3; ++i)
-    if ((rc = make_set(dv, ms[i], ds[i], resident, st))) return rc;
+  if ((rc = make_sets(dv, ms, ds, 3, resident, st))) return rc;
   double* f[6];
   for (int k = 0; k < 6; ++k)
     if ((rc = dv.get(&f[k], (size_t)lens[k])) || (rc = rec(k, lens[k], f[k]))) return rc;
@@ -1422,13 +1430,11 @@ int bcg_sets(Dev& dv, DevSet ds[4], int dN_x, int dN_y, int N_x, int N_y, const 
   const long long dat_off[4] = {0, 2LL * dN_y + 4, 2LL * (dN_y + dN_x) + 8, 4LL * dN_y + 2LL * dN_x + 12};
   const long long sim_off[4] = {0, 2LL * N_y, 2LL * (N_y + N_x), 4LL * N_y + 2LL * N_x};
   const long long map_off[4] = {0, 4LL * N_y, 4LL * (N_y + N_x), 8LL * N_y + 4LL * N_x};
-  int rc;
-  for (int s = 0; s < 4; ++s) {
-    const MapSet ms = {Dat_Grid_Bnds + dat_off[s], Sim_Grid_Bnds + sim_off[s], GMap + map_off[s], VMap + map_off[s],
-                       n[s] + 2, m[s]};
-    if ((rc = make_set(dv, ms, ds[s], resident, st))) return rc;
-  }
-  return TRT_OK;
+  MapSet ms[4];
+  for (int s = 0; s < 4; ++s)
+    ms[s] = {Dat_Grid_Bnds + dat_off[s], Sim_Grid_Bnds + sim_off[s], GMap + map_off[s], VMap + map_off[s], n[s] + 2,
+             m[s]};
+  return make_sets(dv, ms, ds, 4, resident, st);
 }
 
 int bcg_driver(Dev& dv, const double* BC, double* const out[4], int dN_x, int dN_y, int dN_g, int N_g,

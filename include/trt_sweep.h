@@ -214,6 +214,11 @@ int trt_mgqd_set_graphs(int on);
  * (on, the default) or as one kernel per half-sweep (0); the cell arithmetic and its order are the same, so the
  * results are identical. */
 int trt_mgqd_set_fused_levels(int on);
+/* No counterpart in the reference.  The multigrid levels of at most 64 x 64 cells run in one kernel per group
+ * that keeps them in shared memory (on, the default, where they fit in 200 KB) or the levels above 32 x 32 in
+ * the tiled level passes and the rest in a one-CTA kernel over global memory (0); the cell arithmetic and its
+ * order are the same, so the results are identical. */
+int trt_mgqd_set_smem_vcycle(int on);
 
 /* Of the last trt_mloqd_fv call: device time (ms, events around the solve, excluding host<->device
  * copies), the largest iteration count, and the device time of its first matrix-vector product (ms;

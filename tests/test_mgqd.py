@@ -207,6 +207,27 @@ def test_fused_level_passes_are_bit_identical(shape, oracle):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(96, 80, 4), (300, 140, 3)])
+def test_smem_vcycle_is_bit_identical(shape, oracle):
+    """The multigrid levels of at most 64 x 64 cells in the shared-memory kernel (its coarsest level solved in
+    registers by one warp) or in the tiled level passes and the global-memory one-CTA kernel: the same cell
+    arithmetic in the same order, so the same iterates bit for bit.  96 x 80 starts the shared-memory levels at
+    48 x 40 (a 2 x 2 coarsest level), 300 x 140 at 75 x 35 (ragged levels, a 2 x 1 coarsest level)."""
+    d, c, dt, th = make(*shape, 1.0, 23, False, oracle)
+    try:
+        pkg.mgqd_set_smem_vcycle(False)
+        a = call_device(d, c, dt, th)
+        pkg.mgqd_set_smem_vcycle(True)
+        b = call_device(d, c, dt, th)
+        b2 = call_device(d, c, dt, th)
+    finally:
+        pkg.mgqd_set_smem_vcycle(True)
+    assert (a["MGQD_Kits"] > 4).all()
+    for k in ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH", "MGQD_Residual", "MGQD_Kits"):
+        assert np.array_equal(a[k], b[k]) and np.array_equal(b[k], b2[k]), k
+
+
+@pytest.mark.gpu
 def test_device_mloqd_fv_reports_non_convergence(oracle):
     d, c, dt, th = make(16, 16, 3, 1.0, 13, True, oracle)
     try:
