@@ -563,10 +563,22 @@ void fill_dirtab(const trt_ctx* c, std::vector<Real>& tab, std::vector<double>& 
   }
 }
 
+// The step's material handed to the handle in one pass over SMs (a device-to-device cudaMemcpyAsync runs on a
+// copy engine, about 1 ms for C1's four planes): the FP64 copies (kap64, q64; skipped when null, i.e. the
+// sources are those arrays already) and the sweep's Real copies.
 template <class Real>
-__global__ void cast_kernel(long long n, const double* __restrict__ src, Real* __restrict__ dst) {
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-    dst[k] = (Real)src[k];
+__global__ void material_copy_kernel(long long n, const double* __restrict__ kin, const double* __restrict__ qin,
+                                     double* __restrict__ kap64, double* __restrict__ q64, Real* __restrict__ kapR,
+                                     Real* __restrict__ qR) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const double a = kin[k], b = qin[k];
+    if (kap64) {
+      kap64[k] = a;
+      q64[k] = b;
+    }
+    kapR[k] = (Real)a;
+    qR[k] = (Real)b;
+  }
 }
 
 int ensure_stage(trt_ctx* c) {
@@ -754,19 +766,17 @@ int sweep_epilogue(trt_ctx* c, unsigned flags) {
 template <class Real>
 int set_material_impl(trt_ctx* c, const double* kap, const double* q, bool device) {
   const size_t n = (size_t)c->nx * c->ny * c->ng;
-  const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  TRT_CUDA(cudaMemcpyAsync(c->d_kap64, kap, n * sizeof(double), kind, c->stream));
-  TRT_CUDA(cudaMemcpyAsync(c->d_q64, q, n * sizeof(double), kind, c->stream));
-  if (sizeof(Real) == sizeof(double)) {
-    TRT_CUDA(cudaMemcpyAsync(c->d_kap, c->d_kap64, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    TRT_CUDA(cudaMemcpyAsync(c->d_q, c->d_q64, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  if (device) {
+    material_copy_kernel<Real><<<grid_for(n), 256, 0, c->stream>>>(n, kap, q, c->d_kap64, c->d_q64, (Real*)c->d_kap,
+                                                                   (Real*)c->d_q);
   } else {
-    cast_kernel<float><<<grid_for(n), 256, 0, c->stream>>>(n, c->d_kap64, (float*)c->d_kap);
-    TRT_LAUNCHED();
-    cast_kernel<float><<<grid_for(n), 256, 0, c->stream>>>(n, c->d_q64, (float*)c->d_q);
-    TRT_LAUNCHED();
-    TRT_CUDA(cudaGetLastError());
+    TRT_CUDA(cudaMemcpyAsync(c->d_kap64, kap, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    TRT_CUDA(cudaMemcpyAsync(c->d_q64, q, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    material_copy_kernel<Real><<<grid_for(n), 256, 0, c->stream>>>(n, c->d_kap64, c->d_q64, nullptr, nullptr,
+                                                                   (Real*)c->d_kap, (Real*)c->d_q);
   }
+  TRT_LAUNCHED();
+  TRT_CUDA(cudaGetLastError());
   if (!device) TRT_CUDA(cudaStreamSynchronize(c->stream));
   return TRT_OK;
 }
