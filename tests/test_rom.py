@@ -657,6 +657,21 @@ def test_pod_rom_through_the_reconstruction_drivers():
             assert st["sweeps"] == 0 and st["mgqd_nonconv"] == 0
             T = s.mlqd_field("Temp")
             assert float(np.max(np.abs(T - T_full[t - 1])) / np.max(T_full[t - 1])) < 1e-7
+    # one bad entry in the last of the three map sets (checked together on the device, one verdict): the call is
+    # refused before any FMAP reads through it, and the outputs are left untouched
+    bad = dict(dgr)
+    bad["VMap_xyEdgH"] = dgr["VMap_xyEdgH"].clone()
+    bad["VMap_xyEdgH"][-1] = 0
+    dout = {k: torch.full((snaps[k][0].size,), -7.0, dtype=torch.float64, device="cuda") for k in FACTORS[:6]}
+    rc = pkg.lib().trt_pod_reconstruct_fg_device(
+        *[P(dout[k]) for k in FACTORS[:6]], *[P(a) for k in names for a in ddec[k]],
+        *[dec[k][4].ctypes.data_as(I) for k in names], nx, ny, ng, nt, nx, ny, ng, nt, 1, 0,
+        *[P(bad[p + k]) for p in ("Sim_Grid_", "Dat_Grid_") for k in ("Avg", "EdgV", "EdgH")],
+        *[a.ctypes.data_as(D) for a in tg],
+        *[P(bad[p + k]) for p in ("GMap_xy", "VMap_xy") for k in ("Avg", "EdgV", "EdgH")], tm.ctypes.data_as(I), None)
+    assert rc == pkg._lib.TRT_ERR_ARG
+    for k in FACTORS[:6]:
+        assert bool((dout[k] == -7.0).all()), k
 
 
 def test_rrank_calc_matches_oracle(oracle):
