@@ -28,7 +28,8 @@ __global__ void collapse_kernel(const Dims d, const double* __restrict__ Eg, con
                                 double* FH) {
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (pos >= d.npos()) return;
-  const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+  int i, j;
+  trt_mgqd::pos_ij(pos, d.nx, i, j);
   if (i < d.nx && j < d.ny) {
     const long k = i + (long)d.nx * j;
     double s = 0.0;
@@ -405,7 +406,8 @@ __global__ void egp_coef_kernel(const Egp e, const Dims d, const Coefs cf) {
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (pos >= d.npos()) return;
   const int nx = e.nx, ny = e.ny;
-  const int i = (int)(pos % (nx + 1)), j = (int)(pos / (nx + 1));
+  int i, j;
+  trt_mgqd::pos_ij(pos, nx, i, j);
   const double c = kEgpC, pi4 = 97.40909103400243723644033268870511;   // pi^4
   const double Qdt = 15.0 * e.Kap0 * c * e.aR / pi4;
   if (i < nx && j < ny) {
@@ -502,7 +504,8 @@ __global__ void __launch_bounds__(trt_mgqd::kRedBlock) egp_delta_kernel(const Eg
   double v[6] = {0, 0, 0, 0, 0, 0};
   const int nx = e.nx, ny = e.ny;
   if (pos < d.npos()) {
-    const int i = (int)(pos % (nx + 1)), j = (int)(pos / (nx + 1));
+    int i, j;
+    trt_mgqd::pos_ij(pos, nx, i, j);
     const double c = kEgpC;
     const double* dE = x;
     const double* dEV = x + d.oV();
@@ -577,7 +580,8 @@ __global__ void egp_safety_kernel(const Egp e, const Dims d, const double* __res
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (pos >= d.npos()) return;
   const int nx = e.nx, ny = e.ny;
-  const int i = (int)(pos % (nx + 1)), j = (int)(pos / (nx + 1));
+  int i, j;
+  trt_mgqd::pos_ij(pos, nx, i, j);
   int k = 0;
   if (i < nx && j < ny) {
     const long c = i + (long)nx * j;
@@ -601,7 +605,8 @@ __global__ void egp_update_kernel(const Egp e, const Dims d, double* x, double s
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (pos >= d.npos()) return;
   const int nx = e.nx, ny = e.ny;
-  const int i = (int)(pos % (nx + 1)), j = (int)(pos / (nx + 1));
+  int i, j;
+  trt_mgqd::pos_ij(pos, nx, i, j);
   const double c = kEgpC, pi4 = 97.40909103400243723644033268870511;
   if (i < nx && j < ny) {
     const long k = i + (long)nx * j;

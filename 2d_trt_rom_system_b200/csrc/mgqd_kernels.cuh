@@ -39,6 +39,15 @@ namespace trt_mgqd {
 constexpr int kMaxLevels = 16;
 constexpr int kRedBlock = 256;   // threads of every reducing kernel
 
+// Column i and row j of position pos in a group's (nx + 1) x (ny + 1) position grid, in 32-bit arithmetic: a
+// group's positions number fewer than 2^31, and a 64-bit division costs several times the instructions.
+__device__ __forceinline__ void pos_ij(long pos, int nx, int& i, int& j) {
+  const unsigned p = (unsigned)pos, w = (unsigned)nx + 1u;
+  const unsigned q = p / w;
+  j = (int)q;
+  i = (int)(p - q * w);
+}
+
 struct Dims {
   int nx, ny, ng;
   long nC, nV, nH, nU;   // per-group sizes
@@ -104,7 +113,8 @@ __global__ void coef_kernel(const Inputs in, const Dims d, const Coefs cf) {
   const int g = blockIdx.y;
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (pos >= d.npos()) return;
-  const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+  int i, j;
+  pos_ij(pos, d.nx, i, j);
   const int nx = d.nx, ny = d.ny;
   const double c = in.c;
   const long gC = d.nC * g, gV = d.nV * g, gH = d.nH * g;
@@ -214,7 +224,8 @@ __global__ void prec_coef_kernel(const Dims d, const Coefs cf, const Level L0) {
   const int g = blockIdx.y;
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (pos >= d.npos()) return;
-  const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+  int i, j;
+  pos_ij(pos, d.nx, i, j);
   if (j < d.ny) {
     double a, bl, br;
     edgeV_elim(cf, d, g, i, j, &a, &bl, &br);
@@ -860,7 +871,8 @@ __global__ void __launch_bounds__(kRedBlock) init_kernel(const Coefs cf, const D
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
   double v3[3] = {0.0, 0.0, 0.0};
   if (pos < d.npos()) {
-    const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+    int i, j;
+    pos_ij(pos, d.nx, i, j);
     const RowOut o = apply_rows(cf, d, g, i, j, K.x);
     const long base = d.nU * g;
     auto emit = [&](bool has, long u, double y, int kind, long e) {
@@ -915,7 +927,8 @@ __global__ void elim_kernel(const Coefs cf, const Dims d, const Krylov K, const 
   if (K.done[g]) return;
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (pos >= d.npos()) return;
-  const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+  int i, j;
+  pos_ij(pos, d.nx, i, j);
   const int nx = d.nx, ny = d.ny;
   const long base = d.nU * g;
   const Scal sc = K.sc[g];
@@ -945,7 +958,8 @@ __global__ void backsub_kernel(const Coefs cf, const Dims d, const Krylov K, con
   if (K.done[g]) return;
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (pos >= d.npos()) return;
-  const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+  int i, j;
+  pos_ij(pos, d.nx, i, j);
   const int nx = d.nx, ny = d.ny;
   const long base = d.nU * g;
   const float* xc = L0.x + d.nC * g;
@@ -975,7 +989,8 @@ __global__ void __launch_bounds__(kRedBlock) matvec_kernel(const Coefs cf, const
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
   double v2[2] = {0.0, 0.0};
   if (pos < d.npos()) {
-    const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+    int i, j;
+    pos_ij(pos, d.nx, i, j);
     const RowOut o = apply_rows(cf, d, g, i, j, in);
     const long base = d.nU * g;
     auto emit = [&](bool has, long u, double y) {
@@ -1021,7 +1036,8 @@ __global__ void __launch_bounds__(kRedBlock) update_kernel(const Coefs cf, const
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
   double v5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   if (pos < d.npos()) {
-    const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+    int i, j;
+    pos_ij(pos, d.nx, i, j);
     const Scal sc = K.sc[g];
     const long base = d.nU * g;
     auto emit = [&](long u, int kind, long e) {
@@ -1089,7 +1105,8 @@ __global__ void flux_kernel(const Inputs in, const Dims d, const Coefs cf, const
   const int g = blockIdx.y;
   const long pos = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (pos >= d.npos()) return;
-  const int i = (int)(pos % (d.nx + 1)), j = (int)(pos / (d.nx + 1));
+  int i, j;
+  pos_ij(pos, d.nx, i, j);
   const int nx = d.nx, ny = d.ny;
   const double c = in.c;
   const double* E = x + d.nU * g;
@@ -1151,7 +1168,8 @@ __global__ void __launch_bounds__(kRedBlock) residual_kernel(const Inputs in, co
   for (int q = 0; q < kNRes; ++q) v[q] = 0.0;
   const int nx = d.nx, ny = d.ny;
   if (pos < d.npos()) {
-    const int i = (int)(pos % (nx + 1)), j = (int)(pos / (nx + 1));
+    int i, j;
+    pos_ij(pos, nx, i, j);
     const double c = in.c, th = in.Theta, dt = in.Delt;
     const double* E = x + d.nU * g;
     const double* EV = E + d.oV();
