@@ -102,7 +102,9 @@ struct Solver {
     return TRT_OK;
   }
   int init(int nx, int ny, int ng, bool own_inputs = true);   // own_inputs: allocate the Inputs planes
-  int solve(cudaStream_t s);    // MLOQD_FV: coefficients, Krylov solve, fluxes, residuals
+  // MLOQD_FV: coefficients, Krylov solve, fluxes, and the residual norms when residuals is set (the reference
+  // forms them under Res_Calc only, as diagnostics)
+  int solve(cudaStream_t s, bool residuals = true);
   int krylov(cudaStream_t s);   // the solve of whatever system the coefficient planes hold
   int pos_blocks() const { return (int)((d.npos() + kRedBlock - 1) / kRedBlock); }
 };
@@ -196,7 +198,7 @@ int Solver::init(int nx, int ny, int ng, bool own_inputs) {
 int grid1(long n) { return (int)((n + 255) / 256); }
 
 // MLOQD_FV on the device; inputs and the initial guess (K.x) already uploaded.
-int Solver::solve(cudaStream_t s) {
+int Solver::solve(cudaStream_t s, bool residuals) {
   const dim3 gpos(pos_blocks(), d.ng);
   const int nblk = pos_blocks();
   coef_kernel<<<gpos, kRedBlock, 0, s>>>(in, d, cf);
@@ -206,6 +208,7 @@ int Solver::solve(cudaStream_t s) {
   const Outputs out{Fx, Fy};
   flux_kernel<<<gpos, kRedBlock, 0, s>>>(in, d, cf, K.x, out);
   MG_LAUNCHED();
+  if (!residuals) return TRT_OK;
   residual_kernel<<<gpos, kRedBlock, 0, s>>>(in, d, K.x, out, rpart);
   MG_LAUNCHED();
   residual_finish_kernel<<<d.ng, 32, 0, s>>>(rpart, nblk, d.ng, res, bcres);
@@ -563,7 +566,7 @@ int trt_mloqd_fv(int n_x, int n_y, int n_g, double* Eg_avg, double* Eg_edgV, dou
   MG_CUDA(cudaMemcpy2DAsync(S->K.x + d.oH(), pitch, Eg_edgH, d.nH * sizeof(double), d.nH * sizeof(double), n_g,
                             cudaMemcpyHostToDevice, st));
   MG_CUDA(cudaEventRecord(S->e0, st));
-  if ((rc = S->solve(st))) return rc;
+  if ((rc = S->solve(st, Res_Calc != 0))) return rc;
   MG_CUDA(cudaEventRecord(S->e1, st));
   MG_CUDA(cudaMemcpy2DAsync(Eg_avg, d.nC * sizeof(double), S->K.x, pitch, d.nC * sizeof(double), n_g,
                             cudaMemcpyDeviceToHost, st));
@@ -1420,7 +1423,7 @@ int ph_mgqd_local(Mlqd& m, double* part) {
   cudaStream_t st = v.stream;
   int rc;
   MG_CUDA(cudaEventRecord(m.ev[4], st));
-  if ((rc = m.MG->solve(st))) return rc;
+  if ((rc = m.MG->solve(st, false))) return rc;   // the time step reports no MGQD residuals
   MG_CUDA(cudaEventRecord(m.ev[5], st));
   MG_CUDA(cudaMemcpyAsync(m.MG->h_scal, m.MG->K.sc, sizeof(Scal) * ng, cudaMemcpyDeviceToHost, st));
   if ((rc = unknowns_to_fields(m, st))) return rc;

@@ -228,6 +228,19 @@ def test_smem_vcycle_is_bit_identical(shape, oracle):
 
 
 @pytest.mark.gpu
+def test_res_calc_off_skips_only_the_residuals(oracle):
+    """Res_Calc = .FALSE.: the same solution and fluxes bit for bit, and MGQD_Residual / MGQD_BC_Residual left as
+    the caller passed them (the reference forms them under Res_Calc only)."""
+    d, c, dt, th = make(20, 16, 3, 1.0, 29, False, oracle)
+    a = call_device(d, c, dt, th, res_calc=True)
+    b = call_device(d, c, dt, th, res_calc=False)
+    for k in ("Eg_avg", "Eg_edgV", "Eg_edgH", "Fxg_edgV", "Fyg_edgH", "MGQD_Kits"):
+        assert np.array_equal(a[k], b[k]), k
+    assert np.any(a["MGQD_Residual"] != 0.0)
+    assert not np.any(b["MGQD_Residual"]) and not np.any(b["MGQD_BC_Residual"])
+
+
+@pytest.mark.gpu
 def test_device_mloqd_fv_reports_non_convergence(oracle):
     d, c, dt, th = make(16, 16, 3, 1.0, 13, True, oracle)
     try:
