@@ -1067,8 +1067,33 @@ struct Mlqd {
 
 void mlqd_release(void* p) { delete static_cast<Mlqd*>(p); }
 
+// Device copies of the time step run on the SMs: a device-to-device cudaMemcpy(2D)Async goes to a copy engine,
+// which moves a few hundred GB/s and adds its own latency to each of the step's many small copies.
+__global__ void copy_kernel(double* __restrict__ dst, const double* __restrict__ src, long n) {
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) dst[k] = src[k];
+}
+
+// The three fields of every group between the solver's unknown layout (one [E_avg | E_edgV | E_edgH] segment of
+// nU values per group) and the reference layouts (group-major planes of nC, nV, nH values); to_fields picks the
+// direction.
+__global__ void unknowns_fields_kernel(const Dims d, double* __restrict__ x, double* __restrict__ Eg,
+                                       double* __restrict__ EgV, double* __restrict__ EgH, int to_fields) {
+  const int g = blockIdx.y;
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < d.nU; k += (long)gridDim.x * blockDim.x) {
+    double* f = k < d.nC ? Eg + d.nC * g + k
+                         : (k < d.nC + d.nV ? EgV + d.nV * g + (k - d.nC) : EgH + d.nH * g + (k - d.nC - d.nV));
+    double* u = x + d.nU * g + k;
+    if (to_fields) *f = *u;
+    else *u = *f;
+  }
+}
+
+int copy_grid(long n) { return (int)std::min<long>((n + 255) / 256, 148L * 8); }
+
 int d2d(double* dst, const double* src, size_t n, cudaStream_t st) {
-  MG_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  if (n == 0) return TRT_OK;
+  copy_kernel<<<copy_grid((long)n), 256, 0, st>>>(dst, src, (long)n);
+  MG_LAUNCHED();
   return TRT_OK;
 }
 
@@ -1078,29 +1103,17 @@ int h2d(double* dst, const std::vector<double>& src, cudaStream_t st) {
 }
 
 // MLOQD_FV's solution in the unknown layout <-> the reference layouts (one strided copy per field).
-int unknowns_to_fields(const Mlqd& m, cudaStream_t st) {
+int unknowns_fields(const Mlqd& m, cudaStream_t st, int to_fields) {
   const Dims& d = m.d;
-  const size_t pitch = (size_t)d.nU * sizeof(double);
-  MG_CUDA(cudaMemcpy2DAsync(m.Eg, d.nC * sizeof(double), m.MG->K.x, pitch, d.nC * sizeof(double), d.ng,
-                            cudaMemcpyDeviceToDevice, st));
-  MG_CUDA(cudaMemcpy2DAsync(m.EgV, d.nV * sizeof(double), m.MG->K.x + d.oV(), pitch, d.nV * sizeof(double), d.ng,
-                            cudaMemcpyDeviceToDevice, st));
-  MG_CUDA(cudaMemcpy2DAsync(m.EgH, d.nH * sizeof(double), m.MG->K.x + d.oH(), pitch, d.nH * sizeof(double), d.ng,
-                            cudaMemcpyDeviceToDevice, st));
+  const int per_group = (int)std::max<long>(1, std::min<long>((d.nU + 255) / 256, (148L * 8 + d.ng - 1) / d.ng));
+  unknowns_fields_kernel<<<dim3(per_group, d.ng), 256, 0, st>>>(d, m.MG->K.x, m.Eg, m.EgV, m.EgH, to_fields);
+  MG_LAUNCHED();
   return TRT_OK;
 }
 
-int fields_to_unknowns(const Mlqd& m, cudaStream_t st) {
-  const Dims& d = m.d;
-  const size_t pitch = (size_t)d.nU * sizeof(double);
-  MG_CUDA(cudaMemcpy2DAsync(m.MG->K.x, pitch, m.Eg, d.nC * sizeof(double), d.nC * sizeof(double), d.ng,
-                            cudaMemcpyDeviceToDevice, st));
-  MG_CUDA(cudaMemcpy2DAsync(m.MG->K.x + d.oV(), pitch, m.EgV, d.nV * sizeof(double), d.nV * sizeof(double), d.ng,
-                            cudaMemcpyDeviceToDevice, st));
-  MG_CUDA(cudaMemcpy2DAsync(m.MG->K.x + d.oH(), pitch, m.EgH, d.nH * sizeof(double), d.nH * sizeof(double), d.ng,
-                            cudaMemcpyDeviceToDevice, st));
-  return TRT_OK;
-}
+int unknowns_to_fields(const Mlqd& m, cudaStream_t st) { return unknowns_fields(m, st, 1); }
+
+int fields_to_unknowns(const Mlqd& m, cudaStream_t st) { return unknowns_fields(m, st, 0); }
 
 // ng_total > 0: the handle holds groups g_first .. g_first + ng - 1 of an instance of ng_total groups whose
 // group edges are nu_total (ng_total + 1 values); the initial grey fields and incoming energies are the sums
